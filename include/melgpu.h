@@ -1,0 +1,247 @@
+/*
+ * melgpu.h -- C ABI of the B200 solver for the MELODY 2D explicit-dynamics step.
+ *
+ * The reference has no plugin or FFI: its step is the C++ call
+ *   Euler_step(...)            Code/Solver.h:10-88   (dispatched at Code/main.cpp:148-155)
+ *   Solver_step(...)           Code/Solver.h:98-486  (dispatched at Code/main.cpp:156-167)
+ *   Update_proximity(...)      Code/Proximity.h:48-473 (called at Code/main.cpp:191-196)
+ * operating in place on `vector<Body>` filled by Load_static (Code/IO.h:598) and
+ * Load_dynamic (Code/IO.h:1871).  This header is the seam that replaces those calls:
+ * a host main of the same shape as Code/main.cpp loads the same input files, hands the
+ * flattened model to mel_create / mel_create_from_files, advances it with mel_step and
+ * reads state back with mel_download at monitoring / save cadence.
+ *
+ * Conventions: plain C, host pointers and counts only; the library owns all device memory;
+ * every call returns a mel_status; one host thread per handle; one CUDA stream per handle.
+ * Node, border and Gauss-point indices inside a body are body-local, exactly as in the
+ * reference input files.
+ */
+#ifndef MELGPU_H
+#define MELGPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MELGPU_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+typedef enum {
+    MEL_OK = 0,
+    MEL_ERR_INVALID = 1,      /* bad argument or malformed model description          */
+    MEL_ERR_UNSUPPORTED = 2,  /* valid reference input this build does not run yet    */
+    MEL_ERR_CUDA = 3,         /* CUDA runtime error (message in mel_last_error_string) */
+    MEL_ERR_OOM = 4,          /* device allocation failed                              */
+    MEL_ERR_NAN = 5,          /* non-finite state detected (Code/main.cpp:227-237)     */
+    MEL_ERR_BOUNDS = 6,       /* device-side index check failed                        */
+    MEL_ERR_TIMEOUT = 7,      /* a bounded device wait gave up                         */
+    MEL_ERR_IO = 8,           /* input file missing or unreadable                      */
+    MEL_ERR_NO_DEVICE = 9     /* no CUDA device                                        */
+} mel_status;
+
+/* ---- enumerations mirroring the reference's string tags ---------------------------- */
+enum { MEL_BODY_DEFORMABLE = 0, MEL_BODY_RIGID = 1 };                 /* Body::type        */
+enum { MEL_STATUS_ACTIVE = 0, MEL_STATUS_INACTIVE = 1, MEL_STATUS_NOGRAVITY = 2 }; /* Body::status */
+enum { MEL_PER_CLOSED = 0, MEL_PER_SIMPLE = 1, MEL_PER_PERIODIC = 2 };  /* Border/Body periodicity */
+enum { MEL_INTERP_LINEAR = 0, MEL_INTERP_SPLINE = 1 };                 /* Border::interpolant */
+enum { MEL_BC_NONE = 0, MEL_BC_SOFT = 1, MEL_BC_DRIVEN = 2, MEL_BC_ORIENTED = 3, MEL_BC_FOLLOWING = 4 };
+enum { MEL_MAT_ELASTIC_LINEAR = 0, MEL_MAT_NEOHOOKEAN = 1 };
+enum { MEL_LAW_FRICTIONLESS = 0, MEL_LAW_COHESION = 1, MEL_LAW_MOHR_COULOMB = 2,
+       MEL_LAW_DAMPED_MOHR_COULOMB = 3, MEL_LAW_TWO_SLOPES_MOHR_COULOMB = 4,
+       MEL_LAW_BONDED_MOHR_COULOMB = 5, MEL_LAW_CZM_LINEAR = 6, MEL_LAW_CZM_FATIGUE = 7 };
+enum { MEL_LENGTH_FIXED = 0, MEL_LENGTH_EVOLUTIVE = 1 };
+enum { MEL_SOLVER_EULER = 0, MEL_SOLVER_ADAPTIVE_EULER = 1, MEL_SOLVER_MASS_SCALING = 2,
+       MEL_SOLVER_ADAPTIVE_MASS_SCALING = 3, MEL_SOLVER_EULER_2 = 4 };
+/* Arithmetic of the Gauss-point pass: all-FP64 drop-in, or FP32 shape-function
+ * derivatives / strain / stress with FP64 kinematics, gaps and nodal sums. */
+enum { MEL_PREC_FP64 = 0, MEL_PREC_MIXED = 1 };
+
+#define MEL_MAT_NPARAM   6   /* rho, alpha, beta, mu, lambda|kappa, heat_capacity  (Code/IO.h:672-685) */
+#define MEL_LAW_NPARAM  11   /* largest law: BondedMohrCoulomb                     (Code/IO.h:775-783) */
+#define MEL_RIGID_NF    20   /* see MEL_RG_* below                                                    */
+#define MEL_NFLAGS      11   /* DYNAMIC flags[0..10]                               (Code/IO.h:1912-1933) */
+#define MEL_NINTERNAL    3   /* Contact_element::internal values kept on device                         */
+
+/* Layout of one rigid-body record in mel_model_desc::rigid (Body.h:46-95 rigid attributes). */
+enum { MEL_RG_X0 = 0, MEL_RG_Y0, MEL_RG_R0, MEL_RG_MASS, MEL_RG_INERTIA, MEL_RG_INV_MASS, MEL_RG_INV_INERTIA,
+       MEL_RG_XC, MEL_RG_YC, MEL_RG_RC, MEL_RG_XD, MEL_RG_YD, MEL_RG_RD, MEL_RG_XV, MEL_RG_YV, MEL_RG_RV,
+       MEL_RG_XA, MEL_RG_YA, MEL_RG_RA, MEL_RG_PAD };
+
+/* Flattened model: the content of STATIC_CONTROL.asc + STATIC_DATA.asc + DYNAMIC_nnnnn.asc
+ * after Load_static / Load_dynamic, as structure-of-arrays.  All arrays are host memory
+ * owned by the caller and only read during mel_create. */
+typedef struct mel_model_desc {
+    int    abi_version;                 /* = MELGPU_ABI_VERSION */
+    /* scene (Code/IO.h:821-915, 1944-1953) */
+    double period[2];                   /* Xmin_period, Xmax_period */
+    double gravity[2];                  /* Xgravity, Ygravity */
+    double time, dt, tend;
+    double contact_update_period, next_contact_update;
+    int    solver;                      /* MEL_SOLVER_* */
+    double solver_params[8];            /* Target_error, Control_parameter, Accepted_ratio, Max_mass_scaling,
+                                           Control_parameter_mass_scaling, Error_factor_mass_scaling,
+                                           Decrease_factor_mass_scaling, Inv_Target_error */
+    int    flags[MEL_NFLAGS];
+    /* materials and contact laws (Code/IO.h:660-812) */
+    int           n_materials;
+    const int*    material_type;        /* [n_materials] MEL_MAT_* */
+    const double* material_params;      /* [n_materials*MEL_MAT_NPARAM] */
+    int           n_laws;
+    const int*    law_type;             /* [n_laws] MEL_LAW_* */
+    const int*    law_length;           /* [n_laws] MEL_LENGTH_* */
+    const double* law_params;           /* [n_laws*MEL_LAW_NPARAM] */
+    const int*    contacts_table;       /* [n_materials*n_materials], -1 = no law */
+    /* bodies (Code/IO.h:1013-1070, 1494-1520) */
+    int           n_bodies;
+    const int*    body_type;            /* MEL_BODY_* */
+    const int*    body_material;
+    const int*    body_periodic;        /* 1 when the body's type string is "Periodic" */
+    const int*    body_status;          /* MEL_STATUS_* */
+    const double* body_dist;            /* [n_bodies*3] nodal, detection, contact distance */
+    const int*    body_node_ptr;        /* [n_bodies+1] into node arrays */
+    const int*    body_border_ptr;      /* [n_bodies+1] into border arrays */
+    const int*    body_gp_ptr;          /* [n_bodies+1] into Gauss-point arrays */
+    const int*    body_cell_ptr;        /* [n_bodies+1] into cells */
+    const double* rigid;                /* [n_bodies*MEL_RIGID_NF] (ignored for deformable bodies) */
+    /* nodes of all bodies, body-contiguous (Node.h, Code/IO.h:1522-1630, 1796-1830) */
+    int           n_nodes;
+    const double* node_x0;              /* [2*n_nodes] x_initial, y_initial */
+    const double* node_mass;            /* [2*n_nodes] x_mass, y_mass */
+    const double* node_inv_mass;        /* [2*n_nodes] */
+    const double* node_domain;          /* [n_nodes] domain_size */
+    const int*    node_sup_ptr;         /* [n_nodes+1] DOF_TO_DISP supports (empty for rigid nodes) */
+    const int*    node_sup_idx;         /* body-local */
+    const double* node_sup_N;           /* shape function values */
+    const double* node_state;           /* [n_nodes*12]: u x,y  v x,y  a x,y  up x,y  vp x,y  ap x,y */
+    /* borders (Border.h; Code/IO.h:1072-1290, 1632-1660) */
+    int           n_borders;
+    const int*    border_body;
+    const int*    border_periodicity;   /* MEL_PER_* */
+    const int*    border_interpolant;   /* MEL_INTERP_* */
+    const int*    border_before;        /* body-local border index */
+    const int*    border_after;
+    const int*    border_node_ptr;      /* [n_borders+1] */
+    const int*    border_nodes;         /* body-local node index per border node */
+    const int*    border_bc_type;       /* [2*n_borders] x then y, MEL_BC_* */
+    const double* border_bc_param;      /* [4*n_borders] soft penalty,damping for x then y */
+    const int*    border_hist_ptr;      /* [2*n_borders+1] history of (border,dir) k is [ptr[k],ptr[k+1]) */
+    const double* hist_time;
+    const double* hist_value;
+    /* Gauss points (Code/IO.h:1662-1760) */
+    int           n_gauss;
+    const int*    gp_sup_ptr;           /* [n_gauss+1] */
+    const int*    gp_sup_idx;           /* body-local */
+    const double* gp_N;
+    const double* gp_dNdx;
+    const double* gp_dNdy;
+    const double* gp_weight;            /* [n_gauss] */
+    const double* gp_jacobian;          /* [n_gauss] */
+    /* background triangulation (rigid mass and inertia, Body.h:2871-2897) */
+    int           n_cells;
+    const int*    cells;                /* [3*n_cells] body-local */
+    /* damping matrix triplets (Code/IO.h:1832-1855): dof0, dof1 body-local dofs */
+    int           n_matrix;
+    const int*    body_matrix_ptr;      /* [n_bodies+1] or NULL when n_matrix == 0 */
+    const int*    matrix_dofs;          /* [2*n_matrix] */
+    const double* matrix_stiffness;
+    const double* matrix_damping;
+} mel_model_desc;
+
+/* One contact element (Contact_Element.h:5-55) in the reference's own field order. */
+typedef struct mel_contact {
+    int32_t bodyS, borderS, border_nodeS, nodeS;
+    int32_t bodyM, borderM, shiftM, segmentM;
+    int32_t nodeM[4], shiftMk[4];
+    double  shapeM[4];
+    double  gapn, vgapn, gapt, vgapt, xsi, xnorm, ynorm, xtan, ytan;
+    double  effective_mass, length, fx, fy;
+    int32_t nb_internal, pad_;
+    double  internal[MEL_NINTERNAL];
+} mel_contact;
+
+/* Step parameters and outputs of mel_step. */
+typedef struct mel_step_io {
+    int    nsteps;          /* accepted steps to take */
+    int    run_proximity;   /* 1: run Update_proximity when Time >= Next_contact_update (Code/main.cpp:191) */
+    double time;            /* out: Time after the call */
+    double dt;              /* out: Deltat after the call */
+    double next_contact_update; /* out */
+    int    n_contacts;      /* out: contact elements after the call */
+    int    n_proximity;     /* out: proximity updates performed */
+} mel_step_io;
+
+/* Parity quantities reduced on the device (Code/Monitoring.h). */
+typedef struct mel_monitor {
+    double time;
+    double kinetic_energy;          /* Σ ½ m v² over nodal velocities  (Monitoring.h:528-531) */
+    double mean_displacement[2];    /* mass-weighted over deformable nodes (Monitoring.h:88-101) */
+    double rigid_force[2*4];        /* first four rigid bodies: Σ contact force x,y  */
+    double rigid_dirichlet[2*4];    /* first four rigid bodies: driven-DOF reaction x,y (Body.h:2093,2105) */
+    int    active_contacts;         /* contact elements with nonzero force */
+    int    n_contacts;
+} mel_monitor;
+
+typedef struct mel_options {
+    int precision;          /* MEL_PREC_* */
+    int device;             /* CUDA device ordinal */
+    int use_graph;          /* capture the per-step launches in a CUDA graph */
+    int max_contacts;       /* capacity hint (0 = automatic) */
+} mel_options;
+
+typedef struct mel_handle mel_handle;
+
+/* ---- lifecycle -------------------------------------------------------------------- */
+/* Replaces Load_static + Load_dynamic + the initialisation block of Code/main.cpp:104-127
+ * (Update_borders, Update_bc, Update_proximity x2, Update_material). */
+mel_status mel_create(const mel_model_desc* desc, const mel_options* opt, mel_handle** out);
+/* Same, reading STATIC_CONTROL.asc / STATIC_DATA.asc / DYNAMIC_nnnnn.asc from `dir`
+ * (Code/IO.h:598, Code/IO.h:1871; `restart_index` is argv[1] of Code/main.cpp:94). */
+mel_status mel_create_from_files(const char* dir, int restart_index, const mel_options* opt, mel_handle** out);
+mel_status mel_destroy(mel_handle* h);
+
+/* ---- stepping --------------------------------------------------------------------- */
+/* io->nsteps iterations of the loop body of Code/main.cpp:141-238 restricted to the solver
+ * (Euler_step, Code/Solver.h:10-88) and the proximity update (Code/main.cpp:191-196). */
+mel_status mel_step(mel_handle* h, mel_step_io* io);
+/* Update_proximity (Code/Proximity.h:48-473) on the current positions. */
+mel_status mel_update_proximity(mel_handle* h);
+/* Replace the contact list (restart or host-side proximity; mirrors Load_dynamic CONTACTS). */
+mel_status mel_set_contacts(mel_handle* h, const mel_contact* contacts, int n);
+
+/* ---- state transfer --------------------------------------------------------------- */
+/* node_state layout as in mel_model_desc::node_state (12 doubles per node). */
+mel_status mel_get_node_state(mel_handle* h, double* node_state);
+mel_status mel_set_node_state(mel_handle* h, const double* node_state);
+/* current positions, 2 doubles per node */
+mel_status mel_get_positions(mel_handle* h, double* xy);
+/* nodal force components of the last step, [n_nodes*2] each; any pointer may be NULL.
+ * internal = Σ regions internal force (Node.h:216-222), contact, neumann, dirichlet, total. */
+mel_status mel_get_forces(mel_handle* h, double* internal, double* contact, double* neumann,
+                          double* dirichlet, double* total);
+mel_status mel_get_rigid(mel_handle* h, double* rigid /* [n_bodies*MEL_RIGID_NF] */,
+                         double* rigid_forces /* [n_bodies*12]: contact, body, dirichlet, neumann (x,y,r) */);
+/* works per body [n_bodies*7]: internal, contact, body, dirichlet, neumann, damping, alid (Body.h:111-117) */
+mel_status mel_get_works(mel_handle* h, double* works);
+mel_status mel_get_contact_count(mel_handle* h, int* n);
+mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* n);
+mel_status mel_get_time(mel_handle* h, double* time, double* dt);
+mel_status mel_monitor_compute(mel_handle* h, mel_monitor* out);
+
+/* ---- introspection ---------------------------------------------------------------- */
+const char* mel_last_error_string(void);
+int         mel_abi_version(void);
+/* Per-kernel timing of the last mel_step call, CUDA events on the handle's stream.
+ * names: "contact", "body", "rigid", "proximity"; returns total milliseconds. */
+mel_status  mel_get_kernel_times(mel_handle* h, double* ms_contact, double* ms_body,
+                                 double* ms_rigid, double* ms_proximity, int* launches);
+/* Sizes of the resident model. */
+mel_status  mel_get_sizes(mel_handle* h, int* n_bodies, int* n_nodes, int* n_gauss,
+                          int* n_gp_entries, int* n_node_entries, int* n_border_nodes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MELGPU_H */

@@ -1,0 +1,695 @@
+"""Seeded synthetic grain packings for the MELODY 2D step, written in the reference's formats.
+
+The reference preprocessor is MATLAB (Preprocessor/*.m) and cannot run here, so this module
+restates the parts of it the solver's inputs depend on:
+
+* Gauss points: 3-point triangle rule of Preprocessor/GaussCoefficientsTriangle.m:4-7 mapped by
+  Preprocessor/TriangleGaussPoints.m:17-27 (weights 1/3, jacobian = triangle area).
+* MLS shape functions with a linear basis and the cubic-spline weight W1:
+  Preprocessor/MLS2DWithDerivatives.m:65-165 and Preprocessor/WeightW1WithDerivatives.m:17-47.
+  The basis is expressed relative to the body centre, which leaves the MLS functions unchanged
+  and keeps the 3x3 moment matrix well conditioned.
+* Support domains: nodes whose influence radius covers the point
+  (Preprocessor/SupportDomain.m:16-18).
+* Lumped masses = row sums of the consistent mass matrix (Preprocessor/AnalyseSimpleBody.m:316-331).
+* Closed borders list their nodes counter-clockwise and repeat the first node at the end
+  (Preprocessor/SetUnstructuredNodesForClosedContour.m:154-159), border nodes first.
+* Rigid bodies: centre of mass, mass and inertia of Preprocessor/AnalyseRigidBody.m.
+
+File layout follows Preprocessor/ExportStatic.m and Preprocessor/ExportDynamic.m as read by
+Load_static (Code/IO.h:598-1861) and Load_dynamic (Code/IO.h:1871-2345).
+
+Deviations, all stated in DESIGN.md: the support radius is 2.0x the body's mean Delaunay edge
+length (the workload's definition) instead of the k-nearest-neighbour rule of
+AnalyseSimpleBody.m:64-68; interior nodes come from seeded rejection sampling instead of
+Distmesh; the large packings use a box enlarged to hold 2000 discs at random-sequential-addition
+density.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+from scipy.spatial import Delaunay, cKDTree
+
+# 3-point rule exactly as typed in Preprocessor/GaussCoefficientsTriangle.m:4-7
+_GAUSS3 = np.array([[0.16666666666667, 0.16666666666667, 0.33333333333333],
+                    [0.16666666666667, 0.66666666666667, 0.33333333333333],
+                    [0.66666666666667, 0.16666666666667, 0.33333333333333]])
+
+BC_NONE, BC_SOFT, BC_DRIVEN, BC_ORIENTED, BC_FOLLOWING = 0, 1, 2, 3, 4
+LAW_NAMES = ["Frictionless", "Cohesion", "MohrCoulomb", "DampedMohrCoulomb", "TwoSlopesMohrCoulomb",
+             "BondedMohrCoulomb", "CZMlinear", "CZMfatigue"]
+LAW_NPARAM_FILE = [1, 4, 5, 6, 6, 11, 6, 9]
+MAT_NAMES = ["ElasticLinear", "NeoHookean"]
+SOLVER_NAMES = ["Euler", "Adaptive_Euler", "Mass_Scaling", "Adaptive_Mass_Scaling", "Euler_2"]
+T_HIST_END = 1.0e3   # last instant of every boundary-condition history (s)
+
+
+# --------------------------------------------------------------------------------------------
+# MLS shape functions (Preprocessor/MLS2DWithDerivatives.m, WeightW1WithDerivatives.m)
+# --------------------------------------------------------------------------------------------
+
+def _w1(relx: np.ndarray, rely: np.ndarray, d: np.ndarray):
+    """Cubic-spline weight and its gradient with respect to the point of interest
+    (Preprocessor/WeightW1WithDerivatives.m:25-44); relx = x_point - x_node."""
+    rho = np.sqrt(relx * relx + rely * rely)
+    r = rho / d
+    w = np.zeros_like(r)
+    dwdx = np.zeros_like(r)
+    dwdy = np.zeros_like(r)
+    inner = r <= 0.5
+    outer = (r > 0.5) & (r <= 1.0)
+    w[inner] = (2.0 / 3.0) - 4.0 * r[inner] ** 2 + 4.0 * r[inner] ** 3
+    d3 = d ** 3
+    dwdx[inner] = (-8.0 * d[inner] * relx[inner] + 12.0 * relx[inner] * rho[inner]) / d3[inner]
+    dwdy[inner] = (-8.0 * d[inner] * rely[inner] + 12.0 * rely[inner] * rho[inner]) / d3[inner]
+    ro = r[outer]
+    w[outer] = (4.0 / 3.0) - 4.0 * ro + 4.0 * ro ** 2 - (4.0 / 3.0) * ro ** 3
+    # dw/dr * dr/dx with dw/dr = -4 + 8r - 4r^2 and dr/dx = x / (r d^2)
+    fac = 4.0 * (-1.0 + 2.0 * ro - ro * ro) / (ro * d[outer] ** 2)
+    dwdx[outer] = fac * relx[outer]
+    dwdy[outer] = fac * rely[outer]
+    return w, dwdx, dwdy
+
+
+def mls_shape(points: np.ndarray, nodes: np.ndarray, radii: np.ndarray, origin: np.ndarray):
+    """Linear-basis MLS shape functions N, dN/dx, dN/dy at `points` from `nodes` with influence
+    radii `radii` (Preprocessor/MLS2DWithDerivatives.m:65-165).
+
+    Returns (ptr, idx, N, dNdx, dNdy) in CSR form with support lists in ascending node order
+    (the order Preprocessor/SupportDomain.m:17-18 produces)."""
+    tree = cKDTree(nodes)
+    cand = tree.query_ball_point(points, r=float(radii.max()))
+    P = points.shape[0]
+    rows: List[np.ndarray] = []
+    for i in range(P):
+        c = np.asarray(sorted(cand[i]), dtype=np.int64)
+        dx = points[i, 0] - nodes[c, 0]
+        dy = points[i, 1] - nodes[c, 1]
+        keep = dx * dx + dy * dy - radii[c] ** 2 < 0.0
+        rows.append(c[keep])
+    counts = np.array([len(r) for r in rows], dtype=np.int64)
+    K = int(counts.max())
+    idx = np.zeros((P, K), dtype=np.int64)
+    mask = np.zeros((P, K), dtype=bool)
+    for i, r in enumerate(rows):
+        idx[i, :len(r)] = r
+        mask[i, :len(r)] = True
+    relx = points[:, 0:1] - nodes[idx, 0]
+    rely = points[:, 1:2] - nodes[idx, 1]
+    d = radii[idx]
+    w, wx, wy = _w1(relx, rely, d)
+    w = np.where(mask, w, 0.0)
+    wx = np.where(mask, wx, 0.0)
+    wy = np.where(mask, wy, 0.0)
+    p = np.stack([np.ones_like(relx), nodes[idx, 0] - origin[0], nodes[idx, 1] - origin[1]], axis=-1)
+    pp = p[..., :, None] * p[..., None, :]                      # P,K,3,3
+    A = np.einsum("pk,pkij->pij", w, pp)
+    Ax = np.einsum("pk,pkij->pij", wx, pp)
+    Ay = np.einsum("pk,pkij->pij", wy, pp)
+    c = np.stack([np.ones(P), points[:, 0] - origin[0], points[:, 1] - origin[1]], axis=-1)
+    g1 = np.linalg.solve(A, c[..., None])[..., 0]
+    ex = np.zeros((P, 3)); ex[:, 1] = 1.0
+    ey = np.zeros((P, 3)); ey[:, 2] = 1.0
+    g2 = np.linalg.solve(A, (ex - np.einsum("pij,pj->pi", Ax, g1))[..., None])[..., 0]
+    g3 = np.linalg.solve(A, (ey - np.einsum("pij,pj->pi", Ay, g1))[..., None])[..., 0]
+    gp1 = np.einsum("pj,pkj->pk", g1, p)
+    N = gp1 * w
+    dNdx = np.einsum("pj,pkj->pk", g2, p) * w + gp1 * wx
+    dNdy = np.einsum("pj,pkj->pk", g3, p) * w + gp1 * wy
+    ptr = np.zeros(P + 1, dtype=np.int64)
+    ptr[1:] = np.cumsum(counts)
+    return ptr, idx[mask], N[mask], dNdx[mask], dNdy[mask]
+
+
+# --------------------------------------------------------------------------------------------
+# Bodies
+# --------------------------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class Body:
+    kind: str                       # "deformable" | "rigid"
+    material: int
+    nodes: np.ndarray               # (n,2)
+    borders: List[dict]             # each: nodes (list, closed repeats first), periodicity, interpolant,
+                                    #       before, after, bc: [(type, params(2), hist(t,v))] x2
+    cells: np.ndarray               # (m,3) CCW
+    nodal_distance: float
+    detection: float
+    contact: float
+    periodic: int = 0
+    status: int = 0
+    # deformable only
+    domain: Optional[np.ndarray] = None
+    mass: Optional[np.ndarray] = None            # (n,2)
+    sup: Optional[Tuple] = None                  # DOF_TO_DISP csr (ptr, idx, N, dNdx, dNdy)
+    gp_xy: Optional[np.ndarray] = None
+    gp_w: Optional[np.ndarray] = None
+    gp_J: Optional[np.ndarray] = None
+    gp: Optional[Tuple] = None                   # csr (ptr, idx, N, dNdx, dNdy)
+    n_regions: int = 1
+    # rigid only
+    centre: Optional[np.ndarray] = None
+    rigid_mass: float = 0.0
+    rigid_inertia: float = 0.0
+    velocity: Tuple[float, float] = (0.0, 0.0)
+
+
+def _ccw(nodes: np.ndarray, tri: np.ndarray) -> np.ndarray:
+    p0, p1, p2 = nodes[tri[:, 0]], nodes[tri[:, 1]], nodes[tri[:, 2]]
+    cross = (p1[:, 0] - p0[:, 0]) * (p2[:, 1] - p0[:, 1]) - (p1[:, 1] - p0[:, 1]) * (p2[:, 0] - p0[:, 0])
+    tri = tri.copy()
+    flip = cross < 0
+    tri[flip] = tri[flip][:, [0, 2, 1]]
+    area = 0.5 * np.abs(cross)
+    return tri[area > 1e-14 * np.max(area)]
+
+
+def _rejection_interior(rng, centre, radius, n_target, min_sep, existing, margin, max_tries=200000):
+    pts = []
+    tree_pts = [tuple(p) for p in existing]
+    grid: Dict[Tuple[int, int], List[Tuple[float, float]]] = {}
+    cs = min_sep
+    def key(x, y):
+        return (int(math.floor(x / cs)), int(math.floor(y / cs)))
+    for p in tree_pts:
+        grid.setdefault(key(*p), []).append(p)
+    tries = 0
+    rin = radius - margin
+    while len(pts) < n_target and tries < max_tries:
+        tries += 1
+        rr = rin * math.sqrt(rng.random())
+        th = 2.0 * math.pi * rng.random()
+        x = centre[0] + rr * math.cos(th)
+        y = centre[1] + rr * math.sin(th)
+        kx, ky = key(x, y)
+        ok = True
+        for ix in (kx - 1, kx, kx + 1):
+            for iy in (ky - 1, ky, ky + 1):
+                for q in grid.get((ix, iy), ()):
+                    if (q[0] - x) ** 2 + (q[1] - y) ** 2 < min_sep * min_sep:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            pts.append((x, y))
+            grid.setdefault((kx, ky), []).append((x, y))
+    return np.array(pts).reshape(-1, 2)
+
+
+def make_disc(rng, centre, radius, n_border, n_interior, min_sep, material, rho, support_factor=2.0,
+              mass_factor=1.0, regions=1):
+    """Deformable disc: n_border equispaced border nodes (CCW), seeded interior nodes, Delaunay
+    cells, 3 Gauss points per cell, MLS shape functions, lumped masses."""
+    th = 2.0 * np.pi * np.arange(n_border) / n_border
+    border = np.stack([centre[0] + radius * np.cos(th), centre[1] + radius * np.sin(th)], axis=1)
+    h_b = 2.0 * math.pi * radius / n_border
+    interior = _rejection_interior(rng, centre, radius, n_interior, min_sep, border, margin=0.5 * h_b)
+    nodes = np.concatenate([border, interior], axis=0)
+    tri = _ccw(nodes, Delaunay(nodes).simplices.astype(np.int64))
+    edges = np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]])
+    edges = np.unique(np.sort(edges, axis=1), axis=0)
+    h_mean = float(np.mean(np.linalg.norm(nodes[edges[:, 0]] - nodes[edges[:, 1]], axis=1)))
+    domain = np.full(nodes.shape[0], support_factor * h_mean)
+    # Gauss points (Preprocessor/TriangleGaussPoints.m)
+    X1, X2, X3 = nodes[tri[:, 0]], nodes[tri[:, 1]], nodes[tri[:, 2]]
+    J = np.abs(X1[:, 0] * (X2[:, 1] - X3[:, 1]) + X2[:, 0] * (X3[:, 1] - X1[:, 1]) + X3[:, 0] * (X1[:, 1] - X2[:, 1])) / 2.0
+    gxy = []
+    for a1, a2, _ in _GAUSS3:
+        a3 = 1.0 - a1 - a2
+        gxy.append(a3 * X1 + a1 * X2 + a2 * X3)
+    gp_xy = np.stack(gxy, axis=1).reshape(-1, 2)          # cell-major, 3 per cell
+    gp_w = np.tile(_GAUSS3[:, 2], tri.shape[0])
+    gp_J = np.repeat(J, 3)
+    origin = np.asarray(centre, dtype=np.float64)
+    gp = mls_shape(gp_xy, nodes, domain, origin)
+    sup = mls_shape(nodes, nodes, domain, origin)
+    # lumped mass: m_i = rho * sum_g wJ N_gi sum_j N_gj   (AnalyseSimpleBody.m:316-331)
+    ptr, idx, N = gp[0], gp[1], gp[2]
+    rowsum = np.add.reduceat(N, ptr[:-1])
+    c0 = gp_w * gp_J
+    contrib = rho * np.repeat(c0 * rowsum, np.diff(ptr)) * N
+    m = np.zeros(nodes.shape[0])
+    np.add.at(m, idx, contrib)
+    m *= mass_factor
+    mass = np.stack([m, m], axis=1)
+    bl = list(range(n_border)) + [0]
+    border_rec = dict(nodes=bl, periodicity=0, interpolant=0, before=0, after=0,
+                      bc=[(BC_NONE, (0.0, 0.0), None), (BC_NONE, (0.0, 0.0), None)])
+    return Body(kind="deformable", material=material, nodes=nodes, borders=[border_rec], cells=tri,
+                nodal_distance=h_b, detection=0.5 * h_b, contact=0.5 * h_b, domain=domain, mass=mass,
+                sup=sup, gp_xy=gp_xy, gp_w=gp_w, gp_J=gp_J, gp=gp, n_regions=regions)
+
+
+def make_rect_rigid(x0, y0, x1, y1, spacing, material, rho, bcx, bcy, det, con):
+    """Rigid rectangle with CCW border nodes of roughly `spacing` and two cells."""
+    pts = []
+    def edge(a, b):
+        L = math.hypot(b[0] - a[0], b[1] - a[1])
+        n = max(1, int(math.ceil(L / spacing)))
+        for k in range(n):
+            t = k / n
+            pts.append((a[0] + t * (b[0] - a[0]), a[1] + t * (b[1] - a[1])))
+    c = [(x0, y0), (x1, y0), (x1, y1), (x0, y1)]
+    corner_idx = []
+    for k in range(4):
+        corner_idx.append(len(pts))
+        edge(c[k], c[(k + 1) % 4])
+    nodes = np.array(pts)
+    n = nodes.shape[0]
+    cells = np.array([[corner_idx[0], corner_idx[1], corner_idx[2]],
+                      [corner_idx[0], corner_idx[2], corner_idx[3]]], dtype=np.int64)
+    # AnalyseRigidBody.m: centre of mass, mass, inertia
+    m = 0.0; cx = 0.0; cy = 0.0
+    for tri in cells:
+        p = nodes[tri]
+        area = 0.5 * abs((p[1, 0] - p[0, 0]) * (p[2, 1] - p[0, 1]) - (p[2, 0] - p[0, 0]) * (p[1, 1] - p[0, 1]))
+        xc, yc = p[:, 0].mean(), p[:, 1].mean()
+        m += area * rho; cx += area * rho * xc; cy += area * rho * yc
+    cx /= m; cy /= m
+    inertia = 0.0
+    for tri in cells:
+        p = nodes[tri]
+        area = 0.5 * abs((p[1, 0] - p[0, 0]) * (p[2, 1] - p[0, 1]) - (p[2, 0] - p[0, 0]) * (p[1, 1] - p[0, 1]))
+        xc, yc = p[:, 0].mean(), p[:, 1].mean()
+        inertia += area * rho * ((xc - cx) ** 2 + (yc - cy) ** 2)
+        for (a, b) in ((0, 1), (1, 2), (2, 0)):
+            A = 0.5 * abs((p[a, 0] - xc) * (p[b, 1] - yc) - (p[b, 0] - xc) * (p[a, 1] - yc))
+            PP = (p[a, 0] - xc) ** 2 + (p[a, 1] - yc) ** 2
+            PQ = (p[a, 0] - xc) * (p[b, 0] - xc) + (p[a, 1] - yc) * (p[b, 1] - yc)
+            QQ = (p[b, 0] - xc) ** 2 + (p[b, 1] - yc) ** 2
+            inertia += rho * A / 6.0 * (PP + PQ + QQ)
+    bl = list(range(n)) + [0]
+    border_rec = dict(nodes=bl, periodicity=0, interpolant=0, before=0, after=0, bc=[bcx, bcy])
+    return Body(kind="rigid", material=material, nodes=nodes, borders=[border_rec], cells=cells,
+                nodal_distance=spacing, detection=det, contact=con, centre=np.array([cx, cy]),
+                rigid_mass=m, rigid_inertia=abs(inertia))
+
+
+# --------------------------------------------------------------------------------------------
+# Scene
+# --------------------------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    bodies: List[Body]
+    materials: List[Tuple[str, int, List[float]]]     # name, type, file params (rho, alpha, beta, E, nu, heat)
+    laws: List[Tuple[str, str, int, int, List[float]]] # mat1, mat2, type, length(0 fixed), file params
+    dt: float
+    nsteps: int
+    contact_update_period: float
+    period: Tuple[float, float] = (-1.0, 1.0)
+    gravity: Tuple[float, float] = (0.0, 0.0)
+    solver: int = 0
+    solver_params: Tuple[float, ...] = (1e-3, 0.2, 1.0, 100.0, 1.0, 1.0, 0.99, 1e3)
+    self_contact: bool = True
+    meta: dict = dataclasses.field(default_factory=dict)
+
+    @property
+    def n_deformable_nodes(self) -> int:
+        return int(sum(b.nodes.shape[0] for b in self.bodies if b.kind == "deformable"))
+
+
+def material_params_stored(mtype: int, p: List[float]) -> List[float]:
+    """Parameters as Load_static stores them (Code/IO.h:672-685): rho, alpha, beta, mu, lambda|kappa, heat."""
+    E, nu = p[3], p[4]
+    mu = E / (2.0 * (1.0 + nu))
+    if mtype == 0:
+        lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    else:
+        lam = E / (3.0 * (1.0 - 2.0 * nu))
+    return [p[0], p[1], p[2], mu, lam, p[5]]
+
+
+def critical_dt(body: Body, mu: float, lam: float, kn: float) -> float:
+    """2/omega_max of the body's lumped-mass elastic operator (the linear part of
+    Update_internal_forces, Body.h:974-997), plus the contact penalty kn*length/m of border nodes."""
+    import scipy.sparse as sp
+    from scipy.sparse.linalg import eigsh
+    n = body.nodes.shape[0]
+    ptr, idx, _, dx, dy = body.gp
+    c0 = body.gp_w * body.gp_J
+    G = ptr.shape[0] - 1
+    cnt = np.diff(ptr)
+    g_of = np.repeat(np.arange(G), cnt)
+    # strain rows: e11 = dx*ux, e22 = dy*uy, g12 = dy*ux + dx*uy
+    rows_e11 = 3 * g_of; rows_e22 = 3 * g_of + 1; rows_g = 3 * g_of + 2
+    r = np.concatenate([rows_e11, rows_e22, rows_g, rows_g])
+    c = np.concatenate([2 * idx, 2 * idx + 1, 2 * idx, 2 * idx + 1])
+    v = np.concatenate([dx, dy, dy, dx])
+    B = sp.csr_matrix((v, (r, c)), shape=(3 * G, 2 * n))
+    D = np.array([[lam + 2 * mu, lam, 0.0], [lam, lam + 2 * mu, 0.0], [0.0, 0.0, mu]])
+    Dg = sp.kron(sp.diags(c0), sp.csr_matrix(D))
+    K = (B.T @ Dg @ B).tocsr()
+    minv_sqrt = 1.0 / np.sqrt(body.mass.reshape(-1))
+    S = sp.diags(minv_sqrt) @ K @ sp.diags(minv_sqrt)
+    lam_max = float(eigsh(S, k=1, which="LA", return_eigenvectors=False, tol=1e-6)[0])
+    h_b = body.nodal_distance
+    m_border = body.mass[: len(body.borders[0]["nodes"]) - 1, 0]
+    lam_c = float(np.max(kn * h_b / m_border))
+    return 2.0 / math.sqrt(max(lam_max, lam_c))
+
+
+def disc_lattice_scene(seed: int = 0, nx: int = 4, ny: int = 4, pitch: float = 2.2e-3,
+                       rmin: float = 0.9e-3, rmax: float = 1.1e-3, n_border: int = 48,
+                       n_interior: int = 100, min_sep: float = 0.1e-3, v_plate: float = 0.01,
+                       nsteps: int = 10000, gap0: float = 5e-6, prox_every: int = 10,
+                       mass_factor: float = 1.0, name: str = "lattice") -> Scene:
+    """Config 0: 4x4 lattice of deformable discs between two rigid plates driven at +-v_plate."""
+    rng = np.random.default_rng(seed)
+    import random
+    prng = random.Random(seed + 1)
+    E, nu, rho = 1e8, 0.3, 2500.0
+    mats = [("Grain", 0, [rho, 0.0, 0.0, E, nu, 1000.0]), ("Steel", 0, [7800.0, 0.0, 0.0, 2e11, 0.3, 500.0])]
+    laws = [("Grain", "Grain", 2, 0, [1e10, 1e9, 0.3, 0.0, 0.0]),
+            ("Grain", "Steel", 2, 0, [1e10, 1e9, 0.3, 0.0, 0.0])]
+    bodies = []
+    radii = rng.uniform(rmin, rmax, size=nx * ny)
+    k = 0
+    for j in range(ny):
+        for i in range(nx):
+            c = (0.5 * pitch + i * pitch, 0.5 * pitch + j * pitch)
+            bodies.append(make_disc(prng, c, float(radii[k]), n_border, n_interior, min_sep, 0, rho,
+                                    mass_factor=mass_factor))
+            k += 1
+    ymin = min(b.nodes[:, 1].min() for b in bodies)
+    ymax = max(b.nodes[:, 1].max() for b in bodies)
+    xmin = min(b.nodes[:, 0].min() for b in bodies)
+    xmax = max(b.nodes[:, 0].max() for b in bodies)
+    h_b = 2.0 * math.pi * rmin / n_border
+    margin = 0.1 * (xmax - xmin)
+    thick = 0.1 * (xmax - xmin)
+    hist = lambda v: (np.array([0.0, T_HIST_END]), np.array([v, v]))
+    bot = make_rect_rigid(xmin - margin, ymin - gap0 - thick, xmax + margin, ymin - gap0, h_b, 1, 7800.0,
+                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(v_plate)),
+                          0.5 * h_b, 0.5 * h_b)
+    top = make_rect_rigid(xmin - margin, ymax + gap0, xmax + margin, ymax + gap0 + thick, h_b, 1, 7800.0,
+                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(-v_plate)),
+                          0.5 * h_b, 0.5 * h_b)
+    bodies += [bot, top]
+    mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    dtc = min(critical_dt(b, mu, lam, 1e10) for b in bodies if b.kind == "deformable")
+    dt = 0.5 * dtc
+    return Scene(name=name, bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
+                 contact_update_period=prox_every * dt,
+                 meta=dict(config="lattice", seed=seed, dt_crit=dtc))
+
+
+# --------------------------------------------------------------------------------------------
+# Flattening (the arrays behind mel_model_desc)
+# --------------------------------------------------------------------------------------------
+
+def flatten(scene: Scene) -> Dict[str, np.ndarray]:
+    """Structure-of-arrays view of the scene, field by field as in mel_model_desc (include/melgpu.h)."""
+    f: Dict[str, object] = {}
+    nb = len(scene.bodies)
+    f["period"] = np.array(scene.period, dtype=np.float64)
+    f["gravity"] = np.array(scene.gravity, dtype=np.float64)
+    f["time"] = 0.0
+    f["dt"] = float(scene.dt)
+    f["tend"] = float(scene.dt * scene.nsteps)
+    f["contact_update_period"] = float(scene.contact_update_period)
+    f["next_contact_update"] = 0.0
+    f["solver"] = int(scene.solver)
+    sp_ = list(scene.solver_params)
+    f["solver_params"] = np.array(sp_, dtype=np.float64)
+    flags = np.zeros(11, dtype=np.int32)
+    flags[7] = 1                          # NO_LOG
+    if not scene.self_contact:
+        flags[8] = 1                      # NO_MONITORING (also disables self contact, Proximity.h:332)
+    f["flags"] = flags
+    names = [m[0] for m in scene.materials]
+    f["material_type"] = np.array([m[1] for m in scene.materials], dtype=np.int32)
+    f["material_params"] = np.array([material_params_stored(m[1], m[2]) for m in scene.materials],
+                                    dtype=np.float64).reshape(-1)
+    nl = len(scene.laws)
+    f["law_type"] = np.array([l[2] for l in scene.laws], dtype=np.int32)
+    f["law_length"] = np.array([l[3] for l in scene.laws], dtype=np.int32)
+    lp = np.zeros((nl, 11))
+    for i, l in enumerate(scene.laws):
+        lp[i, :len(l[4])] = l[4]
+    f["law_params"] = lp.reshape(-1)
+    nm = len(names)
+    table = -np.ones((nm, nm), dtype=np.int32)
+    for i, l in enumerate(scene.laws):       # Code/IO.h:797-812 (last law wins)
+        a = names.index(l[0]); b = names.index(l[1])
+        table[a, b] = i; table[b, a] = i
+    f["contacts_table"] = table.reshape(-1)
+    f["body_type"] = np.array([0 if b.kind == "deformable" else 1 for b in scene.bodies], dtype=np.int32)
+    f["body_material"] = np.array([b.material for b in scene.bodies], dtype=np.int32)
+    f["body_periodic"] = np.array([b.periodic for b in scene.bodies], dtype=np.int32)
+    f["body_status"] = np.array([b.status for b in scene.bodies], dtype=np.int32)
+    f["body_dist"] = np.array([[b.nodal_distance, b.detection, b.contact] for b in scene.bodies]).reshape(-1)
+    nn = np.array([b.nodes.shape[0] for b in scene.bodies])
+    f["body_node_ptr"] = np.concatenate([[0], np.cumsum(nn)]).astype(np.int32)
+    nbd = np.array([len(b.borders) for b in scene.bodies])
+    f["body_border_ptr"] = np.concatenate([[0], np.cumsum(nbd)]).astype(np.int32)
+    ng = np.array([0 if b.gp is None else b.gp[0].shape[0] - 1 for b in scene.bodies])
+    f["body_gp_ptr"] = np.concatenate([[0], np.cumsum(ng)]).astype(np.int32)
+    nc = np.array([b.cells.shape[0] for b in scene.bodies])
+    f["body_cell_ptr"] = np.concatenate([[0], np.cumsum(nc)]).astype(np.int32)
+    rigid = np.zeros((nb, 20))
+    for i, b in enumerate(scene.bodies):
+        if b.kind == "rigid":
+            rigid[i, 0:2] = b.centre
+            rigid[i, 3] = b.rigid_mass
+            rigid[i, 4] = b.rigid_inertia
+            rigid[i, 5] = 1.0 / b.rigid_mass
+            rigid[i, 6] = 1.0 / b.rigid_inertia
+            rigid[i, 7:9] = b.centre            # current
+            rigid[i, 13:15] = b.velocity
+    f["rigid"] = rigid.reshape(-1)
+    N = int(nn.sum())
+    x0 = np.concatenate([b.nodes for b in scene.bodies])
+    f["node_x0"] = x0.reshape(-1).astype(np.float64)
+    mass = np.zeros((N, 2)); dom = np.zeros(N)
+    o = 0
+    for b in scene.bodies:
+        n = b.nodes.shape[0]
+        if b.kind == "deformable":
+            mass[o:o + n] = b.mass
+            dom[o:o + n] = b.domain
+        o += n
+    f["node_mass"] = mass.reshape(-1)
+    with np.errstate(divide="ignore"):
+        inv = np.where(mass > 0, 1.0 / np.where(mass > 0, mass, 1.0), 0.0)
+    f["node_inv_mass"] = inv.reshape(-1)
+    f["node_domain"] = dom
+    sptr = [np.zeros(1, dtype=np.int64)]; sidx = []; sN = []
+    base = 0
+    for b in scene.bodies:
+        n = b.nodes.shape[0]
+        if b.kind == "deformable":
+            p, ix, Nv, _, _ = b.sup
+            sptr.append(base + p[1:]); sidx.append(ix); sN.append(Nv)
+            base += int(p[-1])
+        else:
+            sptr.append(np.full(n, base, dtype=np.int64))
+    f["node_sup_ptr"] = np.concatenate(sptr).astype(np.int32)
+    f["node_sup_idx"] = (np.concatenate(sidx) if sidx else np.zeros(0)).astype(np.int32)
+    f["node_sup_N"] = (np.concatenate(sN) if sN else np.zeros(0)).astype(np.float64)
+    state = np.zeros((N, 12))
+    o = 0
+    for b in scene.bodies:
+        n = b.nodes.shape[0]
+        state[o:o + n, 2:4] = b.velocity      # nodal velocity
+        state[o:o + n, 8:10] = b.velocity     # velocity parameters
+        o += n
+    f["node_state"] = state.reshape(-1)
+    bb, bper, bint, bbef, baft, bptr, bnodes, bct, bcp, hptr, ht, hv = ([] for _ in range(12))
+    bptr.append(0); hptr.append(0)
+    for bi, b in enumerate(scene.bodies):
+        for br in b.borders:
+            bb.append(bi); bper.append(br["periodicity"]); bint.append(br["interpolant"])
+            bbef.append(br["before"]); baft.append(br["after"])
+            bnodes.extend(br["nodes"]); bptr.append(len(bnodes))
+            for d in range(2):
+                t, prm, hist = br["bc"][d]
+                bct.append(t); bcp.extend(prm)
+                if hist is not None:
+                    ht.extend(hist[0]); hv.extend(hist[1])
+                hptr.append(len(ht))
+    f["border_body"] = np.array(bb, dtype=np.int32)
+    f["border_periodicity"] = np.array(bper, dtype=np.int32)
+    f["border_interpolant"] = np.array(bint, dtype=np.int32)
+    f["border_before"] = np.array(bbef, dtype=np.int32)
+    f["border_after"] = np.array(baft, dtype=np.int32)
+    f["border_node_ptr"] = np.array(bptr, dtype=np.int32)
+    f["border_nodes"] = np.array(bnodes, dtype=np.int32)
+    f["border_bc_type"] = np.array(bct, dtype=np.int32)
+    f["border_bc_param"] = np.array(bcp, dtype=np.float64)
+    f["border_hist_ptr"] = np.array(hptr, dtype=np.int32)
+    f["hist_time"] = np.array(ht, dtype=np.float64)
+    f["hist_value"] = np.array(hv, dtype=np.float64)
+    gptr = [np.zeros(1, dtype=np.int64)]; gidx = []; gN = []; gx = []; gy = []; gw = []; gJ = []
+    base = 0
+    for b in scene.bodies:
+        if b.gp is None:
+            continue
+        p, ix, Nv, dx, dy = b.gp
+        gptr.append(base + p[1:]); gidx.append(ix); gN.append(Nv); gx.append(dx); gy.append(dy)
+        gw.append(b.gp_w); gJ.append(b.gp_J)
+        base += int(p[-1])
+    f["gp_sup_ptr"] = np.concatenate(gptr).astype(np.int32)
+    f["gp_sup_idx"] = np.concatenate(gidx).astype(np.int32)
+    f["gp_N"] = np.concatenate(gN).astype(np.float64)
+    f["gp_dNdx"] = np.concatenate(gx).astype(np.float64)
+    f["gp_dNdy"] = np.concatenate(gy).astype(np.float64)
+    f["gp_weight"] = np.concatenate(gw).astype(np.float64)
+    f["gp_jacobian"] = np.concatenate(gJ).astype(np.float64)
+    f["cells"] = np.concatenate([b.cells for b in scene.bodies]).reshape(-1).astype(np.int32)
+    f["body_matrix_ptr"] = np.zeros(nb + 1, dtype=np.int32)
+    f["matrix_dofs"] = np.zeros(0, dtype=np.int32)
+    f["matrix_stiffness"] = np.zeros(0, dtype=np.float64)
+    f["matrix_damping"] = np.zeros(0, dtype=np.float64)
+    f["material_names"] = names
+    return f  # type: ignore[return-value]
+
+
+# --------------------------------------------------------------------------------------------
+# ASCII writer (Preprocessor/ExportStatic.m, Preprocessor/ExportDynamic.m layouts)
+# --------------------------------------------------------------------------------------------
+
+def _g(x: float) -> str:
+    return repr(float(x)) if math.isfinite(x) else str(x)
+
+
+def _bc_lines(axis: str, bc) -> List[str]:
+    t, prm, hist = bc
+    if t == BC_NONE:
+        return [f"{axis} None"]
+    out = []
+    if t == BC_DRIVEN:
+        out.append(f"{axis} Dirichlet Driven")
+    elif t == BC_SOFT:
+        out.append(f"{axis} Dirichlet Soft {_g(prm[0])} {_g(prm[1])}")
+    elif t == BC_ORIENTED:
+        out.append(f"{axis} Neumann Oriented")
+    elif t == BC_FOLLOWING:
+        out.append(f"{axis} Neumann Following")
+    out.append(str(len(hist[0])))
+    out += [f"{_g(a)} {_g(b)}" for a, b in zip(hist[0], hist[1])]
+    return out
+
+
+def write_asc(scene: Scene, directory: str) -> None:
+    """Write STATIC_CONTROL.asc, STATIC_DATA.asc and DYNAMIC_00000.asc readable by Load_static /
+    Load_dynamic (Code/IO.h).  Numbers use 17 significant digits so the files round-trip."""
+    os.makedirs(directory, exist_ok=True)
+    mats = scene.materials
+    names = [m[0] for m in mats]
+    per = ["Closed", "Simple", "Periodic"]
+    itp = ["Linear", "Spline"]
+    L: List[str] = [" ", "SIMULATION_NAME", scene.name, " ", "MATERIALS", str(len(mats)), " "]
+    for name, t, p in mats:
+        L += [name, MAT_NAMES[t], " ".join(_g(v) for v in p) + " ", " "]
+    L += [" ", "CONTACT_LAWS", str(len(scene.laws)), " "]
+    for m1, m2, t, le, p in scene.laws:
+        L += [m1, m2, LAW_NAMES[t], ["Fixed", "Evolutive"][le],
+              " ".join(_g(v) for v in p[:LAW_NPARAM_FILE[t]]) + " ", " "]
+    tend = scene.dt * scene.nsteps
+    sp_ = scene.solver_params
+    L += [" ", "SOLVER", SOLVER_NAMES[scene.solver], f"{_g(0.0)} {_g(scene.dt)} {_g(tend)}"]
+    if scene.solver != 4:
+        L.append(f"{_g(sp_[0])} {_g(sp_[1])} {_g(sp_[2])}")
+    if scene.solver in (2, 3):
+        L.append(f"{_g(sp_[3])} {_g(sp_[4])} {_g(sp_[5])} {_g(sp_[6])}")
+    L += [f"{_g(tend)} {_g(tend)} {_g(scene.contact_update_period)}", " ",
+          "PERIODIC_BOUNDARIES", f"{_g(scene.period[0])} {_g(scene.period[1])}", " ",
+          "GRAVITY", f"{_g(scene.gravity[0])} {_g(scene.gravity[1])}", " ",
+          "NUMBER_BODIES", str(len(scene.bodies)), " ",
+          "MONITORING", "0", " ", "SPIES", "0", " ", "DEACTIVATION", "0", " "]
+    for bi, b in enumerate(scene.bodies):
+        L += [" ", "DEFORMABLE" if b.kind == "deformable" else "RIGID", str(bi), names[b.material],
+              "Periodic" if b.periodic else "Simple",
+              f"{_g(b.nodal_distance)} {_g(b.detection)} {_g(b.contact)}", " ",
+              "NODES", str(b.nodes.shape[0]), " ", "BORDERS", str(len(b.borders)), " "]
+        for br in b.borders:
+            L += [f"{per[br['periodicity']]} {itp[br['interpolant']]}", str(len(br["nodes"]))]
+            L += _bc_lines("X", br["bc"][0])
+            L += _bc_lines("Y", br["bc"][1])
+            L += [" "]
+        if b.kind == "deformable":
+            L += ["INTEGRATION", f"{b.gp[0].shape[0] - 1} {b.n_regions}", " "]
+        L += ["TRIANGULATION", str(b.cells.shape[0]), " ", " "]
+    with open(os.path.join(directory, "STATIC_CONTROL.asc"), "w") as fh:
+        fh.write("\n".join(L) + "\n")
+
+    with open(os.path.join(directory, "STATIC_DATA.asc"), "w") as fh:
+        w = fh.write
+        w(" \nSIMULATION_NAME\n%s\n \n \nNUMBER_BODIES\n%d\n \n \n" % (scene.name, len(scene.bodies)))
+        for bi, b in enumerate(scene.bodies):
+            n = b.nodes.shape[0]
+            if b.kind == "deformable":
+                w(" \nDEFORMABLE\n%d\n \nNODES\n%d\n \n" % (bi, n))
+                inv = 1.0 / b.mass
+                for i in range(n):
+                    w("%d %s %s %s %s %s %s %s\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1]), _g(b.domain[i]),
+                                                     _g(b.mass[i, 0]), _g(b.mass[i, 1]), _g(inv[i, 0]), _g(inv[i, 1])))
+            else:
+                w(" \nRIGID\n%d\n%s %s\n%s %s %s %s\n \nNODES\n%d\n \n" % (
+                    bi, _g(b.centre[0]), _g(b.centre[1]), _g(b.rigid_mass), _g(b.rigid_inertia),
+                    _g(1.0 / b.rigid_mass), _g(1.0 / b.rigid_inertia), n))
+                for i in range(n):
+                    w("%d %s %s\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1])))
+            w(" \nBORDERS\n%d\n \n" % len(b.borders))
+            for br in b.borders:
+                w("%s %s\n%d %d %d\n" % (per[br["periodicity"]], itp[br["interpolant"]], len(br["nodes"]),
+                                        br["before"], br["after"]))
+                w("".join("%d\n" % k for k in br["nodes"]))
+                w(" \n")
+            if b.kind == "deformable":
+                ptr, idx, Nv, dx, dy = b.gp
+                w("INTEGRATION\nGauss\n%d %d\n \n" % (ptr.shape[0] - 1, b.n_regions))
+                for g in range(ptr.shape[0] - 1):
+                    w("Gauss Point %d\n%s %s %s %s\n%d\n" % (g, _g(b.gp_xy[g, 0]), _g(b.gp_xy[g, 1]),
+                                                            _g(b.gp_w[g]), _g(b.gp_J[g]), ptr[g + 1] - ptr[g]))
+                    for e in range(ptr[g], ptr[g + 1]):
+                        k = idx[e]
+                        w("%d %d %d %s %s %s\n" % (k, 2 * k, 2 * k + 1, _g(Nv[e]), _g(dx[e]), _g(dy[e])))
+                    w(" \n")
+            w("TRIANGULATION\n%d\n" % b.cells.shape[0])
+            for c, t in enumerate(b.cells):
+                w("%d %d %d %d\n" % (c, t[0], t[1], t[2]))
+            w(" \n")
+            if b.kind == "deformable":
+                ptr, idx, Nv, dx, dy = b.sup
+                w("DOF_TO_DISP\n")
+                for i in range(n):
+                    w(" \nNODE %d\n%d\n" % (i, ptr[i + 1] - ptr[i]))
+                    for e in range(ptr[i], ptr[i + 1]):
+                        w("%d %s %s %s\n" % (idx[e], _g(Nv[e]), _g(dx[e]), _g(dy[e])))
+                w(" \n \nMATRICES\n0\n \n \n \n \n")
+
+    with open(os.path.join(directory, "DYNAMIC_00000.asc"), "w") as fh:
+        w = fh.write
+        tend = scene.dt * scene.nsteps
+        w(" \nSIMULATION_NAME\n%s\n \nSOLVER\n%s\n0 0 0 0 \n%s\n%s %s %s \nNO_LOG\n" % (
+            scene.name, SOLVER_NAMES[scene.solver], _g(scene.dt), _g(tend), _g(tend), _g(0.0)))
+        if not scene.self_contact:
+            w("NO_MONITORING\n")
+        w(" \n")
+        for bi, b in enumerate(scene.bodies):
+            n = b.nodes.shape[0]
+            vx, vy = b.velocity
+            if b.kind == "deformable":
+                w(" \nDEFORMABLE\nactive\n%d\n \nKINEMATICS\n%d\n" % (bi, n))
+                for i in range(n):
+                    w("%d %s %s 0 0 %s %s 0 0 0 0 %s %s 0 0\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1]),
+                                                                _g(vx), _g(vy), _g(vx), _g(vy)))
+                w(" \nFORCES\n")
+                for i in range(n):
+                    w("%d 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0\n" % i)
+                w(" \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
+            else:
+                w(" \nRIGID\nactive\n%d\n \nKINEMATICS\n%s %s 0\n0 0 0\n%s %s 0\n \n" % (
+                    bi, _g(b.centre[0]), _g(b.centre[1]), _g(vx), _g(vy)))
+                w("FORCES\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
