@@ -230,6 +230,21 @@ mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* 
 mel_status mel_get_time(mel_handle* h, double* time, double* dt);
 mel_status mel_monitor_compute(mel_handle* h, mel_monitor* out);
 
+/* Rigid-body records (layout MEL_RG_*, n_bodies records); node positions follow (restart upload). */
+mel_status mel_set_rigid(mel_handle* h, const double* rigid);
+/* Time, Deltat and Next_contact_update of the loop (Code/IO.h:1944-1953; restart upload). */
+mel_status mel_set_time(mel_handle* h, double time, double dt, double next_contact_update);
+/* Keep per-node force components of each step for mel_get_forces (off by default: extra writes). */
+mel_status mel_record_forces(mel_handle* h, int on);
+/* Time each launch of mel_step with CUDA events on the handle's stream (mel_get_kernel_times). */
+mel_status mel_set_timing(mel_handle* h, int on);
+/* Device diagnostic words: [0] index checks, [1] neighbour overflow, [2] contacts whose projection
+ * weights the reference would take from another contact (Code/Body.h:1347), ... */
+mel_status mel_get_error_words(mel_handle* h, unsigned* words, int n);
+/* Parse the input files into a mel_model_desc owned by the library (release with mel_free_desc). */
+mel_status mel_load_desc(const char* dir, int restart_index, mel_model_desc** desc, void** owner);
+mel_status mel_free_desc(void* owner);
+
 /* ---- introspection ---------------------------------------------------------------- */
 const char* mel_last_error_string(void);
 int         mel_abi_version(void);

@@ -1,0 +1,750 @@
+// Step kernels of the B200 solver.
+//
+//   contact_kernel  one thread per contact element: Body::Update_contacts (Code/Body.h:1341-1634)
+//                   for that element, the slave border length of Body::Update_borders
+//                   (Code/Body.h:614-661) and the contact law of Body::Update_contact_forces
+//                   (Code/Body.h:1642-1849); extra threads refresh every border entry's length.
+//   body_kernel     one CTA per body: Update_bc_forces, Update_body_forces, the contact force
+//                   scatter of Update_contact_forces + Send_contact_forces (Code/Body.h:1855-1967),
+//                   Update_internal_forces (Code/Body.h:937-1049), Sum_up_forces, Apply_Newton,
+//                   Update_bc(t+dt), Apply_Euler, Update_kinematics, Update_current_positions.
+//
+// Every floating-point accumulation keeps the reference's order (Gauss points ascending for the
+// internal forces, contact list order then send order for contact forces), so with identical inputs
+// the FP64 path reproduces the reference's values exactly; this file is compiled with
+// -fmad=false.
+#include <cstdio>
+#include "mel_internal.h"
+#include "mel_geometry.cuh"
+
+namespace mel {
+
+__device__ __forceinline__ void set_err(const mel_dev& d, int w, unsigned v = 1u) { atomicOr(&d.err[w], v); }
+
+// Body::Update_borders length of entry j of global border g of deformable body b
+__device__ __forceinline__ double border_length(const mel_dev& d, int b, int g, int j)
+{
+    int e = d.bd_e0[g] + j;
+    int nbn = d.bd_e0[g + 1] - d.bd_e0[g];
+    int n0 = d.b_node0[b];
+    const int* sn = d.e_sn + 4 * e;
+    const int* ss = d.e_ss + 4 * e;
+    double2 p0 = d.x[n0 + sn[0]], p1 = d.x[n0 + sn[1]], p2 = d.x[n0 + sn[2]];
+    double x0 = p0.x + d.period * ss[0], y0 = p0.y;
+    double x1 = p1.x + d.period * ss[1], y1 = p1.y;
+    double x2 = p2.x + d.period * ss[2], y2 = p2.y;
+    bool simple = d.bd_per[g] == MEL_PER_SIMPLE;
+    if (j == 0 && simple) return sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1)) * 0.5;
+    if (j == nbn - 1 && simple) return sqrt((x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0)) * 0.5;
+    return (sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1)) + sqrt((x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0))) * 0.5;
+}
+
+__device__ __forceinline__ double entry_length(const mel_dev& d, int b, int g, int j)
+{
+    if (d.b_type[b] == MEL_BODY_DEFORMABLE) return border_length(d, b, g, j);
+    return d.e_len0[d.bd_e0[g] + j];
+}
+
+// ------------------------------------------------------------------------------------------
+// contact kernel
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void seg_points(const mel_dev& d, int bodyM, int e, int shiftM, int* nd, int* sh,
+                                           double* X, double* Y)
+{
+    int mb = d.b_node0[bodyM];
+    for (int k = 0; k < 4; k++) {
+        nd[k] = d.e_sn[4 * e + k];
+        sh[k] = d.e_ss[4 * e + k];
+        double2 p = d.x[mb + nd[k]];
+        X[k] = p.x + d.period * (shiftM + sh[k]);
+        Y[k] = p.y;
+    }
+}
+
+__global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale)
+{
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= d.ncont) {
+        // refresh stored border lengths (read by Update_proximity for new contacts)
+        int e = tid - d.ncont;
+        if (e >= d.ne) return;
+        // find the border of entry e: binary search on bd_e0
+        int lo = 0, hi = d.nbd;
+        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (d.bd_e0[mid] <= e) lo = mid; else hi = mid; }
+        int b = d.bd_body[lo];
+        if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
+        if (d.b_type[b] == MEL_BODY_DEFORMABLE) d.e_len[e] = border_length(d, b, lo, e - d.bd_e0[lo]);
+        return;
+    }
+    mel_contact c = d.cont[tid];
+    int b = c.bodyS;
+    if (b < 0 || b >= d.nb || c.bodyM < 0 || c.bodyM >= d.nb) { set_err(d, MEL_E_BOUNDS); return; }
+    if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
+    // ---- Update_contacts (Code/Body.h:1352-1632) -----------------------------------------
+    int bodyM = c.bodyM, borderM = c.borderM, shiftM = c.shiftM, segmentM = c.segmentM;
+    int gM = d.b_bd0[bodyM] + borderM;
+    int per = d.bd_per[gM];
+    Proj p;
+    p.gap = c.gapn; p.xsi = c.xsi; p.xn = c.xnorm; p.yn = c.ynorm; p.xt = c.xtan; p.yt = c.ytan;
+    p.N[0] = c.shapeM[0]; p.N[1] = c.shapeM[1]; p.N[2] = c.shapeM[2]; p.N[3] = c.shapeM[3];
+    p.flag = 0;
+    double gapt = c.gapt;
+    int nd[4], sh[4];
+    double X[4], Y[4];
+    int e = d.bd_e0[gM] + segmentM;
+    seg_points(d, bodyM, e, shiftM, nd, sh, X, Y);
+    double xsi_previous = p.xsi;
+    int s0 = d.b_node0[b] + c.nodeS;
+    double2 xs = d.x[s0];
+    bool self1 = (b == bodyM && (nd[0] == c.nodeS || nd[3] == c.nodeS));
+    if (self1) closest_self(xs.x, xs.y, X[1], Y[1], X[2], Y[2], p);
+    else closest_linear(xs.x, xs.y, X[0], Y[0], X[1], Y[1], X[2], Y[2], X[3], Y[3], p);
+    bool set1 = !self1 && (p.flag >= -2 && p.flag <= 2);
+    if (p.flag == -2 || p.flag == -3 || p.flag == 2 || p.flag == 3) {
+        bool back = (p.flag == -2 || p.flag == -3);
+        double L = sqrt((X[2] - X[1]) * (X[2] - X[1]) + (Y[2] - Y[1]) * (Y[2] - Y[1]));
+        if (back) gapt = gapt + 0.5 * (-1. - xsi_previous) * L;
+        else gapt = gapt + 0.5 * (-1. + xsi_previous) * L;
+        int gb = gM;
+        int nseg = d.bd_e0[gb + 1] - d.bd_e0[gb] - 2;       // index of the last segment
+        if (back) {
+            if (per == MEL_PER_SIMPLE) {
+                if (segmentM == 0) { borderM = d.bd_bef[gb]; gb = d.b_bd0[bodyM] + borderM; segmentM = d.bd_e0[gb + 1] - d.bd_e0[gb] - 2; }
+                else segmentM--;
+            } else if (per == MEL_PER_PERIODIC) {
+                if (segmentM == 0) {
+                    if (borderM == 0) shiftM--; else if (borderM == 1) shiftM++;
+                    segmentM = nseg;
+                } else segmentM--;
+            } else {
+                if (segmentM == 0) segmentM = nseg; else segmentM--;
+            }
+        } else {
+            if (per == MEL_PER_SIMPLE) {
+                if (segmentM == nseg) { borderM = d.bd_aft[gb]; gb = d.b_bd0[bodyM] + borderM; segmentM = 0; }
+                else segmentM++;
+            } else if (per == MEL_PER_PERIODIC) {
+                if (segmentM == nseg) { if (borderM == 0) shiftM++; else if (borderM == 1) shiftM--; segmentM = 0; }
+                else segmentM++;
+            } else {
+                if (segmentM == nseg) segmentM = 0; else segmentM++;
+            }
+        }
+        gM = d.b_bd0[bodyM] + borderM;
+        e = d.bd_e0[gM] + segmentM;
+        seg_points(d, bodyM, e, shiftM, nd, sh, X, Y);
+        p.xsi = back ? 1. : -1.;
+        bool self2 = (b == bodyM && (nd[0] == c.nodeS || nd[3] == c.nodeS));
+        if (self2) closest_self(xs.x, xs.y, X[1], Y[1], X[2], Y[2], p);
+        else closest_linear(xs.x, xs.y, X[0], Y[0], X[1], Y[1], X[2], Y[2], X[3], Y[3], p);
+        bool set2 = !self2 && (p.flag >= -2 && p.flag <= 2);
+        if (!set1 && !set2) set_err(d, MEL_E_STALE);   // the reference would reuse another contact's weights
+        double L2 = sqrt((X[2] - X[1]) * (X[2] - X[1]) + (Y[2] - Y[1]) * (Y[2] - Y[1]));
+        if (back) gapt = gapt + 0.5 * (-1. + p.xsi) * L2;
+        else gapt = gapt + 0.5 * (1. + p.xsi) * L2;
+        c.bodyM = bodyM; c.borderM = borderM; c.shiftM = shiftM; c.segmentM = segmentM;
+    } else {
+        gapt = gapt + 0.5 * (p.xsi - xsi_previous) * sqrt((X[2] - X[1]) * (X[2] - X[1]) + (Y[2] - Y[1]) * (Y[2] - Y[1]));
+    }
+    int mb = d.b_node0[bodyM];
+    double2 vs = d.v[s0];
+    double2 v0 = d.v[mb + nd[0]], v1 = d.v[mb + nd[1]], v2 = d.v[mb + nd[2]], v3 = d.v[mb + nd[3]];
+    double vgapx = vs.x - (p.N[0] * v0.x + p.N[1] * v1.x + p.N[2] * v2.x + p.N[3] * v3.x);
+    double vgapy = vs.y - (p.N[0] * v0.y + p.N[1] * v1.y + p.N[2] * v2.y + p.N[3] * v3.y);
+    double vgapn = vgapx * p.xn + vgapy * p.yn;
+    double vgapt = vgapx * p.xt + vgapy * p.yt;
+    for (int k = 0; k < 4; k++) { c.nodeM[k] = nd[k]; c.shiftMk[k] = sh[k]; c.shapeM[k] = p.N[k]; }
+    c.xsi = p.xsi; c.xnorm = p.xn; c.ynorm = p.yn; c.xtan = p.xt; c.ytan = p.yt;
+    c.vgapn = vgapn; c.vgapt = vgapt;
+    // ---- Update_contact_forces (Code/Body.h:1657-1849) ----------------------------------
+    int gS = d.b_bd0[b] + c.borderS;
+    double length = entry_length(d, b, gS, c.border_nodeS);
+    double initial_length = d.e_len0[d.bd_e0[gS] + c.border_nodeS];
+    double gapn = p.gap;
+    int li = d.table[d.b_mat[b] * d.nmat + d.b_mat[bodyM]];
+    if (li > -1) {
+        double W = 0., Pn = 0., Pt = 0.;
+        int nbi = c.nb_internal;
+        apply_law(d.law_type[li], d.law_p + MEL_LAW_NPARAM * li, c.effective_mass, initial_length, gapn, vgapn, gapt,
+                  vgapt, Pn, Pt, W, nbi, c.internal);
+        c.nb_internal = nbi;
+        double Px = p.xn * Pn + p.xt * Pt, Py = p.yn * Pn + p.yt * Pt;
+        double Fsx, Fsy;
+        double dtl = d.dt[0] * law_dt_scale;
+        if (d.law_len[li] == MEL_LENGTH_FIXED) { Fsx = Px * initial_length; Fsy = Py * initial_length; W *= initial_length * dtl; }
+        else { Fsx = Px * length; Fsy = Py * length; W *= length * dtl; }
+        c.length = length; c.fx = Fsx; c.fy = Fsy;
+        c.gapn = gapn; c.gapt = gapt;
+        d.cont[tid] = c;
+        d.cont_w[tid] = W;     // work increment, summed per body in the reference's order by body_kernel
+        return;
+    }
+    // no law for this material pair: Update_contacts ran, forces untouched (Code/Body.h:1700-1701)
+    c.gapn = gapn; c.gapt = gapt;
+    d.cont[tid] = c;
+    d.cont_w[tid] = 0.;
+}
+
+// ------------------------------------------------------------------------------------------
+// boundary-condition histories (Code/Border.h:120-215, Code/Body.h:335-395)
+// ------------------------------------------------------------------------------------------
+__device__ void border_bc_value(const mel_dev& d, int g, int dir, double T, double& val, double& vel)
+{
+    int t = d.bd_bc[2 * g + dir];
+    int h0 = d.bd_h0[2 * g + dir], h1 = d.bd_h0[2 * g + dir + 1];
+    const double* ti = d.ht + h0;
+    const double* va = d.hv + h0;
+    int nh = h1 - h0;
+    val = 0.; vel = 0.;
+    if (t == MEL_BC_SOFT) {
+        int n = 0, ex = 0;
+        double v = 0.;
+        while (ex == 0 && n + 1 < nh) {
+            double t0 = ti[n], p0 = va[n], t1 = ti[n + 1], p1 = va[n + 1];
+            if (T >= t1) v = v + (t1 - t0) * (p1 + p0) * 0.5;
+            else { v = v + (T - t0) * (p0 + (p1 - p0) / (t1 - t0) * ((T - t0) * 0.5)); vel = p0 + (p1 - p0) / (t1 - t0) * (T - t0); ex = 1; }
+            n++;
+        }
+        val = v;
+    } else if (t == MEL_BC_ORIENTED || t == MEL_BC_FOLLOWING) {
+        for (int n = 0; n + 1 < nh; n++) {
+            double t0 = ti[n], p0 = va[n], t1 = ti[n + 1], p1 = va[n + 1];
+            if ((t0 <= T) & (T <= t1)) { val = p0 + (p1 - p0) / (t1 - t0) * (T - t0); break; }
+        }
+    }
+}
+
+// drivendof of Body::Update_bc for one body at time T (drv[8] updated in place)
+__device__ void body_drivendof(const mel_dev& d, int b, double T, double* drv)
+{
+    for (int n = d.b_bd0[b]; n < d.b_bd0[b + 1]; n++) {
+        for (int dir = 0; dir < 2; dir++) {
+            if (d.bd_bc[2 * n + dir] != MEL_BC_DRIVEN) continue;
+            int h0 = d.bd_h0[2 * n + dir], nh = d.bd_h0[2 * n + dir + 1] - h0;
+            const double* ti = d.ht + h0;
+            const double* va = d.hv + h0;
+            int base = 4 * dir;
+            drv[base] = 1.;
+            drv[base + 1] = 0.;
+            int ex = 0, k = 0;
+            while (ex == 0 && k + 1 < nh) {
+                double t0 = ti[k], p0 = va[k], t1 = ti[k + 1], p1 = va[k + 1];
+                if (T >= t1) drv[base + 1] += (t1 - t0) * (p1 + p0) * 0.5;
+                else {
+                    drv[base + 1] += (T - t0) * (p0 + (p1 - p0) / (t1 - t0) * ((T - t0) * 0.5));
+                    drv[base + 2] = (T - t0) * (p1 - p0) / (t1 - t0);
+                    drv[base + 3] = (p1 - p0) / (t1 - t0);
+                    ex = 1;
+                }
+                k++;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// body kernel: deformable path
+// ------------------------------------------------------------------------------------------
+// scatter v * N_j onto the supports of body-local node `node` (one warp; lanes over supports)
+__device__ __forceinline__ void warp_scatter(const mel_dev& d, int n0, int node, double fx, double fy, double2* acc, int lane)
+{
+    int gn = n0 + node;
+    int a = d.sup_ptr[gn], bnd = d.sup_ptr[gn + 1];
+    for (int j = a + lane; j < bnd; j += 32) {
+        double N = d.sup_N[j];
+        int t = d.sup_idx[j];
+        double2 f = acc[t];
+        f.x = f.x + fx * N;
+        f.y = f.y + fy * N;
+        acc[t] = f;
+    }
+}
+
+__device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
+{
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int n0 = d.b_node0[b];
+    const int n = d.b_node0[b + 1] - n0;
+    const double T = d.time2[parity];
+    const double dt = d.dt[0];
+    double2* s_up = reinterpret_cast<double2*>(smem);
+    double2* s_f = s_up + n;
+    char* region = reinterpret_cast<char*>(s_f + n);
+    for (int i = tid; i < n; i += blockDim.x) { s_up[i] = d.up[n0 + i]; s_f[i] = make_double2(0., 0.); }
+    __syncthreads();
+    // ---- Update_internal_forces: chunked Gauss-point pass (one region per body) -----------
+    const int mat = d.b_mat[b];
+    const int mtype = d.mat_type[mat];
+    const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
+    const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
+    uint16_t* s_idx = reinterpret_cast<uint16_t*>(region);
+    uint16_t* s_tpos = s_idx + MEL_CHUNK_E;
+    double2* s_p = reinterpret_cast<double2*>(s_tpos + MEL_CHUNK_E);
+    for (int ci = d.b_chunk0[b]; ci < d.b_chunk0[b + 1]; ci++) {
+        const mel_chunk ch = d.chunk[ci];
+        // stage the chunk's entries (16-byte vector loads; chunk starts are 8-entry aligned)
+        {
+            const int4* gi = reinterpret_cast<const int4*>(d.ge_idx + ch.e0);
+            const int4* gt = reinterpret_cast<const int4*>(d.ge_tpos + ch.e0);
+            int4* si = reinterpret_cast<int4*>(s_idx);
+            int4* st = reinterpret_cast<int4*>(s_tpos);
+            int nv = ch.ne >> 3;
+            for (int k = tid; k < nv; k += blockDim.x) { si[k] = gi[k]; st[k] = gt[k]; }
+            const double2* gd = d.ge_dN + ch.e0;
+            for (int k = tid; k < ch.ne; k += blockDim.x) s_p[k] = gd[k];
+        }
+        __syncthreads();
+        if (tid < ch.ngp) {
+            int g = ch.gp0 + tid;
+            int e = d.gp_e0[g] - ch.e0;
+            int ns = d.gp_ns[g];
+            double c0 = d.gp_c0[g];
+            if (mtype == MEL_MAT_ELASTIC_LINEAR) {
+                double E11 = 0., E12 = 0., E22 = 0.;
+                for (int k = 0; k < ns; k++) {
+                    double2 dN = s_p[e + k];
+                    double2 u = s_up[s_idx[e + k]];
+                    E11 = E11 + dN.x * u.x;
+                    E12 = E12 + (dN.x * u.y + dN.y * u.x);
+                    E22 = E22 + dN.y * u.y;
+                }
+                E12 = 0.5 * E12;
+                double J = 1. + E11 + E22;               // Apply_Elastic_Linear (Code/Model.h:19-29)
+                double S33 = Lam * (J - 1.);
+                double Mu2 = 2 * Mu;
+                double S11 = S33 + Mu2 * E11, S22 = S33 + Mu2 * E22, S12 = Mu2 * E12;
+                for (int k = 0; k < ns; k++) {
+                    double2 dN = s_p[e + k];
+                    double2 q;
+                    q.x = c0 * (dN.x * S11 + dN.y * S12);
+                    q.y = c0 * (dN.y * S22 + dN.x * S12);
+                    s_p[e + k] = q;
+                }
+            } else {
+                double F11 = 1., F12 = 0., F21 = 0., F22 = 1.;
+                for (int k = 0; k < ns; k++) {
+                    double2 dN = s_p[e + k];
+                    double2 u = s_up[s_idx[e + k]];
+                    F11 += dN.x * u.x; F12 += dN.y * u.x; F21 += dN.x * u.y; F22 += dN.y * u.y;
+                }
+                double Kappa = Lam;                       // Apply_NeoHookean (Code/Model.h:52-73)
+                double F11F12 = F11 * F11 + F12 * F12, F21F22 = F21 * F21 + F22 * F22;
+                double J = F11 * F22 - F12 * F21;
+                double invJ = 1. / J;
+                double K = Kappa * (J - 1.);
+                double MuJ53 = Mu * pow(J, -1.666666666667);
+                double trB = 0.333333333333 * (F11F12 + F21F22 + 1.);
+                double s11 = K + MuJ53 * (F11F12 - trB), s22 = K + MuJ53 * (F21F22 - trB);
+                double s12 = MuJ53 * (F11 * F21 + F12 * F22);
+                double S11 = (F12 * (F12 * s22 - F22 * s12) - F22 * (F12 * s12 - F22 * s11)) * invJ;
+                double S22 = (F11 * (F11 * s22 - F21 * s12) - F21 * (F11 * s12 - F21 * s11)) * invJ;
+                double S12 = (F21 * (F12 * s12 - F22 * s11) - F11 * (F12 * s22 - F22 * s12)) * invJ;
+                for (int k = 0; k < ns; k++) {
+                    double2 dN = s_p[e + k];
+                    double2 q;
+                    q.x = c0 * (dN.x * (F11 * S11 + F12 * S12) + dN.y * (F12 * S22 + F11 * S12));
+                    q.y = c0 * (dN.x * (F21 * S11 + F22 * S12) + dN.y * (F22 * S22 + F21 * S12));
+                    s_p[e + k] = q;
+                }
+            }
+        }
+        __syncthreads();
+        // pull: each touched node subtracts its contributions in ascending Gauss-point order
+        for (int t = tid; t < ch.ntn; t += blockDim.x) {
+            int node = d.tn_node[ch.tn0 + t];
+            int q0 = d.tn_start[ch.tn0 + t];
+            int cnt = d.tn_cnt[ch.tn0 + t];
+            double2 f = s_f[node];
+            for (int q = q0; q < q0 + cnt; q++) {
+                double2 c = s_p[s_tpos[q]];
+                f.x = f.x - c.x;
+                f.y = f.y - c.y;
+            }
+            s_f[node] = f;
+        }
+        __syncthreads();
+    }
+    // ---- contact forces: slave scatter in list order, then master scatter in send order ---
+    double2* s_fc = reinterpret_cast<double2*>(region);
+    double2* s_fn = s_fc + n;
+    double2* s_fd = s_fn + n;
+    double2* s_vp = s_fd + n;
+    double2* s_ap = s_vp + n;
+    const int has_bc = d.b_has_bc[b];
+    for (int i = tid; i < n; i += blockDim.x) {
+        s_fc[i] = make_double2(0., 0.);
+        s_fn[i] = make_double2(0., 0.);
+        s_fd[i] = make_double2(0., 0.);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
+            const mel_contact* ct = d.cont + c;
+            if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
+            double Fsx = ct->fx, Fsy = ct->fy;
+            warp_scatter(d, n0, ct->nodeS, Fsx, Fsy, s_fc, lane);
+            __syncwarp();
+        }
+        for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
+            int2 rg = d.inc_rng[r];
+            for (int c = rg.x; c < rg.y; c++) {
+                const mel_contact* ct = d.cont + c;
+                if (d.table[d.b_mat[ct->bodyS] * d.nmat + d.b_mat[b]] <= -1) continue;
+                double Fsx = ct->fx, Fsy = ct->fy;
+                for (int k = 0; k < 4; k++) {
+                    double sk = ct->shapeM[k];
+                    warp_scatter(d, n0, ct->nodeM[k], -Fsx * sk, -Fsy * sk, s_fc, lane);
+                    __syncwarp();
+                }
+            }
+        }
+    } else if (warp == 1 && has_bc) {
+        // ---- Update_bc_forces, deformable (Code/Body.h:669-799) --------------------------
+        for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
+            int tx = d.bd_bc[2 * g], ty = d.bd_bc[2 * g + 1];
+            if (tx == MEL_BC_NONE && ty == MEL_BC_NONE) continue;
+            double xv, xvel, yv, yvel;
+            border_bc_value(d, g, 0, T, xv, xvel);
+            border_bc_value(d, g, 1, T, yv, yvel);
+            int e0 = d.bd_e0[g], nbn = d.bd_e0[g + 1] - e0;
+            for (int k = 0; k < nbn - 1; k++) {
+                int e = e0 + k;
+                int bn = d.e_node[e];
+                double length = border_length(d, b, g, k);
+                double px = 0., py = 0.;
+                double ftx = 0., fty = 0., ftpx = 0., ftpy = 0.;
+                if (tx == MEL_BC_FOLLOWING || ty == MEL_BC_FOLLOWING) {
+                    int a0 = n0 + d.e_sn[4 * e], a2 = n0 + d.e_sn[4 * e + 2];
+                    double2 X0 = d.X0[a0], X2 = d.X0[a2], x0 = d.x[a0], x2 = d.x[a2];
+                    double invl = mel_rsqrt((X2.x - X0.x) * (X2.x - X0.x) + (X2.y - X0.y) * (X2.y - X0.y));
+                    double invlp = mel_rsqrt((x2.x - x0.x) * (x2.x - x0.x) + (x2.y - x0.y) * (x2.y - x0.y));
+                    ftx = (X2.x - X0.x) * invl; fty = (X2.y - X0.y) * invl;
+                    ftpx = (x2.x - x0.x) * invlp; ftpy = (x2.y - x0.y) * invlp;
+                }
+                double2 ub = d.u[n0 + bn], vb = d.v[n0 + bn];
+                if (tx == MEL_BC_ORIENTED) px = xv;
+                else if (tx == MEL_BC_FOLLOWING) { px += xv * (ftx * ftpx + fty * ftpy); py += xv * (ftx * ftpy - fty * ftpx); }
+                else if (tx == MEL_BC_SOFT) px = d.bd_bcp[4 * g] * (xv - ub.x) - d.bd_bcp[4 * g + 1] * (xvel - vb.x);
+                if (ty == MEL_BC_ORIENTED) py = yv;
+                else if (ty == MEL_BC_FOLLOWING) { px += yv * (fty * ftpx - ftx * ftpy); py += yv * (fty * ftpy + ftx * ftpx); }
+                else if (ty == MEL_BC_SOFT) py = d.bd_bcp[4 * g + 2] * (yv - ub.y) - d.bd_bcp[4 * g + 3] * (yvel - vb.y);
+                int gn = n0 + bn;
+                for (int j = d.sup_ptr[gn] + lane; j < d.sup_ptr[gn + 1]; j += 32) {
+                    double sf = d.sup_N[j];
+                    double fxn = 0., fyn = 0., fxd = 0., fyd = 0.;
+                    if (tx == MEL_BC_ORIENTED) fxn = px * length * sf;
+                    else if (tx == MEL_BC_FOLLOWING) { fxn = px * length * sf; fyn = py * length * sf; }
+                    else if (tx == MEL_BC_SOFT) fxd = px * length * sf;
+                    if (ty == MEL_BC_ORIENTED) fyn = py * length * sf;
+                    else if (ty == MEL_BC_FOLLOWING) { fxn = px * length * sf; fyn = py * length * sf; }
+                    else if (ty == MEL_BC_SOFT) fyd = py * length * sf;
+                    int t = d.sup_idx[j];
+                    double2 a = s_fn[t]; a.x = a.x + fxn; a.y = a.y + fyn; s_fn[t] = a;
+                    double2 c = s_fd[t]; c.x = c.x + fxd; c.y = c.y + fyd; s_fd[t] = c;
+                }
+                __syncwarp();
+            }
+        }
+    }
+    __syncthreads();
+    // ---- Sum_up_forces, Apply_Newton (Code/Node.h:212-231) --------------------------------
+    const double gx = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gx;
+    const double gy = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gy;
+    for (int i = tid; i < n; i += blockDim.x) {
+        int gi = n0 + i;
+        double2 m = d.mass[gi], im = d.minv[gi];
+        double2 fb = make_double2(m.x * gx, m.y * gy);
+        double2 fi = s_f[i], fc = s_fc[i], fn = s_fn[i], fd = s_fd[i];
+        double2 ft;
+        ft.x = fi.x + fc.x + 0. + fb.x + fd.x + fn.x + 0. + 0.;
+        ft.y = fi.y + fc.y + 0. + fb.y + fd.y + fn.y + 0. + 0.;
+        double2 ap = make_double2(ft.x * im.x / 1., ft.y * im.y / 1.);
+        s_ap[i] = ap;
+        s_vp[i] = d.vp[gi];
+        if (d.record_forces) {
+            d.o_fint[gi] = fi; d.o_fcon[gi] = fc; d.o_fneu[gi] = fn; d.o_fdir[gi] = fd; d.o_ftot[gi] = ft;
+        }
+    }
+    __syncthreads();
+    // ---- works of Body::Apply_Euler (Code/Body.h:2058-2066), summed in node order -----------
+    if (warp == 0 && lane < 6) {
+        const int widx[6] = { 0, 2, 3, 4, 5, 6 };
+        double W = d.works[7 * b + widx[lane]];
+        const double hdt = 0.5 * dt;
+        for (int i = 0; i < n; i++) {
+            double2 vp = s_vp[i], ap = s_ap[i];
+            double vx = vp.x + hdt * ap.x, vy = vp.y + hdt * ap.y;
+            double2 f;
+            if (lane == 0) f = s_f[i];
+            else if (lane == 1) { double2 m = d.mass[n0 + i]; f = make_double2(m.x * gx, m.y * gy); }
+            else if (lane == 2) f = s_fd[i];
+            else if (lane == 3) f = s_fn[i];
+            else f = make_double2(0., 0.);
+            W += dt * (vx * f.x + vy * f.y);
+        }
+        d.works[7 * b + widx[lane]] = W;
+    }
+    __syncthreads();
+    // ---- Apply_Euler (Code/Node.h:239-245) -------------------------------------------------
+    for (int i = tid; i < n; i += blockDim.x) {
+        int gi = n0 + i;
+        double2 ap = s_ap[i], vp = s_vp[i], up = s_up[i];
+        vp.x = vp.x + dt * ap.x; vp.y = vp.y + dt * ap.y;
+        up.x = up.x + dt * vp.x; up.y = up.y + dt * vp.y;
+        s_vp[i] = vp; s_up[i] = up;
+        d.ap[gi] = ap; d.vp[gi] = vp; d.up[gi] = up;
+    }
+    __syncthreads();
+    // ---- Update_kinematics + Update_current_positions (Code/Body.h:2176-2227, 2272-2283) --
+    for (int i = tid; i < n; i += blockDim.x) {
+        int gi = n0 + i;
+        double dx = 0., dy = 0., vx = 0., vy = 0., ax = 0., ay = 0.;
+        for (int j = d.sup_ptr[gi]; j < d.sup_ptr[gi + 1]; j++) {
+            int t = d.sup_idx[j];
+            double s = d.sup_N[j];
+            double2 up = s_up[t], vp = s_vp[t], ap = s_ap[t];
+            dx += s * up.x; dy += s * up.y;
+            vx += s * vp.x; vy += s * vp.y;
+            ax += s * ap.x; ay += s * ap.y;
+        }
+        d.u[gi] = make_double2(dx, dy);
+        d.v[gi] = make_double2(vx, vy);
+        d.a[gi] = make_double2(ax, ay);
+        double2 X = d.X0[gi];
+        d.x[gi] = make_double2(X.x + dx, X.y + dy);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// body kernel: rigid path
+// ------------------------------------------------------------------------------------------
+__device__ void rigid_body(const mel_dev& d, int b, int parity, char* smem)
+{
+    const int tid = threadIdx.x;
+    const int n0 = d.b_node0[b];
+    const int n = d.b_node0[b + 1] - n0;
+    const double T = d.time2[parity];
+    const double dt = d.dt[0];
+    double* rg = d.rg + MEL_RIGID_NF * b;
+    double* rf = d.rf + 15 * b;
+    double* sh = reinterpret_cast<double*>(smem);   // [0..14] forces, [16..23] drivendof
+    if (tid == 0) {
+        // Update_bc_forces, rigid (Code/Body.h:800-899)
+        double xc = rg[MEL_RG_XC], yc = rg[MEL_RG_YC];
+        double neu[3] = { 0., 0., 0. }, dir[3] = { 0., 0., 0. };
+        for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
+            int tx = d.bd_bc[2 * g], ty = d.bd_bc[2 * g + 1];
+            if (tx == MEL_BC_NONE && ty == MEL_BC_NONE) continue;
+            double xv, xvel, yv, yvel;
+            border_bc_value(d, g, 0, T, xv, xvel);
+            border_bc_value(d, g, 1, T, yv, yvel);
+            for (int e = d.bd_e0[g]; e < d.bd_e0[g + 1]; e++) {
+                int gn = n0 + d.e_node[e];
+                double length = d.e_len0[e];
+                double fxn = 0., fyn = 0., fxd = 0., fyd = 0.;
+                double2 ub = d.u[gn], vb = d.v[gn], xb = d.x[gn];
+                if (tx == MEL_BC_ORIENTED || tx == MEL_BC_FOLLOWING) fxn = xv * length;
+                else if (tx == MEL_BC_SOFT) fxd = (d.bd_bcp[4 * g] * (xv - ub.x) + d.bd_bcp[4 * g + 1] * (xvel - vb.x)) * length;
+                if (ty == MEL_BC_ORIENTED || ty == MEL_BC_FOLLOWING) fyn = yv * length;
+                else if (ty == MEL_BC_SOFT) fyd = (d.bd_bcp[4 * g + 2] * (yv - ub.y) + d.bd_bcp[4 * g + 3] * (yvel - vb.y)) * length;
+                double dx = xb.x - xc, dy = xb.y - yc;
+                neu[0] += fxn; neu[1] += fyn; neu[2] += -fxn * dy + fyn * dx;
+                dir[0] += fxd; dir[1] += fyd; dir[2] += -fxd * dy + fyd * dx;
+            }
+        }
+        // Update_body_forces (Code/Body.h:925-928)
+        double gx = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gx;
+        double gy = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gy;
+        double body[3] = { rg[MEL_RG_MASS] * gx, rg[MEL_RG_MASS] * gy, rf[5] };
+        // contact forces: own contacts in list order (Code/Body.h:1866-1877), then send order
+        double con[3] = { 0., 0., 0. };
+        for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
+            const mel_contact* ct = d.cont + c;
+            if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
+            double2 xs = d.x[n0 + ct->nodeS];
+            double dx = xs.x - xc, dy = xs.y - yc;
+            con[0] += ct->fx; con[1] += ct->fy; con[2] += -ct->fx * dy + ct->fy * dx;
+        }
+        for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
+            int2 rr = d.inc_rng[r];
+            for (int c = rr.x; c < rr.y; c++) {
+                const mel_contact* ct = d.cont + c;
+                int bs = ct->bodyS;
+                if (d.table[d.b_mat[bs] * d.nmat + d.b_mat[b]] <= -1) continue;
+                double2 xs = d.x[d.b_node0[bs] + ct->nodeS];
+                double dx = xs.x - xc - ct->shiftM * d.period;
+                double dy = xs.y - yc;
+                double Fsx = ct->fx, Fsy = ct->fy;
+                con[0] += -Fsx; con[1] += -Fsy; con[2] += Fsx * dy - Fsy * dx;
+            }
+        }
+        for (int k = 0; k < 3; k++) { rf[k] = con[k]; rf[3 + k] = body[k]; rf[6 + k] = dir[k]; rf[9 + k] = neu[k]; }
+        // Sum_up_forces (Code/Body.h:1996-1998), Apply_Newton (Code/Body.h:2034-2036)
+        double tot[3];
+        for (int k = 0; k < 3; k++) tot[k] = rf[k] + rf[3 + k] + rf[6 + k] + rf[9 + k] + rf[12 + k];
+        for (int k = 0; k < 3; k++) d.rtot[3 * b + k] = tot[k];
+        rg[MEL_RG_XA] = tot[0] * rg[MEL_RG_INV_MASS] / 1.;
+        rg[MEL_RG_YA] = tot[1] * rg[MEL_RG_INV_MASS] / 1.;
+        rg[MEL_RG_RA] = tot[2] * rg[MEL_RG_INV_INERTIA] / 1.;
+        sh[0] = rg[MEL_RG_XA]; sh[1] = rg[MEL_RG_YA];
+        // nodal copies of the body forces made by Body::Sum_up_forces (Code/Body.h:2000-2013)
+        for (int k = 0; k < 3; k++) sh[2 + k] = rf[k];
+        for (int k = 0; k < 3; k++) sh[5 + k] = rf[6 + k];
+        for (int k = 0; k < 3; k++) sh[8 + k] = rf[9 + k];
+        for (int k = 0; k < 3; k++) sh[11 + k] = tot[k];
+        // Update_bc(t+dt) (Code/Body.h:335-395)
+        double* drv = d.drv + 8 * b;
+        body_drivendof(d, b, T + dt, drv);
+        // Apply_Euler, rigid (Code/Body.h:2071-2117)
+        double* W = d.works + 7 * b;
+        double vx = rg[MEL_RG_XV] + 0.5 * dt * rg[MEL_RG_XA];
+        double vy = rg[MEL_RG_YV] + 0.5 * dt * rg[MEL_RG_YA];
+        double vr = rg[MEL_RG_RV] + 0.5 * dt * rg[MEL_RG_RA];
+        W[2] += dt * (vx * rf[3] + vy * rf[4] + vr * rf[5]);
+        W[3] += dt * (vx * rf[6] + vy * rf[7] + vr * rf[8]);
+        W[4] += dt * (vx * rf[9] + vy * rf[10] + vr * rf[11]);
+        W[5] += dt * (vx * rf[12] + vy * rf[13] + vr * rf[14]);
+        if (drv[0] == 0.) { rg[MEL_RG_XV] += dt * rg[MEL_RG_XA]; rg[MEL_RG_XD] = rg[MEL_RG_XD] + dt * rg[MEL_RG_XV]; }
+        else if (drv[0] == 1.) { rg[MEL_RG_XA] = drv[3]; rg[MEL_RG_XV] = drv[2]; rg[MEL_RG_XD] = drv[1]; rf[6] = rg[MEL_RG_MASS] * rg[MEL_RG_XA] - tot[0]; }
+        if (drv[4] == 0.) { rg[MEL_RG_YV] += dt * rg[MEL_RG_YA]; rg[MEL_RG_YD] = rg[MEL_RG_YD] + dt * rg[MEL_RG_YV]; }
+        else if (drv[4] == 1.) { rg[MEL_RG_YA] = drv[7]; rg[MEL_RG_YV] = drv[6]; rg[MEL_RG_YD] = drv[5]; rf[7] = rg[MEL_RG_MASS] * rg[MEL_RG_YA] - tot[1]; }
+        if (drv[0] == 0. && drv[4] == 0. && !d.b_per[b]) { rg[MEL_RG_RV] += dt * rg[MEL_RG_RA]; rg[MEL_RG_RD] = rg[MEL_RG_RD] + dt * rg[MEL_RG_RV]; }
+        else { rg[MEL_RG_RV] = 0.; rg[MEL_RG_RD] = 0.; }
+        rg[MEL_RG_XC] = rg[MEL_RG_X0] + rg[MEL_RG_XD];
+        rg[MEL_RG_YC] = rg[MEL_RG_Y0] + rg[MEL_RG_YD];
+        rg[MEL_RG_RC] = rg[MEL_RG_R0] + rg[MEL_RG_RD];
+    }
+    __syncthreads();
+    // node kinematics (Code/Body.h:2212-2225, 2284-2300); Apply_Newton's nodal accelerations
+    const double ax = sh[0], ay = sh[1];
+    const double xc = rg[MEL_RG_XC], yc = rg[MEL_RG_YC];
+    const double xd = rg[MEL_RG_XD], yd = rg[MEL_RG_YD], rd = rg[MEL_RG_RD];
+    const double xvb = rg[MEL_RG_XV], yvb = rg[MEL_RG_YV], rv = rg[MEL_RG_RV];
+    const double x0 = rg[MEL_RG_X0], y0 = rg[MEL_RG_Y0], r0 = rg[MEL_RG_R0];
+    const double dr = rd - r0;
+    const double cr = cos(dr), sr = sin(dr);
+    for (int i = tid; i < n; i += blockDim.x) {
+        int gi = n0 + i;
+        double2 X = d.X0[gi];
+        double dx = X.x - x0, dy = X.y - y0;
+        d.u[gi] = make_double2(xd + dx * cr - dy * sr - dx, yd + dx * sr + dy * cr - dy);
+        double2 xn = make_double2(xc + dx * cr - dy * sr, yc + dx * sr + dy * cr);
+        d.x[gi] = xn;
+        double ddx = xn.x - xc, ddy = xn.y - yc;
+        d.v[gi] = make_double2(-ddy * rv + xvb, ddx * rv + yvb);
+        d.a[gi] = make_double2(ax, ay);
+        if (d.record_forces) {
+            d.o_fint[gi] = make_double2(0., 0.);
+            d.o_fcon[gi] = make_double2(sh[2], sh[3]);
+            d.o_fdir[gi] = make_double2(sh[5], sh[6]);
+            d.o_fneu[gi] = make_double2(sh[8], sh[9]);
+            d.o_ftot[gi] = make_double2(sh[11], sh[12]);
+        }
+    }
+}
+
+// contact_work of body b: the reference adds 0.5*W to the slave body and to the master body while
+// looping over bodies in index order (Code/Body.h:1847-1848); incoming ranges are in that order.
+__device__ void contact_work(const mel_dev& d, int b)
+{
+    double w = d.works[7 * b + 1];
+    bool own_done = false;
+    for (int r = d.b_inc0[b]; r <= d.b_inc0[b + 1]; r++) {
+        bool last = (r == d.b_inc0[b + 1]);
+        int2 rr = last ? make_int2(0, 0) : d.inc_rng[r];
+        if (!last && rr.x == rr.y) continue;                      // empty range: nothing to read
+        int sender = last ? d.nb : d.cont[rr.x].bodyS;
+        if (!own_done && sender >= b) {
+            for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
+                double h = 0.5 * d.cont_w[c];
+                w += h;
+                if (d.cont[c].bodyM == b) w += h;
+            }
+            own_done = true;
+        }
+        if (last) break;
+        if (sender == b) continue;                                // self contacts were added above
+        for (int c = rr.x; c < rr.y; c++) w += 0.5 * d.cont_w[c];
+    }
+    d.works[7 * b + 1] = w;
+}
+
+__global__ void __launch_bounds__(MEL_BODY_THREADS) body_kernel(mel_dev d, int parity)
+{
+    extern __shared__ __align__(16) char smem[];
+    int b = d.b_order[blockIdx.x];
+    if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
+    if (d.any_damped && threadIdx.x == 32) contact_work(d, b);
+    if (d.b_type[b] == MEL_BODY_RIGID) rigid_body(d, b, parity, smem);
+    else deformable_body(d, b, parity, smem);
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.time2[parity ^ 1] = d.time2[parity] + d.dt[0];
+}
+
+// ------------------------------------------------------------------------------------------
+// monitor: kinetic energy (Monitoring.h:528-531), mass-weighted mean displacement (88-101)
+// ------------------------------------------------------------------------------------------
+__global__ void monitor_kernel(mel_dev d, double* out)
+{
+    // one block; fixed-order tree reduction (deterministic)
+    __shared__ double s[4][256];
+    double ke = 0., ux = 0., uy = 0., mt = 0.;
+    for (int b = 0; b < d.nb; b++) {
+        if (d.b_type[b] != MEL_BODY_DEFORMABLE) continue;
+        for (int i = d.b_node0[b] + threadIdx.x; i < d.b_node0[b + 1]; i += blockDim.x) {
+            double2 v = d.v[i], m = d.mass[i], u = d.u[i];
+            ke += 0.5 * v.x * v.x * m.x + 0.5 * v.y * v.y * m.y;
+            ux += u.x * m.x; uy += u.y * m.y; mt += m.x;
+        }
+    }
+    s[0][threadIdx.x] = ke; s[1][threadIdx.x] = ux; s[2][threadIdx.x] = uy; s[3][threadIdx.x] = mt;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 4; k++) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = s[0][0];
+        out[1] = s[3][0] > 0 ? s[1][0] / s[3][0] : 0.;
+        out[2] = s[3][0] > 0 ? s[2][0] / s[3][0] : 0.;
+        int act = 0;
+        for (int c = 0; c < d.ncont; c++) if (d.cont[c].fx != 0. || d.cont[c].fy != 0.) act++;
+        out[3] = act;
+    }
+}
+
+} // namespace mel
+
+void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s)
+{
+    int total = d.ncont + d.ne;
+    if (total <= 0) return;
+    mel::contact_kernel<<<(total + 127) / 128, 128, 0, s>>>(d, law_dt_scale);
+}
+
+size_t mel_body_smem_bytes(int max_nodes, int max_border_nodes)
+{
+    (void)max_border_nodes;
+    size_t base = 2 * sizeof(double2) * (size_t)max_nodes;
+    size_t chunk = (size_t)MEL_CHUNK_E * (2 + 2 + sizeof(double2));
+    size_t post = 5 * sizeof(double2) * (size_t)max_nodes;
+    size_t rigid = 64 * sizeof(double);
+    size_t r = base + (chunk > post ? chunk : post);
+    return r > rigid ? r : rigid;
+}
+
+void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s)
+{
+    mel::body_kernel<<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
+}
+
+void mel_launch_monitor(const mel_dev& d, double* out, cudaStream_t s)
+{
+    mel::monitor_kernel<<<1, 256, 0, s>>>(d, out);
+}
+
+void mel_body_kernel_configure(size_t smem)
+{
+    cudaFuncSetAttribute(mel::body_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}

@@ -1,0 +1,918 @@
+// Host side of the B200 solver: builds the device-resident model from a mel_model_desc, runs the
+// set-up of Code/main.cpp:104-127, advances the step loop of Code/main.cpp:141-196 and implements
+// the C ABI declared in include/melgpu.h.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "mel_internal.h"
+#include "mel_prox_host.h"
+#include "mel_host.h"   // .asc loader (mel_loader.cpp)
+
+// ---------------------------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------------------------
+static thread_local std::string g_err;
+void mel_set_error(const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+void mel_set_cuda_error(cudaError_t e, const char* what, const char* file, int line)
+{
+    mel_set_error("CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), what, file, line);
+}
+
+// ---------------------------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------------------------
+struct mel_handle {
+    mel_dev d;
+    mel_prox_state P;
+    mel_prox_host H;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    std::vector<void*> allocs;
+    // host mirrors
+    int nb = 0, nn = 0, nbd = 0, ne = 0, ng = 0, nge = 0, nse = 0;
+    std::vector<int> b_type, b_status, b_node0, b_mat;
+    std::vector<double> X0, rg_file, rg_mat;
+    double time = 0., dt = 0., cup = 0., next_cup = 0.;
+    int solver = 0;
+    int flags[MEL_NFLAGS] = { 0 };
+    int parity = 0;
+    size_t body_smem = 0;
+    int nblocks_body = 0;
+    int launches = 0;
+    double t_contact = 0., t_body = 0., t_prox = 0.;
+    int timing = 0;
+    double* d_monitor = nullptr;
+    int precision = MEL_PREC_FP64;
+};
+
+template <typename T>
+static T* dalloc(mel_handle* h, size_t n)
+{
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, n * sizeof(T));
+    h->allocs.push_back(p);
+    return (T*)p;
+}
+template <typename T>
+static T* dupload(mel_handle* h, const T* src, size_t n)
+{
+    T* p = dalloc<T>(h, n);
+    if (p && src && n) cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice);
+    return p;
+}
+template <typename T>
+static T* dupload(mel_handle* h, const std::vector<T>& v) { return dupload(h, v.data(), v.size()); }
+
+// ---------------------------------------------------------------------------------------------
+// host restatements of set-up functions
+// ---------------------------------------------------------------------------------------------
+// Body::Initialize_segments (Code/Body.h:403-606): segment node tables and initial lengths
+static void initialize_segments(const mel_model_desc* d, int b, std::vector<int>& sn, std::vector<int>& ss,
+                                std::vector<double>& len0)
+{
+    double period = d->period[1] - d->period[0];
+    int n0 = d->body_node_ptr[b];
+    for (int gi = d->body_border_ptr[b]; gi < d->body_border_ptr[b + 1]; gi++) {
+        int i = gi - d->body_border_ptr[b];
+        int off = d->border_node_ptr[gi];
+        int nbn = d->border_node_ptr[gi + 1] - off;
+        const int* bn = d->border_nodes + off;
+        int gb = d->body_border_ptr[b] + d->border_before[gi];
+        int ga = d->body_border_ptr[b] + d->border_after[gi];
+        const int* bnb = d->border_nodes + d->border_node_ptr[gb];
+        int nbb = d->border_node_ptr[gb + 1] - d->border_node_ptr[gb];
+        const int* bna = d->border_nodes + d->border_node_ptr[ga];
+        int per = d->border_periodicity[gi];
+        auto N = [&](int k, int j) -> int& { return sn[4 * (off + j) + k]; };
+        auto S = [&](int k, int j) -> int& { return ss[4 * (off + j) + k]; };
+        N(0, 0) = bnb[nbb - 2]; N(1, 0) = bn[0]; N(2, 0) = bn[1]; N(3, 0) = bn[2];
+        if (per == MEL_PER_PERIODIC && i == 0) S(0, 0) = -1;
+        else if (per == MEL_PER_PERIODIC) S(0, 0) = 1;
+        for (int j = 1; j < nbn - 2; j++) { N(0, j) = bn[j - 1]; N(1, j) = bn[j]; N(2, j) = bn[j + 1]; N(3, j) = bn[j + 2]; }
+        N(0, nbn - 2) = bn[nbn - 3]; N(1, nbn - 2) = bn[nbn - 2]; N(2, nbn - 2) = bn[nbn - 1]; N(3, nbn - 2) = bna[1];
+        if (per == MEL_PER_PERIODIC && i == 0) { S(2, nbn - 2) = 1; S(3, nbn - 2) = 1; }
+        else if (per == MEL_PER_PERIODIC) { S(2, nbn - 2) = -1; S(3, nbn - 2) = -1; }
+        N(0, nbn - 1) = bn[nbn - 2]; N(1, nbn - 1) = bn[nbn - 1]; N(2, nbn - 1) = bna[1]; N(3, nbn - 1) = bna[2];
+        if (per == MEL_PER_PERIODIC) {
+            int s = (i == 0) ? 1 : -1;
+            S(1, nbn - 1) = s; S(2, nbn - 1) = s; S(3, nbn - 1) = s;
+        }
+        for (int j = 0; j < nbn; j++) {
+            const double* X = d->node_x0;
+            double x0 = X[2 * (n0 + N(0, j))] + S(0, j) * period, y0 = X[2 * (n0 + N(0, j)) + 1];
+            double x1 = X[2 * (n0 + N(1, j))] + S(1, j) * period, y1 = X[2 * (n0 + N(1, j)) + 1];
+            double x2 = X[2 * (n0 + N(2, j))] + S(2, j) * period, y2 = X[2 * (n0 + N(2, j)) + 1];
+            len0[off + j] = 0.5 * sqrt((x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0)) + 0.5 * sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+        }
+    }
+}
+
+static double tri_surface(double x0, double y0, double x1, double y1, double x2, double y2)
+{   // Code/Tools.h:377-380
+    return 0.5 * fabs((x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0));
+}
+static double tri_inertia(double x0, double y0, double x1, double y1, double x2, double y2, double xc, double yc)
+{   // Code/Tools.h:388-412
+    double a, PP, PQ, QQ, I = 0;
+    a = tri_surface(xc, yc, x0, y0, x1, y1);
+    PP = (x0 - xc) * (x0 - xc) + (y0 - yc) * (y0 - yc); PQ = (x0 - xc) * (x1 - xc) + (y0 - yc) * (y1 - yc); QQ = (x1 - xc) * (x1 - xc) + (y1 - yc) * (y1 - yc);
+    I += a * (PP + PQ + QQ);
+    a = tri_surface(xc, yc, x1, y1, x2, y2);
+    PP = (x1 - xc) * (x1 - xc) + (y1 - yc) * (y1 - yc); PQ = (x1 - xc) * (x2 - xc) + (y1 - yc) * (y2 - yc); QQ = (x2 - xc) * (x2 - xc) + (y2 - yc) * (y2 - yc);
+    I += a * (PP + PQ + QQ);
+    a = tri_surface(xc, yc, x2, y2, x0, y0);
+    PP = (x2 - xc) * (x2 - xc) + (y2 - yc) * (y2 - yc); PQ = (x2 - xc) * (x0 - xc) + (y2 - yc) * (y0 - yc); QQ = (x0 - xc) * (x0 - xc) + (y0 - yc) * (y0 - yc);
+    I += a * (PP + PQ + QQ);
+    return fabs(I / 6.);
+}
+
+// ---------------------------------------------------------------------------------------------
+// construction
+// ---------------------------------------------------------------------------------------------
+static mel_status validate(const mel_model_desc* d)
+{
+    if (!d) { mel_set_error("null model description"); return MEL_ERR_INVALID; }
+    if (d->abi_version != MELGPU_ABI_VERSION) { mel_set_error("abi_version %d, library %d", d->abi_version, MELGPU_ABI_VERSION); return MEL_ERR_INVALID; }
+    if (d->n_bodies <= 0 || d->n_nodes <= 0 || d->n_borders <= 0) { mel_set_error("empty model"); return MEL_ERR_INVALID; }
+    if (!(d->period[1] > d->period[0])) { mel_set_error("PERIODIC_BOUNDARIES must satisfy Xmin < Xmax"); return MEL_ERR_INVALID; }
+    if (!(d->dt > 0.)) { mel_set_error("time step must be positive"); return MEL_ERR_INVALID; }
+    if (d->solver != MEL_SOLVER_EULER) { mel_set_error("solver %d: this build runs the Euler scheme (Code/Solver.h:10-88)", d->solver); return MEL_ERR_UNSUPPORTED; }
+    if (d->body_node_ptr[d->n_bodies] != d->n_nodes) { mel_set_error("body_node_ptr does not cover n_nodes"); return MEL_ERR_INVALID; }
+    if (d->body_border_ptr[d->n_bodies] != d->n_borders) { mel_set_error("body_border_ptr does not cover n_borders"); return MEL_ERR_INVALID; }
+    for (int g = 0; g < d->n_borders; g++) {
+        int nbn = d->border_node_ptr[g + 1] - d->border_node_ptr[g];
+        if (nbn < 3) { mel_set_error("border %d has %d nodes (need >= 3)", g, nbn); return MEL_ERR_INVALID; }
+        if (d->border_interpolant[g] != MEL_INTERP_LINEAR) { mel_set_error("border %d: Spline interpolant is not supported on the GPU path", g); return MEL_ERR_UNSUPPORTED; }
+        int b = d->border_body[g];
+        int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+        for (int k = d->border_node_ptr[g]; k < d->border_node_ptr[g + 1]; k++)
+            if (d->border_nodes[k] < 0 || d->border_nodes[k] >= nnb) { mel_set_error("border %d node index out of range", g); return MEL_ERR_INVALID; }
+    }
+    for (int b = 0; b < d->n_bodies; b++) {
+        int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+        if (d->body_type[b] == MEL_BODY_DEFORMABLE && nnb > MEL_MAX_BODY_NODES) {
+            mel_set_error("deformable body %d has %d nodes; this build holds at most %d nodes of a body in shared memory", b, nnb, MEL_MAX_BODY_NODES);
+            return MEL_ERR_UNSUPPORTED;
+        }
+        if (d->body_material[b] < 0 || d->body_material[b] >= d->n_materials) { mel_set_error("body %d material out of range", b); return MEL_ERR_INVALID; }
+    }
+    for (int i = 0; i < d->n_matrix; i++)
+        if (d->matrix_damping[i] != 0. || d->flags[6] == 1) { mel_set_error("damping matrices (Body::Update_damping_forces) are not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
+    return MEL_OK;
+}
+
+static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_options* opt)
+{
+    mel_dev& D = h->d;
+    memset(&D, 0, sizeof D);
+    h->nb = d->n_bodies; h->nn = d->n_nodes; h->nbd = d->n_borders;
+    h->ne = d->border_node_ptr[d->n_borders];
+    h->ng = d->n_gauss;
+    h->time = d->time; h->dt = d->dt; h->cup = d->contact_update_period; h->next_cup = d->next_contact_update;
+    h->solver = d->solver;
+    memcpy(h->flags, d->flags, sizeof h->flags);
+    h->precision = opt ? opt->precision : MEL_PREC_FP64;
+    const int nb = h->nb, nn = h->nn, nbd = h->nbd, ne = h->ne;
+    D.nb = nb; D.nn = nn; D.nbd = nbd; D.ne = ne; D.ng = h->ng;
+    D.nmat = d->n_materials;
+    D.self_contact = (d->flags[8] == 0);
+    D.xmin = d->period[0]; D.period = d->period[1] - d->period[0];
+    D.gx = d->gravity[0]; D.gy = d->gravity[1];
+    D.precision = h->precision;
+    // time
+    double t2[2] = { d->time, d->time };
+    D.time2 = dupload(h, t2, 2);
+    D.dt = dupload(h, &d->dt, 1);
+    // materials, laws
+    D.mat_type = dupload(h, d->material_type, d->n_materials);
+    D.mat_p = dupload(h, d->material_params, (size_t)d->n_materials * MEL_MAT_NPARAM);
+    D.law_type = dupload(h, d->law_type, d->n_laws);
+    D.law_len = dupload(h, d->law_length, d->n_laws);
+    D.law_p = dupload(h, d->law_params, (size_t)d->n_laws * MEL_LAW_NPARAM);
+    D.table = dupload(h, d->contacts_table, (size_t)d->n_materials * d->n_materials);
+    for (int i = 0; i < d->n_laws; i++) if (d->law_type[i] == MEL_LAW_DAMPED_MOHR_COULOMB) D.any_damped = 1;
+    // bodies
+    h->b_type.assign(d->body_type, d->body_type + nb);
+    h->b_status.assign(d->body_status, d->body_status + nb);
+    h->b_node0.assign(d->body_node_ptr, d->body_node_ptr + nb + 1);
+    h->b_mat.assign(d->body_material, d->body_material + nb);
+    D.b_type = dupload(h, d->body_type, nb);
+    D.b_mat = dupload(h, d->body_material, nb);
+    D.b_per = dupload(h, d->body_periodic, nb);
+    D.b_status = dupload(h, d->body_status, nb);
+    D.b_node0 = dupload(h, d->body_node_ptr, nb + 1);
+    D.b_bd0 = dupload(h, d->body_border_ptr, nb + 1);
+    D.b_dist = dupload(h, d->body_dist, 3 * (size_t)nb);
+    std::vector<int> has_bc(nb, 0);
+    for (int g = 0; g < nbd; g++)
+        if (d->border_bc_type[2 * g] != MEL_BC_NONE || d->border_bc_type[2 * g + 1] != MEL_BC_NONE) has_bc[d->border_body[g]] = 1;
+    D.b_has_bc = dupload(h, has_bc);
+    std::vector<int> order;
+    for (int b = 0; b < nb; b++) if (d->body_type[b] == MEL_BODY_RIGID) order.push_back(b);
+    for (int b = 0; b < nb; b++) if (d->body_type[b] != MEL_BODY_RIGID) order.push_back(b);
+    D.b_order = dupload(h, order);
+    h->nblocks_body = nb;
+    // rigid state: file masses first (the first Update_proximity precedes Update_material,
+    // Code/main.cpp:112-123); Update_material masses kept for later
+    h->rg_file.assign(d->rigid, d->rigid + (size_t)nb * MEL_RIGID_NF);
+    h->rg_mat = h->rg_file;
+    for (int b = 0; b < nb; b++) {
+        double* rg = &h->rg_mat[(size_t)b * MEL_RIGID_NF];
+        const double Rho = d->material_params[MEL_MAT_NPARAM * d->body_material[b]];
+        int n0 = d->body_node_ptr[b];
+        if (d->body_type[b] == MEL_BODY_RIGID) {   // Body::Update_material, rigid branch (Code/Body.h:2867-2905)
+            double mass = 0., inertia = 0.;
+            for (int c = d->body_cell_ptr[b]; c < d->body_cell_ptr[b + 1]; c++) {
+                int a0 = d->cells[3 * c], a1 = d->cells[3 * c + 1], a2 = d->cells[3 * c + 2];
+                const double* X = d->node_x0;
+                double x0 = X[2 * (n0 + a0)], y0 = X[2 * (n0 + a0) + 1], x1 = X[2 * (n0 + a1)], y1 = X[2 * (n0 + a1) + 1];
+                double x2 = X[2 * (n0 + a2)], y2 = X[2 * (n0 + a2) + 1];
+                double xc = (x0 + x1 + x2) / 3., yc = (y0 + y1 + y2) / 3.;
+                double surf = tri_surface(x0, y0, x1, y1, x2, y2);
+                mass += surf;
+                inertia += surf * ((xc - rg[MEL_RG_X0]) * (xc - rg[MEL_RG_X0]) + (yc - rg[MEL_RG_Y0]) * (yc - rg[MEL_RG_Y0]));
+                inertia += tri_inertia(x0, y0, x1, y1, x2, y2, xc, yc);
+            }
+            mass *= Rho; inertia *= Rho;
+            rg[MEL_RG_MASS] = mass; rg[MEL_RG_INERTIA] = inertia;
+            rg[MEL_RG_INV_MASS] = 1. / mass; rg[MEL_RG_INV_INERTIA] = 1. / inertia;
+        }
+    }
+    // rigid bodies start from their centre + displacement (Load_dynamic -> Update_current_positions)
+    for (int b = 0; b < nb; b++) {
+        if (d->body_type[b] != MEL_BODY_RIGID) continue;
+        for (double* rg : { &h->rg_file[(size_t)b * MEL_RIGID_NF], &h->rg_mat[(size_t)b * MEL_RIGID_NF] }) {
+            rg[MEL_RG_XC] = rg[MEL_RG_X0] + rg[MEL_RG_XD];
+            rg[MEL_RG_YC] = rg[MEL_RG_Y0] + rg[MEL_RG_YD];
+            rg[MEL_RG_RC] = rg[MEL_RG_R0] + rg[MEL_RG_RD];
+        }
+    }
+    D.rg = dupload(h, h->rg_file);
+    D.rf = dalloc<double>(h, 15 * (size_t)nb);
+    D.rtot = dalloc<double>(h, 3 * (size_t)nb);
+    D.drv = dalloc<double>(h, 8 * (size_t)nb);
+    D.works = dalloc<double>(h, 7 * (size_t)nb);
+    // nodes
+    std::vector<double> mass(d->node_mass, d->node_mass + 2 * (size_t)nn), minv(d->node_inv_mass, d->node_inv_mass + 2 * (size_t)nn);
+    if (d->flags[4] == 1) {   // Body::Update_material, consistent row-sum masses (Code/Body.h:2755-2783)
+        for (int b = 0; b < nb; b++) {
+            if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+            const double Rho = d->material_params[MEL_MAT_NPARAM * d->body_material[b]];
+            int n0 = d->body_node_ptr[b];
+            for (int i = n0; i < d->body_node_ptr[b + 1]; i++) { mass[2 * i] = 0.; mass[2 * i + 1] = 0.; }
+            for (int g = d->body_gp_ptr[b]; g < d->body_gp_ptr[b + 1]; g++)
+                for (int j = d->gp_sup_ptr[g]; j < d->gp_sup_ptr[g + 1]; j++)
+                    for (int k = d->gp_sup_ptr[g]; k < d->gp_sup_ptr[g + 1]; k++) {
+                        double dm = d->gp_weight[g] * d->gp_jacobian[g] * d->gp_N[j] * d->gp_N[k];
+                        mass[2 * (n0 + d->gp_sup_idx[j])] += dm;
+                        mass[2 * (n0 + d->gp_sup_idx[j]) + 1] += dm;
+                    }
+            double bm = 0.;
+            for (int i = n0; i < d->body_node_ptr[b + 1]; i++) {
+                mass[2 * i] *= Rho; mass[2 * i + 1] *= Rho;
+                minv[2 * i] = 1. / mass[2 * i]; minv[2 * i + 1] = 1. / mass[2 * i + 1];
+                bm += sqrt(mass[2 * i] * mass[2 * i] + mass[2 * i + 1] * mass[2 * i + 1]);
+            }
+            h->rg_mat[(size_t)b * MEL_RIGID_NF + MEL_RG_MASS] = bm;
+            h->rg_mat[(size_t)b * MEL_RIGID_NF + MEL_RG_INV_MASS] = 1 / bm;
+        }
+    }
+    h->X0.assign(d->node_x0, d->node_x0 + 2 * (size_t)nn);
+    D.X0 = (const double2*)dupload(h, d->node_x0, 2 * (size_t)nn);
+    D.mass = (const double2*)dupload(h, mass);
+    D.minv = (const double2*)dupload(h, minv);
+    D.x = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.u = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.v = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.a = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.up = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.vp = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.ap = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    h->nse = d->node_sup_ptr[nn];
+    std::vector<uint16_t> sidx(h->nse);
+    for (int b = 0; b < nb; b++)
+        for (int i = d->body_node_ptr[b]; i < d->body_node_ptr[b + 1]; i++)
+            for (int j = d->node_sup_ptr[i]; j < d->node_sup_ptr[i + 1]; j++) {
+                int v = d->node_sup_idx[j];
+                if (v < 0 || v >= d->body_node_ptr[b + 1] - d->body_node_ptr[b]) { mel_set_error("node support index out of range"); return MEL_ERR_INVALID; }
+                sidx[j] = (uint16_t)v;
+            }
+    D.sup_ptr = dupload(h, d->node_sup_ptr, nn + 1);
+    D.sup_idx = dupload(h, sidx);
+    D.sup_N = dupload(h, d->node_sup_N, h->nse);
+    D.o_fint = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.o_fcon = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.o_fneu = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.o_fdir = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.o_ftot = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    // borders
+    D.bd_body = dupload(h, d->border_body, nbd);
+    D.bd_per = dupload(h, d->border_periodicity, nbd);
+    D.bd_bef = dupload(h, d->border_before, nbd);
+    D.bd_aft = dupload(h, d->border_after, nbd);
+    D.bd_e0 = dupload(h, d->border_node_ptr, nbd + 1);
+    D.bd_bc = dupload(h, d->border_bc_type, 2 * (size_t)nbd);
+    D.bd_bcp = dupload(h, d->border_bc_param, 4 * (size_t)nbd);
+    D.bd_h0 = dupload(h, d->border_hist_ptr, 2 * (size_t)nbd + 1);
+    int nh = d->border_hist_ptr[2 * nbd];
+    D.ht = dupload(h, d->hist_time, nh);
+    D.hv = dupload(h, d->hist_value, nh);
+    D.e_node = dupload(h, d->border_nodes, ne);
+    std::vector<int> sn(4 * (size_t)ne, 0), ss(4 * (size_t)ne, 0);
+    std::vector<double> len0(ne, 0.);
+    for (int b = 0; b < nb; b++) initialize_segments(d, b, sn, ss, len0);
+    D.e_sn = dupload(h, sn);
+    D.e_ss = dupload(h, ss);
+    D.e_len0 = dupload(h, len0);
+    std::vector<double> len(len0);
+    D.e_len = dupload(h, len);
+    h->H.b_type = h->b_type;
+    h->H.b_per.assign(d->body_periodic, d->body_periodic + nb);
+    h->H.b_bd0.assign(d->body_border_ptr, d->body_border_ptr + nb + 1);
+    h->H.bd_e0.assign(d->border_node_ptr, d->border_node_ptr + nbd + 1);
+    // Gauss points: chunks of <= MEL_CHUNK_GP points and <= MEL_CHUNK_E entries, 8-entry aligned
+    std::vector<mel_chunk> chunks;
+    std::vector<int> b_chunk0(nb + 1, 0);
+    std::vector<double> gp_c0(h->ng);
+    std::vector<int> gp_e0(h->ng);
+    std::vector<uint8_t> gp_ns(h->ng);
+    std::vector<uint16_t> ge_idx, ge_tpos, tn_node, tn_start, tn_cnt;
+    std::vector<double> ge_dN;
+    std::vector<float> ge_dNf;
+    int max_def_nodes = 1;
+    for (int b = 0; b < nb; b++) {
+        b_chunk0[b] = (int)chunks.size();
+        if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+        int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+        max_def_nodes = std::max(max_def_nodes, nnb);
+        int g = d->body_gp_ptr[b], g1 = d->body_gp_ptr[b + 1];
+        while (g < g1) {
+            mel_chunk ch;
+            memset(&ch, 0, sizeof ch);
+            ch.gp0 = g;
+            ch.e0 = (int)ge_idx.size();
+            int ne_c = 0;
+            while (g < g1 && ch.ngp < MEL_CHUNK_GP) {
+                int ns = d->gp_sup_ptr[g + 1] - d->gp_sup_ptr[g];
+                if (ns > 255 || ns <= 0) { mel_set_error("Gauss point %d has %d supports (1..255 supported)", g, ns); return MEL_ERR_UNSUPPORTED; }
+                if (ne_c + ns > MEL_CHUNK_E) break;
+                gp_e0[g] = ch.e0 + ne_c;
+                gp_ns[g] = (uint8_t)ns;
+                gp_c0[g] = d->gp_weight[g] * d->gp_jacobian[g];   // c0 of Code/Body.h:994
+                for (int j = d->gp_sup_ptr[g]; j < d->gp_sup_ptr[g + 1]; j++) {
+                    int v = d->gp_sup_idx[j];
+                    if (v < 0 || v >= nnb) { mel_set_error("Gauss support index out of range"); return MEL_ERR_INVALID; }
+                    ge_idx.push_back((uint16_t)v);
+                    ge_dN.push_back(d->gp_dNdx[j]); ge_dN.push_back(d->gp_dNdy[j]);
+                    ge_dNf.push_back((float)d->gp_dNdx[j]); ge_dNf.push_back((float)d->gp_dNdy[j]);
+                }
+                ne_c += ns;
+                ch.ngp++;
+                g++;
+            }
+            // transposed pull lists: positions sorted by (node, position)
+            std::vector<std::pair<int, int>> tp;
+            tp.reserve(ne_c);
+            for (int q = 0; q < ne_c; q++) tp.push_back({ ge_idx[ch.e0 + q], q });
+            std::sort(tp.begin(), tp.end());
+            ch.tn0 = (int)tn_node.size();
+            std::vector<uint16_t> pos(ne_c);
+            for (int q = 0; q < ne_c; q++) {
+                pos[q] = (uint16_t)tp[q].second;
+                if (q == 0 || tp[q].first != tp[q - 1].first) {
+                    tn_node.push_back((uint16_t)tp[q].first);
+                    tn_start.push_back((uint16_t)q);
+                    tn_cnt.push_back(0);
+                }
+                tn_cnt.back()++;
+            }
+            ch.ntn = (int)tn_node.size() - ch.tn0;
+            for (int q = 0; q < ne_c; q++) ge_tpos.push_back(pos[q]);
+            int pad = (8 - (ne_c & 7)) & 7;
+            for (int q = 0; q < pad; q++) { ge_idx.push_back(0); ge_tpos.push_back(0); ge_dN.push_back(0.); ge_dN.push_back(0.); ge_dNf.push_back(0.f); ge_dNf.push_back(0.f); }
+            ch.ne = ne_c + pad;
+            chunks.push_back(ch);
+        }
+    }
+    b_chunk0[nb] = (int)chunks.size();
+    h->nge = (int)ge_idx.size();
+    D.nchunk = (int)chunks.size();
+    D.chunk = dupload(h, chunks);
+    D.b_chunk0 = dupload(h, b_chunk0);
+    D.gp_c0 = dupload(h, gp_c0);
+    D.gp_e0 = dupload(h, gp_e0);
+    D.gp_ns = dupload(h, gp_ns);
+    D.ge_idx = dupload(h, ge_idx);
+    D.ge_tpos = dupload(h, ge_tpos);
+    D.ge_dN = (const double2*)dupload(h, ge_dN);
+    D.ge_dNf = (const float2*)dupload(h, ge_dNf);
+    D.tn_node = dupload(h, tn_node);
+    D.tn_start = dupload(h, tn_start);
+    D.tn_cnt = dupload(h, tn_cnt);
+    // contacts and proximity buffers
+    D.err = dalloc<unsigned>(h, MEL_E_NWORDS);
+    D.ncont = 0;
+    mel_prox_state& P = h->P;
+    P.nbr_cap = MEL_NBR_CAP_DEFAULT;
+    if (cudaMalloc(&P.nbr, sizeof(int) * 3 * (size_t)P.nbr_cap * nb) != cudaSuccess) return MEL_ERR_OOM;
+    P.nbn = dalloc<int>(h, nb);
+    P.aabb = dalloc<double>(h, 4 * (size_t)nbd);
+    P.shmin = dalloc<int>(h, nbd);
+    P.shmax = dalloc<int>(h, nbd);
+    P.b_inc0 = dalloc<int>(h, nb + 1);
+    P.b_cont0 = dalloc<int>(h, nb + 1);
+    P.e_cnt = dalloc<int>(h, ne + 1);
+    P.e_ptr = dalloc<int>(h, ne + 2);
+    P.e_cur = dalloc<int>(h, ne + 2);
+    size_t cb = sizeof(mel_contact) * 1024;
+    if (cudaMalloc(&D.cont, cb) != cudaSuccess) return MEL_ERR_OOM;
+    P.cont_bytes = cb;
+    if (cudaMalloc(&P.cont_w, sizeof(double) * 1024) != cudaSuccess) return MEL_ERR_OOM;
+    P.cont_w_bytes = sizeof(double) * 1024;
+    D.cont_w = P.cont_w;
+    D.b_cont0 = P.b_cont0; D.b_inc0 = P.b_inc0;
+    if (cudaMalloc(&P.inc_rng, sizeof(int2) * 16) != cudaSuccess) return MEL_ERR_OOM;
+    P.inc_rng_bytes = sizeof(int2) * 16;
+    D.inc_rng = P.inc_rng;
+    h->body_smem = mel_body_smem_bytes(max_def_nodes, 0);
+    if (h->body_smem > 227 * 1024) { mel_set_error("body of %d nodes needs %zu bytes of shared memory", max_def_nodes, h->body_smem); return MEL_ERR_UNSUPPORTED; }
+    mel_body_kernel_configure(h->body_smem);
+    h->d_monitor = dalloc<double>(h, 8);
+    if (cudaDeviceSynchronize() != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "build", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    return MEL_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// set-up and stepping
+// ---------------------------------------------------------------------------------------------
+static mel_status check_errors(mel_handle* h)
+{
+    unsigned w[MEL_E_NWORDS];
+    if (cudaMemcpy(w, h->d.err, sizeof w, cudaMemcpyDeviceToHost) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "err", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    if (w[MEL_E_BOUNDS]) { mel_set_error("device index check failed (code %u)", w[MEL_E_BOUNDS]); return MEL_ERR_BOUNDS; }
+    return MEL_OK;
+}
+
+static mel_status proximity(mel_handle* h)
+{
+    cudaEvent_t e0, e1;
+    if (h->timing) { cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventRecord(e0, h->stream); }
+    int rc = mel_run_proximity(h->d, h->P, h->H, h->stream);
+    if (h->timing) {
+        cudaEventRecord(e1, h->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        h->t_prox += ms;
+        cudaEventDestroy(e0); cudaEventDestroy(e1);
+    }
+    if (rc) { if (rc == MEL_ERR_CUDA) mel_set_cuda_error(cudaGetLastError(), "proximity", __FILE__, __LINE__); else mel_set_error("proximity failed (%d)", rc); return (mel_status)rc; }
+    return MEL_OK;
+}
+
+static void update_borders_only(mel_handle* h)
+{
+    mel_dev d = h->d;
+    d.ncont = 0;
+    mel_launch_contact(d, 1.0, h->stream);
+}
+
+static mel_status setup(mel_handle* h)
+{
+    // Code/main.cpp:104-127: Update_borders, Update_bc, Update_proximity, Update_material,
+    // Update_proximity.  Update_bc values are evaluated when used; Initialize_CZM is not run.
+    if (h->flags[3] == 1) { mel_set_error("INITIALIZE_CZM is not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
+    // rigid nodes take their positions from the body state
+    std::vector<double> st(12 * (size_t)h->nn, 0.);
+    mel_status rc = MEL_OK;
+    update_borders_only(h);
+    if ((rc = proximity(h))) return rc;
+    cudaMemcpyAsync(h->d.rg, h->rg_mat.data(), sizeof(double) * h->rg_mat.size(), cudaMemcpyHostToDevice, h->stream);
+    if ((rc = proximity(h))) return rc;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "setup", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    return check_errors(h);
+}
+
+// node positions from node_state (deformable: X0 + u, Code/Node.h:233-237) and rigid body state
+// (Code/Body.h:2272-2300), uploaded together
+static mel_status upload_state(mel_handle* h, const double* st, const double* rigid)
+{
+    const int nn = h->nn;
+    std::vector<double> u(2 * (size_t)nn), v(2 * (size_t)nn), a(2 * (size_t)nn), up(2 * (size_t)nn), vp(2 * (size_t)nn), ap(2 * (size_t)nn), x(2 * (size_t)nn);
+    std::vector<double> rg(rigid ? std::vector<double>(rigid, rigid + (size_t)h->nb * MEL_RIGID_NF) : std::vector<double>());
+    if (!rigid) {
+        rg.resize((size_t)h->nb * MEL_RIGID_NF);
+        cudaMemcpy(rg.data(), h->d.rg, sizeof(double) * rg.size(), cudaMemcpyDeviceToHost);
+    }
+    if (!st) {
+        std::vector<double> tmp(12 * (size_t)nn);
+        mel_get_node_state(h, tmp.data());
+        return upload_state(h, tmp.data(), rg.data());
+    }
+    for (int i = 0; i < nn; i++) {
+        const double* s = st + 12 * (size_t)i;
+        for (int k = 0; k < 2; k++) {
+            u[2 * i + k] = s[k]; v[2 * i + k] = s[2 + k]; a[2 * i + k] = s[4 + k];
+            up[2 * i + k] = s[6 + k]; vp[2 * i + k] = s[8 + k]; ap[2 * i + k] = s[10 + k];
+            x[2 * i + k] = h->X0[2 * i + k] + u[2 * i + k];
+        }
+    }
+    for (int b = 0; b < h->nb; b++) {
+        if (h->b_type[b] != MEL_BODY_RIGID) continue;
+        double* r = &rg[(size_t)b * MEL_RIGID_NF];
+        r[MEL_RG_XC] = r[MEL_RG_X0] + r[MEL_RG_XD];
+        r[MEL_RG_YC] = r[MEL_RG_Y0] + r[MEL_RG_YD];
+        r[MEL_RG_RC] = r[MEL_RG_R0] + r[MEL_RG_RD];
+        double dr = r[MEL_RG_RD] - r[MEL_RG_R0];
+        for (int i = h->b_node0[b]; i < h->b_node0[b + 1]; i++) {
+            double dx = h->X0[2 * i] - r[MEL_RG_X0], dy = h->X0[2 * i + 1] - r[MEL_RG_Y0];
+            x[2 * i] = r[MEL_RG_XC] + dx * cos(dr) - dy * sin(dr);
+            x[2 * i + 1] = r[MEL_RG_YC] + dx * sin(dr) + dy * cos(dr);
+            double ddx = x[2 * i] - r[MEL_RG_XC], ddy = x[2 * i + 1] - r[MEL_RG_YC];
+            v[2 * i] = -ddy * r[MEL_RG_RV] + r[MEL_RG_XV];
+            v[2 * i + 1] = ddx * r[MEL_RG_RV] + r[MEL_RG_YV];
+        }
+    }
+    size_t bytes = sizeof(double) * 2 * (size_t)nn;
+    MEL_CUDA_OK(cudaMemcpy(h->d.u, u.data(), bytes, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.v, v.data(), bytes, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.a, a.data(), bytes, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.up, up.data(), bytes, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.vp, vp.data(), bytes, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.ap, ap.data(), bytes, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.x, x.data(), bytes, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.rg, rg.data(), sizeof(double) * rg.size(), cudaMemcpyHostToDevice));
+    return MEL_OK;
+}
+
+extern "C" {
+
+static mel_status create_impl(const mel_model_desc* desc, const mel_options* opt, const mel_contact* c0, int nc0,
+                              mel_handle** out)
+{
+    if (!out) { mel_set_error("null output handle"); return MEL_ERR_INVALID; }
+    *out = nullptr;
+    mel_status rc = validate(desc);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { mel_set_error("no CUDA device"); return MEL_ERR_NO_DEVICE; }
+    mel_handle* h = new mel_handle();
+    h->device = opt ? opt->device : 0;
+    if (cudaSetDevice(h->device) != cudaSuccess) { mel_set_error("cudaSetDevice(%d) failed", h->device); delete h; return MEL_ERR_NO_DEVICE; }
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { mel_set_error("stream"); delete h; return MEL_ERR_CUDA; }
+    rc = build(h, desc, opt);
+    if (!rc) rc = upload_state(h, desc->node_state, h->rg_file.data());
+    if (!rc && nc0 > 0) rc = mel_set_contacts(h, c0, nc0);   // contacts of the DYNAMIC file (Code/IO.h:2236-2302)
+    if (!rc) rc = setup(h);
+    if (rc) { mel_destroy(h); return rc; }
+    *out = h;
+    return MEL_OK;
+}
+
+mel_status mel_create(const mel_model_desc* desc, const mel_options* opt, mel_handle** out)
+{
+    return create_impl(desc, opt, nullptr, 0, out);
+}
+
+mel_status mel_create_from_files(const char* dir, int restart_index, const mel_options* opt, mel_handle** out)
+{
+    mel_host_model hm;
+    mel_status rc = mel_load_files(dir, restart_index, &hm);
+    if (rc) return rc;
+    return create_impl(&hm.desc, opt, hm.contacts.data(), (int)hm.contacts.size(), out);
+}
+
+/* the model read from the files, for callers that drive their own copy (returns a heap object) */
+mel_status mel_load_desc(const char* dir, int restart_index, mel_model_desc** desc_out, void** owner)
+{
+    if (!desc_out || !owner) return MEL_ERR_INVALID;
+    mel_host_model* hm = new mel_host_model();
+    mel_status rc = mel_load_files(dir, restart_index, hm);
+    if (rc) { delete hm; return rc; }
+    *desc_out = &hm->desc;
+    *owner = hm;
+    return MEL_OK;
+}
+
+mel_status mel_free_desc(void* owner)
+{
+    delete static_cast<mel_host_model*>(owner);
+    return MEL_OK;
+}
+
+mel_status mel_destroy(mel_handle* h)
+{
+    if (!h) return MEL_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocs) cudaFree(p);
+    mel_prox_state& P = h->P;
+    for (void* p : { (void*)P.nbr, (void*)P.task, (void*)P.inc_task, (void*)P.slot_cnt, (void*)P.slot_off, (void*)P.inc_rng,
+                     (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)h->d.cont })
+        if (p) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MEL_OK;
+}
+
+mel_status mel_step(mel_handle* h, mel_step_io* io)
+{
+    if (!h || !io || io->nsteps < 0) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    h->t_contact = h->t_body = h->t_prox = 0.;
+    h->launches = 0;
+    int nprox = 0;
+    std::vector<cudaEvent_t> ev;
+    auto mark = [&]() { if (!h->timing) return; cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); ev.push_back(e); };
+    std::vector<int> kinds;
+    for (int s = 0; s < io->nsteps; s++) {
+        mark();
+        mel_launch_contact(h->d, 1.0, h->stream);
+        mark(); kinds.push_back(0);
+        mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream);
+        mark(); kinds.push_back(1);
+        h->launches += 2;
+        h->parity ^= 1;
+        h->time += h->dt;                       // Code/Solver.h:86
+        if (io->run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
+            h->next_cup = h->next_cup + h->cup;
+            mel_status rc = proximity(h);
+            if (rc) return rc;
+            nprox++;
+            h->launches += 8;
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { mel_set_cuda_error(e, "mel_step", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    if (h->timing) {
+        for (size_t k = 0; k + 1 < ev.size(); k += 3) {
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, ev[k], ev[k + 1]);
+            cudaEventElapsedTime(&b, ev[k + 1], ev[k + 2]);
+            h->t_contact += a; h->t_body += b;
+        }
+        for (auto x : ev) cudaEventDestroy(x);
+    }
+    mel_status rc = check_errors(h);
+    if (rc) return rc;
+    io->time = h->time; io->dt = h->dt; io->next_contact_update = h->next_cup;
+    io->n_contacts = h->d.ncont; io->n_proximity = nprox;
+    return MEL_OK;
+}
+
+mel_status mel_update_proximity(mel_handle* h)
+{
+    if (!h) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    mel_status rc = proximity(h);
+    if (rc) return rc;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "proximity", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    return check_errors(h);
+}
+
+mel_status mel_set_contacts(mel_handle* h, const mel_contact* c, int n)
+{
+    if (!h || n < 0 || (n > 0 && !c)) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    const std::vector<int>& bb = h->H.b_bd0;
+    const std::vector<int>& be = h->H.bd_e0;
+    for (int i = 0; i < n; i++) {
+        const mel_contact& k = c[i];
+        if (k.bodyS < 0 || k.bodyS >= h->nb || k.bodyM < 0 || k.bodyM >= h->nb) { mel_set_error("contact %d: body out of range", i); return MEL_ERR_INVALID; }
+        if (i > 0 && k.bodyS < c[i - 1].bodyS) { mel_set_error("contact list must be ordered by slave body"); return MEL_ERR_INVALID; }
+        int nbS = bb[k.bodyS + 1] - bb[k.bodyS], nbM = bb[k.bodyM + 1] - bb[k.bodyM];
+        if (k.borderS < 0 || k.borderS >= nbS || k.borderM < 0 || k.borderM >= nbM) { mel_set_error("contact %d: border out of range", i); return MEL_ERR_INVALID; }
+        int gS = bb[k.bodyS] + k.borderS, gM = bb[k.bodyM] + k.borderM;
+        if (k.border_nodeS < 0 || k.border_nodeS >= be[gS + 1] - be[gS]) { mel_set_error("contact %d: border node out of range", i); return MEL_ERR_INVALID; }
+        if (k.segmentM < 0 || k.segmentM > be[gM + 1] - be[gM] - 2) { mel_set_error("contact %d: segment out of range", i); return MEL_ERR_INVALID; }
+        int nnS = h->b_node0[k.bodyS + 1] - h->b_node0[k.bodyS];
+        if (k.nodeS < 0 || k.nodeS >= nnS) { mel_set_error("contact %d: slave node out of range", i); return MEL_ERR_INVALID; }
+    }
+    size_t need = sizeof(mel_contact) * (size_t)(n + 1);
+    if (need > h->P.cont_bytes) {
+        cudaFree(h->d.cont);
+        if (cudaMalloc(&h->d.cont, need) != cudaSuccess) return MEL_ERR_OOM;
+        h->P.cont_bytes = need;
+    }
+    if (sizeof(double) * (size_t)(n + 1) > h->P.cont_w_bytes) {
+        cudaFree(h->P.cont_w);
+        if (cudaMalloc(&h->P.cont_w, sizeof(double) * (n + 1)) != cudaSuccess) return MEL_ERR_OOM;
+        h->P.cont_w_bytes = sizeof(double) * (n + 1);
+    }
+    h->d.cont_w = h->P.cont_w;
+    cudaMemset(h->P.cont_w, 0, sizeof(double) * (n + 1));
+    if (n) MEL_CUDA_OK(cudaMemcpy(h->d.cont, c, sizeof(mel_contact) * n, cudaMemcpyHostToDevice));
+    h->d.ncont = n;
+    int rc = mel_index_external(h->d, h->P, c, n, h->stream);
+    if (rc) return (mel_status)rc;
+    return check_errors(h);
+}
+
+mel_status mel_get_node_state(mel_handle* h, double* st)
+{
+    if (!h || !st) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    const int nn = h->nn;
+    std::vector<double> buf(2 * (size_t)nn);
+    double2* arrs[6] = { h->d.u, h->d.v, h->d.a, h->d.up, h->d.vp, h->d.ap };
+    for (int k = 0; k < 6; k++) {
+        MEL_CUDA_OK(cudaMemcpy(buf.data(), arrs[k], sizeof(double) * 2 * (size_t)nn, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nn; i++) { st[12 * (size_t)i + 2 * k] = buf[2 * i]; st[12 * (size_t)i + 2 * k + 1] = buf[2 * i + 1]; }
+    }
+    return MEL_OK;
+}
+
+mel_status mel_set_node_state(mel_handle* h, const double* st)
+{
+    if (!h || !st) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    return upload_state(h, st, nullptr);
+}
+
+mel_status mel_set_rigid(mel_handle* h, const double* rigid)
+{
+    if (!h || !rigid) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    return upload_state(h, nullptr, rigid);
+}
+
+mel_status mel_set_time(mel_handle* h, double time, double dt, double next_contact_update)
+{
+    if (!h || !(dt > 0.)) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    h->time = time; h->dt = dt; h->next_cup = next_contact_update;
+    double t2[2] = { time, time };
+    MEL_CUDA_OK(cudaMemcpy(h->d.time2, t2, sizeof t2, cudaMemcpyHostToDevice));
+    MEL_CUDA_OK(cudaMemcpy(h->d.dt, &dt, sizeof dt, cudaMemcpyHostToDevice));
+    h->parity = 0;
+    return MEL_OK;
+}
+
+mel_status mel_get_positions(mel_handle* h, double* xy)
+{
+    if (!h || !xy) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    MEL_CUDA_OK(cudaMemcpy(xy, h->d.x, sizeof(double) * 2 * (size_t)h->nn, cudaMemcpyDeviceToHost));
+    return MEL_OK;
+}
+
+mel_status mel_get_forces(mel_handle* h, double* internal, double* contact, double* neumann, double* dirichlet, double* total)
+{
+    if (!h) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    if (!h->d.record_forces) { mel_set_error("force recording is off: call mel_record_forces(h, 1) before stepping"); return MEL_ERR_INVALID; }
+    size_t b = sizeof(double) * 2 * (size_t)h->nn;
+    if (internal) MEL_CUDA_OK(cudaMemcpy(internal, h->d.o_fint, b, cudaMemcpyDeviceToHost));
+    if (contact) MEL_CUDA_OK(cudaMemcpy(contact, h->d.o_fcon, b, cudaMemcpyDeviceToHost));
+    if (neumann) MEL_CUDA_OK(cudaMemcpy(neumann, h->d.o_fneu, b, cudaMemcpyDeviceToHost));
+    if (dirichlet) MEL_CUDA_OK(cudaMemcpy(dirichlet, h->d.o_fdir, b, cudaMemcpyDeviceToHost));
+    if (total) MEL_CUDA_OK(cudaMemcpy(total, h->d.o_ftot, b, cudaMemcpyDeviceToHost));
+    return MEL_OK;
+}
+
+mel_status mel_record_forces(mel_handle* h, int on)
+{
+    if (!h) return MEL_ERR_INVALID;
+    h->d.record_forces = on ? 1 : 0;
+    return MEL_OK;
+}
+
+mel_status mel_set_timing(mel_handle* h, int on)
+{
+    if (!h) return MEL_ERR_INVALID;
+    h->timing = on ? 1 : 0;
+    return MEL_OK;
+}
+
+mel_status mel_get_rigid(mel_handle* h, double* rigid, double* rigid_forces)
+{
+    if (!h) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    if (rigid) MEL_CUDA_OK(cudaMemcpy(rigid, h->d.rg, sizeof(double) * MEL_RIGID_NF * (size_t)h->nb, cudaMemcpyDeviceToHost));
+    if (rigid_forces) {
+        std::vector<double> rf(15 * (size_t)h->nb);
+        MEL_CUDA_OK(cudaMemcpy(rf.data(), h->d.rf, sizeof(double) * rf.size(), cudaMemcpyDeviceToHost));
+        for (int b = 0; b < h->nb; b++) memcpy(rigid_forces + 12 * (size_t)b, &rf[15 * (size_t)b], 12 * sizeof(double));
+    }
+    return MEL_OK;
+}
+
+mel_status mel_get_works(mel_handle* h, double* works)
+{
+    if (!h || !works) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    MEL_CUDA_OK(cudaMemcpy(works, h->d.works, sizeof(double) * 7 * (size_t)h->nb, cudaMemcpyDeviceToHost));
+    return MEL_OK;
+}
+
+mel_status mel_get_contact_count(mel_handle* h, int* n)
+{
+    if (!h || !n) return MEL_ERR_INVALID;
+    *n = h->d.ncont;
+    return MEL_OK;
+}
+
+mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* n)
+{
+    if (!h) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    if (n) *n = h->d.ncont;
+    int m = std::min(capacity, h->d.ncont);
+    if (out && m > 0) MEL_CUDA_OK(cudaMemcpy(out, h->d.cont, sizeof(mel_contact) * m, cudaMemcpyDeviceToHost));
+    return MEL_OK;
+}
+
+mel_status mel_get_time(mel_handle* h, double* time, double* dt)
+{
+    if (!h) return MEL_ERR_INVALID;
+    if (time) *time = h->time;
+    if (dt) *dt = h->dt;
+    return MEL_OK;
+}
+
+mel_status mel_monitor_compute(mel_handle* h, mel_monitor* out)
+{
+    if (!h || !out) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    memset(out, 0, sizeof *out);
+    mel_launch_monitor(h->d, h->d_monitor, h->stream);
+    double m[4];
+    MEL_CUDA_OK(cudaMemcpyAsync(m, h->d_monitor, sizeof m, cudaMemcpyDeviceToHost, h->stream));
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    out->time = h->time;
+    out->kinetic_energy = m[0];
+    out->mean_displacement[0] = m[1];
+    out->mean_displacement[1] = m[2];
+    out->active_contacts = (int)m[3];
+    out->n_contacts = h->d.ncont;
+    std::vector<double> rf(15 * (size_t)h->nb);
+    MEL_CUDA_OK(cudaMemcpy(rf.data(), h->d.rf, sizeof(double) * rf.size(), cudaMemcpyDeviceToHost));
+    int r = 0;
+    for (int b = 0; b < h->nb && r < 4; b++) {
+        if (h->b_type[b] != MEL_BODY_RIGID) continue;
+        out->rigid_force[2 * r] = rf[15 * b]; out->rigid_force[2 * r + 1] = rf[15 * b + 1];
+        out->rigid_dirichlet[2 * r] = rf[15 * b + 6]; out->rigid_dirichlet[2 * r + 1] = rf[15 * b + 7];
+        r++;
+    }
+    return MEL_OK;
+}
+
+const char* mel_last_error_string(void) { return g_err.c_str(); }
+int mel_abi_version(void) { return MELGPU_ABI_VERSION; }
+
+mel_status mel_get_kernel_times(mel_handle* h, double* ms_contact, double* ms_body, double* ms_rigid, double* ms_proximity, int* launches)
+{
+    if (!h) return MEL_ERR_INVALID;
+    if (ms_contact) *ms_contact = h->t_contact;
+    if (ms_body) *ms_body = h->t_body;
+    if (ms_rigid) *ms_rigid = 0.;
+    if (ms_proximity) *ms_proximity = h->t_prox;
+    if (launches) *launches = h->launches;
+    return MEL_OK;
+}
+
+mel_status mel_get_sizes(mel_handle* h, int* n_bodies, int* n_nodes, int* n_gauss, int* n_gp_entries, int* n_node_entries, int* n_border_nodes)
+{
+    if (!h) return MEL_ERR_INVALID;
+    if (n_bodies) *n_bodies = h->nb;
+    if (n_nodes) *n_nodes = h->nn;
+    if (n_gauss) *n_gauss = h->ng;
+    if (n_gp_entries) *n_gp_entries = h->nge;
+    if (n_node_entries) *n_node_entries = h->nse;
+    if (n_border_nodes) *n_border_nodes = h->ne;
+    return MEL_OK;
+}
+
+mel_status mel_get_error_words(mel_handle* h, unsigned* words, int n)
+{
+    if (!h || !words) return MEL_ERR_INVALID;
+    unsigned w[MEL_E_NWORDS];
+    MEL_CUDA_OK(cudaMemcpy(w, h->d.err, sizeof w, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n && i < MEL_E_NWORDS; i++) words[i] = w[i];
+    return MEL_OK;
+}
+
+} // extern "C"

@@ -76,29 +76,41 @@ def _w1(relx: np.ndarray, rely: np.ndarray, d: np.ndarray):
     return w, dwdx, dwdy
 
 
+def _supports(points: np.ndarray, nodes: np.ndarray, radii: np.ndarray, kmax: int = 40):
+    """Support lists of Preprocessor/SupportDomain.m:16-18 (nodes whose radius covers the point),
+    ascending node order, as a padded (P, K) index array and mask."""
+    tree = cKDTree(nodes)
+    n = nodes.shape[0]
+    k = min(kmax, n)
+    while True:
+        dist, idx = tree.query(points, k=k, distance_upper_bound=float(radii.max()) * (1 + 1e-12))
+        if k == 1:
+            dist = dist[:, None]; idx = idx[:, None]
+        valid = idx < n
+        idx_c = np.where(valid, idx, 0)
+        dx = points[:, 0:1] - nodes[idx_c, 0]
+        dy = points[:, 1:2] - nodes[idx_c, 1]
+        keep = valid & (dx * dx + dy * dy - radii[idx_c] ** 2 < 0.0)
+        if k >= n or not np.any(keep.sum(axis=1) == k):
+            break
+        k = min(2 * k, n)
+    key = np.where(keep, idx_c, n + 1)
+    order = np.argsort(key, axis=1, kind="stable")
+    idx_s = np.take_along_axis(idx_c, order, axis=1)
+    keep_s = np.take_along_axis(keep, order, axis=1)
+    K = int(keep_s.sum(axis=1).max())
+    return idx_s[:, :K], keep_s[:, :K]
+
+
 def mls_shape(points: np.ndarray, nodes: np.ndarray, radii: np.ndarray, origin: np.ndarray):
     """Linear-basis MLS shape functions N, dN/dx, dN/dy at `points` from `nodes` with influence
     radii `radii` (Preprocessor/MLS2DWithDerivatives.m:65-165).
 
     Returns (ptr, idx, N, dNdx, dNdy) in CSR form with support lists in ascending node order
     (the order Preprocessor/SupportDomain.m:17-18 produces)."""
-    tree = cKDTree(nodes)
-    cand = tree.query_ball_point(points, r=float(radii.max()))
+    idx, mask = _supports(points, nodes, radii)
     P = points.shape[0]
-    rows: List[np.ndarray] = []
-    for i in range(P):
-        c = np.asarray(sorted(cand[i]), dtype=np.int64)
-        dx = points[i, 0] - nodes[c, 0]
-        dy = points[i, 1] - nodes[c, 1]
-        keep = dx * dx + dy * dy - radii[c] ** 2 < 0.0
-        rows.append(c[keep])
-    counts = np.array([len(r) for r in rows], dtype=np.int64)
-    K = int(counts.max())
-    idx = np.zeros((P, K), dtype=np.int64)
-    mask = np.zeros((P, K), dtype=bool)
-    for i, r in enumerate(rows):
-        idx[i, :len(r)] = r
-        mask[i, :len(r)] = True
+    counts = mask.sum(axis=1).astype(np.int64)
     relx = points[:, 0:1] - nodes[idx, 0]
     rely = points[:, 1:2] - nodes[idx, 1]
     d = radii[idx]
@@ -351,7 +363,8 @@ def critical_dt(body: Body, mu: float, lam: float, kn: float) -> float:
     K = (B.T @ Dg @ B).tocsr()
     minv_sqrt = 1.0 / np.sqrt(body.mass.reshape(-1))
     S = sp.diags(minv_sqrt) @ K @ sp.diags(minv_sqrt)
-    lam_max = float(eigsh(S, k=1, which="LA", return_eigenvectors=False, tol=1e-6)[0])
+    v0 = np.ones(S.shape[0])
+    lam_max = float(eigsh(S, k=1, which="LA", return_eigenvectors=False, tol=1e-6, v0=v0)[0])
     h_b = body.nodal_distance
     m_border = body.mass[: len(body.borders[0]["nodes"]) - 1, 0]
     lam_c = float(np.max(kn * h_b / m_border))
@@ -397,7 +410,7 @@ def disc_lattice_scene(seed: int = 0, nx: int = 4, ny: int = 4, pitch: float = 2
     bodies += [bot, top]
     mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
     dtc = min(critical_dt(b, mu, lam, 1e10) for b in bodies if b.kind == "deformable")
-    dt = 0.5 * dtc
+    dt = float("%.4g" % (0.5 * dtc))      # 4 significant digits: reproducible across BLAS builds
     return Scene(name=name, bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
                  contact_update_period=prox_every * dt,
                  meta=dict(config="lattice", seed=seed, dt_crit=dtc))
@@ -420,6 +433,13 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
     f["next_contact_update"] = 0.0
     f["solver"] = int(scene.solver)
     sp_ = list(scene.solver_params)
+    if scene.solver not in (2, 3):          # Code/IO.h:821-893 reads these only for mass scaling
+        sp_[3:7] = [0.0, 0.0, 0.0, 0.0]
+    if scene.solver == 4:
+        sp_[0:3] = [0.0, 0.0, 0.0]
+        sp_[7] = 0.0
+    else:
+        sp_[7] = 1.0 / sp_[0]
     f["solver_params"] = np.array(sp_, dtype=np.float64)
     flags = np.zeros(11, dtype=np.int32)
     flags[7] = 1                          # NO_LOG
@@ -464,7 +484,6 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
             rigid[i, 4] = b.rigid_inertia
             rigid[i, 5] = 1.0 / b.rigid_mass
             rigid[i, 6] = 1.0 / b.rigid_inertia
-            rigid[i, 7:9] = b.centre            # current
             rigid[i, 13:15] = b.velocity
     f["rigid"] = rigid.reshape(-1)
     N = int(nn.sum())
@@ -693,3 +712,119 @@ def write_asc(scene: Scene, directory: str) -> None:
                 w(" \nRIGID\nactive\n%d\n \nKINEMATICS\n%s %s 0\n0 0 0\n%s %s 0\n \n" % (
                     bi, _g(b.centre[0]), _g(b.centre[1]), _g(vx), _g(vy)))
                 w("FORCES\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
+
+
+# --------------------------------------------------------------------------------------------
+# Biaxial grain packings (the 2000-disc workload and the batched sample distribution)
+# --------------------------------------------------------------------------------------------
+
+def _rsa_pack(rng, radii, width, height, gap, max_tries=2000):
+    """Seeded random sequential addition, largest discs first, inside [0,width]x[0,height]."""
+    order = np.argsort(-radii, kind="stable")
+    cell = 2.0 * float(radii.max()) + gap
+    grid: Dict[Tuple[int, int], List[int]] = {}
+    centres = np.zeros((len(radii), 2))
+    placed = np.zeros(len(radii), dtype=bool)
+    for i in order:
+        r = radii[i]
+        for _ in range(max_tries):
+            x = rng.uniform(r + gap, width - r - gap)
+            y = rng.uniform(r + gap, height - r - gap)
+            gx, gy = int(x // cell), int(y // cell)
+            ok = True
+            for ix in range(gx - 1, gx + 2):
+                for iy in range(gy - 1, gy + 2):
+                    for j in grid.get((ix, iy), ()):
+                        dx = centres[j, 0] - x; dy = centres[j, 1] - y
+                        if dx * dx + dy * dy < (r + radii[j] + gap) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                centres[i] = (x, y)
+                placed[i] = True
+                grid.setdefault((gx, gy), []).append(i)
+                break
+    return centres, placed
+
+
+def _disc_worker(args):
+    seed, centre, radius, n_border, n_interior, rho, mass_factor = args
+    import random as _r
+    prng = _r.Random(int(seed))
+    area = math.pi * radius * radius
+    h = math.sqrt(area / (n_border + n_interior))
+    return make_disc(prng, centre, radius, n_border, n_interior, 0.6 * h, 0, rho, mass_factor=mass_factor)
+
+
+def make_discs_parallel(jobs, workers: Optional[int] = None):
+    """Builds discs in a spawn-started process pool (no fork after CUDA initialisation)."""
+    if workers is None:
+        workers = max(1, min(32, (os.cpu_count() or 2)))
+    if workers <= 1 or len(jobs) < 16:
+        return [_disc_worker(j) for j in jobs]
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    ctx = mp.get_context("spawn")
+    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
+        return list(ex.map(_disc_worker, jobs, chunksize=max(1, len(jobs) // (4 * workers))))
+
+
+def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax: float = 1.5e-3,
+                  n_border: int = 64, n_interior: int = 340, aspect: float = 100.0 / 60.0, fill: float = 0.45,
+                  gap: float = 0.02e-3, v_plate: float = 0.05, sigma: float = 100e3, mass_factor: float = 100.0,
+                  mu_fric: float = 0.3, nsteps: int = 50000, prox_every: int = 10, workers: Optional[int] = None,
+                  name: str = "biaxial") -> Scene:
+    """Biaxial compression sample: polydisperse deformable discs packed by seeded random sequential
+    addition, rigid top/bottom plates driven towards each other at v_plate, rigid lateral walls
+    loaded by a constant confining pressure (Neumann, oriented) and fixed vertically.
+
+    The box keeps the workload's 100:60 aspect ratio but is sized so the discs fill `fill` of it
+    (2000 discs with radii in [0.5,1.5] mm cover 1.13x the area of a 100x60 mm box)."""
+    rng = np.random.default_rng(seed)
+    radii = rng.uniform(rmin, rmax, size=n_discs)
+    area = float(np.sum(np.pi * radii ** 2))
+    W = math.sqrt(area / fill * aspect)
+    H = W / aspect
+    centres, placed = _rsa_pack(rng, radii, W, H, gap)
+    tries = 0
+    while not placed.all() and tries < 5:      # enlarge slightly until every disc fits
+        W *= 1.03; H *= 1.03; tries += 1
+        centres, placed = _rsa_pack(rng, radii, W, H, gap)
+    if not placed.all():
+        raise RuntimeError("packing failed")
+    E, nu, rho = 1e8, 0.3, 2500.0
+    mats = [("Grain", 0, [rho, 0.0, 0.0, E, nu, 1000.0]), ("Steel", 0, [7800.0, 0.0, 0.0, 2e11, 0.3, 500.0])]
+    laws = [("Grain", "Grain", 2, 0, [1e10, 1e9, mu_fric, 0.0, 0.0]),
+            ("Grain", "Steel", 2, 0, [1e10, 1e9, mu_fric, 0.0, 0.0])]
+    seeds = rng.integers(0, 2 ** 31 - 1, size=n_discs)
+    jobs = [(int(seeds[i]), (float(centres[i, 0]), float(centres[i, 1])), float(radii[i]), n_border, n_interior,
+             rho, mass_factor) for i in range(n_discs)]
+    bodies = make_discs_parallel(jobs, workers)
+    h_min = 2.0 * math.pi * rmin / n_border
+    thick = 0.05 * H
+    hist = lambda v: (np.array([0.0, T_HIST_END]), np.array([v, v]))
+    bot = make_rect_rigid(-0.05 * W, -thick, 1.05 * W, 0.0, 2.0 * h_min, 1, 7800.0,
+                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(v_plate)), 0.5 * h_min, 0.5 * h_min)
+    top = make_rect_rigid(-0.05 * W, H, 1.05 * W, H + thick, 2.0 * h_min, 1, 7800.0,
+                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(-v_plate)), 0.5 * h_min, 0.5 * h_min)
+    wall_h = 0.9 * H
+    y0 = 0.05 * H
+    perim = 2.0 * (wall_h + thick)
+    p_eff = sigma * wall_h / perim          # oriented load per unit border length, total = sigma * wall height
+    left = make_rect_rigid(-thick, y0, 0.0, y0 + wall_h, 2.0 * h_min, 1, 7800.0,
+                           (BC_ORIENTED, (0.0, 0.0), hist(p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
+    right = make_rect_rigid(W, y0, W + thick, y0 + wall_h, 2.0 * h_min, 1, 7800.0,
+                            (BC_ORIENTED, (0.0, 0.0), hist(-p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
+    bodies += [bot, top, left, right]
+    mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    smallest = np.argsort(radii)[:3]
+    dtc = min(critical_dt(bodies[i], mu, lam, 1e10) for i in smallest)
+    dt = float("%.4g" % (0.5 * dtc))
+    return Scene(name=name, bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
+                 contact_update_period=prox_every * dt,
+                 meta=dict(config="biaxial", seed=seed, dt_crit=dtc, box=(W, H), n_discs=n_discs,
+                           radii=(rmin, rmax), sigma=sigma, v_plate=v_plate, mass_factor=mass_factor))

@@ -1,0 +1,282 @@
+"""Python mirror of the solver's C ABI (include/melgpu.h) over libmelgpu.so.
+
+    s = Solver.from_flat(generator.flatten(scene))      # or Solver.from_files(dir)
+    s.step(100)                                          # Euler_step + proximity cadence
+    st = s.node_state()                                  # u, v, a, up, vp, ap per node
+
+The library is required: importing works without it, but every constructor raises if
+libmelgpu.so cannot be loaded or no CUDA device is present (there is no CPU fallback)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmelgpu.so")
+_lib = None
+
+# every exported entry point with its argument types (restype is mel_status unless stated)
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+SIGNATURES = {
+    "mel_create": [C.POINTER(abi.MelModelDesc), C.POINTER(abi.MelOptions), C.POINTER(_vp)],
+    "mel_create_from_files": [C.c_char_p, C.c_int, C.POINTER(abi.MelOptions), C.POINTER(_vp)],
+    "mel_destroy": [_vp],
+    "mel_step": [_vp, C.POINTER(abi.MelStepIO)],
+    "mel_update_proximity": [_vp],
+    "mel_set_contacts": [_vp, C.POINTER(abi.MelContact), C.c_int],
+    "mel_get_node_state": [_vp, _dp],
+    "mel_set_node_state": [_vp, _dp],
+    "mel_get_positions": [_vp, _dp],
+    "mel_get_forces": [_vp, _dp, _dp, _dp, _dp, _dp],
+    "mel_get_rigid": [_vp, _dp, _dp],
+    "mel_get_works": [_vp, _dp],
+    "mel_get_contact_count": [_vp, _ip],
+    "mel_get_contacts": [_vp, C.POINTER(abi.MelContact), C.c_int, _ip],
+    "mel_get_time": [_vp, _dp, _dp],
+    "mel_monitor_compute": [_vp, C.POINTER(abi.MelMonitor)],
+    "mel_set_rigid": [_vp, _dp],
+    "mel_set_time": [_vp, C.c_double, C.c_double, C.c_double],
+    "mel_record_forces": [_vp, C.c_int],
+    "mel_set_timing": [_vp, C.c_int],
+    "mel_get_error_words": [_vp, C.POINTER(C.c_uint), C.c_int],
+    "mel_load_desc": [C.c_char_p, C.c_int, C.POINTER(C.POINTER(abi.MelModelDesc)), C.POINTER(_vp)],
+    "mel_free_desc": [_vp],
+    "mel_get_kernel_times": [_vp, _dp, _dp, _dp, _dp, _ip],
+    "mel_get_sizes": [_vp, _ip, _ip, _ip, _ip, _ip, _ip],
+}
+
+
+class MelError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads libmelgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m melody2d_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.mel_last_error_string.restype = C.c_char_p
+        L.mel_last_error_string.argtypes = []
+        L.mel_abi_version.restype = C.c_int
+        L.mel_abi_version.argtypes = []
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise MelError(rc, lib().mel_last_error_string().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class Solver:
+    """One resident model on one GPU (a mel_handle)."""
+
+    def __init__(self, handle, nn: int, nb: int, keep=None):
+        self.h = handle
+        self.nn = nn
+        self.nb = nb
+        self._keep = keep
+
+    # ---- construction -------------------------------------------------------------------
+    @classmethod
+    def from_flat(cls, flat: dict, precision: int = 0, device: int = 0) -> "Solver":
+        L = lib()
+        desc = abi.Desc(flat)
+        opt = abi.MelOptions(precision=precision, device=device, use_graph=0, max_contacts=0)
+        h = C.c_void_p()
+        _check(L.mel_create(C.byref(desc.desc), C.byref(opt), C.byref(h)))
+        return cls(h, len(flat["node_domain"]), len(flat["body_type"]), keep=desc)
+
+    @classmethod
+    def from_files(cls, directory: str, restart_index: int = 0, precision: int = 0, device: int = 0) -> "Solver":
+        L = lib()
+        opt = abi.MelOptions(precision=precision, device=device, use_graph=0, max_contacts=0)
+        h = C.c_void_p()
+        _check(L.mel_create_from_files(directory.encode(), restart_index, C.byref(opt), C.byref(h)))
+        s = cls(h, 0, 0)
+        sizes = s.sizes()
+        s.nn, s.nb = sizes["n_nodes"], sizes["n_bodies"]
+        return s
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mel_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- stepping -------------------------------------------------------------------------
+    def step(self, n: int = 1, proximity: bool = True) -> abi.MelStepIO:
+        io = abi.MelStepIO(nsteps=int(n), run_proximity=1 if proximity else 0)
+        _check(lib().mel_step(self.h, C.byref(io)))
+        return io
+
+    def update_proximity(self):
+        _check(lib().mel_update_proximity(self.h))
+
+    # ---- state ----------------------------------------------------------------------------
+    def node_state(self) -> np.ndarray:
+        a = np.zeros(12 * self.nn)
+        _check(lib().mel_get_node_state(self.h, _ptr(a)))
+        return a.reshape(-1, 12)
+
+    def set_node_state(self, st: np.ndarray):
+        a = np.ascontiguousarray(st, dtype=np.float64).reshape(-1)
+        _check(lib().mel_set_node_state(self.h, _ptr(a)))
+
+    def positions(self) -> np.ndarray:
+        a = np.zeros(2 * self.nn)
+        _check(lib().mel_get_positions(self.h, _ptr(a)))
+        return a.reshape(-1, 2)
+
+    def record_forces(self, on: bool = True):
+        _check(lib().mel_record_forces(self.h, 1 if on else 0))
+
+    def set_timing(self, on: bool = True):
+        _check(lib().mel_set_timing(self.h, 1 if on else 0))
+
+    def forces(self) -> dict:
+        arrs = [np.zeros(2 * self.nn) for _ in range(5)]
+        _check(lib().mel_get_forces(self.h, *[_ptr(a) for a in arrs]))
+        return {k: a.reshape(-1, 2) for k, a in zip(("internal", "contact", "neumann", "dirichlet", "total"), arrs)}
+
+    def rigid(self):
+        r = np.zeros(abi.MEL_RIGID_NF * self.nb)
+        f = np.zeros(12 * self.nb)
+        _check(lib().mel_get_rigid(self.h, _ptr(r), _ptr(f)))
+        return r.reshape(self.nb, -1), f.reshape(self.nb, -1)
+
+    def set_rigid(self, r: np.ndarray):
+        a = np.ascontiguousarray(r, dtype=np.float64).reshape(-1)
+        _check(lib().mel_set_rigid(self.h, _ptr(a)))
+
+    def set_time(self, time: float, dt: float, next_contact_update: float):
+        _check(lib().mel_set_time(self.h, float(time), float(dt), float(next_contact_update)))
+
+    def works(self) -> np.ndarray:
+        w = np.zeros(7 * self.nb)
+        _check(lib().mel_get_works(self.h, _ptr(w)))
+        return w.reshape(self.nb, 7)
+
+    def contacts(self) -> np.ndarray:
+        n = C.c_int()
+        _check(lib().mel_get_contact_count(self.h, C.byref(n)))
+        buf = (abi.MelContact * max(1, n.value))()
+        _check(lib().mel_get_contacts(self.h, buf, n.value, C.byref(n)))
+        return abi.contacts_to_numpy(buf, n.value)
+
+    def set_contacts(self, arr: np.ndarray):
+        buf = abi.numpy_to_contacts(arr)
+        _check(lib().mel_set_contacts(self.h, buf, len(arr)))
+
+    def time(self):
+        t = C.c_double(); dt = C.c_double()
+        _check(lib().mel_get_time(self.h, C.byref(t), C.byref(dt)))
+        return t.value, dt.value
+
+    def monitor(self) -> abi.MelMonitor:
+        m = abi.MelMonitor()
+        _check(lib().mel_monitor_compute(self.h, C.byref(m)))
+        return m
+
+    def error_words(self) -> np.ndarray:
+        w = (C.c_uint * 8)()
+        _check(lib().mel_get_error_words(self.h, w, 8))
+        return np.array(list(w), dtype=np.uint32)
+
+    def kernel_times(self) -> dict:
+        v = [C.c_double() for _ in range(4)]
+        n = C.c_int()
+        _check(lib().mel_get_kernel_times(self.h, *[C.byref(x) for x in v], C.byref(n)))
+        return dict(contact=v[0].value, body=v[1].value, rigid=v[2].value, proximity=v[3].value, launches=n.value)
+
+    def sizes(self) -> dict:
+        v = [C.c_int() for _ in range(6)]
+        _check(lib().mel_get_sizes(self.h, *[C.byref(x) for x in v]))
+        keys = ("n_bodies", "n_nodes", "n_gauss", "n_gp_entries", "n_node_entries", "n_border_nodes")
+        return {k: x.value for k, x in zip(keys, v)}
+
+
+def load_desc_arrays(directory: str, restart_index: int = 0) -> dict:
+    """Parses the reference's input files with the library's loader (no GPU needed) and returns
+    the flattened arrays (same keys as generator.flatten)."""
+    L = lib()
+    dp = C.POINTER(abi.MelModelDesc)()
+    owner = C.c_void_p()
+    _check(L.mel_load_desc(directory.encode(), restart_index, C.byref(dp), C.byref(owner)))
+    try:
+        d = dp.contents
+        out = {}
+        def arr(ptr, n, dtype):
+            if n <= 0:
+                return np.zeros(0, dtype=dtype)
+            return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype).copy()
+        nb, nn, nbd, ng, nm = d.n_bodies, d.n_nodes, d.n_borders, d.n_gauss, d.n_materials
+        out["period"] = np.array(list(d.period)); out["gravity"] = np.array(list(d.gravity))
+        out["time"] = d.time; out["dt"] = d.dt; out["tend"] = d.tend
+        out["contact_update_period"] = d.contact_update_period; out["next_contact_update"] = d.next_contact_update
+        out["solver"] = d.solver; out["solver_params"] = np.array(list(d.solver_params)); out["flags"] = np.array(list(d.flags))
+        out["material_type"] = arr(d.material_type, nm, np.int32)
+        out["material_params"] = arr(d.material_params, nm * abi.MEL_MAT_NPARAM, np.float64)
+        out["law_type"] = arr(d.law_type, d.n_laws, np.int32); out["law_length"] = arr(d.law_length, d.n_laws, np.int32)
+        out["law_params"] = arr(d.law_params, d.n_laws * abi.MEL_LAW_NPARAM, np.float64)
+        out["contacts_table"] = arr(d.contacts_table, nm * nm, np.int32)
+        for k in ("body_type", "body_material", "body_periodic", "body_status"):
+            out[k] = arr(getattr(d, k), nb, np.int32)
+        out["body_dist"] = arr(d.body_dist, 3 * nb, np.float64)
+        for k in ("body_node_ptr", "body_border_ptr", "body_gp_ptr", "body_cell_ptr"):
+            out[k] = arr(getattr(d, k), nb + 1, np.int32)
+        out["rigid"] = arr(d.rigid, nb * abi.MEL_RIGID_NF, np.float64)
+        out["node_x0"] = arr(d.node_x0, 2 * nn, np.float64); out["node_mass"] = arr(d.node_mass, 2 * nn, np.float64)
+        out["node_inv_mass"] = arr(d.node_inv_mass, 2 * nn, np.float64); out["node_domain"] = arr(d.node_domain, nn, np.float64)
+        out["node_sup_ptr"] = arr(d.node_sup_ptr, nn + 1, np.int32)
+        ns = int(out["node_sup_ptr"][-1])
+        out["node_sup_idx"] = arr(d.node_sup_idx, ns, np.int32); out["node_sup_N"] = arr(d.node_sup_N, ns, np.float64)
+        out["node_state"] = arr(d.node_state, 12 * nn, np.float64)
+        for k in ("border_body", "border_periodicity", "border_interpolant", "border_before", "border_after"):
+            out[k] = arr(getattr(d, k), nbd, np.int32)
+        out["border_node_ptr"] = arr(d.border_node_ptr, nbd + 1, np.int32)
+        ne = int(out["border_node_ptr"][-1])
+        out["border_nodes"] = arr(d.border_nodes, ne, np.int32)
+        out["border_bc_type"] = arr(d.border_bc_type, 2 * nbd, np.int32)
+        out["border_bc_param"] = arr(d.border_bc_param, 4 * nbd, np.float64)
+        out["border_hist_ptr"] = arr(d.border_hist_ptr, 2 * nbd + 1, np.int32)
+        nh = int(out["border_hist_ptr"][-1])
+        out["hist_time"] = arr(d.hist_time, nh, np.float64); out["hist_value"] = arr(d.hist_value, nh, np.float64)
+        out["gp_sup_ptr"] = arr(d.gp_sup_ptr, ng + 1, np.int32)
+        nge = int(out["gp_sup_ptr"][-1])
+        out["gp_sup_idx"] = arr(d.gp_sup_idx, nge, np.int32)
+        for k in ("gp_N", "gp_dNdx", "gp_dNdy"):
+            out[k] = arr(getattr(d, k), nge, np.float64)
+        out["gp_weight"] = arr(d.gp_weight, ng, np.float64); out["gp_jacobian"] = arr(d.gp_jacobian, ng, np.float64)
+        out["cells"] = arr(d.cells, 3 * d.n_cells, np.int32)
+        out["body_matrix_ptr"] = arr(d.body_matrix_ptr, nb + 1, np.int32)
+        out["matrix_dofs"] = arr(d.matrix_dofs, 2 * d.n_matrix, np.int32)
+        out["matrix_stiffness"] = arr(d.matrix_stiffness, d.n_matrix, np.float64)
+        out["matrix_damping"] = arr(d.matrix_damping, d.n_matrix, np.float64)
+        return out
+    finally:
+        L.mel_free_desc(owner)

@@ -10,10 +10,17 @@
  * -ffp-contract=off, as oracle/Makefile does).
  */
 #include "mel_oracle.h"
+#include "../melody2d_b200/csrc/mel_rsqrt.h"
 
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+
+/* x^(-1/2) as the reference computes it (glibc pow) or correctly rounded (the GPU's value);
+ * see orc_set_rsqrt_mode. */
+static int g_cr_rsqrt = 0;
+static inline double orc_rsqrt(double x) { return g_cr_rsqrt ? mel_rsqrt(x) : pow(x, -0.5); }
+void orc_set_rsqrt_mode(int correctly_rounded) { g_cr_rsqrt = correctly_rounded; }
 
 typedef struct { int n, cap; mel_contact* a; } cvec;
 typedef struct { int body2, border2, shift; } nbr_t;
@@ -103,9 +110,9 @@ static void closest_2_segment_linear(double Xs, double Ys, double X0, double Y0,
                                      double* Ytan, double* N0, double* N1, double* N2, double* N3, int* flag)
 {
     double Xclosest, Yclosest;
-    double ilength = pow((X2 - X1) * (X2 - X1) + (Y2 - Y1) * (Y2 - Y1), -0.5);
-    double ilengthm = pow((X1 - X0) * (X1 - X0) + (Y1 - Y0) * (Y1 - Y0), -0.5);
-    double ilengthp = pow((X3 - X2) * (X3 - X2) + (Y3 - Y2) * (Y3 - Y2), -0.5);
+    double ilength = orc_rsqrt((X2 - X1) * (X2 - X1) + (Y2 - Y1) * (Y2 - Y1));
+    double ilengthm = orc_rsqrt((X1 - X0) * (X1 - X0) + (Y1 - Y0) * (Y1 - Y0));
+    double ilengthp = orc_rsqrt((X3 - X2) * (X3 - X2) + (Y3 - Y2) * (Y3 - Y2));
     *Xtan = (X2 - X1) * ilength;
     *Ytan = (Y2 - Y1) * ilength;
     *Xnorm = *Ytan;
@@ -130,7 +137,7 @@ static void closest_2_segment_linear(double Xs, double Ys, double X0, double Y0,
                 *N0 = 0.; *N1 = 1.; *N2 = 0.; *N3 = 0.;
                 *flag = -1;
             } else if (xsi < -1.) {
-                double invdistm = pow((Xs - X1) * (Xs - X1) + (Ys - Y1) * (Ys - Y1), -0.5);
+                double invdistm = orc_rsqrt((Xs - X1) * (Xs - X1) + (Ys - Y1) * (Ys - Y1));
                 double xn = (Xs - X1) * invdistm, yn = (Ys - Y1) * invdistm;
                 if (-yn * (xt + Xtanm) + xn * (yt + Ytanm) < 0.) { xn = -xn; yn = -yn; }
                 *Xnorm = xn; *Ynorm = yn; *Xtan = -yn; *Ytan = xn;
@@ -144,7 +151,7 @@ static void closest_2_segment_linear(double Xs, double Ys, double X0, double Y0,
                 *N0 = 0.; *N1 = 0.; *N2 = 1.; *N3 = 0.;
                 *flag = 1;
             } else if (xsi > 1.) {
-                double invdistp = pow((Xs - X2) * (Xs - X2) + (Ys - Y2) * (Ys - Y2), -0.5);
+                double invdistp = orc_rsqrt((Xs - X2) * (Xs - X2) + (Ys - Y2) * (Ys - Y2));
                 double xn = (Xs - X2) * invdistp, yn = (Ys - Y2) * invdistp;
                 if (-yn * (xt + Xtanp) + xn * (yt + Ytanp) < 0.) { xn = -xn; yn = -yn; }
                 *Xnorm = xn; *Ynorm = yn; *Xtan = -yn; *Ytan = xn;
@@ -169,7 +176,7 @@ static void closest_2_segment_self(double Xs, double Ys, double X1, double Y1, d
                                    double* Gap, double* Xsi, double* Xnorm, double* Ynorm, double* Xtan,
                                    double* Ytan, double* N0, double* N1, double* N2, double* N3, int* flag)
 {
-    double ilength = pow((X2 - X1) * (X2 - X1) + (Y2 - Y1) * (Y2 - Y1), -0.5);
+    double ilength = orc_rsqrt((X2 - X1) * (X2 - X1) + (Y2 - Y1) * (Y2 - Y1));
     double xt = (X2 - X1) * ilength, yt = (Y2 - Y1) * ilength;
     *Xtan = xt; *Ytan = yt;
     if (((Xs - X1) * xt + (Ys - Y1) * yt) * (xt * xt + yt * yt) >= 0.) {
@@ -642,8 +649,8 @@ static void update_bc_forces(orc_model* m, int b)
                     int a = n0 + m->s_node[0][e], c = n0 + m->s_node[2][e];
                     double x0 = m->X0[2 * a], y0 = m->X0[2 * a + 1], x2 = m->X0[2 * c], y2 = m->X0[2 * c + 1];
                     double xp0 = m->x[2 * a], yp0 = m->x[2 * a + 1], xp2 = m->x[2 * c], yp2 = m->x[2 * c + 1];
-                    double invl = pow((x2 - x0) * (x2 - x0) + (y2 - y0) * (y2 - y0), -0.5);
-                    double invlp = pow((xp2 - xp0) * (xp2 - xp0) + (yp2 - yp0) * (yp2 - yp0), -0.5);
+                    double invl = orc_rsqrt((x2 - x0) * (x2 - x0) + (y2 - y0) * (y2 - y0));
+                    double invlp = orc_rsqrt((xp2 - xp0) * (xp2 - xp0) + (yp2 - yp0) * (yp2 - yp0));
                     ftx = (x2 - x0) * invl; fty = (y2 - y0) * invl;
                     ftpx = (xp2 - xp0) * invlp; ftpy = (yp2 - yp0) * invlp;
                 }

@@ -46,6 +46,7 @@ def lib():
         L.orc_get_neighbours.argtypes = [vp, C.POINTER(C.c_int), C.c_int]
         L.orc_stale_shape_events.argtypes = [vp]; L.orc_stale_shape_events.restype = C.c_long
         L.orc_solver_stats.argtypes = [vp, C.POINTER(C.c_double)]
+        L.orc_set_rsqrt_mode.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -54,11 +55,18 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def set_rsqrt_mode(correctly_rounded: bool) -> None:
+    """0: x^(-1/2) through glibc pow as the reference; 1: correctly rounded, as the GPU kernels."""
+    lib().orc_set_rsqrt_mode(1 if correctly_rounded else 0)
+
+
 class Oracle:
     """CPU restatement of the reference step on a flattened scene (generator.flatten)."""
 
-    def __init__(self, flat: dict, n_regions: Optional[np.ndarray] = None):
+    def __init__(self, flat: dict, n_regions: Optional[np.ndarray] = None, correctly_rounded: bool = False):
         self.L = lib()
+        self.cr = bool(correctly_rounded)
+        set_rsqrt_mode(self.cr)
         self.flat = flat
         self.desc = abi.Desc(flat)
         self.nn = len(flat["node_domain"])
@@ -85,9 +93,11 @@ class Oracle:
             pass
 
     def step(self, n: int, proximity: bool = True):
+        set_rsqrt_mode(self.cr)
         self.L.orc_step(self.h, int(n), 1 if proximity else 0)
 
     def update_proximity(self):
+        set_rsqrt_mode(self.cr)
         self.L.orc_update_proximity(self.h)
 
     @property

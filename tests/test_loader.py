@@ -1,0 +1,25 @@
+"""The library's reader of STATIC_CONTROL / STATIC_DATA / DYNAMIC files reproduces the flattened
+model the generator wrote (Load_static / Load_dynamic token order, Code/IO.h:598-2345)."""
+import numpy as np
+
+from conftest import flat_of, squeezed_lattice
+
+
+def test_asc_roundtrip(tmp_path, gpu_lib):
+    from melody2d_b200 import generator as g, solver
+    scene = squeezed_lattice(3, 3)
+    g.write_asc(scene, str(tmp_path))
+    d = solver.load_desc_arrays(str(tmp_path))
+    f = flat_of(scene)
+    for k, v in f.items():
+        if k == "material_names":
+            continue
+        np.testing.assert_array_equal(np.asarray(v), np.asarray(d[k]), err_msg=k)
+
+
+def test_missing_files_report_io_error(tmp_path, gpu_lib):
+    from melody2d_b200 import solver
+    import pytest
+    with pytest.raises(solver.MelError) as e:
+        solver.load_desc_arrays(str(tmp_path / "nope"))
+    assert e.value.code == 8
