@@ -1,0 +1,291 @@
+"""Throughput of the MELODY 2D explicit step on B200: node-steps/s on the 2000-disc biaxial sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--discs 2000]
+
+One JSON line on rank 0.  A step is one Euler_step (Code/Solver.h:10-88) of the whole sample plus
+the proximity updates that fall in it (Code/main.cpp:191-196, every 10 steps).  `value` is deformable
+node-steps per second of device time over the timed K steps (inputs ~1.5 GB per step, larger than
+L2); `e2e` repeats the measurement through the public C ABI with a device->host read of the
+monitored quantities every step; `cpu_baseline` is the reference solver, compiled from its sources,
+timed on this host's cores on a bounded sample of the same workload.  Under torchrun every rank
+advances its own independent sample (weak scaling, no collective in the step)."""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-steps/s"
+DEFAULT_STEPS = 2000
+DEFAULT_WARMUP = 20
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() in ("active", "1", "yes")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def allreduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------------------------
+# reference CPU path (the reference solver compiled from its sources, oracle/_ref)
+# --------------------------------------------------------------------------------------------
+def reference_sample(n_discs: int, steps: int, threads: int, seed: int = 1):
+    """Runs the reference's own Euler_step loop (oracle/_ref/ref_harness) on a seeded sample of the
+    biaxial workload (same disc size distribution, nodes per disc, materials, contact law, loading)
+    and returns node-steps/s of its step loop."""
+    from melody2d_b200 import generator as g
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    scene = g.biaxial_scene(seed=seed, n_discs=n_discs)
+    with tempfile.TemporaryDirectory() as tmp:
+        g.write_asc(scene, tmp)
+        if os.path.exists(harness):
+            out = subprocess.run([harness, tmp, str(steps), "-", "0", str(threads)], check=True,
+                                 capture_output=True, text=True).stdout
+            r = json.loads(out.strip().splitlines()[-1])
+            return r["deformable_nodes"] * r["steps"] / r["wall_s"], threads, "reference", scene
+    # no compiled reference on this machine: the C restatement (one thread)
+    from oracle.pyoracle import Oracle
+    flat = g.flatten(scene)
+    o = Oracle(flat)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return scene.n_deformable_nodes * steps / dt, 1, "port", scene
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world, pg):
+    if rank != 0:
+        return
+    threads = host_threads()
+    rate, cores, kind, scene = reference_sample(args.ref_discs, args.ref_steps, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "node-steps/s", "n_gpus": args.gpus,
+            "steps": args.ref_steps, "warmup": 0, "ms_per_step": 1e3 * scene.n_deformable_nodes / rate,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded biaxial packing generator)",
+            "config": {"workload": f"biaxial sample: {args.ref_discs} deformable discs of the 2000-disc workload "
+                                   f"(radii U[0.5,1.5] mm, 64 border + 340 interior nodes, MLS, MohrCoulomb), "
+                                   f"2 driven plates, 2 confining walls", "nodes": scene.n_deformable_nodes},
+            "cpu_baseline": {"value": rate, "unit": "node-steps/s", "cores": cores, "kind": kind,
+                             "sample": f"{args.ref_discs}-disc sample, {args.ref_steps} steps"},
+            "e2e": {"value": rate, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------------------------
+# our path
+# --------------------------------------------------------------------------------------------
+def run_ours(args, rank, world, local, pg):
+    from melody2d_b200 import abi, generator as g
+    from melody2d_b200.solver import Solver
+    workers = max(1, host_threads() // max(1, world))
+    t0 = time.perf_counter()
+    scene = g.biaxial_scene(seed=1 + rank, n_discs=args.discs, workers=workers)
+    flat = g.flatten(scene)
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    s = Solver.from_flat(flat, precision=0, device=local)
+    t_create = time.perf_counter() - t0
+    model_bytes = sum(np.asarray(v).nbytes for k, v in flat.items() if k != "material_names")
+    nodes = s.step_stats()["n_deformable_nodes"]
+    s.step(args.warmup)
+    s.set_timing(True)
+    clocks = ClockSampler(local)
+    barrier(pg)
+    clocks.start()
+    io = s.step(args.steps)                               # synchronises on its stream at the end
+    barrier(pg)
+    clk = clocks.stop()
+    st = s.step_stats()
+    kt = s.kernel_times()
+    ms_total = allreduce_max(pg, st["ms_total"])
+    value = allreduce_sum(pg, nodes) * args.steps / (ms_total * 1e-3)
+    # roofline of the dominant kernel (body kernel), from its CUDA-event time in the region
+    body_ms = kt["body"] / args.steps
+    contact_ms = kt["contact"] / args.steps
+    peak, peak_kind = measured_hbm_peak()
+    achieved = st["bytes_body"] / (body_ms * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "body_kernel_traffic.json")
+    if os.path.exists(prof):
+        try:
+            pj = json.load(open(prof))
+            traffic = pj["dram_bytes_per_gauss_point"] * s.sizes()["n_gauss"]
+        except Exception:
+            traffic = None
+    # end to end through the C ABI: every iteration steps and reads the monitored quantities back
+    s.set_timing(False)
+    n_e2e = min(args.steps, args.e2e_steps)
+    mon = abi.MelMonitor()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        s.step(1)
+        m = s.monitor()
+    t_e2e = time.perf_counter() - t0
+    t_e2e = allreduce_max(pg, t_e2e)
+    e2e_value = allreduce_sum(pg, nodes) * n_e2e / t_e2e
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, cores, kind, _ = reference_sample(args.ref_discs, args.ref_steps, host_threads())
+        cpu = {"value": rate, "unit": "node-steps/s", "cores": cores, "kind": kind,
+               "sample": f"{args.ref_discs}-disc sample of the same workload, {args.ref_steps} steps, all host threads"}
+    if rank == 0:
+        sizes = s.sizes()
+        line = {
+            "metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded biaxial packing generator)",
+            "config": {"workload": f"biaxial: {args.discs} deformable discs, radii U[0.5,1.5] mm, 64 border + 340 "
+                                   f"interior nodes each, MLS (linear, W1), ElasticLinear, MohrCoulomb, mass x100, "
+                                   f"plates 0.05 m/s, walls 100 kPa; Euler, dt=0.5 dt_crit; proximity every 10 steps",
+                       "nodes_per_gpu": nodes, "gauss_points": sizes["n_gauss"], "gp_entries": sizes["n_gp_entries"],
+                       "contacts": st["n_contacts"], "precision": "fp64",
+                       "l2": "inputs larger than L2 (%.2f GB streamed per step)" % ((st["bytes_body"] + st["bytes_contact"]) / 1e9),
+                       "generate_s": round(t_gen, 2), "create_s": round(t_create, 2)},
+            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 20 * 8, "steps": n_e2e,
+                    "setup": {"h2d_bytes": int(model_bytes), "create_s": round(t_create, 2)}},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "kernel": "body_kernel", "peak_source": peak_kind,
+                         "bytes_per_launch": st["bytes_body"], "ms_per_launch": body_ms,
+                         "contact_kernel_ms": contact_ms, "proximity_ms_per_step": kt["proximity"] / args.steps},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": kt["launches"],
+            "proximity_updates": io.n_proximity,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=DEFAULT_STEPS)
+    ap.add_argument("--warmup", type=int, default=DEFAULT_WARMUP)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--discs", type=int, default=2000)
+    ap.add_argument("--e2e-steps", type=int, default=500)
+    ap.add_argument("--ref-discs", type=int, default=24)
+    ap.add_argument("--ref-steps", type=int, default=400)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world, pg)
+        else:
+            run_ours(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

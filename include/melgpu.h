@@ -252,6 +252,11 @@ int         mel_abi_version(void);
  * names: "contact", "body", "rigid", "proximity"; returns total milliseconds. */
 mel_status  mel_get_kernel_times(mel_handle* h, double* ms_contact, double* ms_body,
                                  double* ms_rigid, double* ms_proximity, int* launches);
+/* Device time of the last mel_step call (CUDA events around all of its launches), the
+ * algorithmic bytes one launch of the body kernel and of the contact kernel moves (exact array
+ * sizes of the resident layout), deformable node count and current contact count. */
+mel_status  mel_get_step_stats(mel_handle* h, double* ms_total, double* bytes_body, double* bytes_contact,
+                               int* n_deformable_nodes, int* n_contacts);
 /* Sizes of the resident model. */
 mel_status  mel_get_sizes(mel_handle* h, int* n_bodies, int* n_nodes, int* n_gauss,
                           int* n_gp_entries, int* n_node_entries, int* n_border_nodes);

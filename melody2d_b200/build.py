@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmelgpu.so")
+EXE = os.path.join(HERE, "melody_gpu")
 BUILD = os.path.join(HERE, "_build")
 
 CU_SOURCES = ["mel_kernels.cu", "mel_prox.cu", "mel_model.cu"]
@@ -64,6 +65,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(o)
     if force or _newer(LIB, objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    main_src = os.path.join(CSRC, "melody_gpu_main.cpp")
+    if force or _newer(EXE, [main_src, LIB]):
+        cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), main_src, "-o", EXE,
+               "-L" + HERE, "-lmelgpu", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

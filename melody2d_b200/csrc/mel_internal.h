@@ -78,7 +78,7 @@ void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s);
 size_t mel_body_smem_bytes(int max_nodes, int max_border_nodes);
 void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
-void mel_launch_monitor(const mel_dev& d, double* out, cudaStream_t s);
+void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);
 
 void mel_body_kernel_configure(size_t smem);
 // proximity (mel_prox.cu)

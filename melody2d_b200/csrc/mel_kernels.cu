@@ -682,35 +682,45 @@ __global__ void __launch_bounds__(MEL_BODY_THREADS) body_kernel(mel_dev d, int p
 }
 
 // ------------------------------------------------------------------------------------------
-// monitor: kinetic energy (Monitoring.h:528-531), mass-weighted mean displacement (88-101)
+// monitor: kinetic energy (Monitoring.h:528-531), mass-weighted mean displacement (88-101),
+// active contact elements; block partials then a fixed-order final sum (deterministic)
 // ------------------------------------------------------------------------------------------
-__global__ void monitor_kernel(mel_dev d, double* out)
+#define MON_BLOCKS 148
+__global__ void monitor_partial_kernel(mel_dev d, double* part)
 {
-    // one block; fixed-order tree reduction (deterministic)
-    __shared__ double s[4][256];
-    double ke = 0., ux = 0., uy = 0., mt = 0.;
-    for (int b = 0; b < d.nb; b++) {
-        if (d.b_type[b] != MEL_BODY_DEFORMABLE) continue;
-        for (int i = d.b_node0[b] + threadIdx.x; i < d.b_node0[b + 1]; i += blockDim.x) {
-            double2 v = d.v[i], m = d.mass[i], u = d.u[i];
-            ke += 0.5 * v.x * v.x * m.x + 0.5 * v.y * v.y * m.y;
-            ux += u.x * m.x; uy += u.y * m.y; mt += m.x;
-        }
+    __shared__ double s[5][256];
+    double ke = 0., ux = 0., uy = 0., mt = 0., act = 0.;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.nn; i += gridDim.x * blockDim.x) {
+        double2 v = d.v[i], m = d.mass[i], u = d.u[i];
+        ke += 0.5 * v.x * v.x * m.x + 0.5 * v.y * v.y * m.y;
+        ux += u.x * m.x; uy += u.y * m.y; mt += m.x;      // rigid nodes carry zero mass
     }
-    s[0][threadIdx.x] = ke; s[1][threadIdx.x] = ux; s[2][threadIdx.x] = uy; s[3][threadIdx.x] = mt;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.ncont; c += gridDim.x * blockDim.x)
+        if (d.cont[c].fx != 0. || d.cont[c].fy != 0.) act += 1.;
+    s[0][threadIdx.x] = ke; s[1][threadIdx.x] = ux; s[2][threadIdx.x] = uy; s[3][threadIdx.x] = mt; s[4][threadIdx.x] = act;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
         if (threadIdx.x < w)
-            for (int k = 0; k < 4; k++) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+            for (int k = 0; k < 5; k++) s[k][threadIdx.x] += s[k][threadIdx.x + w];
         __syncthreads();
     }
+    if (threadIdx.x < 5) part[threadIdx.x * MON_BLOCKS + blockIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void monitor_final_kernel(mel_dev d, const double* part, const int* rigid_ids, int nrigid, double* out)
+{
     if (threadIdx.x == 0) {
-        out[0] = s[0][0];
-        out[1] = s[3][0] > 0 ? s[1][0] / s[3][0] : 0.;
-        out[2] = s[3][0] > 0 ? s[2][0] / s[3][0] : 0.;
-        int act = 0;
-        for (int c = 0; c < d.ncont; c++) if (d.cont[c].fx != 0. || d.cont[c].fy != 0.) act++;
-        out[3] = act;
+        double t[5] = { 0., 0., 0., 0., 0. };
+        for (int k = 0; k < 5; k++)
+            for (int b = 0; b < MON_BLOCKS; b++) t[k] += part[k * MON_BLOCKS + b];
+        out[0] = t[0];
+        out[1] = t[3] > 0 ? t[1] / t[3] : 0.;
+        out[2] = t[3] > 0 ? t[2] / t[3] : 0.;
+        out[3] = t[4];
+        for (int r = 0; r < nrigid && r < 4; r++) {
+            const double* rf = d.rf + 15 * rigid_ids[r];
+            out[4 + 4 * r] = rf[0]; out[5 + 4 * r] = rf[1]; out[6 + 4 * r] = rf[6]; out[7 + 4 * r] = rf[7];
+        }
     }
 }
 
@@ -739,9 +749,10 @@ void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cud
     mel::body_kernel<<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
 }
 
-void mel_launch_monitor(const mel_dev& d, double* out, cudaStream_t s)
+void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s)
 {
-    mel::monitor_kernel<<<1, 256, 0, s>>>(d, out);
+    mel::monitor_partial_kernel<<<MON_BLOCKS, 256, 0, s>>>(d, part);
+    mel::monitor_final_kernel<<<1, 32, 0, s>>>(d, part, rigid_ids, nrigid, out);
 }
 
 void mel_body_kernel_configure(size_t smem)

@@ -54,7 +54,15 @@ struct mel_handle {
     double t_contact = 0., t_body = 0., t_prox = 0.;
     int timing = 0;
     double* d_monitor = nullptr;
+    double* d_monitor_part = nullptr;
+    int* d_rigid_ids = nullptr;
+    int nrigid = 0;
     int precision = MEL_PREC_FP64;
+    double t_total = 0.;
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+    std::vector<cudaEvent_t> ev_pool;
+    double bytes_body = 0., bytes_contact = 0.;
+    int n_def_nodes = 0;
 };
 
 template <typename T>
@@ -451,7 +459,30 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     h->body_smem = mel_body_smem_bytes(max_def_nodes, 0);
     if (h->body_smem > 227 * 1024) { mel_set_error("body of %d nodes needs %zu bytes of shared memory", max_def_nodes, h->body_smem); return MEL_ERR_UNSUPPORTED; }
     mel_body_kernel_configure(h->body_smem);
-    h->d_monitor = dalloc<double>(h, 8);
+    h->d_monitor = dalloc<double>(h, 32);
+    h->d_monitor_part = dalloc<double>(h, 5 * 148);
+    {
+        std::vector<int> rid;
+        for (int b = 0; b < nb; b++) if (d->body_type[b] == MEL_BODY_RIGID) rid.push_back(b);
+        h->nrigid = (int)rid.size();
+        h->d_rigid_ids = dupload(h, rid);
+    }
+    // algorithmic bytes moved by one launch of each step kernel (exact array sizes):
+    // body kernel: Gauss entries (16-bit index + 16-bit pull position + dN/dx,dN/dy), per point
+    // c0, entry offset, support count; pull records; node state read (up, vp, 1/m, m) and written
+    // (up, vp, ap, u, v, a, x); node supports (16-bit index + N) and offsets; contact records read.
+    {
+        double nd = 0;
+        for (int b = 0; b < nb; b++) if (d->body_type[b] == MEL_BODY_DEFORMABLE) nd += d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+        h->n_def_nodes = (int)nd;
+        double nse_def = 0;
+        for (int b = 0; b < nb; b++)
+            if (d->body_type[b] == MEL_BODY_DEFORMABLE)
+                nse_def += d->node_sup_ptr[d->body_node_ptr[b + 1]] - d->node_sup_ptr[d->body_node_ptr[b]];
+        h->bytes_body = (double)h->nge * (2 + 2 + 16) + (double)h->ng * (8 + 4 + 1) + (double)tn_node.size() * 6 +
+                        (double)chunks.size() * sizeof(mel_chunk) + nd * (4 * 16 + 7 * 16) + nse_def * (2 + 8) + (nd + 1) * 4;
+        h->bytes_contact = (double)ne * (4 * 4 + 4 * 4 + 8 + 8);   // refreshed border lengths (contacts added per call)
+    }
     if (cudaDeviceSynchronize() != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "build", __FILE__, __LINE__); return MEL_ERR_CUDA; }
     return MEL_OK;
 }
@@ -624,6 +655,8 @@ mel_status mel_destroy(mel_handle* h)
     for (void* p : { (void*)P.nbr, (void*)P.task, (void*)P.inc_task, (void*)P.slot_cnt, (void*)P.slot_off, (void*)P.inc_rng,
                      (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)h->d.cont })
         if (p) cudaFree(p);
+    for (auto e : h->ev_pool) cudaEventDestroy(e);
+    if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MEL_OK;
@@ -633,11 +666,16 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
 {
     if (!h || !io || io->nsteps < 0) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
     cudaSetDevice(h->device);
-    h->t_contact = h->t_body = h->t_prox = 0.;
+    h->t_contact = h->t_body = h->t_prox = h->t_total = 0.;
     h->launches = 0;
     int nprox = 0;
+    size_t need = h->timing ? (size_t)3 * io->nsteps : 0;
+    while (h->ev_pool.size() < need) { cudaEvent_t e; cudaEventCreate(&e); h->ev_pool.push_back(e); }
+    if (!h->ev_start) { cudaEventCreate(&h->ev_start); cudaEventCreate(&h->ev_end); }
+    cudaEventRecord(h->ev_start, h->stream);
+    size_t nev = 0;
     std::vector<cudaEvent_t> ev;
-    auto mark = [&]() { if (!h->timing) return; cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); ev.push_back(e); };
+    auto mark = [&]() { if (!h->timing) return; cudaEvent_t e = h->ev_pool[nev++]; cudaEventRecord(e, h->stream); ev.push_back(e); };
     std::vector<int> kinds;
     for (int s = 0; s < io->nsteps; s++) {
         mark();
@@ -656,16 +694,21 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             h->launches += 8;
         }
     }
+    cudaEventRecord(h->ev_end, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) { mel_set_cuda_error(e, "mel_step", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    {
+        float tot = 0.f;
+        cudaEventElapsedTime(&tot, h->ev_start, h->ev_end);
+        h->t_total = tot;
+    }
     if (h->timing) {
-        for (size_t k = 0; k + 1 < ev.size(); k += 3) {
+        for (size_t k = 0; k + 2 < ev.size(); k += 3) {
             float a = 0.f, b = 0.f;
             cudaEventElapsedTime(&a, ev[k], ev[k + 1]);
             cudaEventElapsedTime(&b, ev[k + 1], ev[k + 2]);
             h->t_contact += a; h->t_body += b;
         }
-        for (auto x : ev) cudaEventDestroy(x);
     }
     mel_status rc = check_errors(h);
     if (rc) return rc;
@@ -858,8 +901,8 @@ mel_status mel_monitor_compute(mel_handle* h, mel_monitor* out)
     if (!h || !out) return MEL_ERR_INVALID;
     cudaSetDevice(h->device);
     memset(out, 0, sizeof *out);
-    mel_launch_monitor(h->d, h->d_monitor, h->stream);
-    double m[4];
+    mel_launch_monitor(h->d, h->d_monitor_part, h->d_rigid_ids, h->nrigid, h->d_monitor, h->stream);
+    double m[20];
     MEL_CUDA_OK(cudaMemcpyAsync(m, h->d_monitor, sizeof m, cudaMemcpyDeviceToHost, h->stream));
     MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
     out->time = h->time;
@@ -868,14 +911,9 @@ mel_status mel_monitor_compute(mel_handle* h, mel_monitor* out)
     out->mean_displacement[1] = m[2];
     out->active_contacts = (int)m[3];
     out->n_contacts = h->d.ncont;
-    std::vector<double> rf(15 * (size_t)h->nb);
-    MEL_CUDA_OK(cudaMemcpy(rf.data(), h->d.rf, sizeof(double) * rf.size(), cudaMemcpyDeviceToHost));
-    int r = 0;
-    for (int b = 0; b < h->nb && r < 4; b++) {
-        if (h->b_type[b] != MEL_BODY_RIGID) continue;
-        out->rigid_force[2 * r] = rf[15 * b]; out->rigid_force[2 * r + 1] = rf[15 * b + 1];
-        out->rigid_dirichlet[2 * r] = rf[15 * b + 6]; out->rigid_dirichlet[2 * r + 1] = rf[15 * b + 7];
-        r++;
+    for (int r = 0; r < h->nrigid && r < 4; r++) {
+        out->rigid_force[2 * r] = m[4 + 4 * r]; out->rigid_force[2 * r + 1] = m[5 + 4 * r];
+        out->rigid_dirichlet[2 * r] = m[6 + 4 * r]; out->rigid_dirichlet[2 * r + 1] = m[7 + 4 * r];
     }
     return MEL_OK;
 }
@@ -903,6 +941,18 @@ mel_status mel_get_sizes(mel_handle* h, int* n_bodies, int* n_nodes, int* n_gaus
     if (n_gp_entries) *n_gp_entries = h->nge;
     if (n_node_entries) *n_node_entries = h->nse;
     if (n_border_nodes) *n_border_nodes = h->ne;
+    return MEL_OK;
+}
+
+mel_status mel_get_step_stats(mel_handle* h, double* ms_total, double* bytes_body, double* bytes_contact,
+                              int* n_deformable_nodes, int* n_contacts)
+{
+    if (!h) return MEL_ERR_INVALID;
+    if (ms_total) *ms_total = h->t_total;
+    if (bytes_body) *bytes_body = h->bytes_body;
+    if (bytes_contact) *bytes_contact = h->bytes_contact + (double)h->d.ncont * (2 * sizeof(mel_contact) + 8 + 5 * 16 * 2);
+    if (n_deformable_nodes) *n_deformable_nodes = h->n_def_nodes;
+    if (n_contacts) *n_contacts = h->d.ncont;
     return MEL_OK;
 }
 

@@ -50,6 +50,7 @@ SIGNATURES = {
     "mel_free_desc": [_vp],
     "mel_get_kernel_times": [_vp, _dp, _dp, _dp, _dp, _ip],
     "mel_get_sizes": [_vp, _ip, _ip, _ip, _ip, _ip, _ip],
+    "mel_get_step_stats": [_vp, _dp, _dp, _dp, _ip, _ip],
 }
 
 
@@ -212,6 +213,13 @@ class Solver:
         n = C.c_int()
         _check(lib().mel_get_kernel_times(self.h, *[C.byref(x) for x in v], C.byref(n)))
         return dict(contact=v[0].value, body=v[1].value, rigid=v[2].value, proximity=v[3].value, launches=n.value)
+
+    def step_stats(self) -> dict:
+        v = [C.c_double() for _ in range(3)]
+        n = [C.c_int() for _ in range(2)]
+        _check(lib().mel_get_step_stats(self.h, *[C.byref(x) for x in v], *[C.byref(x) for x in n]))
+        return dict(ms_total=v[0].value, bytes_body=v[1].value, bytes_contact=v[2].value,
+                    n_deformable_nodes=n[0].value, n_contacts=n[1].value)
 
     def sizes(self) -> dict:
         v = [C.c_int() for _ in range(6)]
