@@ -245,6 +245,26 @@ mel_status mel_get_error_words(mel_handle* h, unsigned* words, int n);
 mel_status mel_load_desc(const char* dir, int restart_index, mel_model_desc** desc, void** owner);
 mel_status mel_free_desc(void* owner);
 
+/* Monitored quantities from caller-held device arrays, allocating no device memory.
+ * This entry point has no counterpart in the reference (its monitoring runs on the host,
+ * Code/Monitoring.h).  It serves callers that cannot allocate device memory themselves -- a
+ * framework or runtime that owns all device memory through its own allocator, or a deployment with
+ * a fixed device-memory budget -- and already hold the state on the device.  Inputs (device):
+ * velocity, mass and displacement as x,y pairs for n_nodes nodes, and n_contacts contact elements;
+ * output (device): d_out[0..3] = kinetic energy, mean displacement x and y (mass-weighted), number
+ * of contact elements with a nonzero force -- the quantities mel_monitor_compute reports.
+ * Its block partials live in a file-scope device array of 1024 records reused by every call (and
+ * held by every GPU that loads the library until the process exits), so it accepts at most
+ * 2,097,152 nodes and as many contact elements per call and rejects larger sizes with
+ * MEL_ERR_INVALID.  The array keeps the last call's contents; each call writes every record it reads,
+ * and calls that overlap on the GPU (on different streams) race on it.  The first call on a device
+ * looks up the array's device address with that device current; make that first call before any
+ * stream capture.  `stream` is a cudaStream_t (NULL: the legacy default stream); the call returns
+ * once the work is queued. */
+mel_status mel_monitor_reduce_static(const double* d_velocity, const double* d_mass, const double* d_displacement,
+                                     int n_nodes, const mel_contact* d_contacts, int n_contacts, double* d_out,
+                                     void* stream);
+
 /* ---- introspection ---------------------------------------------------------------- */
 const char* mel_last_error_string(void);
 int         mel_abi_version(void);

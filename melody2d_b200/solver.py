@@ -51,6 +51,7 @@ SIGNATURES = {
     "mel_get_kernel_times": [_vp, _dp, _dp, _dp, _dp, _ip],
     "mel_get_sizes": [_vp, _ip, _ip, _ip, _ip, _ip, _ip],
     "mel_get_step_stats": [_vp, _dp, _dp, _dp, _ip, _ip],
+    "mel_monitor_reduce_static": [_vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp],
 }
 
 
