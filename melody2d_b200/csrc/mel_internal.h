@@ -1,33 +1,62 @@
 // Internal definitions of the B200 solver: device-resident model and kernel entry points.
 // Layout (HBM): body-sorted structure-of-arrays; node pairs (x,y) as double2 for 16-byte
-// accesses; Gauss-point supports stored per chunk (<= MEL_CHUNK_GP points, <= MEL_CHUNK_E
-// entries, start padded to 8 entries so every chunk begins on a 16-byte boundary) with
-// 16-bit body-local indices; contact elements in the reference's mel_contact record.
+// accesses; the Gauss points of a deformable body cut into chunks, each chunk one contiguous
+// 16-byte-aligned image (header, dN/dx-dN/dy pairs, 16-bit body-local support indices, pull
+// positions, per-point weights and offsets, touched-node records) that a single bulk copy
+// moves into shared memory; contact elements in the reference's mel_contact record.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "melgpu.h"
 
-#define MEL_CHUNK_GP 128          // Gauss points per chunk (one thread each in the forward pass)
-#define MEL_CHUNK_E 2048          // support entries per chunk (shared-memory staging capacity)
 #define MEL_BODY_THREADS 256      // threads per body CTA
+#define MEL_BODY_CTHREADS 224     // of which run the Gauss-point pipeline (warps 0-6); warp 7 scatters contacts
+#define MEL_CHUNK_GP MEL_BODY_CTHREADS   // Gauss points per chunk (one compute thread each)
+#define MEL_CHUNK_E_MAX 2048      // support entries per chunk, upper bound (the host may choose less)
+#define MEL_WAIT_NS 1000000000ull // bound of every device-side wait (1 s)
 #define MEL_NBR_CAP_DEFAULT 64    // neighbour slots per body (grown on overflow)
 #define MEL_MAX_BODY_NODES 4096   // nodes per deformable body held in shared memory
+#define MEL_SEGB 16               // segments per segment-block box (proximity pruning)
+#define MEL_SEGB2 16              // blocks per superblock box (second pruning level)
+#define MEL_MAX_SHIFT_SPAN 64     // periods one border box may span at a proximity update
 
 // device error words (mel_dev::err)
 enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3, MEL_E_CAPACITY = 4,
-       MEL_E_NBR_NEED = 5, MEL_E_NWORDS = 8 };
+       MEL_E_NBR_NEED = 5, MEL_E_WAIT = 6, MEL_E_NWORDS = 8 };
 
+// Chunk image (all offsets in bytes from the image start, every section 16-byte aligned):
+//   header   int4 {ngp, ne, ntn, bytes}
+//   dN       ne x double2          (ne padded to a multiple of 8 with zero entries)
+//   idx      ne x uint16           body-local support node of each entry
+//   tpos     ne x uint16           entry positions sorted by (node, position): the pull order
+//   c0       ngp2 x double         weight x jacobian (ngp2 = ngp rounded up to 2)
+//   gpm      ngp4 x uint32         first entry of the point | support count << 16
+//   tn       tn4 x uint32          touched node | first tpos << 16, ntn + 1 records (the last
+//                                  one closes the final range)
 struct mel_chunk {        // one chunk of a body's Gauss points
+    long long img;        // byte offset of the image in mel_dev::img
+    int bytes;            // image size (multiple of 16)
+    int ngp, ne, ntn;
     int gp0;              // first Gauss point (global index)
-    int ngp;              // Gauss points in the chunk
-    int e0;               // first entry (padded global entry index, multiple of 8)
-    int ne;               // entries (padded to a multiple of 8)
-    int tn0;              // first touched-node record
-    int ntn;              // touched nodes
-    int pad0, pad1;
+    int pad;
 };
+
+struct mel_chunk_layout {  // section offsets of an image
+    int dN, idx, tpos, c0, gpm, tn, bytes;
+};
+__host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, int ntn)
+{
+    mel_chunk_layout L;
+    L.dN = 16;
+    L.idx = L.dN + 16 * ne;
+    L.tpos = L.idx + 2 * ne;
+    L.c0 = L.tpos + 2 * ne;
+    L.gpm = L.c0 + 8 * ((ngp + 1) & ~1);
+    L.tn = L.gpm + 4 * ((ngp + 3) & ~3);
+    L.bytes = L.tn + 4 * ((ntn + 1 + 3) & ~3);
+    return L;
+}
 
 struct mel_dev {
     // sizes
@@ -56,15 +85,24 @@ struct mel_dev {
     const int *e_node, *e_sn, *e_ss;         // e_sn/e_ss: 4 per entry (node0..3, shift0..3)
     const double* e_len0;
     double* e_len;                            // lengths of the last Update_borders
-    // Gauss points
-    const double* gp_c0; const int* gp_e0; const uint8_t* gp_ns;
-    const uint16_t *ge_idx, *ge_tpos; const double2* ge_dN;
-    const float2* ge_dNf;                     // FP32 copy for the mixed-precision pass
+    int nblk;                                 // segment blocks (MEL_SEGB segments of one border)
+    const int* bd_blk0;                       // [nbd+1] first block of each border
+    const int* blk_border;                    // border of each block
+    double4* seg_blk;                         // block boxes of the current proximity update
+    int nsblk;                                // superblocks (MEL_SEGB2 consecutive blocks of one border)
+    const int* bd_sblk0;                      // [nbd+1] first superblock of each border
+    const int* sblk_border;                   // border of each superblock
+    double4* seg_sblk;                        // superblock boxes (unions of their block boxes)
+    // Gauss points: chunk table and chunk images
     const mel_chunk* chunk;
-    const uint16_t *tn_node, *tn_start, *tn_cnt;
+    const char* img;
+    int img_cap;                              // bytes of one shared-memory staging buffer
     // contacts
     mel_contact* cont;
     double* cont_w;                           // per-contact work increment of the last law evaluation
+    double* cont_rt;                          // 6 per contact: rigid slave and rigid master force and
+                                              // moment terms of the last contact pass (arms from the
+                                              // positions before the body kernel moves any node)
     int any_damped;                           // a law with work terms is in use
     const int* b_cont0;                       // [nb+1] slave contact ranges (list is body-major)
     const int* b_inc0;                        // [nb+1] into inc_rng
@@ -76,7 +114,7 @@ struct mel_dev {
 // kernel launch wrappers (mel_kernels.cu)
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s);
-size_t mel_body_smem_bytes(int max_nodes, int max_border_nodes);
+size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes);
 void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);
 

@@ -61,6 +61,33 @@ __device__ __forceinline__ void seg_points(const mel_dev& d, int bodyM, int e, i
     }
 }
 
+// Moment-arm terms of one contact for rigid bodies (Body::Update_contact_forces, rigid branches,
+// Code/Body.h:1866-1877 and the master side read by Sum_up_forces): the slave side adds
+// (fx, fy, -fx*dy + fy*dx) to a rigid slave, the master side (-fx, -fy, fx*dy - fy*dx) to a rigid
+// master, with arms from the body centre to the slave node.  Contacts whose material pair has no
+// law contribute +0, which leaves the body's running sums unchanged.  Written here, where every
+// contact is one thread, so the rigid body only adds them up in the reference's order.
+__device__ __forceinline__ void rigid_terms(const mel_dev& d, int tid, const mel_contact& c, double2 xs)
+{
+    double* t = d.cont_rt + 6 * (size_t)tid;
+    const bool law = d.table[d.b_mat[c.bodyS] * d.nmat + d.b_mat[c.bodyM]] > -1;
+    if (d.b_type[c.bodyS] == MEL_BODY_RIGID) {
+        const double* rg = d.rg + MEL_RIGID_NF * c.bodyS;
+        double dx = xs.x - rg[MEL_RG_XC], dy = xs.y - rg[MEL_RG_YC];
+        t[0] = law ? c.fx : 0.;
+        t[1] = law ? c.fy : 0.;
+        t[2] = law ? -c.fx * dy + c.fy * dx : 0.;
+    }
+    if (d.b_type[c.bodyM] == MEL_BODY_RIGID) {
+        const double* rg = d.rg + MEL_RIGID_NF * c.bodyM;
+        double dx = xs.x - rg[MEL_RG_XC] - c.shiftM * d.period;
+        double dy = xs.y - rg[MEL_RG_YC];
+        t[3] = law ? -c.fx : 0.;
+        t[4] = law ? -c.fy : 0.;
+        t[5] = law ? c.fx * dy - c.fy * dx : 0.;
+    }
+}
+
 __global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale)
 {
     int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -79,7 +106,7 @@ __global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_s
     mel_contact c = d.cont[tid];
     int b = c.bodyS;
     if (b < 0 || b >= d.nb || c.bodyM < 0 || c.bodyM >= d.nb) { set_err(d, MEL_E_BOUNDS); return; }
-    if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
+    if (d.b_status[b] == MEL_STATUS_INACTIVE) { rigid_terms(d, tid, c, d.x[d.b_node0[b] + c.nodeS]); return; }
     // ---- Update_contacts (Code/Body.h:1352-1632) -----------------------------------------
     int bodyM = c.bodyM, borderM = c.borderM, shiftM = c.shiftM, segmentM = c.segmentM;
     int gM = d.b_bd0[bodyM] + borderM;
@@ -177,12 +204,14 @@ __global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_s
         c.gapn = gapn; c.gapt = gapt;
         d.cont[tid] = c;
         d.cont_w[tid] = W;     // work increment, summed per body in the reference's order by body_kernel
+        rigid_terms(d, tid, c, xs);
         return;
     }
     // no law for this material pair: Update_contacts ran, forces untouched (Code/Body.h:1700-1701)
     c.gapn = gapn; c.gapt = gapt;
     d.cont[tid] = c;
     d.cont_w[tid] = 0.;
+    rigid_terms(d, tid, c, xs);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -260,6 +289,148 @@ __device__ __forceinline__ void warp_scatter(const mel_dev& d, int n0, int node,
     }
 }
 
+// ---- bulk copies into shared memory and their mbarriers (PTX: mbarrier.*, cp.async.bulk) --
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// generic-proxy accesses to a buffer are ordered before the bulk copy that refills it
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// barrier of the Gauss-point warps only (warp 7 runs the contact scatter meanwhile)
+__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, %0;" :: "n"(MEL_BODY_CTHREADS) : "memory"); }
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// wait for phase `parity` of `bar` to complete; gives up after MEL_WAIT_NS
+__device__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        for (int i = 0; i < 64; i++)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > MEL_WAIT_NS) return false;
+    }
+}
+
+// running sums of `n` terms t[k*stride] (k = 0..n-1) added in order to acc; loads batched so
+// that eight are in flight per round trip
+__device__ __forceinline__ double ordered_sum(double acc, const double* t, int n, int stride)
+{
+    int k = 0;
+    for (; k + 8 <= n; k += 8) {
+        double v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = t[(size_t)(k + j) * stride];
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc += v[j];
+    }
+    for (; k < n; k++) acc += t[(size_t)k * stride];
+    return acc;
+}
+
+// Gauss-point pass of one chunk held in shared memory (Body::Update_internal_forces,
+// Code/Body.h:960-1050): thread `t` < ngp forms the strain of its point from the staged dN and
+// the body's displacements, applies the material and overwrites its dN pairs with the
+// contributions c0 * B^T.sigma.
+__device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double Lam, const double2* s_up,
+                                             double2* s_p, const uint16_t* s_idx, const double* s_c0,
+                                             const unsigned* s_gpm)
+{
+    const unsigned m = s_gpm[t];
+    const int e = (int)(m & 0xffffu), ns = (int)(m >> 16);
+    const double c0 = s_c0[t];
+    if (mtype == MEL_MAT_ELASTIC_LINEAR) {
+        // strain sums in support order; loads issued four supports ahead of the adds
+        double E11 = 0., E12 = 0., E22 = 0.;
+        int k = 0;
+        for (; k + 4 <= ns; k += 4) {
+            double2 dN[4], u[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) { dN[j] = s_p[e + k + j]; u[j] = s_up[s_idx[e + k + j]]; }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                E11 = E11 + dN[j].x * u[j].x;
+                E12 = E12 + (dN[j].x * u[j].y + dN[j].y * u[j].x);
+                E22 = E22 + dN[j].y * u[j].y;
+            }
+        }
+        for (; k < ns; k++) {
+            double2 dN = s_p[e + k];
+            double2 u = s_up[s_idx[e + k]];
+            E11 = E11 + dN.x * u.x;
+            E12 = E12 + (dN.x * u.y + dN.y * u.x);
+            E22 = E22 + dN.y * u.y;
+        }
+        E12 = 0.5 * E12;
+        double J = 1. + E11 + E22;               // Apply_Elastic_Linear (Code/Model.h:19-29)
+        double S33 = Lam * (J - 1.);
+        double Mu2 = 2 * Mu;
+        double S11 = S33 + Mu2 * E11, S22 = S33 + Mu2 * E22, S12 = Mu2 * E12;
+#pragma unroll 4
+        for (int k2 = 0; k2 < ns; k2++) {
+            double2 dN = s_p[e + k2];
+            double2 q;
+            q.x = c0 * (dN.x * S11 + dN.y * S12);
+            q.y = c0 * (dN.y * S22 + dN.x * S12);
+            s_p[e + k2] = q;
+        }
+    } else {
+        double F11 = 1., F12 = 0., F21 = 0., F22 = 1.;
+        for (int k = 0; k < ns; k++) {
+            double2 dN = s_p[e + k];
+            double2 u = s_up[s_idx[e + k]];
+            F11 += dN.x * u.x; F12 += dN.y * u.x; F21 += dN.x * u.y; F22 += dN.y * u.y;
+        }
+        double Kappa = Lam;                       // Apply_NeoHookean (Code/Model.h:52-73)
+        double F11F12 = F11 * F11 + F12 * F12, F21F22 = F21 * F21 + F22 * F22;
+        double J = F11 * F22 - F12 * F21;
+        double invJ = 1. / J;
+        double K = Kappa * (J - 1.);
+        double MuJ53 = Mu * pow(J, -1.666666666667);
+        double trB = 0.333333333333 * (F11F12 + F21F22 + 1.);
+        double s11 = K + MuJ53 * (F11F12 - trB), s22 = K + MuJ53 * (F21F22 - trB);
+        double s12 = MuJ53 * (F11 * F21 + F12 * F22);
+        double S11 = (F12 * (F12 * s22 - F22 * s12) - F22 * (F12 * s12 - F22 * s11)) * invJ;
+        double S22 = (F11 * (F11 * s22 - F21 * s12) - F21 * (F11 * s12 - F21 * s11)) * invJ;
+        double S12 = (F21 * (F12 * s12 - F22 * s11) - F11 * (F12 * s22 - F22 * s12)) * invJ;
+        for (int k = 0; k < ns; k++) {
+            double2 dN = s_p[e + k];
+            double2 q;
+            q.x = c0 * (dN.x * (F11 * S11 + F12 * S12) + dN.y * (F12 * S22 + F11 * S12));
+            q.y = c0 * (dN.x * (F21 * S11 + F22 * S12) + dN.y * (F22 * S22 + F21 * S12));
+            s_p[e + k] = q;
+        }
+    }
+}
+
+// Shared memory of a deformable body (n nodes, staging buffers of img_cap bytes each):
+//   s_up, s_f, s_fc        3 x n double2       displacements, internal forces, contact forces
+//   2 mbarriers + abort flag                   32 bytes
+//   region                 max(2 img_cap, 112 n) bytes: two chunk images during the Gauss-point
+//                          pass, then s_fn, s_fd, s_vp, s_ap (n double2 each) and the six work
+//                          terms per node (6 x n double)
 __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
 {
     const int tid = threadIdx.x;
@@ -270,115 +441,93 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
     const double dt = d.dt[0];
     double2* s_up = reinterpret_cast<double2*>(smem);
     double2* s_f = s_up + n;
-    char* region = reinterpret_cast<char*>(s_f + n);
-    for (int i = tid; i < n; i += blockDim.x) { s_up[i] = d.up[n0 + i]; s_f[i] = make_double2(0., 0.); }
-    __syncthreads();
-    // ---- Update_internal_forces: chunked Gauss-point pass (one region per body) -----------
-    const int mat = d.b_mat[b];
-    const int mtype = d.mat_type[mat];
-    const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
-    const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
-    uint16_t* s_idx = reinterpret_cast<uint16_t*>(region);
-    uint16_t* s_tpos = s_idx + MEL_CHUNK_E;
-    double2* s_p = reinterpret_cast<double2*>(s_tpos + MEL_CHUNK_E);
-    for (int ci = d.b_chunk0[b]; ci < d.b_chunk0[b + 1]; ci++) {
-        const mel_chunk ch = d.chunk[ci];
-        // stage the chunk's entries (16-byte vector loads; chunk starts are 8-entry aligned)
-        {
-            const int4* gi = reinterpret_cast<const int4*>(d.ge_idx + ch.e0);
-            const int4* gt = reinterpret_cast<const int4*>(d.ge_tpos + ch.e0);
-            int4* si = reinterpret_cast<int4*>(s_idx);
-            int4* st = reinterpret_cast<int4*>(s_tpos);
-            int nv = ch.ne >> 3;
-            for (int k = tid; k < nv; k += blockDim.x) { si[k] = gi[k]; st[k] = gt[k]; }
-            const double2* gd = d.ge_dN + ch.e0;
-            for (int k = tid; k < ch.ne; k += blockDim.x) s_p[k] = gd[k];
-        }
-        __syncthreads();
-        if (tid < ch.ngp) {
-            int g = ch.gp0 + tid;
-            int e = d.gp_e0[g] - ch.e0;
-            int ns = d.gp_ns[g];
-            double c0 = d.gp_c0[g];
-            if (mtype == MEL_MAT_ELASTIC_LINEAR) {
-                double E11 = 0., E12 = 0., E22 = 0.;
-                for (int k = 0; k < ns; k++) {
-                    double2 dN = s_p[e + k];
-                    double2 u = s_up[s_idx[e + k]];
-                    E11 = E11 + dN.x * u.x;
-                    E12 = E12 + (dN.x * u.y + dN.y * u.x);
-                    E22 = E22 + dN.y * u.y;
-                }
-                E12 = 0.5 * E12;
-                double J = 1. + E11 + E22;               // Apply_Elastic_Linear (Code/Model.h:19-29)
-                double S33 = Lam * (J - 1.);
-                double Mu2 = 2 * Mu;
-                double S11 = S33 + Mu2 * E11, S22 = S33 + Mu2 * E22, S12 = Mu2 * E12;
-                for (int k = 0; k < ns; k++) {
-                    double2 dN = s_p[e + k];
-                    double2 q;
-                    q.x = c0 * (dN.x * S11 + dN.y * S12);
-                    q.y = c0 * (dN.y * S22 + dN.x * S12);
-                    s_p[e + k] = q;
-                }
-            } else {
-                double F11 = 1., F12 = 0., F21 = 0., F22 = 1.;
-                for (int k = 0; k < ns; k++) {
-                    double2 dN = s_p[e + k];
-                    double2 u = s_up[s_idx[e + k]];
-                    F11 += dN.x * u.x; F12 += dN.y * u.x; F21 += dN.x * u.y; F22 += dN.y * u.y;
-                }
-                double Kappa = Lam;                       // Apply_NeoHookean (Code/Model.h:52-73)
-                double F11F12 = F11 * F11 + F12 * F12, F21F22 = F21 * F21 + F22 * F22;
-                double J = F11 * F22 - F12 * F21;
-                double invJ = 1. / J;
-                double K = Kappa * (J - 1.);
-                double MuJ53 = Mu * pow(J, -1.666666666667);
-                double trB = 0.333333333333 * (F11F12 + F21F22 + 1.);
-                double s11 = K + MuJ53 * (F11F12 - trB), s22 = K + MuJ53 * (F21F22 - trB);
-                double s12 = MuJ53 * (F11 * F21 + F12 * F22);
-                double S11 = (F12 * (F12 * s22 - F22 * s12) - F22 * (F12 * s12 - F22 * s11)) * invJ;
-                double S22 = (F11 * (F11 * s22 - F21 * s12) - F21 * (F11 * s12 - F21 * s11)) * invJ;
-                double S12 = (F21 * (F12 * s12 - F22 * s11) - F11 * (F12 * s22 - F22 * s12)) * invJ;
-                for (int k = 0; k < ns; k++) {
-                    double2 dN = s_p[e + k];
-                    double2 q;
-                    q.x = c0 * (dN.x * (F11 * S11 + F12 * S12) + dN.y * (F12 * S22 + F11 * S12));
-                    q.y = c0 * (dN.x * (F21 * S11 + F22 * S12) + dN.y * (F22 * S22 + F21 * S12));
-                    s_p[e + k] = q;
-                }
-            }
-        }
-        __syncthreads();
-        // pull: each touched node subtracts its contributions in ascending Gauss-point order
-        for (int t = tid; t < ch.ntn; t += blockDim.x) {
-            int node = d.tn_node[ch.tn0 + t];
-            int q0 = d.tn_start[ch.tn0 + t];
-            int cnt = d.tn_cnt[ch.tn0 + t];
-            double2 f = s_f[node];
-            for (int q = q0; q < q0 + cnt; q++) {
-                double2 c = s_p[s_tpos[q]];
-                f.x = f.x - c.x;
-                f.y = f.y - c.y;
-            }
-            s_f[node] = f;
-        }
-        __syncthreads();
-    }
-    // ---- contact forces: slave scatter in list order, then master scatter in send order ---
-    double2* s_fc = reinterpret_cast<double2*>(region);
-    double2* s_fn = s_fc + n;
-    double2* s_fd = s_fn + n;
-    double2* s_vp = s_fd + n;
-    double2* s_ap = s_vp + n;
-    const int has_bc = d.b_has_bc[b];
+    double2* s_fc = s_f + n;
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_fc + n);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(s_bar + 2);
+    char* region = reinterpret_cast<char*>(s_bar + 4);
+    char* const buf0 = region;
+    char* const buf1 = region + d.img_cap;
+    const int ch0 = d.b_chunk0[b];
+    const int nch = d.b_chunk0[b + 1] - ch0;
     for (int i = tid; i < n; i += blockDim.x) {
+        s_up[i] = d.up[n0 + i];
+        s_f[i] = make_double2(0., 0.);
         s_fc[i] = make_double2(0., 0.);
-        s_fn[i] = make_double2(0., 0.);
-        s_fd[i] = make_double2(0., 0.);
+    }
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_init_fence();
+        *s_abort = 0;
     }
     __syncthreads();
-    if (warp == 0) {
+    if (warp < MEL_BODY_CTHREADS / 32) {
+        // ---- Update_internal_forces: chunk k is computed while chunk k+1 is in flight ----------
+        const int mat = d.b_mat[b];
+        const int mtype = d.mat_type[mat];
+        const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
+        const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
+        int issued = 0;
+        if (tid == 0)
+            for (; issued < 2 && issued < nch; issued++) {
+                const mel_chunk c = d.chunk[ch0 + issued];
+                mbar_arrive_expect_tx(&s_bar[issued], (unsigned)c.bytes);
+                bulk_load(issued ? buf1 : buf0, d.img + c.img, (unsigned)c.bytes, &s_bar[issued]);
+            }
+        int k = 0;
+        for (; k < nch; k++) {
+            const int sel = k & 1;
+            char* bk = sel ? buf1 : buf0;
+            long long nxt_img = 0;
+            int nxt_bytes = 0;
+            if (tid == 0 && k + 2 < nch) { const mel_chunk c = d.chunk[ch0 + k + 2]; nxt_img = c.img; nxt_bytes = c.bytes; }
+            const bool ok = mbar_wait_bounded(&s_bar[sel], (unsigned)((k >> 1) & 1));
+            if (!ok) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
+            const int4 hdr = ok ? *reinterpret_cast<const int4*>(bk) : make_int4(0, 0, 0, 0);
+            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z);
+            double2* s_p = reinterpret_cast<double2*>(bk + L.dN);
+            const uint16_t* s_idx = reinterpret_cast<const uint16_t*>(bk + L.idx);
+            const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
+            const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
+            if (tid < hdr.x)
+                chunk_points(tid, mtype, Mu, Lam, s_up, s_p, s_idx, reinterpret_cast<const double*>(bk + L.c0),
+                             reinterpret_cast<const unsigned*>(bk + L.gpm));
+            compute_sync();
+            if (*s_abort) break;
+            // pull: each touched node subtracts its contributions in ascending Gauss-point order
+            for (int t = tid; t < hdr.z; t += MEL_BODY_CTHREADS) {
+                const unsigned r0 = s_tn[t], r1 = s_tn[t + 1];
+                const int node = (int)(r0 & 0xffffu);
+                const int q1 = (int)(r1 >> 16);
+                double2 f = s_f[node];
+                int q = (int)(r0 >> 16);
+                for (; q + 4 <= q1; q += 4) {
+                    double2 c[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) c[j] = s_p[s_tpos[q + j]];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) { f.x = f.x - c[j].x; f.y = f.y - c[j].y; }
+                }
+                for (; q < q1; q++) {
+                    double2 c = s_p[s_tpos[q]];
+                    f.x = f.x - c.x;
+                    f.y = f.y - c.y;
+                }
+                s_f[node] = f;
+            }
+            fence_proxy_async();
+            compute_sync();
+            if (tid == 0 && k + 2 < nch) {
+                mbar_arrive_expect_tx(&s_bar[sel], (unsigned)nxt_bytes);
+                bulk_load(bk, d.img + nxt_img, (unsigned)nxt_bytes, &s_bar[sel]);
+                issued++;
+            }
+        }
+        if (tid == 0 && *s_abort)   // give the copies still in flight a bounded time to land
+            for (int c = k; c < issued; c++) mbar_wait_bounded(&s_bar[c & 1], (unsigned)((c >> 1) & 1));
+    } else {
+        // ---- contact forces (warp 7): slave scatter in list order, then master scatter in send
+        // order (Body::Update_contact_forces, Code/Body.h:1642-1900) ---------------------------
         for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
             const mel_contact* ct = d.cont + c;
             if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
@@ -399,108 +548,139 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
                 }
             }
         }
-    } else if (warp == 1 && has_bc) {
-        // ---- Update_bc_forces, deformable (Code/Body.h:669-799) --------------------------
-        for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
-            int tx = d.bd_bc[2 * g], ty = d.bd_bc[2 * g + 1];
-            if (tx == MEL_BC_NONE && ty == MEL_BC_NONE) continue;
-            double xv, xvel, yv, yvel;
-            border_bc_value(d, g, 0, T, xv, xvel);
-            border_bc_value(d, g, 1, T, yv, yvel);
-            int e0 = d.bd_e0[g], nbn = d.bd_e0[g + 1] - e0;
-            for (int k = 0; k < nbn - 1; k++) {
-                int e = e0 + k;
-                int bn = d.e_node[e];
-                double length = border_length(d, b, g, k);
-                double px = 0., py = 0.;
-                double ftx = 0., fty = 0., ftpx = 0., ftpy = 0.;
-                if (tx == MEL_BC_FOLLOWING || ty == MEL_BC_FOLLOWING) {
-                    int a0 = n0 + d.e_sn[4 * e], a2 = n0 + d.e_sn[4 * e + 2];
-                    double2 X0 = d.X0[a0], X2 = d.X0[a2], x0 = d.x[a0], x2 = d.x[a2];
-                    double invl = mel_rsqrt((X2.x - X0.x) * (X2.x - X0.x) + (X2.y - X0.y) * (X2.y - X0.y));
-                    double invlp = mel_rsqrt((x2.x - x0.x) * (x2.x - x0.x) + (x2.y - x0.y) * (x2.y - x0.y));
-                    ftx = (X2.x - X0.x) * invl; fty = (X2.y - X0.y) * invl;
-                    ftpx = (x2.x - x0.x) * invlp; ftpy = (x2.y - x0.y) * invlp;
-                }
-                double2 ub = d.u[n0 + bn], vb = d.v[n0 + bn];
-                if (tx == MEL_BC_ORIENTED) px = xv;
-                else if (tx == MEL_BC_FOLLOWING) { px += xv * (ftx * ftpx + fty * ftpy); py += xv * (ftx * ftpy - fty * ftpx); }
-                else if (tx == MEL_BC_SOFT) px = d.bd_bcp[4 * g] * (xv - ub.x) - d.bd_bcp[4 * g + 1] * (xvel - vb.x);
-                if (ty == MEL_BC_ORIENTED) py = yv;
-                else if (ty == MEL_BC_FOLLOWING) { px += yv * (fty * ftpx - ftx * ftpy); py += yv * (fty * ftpy + ftx * ftpx); }
-                else if (ty == MEL_BC_SOFT) py = d.bd_bcp[4 * g + 2] * (yv - ub.y) - d.bd_bcp[4 * g + 3] * (yvel - vb.y);
-                int gn = n0 + bn;
-                for (int j = d.sup_ptr[gn] + lane; j < d.sup_ptr[gn + 1]; j += 32) {
-                    double sf = d.sup_N[j];
-                    double fxn = 0., fyn = 0., fxd = 0., fyd = 0.;
-                    if (tx == MEL_BC_ORIENTED) fxn = px * length * sf;
-                    else if (tx == MEL_BC_FOLLOWING) { fxn = px * length * sf; fyn = py * length * sf; }
-                    else if (tx == MEL_BC_SOFT) fxd = px * length * sf;
-                    if (ty == MEL_BC_ORIENTED) fyn = py * length * sf;
-                    else if (ty == MEL_BC_FOLLOWING) { fxn = px * length * sf; fyn = py * length * sf; }
-                    else if (ty == MEL_BC_SOFT) fyd = py * length * sf;
-                    int t = d.sup_idx[j];
-                    double2 a = s_fn[t]; a.x = a.x + fxn; a.y = a.y + fyn; s_fn[t] = a;
-                    double2 c = s_fd[t]; c.x = c.x + fxd; c.y = c.y + fyd; s_fd[t] = c;
-                }
-                __syncwarp();
-            }
-        }
     }
     __syncthreads();
-    // ---- Sum_up_forces, Apply_Newton (Code/Node.h:212-231) --------------------------------
+    if (*s_abort) return;
+    double2* s_fn = reinterpret_cast<double2*>(region);
+    double2* s_fd = s_fn + n;
+    double2* s_vp = s_fd + n;
+    double2* s_ap = s_vp + n;
+    double* s_T = reinterpret_cast<double*>(s_ap + n);
+    const int has_bc = d.b_has_bc[b];
+    if (has_bc) {
+        for (int i = tid; i < n; i += blockDim.x) { s_fn[i] = make_double2(0., 0.); s_fd[i] = make_double2(0., 0.); }
+        __syncthreads();
+        if (warp == 1) {
+            // ---- Update_bc_forces, deformable (Code/Body.h:669-799) ----------------------
+            for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
+                int tx = d.bd_bc[2 * g], ty = d.bd_bc[2 * g + 1];
+                if (tx == MEL_BC_NONE && ty == MEL_BC_NONE) continue;
+                double xv, xvel, yv, yvel;
+                border_bc_value(d, g, 0, T, xv, xvel);
+                border_bc_value(d, g, 1, T, yv, yvel);
+                int e0 = d.bd_e0[g], nbn = d.bd_e0[g + 1] - e0;
+                for (int k = 0; k < nbn - 1; k++) {
+                    int e = e0 + k;
+                    int bn = d.e_node[e];
+                    double length = border_length(d, b, g, k);
+                    double px = 0., py = 0.;
+                    double ftx = 0., fty = 0., ftpx = 0., ftpy = 0.;
+                    if (tx == MEL_BC_FOLLOWING || ty == MEL_BC_FOLLOWING) {
+                        int a0 = n0 + d.e_sn[4 * e], a2 = n0 + d.e_sn[4 * e + 2];
+                        double2 X0 = d.X0[a0], X2 = d.X0[a2], x0 = d.x[a0], x2 = d.x[a2];
+                        double invl = mel_rsqrt((X2.x - X0.x) * (X2.x - X0.x) + (X2.y - X0.y) * (X2.y - X0.y));
+                        double invlp = mel_rsqrt((x2.x - x0.x) * (x2.x - x0.x) + (x2.y - x0.y) * (x2.y - x0.y));
+                        ftx = (X2.x - X0.x) * invl; fty = (X2.y - X0.y) * invl;
+                        ftpx = (x2.x - x0.x) * invlp; ftpy = (x2.y - x0.y) * invlp;
+                    }
+                    double2 ub = d.u[n0 + bn], vb = d.v[n0 + bn];
+                    if (tx == MEL_BC_ORIENTED) px = xv;
+                    else if (tx == MEL_BC_FOLLOWING) { px += xv * (ftx * ftpx + fty * ftpy); py += xv * (ftx * ftpy - fty * ftpx); }
+                    else if (tx == MEL_BC_SOFT) px = d.bd_bcp[4 * g] * (xv - ub.x) - d.bd_bcp[4 * g + 1] * (xvel - vb.x);
+                    if (ty == MEL_BC_ORIENTED) py = yv;
+                    else if (ty == MEL_BC_FOLLOWING) { px += yv * (fty * ftpx - ftx * ftpy); py += yv * (fty * ftpy + ftx * ftpx); }
+                    else if (ty == MEL_BC_SOFT) py = d.bd_bcp[4 * g + 2] * (yv - ub.y) - d.bd_bcp[4 * g + 3] * (yvel - vb.y);
+                    int gn = n0 + bn;
+                    for (int j = d.sup_ptr[gn] + lane; j < d.sup_ptr[gn + 1]; j += 32) {
+                        double sf = d.sup_N[j];
+                        double fxn = 0., fyn = 0., fxd = 0., fyd = 0.;
+                        if (tx == MEL_BC_ORIENTED) fxn = px * length * sf;
+                        else if (tx == MEL_BC_FOLLOWING) { fxn = px * length * sf; fyn = py * length * sf; }
+                        else if (tx == MEL_BC_SOFT) fxd = px * length * sf;
+                        if (ty == MEL_BC_ORIENTED) fyn = py * length * sf;
+                        else if (ty == MEL_BC_FOLLOWING) { fxn = px * length * sf; fyn = py * length * sf; }
+                        else if (ty == MEL_BC_SOFT) fyd = py * length * sf;
+                        int t = d.sup_idx[j];
+                        double2 a = s_fn[t]; a.x = a.x + fxn; a.y = a.y + fyn; s_fn[t] = a;
+                        double2 c = s_fd[t]; c.x = c.x + fxd; c.y = c.y + fyd; s_fd[t] = c;
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // ---- Sum_up_forces, Apply_Newton (Code/Node.h:212-231); work terms of Body::Apply_Euler
+    // (Code/Body.h:2058-2066) per node, summed in node order below ---------------------------
     const double gx = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gx;
     const double gy = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gy;
+    const double hdt = 0.5 * dt;
     for (int i = tid; i < n; i += blockDim.x) {
         int gi = n0 + i;
         double2 m = d.mass[gi], im = d.minv[gi];
         double2 fb = make_double2(m.x * gx, m.y * gy);
-        double2 fi = s_f[i], fc = s_fc[i], fn = s_fn[i], fd = s_fd[i];
+        double2 fi = s_f[i], fc = s_fc[i];
+        double2 fn = has_bc ? s_fn[i] : make_double2(0., 0.);
+        double2 fd = has_bc ? s_fd[i] : make_double2(0., 0.);
         double2 ft;
         ft.x = fi.x + fc.x + 0. + fb.x + fd.x + fn.x + 0. + 0.;
         ft.y = fi.y + fc.y + 0. + fb.y + fd.y + fn.y + 0. + 0.;
         double2 ap = make_double2(ft.x * im.x / 1., ft.y * im.y / 1.);
+        double2 vp = d.vp[gi];
         s_ap[i] = ap;
-        s_vp[i] = d.vp[gi];
+        s_vp[i] = vp;
         if (d.record_forces) {
             d.o_fint[gi] = fi; d.o_fcon[gi] = fc; d.o_fneu[gi] = fn; d.o_fdir[gi] = fd; d.o_ftot[gi] = ft;
         }
+        double vx = vp.x + hdt * ap.x, vy = vp.y + hdt * ap.y;
+        s_T[i] = dt * (vx * fi.x + vy * fi.y);
+        s_T[n + i] = dt * (vx * fb.x + vy * fb.y);
+        s_T[2 * n + i] = dt * (vx * fd.x + vy * fd.y);
+        s_T[3 * n + i] = dt * (vx * fn.x + vy * fn.y);
+        double z = dt * (vx * 0. + vy * 0.);
+        s_T[4 * n + i] = z;
+        s_T[5 * n + i] = z;
     }
     __syncthreads();
-    // ---- works of Body::Apply_Euler (Code/Body.h:2058-2066), summed in node order -----------
-    if (warp == 0 && lane < 6) {
-        const int widx[6] = { 0, 2, 3, 4, 5, 6 };
-        double W = d.works[7 * b + widx[lane]];
-        const double hdt = 0.5 * dt;
-        for (int i = 0; i < n; i++) {
-            double2 vp = s_vp[i], ap = s_ap[i];
-            double vx = vp.x + hdt * ap.x, vy = vp.y + hdt * ap.y;
-            double2 f;
-            if (lane == 0) f = s_f[i];
-            else if (lane == 1) { double2 m = d.mass[n0 + i]; f = make_double2(m.x * gx, m.y * gy); }
-            else if (lane == 2) f = s_fd[i];
-            else if (lane == 3) f = s_fn[i];
-            else f = make_double2(0., 0.);
-            W += dt * (vx * f.x + vy * f.y);
+    if (warp == 0) {
+        // works (internal, body, dirichlet, neumann, damping, alid), summed in node order
+        if (lane < 6) {
+            const int w = lane == 0 ? 0 : lane + 1;       // works slots 0, 2, 3, 4, 5, 6
+            d.works[7 * b + w] = ordered_sum(d.works[7 * b + w], s_T + (size_t)lane * n, n, 1);
         }
-        d.works[7 * b + widx[lane]] = W;
-    }
-    __syncthreads();
-    // ---- Apply_Euler (Code/Node.h:239-245) -------------------------------------------------
-    for (int i = tid; i < n; i += blockDim.x) {
-        int gi = n0 + i;
-        double2 ap = s_ap[i], vp = s_vp[i], up = s_up[i];
-        vp.x = vp.x + dt * ap.x; vp.y = vp.y + dt * ap.y;
-        up.x = up.x + dt * vp.x; up.y = up.y + dt * vp.y;
-        s_vp[i] = vp; s_up[i] = up;
-        d.ap[gi] = ap; d.vp[gi] = vp; d.up[gi] = up;
+    } else {
+        // ---- Apply_Euler (Code/Node.h:239-245) ---------------------------------------------
+        for (int i = tid - 32; i < n; i += blockDim.x - 32) {
+            int gi = n0 + i;
+            double2 ap = s_ap[i], vp = s_vp[i], up = s_up[i];
+            vp.x = vp.x + dt * ap.x; vp.y = vp.y + dt * ap.y;
+            up.x = up.x + dt * vp.x; up.y = up.y + dt * vp.y;
+            s_vp[i] = vp; s_up[i] = up;
+            d.ap[gi] = ap; d.vp[gi] = vp; d.up[gi] = up;
+        }
     }
     __syncthreads();
     // ---- Update_kinematics + Update_current_positions (Code/Body.h:2176-2227, 2272-2283) --
     for (int i = tid; i < n; i += blockDim.x) {
         int gi = n0 + i;
         double dx = 0., dy = 0., vx = 0., vy = 0., ax = 0., ay = 0.;
-        for (int j = d.sup_ptr[gi]; j < d.sup_ptr[gi + 1]; j++) {
+        const int j0 = d.sup_ptr[gi], j1 = d.sup_ptr[gi + 1];
+        int j = j0;
+        for (; j + 4 <= j1; j += 4) {            // support lists fetched four entries at a time
+            int t[4];
+            double sN[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) { t[q] = d.sup_idx[j + q]; sN[q] = d.sup_N[j + q]; }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                double2 up = s_up[t[q]], vp = s_vp[t[q]], ap = s_ap[t[q]];
+                double s = sN[q];
+                dx += s * up.x; dy += s * up.y;
+                vx += s * vp.x; vy += s * vp.y;
+                ax += s * ap.x; ay += s * ap.y;
+            }
+        }
+        for (; j < j1; j++) {
             int t = d.sup_idx[j];
             double s = d.sup_N[j];
             double2 up = s_up[t], vp = s_vp[t], ap = s_ap[t];
@@ -519,6 +699,8 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
 // ------------------------------------------------------------------------------------------
 // body kernel: rigid path
 // ------------------------------------------------------------------------------------------
+#define MEL_RIGID_BATCH 512   // border entries whose terms are staged at once (6 doubles each)
+
 __device__ void rigid_body(const mel_dev& d, int b, int parity, char* smem)
 {
     const int tid = threadIdx.x;
@@ -528,18 +710,26 @@ __device__ void rigid_body(const mel_dev& d, int b, int parity, char* smem)
     const double dt = d.dt[0];
     double* rg = d.rg + MEL_RIGID_NF * b;
     double* rf = d.rf + 15 * b;
-    double* sh = reinterpret_cast<double*>(smem);   // [0..14] forces, [16..23] drivendof
-    if (tid == 0) {
-        // Update_bc_forces, rigid (Code/Body.h:800-899)
-        double xc = rg[MEL_RG_XC], yc = rg[MEL_RG_YC];
-        double neu[3] = { 0., 0., 0. }, dir[3] = { 0., 0., 0. };
-        for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
-            int tx = d.bd_bc[2 * g], ty = d.bd_bc[2 * g + 1];
-            if (tx == MEL_BC_NONE && ty == MEL_BC_NONE) continue;
-            double xv, xvel, yv, yvel;
-            border_bc_value(d, g, 0, T, xv, xvel);
-            border_bc_value(d, g, 1, T, yv, yvel);
-            for (int e = d.bd_e0[g]; e < d.bd_e0[g + 1]; e++) {
+    double* sh = reinterpret_cast<double*>(smem);   // [0..14] forces, [16..23] drivendof, [24..32] sums
+    double* sT = sh + 64;                            // staged border terms, 6 x MEL_RIGID_BATCH
+    const double xcs = rg[MEL_RG_XC], ycs = rg[MEL_RG_YC];   // centre at the start of the step
+    // ---- Update_bc_forces, rigid (Code/Body.h:800-899): terms of every border entry computed in
+    // parallel, then each of the six sums (Neumann x, y, moment; Dirichlet x, y, moment) added
+    // in entry order by one lane.  Borders whose conditions are all none or driven add only zero
+    // terms (+0 leaves the sums unchanged for finite positions) and are skipped. -----------------
+    double acc = 0.;                                   // lane k < 6 of warp 0: sum k
+    for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
+        int tx = d.bd_bc[2 * g], ty = d.bd_bc[2 * g + 1];
+        bool activex = tx == MEL_BC_ORIENTED || tx == MEL_BC_FOLLOWING || tx == MEL_BC_SOFT;
+        bool activey = ty == MEL_BC_ORIENTED || ty == MEL_BC_FOLLOWING || ty == MEL_BC_SOFT;
+        if (!activex && !activey) continue;
+        double xv, xvel, yv, yvel;
+        border_bc_value(d, g, 0, T, xv, xvel);
+        border_bc_value(d, g, 1, T, yv, yvel);
+        for (int e0 = d.bd_e0[g]; e0 < d.bd_e0[g + 1]; e0 += MEL_RIGID_BATCH) {
+            int ne = min(MEL_RIGID_BATCH, d.bd_e0[g + 1] - e0);
+            for (int i = tid; i < ne; i += blockDim.x) {
+                int e = e0 + i;
                 int gn = n0 + d.e_node[e];
                 double length = d.e_len0[e];
                 double fxn = 0., fyn = 0., fxd = 0., fyd = 0.;
@@ -548,37 +738,41 @@ __device__ void rigid_body(const mel_dev& d, int b, int parity, char* smem)
                 else if (tx == MEL_BC_SOFT) fxd = (d.bd_bcp[4 * g] * (xv - ub.x) + d.bd_bcp[4 * g + 1] * (xvel - vb.x)) * length;
                 if (ty == MEL_BC_ORIENTED || ty == MEL_BC_FOLLOWING) fyn = yv * length;
                 else if (ty == MEL_BC_SOFT) fyd = (d.bd_bcp[4 * g + 2] * (yv - ub.y) + d.bd_bcp[4 * g + 3] * (yvel - vb.y)) * length;
-                double dx = xb.x - xc, dy = xb.y - yc;
-                neu[0] += fxn; neu[1] += fyn; neu[2] += -fxn * dy + fyn * dx;
-                dir[0] += fxd; dir[1] += fyd; dir[2] += -fxd * dy + fyd * dx;
+                double dx = xb.x - xcs, dy = xb.y - ycs;
+                sT[i] = fxn;
+                sT[MEL_RIGID_BATCH + i] = fyn;
+                sT[2 * MEL_RIGID_BATCH + i] = -fxn * dy + fyn * dx;
+                sT[3 * MEL_RIGID_BATCH + i] = fxd;
+                sT[4 * MEL_RIGID_BATCH + i] = fyd;
+                sT[5 * MEL_RIGID_BATCH + i] = -fxd * dy + fyd * dx;
             }
+            __syncthreads();
+            if (tid < 6) acc = ordered_sum(acc, sT + tid * MEL_RIGID_BATCH, ne, 1);
+            __syncthreads();
         }
+    }
+    // ---- contact forces: own contacts in list order (Code/Body.h:1866-1877), then the incoming
+    // ranges in send order; lanes 8..10 of warp 0 each carry one of the three sums -------------
+    if (tid >= 8 && tid < 11) {
+        const int k = tid - 8;
+        double con = 0.;
+        int c0 = d.b_cont0[b], c1 = d.b_cont0[b + 1];
+        con = ordered_sum(con, d.cont_rt + 6 * (size_t)c0 + k, c1 - c0, 6);
+        for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
+            int2 rr = d.inc_rng[r];
+            con = ordered_sum(con, d.cont_rt + 6 * (size_t)rr.x + 3 + k, rr.y - rr.x, 6);
+        }
+        sh[24 + 6 + k] = con;
+    }
+    if (tid < 6) sh[24 + tid] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        const double neu[3] = { sh[24], sh[25], sh[26] }, dir[3] = { sh[27], sh[28], sh[29] };
+        const double con[3] = { sh[30], sh[31], sh[32] };
         // Update_body_forces (Code/Body.h:925-928)
         double gx = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gx;
         double gy = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gy;
         double body[3] = { rg[MEL_RG_MASS] * gx, rg[MEL_RG_MASS] * gy, rf[5] };
-        // contact forces: own contacts in list order (Code/Body.h:1866-1877), then send order
-        double con[3] = { 0., 0., 0. };
-        for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
-            const mel_contact* ct = d.cont + c;
-            if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
-            double2 xs = d.x[n0 + ct->nodeS];
-            double dx = xs.x - xc, dy = xs.y - yc;
-            con[0] += ct->fx; con[1] += ct->fy; con[2] += -ct->fx * dy + ct->fy * dx;
-        }
-        for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
-            int2 rr = d.inc_rng[r];
-            for (int c = rr.x; c < rr.y; c++) {
-                const mel_contact* ct = d.cont + c;
-                int bs = ct->bodyS;
-                if (d.table[d.b_mat[bs] * d.nmat + d.b_mat[b]] <= -1) continue;
-                double2 xs = d.x[d.b_node0[bs] + ct->nodeS];
-                double dx = xs.x - xc - ct->shiftM * d.period;
-                double dy = xs.y - yc;
-                double Fsx = ct->fx, Fsy = ct->fy;
-                con[0] += -Fsx; con[1] += -Fsy; con[2] += Fsx * dy - Fsy * dx;
-            }
-        }
         for (int k = 0; k < 3; k++) { rf[k] = con[k]; rf[3 + k] = body[k]; rf[6 + k] = dir[k]; rf[9 + k] = neu[k]; }
         // Sum_up_forces (Code/Body.h:1996-1998), Apply_Newton (Code/Body.h:2034-2036)
         double tot[3];
@@ -670,7 +864,7 @@ __device__ void contact_work(const mel_dev& d, int b)
     d.works[7 * b + 1] = w;
 }
 
-__global__ void __launch_bounds__(MEL_BODY_THREADS) body_kernel(mel_dev d, int parity)
+__global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel(mel_dev d, int parity)
 {
     extern __shared__ __align__(16) char smem[];
     int b = d.b_order[blockIdx.x];
@@ -733,14 +927,13 @@ void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s)
     mel::contact_kernel<<<(total + 127) / 128, 128, 0, s>>>(d, law_dt_scale);
 }
 
-size_t mel_body_smem_bytes(int max_nodes, int max_border_nodes)
+size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes)
 {
-    (void)max_border_nodes;
-    size_t base = 2 * sizeof(double2) * (size_t)max_nodes;
-    size_t chunk = (size_t)MEL_CHUNK_E * (2 + 2 + sizeof(double2));
-    size_t post = 5 * sizeof(double2) * (size_t)max_nodes;
-    size_t rigid = 64 * sizeof(double);
-    size_t r = base + (chunk > post ? chunk : post);
+    size_t base = 3 * sizeof(double2) * (size_t)max_nodes + 32;
+    size_t stage = 2 * (size_t)max_image_bytes;
+    size_t post = (4 * sizeof(double2) + 6 * sizeof(double)) * (size_t)max_nodes;
+    size_t rigid = (64 + 6 * MEL_RIGID_BATCH) * sizeof(double);
+    size_t r = base + (stage > post ? stage : post);
     return r > rigid ? r : rigid;
 }
 

@@ -204,6 +204,12 @@ mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* ou
         if (line.compare(0, 17, "PENALTY_PARAMETER") == 0) { double p; C >> p; std::getline(C, token); }
         if (line.compare(0, 7, "GRAVITY") == 0) { C >> gx >> gy; std::getline(C, token); }
         if (line.compare(0, 8, "PLOTTING") == 0) { std::getline(C, token); std::getline(C, token); }
+        if (line.compare(0, 12, "DEACTIVATION") == 0) {     // Code/IO.h:947-951; acted on by Update_status
+            int n = 0;
+            C >> n;
+            std::getline(C, token);
+            if (n > 0) { mel_set_error("DEACTIVATION (Update_status, Code/Proximity.h:550) is not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
+        }
         if (line.compare(0, 13, "NUMBER_BODIES") == 0) { C >> nbodies; std::getline(C, token); B.resize(nbodies); }
         if (line.compare(0, 10, "DEFORMABLE") == 0 || line.compare(0, 5, "RIGID") == 0) {
             bool rigid = line.compare(0, 5, "RIGID") == 0;

@@ -50,6 +50,8 @@ struct mel_handle {
     int parity = 0;
     size_t body_smem = 0;
     int nblocks_body = 0;
+    int chunk_cap = 0;          // support entries per chunk chosen at build time
+    double img_bytes = 0.;      // bytes of all chunk images
     int launches = 0;
     double t_contact = 0., t_body = 0., t_prox = 0.;
     int timing = 0;
@@ -348,89 +350,150 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.e_len0 = dupload(h, len0);
     std::vector<double> len(len0);
     D.e_len = dupload(h, len);
+    {
+        std::vector<int> blk0(nbd + 1, 0), blk_border;
+        for (int g = 0; g < nbd; g++) {
+            int nseg = d->border_node_ptr[g + 1] - d->border_node_ptr[g] - 1;
+            int nbk = (nseg + MEL_SEGB - 1) / MEL_SEGB;
+            blk0[g + 1] = blk0[g] + nbk;
+            for (int k = 0; k < nbk; k++) blk_border.push_back(g);
+        }
+        D.nblk = blk0[nbd];
+        D.bd_blk0 = dupload(h, blk0);
+        D.blk_border = dupload(h, blk_border);
+        D.seg_blk = (double4*)dalloc<double>(h, 4 * (size_t)(D.nblk + 1));
+        std::vector<int> sblk0(nbd + 1, 0), sblk_border;
+        for (int g = 0; g < nbd; g++) {
+            int nsb = (blk0[g + 1] - blk0[g] + MEL_SEGB2 - 1) / MEL_SEGB2;
+            sblk0[g + 1] = sblk0[g] + nsb;
+            for (int k = 0; k < nsb; k++) sblk_border.push_back(g);
+        }
+        D.nsblk = sblk0[nbd];
+        D.bd_sblk0 = dupload(h, sblk0);
+        D.sblk_border = dupload(h, sblk_border);
+        D.seg_sblk = (double4*)dalloc<double>(h, 4 * (size_t)(D.nsblk + 1));
+    }
     h->H.b_type = h->b_type;
     h->H.b_per.assign(d->body_periodic, d->body_periodic + nb);
     h->H.b_bd0.assign(d->body_border_ptr, d->body_border_ptr + nb + 1);
     h->H.bd_e0.assign(d->border_node_ptr, d->border_node_ptr + nbd + 1);
-    // Gauss points: chunks of <= MEL_CHUNK_GP points and <= MEL_CHUNK_E entries, 8-entry aligned
+    // Gauss points: chunk images of <= MEL_CHUNK_GP points and <= ecap support entries.  The entry
+    // cap is the largest that lets two body CTAs share an SM; a body too large for that runs one
+    // CTA per SM.
+    int max_def_nodes = 1;
+    for (int b = 0; b < nb; b++)
+        if (d->body_type[b] == MEL_BODY_DEFORMABLE) max_def_nodes = std::max(max_def_nodes, d->body_node_ptr[b + 1] - d->body_node_ptr[b]);
     std::vector<mel_chunk> chunks;
     std::vector<int> b_chunk0(nb + 1, 0);
-    std::vector<double> gp_c0(h->ng);
-    std::vector<int> gp_e0(h->ng);
-    std::vector<uint8_t> gp_ns(h->ng);
-    std::vector<uint16_t> ge_idx, ge_tpos, tn_node, tn_start, tn_cnt;
-    std::vector<double> ge_dN;
-    std::vector<float> ge_dNf;
-    int max_def_nodes = 1;
-    for (int b = 0; b < nb; b++) {
-        b_chunk0[b] = (int)chunks.size();
-        if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
-        int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
-        max_def_nodes = std::max(max_def_nodes, nnb);
-        int g = d->body_gp_ptr[b], g1 = d->body_gp_ptr[b + 1];
-        while (g < g1) {
-            mel_chunk ch;
-            memset(&ch, 0, sizeof ch);
-            ch.gp0 = g;
-            ch.e0 = (int)ge_idx.size();
-            int ne_c = 0;
-            while (g < g1 && ch.ngp < MEL_CHUNK_GP) {
-                int ns = d->gp_sup_ptr[g + 1] - d->gp_sup_ptr[g];
-                if (ns > 255 || ns <= 0) { mel_set_error("Gauss point %d has %d supports (1..255 supported)", g, ns); return MEL_ERR_UNSUPPORTED; }
-                if (ne_c + ns > MEL_CHUNK_E) break;
-                gp_e0[g] = ch.e0 + ne_c;
-                gp_ns[g] = (uint8_t)ns;
-                gp_c0[g] = d->gp_weight[g] * d->gp_jacobian[g];   // c0 of Code/Body.h:994
-                for (int j = d->gp_sup_ptr[g]; j < d->gp_sup_ptr[g + 1]; j++) {
+    std::vector<uint8_t> img;
+    int img_max = 16;
+    size_t n_tn = 0;
+    auto build_chunks = [&](int ecap) -> mel_status {
+        chunks.clear(); img.clear(); img_max = 16; n_tn = 0;
+        std::vector<std::pair<int, int>> tp;
+        for (int b = 0; b < nb; b++) {
+            b_chunk0[b] = (int)chunks.size();
+            if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+            int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+            int g = d->body_gp_ptr[b], g1 = d->body_gp_ptr[b + 1];
+            while (g < g1) {
+                mel_chunk ch;
+                memset(&ch, 0, sizeof ch);
+                ch.gp0 = g;
+                int ne_c = 0, gend = g;
+                while (gend < g1 && gend - g < MEL_CHUNK_GP) {
+                    int ns = d->gp_sup_ptr[gend + 1] - d->gp_sup_ptr[gend];
+                    if (ns > 255 || ns <= 0) { mel_set_error("Gauss point %d has %d supports (1..255 supported)", gend, ns); return MEL_ERR_UNSUPPORTED; }
+                    if (ne_c + ns > ecap) break;
+                    ne_c += ns;
+                    gend++;
+                }
+                ch.ngp = gend - g;
+                ch.ne = (ne_c + 7) & ~7;
+                // pull order: entry positions sorted by (node, position)
+                tp.clear();
+                for (int q = 0, j = d->gp_sup_ptr[g]; q < ne_c; q++, j++) {
                     int v = d->gp_sup_idx[j];
                     if (v < 0 || v >= nnb) { mel_set_error("Gauss support index out of range"); return MEL_ERR_INVALID; }
-                    ge_idx.push_back((uint16_t)v);
-                    ge_dN.push_back(d->gp_dNdx[j]); ge_dN.push_back(d->gp_dNdy[j]);
-                    ge_dNf.push_back((float)d->gp_dNdx[j]); ge_dNf.push_back((float)d->gp_dNdy[j]);
+                    tp.push_back({ v, q });
                 }
-                ne_c += ns;
-                ch.ngp++;
-                g++;
-            }
-            // transposed pull lists: positions sorted by (node, position)
-            std::vector<std::pair<int, int>> tp;
-            tp.reserve(ne_c);
-            for (int q = 0; q < ne_c; q++) tp.push_back({ ge_idx[ch.e0 + q], q });
-            std::sort(tp.begin(), tp.end());
-            ch.tn0 = (int)tn_node.size();
-            std::vector<uint16_t> pos(ne_c);
-            for (int q = 0; q < ne_c; q++) {
-                pos[q] = (uint16_t)tp[q].second;
-                if (q == 0 || tp[q].first != tp[q - 1].first) {
-                    tn_node.push_back((uint16_t)tp[q].first);
-                    tn_start.push_back((uint16_t)q);
-                    tn_cnt.push_back(0);
+                std::sort(tp.begin(), tp.end());
+                std::vector<uint32_t> tn;
+                for (int q = 0; q < ne_c; q++)
+                    if (q == 0 || tp[q].first != tp[q - 1].first) tn.push_back((uint32_t)tp[q].first | ((uint32_t)q << 16));
+                ch.ntn = (int)tn.size();
+                tn.push_back(0xffffu | ((uint32_t)ne_c << 16));
+                n_tn += ch.ntn;
+                const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn);
+                ch.bytes = L.bytes;
+                ch.img = (long long)img.size();
+                img.resize(img.size() + L.bytes, 0);
+                uint8_t* I = img.data() + ch.img;
+                int hdr[4] = { ch.ngp, ch.ne, ch.ntn, ch.bytes };
+                memcpy(I, hdr, sizeof hdr);
+                double* dN = reinterpret_cast<double*>(I + L.dN);
+                uint16_t* idx = reinterpret_cast<uint16_t*>(I + L.idx);
+                uint16_t* tpos = reinterpret_cast<uint16_t*>(I + L.tpos);
+                double* c0 = reinterpret_cast<double*>(I + L.c0);
+                uint32_t* gpm = reinterpret_cast<uint32_t*>(I + L.gpm);
+                uint32_t* tnr = reinterpret_cast<uint32_t*>(I + L.tn);
+                int q = 0;
+                for (int gg = g; gg < gend; gg++) {
+                    int t = gg - g;
+                    int ns = d->gp_sup_ptr[gg + 1] - d->gp_sup_ptr[gg];
+                    c0[t] = d->gp_weight[gg] * d->gp_jacobian[gg];   // c0 of Code/Body.h:994
+                    gpm[t] = (uint32_t)q | ((uint32_t)ns << 16);
+                    for (int j = d->gp_sup_ptr[gg]; j < d->gp_sup_ptr[gg + 1]; j++, q++) {
+                        idx[q] = (uint16_t)d->gp_sup_idx[j];
+                        dN[2 * q] = d->gp_dNdx[j];
+                        dN[2 * q + 1] = d->gp_dNdy[j];
+                    }
                 }
-                tn_cnt.back()++;
+                for (int k = 0; k < ne_c; k++) tpos[k] = (uint16_t)tp[k].second;
+                memcpy(tnr, tn.data(), sizeof(uint32_t) * tn.size());
+                img_max = std::max(img_max, ch.bytes);
+                chunks.push_back(ch);
+                g = gend;
             }
-            ch.ntn = (int)tn_node.size() - ch.tn0;
-            for (int q = 0; q < ne_c; q++) ge_tpos.push_back(pos[q]);
-            int pad = (8 - (ne_c & 7)) & 7;
-            for (int q = 0; q < pad; q++) { ge_idx.push_back(0); ge_tpos.push_back(0); ge_dN.push_back(0.); ge_dN.push_back(0.); ge_dNf.push_back(0.f); ge_dNf.push_back(0.f); }
-            ch.ne = ne_c + pad;
-            chunks.push_back(ch);
         }
+        b_chunk0[nb] = (int)chunks.size();
+        return MEL_OK;
+    };
+    int smem_sm = 0, smem_blk = 0, smem_res = 0;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device);
+    cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, h->device);
+    const size_t two_per_sm = (size_t)(smem_sm / 2 - smem_res);
+    {
+        const int caps[] = { MEL_CHUNK_E_MAX, 1536, 1024, 768, 512, 256 };
+        int chosen = -1;
+        for (int ecap : caps) {
+            mel_status rc = build_chunks(ecap);
+            if (rc) return rc;
+            size_t sm = mel_body_smem_bytes(max_def_nodes, img_max);
+            if (sm <= two_per_sm) { chosen = ecap; break; }
+        }
+        if (chosen < 0) {   // one CTA per SM: largest cap that fits
+            for (int ecap : caps) {
+                mel_status rc = build_chunks(ecap);
+                if (rc) return rc;
+                if (mel_body_smem_bytes(max_def_nodes, img_max) <= (size_t)smem_blk) { chosen = ecap; break; }
+            }
+        }
+        if (chosen < 0) {
+            mel_set_error("deformable body of %d nodes does not fit the body kernel's shared memory", max_def_nodes);
+            return MEL_ERR_UNSUPPORTED;
+        }
+        h->chunk_cap = chosen;
     }
-    b_chunk0[nb] = (int)chunks.size();
-    h->nge = (int)ge_idx.size();
+    h->nge = 0;
+    for (const mel_chunk& c : chunks) h->nge += c.ne;
     D.nchunk = (int)chunks.size();
     D.chunk = dupload(h, chunks);
     D.b_chunk0 = dupload(h, b_chunk0);
-    D.gp_c0 = dupload(h, gp_c0);
-    D.gp_e0 = dupload(h, gp_e0);
-    D.gp_ns = dupload(h, gp_ns);
-    D.ge_idx = dupload(h, ge_idx);
-    D.ge_tpos = dupload(h, ge_tpos);
-    D.ge_dN = (const double2*)dupload(h, ge_dN);
-    D.ge_dNf = (const float2*)dupload(h, ge_dNf);
-    D.tn_node = dupload(h, tn_node);
-    D.tn_start = dupload(h, tn_start);
-    D.tn_cnt = dupload(h, tn_cnt);
+    D.img = reinterpret_cast<const char*>(dupload(h, img));
+    D.img_cap = img_max;
+    h->img_bytes = (double)img.size();
     // contacts and proximity buffers
     D.err = dalloc<unsigned>(h, MEL_E_NWORDS);
     D.ncont = 0;
@@ -442,6 +505,10 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     P.shmin = dalloc<int>(h, nbd);
     P.shmax = dalloc<int>(h, nbd);
     P.b_inc0 = dalloc<int>(h, nb + 1);
+    P.tcnt = dalloc<int>(h, nb + 1);
+    P.btask0 = dalloc<int>(h, nb + 2);
+    P.scnt = dalloc<int>(h, nb + 1);
+    P.bslot0 = dalloc<int>(h, nb + 2);
     P.b_cont0 = dalloc<int>(h, nb + 1);
     P.e_cnt = dalloc<int>(h, ne + 1);
     P.e_ptr = dalloc<int>(h, ne + 2);
@@ -452,12 +519,14 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     if (cudaMalloc(&P.cont_w, sizeof(double) * 1024) != cudaSuccess) return MEL_ERR_OOM;
     P.cont_w_bytes = sizeof(double) * 1024;
     D.cont_w = P.cont_w;
+    if (cudaMalloc(&P.cont_rt, 6 * sizeof(double) * 1024) != cudaSuccess) return MEL_ERR_OOM;
+    P.cont_rt_bytes = 6 * sizeof(double) * 1024;
+    D.cont_rt = P.cont_rt;
     D.b_cont0 = P.b_cont0; D.b_inc0 = P.b_inc0;
     if (cudaMalloc(&P.inc_rng, sizeof(int2) * 16) != cudaSuccess) return MEL_ERR_OOM;
     P.inc_rng_bytes = sizeof(int2) * 16;
     D.inc_rng = P.inc_rng;
-    h->body_smem = mel_body_smem_bytes(max_def_nodes, 0);
-    if (h->body_smem > 227 * 1024) { mel_set_error("body of %d nodes needs %zu bytes of shared memory", max_def_nodes, h->body_smem); return MEL_ERR_UNSUPPORTED; }
+    h->body_smem = mel_body_smem_bytes(max_def_nodes, img_max);
     mel_body_kernel_configure(h->body_smem);
     h->d_monitor = dalloc<double>(h, 32);
     h->d_monitor_part = dalloc<double>(h, 5 * 148);
@@ -468,9 +537,10 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         h->d_rigid_ids = dupload(h, rid);
     }
     // algorithmic bytes moved by one launch of each step kernel (exact array sizes):
-    // body kernel: Gauss entries (16-bit index + 16-bit pull position + dN/dx,dN/dy), per point
-    // c0, entry offset, support count; pull records; node state read (up, vp, 1/m, m) and written
-    // (up, vp, ap, u, v, a, x); node supports (16-bit index + N) and offsets; contact records read.
+    // body kernel: the chunk images (entries: dN/dx,dN/dy + 16-bit index + 16-bit pull position;
+    // points: c0 + offset/count; touched-node records) and the chunk table; node state read (up,
+    // vp, m, 1/m, X0) and written (up, vp, ap, u, v, a, x); node supports (16-bit index + N) and
+    // their offsets.  Contact records are left out (a few hundred bytes per body).
     {
         double nd = 0;
         for (int b = 0; b < nb; b++) if (d->body_type[b] == MEL_BODY_DEFORMABLE) nd += d->body_node_ptr[b + 1] - d->body_node_ptr[b];
@@ -479,8 +549,8 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         for (int b = 0; b < nb; b++)
             if (d->body_type[b] == MEL_BODY_DEFORMABLE)
                 nse_def += d->node_sup_ptr[d->body_node_ptr[b + 1]] - d->node_sup_ptr[d->body_node_ptr[b]];
-        h->bytes_body = (double)h->nge * (2 + 2 + 16) + (double)h->ng * (8 + 4 + 1) + (double)tn_node.size() * 6 +
-                        (double)chunks.size() * sizeof(mel_chunk) + nd * (4 * 16 + 7 * 16) + nse_def * (2 + 8) + (nd + 1) * 4;
+        h->bytes_body = h->img_bytes + (double)chunks.size() * sizeof(mel_chunk) + nd * (5 * 16 + 7 * 16) +
+                        nse_def * (2 + 8) + (nd + 1) * 4;
         h->bytes_contact = (double)ne * (4 * 4 + 4 * 4 + 8 + 8);   // refreshed border lengths (contacts added per call)
     }
     if (cudaDeviceSynchronize() != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "build", __FILE__, __LINE__); return MEL_ERR_CUDA; }
@@ -495,6 +565,7 @@ static mel_status check_errors(mel_handle* h)
     unsigned w[MEL_E_NWORDS];
     if (cudaMemcpy(w, h->d.err, sizeof w, cudaMemcpyDeviceToHost) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "err", __FILE__, __LINE__); return MEL_ERR_CUDA; }
     if (w[MEL_E_BOUNDS]) { mel_set_error("device index check failed (code %u)", w[MEL_E_BOUNDS]); return MEL_ERR_BOUNDS; }
+    if (w[MEL_E_WAIT]) { mel_set_error("a shared-memory bulk copy did not complete within %llu ns", MEL_WAIT_NS); return MEL_ERR_TIMEOUT; }
     return MEL_OK;
 }
 
@@ -511,7 +582,7 @@ static mel_status proximity(mel_handle* h)
         h->t_prox += ms;
         cudaEventDestroy(e0); cudaEventDestroy(e1);
     }
-    if (rc) { if (rc == MEL_ERR_CUDA) mel_set_cuda_error(cudaGetLastError(), "proximity", __FILE__, __LINE__); else mel_set_error("proximity failed (%d)", rc); return (mel_status)rc; }
+    if (rc) { if (rc == MEL_ERR_CUDA) mel_set_cuda_error(cudaGetLastError(), "proximity", __FILE__, __LINE__); return (mel_status)rc; }
     return MEL_OK;
 }
 
@@ -653,7 +724,8 @@ mel_status mel_destroy(mel_handle* h)
     for (void* p : h->allocs) cudaFree(p);
     mel_prox_state& P = h->P;
     for (void* p : { (void*)P.nbr, (void*)P.task, (void*)P.inc_task, (void*)P.slot_cnt, (void*)P.slot_off, (void*)P.inc_rng,
-                     (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)h->d.cont })
+                     (void*)P.tns, (void*)P.tslot, (void*)P.tkey,
+                     (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)P.cont_rt, (void*)h->d.cont })
         if (p) cudaFree(p);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
@@ -758,6 +830,12 @@ mel_status mel_set_contacts(mel_handle* h, const mel_contact* c, int n)
     }
     h->d.cont_w = h->P.cont_w;
     cudaMemset(h->P.cont_w, 0, sizeof(double) * (n + 1));
+    if (6 * sizeof(double) * (size_t)(n + 1) > h->P.cont_rt_bytes) {
+        cudaFree(h->P.cont_rt);
+        if (cudaMalloc(&h->P.cont_rt, 6 * sizeof(double) * (n + 1)) != cudaSuccess) return MEL_ERR_OOM;
+        h->P.cont_rt_bytes = 6 * sizeof(double) * (n + 1);
+    }
+    h->d.cont_rt = h->P.cont_rt;
     if (n) MEL_CUDA_OK(cudaMemcpy(h->d.cont, c, sizeof(mel_contact) * n, cudaMemcpyHostToDevice));
     h->d.ncont = n;
     int rc = mel_index_external(h->d, h->P, c, n, h->stream);

@@ -92,9 +92,19 @@ __global__ void aabb_kernel(mel_dev d, double* aabb, int* shmin, int* shmax)
     }
     if (lane == 0) {
         double invperiod = 1. / d.period;
+        double f0 = floor((xmin - d.xmin) * invperiod), f1 = floor((xmax - d.xmin) * invperiod);
+        // a box that is not finite, or that spans more periods than any body can, comes from a
+        // diverged state; it is reported and left out of the neighbour search, whose shift loop
+        // it would otherwise drive through billions of iterations
+        bool finite = isfinite(xmin) && isfinite(xmax) && isfinite(ymin) && isfinite(ymax);
+        bool sane = finite && fabs(f0) < 1.e6 && fabs(f1) < 1.e6 && f1 - f0 <= MEL_MAX_SHIFT_SPAN;
+        if (!sane) {
+            atomicOr(&d.err[MEL_E_NAN], finite ? 2u : 1u);
+            xmin = 1.e300; xmax = -1.e300; ymin = 1.e300; ymax = -1.e300; f0 = 0.; f1 = -1.;
+        }
         aabb[4 * g] = xmin; aabb[4 * g + 1] = xmax; aabb[4 * g + 2] = ymin; aabb[4 * g + 3] = ymax;
-        shmin[g] = (int)floor((xmin - d.xmin) * invperiod);
-        shmax[g] = (int)floor((xmax - d.xmin) * invperiod);
+        shmin[g] = (int)f0;
+        shmax[g] = (int)f1;
     }
 }
 
@@ -161,12 +171,72 @@ __global__ void neighbour_kernel(mel_dev d, const double* aabb, const int* shmin
     }
 }
 
-// candidate enumeration shared by the count and write passes -----------------------------------
-struct Cand {
-    int seg, bM, rM, shM;
-    Proj p;
-    int nd[4], sh[4];
-};
+// ---------------------------------------------------------------------------------------------
+// segment blocks: bounding boxes of MEL_SEGB consecutive segments of a border (node1/node2 positions
+// with the border's own period shifts).  Used only to skip segments that cannot pass
+// Detect_Segment_Proximity; the boxes are widened by the detection distance plus a margin, so the
+// accepted candidates and their order are unchanged.
+// ---------------------------------------------------------------------------------------------
+__global__ void segblock_kernel(mel_dev d)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.nblk) return;
+    int g = d.blk_border[k];
+    int b = d.bd_body[g];
+    int e0 = d.bd_e0[g];
+    int nseg = d.bd_e0[g + 1] - e0 - 1;
+    int s0 = (k - d.bd_blk0[g]) * MEL_SEGB;
+    int s1 = min(s0 + MEL_SEGB, nseg);
+    int n0 = d.b_node0[b];
+    double xmin = 1.e300, xmax = -1.e300, ymin = 1.e300, ymax = -1.e300;
+    for (int sg = s0; sg < s1; sg++) {
+        int e = e0 + sg;
+        for (int j = 1; j <= 2; j++) {
+            // shifted (regular search) and unshifted (self search) abscissae both count
+            double2 p = d.x[n0 + d.e_sn[4 * e + j]];
+            double x = p.x + d.period * d.e_ss[4 * e + j];
+            xmin = fmin(xmin, fmin(x, p.x)); xmax = fmax(xmax, fmax(x, p.x));
+            ymin = fmin(ymin, p.y); ymax = fmax(ymax, p.y);
+        }
+    }
+    d.seg_blk[k] = make_double4(xmin, xmax, ymin, ymax);
+}
+
+// superblock boxes: unions of MEL_SEGB2 consecutive block boxes of one border
+__global__ void superblock_kernel(mel_dev d)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.nsblk) return;
+    int g = d.sblk_border[k];
+    int b0 = d.bd_blk0[g] + (k - d.bd_sblk0[g]) * MEL_SEGB2;
+    int b1 = min(b0 + MEL_SEGB2, d.bd_blk0[g + 1]);
+    double4 u = make_double4(1.e300, -1.e300, 1.e300, -1.e300);
+    for (int j = b0; j < b1; j++) {
+        double4 bb = d.seg_blk[j];
+        u.x = fmin(u.x, bb.x); u.y = fmax(u.y, bb.y); u.z = fmin(u.z, bb.z); u.w = fmax(u.w, bb.w);
+    }
+    d.seg_sblk[k] = u;
+}
+
+__device__ __forceinline__ bool block_may_detect(const double4& bb, double xs, double ys, double m)
+{
+    return !(xs < bb.x - m || xs > bb.y + m || ys < bb.z - m || ys > bb.w + m);
+}
+
+// Calls body(kb) for each block kb (border-local index) of border g whose superblock box and
+// block box both lie within `margin` of (x, y), in ascending block order.
+template <typename F>
+__device__ __forceinline__ void for_near_blocks(const mel_dev& d, int g, double x, double y, double margin, F&& body)
+{
+    const int blk0 = d.bd_blk0[g], blk1 = d.bd_blk0[g + 1];
+    for (int ks = d.bd_sblk0[g]; ks < d.bd_sblk0[g + 1]; ks++) {
+        if (!block_may_detect(d.seg_sblk[ks], x, y, margin)) continue;
+        const int k0 = blk0 + (ks - d.bd_sblk0[g]) * MEL_SEGB2;
+        const int k1 = min(k0 + MEL_SEGB2, blk1);
+        for (int k = k0; k < k1; k++)
+            if (block_may_detect(d.seg_blk[k], x, y, margin)) body(k - blk0);
+    }
+}
 
 // regular task: slave node kS of global border gS of body bS against neighbour (bM, rM, shM)
 template <typename F>
@@ -177,23 +247,29 @@ __device__ __forceinline__ void enum_regular(const mel_dev& d, int bS, int gS, i
     int eS = d.bd_e0[gS] + kS;
     double2 xs = d.x[d.b_node0[bS] + d.e_node[eS]];
     double dd = d.b_dist[3 * bS + 1], cd = d.b_dist[3 * bS + 2];
+    double margin = dd * 1.0001 + 1e-12 * (fabs(xs.x) + fabs(xs.y) + fabs(d.period * shM)) + 1e-15;
+    double xrel = xs.x - d.period * shM;
     int mb = d.b_node0[bM];
-    for (int seg = 0; seg < nM - 1; seg++) {
-        int e = eM0 + seg;
-        const int* sn = d.e_sn + 4 * e;
-        const int* ss = d.e_ss + 4 * e;
-        double2 p1 = d.x[mb + sn[1]], p2 = d.x[mb + sn[2]];
-        double X1 = p1.x + d.period * (shM + ss[1]), Y1 = p1.y;
-        double X2 = p2.x + d.period * (shM + ss[2]), Y2 = p2.y;
-        if (detect_proximity(xs.x, xs.y, X1, Y1, X2, Y2, dd) == 0) continue;
-        double2 p0 = d.x[mb + sn[0]], p3 = d.x[mb + sn[3]];
-        double X0 = p0.x + d.period * (shM + ss[0]), Y0 = p0.y;
-        double X3 = p3.x + d.period * (shM + ss[3]), Y3 = p3.y;
-        Proj p;
-        p.gap = 0.; p.xsi = 0.; p.xn = p.yn = p.xt = p.yt = 0.; p.N[0] = p.N[1] = p.N[2] = p.N[3] = 0.; p.flag = 0;
-        closest_linear(xs.x, xs.y, X0, Y0, X1, Y1, X2, Y2, X3, Y3, p);
-        if ((p.flag == -2 || p.flag == -1 || p.flag == 0) && (p.gap > -cd)) f(seg, e, p);
-    }
+    for_near_blocks(d, gM, xrel, xs.y, margin, [&](int kb) {
+        int s0 = kb * MEL_SEGB;
+        int s1 = min(s0 + MEL_SEGB, nM - 1);
+        for (int seg = s0; seg < s1; seg++) {
+            int e = eM0 + seg;
+            const int* sn = d.e_sn + 4 * e;
+            const int* ss = d.e_ss + 4 * e;
+            double2 p1 = d.x[mb + sn[1]], p2 = d.x[mb + sn[2]];
+            double X1 = p1.x + d.period * (shM + ss[1]), Y1 = p1.y;
+            double X2 = p2.x + d.period * (shM + ss[2]), Y2 = p2.y;
+            if (detect_proximity(xs.x, xs.y, X1, Y1, X2, Y2, dd) == 0) continue;
+            double2 p0 = d.x[mb + sn[0]], p3 = d.x[mb + sn[3]];
+            double X0 = p0.x + d.period * (shM + ss[0]), Y0 = p0.y;
+            double X3 = p3.x + d.period * (shM + ss[3]), Y3 = p3.y;
+            Proj p;
+            p.gap = 0.; p.xsi = 0.; p.xn = p.yn = p.xt = p.yt = 0.; p.N[0] = p.N[1] = p.N[2] = p.N[3] = 0.; p.flag = 0;
+            closest_linear(xs.x, xs.y, X0, Y0, X1, Y1, X2, Y2, X3, Y3, p);
+            if ((p.flag == -2 || p.flag == -1 || p.flag == 0) && (p.gap > -cd)) f(seg, e, p);
+        }
+    });
 }
 
 // self task: slave node kS of global border gS of body bS against the body's own segments
@@ -206,31 +282,87 @@ __device__ __forceinline__ void enum_self(const mel_dev& d, int bS, int gS, int 
     int n0 = d.b_node0[bS];
     double2 xs = d.x[n0 + NodeS];
     double dd = d.b_dist[3 * bS + 1], cd = d.b_dist[3 * bS + 2];
+    double margin = dd * 1.0001 + 1e-12 * (fabs(xs.x) + fabs(xs.y)) + 1e-15;
     for (int gM = d.b_bd0[bS]; gM < d.b_bd0[bS + 1]; gM++) {
         int eM0 = d.bd_e0[gM], nM = d.bd_e0[gM + 1] - eM0;
-        for (int seg = 0; seg < nM - 1; seg++) {
-            int e = eM0 + seg;
-            const int* sn = d.e_sn + 4 * e;
-            if (sn[1] == NodeS) continue;
-            if (sn[2] == NodeS) continue;
-            double2 p1 = d.x[n0 + sn[1]], p2 = d.x[n0 + sn[2]];
-            if (detect_proximity(xs.x, xs.y, p1.x, p1.y, p2.x, p2.y, dd) == 0) continue;
-            if (sn[0] == NodeS || sn[3] == NodeS) continue;
-            double2 p0 = d.x[n0 + sn[0]], p3 = d.x[n0 + sn[3]];
-            Proj p;
-            p.gap = 0.; p.xsi = 0.; p.xn = p.yn = p.xt = p.yt = 0.; p.N[0] = p.N[1] = p.N[2] = p.N[3] = 0.; p.flag = 0;
-            closest_linear(xs.x, xs.y, p0.x, p0.y, p1.x, p1.y, p2.x, p2.y, p3.x, p3.y, p);
-            if (p.flag == 0 && (p.gap > -cd)) f(seg, e, p, gM - d.b_bd0[bS]);
-        }
+        for_near_blocks(d, gM, xs.x, xs.y, margin, [&](int kb) {
+            int s0 = kb * MEL_SEGB;
+            int s1 = min(s0 + MEL_SEGB, nM - 1);
+            for (int seg = s0; seg < s1; seg++) {
+                int e = eM0 + seg;
+                const int* sn = d.e_sn + 4 * e;
+                if (sn[1] == NodeS) continue;
+                if (sn[2] == NodeS) continue;
+                double2 p1 = d.x[n0 + sn[1]], p2 = d.x[n0 + sn[2]];
+                if (detect_proximity(xs.x, xs.y, p1.x, p1.y, p2.x, p2.y, dd) == 0) continue;
+                if (sn[0] == NodeS || sn[3] == NodeS) continue;
+                double2 p0 = d.x[n0 + sn[0]], p3 = d.x[n0 + sn[3]];
+                Proj p;
+                p.gap = 0.; p.xsi = 0.; p.xn = p.yn = p.xt = p.yt = 0.; p.N[0] = p.N[1] = p.N[2] = p.N[3] = 0.; p.flag = 0;
+                closest_linear(xs.x, xs.y, p0.x, p0.y, p1.x, p1.y, p2.x, p2.y, p3.x, p3.y, p);
+                if (p.flag == 0 && (p.gap > -cd)) f(seg, e, p, gM - d.b_bd0[bS]);
+            }
+        });
     }
 }
 
-__global__ void count_kernel(mel_dev d, const int* task, int ntask, const int* nbr, int cap, int* slot_cnt)
+// ---------------------------------------------------------------------------------------------
+// task list on the device.  Task t: slave body, slave border (global), neighbour index q (-1: self),
+// slave border nodes; tasks of a body are contiguous: (border, neighbour) pairs in the reference's
+// loop order (Code/Proximity.h:207-212), then one self task per border (Code/Proximity.h:346-356).
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool has_self(const mel_dev& d, int b)
+{
+    return d.self_contact && d.b_type[b] == MEL_BODY_DEFORMABLE && !d.b_per[b];
+}
+
+// per body: task count and slot count (slave border nodes summed over its tasks)
+__global__ void task_count_kernel(mel_dev d, const int* nbn, int* tcnt, int* scnt)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.nb) return;
+    int nbd = d.b_bd0[b + 1] - d.b_bd0[b];
+    int nent = d.bd_e0[d.b_bd0[b + 1]] - d.bd_e0[d.b_bd0[b]];
+    int per = nbn[b] + (has_self(d, b) ? 1 : 0);
+    tcnt[b] = nbd * per;
+    scnt[b] = nent * per;
+}
+
+// task t = (slave body, slave border, neighbour q or -1 for self, first slot), its slave border node
+// count, its first slot and its master body; inc_cnt counts the tasks of each master body
+__global__ void task_fill_kernel(mel_dev d, const int* nbr, const int* nbn, int cap, const int* btask0,
+                                 const int* bslot0, int4* task, int* tns, int* tslot, int* tkey, int* inc_cnt)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.nb) return;
+    int t = btask0[b];
+    int slot = bslot0[b];
+    const int* nb = nbr + (size_t)3 * cap * b;
+    for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
+        int nS = d.bd_e0[g + 1] - d.bd_e0[g];
+        for (int q = 0; q < nbn[b]; q++) {
+            int key = nb[3 * q];
+            task[t] = make_int4(b, g, q, slot); tns[t] = nS; tslot[t] = slot; tkey[t] = key;
+            atomicAdd(&inc_cnt[key], 1);
+            t++; slot += nS;
+        }
+    }
+    if (has_self(d, b))
+        for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
+            int nS = d.bd_e0[g + 1] - d.bd_e0[g];
+            task[t] = make_int4(b, g, -1, slot); tns[t] = nS; tslot[t] = slot; tkey[t] = b;
+            atomicAdd(&inc_cnt[b], 1);
+            t++; slot += nS;
+        }
+}
+
+__global__ void count_kernel(mel_dev d, const int4* task, int ntask, const int* nbr, int cap, int* slot_cnt)
 {
     int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (t >= ntask) return;
-    int bS = task[4 * t], gS = task[4 * t + 1], q = task[4 * t + 2], slot0 = task[4 * t + 3];
+    int4 tk = task[t];
+    int bS = tk.x, gS = tk.y, q = tk.z, slot0 = tk.w;
     int nS = d.bd_e0[gS + 1] - d.bd_e0[gS];
     for (int kS = lane; kS < nS; kS += 32) {
         int cnt = 0;
@@ -244,19 +376,21 @@ __global__ void count_kernel(mel_dev d, const int* task, int ntask, const int* n
     }
 }
 
-__global__ void write_kernel(mel_dev d, const int* task, int ntask, const int* nbr, int cap, const int* slot_off,
+__global__ void write_kernel(mel_dev d, const int4* task, int ntask, const int* nbr, int cap, const int* slot_off,
                              mel_contact* out, const mel_contact* old, const int* old_eptr, const int* old_elist,
                              int have_old)
 {
     int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (t >= ntask) return;
-    int bS = task[4 * t], gS = task[4 * t + 1], q = task[4 * t + 2], slot0 = task[4 * t + 3];
+    int4 tk = task[t];
+    int bS = tk.x, gS = tk.y, q = tk.z, slot0 = tk.w;
     int rS = gS - d.b_bd0[bS];
     int eS0 = d.bd_e0[gS];
     int nS = d.bd_e0[gS + 1] - eS0;
     for (int kS = lane; kS < nS; kS += 32) {
         int pos = slot_off[slot0 + kS];
+        const int end = slot_off[slot0 + kS + 1];   // the count pass found end - pos candidates
         int eS = eS0 + kS;
         int NodeS = d.e_node[eS];
         double length = d.e_len[eS];
@@ -289,7 +423,8 @@ __global__ void write_kernel(mel_dev d, const int* task, int ntask, const int* n
                 }
                 c.bodyS = bS;
                 c.pad_ = found ? 0 : 1;      // new elements get vgapn/vgapt in carry_kernel
-                out[pos++] = c;
+                if (pos < end) out[pos] = c;
+                pos++;
             });
         } else {
             double effm = d.rg[MEL_RIGID_NF * bS + MEL_RG_MASS];
@@ -302,11 +437,49 @@ __global__ void write_kernel(mel_dev d, const int* task, int ntask, const int* n
                 c.xnorm = p.xn; c.ynorm = p.yn; c.xtan = p.xt; c.ytan = p.yt;
                 c.effective_mass = effm; c.length = length; c.fx = 0.; c.fy = 0.;
                 c.nb_internal = 0; c.pad_ = 1; c.internal[0] = 0.; c.internal[1] = 0.; c.internal[2] = 0.;
-                out[pos++] = c;
+                if (pos < end) out[pos] = c;
+                pos++;
             });
         }
+        if (pos != end) atomicOr(&d.err[MEL_E_BOUNDS], 4u);   // count and write passes disagree
     }
 }
+
+// ---------------------------------------------------------------------------------------------
+// incoming (master-side) contact ranges of each body in send order.  Send_contact_forces runs over
+// the sending bodies in index order (Code/Solver.h:61-62) and each sender over its contact list, so
+// the incoming ranges of master body B are the tasks whose master is B, in ascending task order.
+// Tasks are grouped by master with a counting pass and an atomic fill, then each group is put back
+// in ascending order by a rank sort (task ids are unique), one warp per master body.
+// ---------------------------------------------------------------------------------------------
+__global__ void inc_fill_kernel(const int* tkey, int ntask, int* cur, int* tmp)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntask) return;
+    tmp[atomicAdd(&cur[tkey[t]], 1)] = t;
+}
+
+__global__ void inc_sort_kernel(int nb, const int* inc0, const int* tmp, int* sorted)
+{
+    int B = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (B >= nb) return;
+    int i0 = inc0[B], n = inc0[B + 1] - i0;
+    for (int i = lane; i < n; i += 32) {
+        int t = tmp[i0 + i], r = 0;
+        for (int j = 0; j < n; j++) r += (tmp[i0 + j] < t);
+        sorted[i0 + r] = t;
+    }
+}
+
+__global__ void inc_range_kernel(const int* sorted, int n, const int* tslot, const int* tns, const int* slot_off, int2* rng)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int t = sorted[i];
+    rng[i] = make_int2(slot_off[tslot[t]], slot_off[tslot[t] + tns[t]]);
+}
+
 
 // per-body serial counting sort of a body-major contact list by slave border entry
 __global__ void entry_index_kernel(mel_dev d, const mel_contact* cont, const int* b_cont0, int* eptr_cnt, int* elist)
@@ -360,17 +533,6 @@ __global__ void carry_kernel(const mel_dev d, mel_contact* cont, const int* b_co
     }
 }
 
-__global__ void inc_range_kernel(const int* inc_task, int ninc, const int* task, const int* slot_off,
-                                 const mel_dev d, int2* rng)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ninc) return;
-    int t = inc_task[i];
-    int gS = task[4 * t + 1], slot0 = task[4 * t + 3];
-    int nS = d.bd_e0[gS + 1] - d.bd_e0[gS];
-    rng[i] = make_int2(slot_off[slot0], slot_off[slot0 + nS]);
-}
-
 } // namespace mel
 
 // =============================================================================================
@@ -378,17 +540,22 @@ __global__ void inc_range_kernel(const int* inc_task, int ninc, const int* task,
 // =============================================================================================
 #include "mel_prox_host.h"
 
-static int ensure(void** p, size_t* cap_bytes, size_t need)
+static int ensure_impl(void** p, size_t* cap_bytes, size_t need, const char* what)
 {
     if (need <= *cap_bytes && *p) return 0;
     size_t nc = need + need / 2 + 4096;
     void* np = nullptr;
-    if (cudaMalloc(&np, nc) != cudaSuccess) return 1;
+    cudaError_t e = cudaMalloc(&np, nc);
+    if (e != cudaSuccess) {
+        mel_set_error("allocation of %zu bytes for %s failed: %s", nc, what, cudaGetErrorString(e));
+        return 1;
+    }
     if (*p) cudaFree(*p);
     *p = np;
     *cap_bytes = nc;
     return 0;
 }
+#define ensure(p, cap, need) ensure_impl(p, cap, need, #p)
 
 // Rebuilds b_cont0 and the per-entry index of the current list (d.cont, d.ncont).
 int mel_index_contacts(mel_dev& d, mel_prox_state& P, cudaStream_t s)
@@ -407,85 +574,68 @@ int mel_index_contacts(mel_dev& d, mel_prox_state& P, cudaStream_t s)
 int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cudaStream_t s)
 {
     using namespace mel;
+    (void)H;
     const int nb = d.nb;
-    // 1. border boxes
+    // 1. border boxes and segment-block boxes
     aabb_kernel<<<(d.nbd * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax);
-    // 2. neighbours (retry with a larger capacity on overflow)
-    for (int attempt = 0; attempt < 4; attempt++) {
+    if (d.nblk > 0) segblock_kernel<<<(d.nblk + 127) / 128, 128, 0, s>>>(d);
+    if (d.nsblk > 0) superblock_kernel<<<(d.nsblk + 127) / 128, 128, 0, s>>>(d);
+    // 2. neighbours and the task list; one read-back: overflow flag, task count, slot count
+    int ntask = 0, nslot = 0;
+    bool overflow = true;
+    for (int attempt = 0; attempt < 4 && overflow; attempt++) {
         cudaMemsetAsync(d.err + MEL_E_NBR_OVERFLOW, 0, sizeof(unsigned), s);
         cudaMemsetAsync(d.err + MEL_E_NBR_NEED, 0, sizeof(unsigned), s);
         neighbour_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax, P.nbr, P.nbn, P.nbr_cap);
-        unsigned ov[2];
-        cudaMemcpyAsync(ov, d.err + MEL_E_NBR_OVERFLOW, sizeof(unsigned) * 1, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(ov + 1, d.err + MEL_E_NBR_NEED, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+        task_count_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, P.nbn, P.tcnt, P.scnt);
+        mel_scan_exclusive(P.tcnt, P.btask0, nb, s);
+        mel_scan_exclusive(P.scnt, P.bslot0, nb, s);
+        unsigned hv[MEL_E_NWORDS];
+        cudaMemcpyAsync(hv, d.err, sizeof hv, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&ntask, P.btask0 + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&nslot, P.bslot0 + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) return MEL_ERR_CUDA;
-        if (!ov[0]) break;
-        int need = (int)ov[1] + 16;
+        if (hv[MEL_E_NAN]) {
+            mel_set_error(hv[MEL_E_NAN] & 1u ? "non-finite node positions at the proximity update"
+                                             : "a border box spans more than %d periods: diverged positions",
+                          MEL_MAX_SHIFT_SPAN);
+            return MEL_ERR_NAN;
+        }
+        hv[0] = hv[MEL_E_NBR_OVERFLOW]; hv[1] = hv[MEL_E_NBR_NEED];
+        overflow = hv[0] != 0;
+        if (!overflow) break;
+        int need = (int)hv[1] + 16;
         cudaFree(P.nbr); P.nbr = nullptr;
-        if (cudaMalloc(&P.nbr, sizeof(int) * 3 * (size_t)need * nb) != cudaSuccess) return MEL_ERR_OOM;
+        if (cudaMalloc(&P.nbr, sizeof(int) * 3 * (size_t)need * nb) != cudaSuccess) {
+            mel_set_error("allocation of neighbour lists (%d per body) failed", need);
+            return MEL_ERR_OOM;
+        }
         P.nbr_cap = need;
     }
-    // 3. task list on the host (reference loop order, Code/Proximity.h:207-212 and 346-356)
-    P.h_nbn.resize(nb);
-    P.h_nbr.resize((size_t)3 * P.nbr_cap * nb);
-    cudaMemcpyAsync(P.h_nbn.data(), P.nbn, sizeof(int) * nb, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(P.h_nbr.data(), P.nbr, sizeof(int) * 3 * (size_t)P.nbr_cap * nb, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) return MEL_ERR_CUDA;
-    std::vector<int>& T = P.h_task;
-    T.clear();
-    std::vector<int> key;            // master body of each task
-    int slot = 0;
-    for (int b = 0; b < nb; b++) {
-        for (int g = H.b_bd0[b]; g < H.b_bd0[b + 1]; g++) {
-            int nS = H.bd_e0[g + 1] - H.bd_e0[g];
-            for (int q = 0; q < P.h_nbn[b]; q++) {
-                T.push_back(b); T.push_back(g); T.push_back(q); T.push_back(slot);
-                key.push_back(P.h_nbr[(size_t)3 * P.nbr_cap * b + 3 * q]);
-                slot += nS;
-            }
-        }
-        if (d.self_contact && H.b_type[b] == MEL_BODY_DEFORMABLE && !H.b_per[b]) {
-            for (int g = H.b_bd0[b]; g < H.b_bd0[b + 1]; g++) {
-                int nS = H.bd_e0[g + 1] - H.bd_e0[g];
-                T.push_back(b); T.push_back(g); T.push_back(-1); T.push_back(slot);
-                key.push_back(b);
-                slot += nS;
-            }
-        }
-    }
-    int ntask = (int)(T.size() / 4);
-    int nslot = slot;
-    // incoming task lists: tasks grouped by master body, each group in task order (= send order)
-    std::vector<int> inc_cnt(nb + 1, 0);
-    for (int t = 0; t < ntask; t++) inc_cnt[key[t] + 1]++;
-    for (int b = 0; b < nb; b++) inc_cnt[b + 1] += inc_cnt[b];
-    P.h_inc_task.assign(ntask > 0 ? ntask : 1, 0);
-    {
-        std::vector<int> cur(inc_cnt.begin(), inc_cnt.end() - 1);
-        for (int t = 0; t < ntask; t++) P.h_inc_task[cur[key[t]]++] = t;
-    }
-    if (ensure((void**)&P.task, &P.task_bytes, sizeof(int) * 4 * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.inc_task, &P.inc_task_bytes, sizeof(int) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
+    if (overflow) { mel_set_error("neighbour lists still over capacity after 4 attempts"); return MEL_ERR_BOUNDS; }
+    if (ensure((void**)&P.task, &P.task_bytes, sizeof(int4) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
+    if (ensure((void**)&P.tns, &P.tns_bytes, sizeof(int) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
+    if (ensure((void**)&P.tslot, &P.tslot_bytes, sizeof(int) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
+    if (ensure((void**)&P.tkey, &P.tkey_bytes, sizeof(int) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
+    if (ensure((void**)&P.inc_task, &P.inc_task_bytes, sizeof(int) * 2 * (size_t)(ntask + 1))) return MEL_ERR_OOM;
+    int4* task = (int4*)P.task;
+    cudaMemsetAsync(P.tcnt, 0, sizeof(int) * (nb + 1), s);
+    if (ntask > 0)
+        task_fill_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, P.nbr, P.nbn, P.nbr_cap, P.btask0, P.bslot0, task, P.tns,
+                                                          P.tslot, P.tkey, P.tcnt);
     if (ensure((void**)&P.slot_cnt, &P.slot_bytes, sizeof(int) * (size_t)(nslot + 1))) return MEL_ERR_OOM;
     if (ensure((void**)&P.slot_off, &P.slot_off_bytes, sizeof(int) * (size_t)(nslot + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.inc_rng, &P.inc_rng_bytes, sizeof(int2) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    if (ntask > 0) {
-        cudaMemcpyAsync(P.task, T.data(), sizeof(int) * 4 * ntask, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(P.inc_task, P.h_inc_task.data(), sizeof(int) * ntask, cudaMemcpyHostToDevice, s);
-    }
-    cudaMemcpyAsync(P.b_inc0, inc_cnt.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice, s);
-    // 4. count, scan
-    if (ntask > 0) count_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, P.task, ntask, P.nbr, P.nbr_cap, P.slot_cnt);
+    // 3. count, scan, total
+    if (ntask > 0) count_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, task, ntask, P.nbr, P.nbr_cap, P.slot_cnt);
     mel_scan_exclusive(P.slot_cnt, P.slot_off, nslot, s);
     int total = 0;
     cudaMemcpyAsync(&total, P.slot_off + nslot, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return MEL_ERR_CUDA;
-    // 5. write the new list into the spare buffer, inheriting from the current one
+    // 4. write the new list into the spare buffer, inheriting from the current one
     if (ensure((void**)&P.cont_alt, &P.cont_alt_bytes, sizeof(mel_contact) * (size_t)(total + 1))) return MEL_ERR_OOM;
     if (ntask > 0)
-        write_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, P.task, ntask, P.nbr, P.nbr_cap, P.slot_off, P.cont_alt,
+        write_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, task, ntask, P.nbr, P.nbr_cap, P.slot_off, P.cont_alt,
                                                              d.cont, P.e_ptr, P.e_list, d.ncont > 0 ? 1 : 0);
-    // swap buffers
     mel_contact* old = d.cont;
     size_t old_bytes = P.cont_bytes;
     d.cont = P.cont_alt; P.cont_bytes = P.cont_alt_bytes;
@@ -494,10 +644,22 @@ int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cud
     if (ensure((void**)&P.cont_w, &P.cont_w_bytes, sizeof(double) * (size_t)(total + 1))) return MEL_ERR_OOM;
     cudaMemsetAsync(P.cont_w, 0, sizeof(double) * (total + 1), s);
     d.cont_w = P.cont_w;
-    // 6. index structures of the new list
-    if (ntask > 0) inc_range_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(P.inc_task, ntask, P.task, P.slot_off, d, P.inc_rng);
+    if (ensure((void**)&P.cont_rt, &P.cont_rt_bytes, 6 * sizeof(double) * (size_t)(total + 1))) return MEL_ERR_OOM;
+    d.cont_rt = P.cont_rt;
+    // 5. incoming ranges in send order
+    if (ensure((void**)&P.inc_rng, &P.inc_rng_bytes, sizeof(int2) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
+    mel_scan_exclusive(P.tcnt, P.b_inc0, nb, s);
+    if (ntask > 0) {
+        int* tmp = P.inc_task;
+        int* sorted = P.inc_task + ntask;
+        cudaMemcpyAsync(P.tcnt, P.b_inc0, sizeof(int) * nb, cudaMemcpyDeviceToDevice, s);
+        inc_fill_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(P.tkey, ntask, P.tcnt, tmp);
+        inc_sort_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(nb, P.b_inc0, tmp, sorted);
+        inc_range_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(sorted, ntask, P.tslot, P.tns, P.slot_off, P.inc_rng);
+    }
     d.inc_rng = P.inc_rng;
     d.b_inc0 = P.b_inc0;
+    // 6. per-entry index of the new list; vgapn/vgapt carry of new elements
     int rc = mel_index_contacts(d, P, s);
     d.b_cont0 = P.b_cont0;
     carry_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0);

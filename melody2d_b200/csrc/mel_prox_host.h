@@ -7,7 +7,12 @@ struct mel_prox_state {
     int nbr_cap = MEL_NBR_CAP_DEFAULT;
     int* nbr = nullptr; int* nbn = nullptr;
     double* aabb = nullptr; int* shmin = nullptr; int* shmax = nullptr;
-    int* task = nullptr; size_t task_bytes = 0;
+    void* task = nullptr; size_t task_bytes = 0;            // int4 per task
+    int* tns = nullptr; size_t tns_bytes = 0;               // slave border nodes per task
+    int* tslot = nullptr; size_t tslot_bytes = 0;           // first slot of each task
+    int* tkey = nullptr; size_t tkey_bytes = 0;             // master body of each task
+    int* tcnt = nullptr; int* btask0 = nullptr;             // per body: task count, first task
+    int* scnt = nullptr; int* bslot0 = nullptr;             // per body: slot count, first slot
     int* inc_task = nullptr; size_t inc_task_bytes = 0;
     int* slot_cnt = nullptr; size_t slot_bytes = 0;
     int* slot_off = nullptr; size_t slot_off_bytes = 0;
@@ -18,8 +23,8 @@ struct mel_prox_state {
     size_t cont_bytes = 0;
     mel_contact* cont_alt = nullptr; size_t cont_alt_bytes = 0;
     double* cont_w = nullptr; size_t cont_w_bytes = 0;
+    double* cont_rt = nullptr; size_t cont_rt_bytes = 0;
     int ntask = 0, nslot = 0;
-    std::vector<int> h_nbn, h_nbr, h_task, h_inc_task;
 };
 
 struct mel_prox_host {

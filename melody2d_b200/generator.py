@@ -797,9 +797,12 @@ def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax
     if not placed.all():
         raise RuntimeError("packing failed")
     E, nu, rho = 1e8, 0.3, 2500.0
-    mats = [("Grain", 0, [rho, 0.0, 0.0, E, nu, 1000.0]), ("Steel", 0, [7800.0, 0.0, 0.0, 2e11, 0.3, 500.0])]
+    rho_steel = 7800.0 * mass_factor        # mass scaling applies to the rigid plates and walls too
+    mats = [("Grain", 0, [rho, 0.0, 0.0, E, nu, 1000.0]), ("Steel", 0, [rho_steel, 0.0, 0.0, 2e11, 0.3, 500.0])]
+    # plates and walls overlap at the corners; a zero-stiffness law makes rigid-rigid contact inert
     laws = [("Grain", "Grain", 2, 0, [1e10, 1e9, mu_fric, 0.0, 0.0]),
-            ("Grain", "Steel", 2, 0, [1e10, 1e9, mu_fric, 0.0, 0.0])]
+            ("Grain", "Steel", 2, 0, [1e10, 1e9, mu_fric, 0.0, 0.0]),
+            ("Steel", "Steel", 0, 0, [0.0])]
     seeds = rng.integers(0, 2 ** 31 - 1, size=n_discs)
     jobs = [(int(seeds[i]), (float(centres[i, 0]), float(centres[i, 1])), float(radii[i]), n_border, n_interior,
              rho, mass_factor) for i in range(n_discs)]
@@ -807,17 +810,19 @@ def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax
     h_min = 2.0 * math.pi * rmin / n_border
     thick = 0.05 * H
     hist = lambda v: (np.array([0.0, T_HIST_END]), np.array([v, v]))
-    bot = make_rect_rigid(-0.05 * W, -thick, 1.05 * W, 0.0, 2.0 * h_min, 1, 7800.0,
+    # plates span the box and the walls' inward travel; walls span the plates' full height, so no
+    # grain can leave the sample through a corner
+    bot = make_rect_rigid(-0.1 * W, -thick, 1.1 * W, 0.0, 2.0 * h_min, 1, rho_steel,
                           (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(v_plate)), 0.5 * h_min, 0.5 * h_min)
-    top = make_rect_rigid(-0.05 * W, H, 1.05 * W, H + thick, 2.0 * h_min, 1, 7800.0,
+    top = make_rect_rigid(-0.1 * W, H, 1.1 * W, H + thick, 2.0 * h_min, 1, rho_steel,
                           (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(-v_plate)), 0.5 * h_min, 0.5 * h_min)
-    wall_h = 0.9 * H
-    y0 = 0.05 * H
+    wall_h = H + 2.0 * thick
+    y0 = -thick
     perim = 2.0 * (wall_h + thick)
-    p_eff = sigma * wall_h / perim          # oriented load per unit border length, total = sigma * wall height
-    left = make_rect_rigid(-thick, y0, 0.0, y0 + wall_h, 2.0 * h_min, 1, 7800.0,
+    p_eff = sigma * H / perim               # oriented load per unit border length, total = sigma * sample height
+    left = make_rect_rigid(-thick, y0, 0.0, y0 + wall_h, 2.0 * h_min, 1, rho_steel,
                            (BC_ORIENTED, (0.0, 0.0), hist(p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
-    right = make_rect_rigid(W, y0, W + thick, y0 + wall_h, 2.0 * h_min, 1, 7800.0,
+    right = make_rect_rigid(W, y0, W + thick, y0 + wall_h, 2.0 * h_min, 1, rho_steel,
                             (BC_ORIENTED, (0.0, 0.0), hist(-p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
     bodies += [bot, top, left, right]
     mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))

@@ -88,3 +88,26 @@ def test_proximity_from_uploaded_state(gpu_lib, oracle_built):
     g.update_proximity()
     o.update_proximity()
     assert_contacts_equal(g.contacts(), o.contacts())
+
+
+@pytest.mark.parametrize("seed", [5, 11])
+def test_biaxial_sample_identical(gpu_lib, oracle_built, seed):
+    """Small biaxial sample: long rigid plate and wall borders (segment-block pruning of the master
+    search), self contact, rigid-rigid pairs under the inert law, incoming ranges from many senders,
+    60 proximity updates."""
+    from melody2d_b200 import generator as gen
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    flat = gen.flatten(gen.biaxial_scene(seed=seed, n_discs=12, n_border=32, n_interior=80, workers=1))
+    g = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    assert_contacts_equal(g.contacts(), o.contacts())
+    for _ in range(12):
+        g.step(50)
+        o.step(50)
+        np.testing.assert_array_equal(g.node_state(), o.node_state())
+        assert_contacts_equal(g.contacts(), o.contacts())
+    np.testing.assert_array_equal(g.rigid()[0], o.rigid()[0])
+    np.testing.assert_array_equal(g.works(), o.works())
+    assert (g.contacts()["fx"] != 0).sum() > 0
+    g.close()
