@@ -1,0 +1,156 @@
+// Host builder of the chunk images (layout in mel_internal.h).  Points are cut into chunks in
+// index order; within a chunk they are stored row by row in groups of up to 32 slots sorted by
+// support count, and the pull records list, for every touched node, the positions of its entries
+// in ascending Gauss-point order (the order Body::Update_internal_forces accumulates them in,
+// Code/Body.h:960-1050).
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include "mel_chunks.h"
+
+void mel_set_error(const char* fmt, ...);
+
+namespace {
+
+// slots of a chunk whose points have supports ns[0..n): slot order and per-group row tables
+struct slot_plan {
+    std::vector<int> order;      // point offsets within the chunk, in slot order
+    std::vector<int> first_row;  // per slot: start of its group's row table in roff
+    std::vector<int> lane;       // per slot: lane within its group
+    std::vector<int> roff;       // row tables: entry offset of row k of a group
+    int entries = 0;
+};
+
+slot_plan plan_slots(const int* ns, int n)
+{
+    slot_plan P;
+    P.order.resize(n);
+    std::iota(P.order.begin(), P.order.end(), 0);
+    std::stable_sort(P.order.begin(), P.order.end(), [&](int a, int b) { return ns[a] > ns[b]; });
+    P.first_row.resize(n);
+    P.lane.resize(n);
+    for (int s0 = 0; s0 < n; s0 += 32) {
+        const int m = std::min(32, n - s0);
+        const int K = ns[P.order[s0]];
+        const int r0 = (int)P.roff.size();
+        for (int j = 0; j < m; j++) { P.first_row[s0 + j] = r0; P.lane[s0 + j] = j; }
+        for (int k = 0; k < K; k++) {
+            P.roff.push_back(P.entries);
+            int mk = 0;                             // slots with more than k supports: a prefix
+            while (mk < m && ns[P.order[s0 + mk]] > k) mk++;
+            P.entries += mk;
+        }
+    }
+    return P;
+}
+
+// rows of all row tables of points with supports ns[0..n)
+int table_rows(const int* ns, int n)
+{
+    int rows = 0;
+    std::vector<int> v(ns, ns + n);
+    std::sort(v.begin(), v.end(), std::greater<int>());
+    for (int s0 = 0; s0 < n; s0 += 32) rows += v[s0];
+    return rows;
+}
+
+}  // namespace
+
+mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out)
+{
+    const int nb = d->n_bodies;
+    out.chunks.clear();
+    out.img.clear();
+    out.b_chunk0.assign(nb + 1, 0);
+    out.img_max = 16;
+    out.n_entries = 0;
+    out.n_pad = 0;
+    std::vector<int> ns;
+    std::vector<std::pair<long long, int>> tp;   // (node << 32 | point, stored position)
+    for (int b = 0; b < nb; b++) {
+        out.b_chunk0[b] = (int)out.chunks.size();
+        if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+        const int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+        int g = d->body_gp_ptr[b];
+        const int g1 = d->body_gp_ptr[b + 1];
+        while (g < g1) {
+            // as many points as fit MEL_CHUNK_GP slots, ecap entries and the 10-bit row tables
+            int ngp = 0, nent = 0, nsmax = 0;
+            ns.clear();
+            while (g + ngp < g1 && ngp < MEL_CHUNK_GP) {
+                int c = d->gp_sup_ptr[g + ngp + 1] - d->gp_sup_ptr[g + ngp];
+                if (c > 255 || c <= 0) { mel_set_error("Gauss point %d has %d supports (1..255 supported)", g + ngp, c); return MEL_ERR_UNSUPPORTED; }
+                if (nent + c > ecap) break;
+                ns.push_back(c);
+                nsmax = std::max(nsmax, c);
+                // row tables are addressed with 10 bits; the exact count is needed only when the
+                // bound (groups x largest count) could exceed that
+                if (((ngp + 32) / 32) * nsmax > 1023 && table_rows(ns.data(), ngp + 1) > 1023) { ns.pop_back(); break; }
+                nent += c;
+                ngp++;
+            }
+            if (ngp == 0) { mel_set_error("Gauss point %d has more supports than a chunk holds", g); return MEL_ERR_UNSUPPORTED; }
+            const slot_plan P = plan_slots(ns.data(), ngp);
+            mel_chunk ch;
+            memset(&ch, 0, sizeof ch);
+            ch.gp0 = g;
+            ch.ngp = ngp;
+            ch.ne = (P.entries + 7) & ~7;
+            // stored position of every entry; pull order by (node, point index)
+            tp.clear();
+            for (int slot = 0; slot < ngp; slot++) {
+                const int t = P.order[slot];
+                const int gg = g + t;
+                for (int k = 0, j = d->gp_sup_ptr[gg]; j < d->gp_sup_ptr[gg + 1]; k++, j++) {
+                    int v = d->gp_sup_idx[j];
+                    if (v < 0 || v >= nnb) { mel_set_error("Gauss support index out of range"); return MEL_ERR_INVALID; }
+                    tp.push_back({ ((long long)v << 32) | (long long)t, P.roff[P.first_row[slot] + k] + P.lane[slot] });
+                }
+            }
+            std::sort(tp.begin(), tp.end());
+            std::vector<uint32_t> tn;
+            for (int q = 0; q < P.entries; q++)
+                if (q == 0 || (tp[q].first >> 32) != (tp[q - 1].first >> 32))
+                    tn.push_back((uint32_t)(tp[q].first >> 32) | ((uint32_t)q << 16));
+            ch.ntn = (int)tn.size();
+            tn.push_back(0xffffu | ((uint32_t)P.entries << 16));
+            const int nroff = (int)P.roff.size();
+            const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn, nroff);
+            ch.bytes = L.bytes;
+            ch.img = (long long)out.img.size();
+            out.img.resize(out.img.size() + L.bytes, 0);
+            uint8_t* I = out.img.data() + ch.img;
+            int hdr[4] = { ch.ngp, ch.ne, ch.ntn, nroff };
+            memcpy(I, hdr, sizeof hdr);
+            double* dN = reinterpret_cast<double*>(I + L.dN);
+            uint16_t* idx = reinterpret_cast<uint16_t*>(I + L.idx);
+            uint16_t* tpos = reinterpret_cast<uint16_t*>(I + L.tpos);
+            double* c0 = reinterpret_cast<double*>(I + L.c0);
+            uint32_t* gpm = reinterpret_cast<uint32_t*>(I + L.gpm);
+            uint32_t* tnr = reinterpret_cast<uint32_t*>(I + L.tn);
+            uint16_t* roff = reinterpret_cast<uint16_t*>(I + L.roff);
+            for (int slot = 0; slot < ngp; slot++) {
+                const int gg = g + P.order[slot];
+                const int c = d->gp_sup_ptr[gg + 1] - d->gp_sup_ptr[gg];
+                c0[slot] = d->gp_weight[gg] * d->gp_jacobian[gg];   // c0 of Code/Body.h:994
+                gpm[slot] = (uint32_t)P.first_row[slot] | ((uint32_t)P.lane[slot] << 10) | ((uint32_t)c << 15);
+                for (int k = 0, j = d->gp_sup_ptr[gg]; k < c; k++, j++) {
+                    int e = P.roff[P.first_row[slot] + k] + P.lane[slot];
+                    idx[e] = (uint16_t)d->gp_sup_idx[j];
+                    dN[2 * e] = d->gp_dNdx[j];
+                    dN[2 * e + 1] = d->gp_dNdy[j];
+                }
+            }
+            for (int q = 0; q < P.entries; q++) tpos[q] = (uint16_t)tp[q].second;
+            memcpy(tnr, tn.data(), sizeof(uint32_t) * tn.size());
+            for (int r = 0; r < nroff; r++) roff[r] = (uint16_t)P.roff[r];
+            out.img_max = std::max(out.img_max, ch.bytes);
+            out.n_entries += ch.ne;
+            out.n_pad += ch.ne - P.entries;
+            out.chunks.push_back(ch);
+            g += ngp;
+        }
+    }
+    out.b_chunk0[nb] = (int)out.chunks.size();
+    return MEL_OK;
+}

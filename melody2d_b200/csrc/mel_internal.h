@@ -26,14 +26,20 @@ enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3,
        MEL_E_NBR_NEED = 5, MEL_E_WAIT = 6, MEL_E_NWORDS = 8 };
 
 // Chunk image (all offsets in bytes from the image start, every section 16-byte aligned):
-//   header   int4 {ngp, ne, ntn, bytes}
-//   dN       ne x double2          (ne padded to a multiple of 8 with zero entries)
+//   header   int4 {ngp, ne, ntn, nroff}
+//   dN       ne x double2          dN/dx, dN/dy of every stored entry
 //   idx      ne x uint16           body-local support node of each entry
-//   tpos     ne x uint16           entry positions sorted by (node, position): the pull order
-//   c0       ngp2 x double         weight x jacobian (ngp2 = ngp rounded up to 2)
-//   gpm      ngp4 x uint32         first entry of the point | support count << 16
+//   tpos     ne x uint16           entry positions sorted by (node, Gauss point): the pull order
+//   c0       ngp2 x double         weight x jacobian of each point slot (ngp2 = ngp rounded to 2)
+//   gpm      ngp4 x uint32         point slot: row table start | lane << 10 | support count << 15
 //   tn       tn4 x uint32          touched node | first tpos << 16, ntn + 1 records (the last
 //                                  one closes the final range)
+//   roff     nroff8 x uint16       row tables of the slot groups
+// Point slots: the chunk's points sorted by (support count descending, index), cut into groups of
+// up to 32 slots, one warp each.  Row k of a group holds entry k of every slot whose point has
+// more than k supports; these slots are a prefix of the group, so entry k of lane j sits at
+// roff[r0 + k] + j and the lanes of a warp touch consecutive entries.  ne is the number of
+// entries rounded up to a multiple of 8 (zero entries at the end).
 struct mel_chunk {        // one chunk of a body's Gauss points
     long long img;        // byte offset of the image in mel_dev::img
     int bytes;            // image size (multiple of 16)
@@ -43,9 +49,9 @@ struct mel_chunk {        // one chunk of a body's Gauss points
 };
 
 struct mel_chunk_layout {  // section offsets of an image
-    int dN, idx, tpos, c0, gpm, tn, bytes;
+    int dN, idx, tpos, c0, gpm, tn, roff, bytes;
 };
-__host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, int ntn)
+__host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, int ntn, int nroff)
 {
     mel_chunk_layout L;
     L.dN = 16;
@@ -54,7 +60,8 @@ __host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, 
     L.c0 = L.tpos + 2 * ne;
     L.gpm = L.c0 + 8 * ((ngp + 1) & ~1);
     L.tn = L.gpm + 4 * ((ngp + 3) & ~3);
-    L.bytes = L.tn + 4 * ((ntn + 1 + 3) & ~3);
+    L.roff = L.tn + 4 * ((ntn + 1 + 3) & ~3);
+    L.bytes = L.roff + 2 * ((nroff + 7) & ~7);
     return L;
 }
 
@@ -119,8 +126,6 @@ void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);
 
 void mel_body_kernel_configure(size_t smem);
-// proximity (mel_prox.cu)
-void mel_scan_exclusive(const int* in, int* out, int n, cudaStream_t s);
 
 #define MEL_CUDA_OK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { mel_set_cuda_error(e_, #call, __FILE__, __LINE__); return MEL_ERR_CUDA; } } while (0)
 void mel_set_cuda_error(cudaError_t e, const char* what, const char* file, int line);

@@ -352,15 +352,18 @@ __device__ __forceinline__ double ordered_sum(double acc, const double* t, int n
 
 // Gauss-point pass of one chunk held in shared memory (Body::Update_internal_forces,
 // Code/Body.h:960-1050): thread `t` < ngp forms the strain of its point from the staged dN and
-// the body's displacements, applies the material and overwrites its dN pairs with the
-// contributions c0 * B^T.sigma.
+// the body's displacements (supports in the point's own order), applies the material and
+// overwrites its dN pairs with the contributions c0 * B^T.sigma.  Entry k of slot t sits at
+// row[k] + lane (row layout: the lanes of a warp touch consecutive entries).
 __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double Lam, const double2* s_up,
                                              double2* s_p, const uint16_t* s_idx, const double* s_c0,
-                                             const unsigned* s_gpm)
+                                             const unsigned* s_gpm, const uint16_t* s_roff)
 {
-    const unsigned m = s_gpm[t];
-    const int e = (int)(m & 0xffffu), ns = (int)(m >> 16);
+    const unsigned gm = s_gpm[t];
+    const uint16_t* row = s_roff + (gm & 0x3ffu);          // row table of the slot's group
+    const int lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
     const double c0 = s_c0[t];
+#define E(k) (row[(k)] + lane)
     if (mtype == MEL_MAT_ELASTIC_LINEAR) {
         // strain sums in support order; loads issued four supports ahead of the adds
         double E11 = 0., E12 = 0., E22 = 0.;
@@ -368,7 +371,7 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
         for (; k + 4 <= ns; k += 4) {
             double2 dN[4], u[4];
 #pragma unroll
-            for (int j = 0; j < 4; j++) { dN[j] = s_p[e + k + j]; u[j] = s_up[s_idx[e + k + j]]; }
+            for (int j = 0; j < 4; j++) { dN[j] = s_p[E(k + j)]; u[j] = s_up[s_idx[E(k + j)]]; }
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 E11 = E11 + dN[j].x * u[j].x;
@@ -377,8 +380,8 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
             }
         }
         for (; k < ns; k++) {
-            double2 dN = s_p[e + k];
-            double2 u = s_up[s_idx[e + k]];
+            double2 dN = s_p[E(k)];
+            double2 u = s_up[s_idx[E(k)]];
             E11 = E11 + dN.x * u.x;
             E12 = E12 + (dN.x * u.y + dN.y * u.x);
             E22 = E22 + dN.y * u.y;
@@ -390,17 +393,17 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
         double S11 = S33 + Mu2 * E11, S22 = S33 + Mu2 * E22, S12 = Mu2 * E12;
 #pragma unroll 4
         for (int k2 = 0; k2 < ns; k2++) {
-            double2 dN = s_p[e + k2];
+            double2 dN = s_p[E(k2)];
             double2 q;
             q.x = c0 * (dN.x * S11 + dN.y * S12);
             q.y = c0 * (dN.y * S22 + dN.x * S12);
-            s_p[e + k2] = q;
+            s_p[E(k2)] = q;
         }
     } else {
         double F11 = 1., F12 = 0., F21 = 0., F22 = 1.;
         for (int k = 0; k < ns; k++) {
-            double2 dN = s_p[e + k];
-            double2 u = s_up[s_idx[e + k]];
+            double2 dN = s_p[E(k)];
+            double2 u = s_up[s_idx[E(k)]];
             F11 += dN.x * u.x; F12 += dN.y * u.x; F21 += dN.x * u.y; F22 += dN.y * u.y;
         }
         double Kappa = Lam;                       // Apply_NeoHookean (Code/Model.h:52-73)
@@ -416,14 +419,15 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
         double S22 = (F11 * (F11 * s22 - F21 * s12) - F21 * (F11 * s12 - F21 * s11)) * invJ;
         double S12 = (F21 * (F12 * s12 - F22 * s11) - F11 * (F12 * s22 - F22 * s12)) * invJ;
         for (int k = 0; k < ns; k++) {
-            double2 dN = s_p[e + k];
+            double2 dN = s_p[E(k)];
             double2 q;
             q.x = c0 * (dN.x * (F11 * S11 + F12 * S12) + dN.y * (F12 * S22 + F11 * S12));
             q.y = c0 * (dN.x * (F21 * S11 + F22 * S12) + dN.y * (F22 * S22 + F21 * S12));
-            s_p[e + k] = q;
+            s_p[E(k)] = q;
         }
     }
 }
+#undef E
 
 // Shared memory of a deformable body (n nodes, staging buffers of img_cap bytes each):
 //   s_up, s_f, s_fc        3 x n double2       displacements, internal forces, contact forces
@@ -484,14 +488,14 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
             const bool ok = mbar_wait_bounded(&s_bar[sel], (unsigned)((k >> 1) & 1));
             if (!ok) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
             const int4 hdr = ok ? *reinterpret_cast<const int4*>(bk) : make_int4(0, 0, 0, 0);
-            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z);
+            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w);
             double2* s_p = reinterpret_cast<double2*>(bk + L.dN);
             const uint16_t* s_idx = reinterpret_cast<const uint16_t*>(bk + L.idx);
             const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
             const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
             if (tid < hdr.x)
                 chunk_points(tid, mtype, Mu, Lam, s_up, s_p, s_idx, reinterpret_cast<const double*>(bk + L.c0),
-                             reinterpret_cast<const unsigned*>(bk + L.gpm));
+                             reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
             compute_sync();
             if (*s_abort) break;
             // pull: each touched node subtracts its contributions in ascending Gauss-point order

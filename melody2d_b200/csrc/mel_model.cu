@@ -10,6 +10,7 @@
 #include <algorithm>
 #include "mel_internal.h"
 #include "mel_prox_host.h"
+#include "mel_chunks.h"
 #include "mel_host.h"   // .asc loader (mel_loader.cpp)
 
 // ---------------------------------------------------------------------------------------------
@@ -52,6 +53,7 @@ struct mel_handle {
     int nblocks_body = 0;
     int chunk_cap = 0;          // support entries per chunk chosen at build time
     double img_bytes = 0.;      // bytes of all chunk images
+    long long n_pad = 0;        // padding entries in the chunk images
     int launches = 0;
     double t_contact = 0., t_body = 0., t_prox = 0.;
     int timing = 0;
@@ -383,82 +385,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     int max_def_nodes = 1;
     for (int b = 0; b < nb; b++)
         if (d->body_type[b] == MEL_BODY_DEFORMABLE) max_def_nodes = std::max(max_def_nodes, d->body_node_ptr[b + 1] - d->body_node_ptr[b]);
-    std::vector<mel_chunk> chunks;
-    std::vector<int> b_chunk0(nb + 1, 0);
-    std::vector<uint8_t> img;
-    int img_max = 16;
-    size_t n_tn = 0;
-    auto build_chunks = [&](int ecap) -> mel_status {
-        chunks.clear(); img.clear(); img_max = 16; n_tn = 0;
-        std::vector<std::pair<int, int>> tp;
-        for (int b = 0; b < nb; b++) {
-            b_chunk0[b] = (int)chunks.size();
-            if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
-            int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
-            int g = d->body_gp_ptr[b], g1 = d->body_gp_ptr[b + 1];
-            while (g < g1) {
-                mel_chunk ch;
-                memset(&ch, 0, sizeof ch);
-                ch.gp0 = g;
-                int ne_c = 0, gend = g;
-                while (gend < g1 && gend - g < MEL_CHUNK_GP) {
-                    int ns = d->gp_sup_ptr[gend + 1] - d->gp_sup_ptr[gend];
-                    if (ns > 255 || ns <= 0) { mel_set_error("Gauss point %d has %d supports (1..255 supported)", gend, ns); return MEL_ERR_UNSUPPORTED; }
-                    if (ne_c + ns > ecap) break;
-                    ne_c += ns;
-                    gend++;
-                }
-                ch.ngp = gend - g;
-                ch.ne = (ne_c + 7) & ~7;
-                // pull order: entry positions sorted by (node, position)
-                tp.clear();
-                for (int q = 0, j = d->gp_sup_ptr[g]; q < ne_c; q++, j++) {
-                    int v = d->gp_sup_idx[j];
-                    if (v < 0 || v >= nnb) { mel_set_error("Gauss support index out of range"); return MEL_ERR_INVALID; }
-                    tp.push_back({ v, q });
-                }
-                std::sort(tp.begin(), tp.end());
-                std::vector<uint32_t> tn;
-                for (int q = 0; q < ne_c; q++)
-                    if (q == 0 || tp[q].first != tp[q - 1].first) tn.push_back((uint32_t)tp[q].first | ((uint32_t)q << 16));
-                ch.ntn = (int)tn.size();
-                tn.push_back(0xffffu | ((uint32_t)ne_c << 16));
-                n_tn += ch.ntn;
-                const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn);
-                ch.bytes = L.bytes;
-                ch.img = (long long)img.size();
-                img.resize(img.size() + L.bytes, 0);
-                uint8_t* I = img.data() + ch.img;
-                int hdr[4] = { ch.ngp, ch.ne, ch.ntn, ch.bytes };
-                memcpy(I, hdr, sizeof hdr);
-                double* dN = reinterpret_cast<double*>(I + L.dN);
-                uint16_t* idx = reinterpret_cast<uint16_t*>(I + L.idx);
-                uint16_t* tpos = reinterpret_cast<uint16_t*>(I + L.tpos);
-                double* c0 = reinterpret_cast<double*>(I + L.c0);
-                uint32_t* gpm = reinterpret_cast<uint32_t*>(I + L.gpm);
-                uint32_t* tnr = reinterpret_cast<uint32_t*>(I + L.tn);
-                int q = 0;
-                for (int gg = g; gg < gend; gg++) {
-                    int t = gg - g;
-                    int ns = d->gp_sup_ptr[gg + 1] - d->gp_sup_ptr[gg];
-                    c0[t] = d->gp_weight[gg] * d->gp_jacobian[gg];   // c0 of Code/Body.h:994
-                    gpm[t] = (uint32_t)q | ((uint32_t)ns << 16);
-                    for (int j = d->gp_sup_ptr[gg]; j < d->gp_sup_ptr[gg + 1]; j++, q++) {
-                        idx[q] = (uint16_t)d->gp_sup_idx[j];
-                        dN[2 * q] = d->gp_dNdx[j];
-                        dN[2 * q + 1] = d->gp_dNdy[j];
-                    }
-                }
-                for (int k = 0; k < ne_c; k++) tpos[k] = (uint16_t)tp[k].second;
-                memcpy(tnr, tn.data(), sizeof(uint32_t) * tn.size());
-                img_max = std::max(img_max, ch.bytes);
-                chunks.push_back(ch);
-                g = gend;
-            }
-        }
-        b_chunk0[nb] = (int)chunks.size();
-        return MEL_OK;
-    };
+    mel_chunk_set CS;
     int smem_sm = 0, smem_blk = 0, smem_res = 0;
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device);
     cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
@@ -468,16 +395,16 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         const int caps[] = { MEL_CHUNK_E_MAX, 1536, 1024, 768, 512, 256 };
         int chosen = -1;
         for (int ecap : caps) {
-            mel_status rc = build_chunks(ecap);
+            mel_status rc = mel_build_chunks(d, ecap, CS);
             if (rc) return rc;
-            size_t sm = mel_body_smem_bytes(max_def_nodes, img_max);
+            size_t sm = mel_body_smem_bytes(max_def_nodes, CS.img_max);
             if (sm <= two_per_sm) { chosen = ecap; break; }
         }
         if (chosen < 0) {   // one CTA per SM: largest cap that fits
             for (int ecap : caps) {
-                mel_status rc = build_chunks(ecap);
+                mel_status rc = mel_build_chunks(d, ecap, CS);
                 if (rc) return rc;
-                if (mel_body_smem_bytes(max_def_nodes, img_max) <= (size_t)smem_blk) { chosen = ecap; break; }
+                if (mel_body_smem_bytes(max_def_nodes, CS.img_max) <= (size_t)smem_blk) { chosen = ecap; break; }
             }
         }
         if (chosen < 0) {
@@ -486,14 +413,14 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         }
         h->chunk_cap = chosen;
     }
-    h->nge = 0;
-    for (const mel_chunk& c : chunks) h->nge += c.ne;
-    D.nchunk = (int)chunks.size();
-    D.chunk = dupload(h, chunks);
-    D.b_chunk0 = dupload(h, b_chunk0);
-    D.img = reinterpret_cast<const char*>(dupload(h, img));
-    D.img_cap = img_max;
-    h->img_bytes = (double)img.size();
+    h->nge = (int)CS.n_entries;
+    h->n_pad = CS.n_pad;
+    D.nchunk = (int)CS.chunks.size();
+    D.chunk = dupload(h, CS.chunks);
+    D.b_chunk0 = dupload(h, CS.b_chunk0);
+    D.img = reinterpret_cast<const char*>(dupload(h, CS.img));
+    D.img_cap = CS.img_max;
+    h->img_bytes = (double)CS.img.size();
     // contacts and proximity buffers
     D.err = dalloc<unsigned>(h, MEL_E_NWORDS);
     D.ncont = 0;
@@ -526,7 +453,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     if (cudaMalloc(&P.inc_rng, sizeof(int2) * 16) != cudaSuccess) return MEL_ERR_OOM;
     P.inc_rng_bytes = sizeof(int2) * 16;
     D.inc_rng = P.inc_rng;
-    h->body_smem = mel_body_smem_bytes(max_def_nodes, img_max);
+    h->body_smem = mel_body_smem_bytes(max_def_nodes, CS.img_max);
     mel_body_kernel_configure(h->body_smem);
     h->d_monitor = dalloc<double>(h, 32);
     h->d_monitor_part = dalloc<double>(h, 5 * 148);
@@ -537,8 +464,9 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         h->d_rigid_ids = dupload(h, rid);
     }
     // algorithmic bytes moved by one launch of each step kernel (exact array sizes):
-    // body kernel: the chunk images (entries: dN/dx,dN/dy + 16-bit index + 16-bit pull position;
-    // points: c0 + offset/count; touched-node records) and the chunk table; node state read (up,
+    // body kernel: the chunk images without their padding entries (entries: dN/dx,dN/dy + 16-bit
+    // index + 16-bit pull position; points: c0 + slot record; touched-node records; row tables)
+    // and the chunk table; node state read (up,
     // vp, m, 1/m, X0) and written (up, vp, ap, u, v, a, x); node supports (16-bit index + N) and
     // their offsets.  Contact records are left out (a few hundred bytes per body).
     {
@@ -549,7 +477,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         for (int b = 0; b < nb; b++)
             if (d->body_type[b] == MEL_BODY_DEFORMABLE)
                 nse_def += d->node_sup_ptr[d->body_node_ptr[b + 1]] - d->node_sup_ptr[d->body_node_ptr[b]];
-        h->bytes_body = h->img_bytes + (double)chunks.size() * sizeof(mel_chunk) + nd * (5 * 16 + 7 * 16) +
+        h->bytes_body = h->img_bytes - 20. * (double)h->n_pad + (double)CS.chunks.size() * sizeof(mel_chunk) + nd * (5 * 16 + 7 * 16) +
                         nse_def * (2 + 8) + (nd + 1) * 4;
         h->bytes_contact = (double)ne * (4 * 4 + 4 * 4 + 8 + 8);   // refreshed border lengths (contacts added per call)
     }
@@ -569,19 +497,15 @@ static mel_status check_errors(mel_handle* h)
     return MEL_OK;
 }
 
-static mel_status proximity(mel_handle* h)
+// One proximity update.  With e0/e1 given, they bracket it on the stream (read after the
+// caller's final synchronisation, so timing adds no host wait).
+static mel_status proximity(mel_handle* h, cudaEvent_t e0 = nullptr, cudaEvent_t e1 = nullptr)
 {
-    cudaEvent_t e0, e1;
-    if (h->timing) { cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventRecord(e0, h->stream); }
+    if (e0) cudaEventRecord(e0, h->stream);
+    int launches0 = h->P.launches;
     int rc = mel_run_proximity(h->d, h->P, h->H, h->stream);
-    if (h->timing) {
-        cudaEventRecord(e1, h->stream);
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        h->t_prox += ms;
-        cudaEventDestroy(e0); cudaEventDestroy(e1);
-    }
+    h->launches += h->P.launches - launches0;
+    if (e1) cudaEventRecord(e1, h->stream);
     if (rc) { if (rc == MEL_ERR_CUDA) mel_set_cuda_error(cudaGetLastError(), "proximity", __FILE__, __LINE__); return (mel_status)rc; }
     return MEL_OK;
 }
@@ -724,6 +648,7 @@ mel_status mel_destroy(mel_handle* h)
     for (void* p : h->allocs) cudaFree(p);
     mel_prox_state& P = h->P;
     for (void* p : { (void*)P.nbr, (void*)P.task, (void*)P.inc_task, (void*)P.slot_cnt, (void*)P.slot_off, (void*)P.inc_rng,
+                     (void*)P.scan_ws,
                      (void*)P.tns, (void*)P.tslot, (void*)P.tkey,
                      (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)P.cont_rt, (void*)h->d.cont })
         if (p) cudaFree(p);
@@ -741,8 +666,10 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
     h->t_contact = h->t_body = h->t_prox = h->t_total = 0.;
     h->launches = 0;
     int nprox = 0;
-    size_t need = h->timing ? (size_t)3 * io->nsteps : 0;
+    // timing events: three per step, two per proximity update (at most one per step)
+    size_t need = h->timing ? (size_t)5 * io->nsteps : 0;
     while (h->ev_pool.size() < need) { cudaEvent_t e; cudaEventCreate(&e); h->ev_pool.push_back(e); }
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pev;
     if (!h->ev_start) { cudaEventCreate(&h->ev_start); cudaEventCreate(&h->ev_end); }
     cudaEventRecord(h->ev_start, h->stream);
     size_t nev = 0;
@@ -760,10 +687,11 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
         h->time += h->dt;                       // Code/Solver.h:86
         if (io->run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
             h->next_cup = h->next_cup + h->cup;
-            mel_status rc = proximity(h);
+            cudaEvent_t p0 = nullptr, p1 = nullptr;
+            if (h->timing) { p0 = h->ev_pool[nev++]; p1 = h->ev_pool[nev++]; pev.push_back({ p0, p1 }); }
+            mel_status rc = proximity(h, p0, p1);
             if (rc) return rc;
             nprox++;
-            h->launches += 8;
         }
     }
     cudaEventRecord(h->ev_end, h->stream);
@@ -780,6 +708,11 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             cudaEventElapsedTime(&a, ev[k], ev[k + 1]);
             cudaEventElapsedTime(&b, ev[k + 1], ev[k + 2]);
             h->t_contact += a; h->t_body += b;
+        }
+        for (auto& pe : pev) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, pe.first, pe.second);
+            h->t_prox += ms;
         }
     }
     mel_status rc = check_errors(h);

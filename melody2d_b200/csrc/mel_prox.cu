@@ -48,22 +48,6 @@ __global__ void scan_add_kernel(int* out, int n, const int* block_off)
 
 } // namespace mel
 
-// out has n+1 entries: out[n] = total
-void mel_scan_exclusive(const int* in, int* out, int n, cudaStream_t s)
-{
-    int nblk = (n + SCAN_BLOCK) / SCAN_BLOCK;   // covers index n as well
-    int* sums = nullptr;
-    int* soff = nullptr;
-    cudaMallocAsync(&sums, sizeof(int) * (nblk + 1), s);
-    cudaMallocAsync(&soff, sizeof(int) * (nblk + 2), s);
-    mel::scan_block_kernel<<<nblk, SCAN_BLOCK, 0, s>>>(in, out, n, sums);
-    if (nblk > 1) mel_scan_exclusive(sums, soff, nblk, s);
-    else cudaMemsetAsync(soff, 0, sizeof(int), s);
-    mel::scan_add_kernel<<<nblk, SCAN_BLOCK, 0, s>>>(out, n + 1, soff);
-    cudaFreeAsync(sums, s);
-    cudaFreeAsync(soff, s);
-}
-
 namespace mel {
 
 // ---------------------------------------------------------------------------------------------
@@ -557,17 +541,52 @@ static int ensure_impl(void** p, size_t* cap_bytes, size_t need, const char* wha
 }
 #define ensure(p, cap, need) ensure_impl(p, cap, need, #p)
 
+// Exclusive scan of n ints into out[0..n] (out[n] = total): a block scan per 1024 entries, the
+// block totals scanned the same way, then the block offsets added.  Deterministic; the block
+// totals live in the state's persistent scratch (no allocation once it has grown).
+static size_t scan_scratch_ints(int n)
+{
+    size_t t = 0;
+    while (true) {
+        int nblk = (n + SCAN_BLOCK) / SCAN_BLOCK;
+        t += (size_t)nblk + 1 + nblk + 2;
+        if (nblk <= 1) break;
+        n = nblk;
+    }
+    return t;
+}
+
+static void scan_rec(const int* in, int* out, int n, int* ws, int& launches, cudaStream_t s)
+{
+    int nblk = (n + SCAN_BLOCK) / SCAN_BLOCK;     // covers index n as well
+    int* sums = ws;
+    int* soff = ws + nblk + 1;
+    mel::scan_block_kernel<<<nblk, SCAN_BLOCK, 0, s>>>(in, out, n, sums);
+    launches++;
+    if (nblk == 1) return;                        // one block: out[n] already holds the total
+    scan_rec(sums, soff, nblk, soff + nblk + 2, launches, s);
+    mel::scan_add_kernel<<<nblk, SCAN_BLOCK, 0, s>>>(out, n + 1, soff);
+    launches++;
+}
+
+int mel_scan_exclusive(const int* in, int* out, int n, mel_prox_state& P, cudaStream_t s)
+{
+    if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(n))) return MEL_ERR_OOM;
+    scan_rec(in, out, n, P.scan_ws, P.launches, s);
+    return MEL_OK;
+}
+
 // Rebuilds b_cont0 and the per-entry index of the current list (d.cont, d.ncont).
 int mel_index_contacts(mel_dev& d, mel_prox_state& P, cudaStream_t s)
 {
     using namespace mel;
-    body_range_kernel<<<(d.nb + 1 + 127) / 128, 128, 0, s>>>(d.cont, d.ncont, d.nb, P.b_cont0);
+    body_range_kernel<<<(d.nb + 1 + 127) / 128, 128, 0, s>>>(d.cont, d.ncont, d.nb, P.b_cont0); P.launches++;
     cudaMemsetAsync(P.e_cnt, 0, sizeof(int) * (d.ne + 1), s);
-    if (d.ncont > 0) entry_count_kernel<<<(d.ncont + 127) / 128, 128, 0, s>>>(d, d.cont, d.ncont, P.e_cnt);
-    mel_scan_exclusive(P.e_cnt, P.e_ptr, d.ne, s);
+    if (d.ncont > 0) { entry_count_kernel<<<(d.ncont + 127) / 128, 128, 0, s>>>(d, d.cont, d.ncont, P.e_cnt); P.launches++; }
+    if (mel_scan_exclusive(P.e_cnt, P.e_ptr, d.ne, P, s)) return MEL_ERR_OOM;
     if (ensure((void**)&P.e_list, &P.e_list_bytes, sizeof(int) * (size_t)(d.ncont + 1))) return MEL_ERR_OOM;
     cudaMemcpyAsync(P.e_cur, P.e_ptr, sizeof(int) * (d.ne + 1), cudaMemcpyDeviceToDevice, s);
-    entry_index_kernel<<<(d.nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0, P.e_cur, P.e_list);
+    entry_index_kernel<<<(d.nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0, P.e_cur, P.e_list); P.launches++;
     return cudaGetLastError() == cudaSuccess ? MEL_OK : MEL_ERR_CUDA;
 }
 
@@ -577,19 +596,19 @@ int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cud
     (void)H;
     const int nb = d.nb;
     // 1. border boxes and segment-block boxes
-    aabb_kernel<<<(d.nbd * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax);
-    if (d.nblk > 0) segblock_kernel<<<(d.nblk + 127) / 128, 128, 0, s>>>(d);
-    if (d.nsblk > 0) superblock_kernel<<<(d.nsblk + 127) / 128, 128, 0, s>>>(d);
+    aabb_kernel<<<(d.nbd * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax); P.launches++;
+    if (d.nblk > 0) { segblock_kernel<<<(d.nblk + 127) / 128, 128, 0, s>>>(d); P.launches++; }
+    if (d.nsblk > 0) { superblock_kernel<<<(d.nsblk + 127) / 128, 128, 0, s>>>(d); P.launches++; }
     // 2. neighbours and the task list; one read-back: overflow flag, task count, slot count
     int ntask = 0, nslot = 0;
     bool overflow = true;
     for (int attempt = 0; attempt < 4 && overflow; attempt++) {
         cudaMemsetAsync(d.err + MEL_E_NBR_OVERFLOW, 0, sizeof(unsigned), s);
         cudaMemsetAsync(d.err + MEL_E_NBR_NEED, 0, sizeof(unsigned), s);
-        neighbour_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax, P.nbr, P.nbn, P.nbr_cap);
-        task_count_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, P.nbn, P.tcnt, P.scnt);
-        mel_scan_exclusive(P.tcnt, P.btask0, nb, s);
-        mel_scan_exclusive(P.scnt, P.bslot0, nb, s);
+        neighbour_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax, P.nbr, P.nbn, P.nbr_cap); P.launches++;
+        task_count_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, P.nbn, P.tcnt, P.scnt); P.launches++;
+        if (mel_scan_exclusive(P.tcnt, P.btask0, nb, P, s)) return MEL_ERR_OOM;
+        if (mel_scan_exclusive(P.scnt, P.bslot0, nb, P, s)) return MEL_ERR_OOM;
         unsigned hv[MEL_E_NWORDS];
         cudaMemcpyAsync(hv, d.err, sizeof hv, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&ntask, P.btask0 + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -620,22 +639,26 @@ int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cud
     if (ensure((void**)&P.inc_task, &P.inc_task_bytes, sizeof(int) * 2 * (size_t)(ntask + 1))) return MEL_ERR_OOM;
     int4* task = (int4*)P.task;
     cudaMemsetAsync(P.tcnt, 0, sizeof(int) * (nb + 1), s);
-    if (ntask > 0)
+    if (ntask > 0) {
         task_fill_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, P.nbr, P.nbn, P.nbr_cap, P.btask0, P.bslot0, task, P.tns,
                                                           P.tslot, P.tkey, P.tcnt);
+        P.launches++;
+    }
     if (ensure((void**)&P.slot_cnt, &P.slot_bytes, sizeof(int) * (size_t)(nslot + 1))) return MEL_ERR_OOM;
     if (ensure((void**)&P.slot_off, &P.slot_off_bytes, sizeof(int) * (size_t)(nslot + 1))) return MEL_ERR_OOM;
     // 3. count, scan, total
-    if (ntask > 0) count_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, task, ntask, P.nbr, P.nbr_cap, P.slot_cnt);
-    mel_scan_exclusive(P.slot_cnt, P.slot_off, nslot, s);
+    if (ntask > 0) { count_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, task, ntask, P.nbr, P.nbr_cap, P.slot_cnt); P.launches++; }
+    if (mel_scan_exclusive(P.slot_cnt, P.slot_off, nslot, P, s)) return MEL_ERR_OOM;
     int total = 0;
     cudaMemcpyAsync(&total, P.slot_off + nslot, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return MEL_ERR_CUDA;
     // 4. write the new list into the spare buffer, inheriting from the current one
     if (ensure((void**)&P.cont_alt, &P.cont_alt_bytes, sizeof(mel_contact) * (size_t)(total + 1))) return MEL_ERR_OOM;
-    if (ntask > 0)
+    if (ntask > 0) {
         write_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, task, ntask, P.nbr, P.nbr_cap, P.slot_off, P.cont_alt,
                                                              d.cont, P.e_ptr, P.e_list, d.ncont > 0 ? 1 : 0);
+        P.launches++;
+    }
     mel_contact* old = d.cont;
     size_t old_bytes = P.cont_bytes;
     d.cont = P.cont_alt; P.cont_bytes = P.cont_alt_bytes;
@@ -648,21 +671,21 @@ int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cud
     d.cont_rt = P.cont_rt;
     // 5. incoming ranges in send order
     if (ensure((void**)&P.inc_rng, &P.inc_rng_bytes, sizeof(int2) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    mel_scan_exclusive(P.tcnt, P.b_inc0, nb, s);
+    if (mel_scan_exclusive(P.tcnt, P.b_inc0, nb, P, s)) return MEL_ERR_OOM;
     if (ntask > 0) {
         int* tmp = P.inc_task;
         int* sorted = P.inc_task + ntask;
         cudaMemcpyAsync(P.tcnt, P.b_inc0, sizeof(int) * nb, cudaMemcpyDeviceToDevice, s);
-        inc_fill_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(P.tkey, ntask, P.tcnt, tmp);
-        inc_sort_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(nb, P.b_inc0, tmp, sorted);
-        inc_range_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(sorted, ntask, P.tslot, P.tns, P.slot_off, P.inc_rng);
+        inc_fill_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(P.tkey, ntask, P.tcnt, tmp); P.launches++;
+        inc_sort_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(nb, P.b_inc0, tmp, sorted); P.launches++;
+        inc_range_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(sorted, ntask, P.tslot, P.tns, P.slot_off, P.inc_rng); P.launches++;
     }
     d.inc_rng = P.inc_rng;
     d.b_inc0 = P.b_inc0;
     // 6. per-entry index of the new list; vgapn/vgapt carry of new elements
     int rc = mel_index_contacts(d, P, s);
     d.b_cont0 = P.b_cont0;
-    carry_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0);
+    carry_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0); P.launches++;
     P.ntask = ntask; P.nslot = nslot;
     if (rc) return rc;
     return cudaGetLastError() == cudaSuccess ? MEL_OK : MEL_ERR_CUDA;

@@ -24,7 +24,9 @@ struct mel_prox_state {
     mel_contact* cont_alt = nullptr; size_t cont_alt_bytes = 0;
     double* cont_w = nullptr; size_t cont_w_bytes = 0;
     double* cont_rt = nullptr; size_t cont_rt_bytes = 0;
+    int* scan_ws = nullptr; size_t scan_ws_bytes = 0;    // scan block totals
     int ntask = 0, nslot = 0;
+    int launches = 0;                                      // kernels launched by the pipeline (running count)
 };
 
 struct mel_prox_host {
@@ -34,3 +36,4 @@ struct mel_prox_host {
 int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cudaStream_t s);
 int mel_index_contacts(mel_dev& d, mel_prox_state& P, cudaStream_t s);
 int mel_index_external(mel_dev& d, mel_prox_state& P, const mel_contact* host_list, int n, cudaStream_t s);
+int mel_scan_exclusive(const int* in, int* out, int n, mel_prox_state& P, cudaStream_t s);

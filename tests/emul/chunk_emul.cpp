@@ -1,0 +1,103 @@
+// CPU model of the body kernel's Gauss-point pass over the chunk images (test infrastructure).
+// It reads each image exactly as the kernel does (header, sections, slot records, row tables,
+// pull records), checks every index it follows against the image and body bounds, and returns
+// the internal nodal forces, so a test can compare them with the oracle bit for bit.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <utility>
+#include <vector>
+#include "mel_chunks.h"
+
+static char g_err[512];
+void mel_set_error(const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+extern "C" const char* emul_error() { return g_err; }
+
+// up: 2 doubles per node (displacements the pass reads); f: 2 doubles per node (output, rigid
+// nodes left at zero); stats: [chunks, stored entries, padding entries, largest image bytes].
+// Returns 0, or a positive code when an index read from an image is out of bounds.
+extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const double* up, double* f, long long* stats)
+{
+    mel_chunk_set CS;
+    if (mel_build_chunks(d, ecap, CS) != MEL_OK) return 100;
+    stats[0] = (long long)CS.chunks.size(); stats[1] = CS.n_entries; stats[2] = CS.n_pad; stats[3] = CS.img_max;
+    memset(f, 0, sizeof(double) * 2 * (size_t)d->n_nodes);
+    for (int b = 0; b < d->n_bodies; b++) {
+        if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+        const int n0 = d->body_node_ptr[b], n = d->body_node_ptr[b + 1] - n0;
+        const int mat = d->body_material[b];
+        const int mtype = d->material_type[mat];
+        const double Mu = d->material_params[MEL_MAT_NPARAM * mat + 3];
+        const double Lam = d->material_params[MEL_MAT_NPARAM * mat + 4];
+        std::vector<double> sf(2 * (size_t)n, 0.);
+        std::vector<uint8_t> buf;
+        for (int ci = CS.b_chunk0[b]; ci < CS.b_chunk0[b + 1]; ci++) {
+            const mel_chunk& c = CS.chunks[ci];
+            if (c.bytes % 16 || c.img % 16 || c.bytes > CS.img_max) return 1;
+            buf.assign(CS.img.begin() + c.img, CS.img.begin() + c.img + c.bytes);
+            int hdr[4];
+            memcpy(hdr, buf.data(), sizeof hdr);
+            if (hdr[0] > MEL_CHUNK_GP || hdr[1] % 8 || hdr[1] > ecap || hdr[3] > 1024) return 2;
+            const mel_chunk_layout L = mel_chunk_sections(hdr[0], hdr[1], hdr[2], hdr[3]);
+            if (L.bytes != c.bytes) return 3;
+            double* sp = reinterpret_cast<double*>(buf.data() + L.dN);
+            const uint16_t* sidx = reinterpret_cast<const uint16_t*>(buf.data() + L.idx);
+            const uint16_t* stpos = reinterpret_cast<const uint16_t*>(buf.data() + L.tpos);
+            const double* sc0 = reinterpret_cast<const double*>(buf.data() + L.c0);
+            const uint32_t* sgpm = reinterpret_cast<const uint32_t*>(buf.data() + L.gpm);
+            const uint32_t* stn = reinterpret_cast<const uint32_t*>(buf.data() + L.tn);
+            const uint16_t* sroff = reinterpret_cast<const uint16_t*>(buf.data() + L.roff);
+            const int ne = hdr[1];
+            for (int t = 0; t < hdr[0]; t++) {
+                const uint32_t gm = sgpm[t];
+                const int r0 = (int)(gm & 0x3ffu), lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
+                if (r0 + ns > hdr[3] || lane != t % 32) return 4;
+                auto E = [&](int k) { return (int)sroff[r0 + k] + lane; };
+                for (int k = 0; k < ns; k++) if (E(k) >= ne || sidx[E(k)] >= n) return 5;
+                const double c0 = sc0[t];
+                auto U = [&](int k) { int i = sidx[E(k)]; return std::make_pair(up[2 * (n0 + i)], up[2 * (n0 + i) + 1]); };
+                if (mtype != MEL_MAT_ELASTIC_LINEAR) return 6;   // this model covers the linear elastic pass
+                double E11 = 0., E12 = 0., E22 = 0.;
+                for (int k = 0; k < ns; k++) {
+                    double dx = sp[2 * E(k)], dy = sp[2 * E(k) + 1];
+                    auto u = U(k);
+                    E11 = E11 + dx * u.first;
+                    E12 = E12 + (dx * u.second + dy * u.first);
+                    E22 = E22 + dy * u.second;
+                }
+                E12 = 0.5 * E12;
+                double J = 1. + E11 + E22;
+                double S33 = Lam * (J - 1.);
+                double Mu2 = 2 * Mu;
+                double S11 = S33 + Mu2 * E11, S22 = S33 + Mu2 * E22, S12 = Mu2 * E12;
+                for (int k = 0; k < ns; k++) {
+                    double dx = sp[2 * E(k)], dy = sp[2 * E(k) + 1];
+                    sp[2 * E(k)] = c0 * (dx * S11 + dy * S12);
+                    sp[2 * E(k) + 1] = c0 * (dy * S22 + dx * S12);
+                }
+            }
+            for (int t = 0; t < hdr[2]; t++) {
+                const uint32_t r0 = stn[t], r1 = stn[t + 1];
+                const int node = (int)(r0 & 0xffffu);
+                if (node >= n || (r0 >> 16) > (r1 >> 16) || (int)(r1 >> 16) > ne) return 7;
+                double fx = sf[2 * node], fy = sf[2 * node + 1];
+                for (int q = (int)(r0 >> 16); q < (int)(r1 >> 16); q++) {
+                    if (stpos[q] >= ne) return 8;
+                    fx = fx - sp[2 * stpos[q]];
+                    fy = fy - sp[2 * stpos[q] + 1];
+                }
+                sf[2 * node] = fx; sf[2 * node + 1] = fy;
+            }
+        }
+        for (int i = 0; i < 2 * n; i++) f[2 * n0 + i] = sf[i];
+    }
+    return 0;
+}

@@ -1,0 +1,48 @@
+"""Chunk images (the body kernel's Gauss-point input) checked on the CPU: a model of the kernel's
+Gauss-point pass (tests/emul/chunk_emul.cpp, same image parsing and index arithmetic as the CUDA
+code, every followed index bounds-checked) must reproduce the oracle's internal forces bit for
+bit, at every chunk size the build may choose."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, flat_of, squeezed_lattice
+
+
+@pytest.fixture(scope="module")
+def emul(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("emul") / "libchunkemul.so")
+    csrc = os.path.join(ROOT, "melody2d_b200", "csrc")
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-I" + csrc,
+           "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "emul", "chunk_emul.cpp"), os.path.join(csrc, "mel_chunks.cpp"), "-o", out]
+    subprocess.run(cmd, check=True)
+    L = C.CDLL(out)
+    L.emul_internal_forces.restype = C.c_int
+    L.emul_internal_forces.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.emul_error.restype = C.c_char_p
+    return L
+
+
+@pytest.mark.parametrize("ecap", [2048, 1024, 256])
+def test_chunk_pass_matches_oracle(emul, oracle_built, ecap):
+    from melody2d_b200.abi import Desc
+    from oracle.pyoracle import Oracle
+    flat = flat_of(squeezed_lattice(3, 3))
+    o = Oracle(flat)
+    o.step(30)
+    up = np.ascontiguousarray(o.node_state()[:, 6:8]).copy()   # displacements the next pass reads
+    o.step(1)
+    ref = o.forces()["internal"]
+    desc = Desc(flat)
+    f = np.zeros_like(up)
+    stats = np.zeros(4, dtype=np.int64)
+    rc = emul.emul_internal_forces(C.byref(desc.desc), ecap, up.ctypes.data, f.ctypes.data, stats.ctypes.data)
+    assert rc == 0, (rc, emul.emul_error())
+    assert stats[0] > 0 and stats[3] % 16 == 0
+    assert stats[2] < 8 * stats[0], "only the rounding of each chunk to 8 entries pads"
+    np.testing.assert_array_equal(f, ref)
+    assert np.abs(ref).max() > 0
