@@ -187,8 +187,8 @@ typedef struct mel_monitor {
 typedef struct mel_options {
     int precision;          /* MEL_PREC_* */
     int device;             /* CUDA device ordinal */
-    int use_graph;          /* capture the per-step launches in a CUDA graph */
-    int max_contacts;       /* capacity hint (0 = automatic) */
+    int use_graph;          /* reserved, must be 0 */
+    int max_contacts;       /* reserved, must be 0 (contact storage grows as needed) */
 } mel_options;
 
 typedef struct mel_handle mel_handle;

@@ -594,6 +594,8 @@ static mel_status create_impl(const mel_model_desc* desc, const mel_options* opt
     *out = nullptr;
     mel_status rc = validate(desc);
     if (rc) return rc;
+    if (opt && (opt->use_graph != 0 || opt->max_contacts != 0)) { mel_set_error("mel_options: use_graph and max_contacts are reserved and must be 0"); return MEL_ERR_INVALID; }
+    if (opt && opt->precision != MEL_PREC_FP64 && opt->precision != MEL_PREC_MIXED) { mel_set_error("mel_options: unknown precision %d", opt->precision); return MEL_ERR_INVALID; }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { mel_set_error("no CUDA device"); return MEL_ERR_NO_DEVICE; }
     mel_handle* h = new mel_handle();
