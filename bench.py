@@ -186,7 +186,8 @@ def run_ours(args, rank, world, local, pg):
     flat = g.flatten(scene)
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
-    s = Solver.from_flat(flat, precision=0, device=local)
+    precision = 1 if args.precision == "mixed" else 0
+    s = Solver.from_flat(flat, precision=precision, device=local)
     t_create = time.perf_counter() - t0
     model_bytes = sum(np.asarray(v).nbytes for k, v in flat.items() if k != "material_names")
     nodes = s.step_stats()["n_deformable_nodes"]
@@ -211,8 +212,8 @@ def run_ours(args, rank, world, local, pg):
     prof = os.path.join(ROOT, "profiles", "body_kernel_traffic.json")
     if os.path.exists(prof):
         try:
-            pj = json.load(open(prof))
-            traffic = pj["dram_bytes_per_gauss_point"] * s.sizes()["n_gauss"]
+            per_gp = json.load(open(prof))["dram_bytes_per_gauss_point"].get(args.precision)
+            traffic = per_gp * s.sizes()["n_gauss"] if per_gp else None
         except Exception:
             traffic = None
     # end to end through the C ABI: every iteration steps and reads the monitored quantities back
@@ -237,12 +238,13 @@ def run_ours(args, rank, world, local, pg):
         line = {
             "metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded biaxial packing generator)",
+            "vs_baseline": None, "dtype": "f64" if precision == 0 else "f32 (dN, strain, stress, contributions) + f64",
+            "data": "synthetic (seeded biaxial packing generator)",
             "config": {"workload": f"biaxial: {args.discs} deformable discs, radii U[0.5,1.5] mm, 64 border + 340 "
                                    f"interior nodes each, MLS (linear, W1), ElasticLinear, MohrCoulomb, mass x100, "
                                    f"plates 0.05 m/s, walls 100 kPa; Euler, dt=0.5 dt_crit; proximity every 10 steps",
                        "nodes_per_gpu": nodes, "gauss_points": sizes["n_gauss"], "gp_entries": sizes["n_gp_entries"],
-                       "contacts": st["n_contacts"], "precision": "fp64",
+                       "contacts": st["n_contacts"], "precision": args.precision,
                        "l2": "inputs larger than L2 (%.2f GB streamed per step)" % ((st["bytes_body"] + st["bytes_contact"]) / 1e9),
                        "generate_s": round(t_gen, 2), "create_s": round(t_create, 2)},
             "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": 0,
@@ -265,6 +267,42 @@ def run_ours(args, rank, world, local, pg):
     s.close()
 
 
+def compare_precisions(args, rank, world, local, pg):
+    """Config-2 report: the mixed form against the FP64 path (bit-identical to the FP64 oracle) on
+    the same generated sample after K steps: relative errors of kinetic energy, wall reaction
+    (contact force and driven-DOF reaction of the rigid plates and walls), mass-weighted mean
+    displacement, and the two active-contact counts."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Solver
+    if rank != 0:
+        return
+    scene = g.biaxial_scene(seed=1, n_discs=args.discs, workers=host_threads())
+    flat = g.flatten(scene)
+    a = Solver.from_flat(flat, precision=0, device=local)
+    b = Solver.from_flat(flat, precision=1, device=local)
+
+    def rel(x, y):
+        x, y = np.asarray(x, float), np.asarray(y, float)
+        return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    checkpoints = sorted({k for k in (1000, 5000, 10000, 20000, 50000) if k < args.compare_fp64} | {args.compare_fp64})
+    rows, done = [], 0
+    for k in checkpoints:
+        a.step(k - done)
+        b.step(k - done)
+        done = k
+        ma, mb = a.monitor(), b.monitor()
+        rows.append({"steps": k,
+                     "kinetic_energy": rel(mb.kinetic_energy, ma.kinetic_energy),
+                     "wall_contact_force": rel(list(mb.rigid_force), list(ma.rigid_force)),
+                     "wall_reaction": rel(list(mb.rigid_dirichlet), list(ma.rigid_dirichlet)),
+                     "mean_displacement": rel(list(mb.mean_displacement), list(ma.mean_displacement)),
+                     "active_contacts": [mb.active_contacts, ma.active_contacts]})
+    print(json.dumps({"report": "mixed vs fp64 (relative errors; active_contacts = [mixed, fp64])",
+                      "workload": f"biaxial {args.discs} discs", "rows": rows}), flush=True)
+    a.close()
+    b.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -277,12 +315,19 @@ def main():
     ap.add_argument("--ref-discs", type=int, default=400)
     ap.add_argument("--ref-steps", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # fp64: the drop-in path, bit-identical to the oracle; mixed: FP32 shape-function derivatives,
+    # strain and stress with FP64 positions, velocities, contact geometry and force sums
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--compare-fp64", type=int, default=0, metavar="K",
+                    help="instead of timing, report the mixed form's errors against FP64 after K steps")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.compare_fp64 > 0:
+            compare_precisions(args, rank, world, local, pg)
+        elif args.impl == "reference":
             run_reference(args, rank, world, pg)
         else:
             run_ours(args, rank, world, local, pg)

@@ -56,7 +56,7 @@ int table_rows(const int* ns, int n)
 
 }  // namespace
 
-mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out)
+mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out, bool mixed)
 {
     const int nb = d->n_bodies;
     out.chunks.clear();
@@ -115,7 +115,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
             ch.ntn = (int)tn.size();
             tn.push_back(0xffffu | ((uint32_t)P.entries << 16));
             const int nroff = (int)P.roff.size();
-            const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn, nroff);
+            const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn, nroff, mixed ? 8 : 16);
             ch.bytes = L.bytes;
             ch.img = (long long)out.img.size();
             out.img.resize(out.img.size() + L.bytes, 0);
@@ -123,6 +123,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
             int hdr[4] = { ch.ngp, ch.ne, ch.ntn, nroff };
             memcpy(I, hdr, sizeof hdr);
             double* dN = reinterpret_cast<double*>(I + L.dN);
+            float* dNf = reinterpret_cast<float*>(I + L.dN);
             uint16_t* idx = reinterpret_cast<uint16_t*>(I + L.idx);
             uint16_t* tpos = reinterpret_cast<uint16_t*>(I + L.tpos);
             double* c0 = reinterpret_cast<double*>(I + L.c0);
@@ -137,8 +138,8 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 for (int k = 0, j = d->gp_sup_ptr[gg]; k < c; k++, j++) {
                     int e = P.roff[P.first_row[slot] + k] + P.lane[slot];
                     idx[e] = (uint16_t)d->gp_sup_idx[j];
-                    dN[2 * e] = d->gp_dNdx[j];
-                    dN[2 * e + 1] = d->gp_dNdy[j];
+                    if (mixed) { dNf[2 * e] = (float)d->gp_dNdx[j]; dNf[2 * e + 1] = (float)d->gp_dNdy[j]; }
+                    else { dN[2 * e] = d->gp_dNdx[j]; dN[2 * e + 1] = d->gp_dNdy[j]; }
                 }
             }
             for (int q = 0; q < P.entries; q++) tpos[q] = (uint16_t)tp[q].second;

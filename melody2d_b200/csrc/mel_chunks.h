@@ -15,4 +15,5 @@ struct mel_chunk_set {
 
 // Cuts every deformable body's Gauss points into chunks of at most MEL_CHUNK_GP points and
 // at most `ecap` entries.  Returns MEL_OK or an error code with the message set.
-mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out);
+// mixed: dN pairs stored as FP32 (the mixed-precision pass) instead of FP64.
+mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out, bool mixed = false);

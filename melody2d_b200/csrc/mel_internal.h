@@ -27,7 +27,8 @@ enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3,
 
 // Chunk image (all offsets in bytes from the image start, every section 16-byte aligned):
 //   header   int4 {ngp, ne, ntn, nroff}
-//   dN       ne x double2          dN/dx, dN/dy of every stored entry
+//   dN       ne x double2          dN/dx, dN/dy of every stored entry (float2 in the images of
+//                                  the mixed-precision pass)
 //   idx      ne x uint16           body-local support node of each entry
 //   tpos     ne x uint16           entry positions sorted by (node, Gauss point): the pull order
 //   c0       ngp2 x double         weight x jacobian of each point slot (ngp2 = ngp rounded to 2)
@@ -51,11 +52,12 @@ struct mel_chunk {        // one chunk of a body's Gauss points
 struct mel_chunk_layout {  // section offsets of an image
     int dN, idx, tpos, c0, gpm, tn, roff, bytes;
 };
-__host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, int ntn, int nroff)
+// dnb: bytes of one dN pair, 16 (FP64 images) or 8 (FP32 images of the mixed-precision pass)
+__host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, int ntn, int nroff, int dnb)
 {
     mel_chunk_layout L;
     L.dN = 16;
-    L.idx = L.dN + 16 * ne;
+    L.idx = L.dN + dnb * ne;
     L.tpos = L.idx + 2 * ne;
     L.c0 = L.tpos + 2 * ne;
     L.gpm = L.c0 + 8 * ((ngp + 1) & ~1);
@@ -121,11 +123,11 @@ struct mel_dev {
 // kernel launch wrappers (mel_kernels.cu)
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s);
-size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes);
+size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed);
 void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);
 
-void mel_body_kernel_configure(size_t smem);
+int mel_body_kernel_configure(size_t smem);
 
 #define MEL_CUDA_OK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { mel_set_cuda_error(e_, #call, __FILE__, __LINE__); return MEL_ERR_CUDA; } } while (0)
 void mel_set_cuda_error(cudaError_t e, const char* what, const char* file, int line);

@@ -14,6 +14,7 @@
 // the FP64 path reproduces the reference's values exactly; this file is compiled with
 // -fmad=false.
 #include <cstdio>
+#include <mutex>
 #include "mel_internal.h"
 #include "mel_geometry.cuh"
 
@@ -429,12 +430,79 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
 }
 #undef E
 
+// Gauss-point pass of the mixed-precision form: dN pairs stored in FP32, strain, stress and the
+// contributions computed in FP32 (with fused multiply-adds), displacements gathered in FP32 as
+// differences to the body's first node (taken in FP64: sum_j dN_j = 0, so the body's rigid
+// translation cancels exactly and does not eat the FP32 mantissa).  Nodal force sums stay FP64.
+__device__ __forceinline__ void chunk_points_mx(int t, int mtype, float Mu, float Lam, const float2* s_upf,
+                                                float2* s_p, const uint16_t* s_idx, const double* s_c0,
+                                                const unsigned* s_gpm, const uint16_t* s_roff)
+{
+    const unsigned gm = s_gpm[t];
+    const uint16_t* row = s_roff + (gm & 0x3ffu);
+    const int lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
+    const float c0 = (float)s_c0[t];
+    if (mtype == MEL_MAT_ELASTIC_LINEAR) {
+        float E11 = 0.f, E12 = 0.f, E22 = 0.f;
+#pragma unroll 4
+        for (int k = 0; k < ns; k++) {
+            const int e = row[k] + lane;
+            const float2 dN = s_p[e];
+            const float2 u = s_upf[s_idx[e]];
+            E11 = __fmaf_rn(dN.x, u.x, E11);
+            E12 = __fmaf_rn(dN.x, u.y, __fmaf_rn(dN.y, u.x, E12));
+            E22 = __fmaf_rn(dN.y, u.y, E22);
+        }
+        E12 = 0.5f * E12;
+        const float S33 = Lam * (E11 + E22);      // Apply_Elastic_Linear (Code/Model.h:19-29), J - 1 = tr E
+        const float Mu2 = 2.f * Mu;
+        const float S11 = __fmaf_rn(Mu2, E11, S33), S22 = __fmaf_rn(Mu2, E22, S33), S12 = Mu2 * E12;
+#pragma unroll 4
+        for (int k = 0; k < ns; k++) {
+            const int e = row[k] + lane;
+            const float2 dN = s_p[e];
+            s_p[e] = make_float2(c0 * __fmaf_rn(dN.x, S11, dN.y * S12), c0 * __fmaf_rn(dN.y, S22, dN.x * S12));
+        }
+    } else {
+        float G11 = 0.f, G12 = 0.f, G21 = 0.f, G22 = 0.f;   // F - I
+        for (int k = 0; k < ns; k++) {
+            const int e = row[k] + lane;
+            const float2 dN = s_p[e];
+            const float2 u = s_upf[s_idx[e]];
+            G11 = __fmaf_rn(dN.x, u.x, G11); G12 = __fmaf_rn(dN.y, u.x, G12);
+            G21 = __fmaf_rn(dN.x, u.y, G21); G22 = __fmaf_rn(dN.y, u.y, G22);
+        }
+        const float F11 = 1.f + G11, F12 = G12, F21 = G21, F22 = 1.f + G22;
+        const float Kappa = Lam;                   // Apply_NeoHookean (Code/Model.h:52-73)
+        const float F11F12 = F11 * F11 + F12 * F12, F21F22 = F21 * F21 + F22 * F22;
+        const float Jm1 = G11 + G22 + (G11 * G22 - G12 * G21);   // J - 1 without cancellation
+        const float J = 1.f + Jm1;
+        const float invJ = 1.f / J;
+        const float K = Kappa * Jm1;
+        const float MuJ53 = Mu * powf(J, -1.666666667f);
+        const float trB = 0.333333333f * (F11F12 + F21F22 + 1.f);
+        const float s11 = K + MuJ53 * (F11F12 - trB), s22 = K + MuJ53 * (F21F22 - trB);
+        const float s12 = MuJ53 * (F11 * F21 + F12 * F22);
+        const float S11 = (F12 * (F12 * s22 - F22 * s12) - F22 * (F12 * s12 - F22 * s11)) * invJ;
+        const float S22 = (F11 * (F11 * s22 - F21 * s12) - F21 * (F11 * s12 - F21 * s11)) * invJ;
+        const float S12 = (F21 * (F12 * s12 - F22 * s11) - F11 * (F12 * s22 - F22 * s12)) * invJ;
+        for (int k = 0; k < ns; k++) {
+            const int e = row[k] + lane;
+            const float2 dN = s_p[e];
+            s_p[e] = make_float2(c0 * (dN.x * (F11 * S11 + F12 * S12) + dN.y * (F12 * S22 + F11 * S12)),
+                                 c0 * (dN.x * (F21 * S11 + F22 * S12) + dN.y * (F22 * S22 + F21 * S12)));
+        }
+    }
+}
+
 // Shared memory of a deformable body (n nodes, staging buffers of img_cap bytes each):
 //   s_up, s_f, s_fc        3 x n double2       displacements, internal forces, contact forces
+//   s_upf (mixed only)     n2 x float2         displacements relative to node 0 (n2 = n rounded to 2)
 //   2 mbarriers + abort flag                   32 bytes
 //   region                 max(2 img_cap, 112 n) bytes: two chunk images during the Gauss-point
 //                          pass, then s_fn, s_fd, s_vp, s_ap (n double2 each) and the six work
 //                          terms per node (6 x n double)
+template <bool MX>
 __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
 {
     const int tid = threadIdx.x;
@@ -446,7 +514,9 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
     double2* s_up = reinterpret_cast<double2*>(smem);
     double2* s_f = s_up + n;
     double2* s_fc = s_f + n;
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_fc + n);
+    float2* s_upf = reinterpret_cast<float2*>(s_fc + n);
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
+                                                     : reinterpret_cast<char*>(s_fc + n));
     volatile int* s_abort = reinterpret_cast<volatile int*>(s_bar + 2);
     char* region = reinterpret_cast<char*>(s_bar + 4);
     char* const buf0 = region;
@@ -457,6 +527,13 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
         s_up[i] = d.up[n0 + i];
         s_f[i] = make_double2(0., 0.);
         s_fc[i] = make_double2(0., 0.);
+    }
+    if (MX) {
+        const double2 u0 = d.up[n0];
+        for (int i = tid; i < n; i += blockDim.x) {
+            const double2 u = d.up[n0 + i];
+            s_upf[i] = make_float2((float)(u.x - u0.x), (float)(u.y - u0.y));
+        }
     }
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
@@ -488,34 +565,51 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
             const bool ok = mbar_wait_bounded(&s_bar[sel], (unsigned)((k >> 1) & 1));
             if (!ok) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
             const int4 hdr = ok ? *reinterpret_cast<const int4*>(bk) : make_int4(0, 0, 0, 0);
-            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w);
-            double2* s_p = reinterpret_cast<double2*>(bk + L.dN);
+            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
             const uint16_t* s_idx = reinterpret_cast<const uint16_t*>(bk + L.idx);
             const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
             const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
-            if (tid < hdr.x)
-                chunk_points(tid, mtype, Mu, Lam, s_up, s_p, s_idx, reinterpret_cast<const double*>(bk + L.c0),
-                             reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
+            if (tid < hdr.x) {
+                if (MX)
+                    chunk_points_mx(tid, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN), s_idx,
+                                    reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
+                                    reinterpret_cast<const uint16_t*>(bk + L.roff));
+                else
+                    chunk_points(tid, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN), s_idx,
+                                 reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
+                                 reinterpret_cast<const uint16_t*>(bk + L.roff));
+            }
             compute_sync();
             if (*s_abort) break;
             // pull: each touched node subtracts its contributions in ascending Gauss-point order
+            // (the mixed form adds its FP32 contributions in FP64)
             for (int t = tid; t < hdr.z; t += MEL_BODY_CTHREADS) {
                 const unsigned r0 = s_tn[t], r1 = s_tn[t + 1];
                 const int node = (int)(r0 & 0xffffu);
                 const int q1 = (int)(r1 >> 16);
                 double2 f = s_f[node];
                 int q = (int)(r0 >> 16);
-                for (; q + 4 <= q1; q += 4) {
-                    double2 c[4];
+                if (MX) {
+                    const float2* s_q = reinterpret_cast<const float2*>(bk + L.dN);
+                    for (; q < q1; q++) {
+                        const float2 c = s_q[s_tpos[q]];
+                        f.x = f.x - (double)c.x;
+                        f.y = f.y - (double)c.y;
+                    }
+                } else {
+                    const double2* s_p = reinterpret_cast<const double2*>(bk + L.dN);
+                    for (; q + 4 <= q1; q += 4) {
+                        double2 c[4];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) c[j] = s_p[s_tpos[q + j]];
+                        for (int j = 0; j < 4; j++) c[j] = s_p[s_tpos[q + j]];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) { f.x = f.x - c[j].x; f.y = f.y - c[j].y; }
-                }
-                for (; q < q1; q++) {
-                    double2 c = s_p[s_tpos[q]];
-                    f.x = f.x - c.x;
-                    f.y = f.y - c.y;
+                        for (int j = 0; j < 4; j++) { f.x = f.x - c[j].x; f.y = f.y - c[j].y; }
+                    }
+                    for (; q < q1; q++) {
+                        double2 c = s_p[s_tpos[q]];
+                        f.x = f.x - c.x;
+                        f.y = f.y - c.y;
+                    }
                 }
                 s_f[node] = f;
             }
@@ -868,6 +962,7 @@ __device__ void contact_work(const mel_dev& d, int b)
     d.works[7 * b + 1] = w;
 }
 
+template <bool MX>
 __global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel(mel_dev d, int parity)
 {
     extern __shared__ __align__(16) char smem[];
@@ -875,7 +970,7 @@ __global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel(mel_dev d, in
     if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
     if (d.any_damped && threadIdx.x == 32) contact_work(d, b);
     if (d.b_type[b] == MEL_BODY_RIGID) rigid_body(d, b, parity, smem);
-    else deformable_body(d, b, parity, smem);
+    else deformable_body<MX>(d, b, parity, smem);
     if (blockIdx.x == 0 && threadIdx.x == 0) d.time2[parity ^ 1] = d.time2[parity] + d.dt[0];
 }
 
@@ -931,9 +1026,10 @@ void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s)
     mel::contact_kernel<<<(total + 127) / 128, 128, 0, s>>>(d, law_dt_scale);
 }
 
-size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes)
+size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)
 {
     size_t base = 3 * sizeof(double2) * (size_t)max_nodes + 32;
+    if (mixed) base += sizeof(float2) * (size_t)((max_nodes + 1) & ~1);
     size_t stage = 2 * (size_t)max_image_bytes;
     size_t post = (4 * sizeof(double2) + 6 * sizeof(double)) * (size_t)max_nodes;
     size_t rigid = (64 + 6 * MEL_RIGID_BATCH) * sizeof(double);
@@ -943,7 +1039,8 @@ size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes)
 
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s)
 {
-    mel::body_kernel<<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
+    if (d.precision == MEL_PREC_MIXED) mel::body_kernel<true><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
+    else mel::body_kernel<false><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
 }
 
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s)
@@ -952,7 +1049,21 @@ void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, in
     mel::monitor_final_kernel<<<1, 32, 0, s>>>(d, part, rigid_ids, nrigid, out);
 }
 
-void mel_body_kernel_configure(size_t smem)
+// The attribute is per kernel and device, shared by every handle of the process: it is only ever
+// raised (to the largest size any handle needs), never lowered under another handle's launches.
+int mel_body_kernel_configure(size_t smem)
 {
-    cudaFuncSetAttribute(mel::body_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static std::mutex mu;
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MEL_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    if (smem <= configured[dev]) return MEL_OK;
+    if (cudaFuncSetAttribute(mel::body_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        mel_set_cuda_error(cudaGetLastError(), "cudaFuncSetAttribute(body_kernel)", __FILE__, __LINE__);
+        return MEL_ERR_CUDA;
+    }
+    configured[dev] = smem;
+    return MEL_OK;
 }

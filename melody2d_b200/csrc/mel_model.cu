@@ -392,19 +392,24 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, h->device);
     const size_t two_per_sm = (size_t)(smem_sm / 2 - smem_res);
     {
-        const int caps[] = { MEL_CHUNK_E_MAX, 1536, 1024, 768, 512, 256 };
+        const bool mixed = h->precision == MEL_PREC_MIXED;
+        // FP32 images hold 12 bytes per entry instead of 20, so the mixed form tries larger chunks
+        const int caps_fp64[] = { MEL_CHUNK_E_MAX, 1536, 1024, 768, 512, 256 };
+        const int caps_mixed[] = { 2 * MEL_CHUNK_E_MAX, 3584, 3072, 2560, MEL_CHUNK_E_MAX, 1536, 1024, 512, 256 };
+        std::vector<int> caps = mixed ? std::vector<int>(std::begin(caps_mixed), std::end(caps_mixed))
+                                      : std::vector<int>(std::begin(caps_fp64), std::end(caps_fp64));
         int chosen = -1;
         for (int ecap : caps) {
-            mel_status rc = mel_build_chunks(d, ecap, CS);
+            mel_status rc = mel_build_chunks(d, ecap, CS, mixed);
             if (rc) return rc;
-            size_t sm = mel_body_smem_bytes(max_def_nodes, CS.img_max);
+            size_t sm = mel_body_smem_bytes(max_def_nodes, CS.img_max, mixed);
             if (sm <= two_per_sm) { chosen = ecap; break; }
         }
         if (chosen < 0) {   // one CTA per SM: largest cap that fits
             for (int ecap : caps) {
-                mel_status rc = mel_build_chunks(d, ecap, CS);
+                mel_status rc = mel_build_chunks(d, ecap, CS, mixed);
                 if (rc) return rc;
-                if (mel_body_smem_bytes(max_def_nodes, CS.img_max) <= (size_t)smem_blk) { chosen = ecap; break; }
+                if (mel_body_smem_bytes(max_def_nodes, CS.img_max, mixed) <= (size_t)smem_blk) { chosen = ecap; break; }
             }
         }
         if (chosen < 0) {
@@ -453,8 +458,8 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     if (cudaMalloc(&P.inc_rng, sizeof(int2) * 16) != cudaSuccess) return MEL_ERR_OOM;
     P.inc_rng_bytes = sizeof(int2) * 16;
     D.inc_rng = P.inc_rng;
-    h->body_smem = mel_body_smem_bytes(max_def_nodes, CS.img_max);
-    mel_body_kernel_configure(h->body_smem);
+    h->body_smem = mel_body_smem_bytes(max_def_nodes, CS.img_max, h->precision == MEL_PREC_MIXED);
+    if (mel_body_kernel_configure(h->body_smem) != MEL_OK) return MEL_ERR_CUDA;
     h->d_monitor = dalloc<double>(h, 32);
     h->d_monitor_part = dalloc<double>(h, 5 * 148);
     {
@@ -477,7 +482,8 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         for (int b = 0; b < nb; b++)
             if (d->body_type[b] == MEL_BODY_DEFORMABLE)
                 nse_def += d->node_sup_ptr[d->body_node_ptr[b + 1]] - d->node_sup_ptr[d->body_node_ptr[b]];
-        h->bytes_body = h->img_bytes - 20. * (double)h->n_pad + (double)CS.chunks.size() * sizeof(mel_chunk) + nd * (5 * 16 + 7 * 16) +
+        const double entry_bytes = h->precision == MEL_PREC_MIXED ? 12. : 20.;
+        h->bytes_body = h->img_bytes - entry_bytes * (double)h->n_pad + (double)CS.chunks.size() * sizeof(mel_chunk) + nd * (5 * 16 + 7 * 16) +
                         nse_def * (2 + 8) + (nd + 1) * 4;
         h->bytes_contact = (double)ne * (4 * 4 + 4 * 4 + 8 + 8);   // refreshed border lengths (contacts added per call)
     }
@@ -506,7 +512,7 @@ static mel_status proximity(mel_handle* h, cudaEvent_t e0 = nullptr, cudaEvent_t
     int rc = mel_run_proximity(h->d, h->P, h->H, h->stream);
     h->launches += h->P.launches - launches0;
     if (e1) cudaEventRecord(e1, h->stream);
-    if (rc) { if (rc == MEL_ERR_CUDA) mel_set_cuda_error(cudaGetLastError(), "proximity", __FILE__, __LINE__); return (mel_status)rc; }
+    if (rc) return (mel_status)rc;      // the pipeline has set the message
     return MEL_OK;
 }
 
@@ -684,6 +690,10 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
         mark(); kinds.push_back(0);
         mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream);
         mark(); kinds.push_back(1);
+        {
+            cudaError_t le = cudaGetLastError();
+            if (le != cudaSuccess) { mel_set_cuda_error(le, "step kernel launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+        }
         h->launches += 2;
         h->parity ^= 1;
         h->time += h->dt;                       // Code/Solver.h:86

@@ -541,6 +541,22 @@ static int ensure_impl(void** p, size_t* cap_bytes, size_t need, const char* wha
 }
 #define ensure(p, cap, need) ensure_impl(p, cap, need, #p)
 
+// launch errors and stream failures of the pipeline, reported with their CUDA error and line
+static int launch_status(int line)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return MEL_OK;
+    mel_set_cuda_error(e, "proximity kernel launch", __FILE__, line);
+    return MEL_ERR_CUDA;
+}
+static bool sync_failed(cudaStream_t s, int line)
+{
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) return false;
+    mel_set_cuda_error(e, "proximity stream", __FILE__, line);
+    return true;
+}
+
 // Exclusive scan of n ints into out[0..n] (out[n] = total): a block scan per 1024 entries, the
 // block totals scanned the same way, then the block offsets added.  Deterministic; the block
 // totals live in the state's persistent scratch (no allocation once it has grown).
@@ -587,7 +603,7 @@ int mel_index_contacts(mel_dev& d, mel_prox_state& P, cudaStream_t s)
     if (ensure((void**)&P.e_list, &P.e_list_bytes, sizeof(int) * (size_t)(d.ncont + 1))) return MEL_ERR_OOM;
     cudaMemcpyAsync(P.e_cur, P.e_ptr, sizeof(int) * (d.ne + 1), cudaMemcpyDeviceToDevice, s);
     entry_index_kernel<<<(d.nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0, P.e_cur, P.e_list); P.launches++;
-    return cudaGetLastError() == cudaSuccess ? MEL_OK : MEL_ERR_CUDA;
+    return launch_status(__LINE__);
 }
 
 int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cudaStream_t s)
@@ -613,7 +629,7 @@ int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cud
         cudaMemcpyAsync(hv, d.err, sizeof hv, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&ntask, P.btask0 + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&nslot, P.bslot0 + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (cudaStreamSynchronize(s) != cudaSuccess) return MEL_ERR_CUDA;
+        if (sync_failed(s, __LINE__)) return MEL_ERR_CUDA;
         if (hv[MEL_E_NAN]) {
             mel_set_error(hv[MEL_E_NAN] & 1u ? "non-finite node positions at the proximity update"
                                              : "a border box spans more than %d periods: diverged positions",
@@ -651,7 +667,7 @@ int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cud
     if (mel_scan_exclusive(P.slot_cnt, P.slot_off, nslot, P, s)) return MEL_ERR_OOM;
     int total = 0;
     cudaMemcpyAsync(&total, P.slot_off + nslot, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) return MEL_ERR_CUDA;
+    if (sync_failed(s, __LINE__)) return MEL_ERR_CUDA;
     // 4. write the new list into the spare buffer, inheriting from the current one
     if (ensure((void**)&P.cont_alt, &P.cont_alt_bytes, sizeof(mel_contact) * (size_t)(total + 1))) return MEL_ERR_OOM;
     if (ntask > 0) {
@@ -688,7 +704,7 @@ int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cud
     carry_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0); P.launches++;
     P.ntask = ntask; P.nslot = nslot;
     if (rc) return rc;
-    return cudaGetLastError() == cudaSuccess ? MEL_OK : MEL_ERR_CUDA;
+    return launch_status(__LINE__);
 }
 
 // Index structures for a list supplied by the caller (mel_set_contacts): incoming ranges are built
@@ -713,6 +729,6 @@ int mel_index_external(mel_dev& d, mel_prox_state& P, const mel_contact* host_li
     d.b_inc0 = P.b_inc0;
     int rc = mel_index_contacts(d, P, s);
     d.b_cont0 = P.b_cont0;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return MEL_ERR_CUDA;
+    if (sync_failed(s, __LINE__)) return MEL_ERR_CUDA;
     return rc;
 }
