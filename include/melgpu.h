@@ -265,6 +265,25 @@ mel_status mel_monitor_reduce_static(const double* d_velocity, const double* d_m
                                      int n_nodes, const mel_contact* d_contacts, int n_contacts, double* d_out,
                                      void* stream);
 
+/* ---- batches ------------------------------------------------------------------------ */
+/* No counterpart in the reference (one simulation per process there).  A batch advances several
+ * independent handles (samples) with shared launches: per step one contact pass over all members'
+ * contact elements, one body pass over all members' bodies and one time advance, so many small
+ * samples fill the GPU together.  Each member keeps its own device arrays, time, dt and proximity
+ * cadence (Code/main.cpp:191-196, run per member on the batch's stream when its time comes), and
+ * computes exactly what mel_step would compute for it alone.  Members are admitted and retired
+ * between steps (continuous batching); a member cannot be stepped with mel_step, and mel_destroy
+ * retires it first.  All members share the batch's device and precision. */
+typedef struct mel_batch mel_batch;
+mel_status mel_batch_create(int device, int precision, mel_batch** out);
+mel_status mel_batch_admit(mel_batch* b, mel_handle* h);
+mel_status mel_batch_retire(mel_batch* b, mel_handle* h);
+/* nsteps steps of every member; run_proximity as in mel_step_io.  Returns after the work is done. */
+mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity);
+/* device time of the last mel_batch_step call (CUDA events), kernels it launched, current members */
+mel_status mel_batch_stats(mel_batch* b, double* ms_last_call, long long* launches, int* members);
+mel_status mel_batch_destroy(mel_batch* b);
+
 /* ---- introspection ---------------------------------------------------------------- */
 const char* mel_last_error_string(void);
 int         mel_abi_version(void);

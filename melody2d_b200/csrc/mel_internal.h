@@ -123,6 +123,10 @@ struct mel_dev {
 // kernel launch wrappers (mel_kernels.cu)
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s);
+// one step of a batch: the contact pass over thr0[nsamp] threads, the body pass over cta0[nsamp]
+// CTAs and the per-sample time advance (devs, thr0, cta0 in device memory)
+void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta, int nsamp,
+                           int mixed, size_t smem, cudaStream_t s);
 size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed);
 void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);

@@ -89,9 +89,9 @@ __device__ __forceinline__ void rigid_terms(const mel_dev& d, int tid, const mel
     }
 }
 
-__global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale)
+// one thread of the contact pass: contact element `tid`, or border entry tid - ncont
+__device__ void contact_thread(const mel_dev& d, int tid, double law_dt_scale)
 {
-    int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= d.ncont) {
         // refresh stored border lengths (read by Update_proximity for new contacts)
         int e = tid - d.ncont;
@@ -503,13 +503,12 @@ __device__ __forceinline__ void chunk_points_mx(int t, int mtype, float Mu, floa
 //                          pass, then s_fn, s_fd, s_vp, s_ap (n double2 each) and the six work
 //                          terms per node (6 x n double)
 template <bool MX>
-__device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
+__device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
 {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int n0 = d.b_node0[b];
     const int n = d.b_node0[b + 1] - n0;
-    const double T = d.time2[parity];
     const double dt = d.dt[0];
     double2* s_up = reinterpret_cast<double2*>(smem);
     double2* s_f = s_up + n;
@@ -799,12 +798,11 @@ __device__ void deformable_body(const mel_dev& d, int b, int parity, char* smem)
 // ------------------------------------------------------------------------------------------
 #define MEL_RIGID_BATCH 512   // border entries whose terms are staged at once (6 doubles each)
 
-__device__ void rigid_body(const mel_dev& d, int b, int parity, char* smem)
+__device__ void rigid_body(const mel_dev& d, int b, double T, char* smem)
 {
     const int tid = threadIdx.x;
     const int n0 = d.b_node0[b];
     const int n = d.b_node0[b + 1] - n0;
-    const double T = d.time2[parity];
     const double dt = d.dt[0];
     double* rg = d.rg + MEL_RIGID_NF * b;
     double* rf = d.rf + 15 * b;
@@ -963,15 +961,71 @@ __device__ void contact_work(const mel_dev& d, int b)
 }
 
 template <bool MX>
+__device__ __forceinline__ void body_cta(const mel_dev& d, int bb, double T, char* smem)
+{
+    int b = d.b_order[bb];
+    if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
+    if (d.any_damped && threadIdx.x == 32) contact_work(d, b);
+    if (d.b_type[b] == MEL_BODY_RIGID) rigid_body(d, b, T, smem);
+    else deformable_body<MX>(d, b, T, smem);
+}
+
+__global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale)
+{
+    contact_thread(d, blockIdx.x * blockDim.x + threadIdx.x, law_dt_scale);
+}
+
+// One model: CTA i is the body d.b_order[i]; time2[parity] is the step's start time, the step's
+// end time goes to time2[parity ^ 1] (the next launch reads it).
+template <bool MX>
 __global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel(mel_dev d, int parity)
 {
     extern __shared__ __align__(16) char smem[];
-    int b = d.b_order[blockIdx.x];
-    if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
-    if (d.any_damped && threadIdx.x == 32) contact_work(d, b);
-    if (d.b_type[b] == MEL_BODY_RIGID) rigid_body(d, b, parity, smem);
-    else deformable_body<MX>(d, b, parity, smem);
-    if (blockIdx.x == 0 && threadIdx.x == 0) d.time2[parity ^ 1] = d.time2[parity] + d.dt[0];
+    const double T = d.time2[parity];
+    body_cta<MX>(d, blockIdx.x, T, smem);
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.time2[parity ^ 1] = T + d.dt[0];
+}
+
+// ---- batches: several independent models (samples) advanced by the same launches -----------
+// devs[s] is the descriptor of sample s; cta0 / thr0 are prefix sums of the samples' bodies and of
+// their contact-pass threads (contacts + border entries).  A sample's time lives in time2[0] and is
+// advanced by advance_kernel after each step.  Every sample runs exactly the code of a one-model
+// launch on its own arrays, so its results do not depend on the rest of the batch.
+__device__ __forceinline__ int batch_member(const int* prefix, int nsamp, int i)
+{
+    int lo = 0, hi = nsamp;                  // largest s with prefix[s] <= i
+    while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (prefix[mid] <= i) lo = mid; else hi = mid; }
+    return lo;
+}
+
+__global__ void __launch_bounds__(128) contact_kernel_batch(const mel_dev* devs, const int* thr0, int nsamp,
+                                                            double law_dt_scale)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= thr0[nsamp]) return;
+    const int s = batch_member(thr0, nsamp, i);
+    contact_thread(devs[s], i - thr0[s], law_dt_scale);
+}
+
+template <bool MX>
+__global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel_batch(const mel_dev* devs, const int* cta0, int nsamp)
+{
+    extern __shared__ __align__(16) char smem[];
+    __shared__ mel_dev sd;                   // the sample's descriptor, read once per CTA
+    const int s = batch_member(cta0, nsamp, blockIdx.x);
+    {
+        const int* src = reinterpret_cast<const int*>(devs + s);
+        int* dst = reinterpret_cast<int*>(&sd);
+        for (int k = threadIdx.x; k < (int)(sizeof(mel_dev) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    body_cta<MX>(sd, blockIdx.x - cta0[s], sd.time2[0], smem);
+}
+
+__global__ void advance_kernel(const mel_dev* devs, int nsamp)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nsamp) devs[s].time2[0] = devs[s].time2[0] + devs[s].dt[0];
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1037,6 +1091,17 @@ size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)
     return r > rigid ? r : rigid;
 }
 
+void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta, int nsamp,
+                           int mixed, size_t smem, cudaStream_t s)
+{
+    if (nthr > 0) mel::contact_kernel_batch<<<(nthr + 127) / 128, 128, 0, s>>>(devs, thr0, nsamp, 1.0);
+    if (ncta > 0) {
+        if (mixed) mel::body_kernel_batch<true><<<ncta, MEL_BODY_THREADS, smem, s>>>(devs, cta0, nsamp);
+        else mel::body_kernel_batch<false><<<ncta, MEL_BODY_THREADS, smem, s>>>(devs, cta0, nsamp);
+    }
+    mel::advance_kernel<<<(nsamp + 127) / 128, 128, 0, s>>>(devs, nsamp);
+}
+
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s)
 {
     if (d.precision == MEL_PREC_MIXED) mel::body_kernel<true><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
@@ -1060,7 +1125,9 @@ int mel_body_kernel_configure(size_t smem)
     std::lock_guard<std::mutex> lock(mu);
     if (smem <= configured[dev]) return MEL_OK;
     if (cudaFuncSetAttribute(mel::body_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(mel::body_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaFuncSetAttribute(mel::body_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         mel_set_cuda_error(cudaGetLastError(), "cudaFuncSetAttribute(body_kernel)", __FILE__, __LINE__);
         return MEL_ERR_CUDA;
     }

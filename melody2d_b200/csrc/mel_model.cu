@@ -67,6 +67,7 @@ struct mel_handle {
     std::vector<cudaEvent_t> ev_pool;
     double bytes_body = 0., bytes_contact = 0.;
     int n_def_nodes = 0;
+    mel_batch* batch = nullptr;  // batch the handle is a member of (steps only through the batch)
 };
 
 template <typename T>
@@ -652,6 +653,7 @@ mel_status mel_destroy(mel_handle* h)
 {
     if (!h) return MEL_OK;
     cudaSetDevice(h->device);
+    if (h->batch) mel_batch_retire(h->batch, h);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void* p : h->allocs) cudaFree(p);
     mel_prox_state& P = h->P;
@@ -670,6 +672,7 @@ mel_status mel_destroy(mel_handle* h)
 mel_status mel_step(mel_handle* h, mel_step_io* io)
 {
     if (!h || !io || io->nsteps < 0) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    if (h->batch) { mel_set_error("the handle is a member of a batch: step it with mel_batch_step"); return MEL_ERR_INVALID; }
     cudaSetDevice(h->device);
     h->t_contact = h->t_body = h->t_prox = h->t_total = 0.;
     h->launches = 0;
@@ -989,3 +992,176 @@ mel_status mel_get_error_words(mel_handle* h, unsigned* words, int n)
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// batches: independent models advanced by shared launches
+// ---------------------------------------------------------------------------------------------
+struct mel_batch {
+    int device = 0, precision = MEL_PREC_FP64;
+    cudaStream_t stream = nullptr;
+    std::vector<mel_handle*> members;
+    std::vector<mel_dev> h_devs;         // member descriptors as last uploaded
+    std::vector<int> h_thr0, h_cta0;     // prefix sums: contact-pass threads, body CTAs
+    mel_dev* d_devs = nullptr;
+    int* d_thr0 = nullptr;
+    int* d_cta0 = nullptr;
+    size_t cap = 0;                      // members the device arrays hold
+    bool dirty = true;                   // descriptors changed (admission, retirement, proximity)
+    size_t smem = 0;
+    long long launches = 0;
+    double ms_last = 0.;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+// Re-uploads the member descriptors and the work prefixes (the stream is idle afterwards).
+static mel_status batch_refresh(mel_batch* b)
+{
+    const int n = (int)b->members.size();
+    MEL_CUDA_OK(cudaStreamSynchronize(b->stream));
+    if ((size_t)n > b->cap) {
+        size_t cap = std::max((size_t)n, 2 * b->cap);
+        cudaFree(b->d_devs); cudaFree(b->d_thr0); cudaFree(b->d_cta0);
+        b->d_devs = nullptr; b->d_thr0 = nullptr; b->d_cta0 = nullptr;
+        if (cudaMalloc(&b->d_devs, sizeof(mel_dev) * cap) != cudaSuccess ||
+            cudaMalloc(&b->d_thr0, sizeof(int) * (cap + 1)) != cudaSuccess ||
+            cudaMalloc(&b->d_cta0, sizeof(int) * (cap + 1)) != cudaSuccess) {
+            mel_set_error("batch descriptor allocation failed");
+            return MEL_ERR_OOM;
+        }
+        b->cap = cap;
+    }
+    b->h_devs.resize(n);
+    b->h_thr0.assign(n + 1, 0);
+    b->h_cta0.assign(n + 1, 0);
+    b->smem = 0;
+    for (int i = 0; i < n; i++) {
+        mel_handle* h = b->members[i];
+        b->h_devs[i] = h->d;
+        b->h_thr0[i + 1] = b->h_thr0[i] + h->d.ncont + h->d.ne;
+        b->h_cta0[i + 1] = b->h_cta0[i] + h->nblocks_body;
+        b->smem = std::max(b->smem, h->body_smem);
+    }
+    if (n > 0) {
+        MEL_CUDA_OK(cudaMemcpy(b->d_devs, b->h_devs.data(), sizeof(mel_dev) * n, cudaMemcpyHostToDevice));
+        MEL_CUDA_OK(cudaMemcpy(b->d_thr0, b->h_thr0.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        MEL_CUDA_OK(cudaMemcpy(b->d_cta0, b->h_cta0.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    }
+    b->dirty = false;
+    return MEL_OK;
+}
+
+mel_status mel_batch_create(int device, int precision, mel_batch** out)
+{
+    if (!out) { mel_set_error("null output"); return MEL_ERR_INVALID; }
+    *out = nullptr;
+    if (precision != MEL_PREC_FP64 && precision != MEL_PREC_MIXED) { mel_set_error("unknown precision %d", precision); return MEL_ERR_INVALID; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { mel_set_error("no CUDA device"); return MEL_ERR_NO_DEVICE; }
+    if (device < 0 || device >= ndev) { mel_set_error("device %d out of range", device); return MEL_ERR_INVALID; }
+    mel_batch* b = new mel_batch();
+    b->device = device;
+    b->precision = precision;
+    cudaSetDevice(device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) {
+        mel_set_cuda_error(cudaGetLastError(), "batch stream", __FILE__, __LINE__);
+        delete b;
+        return MEL_ERR_CUDA;
+    }
+    *out = b;
+    return MEL_OK;
+}
+
+mel_status mel_batch_admit(mel_batch* b, mel_handle* h)
+{
+    if (!b || !h) return MEL_ERR_INVALID;
+    if (h->batch) { mel_set_error("the handle is already a member of a batch"); return MEL_ERR_INVALID; }
+    if (h->device != b->device || h->precision != b->precision) {
+        mel_set_error("the handle's device or precision differs from the batch's");
+        return MEL_ERR_INVALID;
+    }
+    cudaSetDevice(b->device);
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    MEL_CUDA_OK(cudaStreamSynchronize(b->stream));
+    if (h->parity == 1) {                        // a batch keeps each member's time in time2[0]
+        MEL_CUDA_OK(cudaMemcpy(h->d.time2, h->d.time2 + 1, sizeof(double), cudaMemcpyDeviceToDevice));
+        h->parity = 0;
+    }
+    h->batch = b;
+    b->members.push_back(h);
+    b->dirty = true;
+    return MEL_OK;
+}
+
+mel_status mel_batch_retire(mel_batch* b, mel_handle* h)
+{
+    if (!b || !h || h->batch != b) { mel_set_error("the handle is not a member of this batch"); return MEL_ERR_INVALID; }
+    cudaSetDevice(b->device);
+    MEL_CUDA_OK(cudaStreamSynchronize(b->stream));
+    b->members.erase(std::find(b->members.begin(), b->members.end(), h));
+    h->batch = nullptr;
+    b->dirty = true;
+    return MEL_OK;
+}
+
+mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity)
+{
+    if (!b || nsteps < 0) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    cudaSetDevice(b->device);
+    b->launches = 0;
+    cudaEventRecord(b->e0, b->stream);
+    for (int step = 0; step < nsteps; step++) {
+        if (b->dirty) { mel_status rc = batch_refresh(b); if (rc) return rc; }
+        const int n = (int)b->members.size();
+        if (n == 0) break;
+        mel_launch_batch_step(b->d_devs, b->d_thr0, b->h_thr0[n], b->d_cta0, b->h_cta0[n], n,
+                              b->precision == MEL_PREC_MIXED, b->smem, b->stream);
+        b->launches += 3;
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) { mel_set_cuda_error(le, "batch step launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+        for (mel_handle* h : b->members) {
+            h->time += h->dt;                                    // Code/Solver.h:86
+            if (run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
+                h->next_cup = h->next_cup + h->cup;
+                int l0 = h->P.launches;
+                int rc = mel_run_proximity(h->d, h->P, h->H, b->stream);
+                b->launches += h->P.launches - l0;
+                if (rc) return (mel_status)rc;
+                b->dirty = true;
+            }
+        }
+    }
+    cudaEventRecord(b->e1, b->stream);
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) { mel_set_cuda_error(e, "mel_batch_step", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->e0, b->e1);
+    b->ms_last = ms;
+    for (mel_handle* h : b->members) {
+        mel_status rc = check_errors(h);
+        if (rc) return rc;
+    }
+    return MEL_OK;
+}
+
+mel_status mel_batch_stats(mel_batch* b, double* ms_last_call, long long* launches, int* members)
+{
+    if (!b) return MEL_ERR_INVALID;
+    if (ms_last_call) *ms_last_call = b->ms_last;
+    if (launches) *launches = b->launches;
+    if (members) *members = (int)b->members.size();
+    return MEL_OK;
+}
+
+mel_status mel_batch_destroy(mel_batch* b)
+{
+    if (!b) return MEL_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    for (mel_handle* h : b->members) h->batch = nullptr;
+    cudaFree(b->d_devs); cudaFree(b->d_thr0); cudaFree(b->d_cta0);
+    cudaEventDestroy(b->e0); cudaEventDestroy(b->e1);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return MEL_OK;
+}

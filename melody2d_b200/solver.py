@@ -52,6 +52,12 @@ SIGNATURES = {
     "mel_get_sizes": [_vp, _ip, _ip, _ip, _ip, _ip, _ip],
     "mel_get_step_stats": [_vp, _dp, _dp, _dp, _ip, _ip],
     "mel_monitor_reduce_static": [_vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp],
+    "mel_batch_create": [C.c_int, C.c_int, C.POINTER(_vp)],
+    "mel_batch_admit": [_vp, _vp],
+    "mel_batch_retire": [_vp, _vp],
+    "mel_batch_step": [_vp, C.c_int, C.c_int],
+    "mel_batch_stats": [_vp, _dp, C.POINTER(C.c_longlong), _ip],
+    "mel_batch_destroy": [_vp],
 }
 
 
@@ -289,3 +295,42 @@ def load_desc_arrays(directory: str, restart_index: int = 0) -> dict:
         return out
     finally:
         L.mel_free_desc(owner)
+
+
+class Batch:
+    """Several independent solvers advanced by shared launches (mel_batch_*): admit handles,
+    step them together, retire them when their run ends.  Each member's results are those it
+    would have on its own."""
+
+    def __init__(self, precision: int = 0, device: int = 0):
+        self.b = C.c_void_p()
+        _check(lib().mel_batch_create(int(device), int(precision), C.byref(self.b)))
+        self.members = []
+
+    def admit(self, s: Solver):
+        _check(lib().mel_batch_admit(self.b, s.h))
+        self.members.append(s)
+
+    def retire(self, s: Solver):
+        _check(lib().mel_batch_retire(self.b, s.h))
+        self.members.remove(s)
+
+    def step(self, n: int = 1, proximity: bool = True):
+        _check(lib().mel_batch_step(self.b, int(n), 1 if proximity else 0))
+
+    def stats(self) -> dict:
+        ms, launches, members = C.c_double(), C.c_longlong(), C.c_int()
+        _check(lib().mel_batch_stats(self.b, C.byref(ms), C.byref(launches), C.byref(members)))
+        return {"ms_last_call": ms.value, "launches": launches.value, "members": members.value}
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().mel_batch_destroy(self.b)
+            self.b = None
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
