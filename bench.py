@@ -267,6 +267,166 @@ def run_ours(args, rank, world, local, pg):
     s.close()
 
 
+def _sample_scene(job):
+    """Worker of the batched workload's generation (spawned process): one sample's flat arrays."""
+    seed, counts = job
+    from melody2d_b200 import generator as g
+    templates = _sample_scene.templates
+    sc = g.batch_sample_scene(seed, templates)
+    return seed, g.flatten(sc), sc.meta
+
+
+def _init_sample_worker(counts):
+    from melody2d_b200 import generator as g
+    _sample_scene.templates = g.DiscTemplates(counts, workers=1)
+
+
+def make_batch_samples(seeds, workers):
+    """Flat arrays of the batched workload's samples (config-3 draws), built in a spawn pool whose
+    workers each hold the disc templates."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    counts = list(range(32, 97))
+    ctx = mp.get_context("spawn")
+    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_init_sample_worker,
+                             initargs=(counts,)) as ex:
+        out = list(ex.map(_sample_scene, [(s, counts) for s in seeds]))
+    return out
+
+
+def create_solvers(flats, precision, device, threads):
+    """mel_create for many samples at once (the library call releases the interpreter lock)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from melody2d_b200.solver import Solver
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        return list(ex.map(lambda f: Solver.from_flat(f, precision=precision, device=device), flats))
+
+
+def run_batch(args, rank, world, local, pg):
+    """Batched workload: S independent biaxial samples (grains log-uniform in [50,1000], 32-96
+    border nodes per grain, confinement 50-400 kPa, friction 0.1-0.5) advanced together in one
+    mixed-precision batch, against the plain FP64 path run one sample at a time on a subset.
+    Samples/h are extrapolated from the timed steps to sample_steps steps per sample."""
+    from melody2d_b200.solver import Batch
+    threads = max(1, host_threads() // max(1, world))
+    t0 = time.perf_counter()
+    seeds = [1000 * (rank + 1) + i for i in range(args.samples)]
+    samples = make_batch_samples(seeds, threads)
+    t_gen = time.perf_counter() - t0
+    flats = [f for _, f, _ in samples]
+    t0 = time.perf_counter()
+    solvers = create_solvers(flats, 1, local, threads)
+    t_create = time.perf_counter() - t0
+    nodes = [s.step_stats()["n_deformable_nodes"] for s in solvers]
+    b = Batch(precision=1, device=local)
+    for s in solvers:
+        b.admit(s)
+    b.step(args.warmup)
+    clocks = ClockSampler(local)
+    barrier(pg)
+    clocks.start()
+    b.step(args.steps)
+    barrier(pg)
+    clk = clocks.stop()
+    st = b.stats()
+    ms = allreduce_max(pg, st["ms_last_call"])
+    total_nodes = allreduce_sum(pg, sum(nodes))
+    value = total_nodes * args.steps / (ms * 1e-3)
+    ms_per_step = ms / args.steps
+    samples_h = allreduce_sum(pg, args.samples) * 3600.0 / (ms_per_step * 1e-3 * args.sample_steps)
+    # plain FP64 path, one sample at a time, on a subset; mixed-vs-FP64 errors on the same subset
+    sub = list(range(0, args.samples, max(1, args.samples // args.plain_subset)))[: args.plain_subset]
+    plain_ms, errs = [], []
+    for i in sub:
+        a = create_solvers([flats[i]], 0, local, 1)[0]
+        a.step(args.warmup)
+        a.step(args.steps)
+        plain_ms.append(a.step_stats()["ms_total"] / args.steps)
+        ma, mb = a.monitor(), solvers[i].monitor()
+
+        def rel(x, y):
+            x, y = np.asarray(x, float), np.asarray(y, float)
+            return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+        errs.append({"kinetic_energy": rel(mb.kinetic_energy, ma.kinetic_energy),
+                     "wall_contact_force": rel(list(mb.rigid_force), list(ma.rigid_force)),
+                     "wall_reaction": rel(list(mb.rigid_dirichlet), list(ma.rigid_dirichlet)),
+                     "active_contacts_equal": mb.active_contacts == ma.active_contacts})
+        a.close()
+    # the subset's mean time per step alone stands for the mean sample of the distribution
+    plain_samples_h = 3600.0 / (float(np.mean(plain_ms)) * 1e-3 * args.sample_steps)
+    if rank == 0:
+        line = {
+            "metric": "samples/h", "value": samples_h, "unit": "samples/h", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (dN, strain, stress, contributions) + f64",
+            "data": "synthetic (seeded batched biaxial generator, scaled disc templates)",
+            "config": {"workload": f"batched: {args.samples} independent biaxial samples per GPU, grains log-uniform "
+                                   f"[50,1000], 32-96 border + 5x interior nodes per grain, confinement U[50,400] kPa, "
+                                   f"friction U[0.1,0.5], mass x100, plates 0.05 m/s; mixed precision",
+                       "samples_per_gpu": args.samples, "nodes_per_gpu": int(sum(nodes)),
+                       "samples_h_extrapolated_to_steps": args.sample_steps,
+                       "l2": "inputs larger than L2", "generate_s": round(t_gen, 2), "create_s": round(t_create, 2)},
+            "node_steps_per_s": value,
+            "plain_fp64_one_at_a_time": {"samples_h": plain_samples_h, "subset": len(sub),
+                                         "ms_per_step_mean": float(np.mean(plain_ms))},
+            "ratio_vs_plain_fp64": samples_h / plain_samples_h if world == 1 else None,
+            "accuracy_vs_fp64_after_steps": args.warmup + args.steps,
+            "max_rel_error": {k: max(e[k] for e in errs) for k in ("kinetic_energy", "wall_contact_force", "wall_reaction")},
+            "active_contacts_equal": all(e["active_contacts_equal"] for e in errs),
+            "clocks": clk, "gpu_launches": st["launches"],
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+def run_serve(args, rank, world, local, pg):
+    """Serving: seeded Poisson arrivals (args.rate per second for args.duration seconds) of
+    batched-workload requests, each run to 5 % axial strain or args.step_cap steps; the batched
+    mixed-precision server against the plain FP64 path serving one request at a time, on the same
+    request stream.  Both arms get args.drain seconds after the last arrival to finish."""
+    from melody2d_b200.serving import Server, poisson_arrivals
+    arrivals = poisson_arrivals(args.rate, args.duration, seed=7 + rank)
+    seeds = [50000 * (rank + 1) + i for i in range(len(arrivals))]
+    threads = max(1, host_threads() // max(1, world))
+    arms = {}
+    for name, batched, precision in (("batched_mixed", True, 1), ("plain_fp64", False, 0)):
+        srv = Server(batched=batched, precision=precision, device=local, hbm_budget=args.hbm_budget * 1e9,
+                     step_cap=args.step_cap, build_workers=max(1, threads - 2), create_threads=2)
+        barrier(pg)
+        res = srv.run(arrivals, seeds, args.duration, drain=args.drain)
+        arms[name] = res
+    # same request, both arms: the final monitored quantities agree within the mixed form's tolerance
+    a = {r["rid"]: r for r in arms["batched_mixed"]["requests"]}
+    b = {r["rid"]: r for r in arms["plain_fp64"]["requests"]}
+    common = sorted(set(a) & set(b))
+
+    def rel(x, y):
+        x, y = np.asarray(x, float), np.asarray(y, float)
+        return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    err_ke = max([rel(a[i]["kinetic_energy"], b[i]["kinetic_energy"]) for i in common], default=None)
+    err_wall = max([rel(a[i]["wall_force"], b[i]["wall_force"]) for i in common], default=None)
+    if rank == 0:
+        summary = {k: {kk: v for kk, v in r.items() if kk != "requests"} for k, r in arms.items()}
+        line = {
+            "metric": "samples/h", "value": summary["batched_mixed"]["samples_per_hour"], "unit": "samples/h",
+            "n_gpus": world, "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (dN, strain, stress, contributions) + f64",
+            "data": "synthetic (seeded Poisson request stream of batched-workload samples)",
+            "config": {"workload": f"serving: Poisson arrivals at {args.rate}/s for {args.duration} s, requests from the "
+                                   f"batched-workload distribution, each to 5% axial strain or {args.step_cap} steps, "
+                                   f"HBM budget {args.hbm_budget} GB, {args.drain} s drain"},
+            "arms": summary,
+            "ratio_samples_h_vs_plain_fp64": (summary["batched_mixed"]["samples_per_hour"] /
+                                              max(summary["plain_fp64"]["samples_per_hour"], 1e-300)),
+            "same_requests_compared": len(common),
+            "max_rel_error_vs_plain_fp64": {"kinetic_energy": err_ke, "wall_contact_force": err_wall},
+            "gpu_launches": summary["batched_mixed"]["gpu_launches"],
+        }
+        print(json.dumps(line), flush=True)
+
+
 def compare_precisions(args, rank, world, local, pg):
     """Config-2 report: the mixed form against the FP64 path (bit-identical to the FP64 oracle) on
     the same generated sample after K steps: relative errors of kinetic energy, wall reaction
@@ -320,6 +480,17 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--compare-fp64", type=int, default=0, metavar="K",
                     help="instead of timing, report the mixed form's errors against FP64 after K steps")
+    ap.add_argument("--mode", default="single", choices=["single", "batch", "serve"],
+                    help="single: the 2000-disc sample; batch: many independent samples in one batch; "
+                         "serve: a Poisson request stream served by continuous batching")
+    ap.add_argument("--rate", type=float, default=2.0)
+    ap.add_argument("--duration", type=float, default=60.0)
+    ap.add_argument("--drain", type=float, default=60.0)
+    ap.add_argument("--step-cap", type=int, default=40000)
+    ap.add_argument("--hbm-budget", type=float, default=150.0, help="GB")
+    ap.add_argument("--samples", type=int, default=256)
+    ap.add_argument("--sample-steps", type=int, default=20000)
+    ap.add_argument("--plain-subset", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -327,6 +498,10 @@ def main():
     try:
         if args.compare_fp64 > 0:
             compare_precisions(args, rank, world, local, pg)
+        elif args.mode == "batch" and args.impl == "ours":
+            run_batch(args, rank, world, local, pg)
+        elif args.mode == "serve" and args.impl == "ours":
+            run_serve(args, rank, world, local, pg)
         elif args.impl == "reference":
             run_reference(args, rank, world, pg)
         else:

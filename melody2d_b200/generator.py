@@ -808,6 +808,20 @@ def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax
              rho, mass_factor) for i in range(n_discs)]
     bodies = make_discs_parallel(jobs, workers)
     h_min = 2.0 * math.pi * rmin / n_border
+    bodies += _biaxial_frame(W, H, h_min, rho_steel, v_plate, sigma)
+    mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    smallest = np.argsort(radii)[:3]
+    dtc = min(critical_dt(bodies[i], mu, lam, 1e10) for i in smallest)
+    dt = float("%.4g" % (0.5 * dtc))
+    return Scene(name=name, bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
+                 contact_update_period=prox_every * dt,
+                 meta=dict(config="biaxial", seed=seed, dt_crit=dtc, box=(W, H), n_discs=n_discs,
+                           radii=(rmin, rmax), sigma=sigma, v_plate=v_plate, mass_factor=mass_factor))
+
+
+def _biaxial_frame(W: float, H: float, h_min: float, rho_steel: float, v_plate: float, sigma: float) -> List[Body]:
+    """Rigid plates (bottom, top) driven towards each other at v_plate and lateral walls (left,
+    right) loaded by the confining pressure sigma, fixed vertically."""
     thick = 0.05 * H
     hist = lambda v: (np.array([0.0, T_HIST_END]), np.array([v, v]))
     # plates span the box and the walls' inward travel; walls span the plates' full height, so no
@@ -824,12 +838,103 @@ def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax
                            (BC_ORIENTED, (0.0, 0.0), hist(p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
     right = make_rect_rigid(W, y0, W + thick, y0 + wall_h, 2.0 * h_min, 1, rho_steel,
                             (BC_ORIENTED, (0.0, 0.0), hist(-p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
-    bodies += [bot, top, left, right]
-    mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
-    smallest = np.argsort(radii)[:3]
-    dtc = min(critical_dt(bodies[i], mu, lam, 1e10) for i in smallest)
+    return [bot, top, left, right]
+
+
+# --------------------------------------------------------------------------------------------
+# batched workload: many independent biaxial samples whose grains are scaled disc templates
+# --------------------------------------------------------------------------------------------
+def _dt_terms(body: Body, mu: float, lam: float):
+    """Largest eigenvalue of the lumped-mass elastic operator and the contact term kn*h/m per unit
+    kn, the two parts of critical_dt, for the body as built."""
+    lam_el = (2.0 / critical_dt(body, mu, lam, 0.0)) ** 2
+    h_b = body.nodal_distance
+    m_border = body.mass[: len(body.borders[0]["nodes"]) - 1, 0]
+    return lam_el, float(np.max(h_b / m_border))
+
+
+class DiscTemplates:
+    """Unit-radius deformable discs, one per border-node count, with interior_factor x that many
+    interior nodes (density 1, no mass scaling), and the two critical-time-step terms of each.
+    A grain of radius r is a template scaled by r: N is unchanged, dN/dx and dN/dy scale by 1/r,
+    weight x jacobian and masses by r^2 (times density and mass factor); the elastic eigenvalue
+    scales by 1/r^2 and the contact term by 1/r (both divided by density x mass factor)."""
+
+    def __init__(self, border_counts, interior_factor: int = 5, seed: int = 20240, workers: Optional[int] = None,
+                 E: float = 1e8, nu: float = 0.3):
+        counts = sorted(set(int(c) for c in border_counts))
+        rng = np.random.default_rng(seed)
+        seeds = rng.integers(0, 2 ** 31 - 1, size=len(counts))
+        jobs = [(int(s), (0.0, 0.0), 1.0, nb, interior_factor * nb, 1.0, 1.0) for s, nb in zip(seeds, counts)]
+        bodies = make_discs_parallel(jobs, workers)
+        mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+        self.E, self.nu = E, nu
+        self.discs = dict(zip(counts, bodies))
+        self.terms = {nb: _dt_terms(b, mu, lam) for nb, b in self.discs.items()}
+
+    def grain(self, n_border: int, centre, radius: float, rho: float, mass_factor: float, material: int = 0) -> Body:
+        t = self.discs[n_border]
+        c = np.asarray(centre, dtype=np.float64)
+        r = float(radius)
+        s2 = r * r * rho * mass_factor
+        gp = (t.gp[0], t.gp[1], t.gp[2], t.gp[3] / r, t.gp[4] / r)
+        sup = (t.sup[0], t.sup[1], t.sup[2], t.sup[3] / r, t.sup[4] / r)
+        borders = [dict(b, nodes=list(b["nodes"])) for b in t.borders]
+        return Body(kind="deformable", material=material, nodes=c + r * t.nodes, borders=borders, cells=t.cells,
+                    nodal_distance=r * t.nodal_distance, detection=r * t.detection, contact=r * t.contact,
+                    domain=r * t.domain, mass=t.mass * s2, sup=sup, gp_xy=c + r * t.gp_xy, gp_w=t.gp_w,
+                    gp_J=t.gp_J * (r * r), gp=gp, n_regions=t.n_regions)
+
+    def critical_dt(self, n_border: int, radius: float, rho: float, mass_factor: float, kn: float) -> float:
+        lam_el, lam_c = self.terms[n_border]
+        m = rho * mass_factor
+        return 2.0 / math.sqrt(max(lam_el / (radius * radius * m), kn * lam_c / (radius * m)))
+
+
+def batch_sample_params(seed: int, grains=(50, 1000), border=(32, 96), sigma=(50e3, 400e3), mu_fric=(0.1, 0.5),
+                        rmin: float = 0.5e-3, rmax: float = 1.5e-3):
+    """Per-sample draws of the batched workload: grain count log-uniform, border nodes per grain
+    uniform integers, confining pressure and friction uniform, radii uniform."""
+    rng = np.random.default_rng(seed)
+    n = int(round(math.exp(rng.uniform(math.log(grains[0]), math.log(grains[1])))))
+    return dict(n_grains=n, radii=rng.uniform(rmin, rmax, size=n),
+                n_border=rng.integers(border[0], border[1] + 1, size=n),
+                sigma=float(rng.uniform(*sigma)), mu_fric=float(rng.uniform(*mu_fric)),
+                rng_state=int(rng.integers(0, 2 ** 31 - 1)))
+
+
+def batch_sample_scene(seed: int, templates: DiscTemplates, aspect: float = 100.0 / 60.0, fill: float = 0.45,
+                       gap: float = 0.02e-3, v_plate: float = 0.05, mass_factor: float = 100.0,
+                       nsteps: int = 20000, prox_every: int = 10, **draws) -> Scene:
+    """One sample of the batched workload: the biaxial set-up (plates driven at v_plate, walls
+    under the sample's confining pressure, mass scaling, proximity every prox_every steps) around
+    grains built from `templates`."""
+    p = batch_sample_params(seed, **draws)
+    rng = np.random.default_rng(p["rng_state"])
+    radii = p["radii"]
+    area = float(np.sum(np.pi * radii ** 2))
+    W = math.sqrt(area / fill * aspect)
+    H = W / aspect
+    centres, placed = _rsa_pack(rng, radii, W, H, gap)
+    tries = 0
+    while not placed.all() and tries < 5:
+        W *= 1.03; H *= 1.03; tries += 1
+        centres, placed = _rsa_pack(rng, radii, W, H, gap)
+    if not placed.all():
+        raise RuntimeError("packing failed")
+    E, rho = templates.E, 2500.0
+    rho_steel = 7800.0 * mass_factor
+    mats = [("Grain", 0, [rho, 0.0, 0.0, E, templates.nu, 1000.0]), ("Steel", 0, [rho_steel, 0.0, 0.0, 2e11, 0.3, 500.0])]
+    kn = 1e10
+    laws = [("Grain", "Grain", 2, 0, [kn, 1e9, p["mu_fric"], 0.0, 0.0]),
+            ("Grain", "Steel", 2, 0, [kn, 1e9, p["mu_fric"], 0.0, 0.0]),
+            ("Steel", "Steel", 0, 0, [0.0])]
+    bodies = [templates.grain(int(nb), c, r, rho, mass_factor) for nb, c, r in zip(p["n_border"], centres, radii)]
+    h_min = float(np.min(2.0 * math.pi * radii / p["n_border"]))
+    bodies += _biaxial_frame(W, H, h_min, rho_steel, v_plate, p["sigma"])
+    dtc = min(templates.critical_dt(int(nb), float(r), rho, mass_factor, kn) for nb, r in zip(p["n_border"], radii))
     dt = float("%.4g" % (0.5 * dtc))
-    return Scene(name=name, bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
+    return Scene(name=f"batch{seed}", bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
                  contact_update_period=prox_every * dt,
-                 meta=dict(config="biaxial", seed=seed, dt_crit=dtc, box=(W, H), n_discs=n_discs,
-                           radii=(rmin, rmax), sigma=sigma, v_plate=v_plate, mass_factor=mass_factor))
+                 meta=dict(config="batch", seed=seed, dt_crit=dtc, box=(W, H), n_discs=p["n_grains"],
+                           sigma=p["sigma"], mu_fric=p["mu_fric"], v_plate=v_plate, mass_factor=mass_factor))
