@@ -393,7 +393,7 @@ def run_serve(args, rank, world, local, pg):
     arms = {}
     for name, batched, precision in (("batched_mixed", True, 1), ("plain_fp64", False, 0)):
         srv = Server(batched=batched, precision=precision, device=local, hbm_budget=args.hbm_budget * 1e9,
-                     step_cap=args.step_cap, build_workers=max(1, threads - 2), create_threads=2)
+                     step_cap=args.step_cap, build_workers=max(1, threads - 6), create_threads=6)
         barrier(pg)
         res = srv.run(arrivals, seeds, args.duration, drain=args.drain)
         arms[name] = res

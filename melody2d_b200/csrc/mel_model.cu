@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include "mel_internal.h"
 #include "mel_prox_host.h"
 #include "mel_chunks.h"
@@ -68,6 +70,7 @@ struct mel_handle {
     double bytes_body = 0., bytes_contact = 0.;
     int n_def_nodes = 0;
     mel_batch* batch = nullptr;  // batch the handle is a member of (steps only through the batch)
+    cudaEvent_t ev_prox = nullptr;  // end of the handle's last proximity update within a batch
 };
 
 template <typename T>
@@ -399,24 +402,31 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         const int caps_mixed[] = { 2 * MEL_CHUNK_E_MAX, 3584, 3072, 2560, MEL_CHUNK_E_MAX, 1536, 1024, 512, 256 };
         std::vector<int> caps = mixed ? std::vector<int>(std::begin(caps_mixed), std::end(caps_mixed))
                                       : std::vector<int>(std::begin(caps_fp64), std::end(caps_fp64));
+        // the cap is chosen from an upper bound of the image size (a chunk holds at most ecap
+        // entries, MEL_CHUNK_GP points, min(ecap, nodes) touched nodes and one row per support
+        // of each group's largest point), so the images are built once
+        int max_ns = 1;
+        for (int b = 0; b < nb; b++)
+            if (d->body_type[b] == MEL_BODY_DEFORMABLE)
+                for (int g = d->body_gp_ptr[b]; g < d->body_gp_ptr[b + 1]; g++)
+                    max_ns = std::max(max_ns, d->gp_sup_ptr[g + 1] - d->gp_sup_ptr[g]);
+        auto bound = [&](int ecap) {
+            const int groups = (MEL_CHUNK_GP + 31) / 32;
+            return mel_chunk_sections(MEL_CHUNK_GP, ecap, std::min(ecap, max_def_nodes),
+                                      std::min(1023, groups * max_ns), mixed ? 8 : 16).bytes;
+        };
         int chosen = -1;
-        for (int ecap : caps) {
-            mel_status rc = mel_build_chunks(d, ecap, CS, mixed);
-            if (rc) return rc;
-            size_t sm = mel_body_smem_bytes(max_def_nodes, CS.img_max, mixed);
-            if (sm <= two_per_sm) { chosen = ecap; break; }
-        }
-        if (chosen < 0) {   // one CTA per SM: largest cap that fits
-            for (int ecap : caps) {
-                mel_status rc = mel_build_chunks(d, ecap, CS, mixed);
-                if (rc) return rc;
-                if (mel_body_smem_bytes(max_def_nodes, CS.img_max, mixed) <= (size_t)smem_blk) { chosen = ecap; break; }
-            }
-        }
+        for (int ecap : caps)
+            if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed) <= two_per_sm) { chosen = ecap; break; }
+        if (chosen < 0)     // one CTA per SM: largest cap that fits
+            for (int ecap : caps)
+                if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed) <= (size_t)smem_blk) { chosen = ecap; break; }
         if (chosen < 0) {
             mel_set_error("deformable body of %d nodes does not fit the body kernel's shared memory", max_def_nodes);
             return MEL_ERR_UNSUPPORTED;
         }
+        mel_status rc = mel_build_chunks(d, chosen, CS, mixed);
+        if (rc) return rc;
         h->chunk_cap = chosen;
     }
     h->nge = (int)CS.n_entries;
@@ -664,6 +674,7 @@ mel_status mel_destroy(mel_handle* h)
         if (p) cudaFree(p);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
+    if (h->ev_prox) cudaEventDestroy(h->ev_prox);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MEL_OK;
@@ -1011,6 +1022,7 @@ struct mel_batch {
     long long launches = 0;
     double ms_last = 0.;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e_step = nullptr;        // end of the last step's launches (members' proximity waits on it)
 };
 
 // Re-uploads the member descriptors and the work prefixes (the stream is idle afterwards).
@@ -1050,6 +1062,43 @@ static mel_status batch_refresh(mel_batch* b)
     return MEL_OK;
 }
 
+// Update_proximity of the members due at this step.  Each runs on its own stream, from its own
+// host thread, after the step's launches (an event on the batch stream); the batch stream then
+// waits for all of them.  The members' pipelines share nothing, so their small kernels and host
+// round trips overlap instead of queueing one behind another.
+static mel_status batch_proximity(mel_batch* b, const std::vector<mel_handle*>& due)
+{
+    MEL_CUDA_OK(cudaEventRecord(b->e_step, b->stream));
+    const size_t n = due.size();
+    std::vector<int> rcs(n, 0), launches(n, 0);
+    std::vector<std::string> msgs(n);
+    std::atomic<size_t> next{ 0 };
+    auto work = [&]() {
+        cudaSetDevice(b->device);
+        for (size_t i = next++; i < n; i = next++) {
+            mel_handle* h = due[i];
+            if (!h->ev_prox) cudaEventCreateWithFlags(&h->ev_prox, cudaEventDisableTiming);
+            cudaStreamWaitEvent(h->stream, b->e_step, 0);
+            int l0 = h->P.launches;
+            rcs[i] = mel_run_proximity(h->d, h->P, h->H, h->stream);
+            launches[i] = h->P.launches - l0;
+            if (rcs[i]) msgs[i] = mel_last_error_string();
+            cudaEventRecord(h->ev_prox, h->stream);
+        }
+    };
+    const size_t nthreads = std::min(n, (size_t)16);
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nthreads; t++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (size_t i = 0; i < n; i++) {
+        if (rcs[i]) { mel_set_error("%s", msgs[i].c_str()); return (mel_status)rcs[i]; }
+        MEL_CUDA_OK(cudaStreamWaitEvent(b->stream, due[i]->ev_prox, 0));
+        b->launches += launches[i];
+    }
+    return MEL_OK;
+}
+
 mel_status mel_batch_create(int device, int precision, mel_batch** out)
 {
     if (!out) { mel_set_error("null output"); return MEL_ERR_INVALID; }
@@ -1063,7 +1112,8 @@ mel_status mel_batch_create(int device, int precision, mel_batch** out)
     b->precision = precision;
     cudaSetDevice(device);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) {
+        cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->e_step, cudaEventDisableTiming) != cudaSuccess) {
         mel_set_cuda_error(cudaGetLastError(), "batch stream", __FILE__, __LINE__);
         delete b;
         return MEL_ERR_CUDA;
@@ -1119,16 +1169,18 @@ mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity)
         b->launches += 3;
         cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) { mel_set_cuda_error(le, "batch step launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+        std::vector<mel_handle*> due;
         for (mel_handle* h : b->members) {
             h->time += h->dt;                                    // Code/Solver.h:86
             if (run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
                 h->next_cup = h->next_cup + h->cup;
-                int l0 = h->P.launches;
-                int rc = mel_run_proximity(h->d, h->P, h->H, b->stream);
-                b->launches += h->P.launches - l0;
-                if (rc) return (mel_status)rc;
-                b->dirty = true;
+                due.push_back(h);
             }
+        }
+        if (!due.empty()) {
+            mel_status rc = batch_proximity(b, due);
+            if (rc) return rc;
+            b->dirty = true;
         }
     }
     cudaEventRecord(b->e1, b->stream);
@@ -1160,7 +1212,7 @@ mel_status mel_batch_destroy(mel_batch* b)
     cudaStreamSynchronize(b->stream);
     for (mel_handle* h : b->members) h->batch = nullptr;
     cudaFree(b->d_devs); cudaFree(b->d_thr0); cudaFree(b->d_cta0);
-    cudaEventDestroy(b->e0); cudaEventDestroy(b->e1);
+    cudaEventDestroy(b->e0); cudaEventDestroy(b->e1); cudaEventDestroy(b->e_step);
     cudaStreamDestroy(b->stream);
     delete b;
     return MEL_OK;

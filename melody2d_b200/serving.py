@@ -85,7 +85,12 @@ def estimate_device_bytes(flat: dict) -> float:
 
 class Server:
     def __init__(self, batched: bool = True, precision: int = 1, device: int = 0, hbm_budget: float = 150e9,
-                 strain: float = 0.05, step_cap: int = 40000, build_workers: int = 8, create_threads: int = 4):
+                 strain: float = 0.05, step_cap: int = 40000, build_workers: int = 8, create_threads: int = 4,
+                 min_batch: int = 1):
+        """min_batch: the batched arm holds admission until that many requests are ready (or no
+        more are on their way), a batching window that trades first-request latency for fuller
+        launches."""
+        self.min_batch = min_batch
         self.batched, self.precision, self.device = batched, precision, device
         self.hbm_budget, self.strain, self.step_cap = hbm_budget, strain, step_cap
         self.build_workers, self.create_threads = build_workers, create_threads
@@ -106,6 +111,7 @@ class Server:
         t0 = time.perf_counter()
         gpu_ms = 0.0
         launches = 0
+        max_resident = 0
         try:
             while True:
                 now = time.perf_counter() - t0
@@ -127,7 +133,9 @@ class Server:
                 ready.sort(key=lambda x: x[0].arrival)
                 # admission: the batched arm takes every ready request that fits the budget; the plain
                 # arm runs one request at a time
-                while ready and (self.batched or not resident):
+                more_coming = nxt < len(reqs) or building or creating
+                hold = self.batched and not resident and len(ready) < self.min_batch and more_coming
+                while ready and not hold and (self.batched or not resident):
                     r, s = ready[0]
                     if self.batched and resident and resident_bytes + r.est_bytes > self.hbm_budget:
                         break
@@ -137,6 +145,7 @@ class Server:
                     resident[r.rid] = (r, s)
                     resident_bytes += r.est_bytes
                     r.admitted = time.perf_counter() - t0
+                max_resident = max(max_resident, len(resident))
                 if resident:
                     if self.batched:
                         batch.step(SLICE)
@@ -192,7 +201,7 @@ class Server:
             "latency_p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
             "mean_steps": float(np.mean([r.target_steps for r in done])) if done else None,
             "mean_nodes": float(np.mean([r.nodes for r in done])) if done else None,
-            "gpu_ms": gpu_ms, "gpu_launches": launches,
+            "gpu_ms": gpu_ms, "gpu_launches": launches, "max_resident": max_resident,
             "requests": [{"rid": r.rid, "seed": r.seed, "arrival": r.arrival, "admitted": r.admitted, "done": r.done,
                           "steps": r.target_steps, "nodes": r.nodes, "kinetic_energy": r.kinetic_energy,
                           "wall_force": r.wall_force} for r in done],

@@ -14,14 +14,12 @@ def test_served_results_match_alone_and_plain(gpu_lib):
     from melody2d_b200.solver import Solver
     arrivals = [0.0, 0.05, 0.1, 0.6, 0.65, 1.2]
     seeds = [900 + i for i in range(len(arrivals))]
-    batched = Server(batched=True, precision=1, step_cap=150, build_workers=3, create_threads=2).run(
-        arrivals, seeds, duration=2.0, drain=120.0)
+    # a batching window of all six requests makes them share the GPU whatever the build times
+    batched = Server(batched=True, precision=1, step_cap=150, build_workers=3, create_threads=2,
+                     min_batch=len(arrivals)).run(arrivals, seeds, duration=2.0, drain=120.0)
     assert batched["completed"] == len(arrivals)
+    assert batched["max_resident"] == len(arrivals)
     rows = {r["seed"]: r for r in batched["requests"]}
-    req = batched["requests"]
-    overlap = any(a["admitted"] < b["done"] and b["admitted"] < a["done"]
-                  for i, a in enumerate(req) for b in req[i + 1:])
-    assert overlap, "requests must share the GPU"
     templates = g.DiscTemplates(range(32, 97), workers=1)
     for seed in seeds:
         sc = g.batch_sample_scene(seed, templates)
