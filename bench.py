@@ -444,11 +444,16 @@ def compare_precisions(args, rank, world, local, pg):
     def rel(x, y):
         x, y = np.asarray(x, float), np.asarray(y, float)
         return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
-    checkpoints = sorted({k for k in (1000, 5000, 10000, 20000, 50000) if k < args.compare_fp64} | {args.compare_fp64})
-    rows, done = [], 0
+    from melody2d_b200.solver import MelError
+    checkpoints = sorted({k for k in range(5000, args.compare_fp64, 5000)} | {1000, args.compare_fp64})
+    rows, done, stopped = [], 0, None
     for k in checkpoints:
-        a.step(k - done)
-        b.step(k - done)
+        try:
+            a.step(k - done)
+            b.step(k - done)
+        except MelError as e:          # the sample diverged (both forms run the same physics)
+            stopped = {"after_steps": done, "error": str(e)}
+            break
         done = k
         ma, mb = a.monitor(), b.monitor()
         rows.append({"steps": k,
@@ -458,7 +463,7 @@ def compare_precisions(args, rank, world, local, pg):
                      "mean_displacement": rel(list(mb.mean_displacement), list(ma.mean_displacement)),
                      "active_contacts": [mb.active_contacts, ma.active_contacts]})
     print(json.dumps({"report": "mixed vs fp64 (relative errors; active_contacts = [mixed, fp64])",
-                      "workload": f"biaxial {args.discs} discs", "rows": rows}), flush=True)
+                      "workload": f"biaxial {args.discs} discs", "rows": rows, "diverged": stopped}), flush=True)
     a.close()
     b.close()
 

@@ -278,8 +278,13 @@ typedef struct mel_batch mel_batch;
 mel_status mel_batch_create(int device, int precision, mel_batch** out);
 mel_status mel_batch_admit(mel_batch* b, mel_handle* h);
 mel_status mel_batch_retire(mel_batch* b, mel_handle* h);
-/* nsteps steps of every member; run_proximity as in mel_step_io.  Returns after the work is done. */
+/* nsteps steps of every member; run_proximity as in mel_step_io.  Returns after the work is done.
+ * A member whose state diverges (MEL_ERR_NAN at its proximity update) or fails a device index check
+ * leaves the batch and the others carry on; mel_get_health reports it. */
 mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity);
+/* *failed = 0 for a healthy handle, else the status that retired it from its batch (the message is
+ * then available from mel_last_error_string). */
+mel_status mel_get_health(mel_handle* h, int* failed);
 /* device time of the last mel_batch_step call (CUDA events), kernels it launched, current members */
 mel_status mel_batch_stats(mel_batch* b, double* ms_last_call, long long* launches, int* members);
 mel_status mel_batch_destroy(mel_batch* b);

@@ -18,6 +18,8 @@ MEL_LAW_NPARAM = 11
 MEL_MAT_NPARAM = 6
 MEL_NINTERNAL = 3
 
+MEL_OK, MEL_ERR_INVALID, MEL_ERR_UNSUPPORTED, MEL_ERR_CUDA, MEL_ERR_OOM, MEL_ERR_NAN, MEL_ERR_BOUNDS, \
+    MEL_ERR_TIMEOUT, MEL_ERR_IO, MEL_ERR_NO_DEVICE = range(10)
 STATUS_NAMES = {0: "MEL_OK", 1: "MEL_ERR_INVALID", 2: "MEL_ERR_UNSUPPORTED", 3: "MEL_ERR_CUDA", 4: "MEL_ERR_OOM",
                 5: "MEL_ERR_NAN", 6: "MEL_ERR_BOUNDS", 7: "MEL_ERR_TIMEOUT", 8: "MEL_ERR_IO", 9: "MEL_ERR_NO_DEVICE"}
 

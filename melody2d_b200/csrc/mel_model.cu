@@ -71,6 +71,8 @@ struct mel_handle {
     int n_def_nodes = 0;
     mel_batch* batch = nullptr;  // batch the handle is a member of (steps only through the batch)
     cudaEvent_t ev_prox = nullptr;  // end of the handle's last proximity update within a batch
+    int failed = 0;                 // model-level failure (MEL_ERR_NAN, MEL_ERR_BOUNDS) that retired it from a batch
+    std::string failed_msg;
 };
 
 template <typename T>
@@ -1092,11 +1094,27 @@ static mel_status batch_proximity(mel_batch* b, const std::vector<mel_handle*>& 
     work();
     for (auto& t : pool) t.join();
     for (size_t i = 0; i < n; i++) {
-        if (rcs[i]) { mel_set_error("%s", msgs[i].c_str()); return (mel_status)rcs[i]; }
+        if (rcs[i] == MEL_ERR_NAN || rcs[i] == MEL_ERR_BOUNDS) {      // this sample diverged: it leaves
+            due[i]->failed = rcs[i];                                    // the batch, the others go on
+            due[i]->failed_msg = msgs[i];
+        } else if (rcs[i]) {
+            mel_set_error("%s", msgs[i].c_str());
+            return (mel_status)rcs[i];
+        }
         MEL_CUDA_OK(cudaStreamWaitEvent(b->stream, due[i]->ev_prox, 0));
         b->launches += launches[i];
     }
     return MEL_OK;
+}
+
+// removes the members marked failed (their state stays as it was when they failed)
+static void batch_drop_failed(mel_batch* b)
+{
+    for (size_t i = 0; i < b->members.size();) {
+        mel_handle* h = b->members[i];
+        if (h->failed) { b->members.erase(b->members.begin() + i); h->batch = nullptr; b->dirty = true; }
+        else i++;
+    }
 }
 
 mel_status mel_batch_create(int device, int precision, mel_batch** out)
@@ -1181,6 +1199,7 @@ mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity)
             mel_status rc = batch_proximity(b, due);
             if (rc) return rc;
             b->dirty = true;
+            batch_drop_failed(b);
         }
     }
     cudaEventRecord(b->e1, b->stream);
@@ -1191,8 +1210,18 @@ mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity)
     b->ms_last = ms;
     for (mel_handle* h : b->members) {
         mel_status rc = check_errors(h);
-        if (rc) return rc;
+        if (rc == MEL_ERR_BOUNDS) { h->failed = rc; h->failed_msg = mel_last_error_string(); }
+        else if (rc) return rc;
     }
+    batch_drop_failed(b);
+    return MEL_OK;
+}
+
+mel_status mel_get_health(mel_handle* h, int* failed)
+{
+    if (!h || !failed) return MEL_ERR_INVALID;
+    *failed = h->failed;
+    if (h->failed) mel_set_error("%s", h->failed_msg.c_str());
     return MEL_OK;
 }
 

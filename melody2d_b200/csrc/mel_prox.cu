@@ -61,8 +61,10 @@ __global__ void aabb_kernel(mel_dev d, double* aabb, int* shmin, int* shmax)
     double dd = d.b_dist[3 * b + 1];
     int n0 = d.b_node0[b];
     double xmin = 1.e100, xmax = -1.e100, ymin = 1.e100, ymax = -1.e100;
+    bool nonfinite = false;          // the comparisons below pass over NaN, so it is tested apart
     for (int e = d.bd_e0[g] + lane; e < d.bd_e0[g + 1]; e += 32) {
         double2 p = d.x[n0 + d.e_node[e]];
+        nonfinite |= !isfinite(p.x) || !isfinite(p.y);
         if (p.x - dd < xmin) xmin = p.x - dd;
         if (p.x + dd > xmax) xmax = p.x + dd;
         if (p.y - dd < ymin) ymin = p.y - dd;
@@ -74,13 +76,14 @@ __global__ void aabb_kernel(mel_dev d, double* aabb, int* shmin, int* shmax)
         ymin = fmin(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
         ymax = fmax(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
     }
+    nonfinite = __any_sync(0xffffffffu, nonfinite);
     if (lane == 0) {
         double invperiod = 1. / d.period;
         double f0 = floor((xmin - d.xmin) * invperiod), f1 = floor((xmax - d.xmin) * invperiod);
         // a box that is not finite, or that spans more periods than any body can, comes from a
         // diverged state; it is reported and left out of the neighbour search, whose shift loop
         // it would otherwise drive through billions of iterations
-        bool finite = isfinite(xmin) && isfinite(xmax) && isfinite(ymin) && isfinite(ymax);
+        bool finite = !nonfinite && isfinite(xmin) && isfinite(xmax) && isfinite(ymin) && isfinite(ymax);
         bool sane = finite && fabs(f0) < 1.e6 && fabs(f1) < 1.e6 && f1 - f0 <= MEL_MAX_SHIFT_SPAN;
         if (!sane) {
             atomicOr(&d.err[MEL_E_NAN], finite ? 2u : 1u);

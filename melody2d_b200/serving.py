@@ -39,6 +39,7 @@ class Request:
     steps: int = 0
     kinetic_energy: float = 0.0
     wall_force: Optional[List[float]] = None
+    failed: str = ""             # why the run stopped early (diverged state), empty when it completed
 
 
 def poisson_arrivals(rate: float, duration: float, seed: int) -> List[float]:
@@ -96,7 +97,8 @@ class Server:
         self.build_workers, self.create_threads = build_workers, create_threads
 
     def run(self, arrivals: List[float], seeds: List[int], duration: float, drain: float = 0.0) -> Dict:
-        from melody2d_b200.solver import Batch, Solver
+        from melody2d_b200.solver import Batch, MelError, Solver
+        from melody2d_b200.abi import MEL_ERR_NAN, MEL_ERR_BOUNDS
         reqs = [Request(i, s, a) for i, (a, s) in enumerate(zip(arrivals, seeds))]
         ctx = mp.get_context("spawn")
         pool = ProcessPoolExecutor(max_workers=self.build_workers, mp_context=ctx, initializer=_init_worker,
@@ -147,18 +149,31 @@ class Server:
                     r.admitted = time.perf_counter() - t0
                 max_resident = max(max_resident, len(resident))
                 if resident:
+                    failed = []
                     if self.batched:
-                        batch.step(SLICE)
+                        failed = batch.step(SLICE)
                         st = batch.stats()
                         gpu_ms += st["ms_last_call"]
                         launches += st["launches"]
                     else:
                         (r, s), = resident.values()
-                        s.step(SLICE)
+                        try:
+                            s.step(SLICE)
+                        except MelError as e:
+                            if e.code not in (MEL_ERR_NAN, MEL_ERR_BOUNDS):
+                                raise
+                            failed = [s]
                         gpu_ms += s.step_stats()["ms_total"]
                         launches += s.kernel_times()["launches"]
                     for rid in list(resident):
                         r, s = resident[rid]
+                        if s in failed:                  # the sample diverged: it stops here
+                            r.failed = s.health()[1] if self.batched else "diverged"
+                            s.close()
+                            del resident[rid]
+                            resident_bytes -= r.est_bytes
+                            r.done = time.perf_counter() - t0
+                            continue
                         r.steps += SLICE
                         if r.steps >= r.target_steps:
                             if self.batched:
@@ -189,13 +204,15 @@ class Server:
                     f.result().close()
             pool.shutdown(wait=False, cancel_futures=True)
         wall = time.perf_counter() - t0
-        done = [r for r in reqs if r.done >= 0]
+        failed = [r for r in reqs if r.done >= 0 and r.failed]
+        done = [r for r in reqs if r.done >= 0 and not r.failed]
         lat = np.array([r.done - r.arrival for r in done])
         arrived = [r for r in reqs if r.arrival <= duration]
         return {
             "arm": "batched" if self.batched else "plain",
             "precision": "mixed" if self.precision == 1 else "fp64",
-            "arrived": len(arrived), "completed": len(done), "in_flight_at_end": len(arrived) - len(done),
+            "arrived": len(arrived), "completed": len(done), "failed": len(failed),
+            "in_flight_at_end": len(arrived) - len(done) - len(failed),
             "wall_s": wall, "samples_per_hour": len(done) * 3600.0 / wall,
             "latency_p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
             "latency_p99_s": float(np.percentile(lat, 99)) if len(lat) else None,

@@ -58,6 +58,7 @@ SIGNATURES = {
     "mel_batch_step": [_vp, C.c_int, C.c_int],
     "mel_batch_stats": [_vp, _dp, C.POINTER(C.c_longlong), _ip],
     "mel_batch_destroy": [_vp],
+    "mel_get_health": [_vp, _ip],
 }
 
 
@@ -200,6 +201,13 @@ class Solver:
         buf = abi.numpy_to_contacts(arr)
         _check(lib().mel_set_contacts(self.h, buf, len(arr)))
 
+    def health(self):
+        """(0, "") for a healthy solver, else (status, message) of the failure that retired it
+        from its batch."""
+        f = C.c_int()
+        _check(lib().mel_get_health(self.h, C.byref(f)))
+        return f.value, (lib().mel_last_error_string().decode(errors="replace") if f.value else "")
+
     def time(self):
         t = C.c_double(); dt = C.c_double()
         _check(lib().mel_get_time(self.h, C.byref(t), C.byref(dt)))
@@ -315,8 +323,14 @@ class Batch:
         _check(lib().mel_batch_retire(self.b, s.h))
         self.members.remove(s)
 
-    def step(self, n: int = 1, proximity: bool = True):
+    def step(self, n: int = 1, proximity: bool = True) -> list:
+        """Advances every member; returns the members that diverged during the call (they have
+        left the batch; `Solver.health()` gives the reason)."""
         _check(lib().mel_batch_step(self.b, int(n), 1 if proximity else 0))
+        failed = [s for s in self.members if s.health()[0]]
+        for s in failed:
+            self.members.remove(s)
+        return failed
 
     def stats(self) -> dict:
         ms, launches, members = C.c_double(), C.c_longlong(), C.c_int()

@@ -69,3 +69,30 @@ def test_batch_member_cannot_step_alone(gpu_lib):
         Batch(precision=1).admit(s)
     b.close()
     s.step(1)                       # free again once the batch is gone
+
+
+def test_diverged_member_leaves_batch(gpu_lib):
+    """A member whose state runs away (one border node's parameter moved 1 km: finite values, and
+    no kernel derives an index from a position) is reported by its next proximity update and
+    leaves the batch; the other members carry on exactly as they would alone."""
+    from melody2d_b200.abi import MEL_ERR_NAN
+    from melody2d_b200.solver import Batch, Solver
+    flats = samples()
+    alone = [Solver.from_flat(f) for f in flats]
+    mixed = [Solver.from_flat(f) for f in flats]
+    b = Batch()
+    for s in mixed:
+        b.admit(s)
+    b.step(40)
+    st = mixed[1].node_state()
+    st[5, 6] += 1.0e3                       # nodal parameter up x of one border node
+    mixed[1].set_node_state(st)
+    failed = b.step(30)
+    assert failed == [mixed[1]]
+    code, msg = mixed[1].health()
+    assert code == MEL_ERR_NAN and ("periods" in msg or "non-finite" in msg), msg
+    assert b.stats()["members"] == 2
+    for i in (0, 2):
+        alone[i].step(70)
+        assert_same(state(alone[i]), state(mixed[i]))
+    b.close()
