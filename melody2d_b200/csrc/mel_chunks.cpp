@@ -2,7 +2,7 @@
 // index order; within a chunk they are stored row by row in groups of up to 32 slots sorted by
 // support count, and the pull records list, for every touched node, the positions of its entries
 // in ascending Gauss-point order (the order Body::Update_internal_forces accumulates them in,
-// Code/Body.h:960-1050).
+// Code/Body.h:960-1050), in rows of up to 32 nodes sorted by entry count.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -18,7 +18,10 @@ struct slot_plan {
     std::vector<int> first_row;  // per slot: start of its group's row table in roff
     std::vector<int> lane;       // per slot: lane within its group
     std::vector<int> roff;       // row tables: entry offset of row k of a group
+    std::vector<int> rsw;        // per row: lane swizzle (XOR, 0..7)
     int entries = 0;
+    // stored position of entry k of slot s
+    int pos(int s, int k) const { const int r = first_row[s] + k; return roff[r] + (lane[s] ^ rsw[r]); }
 };
 
 slot_plan plan_slots(const int* ns, int n)
@@ -38,6 +41,12 @@ slot_plan plan_slots(const int* ns, int n)
             P.roff.push_back(P.entries);
             int mk = 0;                             // slots with more than k supports: a prefix
             while (mk < m && ns[P.order[s0 + mk]] > k) mk++;
+            // rows whose width is a multiple of 8 rotate the lanes' bank groups from row to row
+            // (lane ^ (k & 7) stays inside its aligned block of 8, so the row stays a permutation
+            // of consecutive entries); otherwise all entries of a point would share one bank
+            // group, and the pull, whose lanes read entries of points shared by nearby nodes,
+            // would meet them in the same bank
+            P.rsw.push_back(mk % 8 == 0 ? (k & 7) : 0);
             P.entries += mk;
         }
     }
@@ -71,6 +80,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
         out.b_chunk0[b] = (int)out.chunks.size();
         if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
         const int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+        if (nnb > 4096) { mel_set_error("deformable body %d has %d nodes (pull records hold 12-bit node indices)", b, nnb); return MEL_ERR_UNSUPPORTED; }
         int g = d->body_gp_ptr[b];
         const int g1 = d->body_gp_ptr[b + 1];
         while (g < g1) {
@@ -90,6 +100,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 ngp++;
             }
             if (ngp == 0) { mel_set_error("Gauss point %d has more supports than a chunk holds", g); return MEL_ERR_UNSUPPORTED; }
+            if (nent > 4096) { mel_set_error("chunk entry cap %d above 4096", ecap); return MEL_ERR_INVALID; }
             const slot_plan P = plan_slots(ns.data(), ngp);
             mel_chunk ch;
             memset(&ch, 0, sizeof ch);
@@ -104,17 +115,47 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 for (int k = 0, j = d->gp_sup_ptr[gg]; j < d->gp_sup_ptr[gg + 1]; k++, j++) {
                     int v = d->gp_sup_idx[j];
                     if (v < 0 || v >= nnb) { mel_set_error("Gauss support index out of range"); return MEL_ERR_INVALID; }
-                    tp.push_back({ ((long long)v << 32) | (long long)t, P.roff[P.first_row[slot] + k] + P.lane[slot] });
+                    tp.push_back({ ((long long)v << 32) | (long long)t, P.pos(slot, k) });
                 }
             }
             std::sort(tp.begin(), tp.end());
-            std::vector<uint32_t> tn;
+            // touched nodes: (first entry in tp, count), then pull slots sorted by count
+            std::vector<std::pair<int, int>> tnodes;
             for (int q = 0; q < P.entries; q++)
-                if (q == 0 || (tp[q].first >> 32) != (tp[q - 1].first >> 32))
-                    tn.push_back((uint32_t)(tp[q].first >> 32) | ((uint32_t)q << 16));
-            ch.ntn = (int)tn.size();
-            tn.push_back(0xffffu | ((uint32_t)P.entries << 16));
-            const int nroff = (int)P.roff.size();
+                if (q == 0 || (tp[q].first >> 32) != (tp[q - 1].first >> 32)) tnodes.push_back({ q, 1 });
+                else tnodes.back().second++;
+            std::stable_sort(tnodes.begin(), tnodes.end(),
+                             [](const std::pair<int, int>& a, const std::pair<int, int>& b) { return a.second > b.second; });
+            ch.ntn = (int)tnodes.size();
+            // pull row tables after the point groups' rows: row j of a pull group holds entry j of
+            // every slot with more than j entries (a prefix of the group)
+            std::vector<int> roff_all(P.roff);
+            std::vector<int> rsw_all(P.rsw);
+            std::vector<uint32_t> tn(ch.ntn);
+            std::vector<uint16_t> tposv(P.entries);
+            int pe = 0;
+            for (int s0 = 0; s0 < ch.ntn; s0 += 32) {
+                const int m = std::min(32, ch.ntn - s0);
+                const int K = tnodes[s0].second;
+                const int r0 = (int)roff_all.size();
+                for (int j = 0; j < K; j++) {
+                    roff_all.push_back(pe);
+                    rsw_all.push_back(0);
+                    int mj = 0;
+                    while (mj < m && tnodes[s0 + mj].second > j) mj++;
+                    for (int l = 0; l < mj; l++) tposv[pe + l] = (uint16_t)tp[tnodes[s0 + l].first + j].second;
+                    pe += mj;
+                }
+                for (int l = 0; l < m; l++) {
+                    const int node = (int)(tp[tnodes[s0 + l].first].first >> 32);
+                    tn[s0 + l] = (uint32_t)node | ((uint32_t)tnodes[s0 + l].second << 12) | ((uint32_t)r0 << 20);
+                }
+            }
+            const int nroff = (int)roff_all.size();
+            if (nroff > 4095 || pe != P.entries) {
+                mel_set_error("chunk row tables too large (%d rows)", nroff);
+                return MEL_ERR_UNSUPPORTED;
+            }
             const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn, nroff, mixed ? 8 : 16);
             ch.bytes = L.bytes;
             ch.img = (long long)out.img.size();
@@ -136,15 +177,15 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 c0[slot] = d->gp_weight[gg] * d->gp_jacobian[gg];   // c0 of Code/Body.h:994
                 gpm[slot] = (uint32_t)P.first_row[slot] | ((uint32_t)P.lane[slot] << 10) | ((uint32_t)c << 15);
                 for (int k = 0, j = d->gp_sup_ptr[gg]; k < c; k++, j++) {
-                    int e = P.roff[P.first_row[slot] + k] + P.lane[slot];
+                    int e = P.pos(slot, k);
                     idx[e] = (uint16_t)d->gp_sup_idx[j];
                     if (mixed) { dNf[2 * e] = (float)d->gp_dNdx[j]; dNf[2 * e + 1] = (float)d->gp_dNdy[j]; }
                     else { dN[2 * e] = d->gp_dNdx[j]; dN[2 * e + 1] = d->gp_dNdy[j]; }
                 }
             }
-            for (int q = 0; q < P.entries; q++) tpos[q] = (uint16_t)tp[q].second;
+            for (int q = 0; q < P.entries; q++) tpos[q] = tposv[q];
             memcpy(tnr, tn.data(), sizeof(uint32_t) * tn.size());
-            for (int r = 0; r < nroff; r++) roff[r] = (uint16_t)P.roff[r];
+            for (int r = 0; r < nroff; r++) roff[r] = (uint16_t)(roff_all[r] | (rsw_all[r] << 12));
             out.img_max = std::max(out.img_max, ch.bytes);
             out.n_entries += ch.ne;
             out.n_pad += ch.ne - P.entries;

@@ -30,17 +30,22 @@ enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3,
 //   dN       ne x double2          dN/dx, dN/dy of every stored entry (float2 in the images of
 //                                  the mixed-precision pass)
 //   idx      ne x uint16           body-local support node of each entry
-//   tpos     ne x uint16           entry positions sorted by (node, Gauss point): the pull order
+//   tpos     ne x uint16           entry positions in pull order, in pull rows (below)
 //   c0       ngp2 x double         weight x jacobian of each point slot (ngp2 = ngp rounded to 2)
 //   gpm      ngp4 x uint32         point slot: row table start | lane << 10 | support count << 15
-//   tn       tn4 x uint32          touched node | first tpos << 16, ntn + 1 records (the last
-//                                  one closes the final range)
-//   roff     nroff8 x uint16       row tables of the slot groups
+//   tn       tn4 x uint32          pull slot: node | entry count << 12 | row table start << 20
+//   roff     nroff8 x uint16       row tables: the point groups' rows, then the pull groups'
+//                                  rows; each value is an offset (12 bits) | lane swizzle << 12
 // Point slots: the chunk's points sorted by (support count descending, index), cut into groups of
 // up to 32 slots, one warp each.  Row k of a group holds entry k of every slot whose point has
 // more than k supports; these slots are a prefix of the group, so entry k of lane j sits at
-// roff[r0 + k] + j and the lanes of a warp touch consecutive entries.  ne is the number of
-// entries rounded up to a multiple of 8 (zero entries at the end).
+// (r & 0xfff) + (j ^ (r >> 12)) with r = roff[r0 + k]: the lanes of a warp touch a permutation of
+// consecutive entries.  The swizzle (k & 7 in rows whose width is a multiple of 8, else 0) spreads
+// the entries of one point over the shared-memory bank groups.
+// Pull slots: the touched nodes sorted by entry count (descending), cut into groups of 32 (slot t
+// is lane t & 31 of group t >> 5).  Row j of a pull group holds, for every slot with more than j
+// entries, the position of its node's entry j; a node's entries are in ascending point order.
+// ne is the number of entries rounded up to a multiple of 8 (zero entries at the end).
 struct mel_chunk {        // one chunk of a body's Gauss points
     long long img;        // byte offset of the image in mel_dev::img
     int bytes;            // image size (multiple of 16)
@@ -62,7 +67,7 @@ __host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, 
     L.c0 = L.tpos + 2 * ne;
     L.gpm = L.c0 + 8 * ((ngp + 1) & ~1);
     L.tn = L.gpm + 4 * ((ngp + 3) & ~3);
-    L.roff = L.tn + 4 * ((ntn + 1 + 3) & ~3);
+    L.roff = L.tn + 4 * ((ntn + 3) & ~3);
     L.bytes = L.roff + 2 * ((nroff + 7) & ~7);
     return L;
 }

@@ -317,6 +317,8 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 // barrier of the Gauss-point warps only (warp 7 runs the contact scatter meanwhile)
 __device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, %0;" :: "n"(MEL_BODY_CTHREADS) : "memory"); }
+// barrier of warps 1-7 in the body tail (warp 0 sums the works meanwhile)
+__device__ __forceinline__ void tail_sync() { asm volatile("bar.sync 2, %0;" :: "n"(MEL_BODY_THREADS - 32) : "memory"); }
 __device__ __forceinline__ unsigned long long global_ns()
 {
     unsigned long long t;
@@ -351,12 +353,16 @@ __device__ __forceinline__ double ordered_sum(double acc, const double* t, int n
     return acc;
 }
 
+// position of the entry of `lane` in a row whose table value is r (offset | swizzle << 12)
+__device__ __forceinline__ int mel_entry(unsigned r, int lane) { return (int)(r & 0xfffu) + (lane ^ (int)(r >> 12)); }
+
 // Gauss-point pass of one chunk held in shared memory (Body::Update_internal_forces,
 // Code/Body.h:960-1050): thread `t` < ngp forms the strain of its point from the staged dN and
 // the body's displacements (supports in the point's own order), applies the material and
 // overwrites its dN pairs with the contributions c0 * B^T.sigma.  Entry k of slot t sits at
-// row[k] + lane (row layout: the lanes of a warp touch consecutive entries).
-__device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double Lam, const double2* s_up,
+// mel_entry(row[k], lane) (row layout: the lanes of a warp touch a permutation of consecutive
+// entries).
+__device__ __forceinline__ void chunk_points(int t, int ngp, int mtype, double Mu, double Lam, const double2* s_up,
                                              double2* s_p, const uint16_t* s_idx, const double* s_c0,
                                              const unsigned* s_gpm, const uint16_t* s_roff)
 {
@@ -364,11 +370,31 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
     const uint16_t* row = s_roff + (gm & 0x3ffu);          // row table of the slot's group
     const int lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
     const double c0 = s_c0[t];
-#define E(k) (row[(k)] + lane)
+    // rows that every slot of a full group has are 32 wide and contiguous: their positions follow
+    // from the group's first row without a table load (swizzle k & 7)
+    const int nfull = (t | 31) < ngp ? (int)(s_gpm[t | 31] >> 15) : 0;
+    const int base = (int)(row[0] & 0xfffu);
+#define E(k) ((k) < nfull ? base + 32 * (k) + (lane ^ ((k) & 7)) : mel_entry(row[(k)], lane))
     if (mtype == MEL_MAT_ELASTIC_LINEAR) {
-        // strain sums in support order; loads issued four supports ahead of the adds
+        // strain sums in support order; loads issued eight supports ahead of the adds.  Rows below
+        // nfull are addressed without the row table (k is a multiple of 8 there, so the swizzle
+        // of row k + j is j).
         double E11 = 0., E12 = 0., E22 = 0.;
         int k = 0;
+        for (; k + 8 <= nfull; k += 8) {
+            double2 dN[8], u[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int e = base + 32 * (k + j) + (lane ^ j);
+                dN[j] = s_p[e]; u[j] = s_up[s_idx[e]];
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                E11 = E11 + dN[j].x * u[j].x;
+                E12 = E12 + (dN[j].x * u[j].y + dN[j].y * u[j].x);
+                E22 = E22 + dN[j].y * u[j].y;
+            }
+        }
         for (; k + 4 <= ns; k += 4) {
             double2 dN[4], u[4];
 #pragma unroll
@@ -392,13 +418,26 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
         double S33 = Lam * (J - 1.);
         double Mu2 = 2 * Mu;
         double S11 = S33 + Mu2 * E11, S22 = S33 + Mu2 * E22, S12 = Mu2 * E12;
+        int k2 = 0;
+        for (; k2 + 8 <= nfull; k2 += 8) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int e = base + 32 * (k2 + j) + (lane ^ j);
+                const double2 dN = s_p[e];
+                double2 q;
+                q.x = c0 * (dN.x * S11 + dN.y * S12);
+                q.y = c0 * (dN.y * S22 + dN.x * S12);
+                s_p[e] = q;
+            }
+        }
 #pragma unroll 4
-        for (int k2 = 0; k2 < ns; k2++) {
-            double2 dN = s_p[E(k2)];
+        for (; k2 < ns; k2++) {
+            const int e = E(k2);
+            const double2 dN = s_p[e];
             double2 q;
             q.x = c0 * (dN.x * S11 + dN.y * S12);
             q.y = c0 * (dN.y * S22 + dN.x * S12);
-            s_p[E(k2)] = q;
+            s_p[e] = q;
         }
     } else {
         double F11 = 1., F12 = 0., F21 = 0., F22 = 1.;
@@ -428,13 +467,12 @@ __device__ __forceinline__ void chunk_points(int t, int mtype, double Mu, double
         }
     }
 }
-#undef E
 
 // Gauss-point pass of the mixed-precision form: dN pairs stored in FP32, strain, stress and the
 // contributions computed in FP32 (with fused multiply-adds), displacements gathered in FP32 as
 // differences to the body's first node (taken in FP64: sum_j dN_j = 0, so the body's rigid
 // translation cancels exactly and does not eat the FP32 mantissa).  Nodal force sums stay FP64.
-__device__ __forceinline__ void chunk_points_mx(int t, int mtype, float Mu, float Lam, const float2* s_upf,
+__device__ __forceinline__ void chunk_points_mx(int t, int ngp, int mtype, float Mu, float Lam, const float2* s_upf,
                                                 float2* s_p, const uint16_t* s_idx, const double* s_c0,
                                                 const unsigned* s_gpm, const uint16_t* s_roff)
 {
@@ -442,11 +480,28 @@ __device__ __forceinline__ void chunk_points_mx(int t, int mtype, float Mu, floa
     const uint16_t* row = s_roff + (gm & 0x3ffu);
     const int lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
     const float c0 = (float)s_c0[t];
+    const int nfull = (t | 31) < ngp ? (int)(s_gpm[t | 31] >> 15) : 0;   // as in chunk_points
+    const int base = (int)(row[0] & 0xfffu);
     if (mtype == MEL_MAT_ELASTIC_LINEAR) {
         float E11 = 0.f, E12 = 0.f, E22 = 0.f;
+        int k = 0;
+        for (; k + 8 <= nfull; k += 8) {
+            float2 dN[8], u[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int e = base + 32 * (k + j) + (lane ^ j);
+                dN[j] = s_p[e]; u[j] = s_upf[s_idx[e]];
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                E11 = __fmaf_rn(dN[j].x, u[j].x, E11);
+                E12 = __fmaf_rn(dN[j].x, u[j].y, __fmaf_rn(dN[j].y, u[j].x, E12));
+                E22 = __fmaf_rn(dN[j].y, u[j].y, E22);
+            }
+        }
 #pragma unroll 4
-        for (int k = 0; k < ns; k++) {
-            const int e = row[k] + lane;
+        for (; k < ns; k++) {
+            const int e = E(k);
             const float2 dN = s_p[e];
             const float2 u = s_upf[s_idx[e]];
             E11 = __fmaf_rn(dN.x, u.x, E11);
@@ -457,16 +512,25 @@ __device__ __forceinline__ void chunk_points_mx(int t, int mtype, float Mu, floa
         const float S33 = Lam * (E11 + E22);      // Apply_Elastic_Linear (Code/Model.h:19-29), J - 1 = tr E
         const float Mu2 = 2.f * Mu;
         const float S11 = __fmaf_rn(Mu2, E11, S33), S22 = __fmaf_rn(Mu2, E22, S33), S12 = Mu2 * E12;
+        int k2 = 0;
+        for (; k2 + 8 <= nfull; k2 += 8) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int e = base + 32 * (k2 + j) + (lane ^ j);
+                const float2 dN = s_p[e];
+                s_p[e] = make_float2(c0 * __fmaf_rn(dN.x, S11, dN.y * S12), c0 * __fmaf_rn(dN.y, S22, dN.x * S12));
+            }
+        }
 #pragma unroll 4
-        for (int k = 0; k < ns; k++) {
-            const int e = row[k] + lane;
+        for (; k2 < ns; k2++) {
+            const int e = E(k2);
             const float2 dN = s_p[e];
             s_p[e] = make_float2(c0 * __fmaf_rn(dN.x, S11, dN.y * S12), c0 * __fmaf_rn(dN.y, S22, dN.x * S12));
         }
     } else {
         float G11 = 0.f, G12 = 0.f, G21 = 0.f, G22 = 0.f;   // F - I
         for (int k = 0; k < ns; k++) {
-            const int e = row[k] + lane;
+            const int e = E(k);
             const float2 dN = s_p[e];
             const float2 u = s_upf[s_idx[e]];
             G11 = __fmaf_rn(dN.x, u.x, G11); G12 = __fmaf_rn(dN.y, u.x, G12);
@@ -487,13 +551,15 @@ __device__ __forceinline__ void chunk_points_mx(int t, int mtype, float Mu, floa
         const float S22 = (F11 * (F11 * s22 - F21 * s12) - F21 * (F11 * s12 - F21 * s11)) * invJ;
         const float S12 = (F21 * (F12 * s12 - F22 * s11) - F11 * (F12 * s22 - F22 * s12)) * invJ;
         for (int k = 0; k < ns; k++) {
-            const int e = row[k] + lane;
+            const int e = E(k);
             const float2 dN = s_p[e];
             s_p[e] = make_float2(c0 * (dN.x * (F11 * S11 + F12 * S12) + dN.y * (F12 * S22 + F11 * S12)),
                                  c0 * (dN.x * (F21 * S11 + F22 * S12) + dN.y * (F22 * S22 + F21 * S12)));
         }
     }
 }
+
+#undef E
 
 // Shared memory of a deformable body (n nodes, staging buffers of img_cap bytes each):
 //   s_up, s_f, s_fc        3 x n double2       displacements, internal forces, contact forces
@@ -568,48 +634,78 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
             const uint16_t* s_idx = reinterpret_cast<const uint16_t*>(bk + L.idx);
             const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
             const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
+            const uint16_t* s_roff = reinterpret_cast<const uint16_t*>(bk + L.roff);
             if (tid < hdr.x) {
                 if (MX)
-                    chunk_points_mx(tid, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN), s_idx,
+                    chunk_points_mx(tid, hdr.x, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN), s_idx,
                                     reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
                                     reinterpret_cast<const uint16_t*>(bk + L.roff));
                 else
-                    chunk_points(tid, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN), s_idx,
+                    chunk_points(tid, hdr.x, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN), s_idx,
                                  reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
                                  reinterpret_cast<const uint16_t*>(bk + L.roff));
             }
             compute_sync();
             if (*s_abort) break;
             // pull: each touched node subtracts its contributions in ascending Gauss-point order
-            // (the mixed form adds its FP32 contributions in FP64)
+            // (the mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31
+            // of group t >> 5 (t = tid + 224 i keeps the lane), its entry j at row j of the
+            // group's row table.
             for (int t = tid; t < hdr.z; t += MEL_BODY_CTHREADS) {
-                const unsigned r0 = s_tn[t], r1 = s_tn[t + 1];
-                const int node = (int)(r0 & 0xffffu);
-                const int q1 = (int)(r1 >> 16);
+                const unsigned rec = s_tn[t];
+                const int node = (int)(rec & 0xfffu);
+                const int cnt = (int)((rec >> 12) & 0xffu);
+                const uint16_t* prow = s_roff + (rec >> 20);
+                // rows every slot of a full group has: 32 wide and contiguous
+                const int pfull = (t | 31) < hdr.z ? (int)((s_tn[t | 31] >> 12) & 0xffu) : 0;
+                const int pbase = prow[0];
+#define PQ(j) ((j) < pfull ? pbase + 32 * (j) + lane : prow[(j)] + lane)
                 double2 f = s_f[node];
-                int q = (int)(r0 >> 16);
+                int j = 0;
                 if (MX) {
                     const float2* s_q = reinterpret_cast<const float2*>(bk + L.dN);
-                    for (; q < q1; q++) {
-                        const float2 c = s_q[s_tpos[q]];
+                    for (; j + 8 <= pfull; j += 8) {
+                        float2 c[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[pbase + 32 * (j + i) + lane]];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                    }
+                    for (; j + 4 <= cnt; j += 4) {
+                        float2 c[4];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) c[i] = s_q[s_tpos[PQ(j + i)]];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                    }
+                    for (; j < cnt; j++) {
+                        const float2 c = s_q[s_tpos[PQ(j)]];
                         f.x = f.x - (double)c.x;
                         f.y = f.y - (double)c.y;
                     }
                 } else {
                     const double2* s_p = reinterpret_cast<const double2*>(bk + L.dN);
-                    for (; q + 4 <= q1; q += 4) {
+                    for (; j + 8 <= pfull; j += 8) {
+                        double2 c[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[pbase + 32 * (j + i) + lane]];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                    }
+                    for (; j + 4 <= cnt; j += 4) {
                         double2 c[4];
 #pragma unroll
-                        for (int j = 0; j < 4; j++) c[j] = s_p[s_tpos[q + j]];
+                        for (int i = 0; i < 4; i++) c[i] = s_p[s_tpos[PQ(j + i)]];
 #pragma unroll
-                        for (int j = 0; j < 4; j++) { f.x = f.x - c[j].x; f.y = f.y - c[j].y; }
+                        for (int i = 0; i < 4; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
                     }
-                    for (; q < q1; q++) {
-                        double2 c = s_p[s_tpos[q]];
+                    for (; j < cnt; j++) {
+                        const double2 c = s_p[s_tpos[PQ(j)]];
                         f.x = f.x - c.x;
                         f.y = f.y - c.y;
                     }
                 }
+#undef PQ
                 s_f[node] = f;
             }
             fence_proxy_async();
@@ -740,11 +836,13 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
     }
     __syncthreads();
     if (warp == 0) {
-        // works (internal, body, dirichlet, neumann, damping, alid), summed in node order
+        // works (internal, body, dirichlet, neumann, damping, alid), summed in node order; these
+        // serial sums are the body's last work for warp 0, and they overlap the kinematics below
         if (lane < 6) {
             const int w = lane == 0 ? 0 : lane + 1;       // works slots 0, 2, 3, 4, 5, 6
             d.works[7 * b + w] = ordered_sum(d.works[7 * b + w], s_T + (size_t)lane * n, n, 1);
         }
+        return;
     } else {
         // ---- Apply_Euler (Code/Node.h:239-245) ---------------------------------------------
         for (int i = tid - 32; i < n; i += blockDim.x - 32) {
@@ -756,9 +854,9 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
             d.ap[gi] = ap; d.vp[gi] = vp; d.up[gi] = up;
         }
     }
-    __syncthreads();
+    tail_sync();      // warps 1-7: Euler done
     // ---- Update_kinematics + Update_current_positions (Code/Body.h:2176-2227, 2272-2283) --
-    for (int i = tid; i < n; i += blockDim.x) {
+    for (int i = tid - 32; i < n; i += blockDim.x - 32) {
         int gi = n0 + i;
         double dx = 0., dy = 0., vx = 0., vy = 0., ax = 0., ay = 0.;
         const int j0 = d.sup_ptr[gi], j1 = d.sup_ptr[gi + 1];

@@ -407,15 +407,27 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         // the cap is chosen from an upper bound of the image size (a chunk holds at most ecap
         // entries, MEL_CHUNK_GP points, min(ecap, nodes) touched nodes and one row per support
         // of each group's largest point), so the images are built once
-        int max_ns = 1;
+        // Pull rows: the first pull group has at most (the most points any node supports) rows,
+        // and each later group at most its predecessor's smallest count, so all later groups
+        // together at most ecap / 32.
+        int max_ns = 1, max_use = 1;
+        std::vector<int> use;
         for (int b = 0; b < nb; b++)
-            if (d->body_type[b] == MEL_BODY_DEFORMABLE)
-                for (int g = d->body_gp_ptr[b]; g < d->body_gp_ptr[b + 1]; g++)
+            if (d->body_type[b] == MEL_BODY_DEFORMABLE) {
+                use.assign(d->body_node_ptr[b + 1] - d->body_node_ptr[b], 0);
+                for (int g = d->body_gp_ptr[b]; g < d->body_gp_ptr[b + 1]; g++) {
                     max_ns = std::max(max_ns, d->gp_sup_ptr[g + 1] - d->gp_sup_ptr[g]);
+                    for (int j = d->gp_sup_ptr[g]; j < d->gp_sup_ptr[g + 1]; j++) {
+                        const int v = d->gp_sup_idx[j];
+                        if (v >= 0 && v < (int)use.size()) max_use = std::max(max_use, ++use[v]);
+                    }
+                }
+            }
         auto bound = [&](int ecap) {
             const int groups = (MEL_CHUNK_GP + 31) / 32;
+            const int pull_rows = std::min(max_use, MEL_CHUNK_GP) + ecap / 32;
             return mel_chunk_sections(MEL_CHUNK_GP, ecap, std::min(ecap, max_def_nodes),
-                                      std::min(1023, groups * max_ns), mixed ? 8 : 16).bytes;
+                                      std::min(1023, groups * max_ns) + pull_rows, mixed ? 8 : 16).bytes;
         };
         int chosen = -1;
         for (int ecap : caps)

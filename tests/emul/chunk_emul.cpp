@@ -60,7 +60,13 @@ extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const dou
                 const uint32_t gm = sgpm[t];
                 const int r0 = (int)(gm & 0x3ffu), lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
                 if (r0 + ns > hdr[3] || lane != t % 32) return 4;
-                auto E = [&](int k) { return (int)sroff[r0 + k] + lane; };
+                // the kernel computes the positions of rows every slot of a full group has; they
+                // must agree with the row table
+                const int nfull = (t | 31) < hdr[0] ? (int)(sgpm[t | 31] >> 15) : 0;
+                const int base = (int)(sroff[r0] & 0xfffu);
+                auto Et = [&](int k) { const unsigned r = sroff[r0 + k]; return (int)(r & 0xfffu) + (lane ^ (int)(r >> 12)); };
+                for (int k = 0; k < nfull && k < ns; k++) if (base + 32 * k + (lane ^ (k & 7)) != Et(k)) return 10;
+                auto E = [&](int k) { return k < nfull ? base + 32 * k + (lane ^ (k & 7)) : Et(k); };
                 for (int k = 0; k < ns; k++) if (E(k) >= ne || sidx[E(k)] >= n) return 5;
                 const double c0 = sc0[t];
                 auto U = [&](int k) { int i = sidx[E(k)]; return std::make_pair(up[2 * (n0 + i)], up[2 * (n0 + i) + 1]); };
@@ -85,12 +91,19 @@ extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const dou
                 }
             }
             for (int t = 0; t < hdr[2]; t++) {
-                const uint32_t r0 = stn[t], r1 = stn[t + 1];
-                const int node = (int)(r0 & 0xffffu);
-                if (node >= n || (r0 >> 16) > (r1 >> 16) || (int)(r1 >> 16) > ne) return 7;
+                const uint32_t rec = stn[t];
+                const int node = (int)(rec & 0xfffu), cnt = (int)((rec >> 12) & 0xffu), pr = (int)(rec >> 20);
+                const int lane = t & 31;
+                if (node >= n || cnt == 0 || pr + cnt > hdr[3]) return 7;
+                // counts descend within a group, so slots with more than j entries are a prefix
+                if ((t & 31) && ((int)((stn[t - 1] >> 12) & 0xffu) < cnt || (int)(stn[t - 1] >> 20) != pr)) return 9;
+                const int pfull = (t | 31) < hdr[2] ? (int)((stn[t | 31] >> 12) & 0xffu) : 0;
+                const int pbase = (int)sroff[pr];
+                for (int j = 0; j < pfull && j < cnt; j++) if (pbase + 32 * j != (int)sroff[pr + j]) return 11;
                 double fx = sf[2 * node], fy = sf[2 * node + 1];
-                for (int q = (int)(r0 >> 16); q < (int)(r1 >> 16); q++) {
-                    if (stpos[q] >= ne) return 8;
+                for (int j = 0; j < cnt; j++) {
+                    const int q = j < pfull ? pbase + 32 * j + lane : (int)sroff[pr + j] + lane;
+                    if (q >= ne || stpos[q] >= ne) return 8;
                     fx = fx - sp[2 * stpos[q]];
                     fy = fy - sp[2 * stpos[q] + 1];
                 }
