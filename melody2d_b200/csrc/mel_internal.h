@@ -92,6 +92,11 @@ struct mel_dev {
     const double2 *X0, *minv, *mass;
     double2 *x, *u, *v, *a, *up, *vp, *ap;
     const int* sup_ptr; const uint16_t* sup_idx; const double* sup_N;
+    // the same supports of deformable bodies laid out for the kinematics: a body's nodes as slots
+    // sorted by support count (slot ranges start at multiples of 32), groups of 32 slots; slot
+    // record = node | support count << 12; entry k of lane l of group G at kg_base[G] + 32 k + l
+    const int* b_ks0; const unsigned* ks_rec; const int* kg_base;
+    const uint16_t* ks_idx; const double* ks_N;
     double2 *o_fint, *o_fcon, *o_fneu, *o_fdir, *o_ftot;
     // borders and border entries
     const int *bd_body, *bd_per, *bd_bef, *bd_aft, *bd_e0, *bd_bc, *bd_h0;

@@ -856,33 +856,41 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
     }
     tail_sync();      // warps 1-7: Euler done
     // ---- Update_kinematics + Update_current_positions (Code/Body.h:2176-2227, 2272-2283) --
+    // slot i of the body's kinematics layout is lane i & 31 of group i >> 5 (i = tid - 32 + 224 m
+    // keeps the lane); row k of a group is 32 consecutive entries, so the support loads of a warp
+    // are coalesced.  Each node sums its supports in their own order.
+    const int ks = d.b_ks0[b];
     for (int i = tid - 32; i < n; i += blockDim.x - 32) {
-        int gi = n0 + i;
+        const unsigned rec = d.ks_rec[ks + i];
+        const int node = (int)(rec & 0xfffu), cnt = (int)(rec >> 12);
+        const int* kb = d.kg_base + ((ks + i) >> 5);
+        const uint16_t* kidx = d.ks_idx + *kb + lane;
+        const double* kN = d.ks_N + *kb + lane;
         double dx = 0., dy = 0., vx = 0., vy = 0., ax = 0., ay = 0.;
-        const int j0 = d.sup_ptr[gi], j1 = d.sup_ptr[gi + 1];
-        int j = j0;
-        for (; j + 4 <= j1; j += 4) {            // support lists fetched four entries at a time
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
             int t[4];
             double sN[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) { t[q] = d.sup_idx[j + q]; sN[q] = d.sup_N[j + q]; }
+            for (int q = 0; q < 4; q++) { t[q] = kidx[32 * (k + q)]; sN[q] = kN[32 * (k + q)]; }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 double2 up = s_up[t[q]], vp = s_vp[t[q]], ap = s_ap[t[q]];
-                double s = sN[q];
-                dx += s * up.x; dy += s * up.y;
-                vx += s * vp.x; vy += s * vp.y;
-                ax += s * ap.x; ay += s * ap.y;
+                double sv = sN[q];
+                dx += sv * up.x; dy += sv * up.y;
+                vx += sv * vp.x; vy += sv * vp.y;
+                ax += sv * ap.x; ay += sv * ap.y;
             }
         }
-        for (; j < j1; j++) {
-            int t = d.sup_idx[j];
-            double s = d.sup_N[j];
+        for (; k < cnt; k++) {
+            const int t = kidx[32 * k];
+            const double sv = kN[32 * k];
             double2 up = s_up[t], vp = s_vp[t], ap = s_ap[t];
-            dx += s * up.x; dy += s * up.y;
-            vx += s * vp.x; vy += s * vp.y;
-            ax += s * ap.x; ay += s * ap.y;
+            dx += sv * up.x; dy += sv * up.y;
+            vx += sv * vp.x; vy += sv * vp.y;
+            ax += sv * ap.x; ay += sv * ap.y;
         }
+        const int gi = n0 + node;
         d.u[gi] = make_double2(dx, dy);
         d.v[gi] = make_double2(vx, vy);
         d.a[gi] = make_double2(ax, ay);

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <cmath>
 #include <string>
+#include <numeric>
 #include <vector>
 #include <algorithm>
 #include <atomic>
@@ -332,6 +333,50 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.sup_ptr = dupload(h, d->node_sup_ptr, nn + 1);
     D.sup_idx = dupload(h, sidx);
     D.sup_N = dupload(h, d->node_sup_N, h->nse);
+    {
+        // kinematics layout (mel_dev::ks_*): a warp's 32 slots read row k of their supports as 32
+        // consecutive entries; each node's supports keep their order
+        std::vector<int> ks0(nb + 1, 0), kgb;
+        std::vector<unsigned> rec;
+        std::vector<uint16_t> kidx;
+        std::vector<double> kN;
+        std::vector<int> order;
+        for (int b = 0; b < nb; b++) {
+            ks0[b] = (int)rec.size();
+            if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+            const int b0 = d->body_node_ptr[b], nbn = d->body_node_ptr[b + 1] - b0;
+            order.resize(nbn);
+            std::iota(order.begin(), order.end(), 0);
+            auto cnt = [&](int i) { return d->node_sup_ptr[b0 + i + 1] - d->node_sup_ptr[b0 + i]; };
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cnt(x) > cnt(y); });
+            for (int s0 = 0; s0 < nbn; s0 += 32) {
+                const int m = std::min(32, nbn - s0);
+                const int K = cnt(order[s0]);
+                const size_t base = kidx.size();
+                kgb.push_back((int)base);
+                kidx.resize(base + 32 * (size_t)K, 0);
+                kN.resize(base + 32 * (size_t)K, 0.);
+                for (int l = 0; l < m; l++) {
+                    const int i = order[s0 + l];
+                    if (cnt(i) > 0xfffff) { mel_set_error("node %d has %d supports", b0 + i, cnt(i)); return MEL_ERR_UNSUPPORTED; }
+                    rec.push_back((unsigned)i | ((unsigned)cnt(i) << 12));
+                    for (int k = 0, j = d->node_sup_ptr[b0 + i]; k < cnt(i); k++, j++) {
+                        kidx[base + 32 * (size_t)k + l] = sidx[j];
+                        kN[base + 32 * (size_t)k + l] = d->node_sup_N[j];
+                    }
+                }
+                for (int l = m; l < 32; l++) rec.push_back(0u);
+            }
+            if (kidx.size() > (size_t)INT32_MAX) { mel_set_error("node supports above 2^31 entries"); return MEL_ERR_UNSUPPORTED; }
+        }
+        ks0[nb] = (int)rec.size();
+        if (rec.empty()) { rec.push_back(0u); kgb.push_back(0); kidx.push_back(0); kN.push_back(0.); }
+        D.b_ks0 = dupload(h, ks0);
+        D.ks_rec = dupload(h, rec);
+        D.kg_base = dupload(h, kgb);
+        D.ks_idx = dupload(h, kidx);
+        D.ks_N = dupload(h, kN);
+    }
     D.o_fint = (double2*)dalloc<double>(h, 2 * (size_t)nn);
     D.o_fcon = (double2*)dalloc<double>(h, 2 * (size_t)nn);
     D.o_fneu = (double2*)dalloc<double>(h, 2 * (size_t)nn);
