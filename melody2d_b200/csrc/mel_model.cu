@@ -9,8 +9,6 @@
 #include <numeric>
 #include <vector>
 #include <algorithm>
-#include <atomic>
-#include <thread>
 #include "mel_internal.h"
 #include "mel_prox_host.h"
 #include "mel_chunks.h"
@@ -71,7 +69,6 @@ struct mel_handle {
     double bytes_body = 0., bytes_contact = 0.;
     int n_def_nodes = 0;
     mel_batch* batch = nullptr;  // batch the handle is a member of (steps only through the batch)
-    cudaEvent_t ev_prox = nullptr;  // end of the handle's last proximity update within a batch
     int failed = 0;                 // model-level failure (MEL_ERR_NAN, MEL_ERR_BOUNDS) that retired it from a batch
     std::string failed_msg;
 };
@@ -731,9 +728,9 @@ mel_status mel_destroy(mel_handle* h)
                      (void*)P.tns, (void*)P.tslot, (void*)P.tkey,
                      (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)P.cont_rt, (void*)h->d.cont })
         if (p) cudaFree(p);
+    mel_prox_stage_free(P.stage);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
-    if (h->ev_prox) cudaEventDestroy(h->ev_prox);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MEL_OK;
@@ -1081,7 +1078,7 @@ struct mel_batch {
     long long launches = 0;
     double ms_last = 0.;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaEvent_t e_step = nullptr;        // end of the last step's launches (members' proximity waits on it)
+    mel_prox_stage* pstage = nullptr;    // staging of the members' proximity runs
 };
 
 // Re-uploads the member descriptors and the work prefixes (the stream is idle afterwards).
@@ -1121,45 +1118,25 @@ static mel_status batch_refresh(mel_batch* b)
     return MEL_OK;
 }
 
-// Update_proximity of the members due at this step.  Each runs on its own stream, from its own
-// host thread, after the step's launches (an event on the batch stream); the batch stream then
-// waits for all of them.  The members' pipelines share nothing, so their small kernels and host
-// round trips overlap instead of queueing one behind another.
+// Update_proximity of the members due at this step: one run of the pipeline serves all of them
+// (one set of launches and two host read-backs on the batch stream, whatever their number).  A
+// member whose positions diverged leaves the batch; the others go on.
 static mel_status batch_proximity(mel_batch* b, const std::vector<mel_handle*>& due)
 {
-    MEL_CUDA_OK(cudaEventRecord(b->e_step, b->stream));
-    const size_t n = due.size();
-    std::vector<int> rcs(n, 0), launches(n, 0);
-    std::vector<std::string> msgs(n);
-    std::atomic<size_t> next{ 0 };
-    auto work = [&]() {
-        cudaSetDevice(b->device);
-        for (size_t i = next++; i < n; i = next++) {
-            mel_handle* h = due[i];
-            if (!h->ev_prox) cudaEventCreateWithFlags(&h->ev_prox, cudaEventDisableTiming);
-            cudaStreamWaitEvent(h->stream, b->e_step, 0);
-            int l0 = h->P.launches;
-            rcs[i] = mel_run_proximity(h->d, h->P, h->H, h->stream);
-            launches[i] = h->P.launches - l0;
-            if (rcs[i]) msgs[i] = mel_last_error_string();
-            cudaEventRecord(h->ev_prox, h->stream);
+    std::vector<mel_prox_member> m(due.size());
+    for (size_t i = 0; i < due.size(); i++) { m[i].d = &due[i]->d; m[i].P = &due[i]->P; }
+    int launches = 0;
+    const int rc = mel_run_proximity_many(m.data(), (int)m.size(), b->pstage, launches, b->stream);
+    b->launches += launches;
+    if (rc) return (mel_status)rc;
+    for (size_t i = 0; i < due.size(); i++) {
+        if (m[i].rc == MEL_ERR_NAN || m[i].rc == MEL_ERR_BOUNDS) {
+            due[i]->failed = m[i].rc;
+            due[i]->failed_msg = m[i].msg;
+        } else if (m[i].rc) {
+            mel_set_error("%s", m[i].msg.c_str());
+            return (mel_status)m[i].rc;
         }
-    };
-    const size_t nthreads = std::min(n, (size_t)16);
-    std::vector<std::thread> pool;
-    for (size_t t = 1; t < nthreads; t++) pool.emplace_back(work);
-    work();
-    for (auto& t : pool) t.join();
-    for (size_t i = 0; i < n; i++) {
-        if (rcs[i] == MEL_ERR_NAN || rcs[i] == MEL_ERR_BOUNDS) {      // this sample diverged: it leaves
-            due[i]->failed = rcs[i];                                    // the batch, the others go on
-            due[i]->failed_msg = msgs[i];
-        } else if (rcs[i]) {
-            mel_set_error("%s", msgs[i].c_str());
-            return (mel_status)rcs[i];
-        }
-        MEL_CUDA_OK(cudaStreamWaitEvent(b->stream, due[i]->ev_prox, 0));
-        b->launches += launches[i];
     }
     return MEL_OK;
 }
@@ -1187,8 +1164,7 @@ mel_status mel_batch_create(int device, int precision, mel_batch** out)
     b->precision = precision;
     cudaSetDevice(device);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->e_step, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) {
         mel_set_cuda_error(cudaGetLastError(), "batch stream", __FILE__, __LINE__);
         delete b;
         return MEL_ERR_CUDA;
@@ -1298,7 +1274,8 @@ mel_status mel_batch_destroy(mel_batch* b)
     cudaStreamSynchronize(b->stream);
     for (mel_handle* h : b->members) h->batch = nullptr;
     cudaFree(b->d_devs); cudaFree(b->d_thr0); cudaFree(b->d_cta0);
-    cudaEventDestroy(b->e0); cudaEventDestroy(b->e1); cudaEventDestroy(b->e_step);
+    cudaEventDestroy(b->e0); cudaEventDestroy(b->e1);
+    mel_prox_stage_free(b->pstage);
     cudaStreamDestroy(b->stream);
     delete b;
     return MEL_OK;

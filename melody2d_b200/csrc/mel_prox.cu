@@ -13,21 +13,39 @@
 //                     previous list of the same slave border node (Code/Proximity.h:269-284)
 //   entry_index_kernel / incoming ranges   index structures for the next step and update
 #include <cstdio>
+#include <cstring>
+#include <utility>
 #include <vector>
 #include <algorithm>
 #include "mel_internal.h"
 #include "mel_geometry.cuh"
+#include "mel_prox_host.h"
+
+struct mel_scan_job { const int* in; int* out; int n; int* sums; };
 
 namespace mel {
 
 // ---------------------------------------------------------------------------------------------
-// exclusive scan of int (three-phase, deterministic)
+// exclusive scans of int arrays, several per launch (three-phase, deterministic).  Job j scans
+// in[0..n) into out[0..n] (out[n] = total); blocks [bpre[j], bpre[j+1]) of a launch serve job j.
 // ---------------------------------------------------------------------------------------------
 #define SCAN_BLOCK 1024
-__global__ void scan_block_kernel(const int* in, int* out, int n, int* block_sums)
+__device__ __forceinline__ int block_job(const int* bpre, int nj)
+{
+    int lo = 0, hi = nj;                  // largest j with bpre[j] <= blockIdx.x
+    while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (bpre[mid] <= (int)blockIdx.x) lo = mid; else hi = mid; }
+    return lo;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_block_kernel(const mel_scan_job* J, const int* bpre, int nj)
 {
     __shared__ int s[SCAN_BLOCK];
-    int i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+    const int j = block_job(bpre, nj);
+    const int* in = J[j].in;
+    int* out = J[j].out;
+    const int n = J[j].n;
+    const int lb = blockIdx.x - bpre[j];
+    int i = lb * SCAN_BLOCK + threadIdx.x;
     int v = (i < n) ? in[i] : 0;
     s[threadIdx.x] = v;
     __syncthreads();
@@ -38,12 +56,15 @@ __global__ void scan_block_kernel(const int* in, int* out, int n, int* block_sum
         __syncthreads();
     }
     if (i <= n) out[i] = s[threadIdx.x] - v;
-    if (threadIdx.x == SCAN_BLOCK - 1) block_sums[blockIdx.x] = s[threadIdx.x];
+    if (threadIdx.x == SCAN_BLOCK - 1) J[j].sums[lb] = s[threadIdx.x];
 }
-__global__ void scan_add_kernel(int* out, int n, const int* block_off)
+// adds the scanned block totals (in) to out[0..n) block by block
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_add_kernel(const mel_scan_job* J, const int* bpre, int nj)
 {
-    int i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
-    if (i < n) out[i] += block_off[blockIdx.x];   // n here counts the total slot as well
+    const int j = block_job(bpre, nj);
+    const int lb = blockIdx.x - bpre[j];
+    int i = lb * SCAN_BLOCK + threadIdx.x;
+    if (i < J[j].n) J[j].out[i] += J[j].in[lb];
 }
 
 } // namespace mel
@@ -51,10 +72,8 @@ __global__ void scan_add_kernel(int* out, int n, const int* block_off)
 namespace mel {
 
 // ---------------------------------------------------------------------------------------------
-__global__ void aabb_kernel(mel_dev d, double* aabb, int* shmin, int* shmax)
+__device__ __forceinline__ void aabb_item(const mel_dev& d, double* aabb, int* shmin, int* shmax, int g, int lane)
 {
-    int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
     if (g >= d.nbd) return;
     int b = d.bd_body[g];
     if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
@@ -95,11 +114,9 @@ __global__ void aabb_kernel(mel_dev d, double* aabb, int* shmin, int* shmax)
     }
 }
 
-__global__ void neighbour_kernel(mel_dev d, const double* aabb, const int* shmin, const int* shmax,
-                                 int* nbr, int* nbn, int cap)
+__device__ __forceinline__ void neighbour_item(const mel_dev& d, const double* aabb, const int* shmin, const int* shmax,
+                                               int* nbr, int* nbn, int cap, int b1, int lane)
 {
-    int b1 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
     if (b1 >= d.nb) return;
     if (d.b_status[b1] == MEL_STATUS_INACTIVE) { if (lane == 0) nbn[b1] = 0; return; }
     int* out = nbr + (size_t)3 * cap * b1;
@@ -164,9 +181,8 @@ __global__ void neighbour_kernel(mel_dev d, const double* aabb, const int* shmin
 // Detect_Segment_Proximity; the boxes are widened by the detection distance plus a margin, so the
 // accepted candidates and their order are unchanged.
 // ---------------------------------------------------------------------------------------------
-__global__ void segblock_kernel(mel_dev d)
+__device__ __forceinline__ void segblock_item(const mel_dev& d, int k)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.nblk) return;
     int g = d.blk_border[k];
     int b = d.bd_body[g];
@@ -190,9 +206,8 @@ __global__ void segblock_kernel(mel_dev d)
 }
 
 // superblock boxes: unions of MEL_SEGB2 consecutive block boxes of one border
-__global__ void superblock_kernel(mel_dev d)
+__device__ __forceinline__ void superblock_item(const mel_dev& d, int k)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.nsblk) return;
     int g = d.sblk_border[k];
     int b0 = d.bd_blk0[g] + (k - d.bd_sblk0[g]) * MEL_SEGB2;
@@ -304,9 +319,8 @@ __device__ __forceinline__ bool has_self(const mel_dev& d, int b)
 }
 
 // per body: task count and slot count (slave border nodes summed over its tasks)
-__global__ void task_count_kernel(mel_dev d, const int* nbn, int* tcnt, int* scnt)
+__device__ __forceinline__ void task_count_item(const mel_dev& d, const int* nbn, int* tcnt, int* scnt, int b)
 {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= d.nb) return;
     int nbd = d.b_bd0[b + 1] - d.b_bd0[b];
     int nent = d.bd_e0[d.b_bd0[b + 1]] - d.bd_e0[d.b_bd0[b]];
@@ -317,10 +331,10 @@ __global__ void task_count_kernel(mel_dev d, const int* nbn, int* tcnt, int* scn
 
 // task t = (slave body, slave border, neighbour q or -1 for self, first slot), its slave border node
 // count, its first slot and its master body; inc_cnt counts the tasks of each master body
-__global__ void task_fill_kernel(mel_dev d, const int* nbr, const int* nbn, int cap, const int* btask0,
-                                 const int* bslot0, int4* task, int* tns, int* tslot, int* tkey, int* inc_cnt)
+__device__ __forceinline__ void task_fill_item(const mel_dev& d, const int* nbr, const int* nbn, int cap, const int* btask0,
+                                               const int* bslot0, int4* task, int* tns, int* tslot, int* tkey, int* inc_cnt,
+                                               int b)
 {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= d.nb) return;
     int t = btask0[b];
     int slot = bslot0[b];
@@ -343,10 +357,9 @@ __global__ void task_fill_kernel(mel_dev d, const int* nbr, const int* nbn, int 
         }
 }
 
-__global__ void count_kernel(mel_dev d, const int4* task, int ntask, const int* nbr, int cap, int* slot_cnt)
+__device__ __forceinline__ void count_item(const mel_dev& d, const int4* task, int ntask, const int* nbr, int cap,
+                                           int* slot_cnt, int t, int lane)
 {
-    int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
     if (t >= ntask) return;
     int4 tk = task[t];
     int bS = tk.x, gS = tk.y, q = tk.z, slot0 = tk.w;
@@ -363,12 +376,10 @@ __global__ void count_kernel(mel_dev d, const int4* task, int ntask, const int* 
     }
 }
 
-__global__ void write_kernel(mel_dev d, const int4* task, int ntask, const int* nbr, int cap, const int* slot_off,
-                             mel_contact* out, const mel_contact* old, const int* old_eptr, const int* old_elist,
-                             int have_old)
+__device__ __forceinline__ void write_item(const mel_dev& d, const int4* task, int ntask, const int* nbr, int cap,
+                                           const int* slot_off, mel_contact* out, const mel_contact* old,
+                                           const int* old_eptr, const int* old_elist, int have_old, int t, int lane)
 {
-    int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
     if (t >= ntask) return;
     int4 tk = task[t];
     int bS = tk.x, gS = tk.y, q = tk.z, slot0 = tk.w;
@@ -439,17 +450,14 @@ __global__ void write_kernel(mel_dev d, const int4* task, int ntask, const int* 
 // Tasks are grouped by master with a counting pass and an atomic fill, then each group is put back
 // in ascending order by a rank sort (task ids are unique), one warp per master body.
 // ---------------------------------------------------------------------------------------------
-__global__ void inc_fill_kernel(const int* tkey, int ntask, int* cur, int* tmp)
+__device__ __forceinline__ void inc_fill_item(const int* tkey, int ntask, int* cur, int* tmp, int t)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntask) return;
     tmp[atomicAdd(&cur[tkey[t]], 1)] = t;
 }
 
-__global__ void inc_sort_kernel(int nb, const int* inc0, const int* tmp, int* sorted)
+__device__ __forceinline__ void inc_sort_item(int nb, const int* inc0, const int* tmp, int* sorted, int B, int lane)
 {
-    int B = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
     if (B >= nb) return;
     int i0 = inc0[B], n = inc0[B + 1] - i0;
     for (int i = lane; i < n; i += 32) {
@@ -459,9 +467,9 @@ __global__ void inc_sort_kernel(int nb, const int* inc0, const int* tmp, int* so
     }
 }
 
-__global__ void inc_range_kernel(const int* sorted, int n, const int* tslot, const int* tns, const int* slot_off, int2* rng)
+__device__ __forceinline__ void inc_range_item(const int* sorted, int n, const int* tslot, const int* tns,
+                                               const int* slot_off, int2* rng, int i)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int t = sorted[i];
     rng[i] = make_int2(slot_off[tslot[t]], slot_off[tslot[t] + tns[t]]);
@@ -469,9 +477,9 @@ __global__ void inc_range_kernel(const int* sorted, int n, const int* tslot, con
 
 
 // per-body serial counting sort of a body-major contact list by slave border entry
-__global__ void entry_index_kernel(mel_dev d, const mel_contact* cont, const int* b_cont0, int* eptr_cnt, int* elist)
+__device__ __forceinline__ void entry_index_item(const mel_dev& d, const mel_contact* cont, const int* b_cont0,
+                                                 int* eptr_cnt, int* elist, int b)
 {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= d.nb) return;
     int e_lo = d.bd_e0[d.b_bd0[b]], e_hi = d.bd_e0[d.b_bd0[b + 1]];
     int c0 = b_cont0[b], c1 = b_cont0[b + 1];
@@ -485,19 +493,17 @@ __global__ void entry_index_kernel(mel_dev d, const mel_contact* cont, const int
     }
 }
 
-__global__ void entry_count_kernel(mel_dev d, const mel_contact* cont, int n, int* cnt)
+__device__ __forceinline__ void entry_count_item(const mel_dev& d, const mel_contact* cont, int n, int* cnt, int c)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     int b = cont[c].bodyS;
     int e = d.bd_e0[d.b_bd0[b] + cont[c].borderS] + cont[c].border_nodeS;
     atomicAdd(&cnt[e], 1);
 }
 
-__global__ void body_range_kernel(const mel_contact* cont, int n, int nb, int* b_cont0)
+__device__ __forceinline__ void body_range_item(const mel_contact* cont, int n, int nb, int* b_cont0, int b)
 {
     // b_cont0[b] = first index with bodyS >= b (list is body-major)
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b > nb) return;
     int lo = 0, hi = n;
     while (lo < hi) { int mid = (lo + hi) >> 1; if (cont[mid].bodyS < b) lo = mid + 1; else hi = mid; }
@@ -507,9 +513,8 @@ __global__ void body_range_kernel(const mel_contact* cont, int n, int nb, int* b
 // Newly created elements leave vgapn/vgapt unassigned in the reference: they keep the values of the
 // element pushed before them in the slave body's list (the reused new_contact variable,
 // Code/Proximity.h:286-313); self contacts use a fresh variable (Code/Proximity.h:350).
-__global__ void carry_kernel(const mel_dev d, mel_contact* cont, const int* b_cont0)
+__device__ __forceinline__ void carry_item(const mel_dev& d, mel_contact* cont, const int* b_cont0, int b)
 {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= d.nb) return;
     double vn = 0., vt = 0.;
     for (int c = b_cont0[b]; c < b_cont0[b + 1]; c++) {
@@ -520,13 +525,87 @@ __global__ void carry_kernel(const mel_dev d, mel_contact* cont, const int* b_co
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// job-table launches: blocks [bpre[j], bpre[j+1]) serve member j.  The block copies the member's
+// job into shared memory; item `it` of the member is handled by TPI consecutive threads (TPI 32:
+// one warp per item, TPI 1: one thread).
+// ---------------------------------------------------------------------------------------------
+#define PROX_THREADS 256
+#define JOB_KERNEL(name, TPI, ...)                                                                  \
+    __global__ void __launch_bounds__(PROX_THREADS) name(const mel_prox_job* J, const int* bpre, int nj) \
+    {                                                                                               \
+        __shared__ mel_prox_job sj;                                                                 \
+        const int jj = block_job(bpre, nj);                                                         \
+        {                                                                                           \
+            const int* src = reinterpret_cast<const int*>(J + jj);                                  \
+            int* dst = reinterpret_cast<int*>(&sj);                                                 \
+            for (int k = threadIdx.x; k < (int)(sizeof(mel_prox_job) / sizeof(int)); k += blockDim.x) dst[k] = src[k]; \
+        }                                                                                           \
+        __syncthreads();                                                                            \
+        const int it = (blockIdx.x - bpre[jj]) * (PROX_THREADS / (TPI)) + (int)threadIdx.x / (TPI); \
+        const int lane = threadIdx.x & 31;                                                          \
+        (void)lane;                                                                                 \
+        const mel_prox_job& j = sj;                                                                 \
+        const mel_dev& d = sj.d;                                                                    \
+        (void)j; (void)d;                                                                           \
+        __VA_ARGS__;                                                                                \
+    }
+
+JOB_KERNEL(aabb_kernel, 32, aabb_item(d, j.aabb, j.shmin, j.shmax, it, lane))
+JOB_KERNEL(segblock_kernel, 1, segblock_item(d, it))
+JOB_KERNEL(superblock_kernel, 1, superblock_item(d, it))
+JOB_KERNEL(neighbour_kernel, 32, neighbour_item(d, j.aabb, j.shmin, j.shmax, j.nbr, j.nbn, j.nbr_cap, it, lane))
+JOB_KERNEL(task_count_kernel, 1, task_count_item(d, j.nbn, j.tcnt, j.scnt, it))
+JOB_KERNEL(zero_tcnt_kernel, 1, if (it <= d.nb) j.tcnt[it] = 0)
+JOB_KERNEL(task_fill_kernel, 1, task_fill_item(d, j.nbr, j.nbn, j.nbr_cap, j.btask0, j.bslot0, j.task, j.tns, j.tslot,
+                                               j.tkey, j.tcnt, it))
+JOB_KERNEL(count_kernel, 32, count_item(d, j.task, j.ntask, j.nbr, j.nbr_cap, j.slot_cnt, it, lane))
+JOB_KERNEL(write_kernel, 32, write_item(d, j.task, j.ntask, j.nbr, j.nbr_cap, j.slot_off, j.cont_new, d.cont, j.e_ptr,
+                                        j.e_list, j.have_old, it, lane))
+JOB_KERNEL(zero_contw_kernel, 1, if (it <= d.ncont) d.cont_w[it] = 0.)
+JOB_KERNEL(copy_inc_kernel, 1, if (it < d.nb) j.tcnt[it] = j.b_inc0[it])
+JOB_KERNEL(inc_fill_kernel, 1, inc_fill_item(j.tkey, j.ntask, j.tcnt, j.inc_task, it))
+JOB_KERNEL(inc_sort_kernel, 32, inc_sort_item(d.nb, j.b_inc0, j.inc_task, j.inc_task + j.ntask, it, lane))
+JOB_KERNEL(inc_range_kernel, 1, inc_range_item(j.inc_task + j.ntask, j.ntask, j.tslot, j.tns, j.slot_off, j.inc_rng, it))
+JOB_KERNEL(body_range_kernel, 1, body_range_item(d.cont, d.ncont, d.nb, j.b_cont0, it))
+JOB_KERNEL(zero_ecnt_kernel, 1, if (it <= d.ne) j.e_cnt[it] = 0)
+JOB_KERNEL(entry_count_kernel, 1, entry_count_item(d, d.cont, d.ncont, j.e_cnt, it))
+JOB_KERNEL(copy_eptr_kernel, 1, if (it <= d.ne) j.e_cur[it] = j.e_ptr[it])
+JOB_KERNEL(entry_index_kernel, 1, entry_index_item(d, d.cont, j.b_cont0, j.e_cur, j.e_list, it))
+JOB_KERNEL(carry_kernel, 1, carry_item(d, d.cont, j.b_cont0, it))
+
+// one thread per member: clear the neighbour-overflow words before an attempt
+__global__ void nbr_clear_kernel(const mel_prox_job* J, int nj)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nj) return;
+    J[k].d.err[MEL_E_NBR_OVERFLOW] = 0u;
+    J[k].d.err[MEL_E_NBR_NEED] = 0u;
+}
+// one thread per member: the words the host needs after the neighbour stage (0-4) or the count
+// stage (5)
+__global__ void readback_kernel(const mel_prox_job* J, int nj, int stage)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nj) return;
+    const mel_prox_job& j = J[k];
+    int* r = j.readback;
+    if (stage == 0) {
+        r[0] = (int)j.d.err[MEL_E_NAN];
+        r[1] = (int)j.d.err[MEL_E_NBR_OVERFLOW];
+        r[2] = (int)j.d.err[MEL_E_NBR_NEED];
+        r[3] = j.btask0[j.d.nb];
+        r[4] = j.bslot0[j.d.nb];
+    } else {
+        r[5] = j.slot_off[j.nslot];
+    }
+}
+
 } // namespace mel
 
 // =============================================================================================
 // host driver
 // =============================================================================================
-#include "mel_prox_host.h"
-
 static int ensure_impl(void** p, size_t* cap_bytes, size_t need, const char* what)
 {
     if (need <= *cap_bytes && *p) return 0;
@@ -560,10 +639,67 @@ static bool sync_failed(cudaStream_t s, int line)
     return true;
 }
 
-// Exclusive scan of n ints into out[0..n] (out[n] = total): a block scan per 1024 entries, the
-// block totals scanned the same way, then the block offsets added.  Deterministic; the block
-// totals live in the state's persistent scratch (no allocation once it has grown).
-static size_t scan_scratch_ints(int n)
+// Staging of a run: job tables, block prefixes and scan jobs are written to pinned host memory and
+// copied to the same offsets of a device buffer on the run's stream; the space is reused after
+// each synchronisation of the stream.  The read-back words of the members live apart.
+struct mel_prox_stage {
+    char* h = nullptr; char* dv = nullptr; size_t cap = 0, used = 0;
+    int* rb_h = nullptr; int* rb_d = nullptr; int rb_cap = 0;    // 8 words per member; rb_d[8 * rb_cap] = 0
+    const int* zero = nullptr;     // block prefix of a one-member launch (blocks start at 0)
+    std::vector<std::pair<char*, char*>> retired;               // outgrown buffers, freed after a sync
+};
+
+static void stage_release_retired(mel_prox_stage& S)
+{
+    for (auto& b : S.retired) { cudaFreeHost(b.first); cudaFree(b.second); }
+    S.retired.clear();
+}
+
+void mel_prox_stage_free(mel_prox_stage* S)
+{
+    if (!S) return;
+    stage_release_retired(*S);
+    if (S->h) cudaFreeHost(S->h);
+    if (S->dv) cudaFree(S->dv);
+    if (S->rb_h) cudaFreeHost(S->rb_h);
+    if (S->rb_d) cudaFree(S->rb_d);
+    delete S;
+}
+
+// copies `bytes` from src to the device side of the stage (stream ordered); nullptr on failure
+static void* stage_upload(mel_prox_stage& S, const void* src, size_t bytes, cudaStream_t s)
+{
+    const size_t off = (S.used + 15) & ~(size_t)15;
+    if (off + bytes > S.cap) {
+        // grow: data already staged may still be read by work on the stream, so the old buffers
+        // are kept until the next synchronisation
+        size_t nc = 2 * (off + bytes) + (1 << 16);
+        char *nh = nullptr, *nd = nullptr;
+        if (cudaMallocHost(&nh, nc) != cudaSuccess) return nullptr;
+        if (cudaMalloc(&nd, nc) != cudaSuccess) { cudaFreeHost(nh); return nullptr; }
+        if (S.h) S.retired.push_back({ S.h, S.dv });
+        S.h = nh; S.dv = nd; S.cap = nc;
+        S.used = 0;
+        return stage_upload(S, src, bytes, s);
+    }
+    memcpy(S.h + off, src, bytes);
+    if (cudaMemcpyAsync(S.dv + off, S.h + off, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return nullptr;
+    S.used = off + bytes;
+    return S.dv + off;
+}
+
+namespace {
+
+typedef void (*job_kernel_t)(const mel_prox_job*, const int*, int);
+
+struct run_ctx {
+    mel_prox_stage& S;
+    cudaStream_t s;
+    int launches;
+};
+
+// scratch ints of an exclusive scan of n entries (block totals of every level)
+size_t scan_scratch_ints(int n)
 {
     size_t t = 0;
     while (true) {
@@ -575,139 +711,304 @@ static size_t scan_scratch_ints(int n)
     return t;
 }
 
-static void scan_rec(const int* in, int* out, int n, int* ws, int& launches, cudaStream_t s)
+// kernel k over items[j] items of member j of the job table J (TPI threads per item)
+int launch_jobs(run_ctx& C, job_kernel_t k, const mel_prox_job* J, const std::vector<int>& items, int tpi)
 {
-    int nblk = (n + SCAN_BLOCK) / SCAN_BLOCK;     // covers index n as well
-    int* sums = ws;
-    int* soff = ws + nblk + 1;
-    mel::scan_block_kernel<<<nblk, SCAN_BLOCK, 0, s>>>(in, out, n, sums);
-    launches++;
-    if (nblk == 1) return;                        // one block: out[n] already holds the total
-    scan_rec(sums, soff, nblk, soff + nblk + 2, launches, s);
-    mel::scan_add_kernel<<<nblk, SCAN_BLOCK, 0, s>>>(out, n + 1, soff);
-    launches++;
-}
-
-int mel_scan_exclusive(const int* in, int* out, int n, mel_prox_state& P, cudaStream_t s)
-{
-    if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(n))) return MEL_ERR_OOM;
-    scan_rec(in, out, n, P.scan_ws, P.launches, s);
+    const int nj = (int)items.size();
+    const int per_block = PROX_THREADS / tpi;
+    std::vector<int> bpre(nj + 1, 0);
+    for (int j = 0; j < nj; j++) bpre[j + 1] = bpre[j] + (items[j] + per_block - 1) / per_block;
+    if (bpre[nj] == 0) return MEL_OK;
+    const int* dp = nj == 1 ? C.S.zero : (const int*)stage_upload(C.S, bpre.data(), sizeof(int) * (nj + 1), C.s);
+    if (!dp) { mel_set_error("proximity staging upload failed"); return MEL_ERR_CUDA; }
+    k<<<bpre[nj], PROX_THREADS, 0, C.s>>>(J, dp, nj);
+    C.launches++;
     return MEL_OK;
 }
 
-// Rebuilds b_cont0 and the per-entry index of the current list (d.cont, d.ncont).
-int mel_index_contacts(mel_dev& d, mel_prox_state& P, cudaStream_t s)
+// exclusive scans: req[j] scans in[0..n) into out[0..n] using the scratch ws (scan_scratch_ints(n))
+struct scan_req { const int* in; int* out; int n; int* ws; };
+int scan_many(run_ctx& C, const std::vector<scan_req>& req)
+{
+    if (req.empty()) return MEL_OK;
+    const int nj = (int)req.size();
+    std::vector<mel_scan_job> jobs(nj), adds;
+    std::vector<int> bpre(nj + 1, 0), apre(1, 0);
+    std::vector<scan_req> next;
+    for (int j = 0; j < nj; j++) {
+        const int nblk = (req[j].n + SCAN_BLOCK) / SCAN_BLOCK;      // covers index n as well
+        jobs[j] = { req[j].in, req[j].out, req[j].n, req[j].ws };
+        bpre[j + 1] = bpre[j] + nblk;
+        if (nblk > 1) {                                              // block totals scanned the same way
+            int* soff = req[j].ws + nblk + 1;
+            next.push_back({ req[j].ws, soff, nblk, soff + nblk + 2 });
+            adds.push_back({ soff, req[j].out, req[j].n + 1, nullptr });
+            apre.push_back(apre.back() + nblk);
+        }
+    }
+    const mel_scan_job* dj = (const mel_scan_job*)stage_upload(C.S, jobs.data(), sizeof(mel_scan_job) * nj, C.s);
+    const int* db = nj == 1 ? C.S.zero : (const int*)stage_upload(C.S, bpre.data(), sizeof(int) * (nj + 1), C.s);
+    if (!dj || !db) { mel_set_error("proximity staging upload failed"); return MEL_ERR_CUDA; }
+    mel::scan_block_kernel<<<bpre[nj], SCAN_BLOCK, 0, C.s>>>(dj, db, nj);
+    C.launches++;
+    if (next.empty()) return MEL_OK;
+    if (int rc = scan_many(C, next)) return rc;
+    const mel_scan_job* da = (const mel_scan_job*)stage_upload(C.S, adds.data(), sizeof(mel_scan_job) * adds.size(), C.s);
+    const int* dap = adds.size() == 1 ? C.S.zero : (const int*)stage_upload(C.S, apre.data(), sizeof(int) * apre.size(), C.s);
+    if (!da || !dap) { mel_set_error("proximity staging upload failed"); return MEL_ERR_CUDA; }
+    mel::scan_add_kernel<<<apre.back(), SCAN_BLOCK, 0, C.s>>>(da, dap, (int)adds.size());
+    C.launches++;
+    return MEL_OK;
+}
+
+mel_prox_job make_job(const mel_prox_member& m, int* readback)
+{
+    mel_prox_job j;
+    memset(&j, 0, sizeof j);
+    const mel_prox_state& P = *m.P;
+    j.d = *m.d;
+    j.aabb = P.aabb; j.shmin = P.shmin; j.shmax = P.shmax;
+    j.nbr = P.nbr; j.nbn = P.nbn; j.nbr_cap = P.nbr_cap;
+    j.ntask = P.ntask; j.nslot = P.nslot; j.have_old = m.d->ncont > 0 ? 1 : 0;
+    j.task = (int4*)P.task; j.tns = P.tns; j.tslot = P.tslot; j.tkey = P.tkey;
+    j.tcnt = P.tcnt; j.btask0 = P.btask0; j.scnt = P.scnt; j.bslot0 = P.bslot0;
+    j.slot_cnt = P.slot_cnt; j.slot_off = P.slot_off; j.inc_task = P.inc_task;
+    j.inc_rng = P.inc_rng; j.b_inc0 = P.b_inc0; j.b_cont0 = P.b_cont0;
+    j.e_cnt = P.e_cnt; j.e_ptr = P.e_ptr; j.e_cur = P.e_cur; j.e_list = P.e_list;
+    j.cont_new = P.cont_alt;
+    j.readback = readback;
+    return j;
+}
+
+// job table of the members idx (read-back words by member index) on the device
+const mel_prox_job* upload_jobs(run_ctx& C, mel_prox_member* m, const std::vector<int>& idx,
+                                std::vector<mel_prox_job>& hj)
+{
+    hj.clear();
+    for (int i : idx) hj.push_back(make_job(m[i], C.S.rb_d + 8 * i));
+    const mel_prox_job* J = (const mel_prox_job*)stage_upload(C.S, hj.data(), sizeof(mel_prox_job) * hj.size(), C.s);
+    if (!J) mel_set_error("proximity staging upload failed");
+    return J;
+}
+
+template <typename F>
+std::vector<int> items_of(const std::vector<mel_prox_job>& hj, F&& f)
+{
+    std::vector<int> v;
+    for (const mel_prox_job& j : hj) v.push_back(f(j));
+    return v;
+}
+
+// the per-entry index of each member's current list (d.cont, d.ncont) and b_cont0.  The members'
+// e_list must hold ncont + 1 entries and their scan scratch scan_scratch_ints(ne); J / hj is the
+// job table of the members idx.
+int index_stage(run_ctx& C, mel_prox_member* m, const std::vector<int>& idx, const mel_prox_job* J,
+                const std::vector<mel_prox_job>& hj)
 {
     using namespace mel;
-    body_range_kernel<<<(d.nb + 1 + 127) / 128, 128, 0, s>>>(d.cont, d.ncont, d.nb, P.b_cont0); P.launches++;
-    cudaMemsetAsync(P.e_cnt, 0, sizeof(int) * (d.ne + 1), s);
-    if (d.ncont > 0) { entry_count_kernel<<<(d.ncont + 127) / 128, 128, 0, s>>>(d, d.cont, d.ncont, P.e_cnt); P.launches++; }
-    if (mel_scan_exclusive(P.e_cnt, P.e_ptr, d.ne, P, s)) return MEL_ERR_OOM;
-    if (ensure((void**)&P.e_list, &P.e_list_bytes, sizeof(int) * (size_t)(d.ncont + 1))) return MEL_ERR_OOM;
-    cudaMemcpyAsync(P.e_cur, P.e_ptr, sizeof(int) * (d.ne + 1), cudaMemcpyDeviceToDevice, s);
-    entry_index_kernel<<<(d.nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0, P.e_cur, P.e_list); P.launches++;
+    int rc;
+    if ((rc = launch_jobs(C, body_range_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb + 1; }), 1))) return rc;
+    if ((rc = launch_jobs(C, zero_ecnt_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.ne + 1; }), 1))) return rc;
+    if ((rc = launch_jobs(C, entry_count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.ncont; }), 1))) return rc;
+    std::vector<scan_req> sc;
+    for (int i : idx) sc.push_back({ m[i].P->e_cnt, m[i].P->e_ptr, m[i].d->ne, m[i].P->scan_ws });
+    if ((rc = scan_many(C, sc))) return rc;
+    if ((rc = launch_jobs(C, copy_eptr_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.ne + 1; }), 1))) return rc;
+    return launch_jobs(C, entry_index_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 1);
+}
+
+bool stage_ready(mel_prox_stage*& stage, int n)
+{
+    if (!stage) stage = new mel_prox_stage();
+    mel_prox_stage& S = *stage;
+    if (S.rb_cap >= n) return true;
+    if (S.rb_h) { cudaFreeHost(S.rb_h); S.rb_h = nullptr; }
+    if (S.rb_d) { cudaFree(S.rb_d); S.rb_d = nullptr; }
+    S.rb_cap = 0;
+    const int cap = std::max(n, 16);
+    if (cudaMallocHost(&S.rb_h, sizeof(int) * 8 * (size_t)cap) != cudaSuccess) return false;
+    if (cudaMalloc(&S.rb_d, sizeof(int) * (8 * (size_t)cap + 1)) != cudaSuccess) return false;
+    if (cudaMemset(S.rb_d, 0, sizeof(int) * (8 * (size_t)cap + 1)) != cudaSuccess) return false;
+    S.zero = S.rb_d + 8 * (size_t)cap;
+    S.rb_cap = cap;
+    return true;
+}
+
+// read-back words of members 0..n-1 to the host (one copy, one synchronisation); the stage space is
+// free again afterwards
+bool read_back(run_ctx& C, int n)
+{
+    if (cudaMemcpyAsync(C.S.rb_h, C.S.rb_d, sizeof(int) * 8 * (size_t)n, cudaMemcpyDeviceToHost, C.s) != cudaSuccess) return false;
+    if (sync_failed(C.s, __LINE__)) return false;
+    C.S.used = 0;
+    stage_release_retired(C.S);
+    return true;
+}
+
+}  // namespace
+
+int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, int& launches, cudaStream_t s)
+{
+    using namespace mel;
+    if (n <= 0) return MEL_OK;
+    if (!stage_ready(stage, n)) { mel_set_error("proximity read-back buffers could not be allocated"); return MEL_ERR_OOM; }
+    run_ctx C{ *stage, s, 0 };
+    std::vector<mel_prox_job> hj;
+    std::vector<int> act;
+    int rc;
+    for (int i = 0; i < n; i++) {
+        m[i].rc = MEL_OK;
+        m[i].msg.clear();
+        mel_prox_state& P = *m[i].P;
+        const int nsc = std::max(m[i].d->nb, m[i].d->ne);
+        if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(nsc))) return MEL_ERR_OOM;
+        act.push_back(i);
+    }
+    // 1. border boxes and segment-block boxes
+    const mel_prox_job* J = upload_jobs(C, m, act, hj);
+    if (!J) return MEL_ERR_CUDA;
+    if ((rc = launch_jobs(C, aabb_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nbd; }), 32))) return rc;
+    if ((rc = launch_jobs(C, segblock_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nblk; }), 1))) return rc;
+    if ((rc = launch_jobs(C, superblock_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nsblk; }), 1))) return rc;
+    // 2. neighbours and the task counts; a member whose neighbour lists overflow grows them and
+    //    repeats this stage (up to 4 attempts)
+    std::vector<int> pend = act;
+    for (int attempt = 0; attempt < 4 && !pend.empty(); attempt++) {
+        J = upload_jobs(C, m, pend, hj);
+        if (!J) return MEL_ERR_CUDA;
+        const int np = (int)pend.size();
+        nbr_clear_kernel<<<(np + 127) / 128, 128, 0, s>>>(J, np); C.launches++;
+        if ((rc = launch_jobs(C, neighbour_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 32))) return rc;
+        if ((rc = launch_jobs(C, task_count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 1))) return rc;
+        std::vector<scan_req> sc1, sc2;
+        for (int i : pend) {
+            sc1.push_back({ m[i].P->tcnt, m[i].P->btask0, m[i].d->nb, m[i].P->scan_ws });
+            sc2.push_back({ m[i].P->scnt, m[i].P->bslot0, m[i].d->nb, m[i].P->scan_ws });
+        }
+        if ((rc = scan_many(C, sc1))) return rc;
+        if ((rc = scan_many(C, sc2))) return rc;
+        readback_kernel<<<(np + 127) / 128, 128, 0, s>>>(J, np, 0); C.launches++;
+        if ((rc = launch_status(__LINE__))) return rc;
+        if (!read_back(C, n)) return MEL_ERR_CUDA;
+        std::vector<int> retry;
+        for (int i : pend) {
+            const int* r = C.S.rb_h + 8 * i;
+            mel_prox_state& P = *m[i].P;
+            if (r[0]) {
+                m[i].rc = MEL_ERR_NAN;
+                char buf[160];
+                if (r[0] & 1) snprintf(buf, sizeof buf, "non-finite node positions at the proximity update");
+                else snprintf(buf, sizeof buf, "a border box spans more than %d periods: diverged positions", MEL_MAX_SHIFT_SPAN);
+                m[i].msg = buf;
+                continue;
+            }
+            if (r[1]) {
+                const int need = r[2] + 16;
+                cudaFree(P.nbr); P.nbr = nullptr;
+                if (cudaMalloc(&P.nbr, sizeof(int) * 3 * (size_t)need * m[i].d->nb) != cudaSuccess) {
+                    mel_set_error("allocation of neighbour lists (%d per body) failed", need);
+                    return MEL_ERR_OOM;
+                }
+                P.nbr_cap = need;
+                retry.push_back(i);
+                continue;
+            }
+            P.ntask = r[3];
+            P.nslot = r[4];
+        }
+        pend = retry;
+    }
+    for (int i : pend) { m[i].rc = MEL_ERR_BOUNDS; m[i].msg = "neighbour lists still over capacity after 4 attempts"; }
+    act.clear();
+    for (int i = 0; i < n; i++) if (m[i].rc == MEL_OK) act.push_back(i);
+    if (act.empty()) { launches += C.launches; return launch_status(__LINE__); }
+    // 3. the task list and the candidate count of every slot
+    for (int i : act) {
+        mel_prox_state& P = *m[i].P;
+        const size_t nt = (size_t)P.ntask + 1, ns = (size_t)P.nslot + 1;
+        if (ensure((void**)&P.task, &P.task_bytes, sizeof(int4) * nt)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.tns, &P.tns_bytes, sizeof(int) * nt)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.tslot, &P.tslot_bytes, sizeof(int) * nt)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.tkey, &P.tkey_bytes, sizeof(int) * nt)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.inc_task, &P.inc_task_bytes, sizeof(int) * 2 * nt)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.slot_cnt, &P.slot_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.slot_off, &P.slot_off_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
+        const int nsc = std::max(std::max(m[i].d->nb, m[i].d->ne), P.nslot);
+        if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(nsc))) return MEL_ERR_OOM;
+    }
+    J = upload_jobs(C, m, act, hj);
+    if (!J) return MEL_ERR_CUDA;
+    if ((rc = launch_jobs(C, zero_tcnt_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb + 1; }), 1))) return rc;
+    if ((rc = launch_jobs(C, task_fill_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.d.nb : 0; }), 1))) return rc;
+    if ((rc = launch_jobs(C, count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 32))) return rc;
+    {
+        std::vector<scan_req> sc;
+        for (int i : act) sc.push_back({ m[i].P->slot_cnt, m[i].P->slot_off, m[i].P->nslot, m[i].P->scan_ws });
+        if ((rc = scan_many(C, sc))) return rc;
+    }
+    readback_kernel<<<((int)act.size() + 127) / 128, 128, 0, s>>>(J, (int)act.size(), 1); C.launches++;
+    if ((rc = launch_status(__LINE__))) return rc;
+    if (!read_back(C, n)) return MEL_ERR_CUDA;
+    // 4. the new list, written into the spare buffer with history inherited from the current one
+    for (int i : act) {
+        mel_prox_state& P = *m[i].P;
+        const size_t total = (size_t)C.S.rb_h[8 * i + 5];
+        if (ensure((void**)&P.cont_alt, &P.cont_alt_bytes, sizeof(mel_contact) * (total + 1))) return MEL_ERR_OOM;
+        if (ensure((void**)&P.cont_w, &P.cont_w_bytes, sizeof(double) * (total + 1))) return MEL_ERR_OOM;
+        if (ensure((void**)&P.cont_rt, &P.cont_rt_bytes, 6 * sizeof(double) * (total + 1))) return MEL_ERR_OOM;
+        if (ensure((void**)&P.inc_rng, &P.inc_rng_bytes, sizeof(int2) * ((size_t)P.ntask + 1))) return MEL_ERR_OOM;
+    }
+    J = upload_jobs(C, m, act, hj);
+    if (!J) return MEL_ERR_CUDA;
+    if ((rc = launch_jobs(C, write_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 32))) return rc;
+    for (int i : act) {
+        mel_dev& d = *m[i].d;
+        mel_prox_state& P = *m[i].P;
+        mel_contact* old = d.cont;
+        const size_t old_bytes = P.cont_bytes;
+        d.cont = P.cont_alt; P.cont_bytes = P.cont_alt_bytes;
+        P.cont_alt = old; P.cont_alt_bytes = old_bytes;
+        d.ncont = C.S.rb_h[8 * i + 5];
+        d.cont_w = P.cont_w;
+        d.cont_rt = P.cont_rt;
+        d.inc_rng = P.inc_rng;
+        d.b_inc0 = P.b_inc0;
+        d.b_cont0 = P.b_cont0;
+        // the old index is read by the write pass just launched; freeing it waits for that pass
+        if (ensure((void**)&P.e_list, &P.e_list_bytes, sizeof(int) * ((size_t)d.ncont + 1))) return MEL_ERR_OOM;
+    }
+    J = upload_jobs(C, m, act, hj);
+    if (!J) return MEL_ERR_CUDA;
+    if ((rc = launch_jobs(C, zero_contw_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.ncont + 1; }), 1))) return rc;
+    // 5. incoming ranges in send order
+    {
+        std::vector<scan_req> sc;
+        for (int i : act) sc.push_back({ m[i].P->tcnt, m[i].P->b_inc0, m[i].d->nb, m[i].P->scan_ws });
+        if ((rc = scan_many(C, sc))) return rc;
+    }
+    if ((rc = launch_jobs(C, copy_inc_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.d.nb : 0; }), 1))) return rc;
+    if ((rc = launch_jobs(C, inc_fill_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 1))) return rc;
+    if ((rc = launch_jobs(C, inc_sort_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.d.nb : 0; }), 32))) return rc;
+    if ((rc = launch_jobs(C, inc_range_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 1))) return rc;
+    // 6. per-entry index of the new list; vgapn/vgapt carry of new elements
+    if ((rc = index_stage(C, m, act, J, hj))) return rc;
+    if ((rc = launch_jobs(C, carry_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 1))) return rc;
+    launches += C.launches;
     return launch_status(__LINE__);
 }
 
 int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cudaStream_t s)
 {
-    using namespace mel;
     (void)H;
-    const int nb = d.nb;
-    // 1. border boxes and segment-block boxes
-    aabb_kernel<<<(d.nbd * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax); P.launches++;
-    if (d.nblk > 0) { segblock_kernel<<<(d.nblk + 127) / 128, 128, 0, s>>>(d); P.launches++; }
-    if (d.nsblk > 0) { superblock_kernel<<<(d.nsblk + 127) / 128, 128, 0, s>>>(d); P.launches++; }
-    // 2. neighbours and the task list; one read-back: overflow flag, task count, slot count
-    int ntask = 0, nslot = 0;
-    bool overflow = true;
-    for (int attempt = 0; attempt < 4 && overflow; attempt++) {
-        cudaMemsetAsync(d.err + MEL_E_NBR_OVERFLOW, 0, sizeof(unsigned), s);
-        cudaMemsetAsync(d.err + MEL_E_NBR_NEED, 0, sizeof(unsigned), s);
-        neighbour_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(d, P.aabb, P.shmin, P.shmax, P.nbr, P.nbn, P.nbr_cap); P.launches++;
-        task_count_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, P.nbn, P.tcnt, P.scnt); P.launches++;
-        if (mel_scan_exclusive(P.tcnt, P.btask0, nb, P, s)) return MEL_ERR_OOM;
-        if (mel_scan_exclusive(P.scnt, P.bslot0, nb, P, s)) return MEL_ERR_OOM;
-        unsigned hv[MEL_E_NWORDS];
-        cudaMemcpyAsync(hv, d.err, sizeof hv, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&ntask, P.btask0 + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&nslot, P.bslot0 + nb, sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (sync_failed(s, __LINE__)) return MEL_ERR_CUDA;
-        if (hv[MEL_E_NAN]) {
-            mel_set_error(hv[MEL_E_NAN] & 1u ? "non-finite node positions at the proximity update"
-                                             : "a border box spans more than %d periods: diverged positions",
-                          MEL_MAX_SHIFT_SPAN);
-            return MEL_ERR_NAN;
-        }
-        hv[0] = hv[MEL_E_NBR_OVERFLOW]; hv[1] = hv[MEL_E_NBR_NEED];
-        overflow = hv[0] != 0;
-        if (!overflow) break;
-        int need = (int)hv[1] + 16;
-        cudaFree(P.nbr); P.nbr = nullptr;
-        if (cudaMalloc(&P.nbr, sizeof(int) * 3 * (size_t)need * nb) != cudaSuccess) {
-            mel_set_error("allocation of neighbour lists (%d per body) failed", need);
-            return MEL_ERR_OOM;
-        }
-        P.nbr_cap = need;
-    }
-    if (overflow) { mel_set_error("neighbour lists still over capacity after 4 attempts"); return MEL_ERR_BOUNDS; }
-    if (ensure((void**)&P.task, &P.task_bytes, sizeof(int4) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.tns, &P.tns_bytes, sizeof(int) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.tslot, &P.tslot_bytes, sizeof(int) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.tkey, &P.tkey_bytes, sizeof(int) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.inc_task, &P.inc_task_bytes, sizeof(int) * 2 * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    int4* task = (int4*)P.task;
-    cudaMemsetAsync(P.tcnt, 0, sizeof(int) * (nb + 1), s);
-    if (ntask > 0) {
-        task_fill_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, P.nbr, P.nbn, P.nbr_cap, P.btask0, P.bslot0, task, P.tns,
-                                                          P.tslot, P.tkey, P.tcnt);
-        P.launches++;
-    }
-    if (ensure((void**)&P.slot_cnt, &P.slot_bytes, sizeof(int) * (size_t)(nslot + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.slot_off, &P.slot_off_bytes, sizeof(int) * (size_t)(nslot + 1))) return MEL_ERR_OOM;
-    // 3. count, scan, total
-    if (ntask > 0) { count_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, task, ntask, P.nbr, P.nbr_cap, P.slot_cnt); P.launches++; }
-    if (mel_scan_exclusive(P.slot_cnt, P.slot_off, nslot, P, s)) return MEL_ERR_OOM;
-    int total = 0;
-    cudaMemcpyAsync(&total, P.slot_off + nslot, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (sync_failed(s, __LINE__)) return MEL_ERR_CUDA;
-    // 4. write the new list into the spare buffer, inheriting from the current one
-    if (ensure((void**)&P.cont_alt, &P.cont_alt_bytes, sizeof(mel_contact) * (size_t)(total + 1))) return MEL_ERR_OOM;
-    if (ntask > 0) {
-        write_kernel<<<(ntask * 32 + 255) / 256, 256, 0, s>>>(d, task, ntask, P.nbr, P.nbr_cap, P.slot_off, P.cont_alt,
-                                                             d.cont, P.e_ptr, P.e_list, d.ncont > 0 ? 1 : 0);
-        P.launches++;
-    }
-    mel_contact* old = d.cont;
-    size_t old_bytes = P.cont_bytes;
-    d.cont = P.cont_alt; P.cont_bytes = P.cont_alt_bytes;
-    P.cont_alt = old; P.cont_alt_bytes = old_bytes;
-    d.ncont = total;
-    if (ensure((void**)&P.cont_w, &P.cont_w_bytes, sizeof(double) * (size_t)(total + 1))) return MEL_ERR_OOM;
-    cudaMemsetAsync(P.cont_w, 0, sizeof(double) * (total + 1), s);
-    d.cont_w = P.cont_w;
-    if (ensure((void**)&P.cont_rt, &P.cont_rt_bytes, 6 * sizeof(double) * (size_t)(total + 1))) return MEL_ERR_OOM;
-    d.cont_rt = P.cont_rt;
-    // 5. incoming ranges in send order
-    if (ensure((void**)&P.inc_rng, &P.inc_rng_bytes, sizeof(int2) * (size_t)(ntask + 1))) return MEL_ERR_OOM;
-    if (mel_scan_exclusive(P.tcnt, P.b_inc0, nb, P, s)) return MEL_ERR_OOM;
-    if (ntask > 0) {
-        int* tmp = P.inc_task;
-        int* sorted = P.inc_task + ntask;
-        cudaMemcpyAsync(P.tcnt, P.b_inc0, sizeof(int) * nb, cudaMemcpyDeviceToDevice, s);
-        inc_fill_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(P.tkey, ntask, P.tcnt, tmp); P.launches++;
-        inc_sort_kernel<<<(nb * 32 + 255) / 256, 256, 0, s>>>(nb, P.b_inc0, tmp, sorted); P.launches++;
-        inc_range_kernel<<<(ntask + 127) / 128, 128, 0, s>>>(sorted, ntask, P.tslot, P.tns, P.slot_off, P.inc_rng); P.launches++;
-    }
-    d.inc_rng = P.inc_rng;
-    d.b_inc0 = P.b_inc0;
-    // 6. per-entry index of the new list; vgapn/vgapt carry of new elements
-    int rc = mel_index_contacts(d, P, s);
-    d.b_cont0 = P.b_cont0;
-    carry_kernel<<<(nb + 127) / 128, 128, 0, s>>>(d, d.cont, P.b_cont0); P.launches++;
-    P.ntask = ntask; P.nslot = nslot;
+    mel_prox_member m;
+    m.d = &d;
+    m.P = &P;
+    int launches = 0;
+    const int rc = mel_run_proximity_many(&m, 1, P.stage, launches, s);
+    P.launches += launches;
     if (rc) return rc;
-    return launch_status(__LINE__);
+    if (m.rc) { mel_set_error("%s", m.msg.c_str()); return m.rc; }
+    return MEL_OK;
 }
 
 // Index structures for a list supplied by the caller (mel_set_contacts): incoming ranges are built
@@ -730,8 +1031,23 @@ int mel_index_external(mel_dev& d, mel_prox_state& P, const mel_contact* host_li
     cudaMemcpyAsync(P.b_inc0, cnt.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice, s);
     d.inc_rng = P.inc_rng;
     d.b_inc0 = P.b_inc0;
-    int rc = mel_index_contacts(d, P, s);
     d.b_cont0 = P.b_cont0;
+    if (ensure((void**)&P.e_list, &P.e_list_bytes, sizeof(int) * ((size_t)d.ncont + 1))) return MEL_ERR_OOM;
+    if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(std::max(d.nb, d.ne)))) return MEL_ERR_OOM;
+    if (!stage_ready(P.stage, 1)) { mel_set_error("proximity read-back buffers could not be allocated"); return MEL_ERR_OOM; }
+    mel_prox_member m;
+    m.d = &d;
+    m.P = &P;
+    run_ctx C{ *P.stage, s, 0 };
+    std::vector<mel_prox_job> hj;
+    const std::vector<int> idx{ 0 };
+    const mel_prox_job* J = upload_jobs(C, &m, idx, hj);
+    if (!J) return MEL_ERR_CUDA;
+    int rc = index_stage(C, &m, idx, J, hj);
+    P.launches += C.launches;
+    if (rc) return rc;
     if (sync_failed(s, __LINE__)) return MEL_ERR_CUDA;
-    return rc;
+    C.S.used = 0;
+    stage_release_retired(C.S);
+    return launch_status(__LINE__);
 }

@@ -1,7 +1,11 @@
-// Host-side state of the proximity pipeline (mel_prox.cu) owned by a solver handle.
+// Host-side state of the proximity pipeline (mel_prox.cu) owned by a solver handle, and the job
+// table through which one set of launches serves several models (the members of a batch).
 #pragma once
+#include <string>
 #include <vector>
 #include "mel_internal.h"
+
+struct mel_prox_stage;   // staging buffers of a run (pinned host + device), opaque
 
 struct mel_prox_state {
     int nbr_cap = MEL_NBR_CAP_DEFAULT;
@@ -27,13 +31,42 @@ struct mel_prox_state {
     int* scan_ws = nullptr; size_t scan_ws_bytes = 0;    // scan block totals
     int ntask = 0, nslot = 0;
     int launches = 0;                                      // kernels launched by the pipeline (running count)
+    mel_prox_stage* stage = nullptr;                       // staging of this handle's own runs
 };
 
 struct mel_prox_host {
     std::vector<int> b_type, b_per, b_bd0, bd_e0;
 };
 
+// One model's part of a run, as the kernels see it: its descriptor and its own buffers.
+struct mel_prox_job {
+    mel_dev d;
+    double* aabb; int* shmin; int* shmax;
+    int* nbr; int* nbn; int nbr_cap;
+    int ntask, nslot, have_old;
+    int4* task; int* tns; int* tslot; int* tkey;
+    int* tcnt; int* btask0; int* scnt; int* bslot0;
+    int* slot_cnt; int* slot_off; int* inc_task;
+    int2* inc_rng; int* b_inc0; int* b_cont0;
+    int* e_cnt; int* e_ptr; int* e_cur; int* e_list;
+    mel_contact* cont_new;        // the list being written (write stage)
+    int* readback;                // this member's words of the run's read-back array
+};
+
+// A model taking part in a run.  rc: MEL_OK, or the member's own failure (MEL_ERR_NAN,
+// MEL_ERR_BOUNDS) with msg; the other members carry on.
+struct mel_prox_member {
+    mel_dev* d;
+    mel_prox_state* P;
+    int rc = 0;
+    std::string msg;
+};
+
+// Update_proximity of several models with one set of launches on stream s.  Returns MEL_OK when
+// the run itself went through (members may still have failed: see their rc), else the status of
+// a failure that stops every member (allocation, CUDA).  launches: kernels launched.
+int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, int& launches, cudaStream_t s);
+void mel_prox_stage_free(mel_prox_stage* stage);
+
 int mel_run_proximity(mel_dev& d, mel_prox_state& P, const mel_prox_host& H, cudaStream_t s);
-int mel_index_contacts(mel_dev& d, mel_prox_state& P, cudaStream_t s);
 int mel_index_external(mel_dev& d, mel_prox_state& P, const mel_contact* host_list, int n, cudaStream_t s);
-int mel_scan_exclusive(const int* in, int* out, int n, mel_prox_state& P, cudaStream_t s);
