@@ -649,9 +649,13 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
             if (*s_abort) break;
             // pull: each touched node subtracts its contributions in ascending Gauss-point order
             // (the mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31
-            // of group t >> 5 (t = tid + 224 i keeps the lane), its entry j at row j of the
-            // group's row table.
-            for (int t = tid; t < hdr.z; t += MEL_BODY_CTHREADS) {
+            // of group t >> 5, its entry j at row j of the group's row table.  Groups are sorted
+            // by entry count; warp w takes groups w, 13 - w, 14 + w, ... (snake order), so the
+            // heaviest group has a warp to itself and the lighter ones pair up.
+            const int ngrp = (hdr.z + 31) >> 5;
+            for (int i = 0; 7 * i < ngrp; i++) {
+                const int t = (7 * i + ((i & 1) ? 6 - warp : warp)) * 32 + lane;
+                if (t >= hdr.z) continue;
                 const unsigned rec = s_tn[t];
                 const int node = (int)(rec & 0xfffu);
                 const int cnt = (int)((rec >> 12) & 0xffu);
@@ -668,6 +672,16 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
                         float2 c[8];
 #pragma unroll
                         for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[pbase + 32 * (j + i) + lane]];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                    }
+                    for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
+                        int q[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
+                        float2 c[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[q[i]]];
 #pragma unroll
                         for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
                     }
@@ -689,6 +703,16 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
                         double2 c[8];
 #pragma unroll
                         for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[pbase + 32 * (j + i) + lane]];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                    }
+                    for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
+                        int q[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
+                        double2 c[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[q[i]]];
 #pragma unroll
                         for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
                     }
