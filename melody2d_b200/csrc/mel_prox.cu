@@ -357,14 +357,26 @@ __device__ __forceinline__ void task_fill_item(const mel_dev& d, const int* nbr,
         }
 }
 
-__device__ __forceinline__ void count_item(const mel_dev& d, const int4* task, int ntask, const int* nbr, int cap,
-                                           int* slot_cnt, int t, int lane)
+// slot -> task map: warp per task, lanes over its slots
+__device__ __forceinline__ void slot_task_item(const mel_dev& d, const int4* task, int ntask, int* tmap, int t, int lane)
 {
     if (t >= ntask) return;
+    const int4 tk = task[t];
+    const int nS = d.bd_e0[tk.y + 1] - d.bd_e0[tk.y];
+    for (int kS = lane; kS < nS; kS += 32) tmap[tk.w + kS] = t;
+}
+
+// candidates of slot s (one slave border node of one task); one thread per slot, so a task with a
+// long slave border (a plate or a wall) spreads over many warps
+__device__ __forceinline__ void count_item(const mel_dev& d, const int4* task, const int* tmap, int nslot, const int* nbr,
+                                           int cap, int* slot_cnt, int s)
+{
+    if (s >= nslot) return;
+    int t = tmap[s];
     int4 tk = task[t];
     int bS = tk.x, gS = tk.y, q = tk.z, slot0 = tk.w;
-    int nS = d.bd_e0[gS + 1] - d.bd_e0[gS];
-    for (int kS = lane; kS < nS; kS += 32) {
+    {
+        const int kS = s - slot0;
         int cnt = 0;
         if (q >= 0) {
             const int* nb = nbr + (size_t)3 * cap * bS + 3 * q;
@@ -376,17 +388,19 @@ __device__ __forceinline__ void count_item(const mel_dev& d, const int4* task, i
     }
 }
 
-__device__ __forceinline__ void write_item(const mel_dev& d, const int4* task, int ntask, const int* nbr, int cap,
-                                           const int* slot_off, mel_contact* out, const mel_contact* old,
-                                           const int* old_eptr, const int* old_elist, int have_old, int t, int lane)
+// writes the candidates of slot s at their canonical positions; one thread per slot
+__device__ __forceinline__ void write_item(const mel_dev& d, const int4* task, const int* tmap, int nslot, const int* nbr,
+                                           int cap, const int* slot_off, mel_contact* out, const mel_contact* old,
+                                           const int* old_eptr, const int* old_elist, int have_old, int s)
 {
-    if (t >= ntask) return;
+    if (s >= nslot) return;
+    int t = tmap[s];
     int4 tk = task[t];
     int bS = tk.x, gS = tk.y, q = tk.z, slot0 = tk.w;
     int rS = gS - d.b_bd0[bS];
     int eS0 = d.bd_e0[gS];
-    int nS = d.bd_e0[gS + 1] - eS0;
-    for (int kS = lane; kS < nS; kS += 32) {
+    {
+        const int kS = s - slot0;
         int pos = slot_off[slot0 + kS];
         const int end = slot_off[slot0 + kS + 1];   // the count pass found end - pos candidates
         int eS = eS0 + kS;
@@ -476,20 +490,31 @@ __device__ __forceinline__ void inc_range_item(const int* sorted, int n, const i
 }
 
 
-// per-body serial counting sort of a body-major contact list by slave border entry
+// per-body counting sort of a body-major contact list by slave border entry: one warp per body,
+// 32 contacts at a time in list order; lanes with the same entry take consecutive places in lane
+// order, so every entry lists its contacts in list order (as a serial pass would)
 __device__ __forceinline__ void entry_index_item(const mel_dev& d, const mel_contact* cont, const int* b_cont0,
-                                                 int* eptr_cnt, int* elist, int b)
+                                                 int* eptr_cnt, int* elist, int b, int lane)
 {
     if (b >= d.nb) return;
-    int e_lo = d.bd_e0[d.b_bd0[b]], e_hi = d.bd_e0[d.b_bd0[b + 1]];
-    int c0 = b_cont0[b], c1 = b_cont0[b + 1];
-    // eptr_cnt holds the exclusive offsets of this body's entries (prepared by the caller);
-    // fill in list order, advancing a per-entry cursor kept in elist space of the body
-    for (int c = c0; c < c1; c++) {
-        int e = d.bd_e0[d.b_bd0[b] + cont[c].borderS] + cont[c].border_nodeS;
-        if (e < e_lo || e >= e_hi) { atomicOr(&d.err[MEL_E_BOUNDS], 2u); continue; }
-        int slot = atomicAdd(&eptr_cnt[e], 1);   // only this thread touches the entries of body b
-        elist[slot] = c;
+    const int e_lo = d.bd_e0[d.b_bd0[b]], e_hi = d.bd_e0[d.b_bd0[b + 1]];
+    const int c0 = b_cont0[b], c1 = b_cont0[b + 1];
+    // eptr_cnt holds the exclusive offsets of this body's entries (prepared by the caller) and is
+    // advanced as a cursor; only this warp touches the entries of body b
+    for (int base = c0; base < c1; base += 32) {
+        const int c = base + lane;
+        int e = -1;
+        if (c < c1) {
+            e = d.bd_e0[d.b_bd0[b] + cont[c].borderS] + cont[c].border_nodeS;
+            if (e < e_lo || e >= e_hi) { atomicOr(&d.err[MEL_E_BOUNDS], 2u); e = -1; }
+        }
+        const unsigned same = __match_any_sync(0xffffffffu, e);
+        const int leader = __ffs(same) - 1;
+        int pos = 0;
+        if (lane == leader && e >= 0) { pos = eptr_cnt[e]; eptr_cnt[e] = pos + __popc(same); }
+        pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(same & ((1u << lane) - 1u));
+        if (e >= 0) elist[pos] = c;
+        __syncwarp();
     }
 }
 
@@ -512,16 +537,39 @@ __device__ __forceinline__ void body_range_item(const mel_contact* cont, int n, 
 
 // Newly created elements leave vgapn/vgapt unassigned in the reference: they keep the values of the
 // element pushed before them in the slave body's list (the reused new_contact variable,
-// Code/Proximity.h:286-313); self contacts use a fresh variable (Code/Proximity.h:350).
-__device__ __forceinline__ void carry_item(const mel_dev& d, mel_contact* cont, const int* b_cont0, int b)
+// Code/Proximity.h:286-313); self contacts use a fresh variable (Code/Proximity.h:350).  One warp
+// per body, 32 contacts at a time: a new element takes the values of the last inherited non-self
+// element before it (found by ballot within the 32, else carried over from earlier ones).
+__device__ __forceinline__ void carry_item(const mel_dev& d, mel_contact* cont, const int* b_cont0, int b, int lane)
 {
     if (b >= d.nb) return;
-    double vn = 0., vt = 0.;
-    for (int c = b_cont0[b]; c < b_cont0[b + 1]; c++) {
-        mel_contact& k = cont[c];
-        if (k.bodyM == b) { if (k.pad_) { k.vgapn = 0.; k.vgapt = 0.; } k.pad_ = 0; continue; }
-        if (k.pad_) { k.vgapn = vn; k.vgapt = vt; k.pad_ = 0; }
-        else { vn = k.vgapn; vt = k.vgapt; }
+    double vn = 0., vt = 0.;                 // carried value (equal in all lanes)
+    const int c0 = b_cont0[b], c1 = b_cont0[b + 1];
+    for (int base = c0; base < c1; base += 32) {
+        const int c = base + lane;
+        const bool valid = c < c1;
+        int bodyM = -1, pad = 0;
+        double gn = 0., gt = 0.;
+        if (valid) { bodyM = cont[c].bodyM; pad = cont[c].pad_; gn = cont[c].vgapn; gt = cont[c].vgapt; }
+        const bool self = bodyM == b;
+        const bool src = valid && !self && !pad;          // inherited non-self elements set the value
+        const unsigned m = __ballot_sync(0xffffffffu, src);
+        const unsigned lower = m & ((1u << lane) - 1u);
+        const int from = lower ? 31 - __clz(lower) : 0;
+        const double sn = __shfl_sync(0xffffffffu, gn, from), st = __shfl_sync(0xffffffffu, gt, from);
+        if (valid && pad) {
+            if (self) { cont[c].vgapn = 0.; cont[c].vgapt = 0.; }
+            else if (lower) { cont[c].vgapn = sn; cont[c].vgapt = st; }
+            else { cont[c].vgapn = vn; cont[c].vgapt = vt; }
+            cont[c].pad_ = 0;
+        } else if (valid && self) {
+            cont[c].pad_ = 0;
+        }
+        if (m) {
+            const int last = 31 - __clz(m);
+            vn = __shfl_sync(0xffffffffu, gn, last);
+            vt = __shfl_sync(0xffffffffu, gt, last);
+        }
     }
 }
 
@@ -559,9 +607,10 @@ JOB_KERNEL(task_count_kernel, 1, task_count_item(d, j.nbn, j.tcnt, j.scnt, it))
 JOB_KERNEL(zero_tcnt_kernel, 1, if (it <= d.nb) j.tcnt[it] = 0)
 JOB_KERNEL(task_fill_kernel, 1, task_fill_item(d, j.nbr, j.nbn, j.nbr_cap, j.btask0, j.bslot0, j.task, j.tns, j.tslot,
                                                j.tkey, j.tcnt, it))
-JOB_KERNEL(count_kernel, 32, count_item(d, j.task, j.ntask, j.nbr, j.nbr_cap, j.slot_cnt, it, lane))
-JOB_KERNEL(write_kernel, 32, write_item(d, j.task, j.ntask, j.nbr, j.nbr_cap, j.slot_off, j.cont_new, d.cont, j.e_ptr,
-                                        j.e_list, j.have_old, it, lane))
+JOB_KERNEL(slot_task_kernel, 32, slot_task_item(d, j.task, j.ntask, j.tmap, it, lane))
+JOB_KERNEL(count_kernel, 1, count_item(d, j.task, j.tmap, j.nslot, j.nbr, j.nbr_cap, j.slot_cnt, it))
+JOB_KERNEL(write_kernel, 1, write_item(d, j.task, j.tmap, j.nslot, j.nbr, j.nbr_cap, j.slot_off, j.cont_new, d.cont,
+                                       j.e_ptr, j.e_list, j.have_old, it))
 JOB_KERNEL(zero_contw_kernel, 1, if (it <= d.ncont) d.cont_w[it] = 0.)
 JOB_KERNEL(copy_inc_kernel, 1, if (it < d.nb) j.tcnt[it] = j.b_inc0[it])
 JOB_KERNEL(inc_fill_kernel, 1, inc_fill_item(j.tkey, j.ntask, j.tcnt, j.inc_task, it))
@@ -571,8 +620,8 @@ JOB_KERNEL(body_range_kernel, 1, body_range_item(d.cont, d.ncont, d.nb, j.b_cont
 JOB_KERNEL(zero_ecnt_kernel, 1, if (it <= d.ne) j.e_cnt[it] = 0)
 JOB_KERNEL(entry_count_kernel, 1, entry_count_item(d, d.cont, d.ncont, j.e_cnt, it))
 JOB_KERNEL(copy_eptr_kernel, 1, if (it <= d.ne) j.e_cur[it] = j.e_ptr[it])
-JOB_KERNEL(entry_index_kernel, 1, entry_index_item(d, d.cont, j.b_cont0, j.e_cur, j.e_list, it))
-JOB_KERNEL(carry_kernel, 1, carry_item(d, d.cont, j.b_cont0, it))
+JOB_KERNEL(entry_index_kernel, 32, entry_index_item(d, d.cont, j.b_cont0, j.e_cur, j.e_list, it, lane))
+JOB_KERNEL(carry_kernel, 32, carry_item(d, d.cont, j.b_cont0, it, lane))
 
 // one thread per member: clear the neighbour-overflow words before an attempt
 __global__ void nbr_clear_kernel(const mel_prox_job* J, int nj)
@@ -772,7 +821,7 @@ mel_prox_job make_job(const mel_prox_member& m, int* readback)
     j.ntask = P.ntask; j.nslot = P.nslot; j.have_old = m.d->ncont > 0 ? 1 : 0;
     j.task = (int4*)P.task; j.tns = P.tns; j.tslot = P.tslot; j.tkey = P.tkey;
     j.tcnt = P.tcnt; j.btask0 = P.btask0; j.scnt = P.scnt; j.bslot0 = P.bslot0;
-    j.slot_cnt = P.slot_cnt; j.slot_off = P.slot_off; j.inc_task = P.inc_task;
+    j.slot_cnt = P.slot_cnt; j.slot_off = P.slot_off; j.inc_task = P.inc_task; j.tmap = P.tmap;
     j.inc_rng = P.inc_rng; j.b_inc0 = P.b_inc0; j.b_cont0 = P.b_cont0;
     j.e_cnt = P.e_cnt; j.e_ptr = P.e_ptr; j.e_cur = P.e_cur; j.e_list = P.e_list;
     j.cont_new = P.cont_alt;
@@ -814,7 +863,7 @@ int index_stage(run_ctx& C, mel_prox_member* m, const std::vector<int>& idx, con
     for (int i : idx) sc.push_back({ m[i].P->e_cnt, m[i].P->e_ptr, m[i].d->ne, m[i].P->scan_ws });
     if ((rc = scan_many(C, sc))) return rc;
     if ((rc = launch_jobs(C, copy_eptr_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.ne + 1; }), 1))) return rc;
-    return launch_jobs(C, entry_index_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 1);
+    return launch_jobs(C, entry_index_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 32);
 }
 
 bool stage_ready(mel_prox_stage*& stage, int n)
@@ -933,6 +982,7 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
         if (ensure((void**)&P.inc_task, &P.inc_task_bytes, sizeof(int) * 2 * nt)) return MEL_ERR_OOM;
         if (ensure((void**)&P.slot_cnt, &P.slot_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
         if (ensure((void**)&P.slot_off, &P.slot_off_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.tmap, &P.tmap_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
         const int nsc = std::max(std::max(m[i].d->nb, m[i].d->ne), P.nslot);
         if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(nsc))) return MEL_ERR_OOM;
     }
@@ -940,7 +990,8 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
     if (!J) return MEL_ERR_CUDA;
     if ((rc = launch_jobs(C, zero_tcnt_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb + 1; }), 1))) return rc;
     if ((rc = launch_jobs(C, task_fill_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.d.nb : 0; }), 1))) return rc;
-    if ((rc = launch_jobs(C, count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 32))) return rc;
+    if ((rc = launch_jobs(C, slot_task_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 32))) return rc;
+    if ((rc = launch_jobs(C, count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.nslot : 0; }), 1))) return rc;
     {
         std::vector<scan_req> sc;
         for (int i : act) sc.push_back({ m[i].P->slot_cnt, m[i].P->slot_off, m[i].P->nslot, m[i].P->scan_ws });
@@ -960,7 +1011,7 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
     }
     J = upload_jobs(C, m, act, hj);
     if (!J) return MEL_ERR_CUDA;
-    if ((rc = launch_jobs(C, write_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 32))) return rc;
+    if ((rc = launch_jobs(C, write_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.nslot : 0; }), 1))) return rc;
     for (int i : act) {
         mel_dev& d = *m[i].d;
         mel_prox_state& P = *m[i].P;
@@ -992,7 +1043,7 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
     if ((rc = launch_jobs(C, inc_range_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 1))) return rc;
     // 6. per-entry index of the new list; vgapn/vgapt carry of new elements
     if ((rc = index_stage(C, m, act, J, hj))) return rc;
-    if ((rc = launch_jobs(C, carry_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 1))) return rc;
+    if ((rc = launch_jobs(C, carry_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 32))) return rc;
     launches += C.launches;
     return launch_status(__LINE__);
 }
