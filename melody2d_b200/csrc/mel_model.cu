@@ -723,7 +723,7 @@ mel_status mel_destroy(mel_handle* h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void* p : h->allocs) cudaFree(p);
     mel_prox_state& P = h->P;
-    for (void* p : { (void*)P.nbr, (void*)P.task, (void*)P.inc_task, (void*)P.slot_cnt, (void*)P.slot_off, (void*)P.tmap, (void*)P.inc_rng,
+    for (void* p : { (void*)P.nbr, (void*)P.task, (void*)P.inc_task, (void*)P.slot_cnt, (void*)P.slot_off, (void*)P.tmap, (void*)P.nzoff, (void*)P.nzlist, (void*)P.inc_rng,
                      (void*)P.scan_ws,
                      (void*)P.tns, (void*)P.tslot, (void*)P.tkey,
                      (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)P.cont_rt, (void*)h->d.cont })

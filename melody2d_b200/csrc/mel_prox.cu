@@ -389,11 +389,13 @@ __device__ __forceinline__ void count_item(const mel_dev& d, const int4* task, c
 }
 
 // writes the candidates of slot s at their canonical positions; one thread per slot
-__device__ __forceinline__ void write_item(const mel_dev& d, const int4* task, const int* tmap, int nslot, const int* nbr,
-                                           int cap, const int* slot_off, mel_contact* out, const mel_contact* old,
-                                           const int* old_eptr, const int* old_elist, int have_old, int s)
+__device__ __forceinline__ void write_item(const mel_dev& d, const int4* task, const int* tmap, const int* nzlist,
+                                           int nnz, const int* nbr, int cap, const int* slot_off, mel_contact* out,
+                                           const mel_contact* old, const int* old_eptr, const int* old_elist,
+                                           int have_old, int i)
 {
-    if (s >= nslot) return;
+    if (i >= nnz) return;
+    const int s = nzlist[i];                 // slots with at least one candidate
     int t = tmap[s];
     int4 tk = task[t];
     int bS = tk.x, gS = tk.y, q = tk.z, slot0 = tk.w;
@@ -609,8 +611,11 @@ JOB_KERNEL(task_fill_kernel, 1, task_fill_item(d, j.nbr, j.nbn, j.nbr_cap, j.bta
                                                j.tkey, j.tcnt, it))
 JOB_KERNEL(slot_task_kernel, 32, slot_task_item(d, j.task, j.ntask, j.tmap, it, lane))
 JOB_KERNEL(count_kernel, 1, count_item(d, j.task, j.tmap, j.nslot, j.nbr, j.nbr_cap, j.slot_cnt, it))
-JOB_KERNEL(write_kernel, 1, write_item(d, j.task, j.tmap, j.nslot, j.nbr, j.nbr_cap, j.slot_off, j.cont_new, d.cont,
-                                       j.e_ptr, j.e_list, j.have_old, it))
+// slots with candidates: flags in place of the counts (after their scan), then their list
+JOB_KERNEL(nz_flag_kernel, 1, if (it < j.nslot) j.slot_cnt[it] = j.slot_cnt[it] > 0 ? 1 : 0)
+JOB_KERNEL(nz_list_kernel, 1, if (it < j.nslot && j.slot_cnt[it]) j.nzlist[j.nzoff[it]] = it)
+JOB_KERNEL(write_kernel, 1, write_item(d, j.task, j.tmap, j.nzlist, j.nnz, j.nbr, j.nbr_cap, j.slot_off, j.cont_new,
+                                       d.cont, j.e_ptr, j.e_list, j.have_old, it))
 JOB_KERNEL(zero_contw_kernel, 1, if (it <= d.ncont) d.cont_w[it] = 0.)
 JOB_KERNEL(copy_inc_kernel, 1, if (it < d.nb) j.tcnt[it] = j.b_inc0[it])
 JOB_KERNEL(inc_fill_kernel, 1, inc_fill_item(j.tkey, j.ntask, j.tcnt, j.inc_task, it))
@@ -647,6 +652,7 @@ __global__ void readback_kernel(const mel_prox_job* J, int nj, int stage)
         r[4] = j.bslot0[j.d.nb];
     } else {
         r[5] = j.slot_off[j.nslot];
+        r[6] = j.nzoff[j.nslot];
     }
 }
 
@@ -658,7 +664,7 @@ __global__ void readback_kernel(const mel_prox_job* J, int nj, int stage)
 static int ensure_impl(void** p, size_t* cap_bytes, size_t need, const char* what)
 {
     if (need <= *cap_bytes && *p) return 0;
-    size_t nc = need + need / 2 + 4096;
+    size_t nc = 2 * need + 4096;            // doubling: few reallocations (each free synchronises the device)
     void* np = nullptr;
     cudaError_t e = cudaMalloc(&np, nc);
     if (e != cudaSuccess) {
@@ -822,6 +828,7 @@ mel_prox_job make_job(const mel_prox_member& m, int* readback)
     j.task = (int4*)P.task; j.tns = P.tns; j.tslot = P.tslot; j.tkey = P.tkey;
     j.tcnt = P.tcnt; j.btask0 = P.btask0; j.scnt = P.scnt; j.bslot0 = P.bslot0;
     j.slot_cnt = P.slot_cnt; j.slot_off = P.slot_off; j.inc_task = P.inc_task; j.tmap = P.tmap;
+    j.nzoff = P.nzoff; j.nzlist = P.nzlist; j.nnz = P.nnz;
     j.inc_rng = P.inc_rng; j.b_inc0 = P.b_inc0; j.b_cont0 = P.b_cont0;
     j.e_cnt = P.e_cnt; j.e_ptr = P.e_ptr; j.e_cur = P.e_cur; j.e_list = P.e_list;
     j.cont_new = P.cont_alt;
@@ -983,6 +990,8 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
         if (ensure((void**)&P.slot_cnt, &P.slot_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
         if (ensure((void**)&P.slot_off, &P.slot_off_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
         if (ensure((void**)&P.tmap, &P.tmap_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.nzoff, &P.nzoff_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
+        if (ensure((void**)&P.nzlist, &P.nzlist_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
         const int nsc = std::max(std::max(m[i].d->nb, m[i].d->ne), P.nslot);
         if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(nsc))) return MEL_ERR_OOM;
     }
@@ -993,9 +1002,16 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
     if ((rc = launch_jobs(C, slot_task_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask; }), 32))) return rc;
     if ((rc = launch_jobs(C, count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.nslot : 0; }), 1))) return rc;
     {
-        std::vector<scan_req> sc;
-        for (int i : act) sc.push_back({ m[i].P->slot_cnt, m[i].P->slot_off, m[i].P->nslot, m[i].P->scan_ws });
+        std::vector<scan_req> sc, sz;
+        for (int i : act) {
+            sc.push_back({ m[i].P->slot_cnt, m[i].P->slot_off, m[i].P->nslot, m[i].P->scan_ws });
+            sz.push_back({ m[i].P->slot_cnt, m[i].P->nzoff, m[i].P->nslot, m[i].P->scan_ws });
+        }
         if ((rc = scan_many(C, sc))) return rc;
+        // the write pass visits only the slots with candidates (a few in a thousand)
+        if ((rc = launch_jobs(C, nz_flag_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.nslot : 0; }), 1))) return rc;
+        if ((rc = scan_many(C, sz))) return rc;
+        if ((rc = launch_jobs(C, nz_list_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.nslot : 0; }), 1))) return rc;
     }
     readback_kernel<<<((int)act.size() + 127) / 128, 128, 0, s>>>(J, (int)act.size(), 1); C.launches++;
     if ((rc = launch_status(__LINE__))) return rc;
@@ -1004,6 +1020,7 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
     for (int i : act) {
         mel_prox_state& P = *m[i].P;
         const size_t total = (size_t)C.S.rb_h[8 * i + 5];
+        P.nnz = C.S.rb_h[8 * i + 6];
         if (ensure((void**)&P.cont_alt, &P.cont_alt_bytes, sizeof(mel_contact) * (total + 1))) return MEL_ERR_OOM;
         if (ensure((void**)&P.cont_w, &P.cont_w_bytes, sizeof(double) * (total + 1))) return MEL_ERR_OOM;
         if (ensure((void**)&P.cont_rt, &P.cont_rt_bytes, 6 * sizeof(double) * (total + 1))) return MEL_ERR_OOM;
@@ -1011,7 +1028,7 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
     }
     J = upload_jobs(C, m, act, hj);
     if (!J) return MEL_ERR_CUDA;
-    if ((rc = launch_jobs(C, write_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.nslot : 0; }), 1))) return rc;
+    if ((rc = launch_jobs(C, write_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.ntask > 0 ? j.nnz : 0; }), 1))) return rc;
     for (int i : act) {
         mel_dev& d = *m[i].d;
         mel_prox_state& P = *m[i].P;

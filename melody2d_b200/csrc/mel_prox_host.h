@@ -21,6 +21,9 @@ struct mel_prox_state {
     int* slot_cnt = nullptr; size_t slot_bytes = 0;
     int* slot_off = nullptr; size_t slot_off_bytes = 0;
     int* tmap = nullptr; size_t tmap_bytes = 0;             // task of each slot
+    int* nzoff = nullptr; size_t nzoff_bytes = 0;           // slots with candidates: offsets, list
+    int* nzlist = nullptr; size_t nzlist_bytes = 0;
+    int nnz = 0;
     int2* inc_rng = nullptr; size_t inc_rng_bytes = 0;
     int* b_inc0 = nullptr; int* b_cont0 = nullptr;
     int* e_cnt = nullptr; int* e_ptr = nullptr; int* e_cur = nullptr;
@@ -48,6 +51,7 @@ struct mel_prox_job {
     int4* task; int* tns; int* tslot; int* tkey;
     int* tcnt; int* btask0; int* scnt; int* bslot0;
     int* slot_cnt; int* slot_off; int* inc_task; int* tmap;
+    int* nzoff; int* nzlist; int nnz;
     int2* inc_rng; int* b_inc0; int* b_cont0;
     int* e_cnt; int* e_ptr; int* e_cur; int* e_list;
     mel_contact* cont_new;        // the list being written (write stage)
