@@ -1,0 +1,96 @@
+"""Every contact law and the NeoHookean material against the oracle.
+
+The contact laws (Code/Model.h:81-506) use only +, -, *, / and sqrt, which round the same way on
+the GPU and on the host, so with each law the FP64 trajectory of a 3x3 lattice pressed by its
+plates (about 45 loaded contacts, grain-grain and grain-plate, after 100 steps) is bit-identical
+to the oracle's correctly-rounded mode: node kinematics, contact list with history and internal
+variables, rigid state, works.
+
+The NeoHookean update (Code/Model.h:52-73) evaluates J^(-5/3) with pow, whose last bit differs
+between CUDA's and glibc's implementations.  Stated tolerances: FP64 node state within 1e-9 of the
+largest displacement after 100 steps and the same active contacts; the mixed-precision form's
+kinetic energy and wall forces within 1e-5 relative after 200 steps."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import assert_contacts_equal
+
+pytestmark = pytest.mark.gpu
+
+# file parameters per law type (MEL_LAW_*, Code/IO.h:775-783), sized against the lattice's contact
+# loads (kn * overlap ~ 1e4) so that the strength limits are reached
+LAWS = {
+    0: [1e10],                                                    # Frictionless: kn
+    1: [1e10, 1e9, 2e3, 2e3],                                     # Cohesion: kn, kt, gtang, gtens
+    2: [1e10, 1e9, 0.3, 0.0, 0.0],                                # MohrCoulomb: kn, kt, fric, coh, tens
+    3: [1e10, 1e9, 0.3, 0.0, 0.0, 0.2],                           # DampedMohrCoulomb: ..., damping
+    4: [1e10, 1e9, 0.3, 0.0, 0.0, 0.5],                           # TwoSlopesMohrCoulomb: ..., unloading ratio
+    5: [1e10, 1e9, 2e10, 0.5, 4e3, 4e3, 0.3, 0.0, 0.0, 0.05],     # BondedMohrCoulomb
+    6: [1e10, 4e3, 1e-6, 1e3, 1.0],                               # CzmLinear: kini, Pnlim, gapnlim, Pnres, NTratio
+    7: [1e10, 4e3, 1e-6, 1e3, 1.0, 2e3, 0.01, 0.01],              # CzmFatigue: ..., Pnfat, Raten, Ratet
+}
+
+
+def flat_with(law_type=None, params=None, neohookean=False):
+    from melody2d_b200 import generator as g
+    sc = g.disc_lattice_scene(seed=0, nx=3, ny=3, pitch=2.0e-3, gap0=-1e-6, nsteps=300, v_plate=0.05)
+    if law_type is not None:
+        sc.laws = [(m1, m2, law_type, 0, list(params)) for (m1, m2, _, _, _) in sc.laws]
+    if neohookean:
+        sc.materials = [(name, 1 if name == "Grain" else t, p) for (name, t, p) in sc.materials]
+    return g.flatten(sc)
+
+
+@pytest.mark.parametrize("law", sorted(LAWS))
+def test_contact_law_bit_identical(gpu_lib, oracle_built, law):
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    flat = flat_with(law, LAWS[law])
+    assert set(np.asarray(flat["law_type"]).tolist()) == {law}
+    g = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    for _ in range(5):
+        g.step(20)
+        o.step(20)
+        np.testing.assert_array_equal(g.node_state(), o.node_state())
+        assert_contacts_equal(g.contacts(), o.contacts())
+    np.testing.assert_array_equal(g.rigid()[0], o.rigid()[0])
+    np.testing.assert_array_equal(g.works(), o.works())
+    assert (g.contacts()["fx"] != 0).sum() > 20
+    g.close()
+
+
+def test_neohookean_fp64_within_tolerance(gpu_lib, oracle_built):
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    flat = flat_with(neohookean=True)
+    assert 1 in np.asarray(flat["material_type"]).tolist()
+    g = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    g.step(100)
+    o.step(100)
+    sg, so = g.node_state(), o.node_state()
+    scale = np.abs(so[:, 6:8]).max()
+    assert scale > 0
+    assert np.abs(sg[:, 6:8] - so[:, 6:8]).max() <= 1e-9 * scale
+    assert g.monitor().active_contacts == o.monitor().active_contacts
+    g.close()
+
+
+def test_neohookean_mixed_within_tolerance(gpu_lib, oracle_built):
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    flat = flat_with(neohookean=True)
+    g = Solver.from_flat(flat, precision=1)
+    o = Oracle(flat, correctly_rounded=True)
+    g.step(200)
+    o.step(200)
+    mg, mo = g.monitor(), o.monitor()
+
+    def rel(a, b):
+        a, b = np.asarray(a, float), np.asarray(b, float)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    assert rel(mg.kinetic_energy, mo.kinetic_energy) <= 1e-5
+    assert rel(list(mg.rigid_force), list(mo.rigid_force)) <= 1e-5
+    assert mg.active_contacts == mo.active_contacts
+    g.close()
