@@ -1,17 +1,25 @@
-// Update_proximity (Code/Proximity.h:48-473) on the device.
+// Update_proximity (Code/Proximity.h:48-473) on the device, for one model or for several models
+// (the members of a batch) with the same launches.
 //
 // Stages (all integer bookkeeping deterministic, geometry bit-identical to the reference):
-//   aabb_kernel       border boxes inflated by the detection distance and their period shifts
-//                     (Code/Proximity.h:63-109), one warp per border
-//   neighbour_kernel  all-pairs (body, border) overlap with periodic shifts and de-duplication
-//                     (Code/Proximity.h:112-169), one warp per body, lanes over candidate bodies
-//   [host]            task list: one task per (slave body, slave border, neighbour) in the
-//                     reference's loop order, then one self task per (slave body, border)
-//   count_kernel      accepted candidates per (task, slave border node) slot, one warp per task
-//   scan              slot offsets = the canonical position of every new contact element
-//   write_kernel      writes the new list in the reference's order; history inheritance searches the
-//                     previous list of the same slave border node (Code/Proximity.h:269-284)
-//   entry_index_kernel / incoming ranges   index structures for the next step and update
+//   aabb_kernel        border boxes inflated by the detection distance and their period shifts
+//                      (Code/Proximity.h:63-109), one warp per border; segment-block and
+//                      superblock boxes for pruning
+//   neighbour_kernel   all-pairs (body, border) overlap with periodic shifts and de-duplication
+//                      (Code/Proximity.h:112-169), one warp per body, lanes over candidate bodies
+//   task_count / scan / task_fill   task list: one task per (slave body, slave border, neighbour)
+//                      in the reference's loop order, then one self task per (slave body, border);
+//                      a slot per (task, slave border node)
+//   [host read-back]   task and slot totals of every member
+//   count_kernel       accepted candidates per slot, one thread per slot (slot_task_kernel maps
+//                      slots to tasks)
+//   scan               slot offsets = the canonical position of every new contact element; the
+//                      slots with candidates are listed for the write pass
+//   [host read-back]   contact totals of every member
+//   write_kernel       writes the new list in the reference's order; history inheritance searches
+//                      the previous list of the same slave border node (Code/Proximity.h:269-284)
+//   incoming ranges, entry index, vgap carry   index structures for the next step and update
+// Every kernel reads a table of member jobs (mel_prox_job); the host driver is at the end.
 #include <cstdio>
 #include <cstring>
 #include <utility>
