@@ -1,10 +1,15 @@
-"""Every contact law and the NeoHookean material against the oracle.
+"""Every contact law, the NeoHookean material and the border conditions of deformable bodies
+against the oracle.
 
 The contact laws (Code/Model.h:81-506) use only +, -, *, / and sqrt, which round the same way on
 the GPU and on the host, so with each law the FP64 trajectory of a 3x3 lattice pressed by its
 plates (about 45 loaded contacts, grain-grain and grain-plate, after 100 steps) is bit-identical
 to the oracle's correctly-rounded mode: node kinematics, contact list with history and internal
 variables, rigid state, works.
+
+Soft Dirichlet, oriented and following Neumann conditions on deformable borders (the plates and
+walls of the other tests carry driven and oriented conditions on rigid bodies) are bit-identical
+as well: force components after one step and the trajectory over 100 steps.
 
 The NeoHookean update (Code/Model.h:52-73) evaluates J^(-5/3) with pow, whose last bit differs
 between CUDA's and glibc's implementations.  Stated tolerances: FP64 node state within 1e-9 of the
@@ -93,4 +98,42 @@ def test_neohookean_mixed_within_tolerance(gpu_lib, oracle_built):
     assert rel(mg.kinetic_energy, mo.kinetic_energy) <= 1e-5
     assert rel(list(mg.rigid_force), list(mo.rigid_force)) <= 1e-5
     assert mg.active_contacts == mo.active_contacts
+    g.close()
+
+
+def flat_with_border_conditions():
+    """The pressed 3x3 lattice with border conditions on three of its deformable discs: soft
+    Dirichlet, oriented Neumann and following Neumann in both directions (Body::Update_bc_forces,
+    Code/Body.h:669-799)."""
+    from melody2d_b200 import generator as g
+    sc = g.disc_lattice_scene(seed=0, nx=3, ny=3, pitch=2.0e-3, gap0=-1e-6, nsteps=300, v_plate=0.05)
+    hist = lambda v: (np.array([0.0, g.T_HIST_END]), np.array([v, v]))
+    combos = [((g.BC_SOFT, (1e8, 1e2), hist(0.02)), (g.BC_ORIENTED, (0.0, 0.0), hist(-2e4))),
+              ((g.BC_FOLLOWING, (0.0, 0.0), hist(3e4)), (g.BC_SOFT, (5e7, 0.0), hist(-0.01))),
+              ((g.BC_ORIENTED, (0.0, 0.0), hist(1e4)), (g.BC_FOLLOWING, (0.0, 0.0), hist(-1e4)))]
+    for body, bc in zip(sc.bodies[:3], combos):
+        assert body.kind == "deformable"
+        body.borders[0]["bc"] = list(bc)
+    return g.flatten(sc)
+
+
+def test_deformable_border_conditions_bit_identical(gpu_lib, oracle_built):
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    flat = flat_with_border_conditions()
+    g = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    g.record_forces(True)
+    g.step(1)
+    o.step(1)
+    fg, fo = g.forces(), o.forces()
+    for k in ("neumann", "dirichlet", "internal", "contact", "total"):
+        np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
+    assert np.abs(fo["neumann"]).max() > 0 and np.abs(fo["dirichlet"]).max() > 0
+    for _ in range(5):
+        g.step(20)
+        o.step(20)
+        np.testing.assert_array_equal(g.node_state(), o.node_state())
+        assert_contacts_equal(g.contacts(), o.contacts())
+    np.testing.assert_array_equal(g.works(), o.works())
     g.close()
