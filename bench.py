@@ -267,39 +267,12 @@ def run_ours(args, rank, world, local, pg):
     s.close()
 
 
-def _sample_scene(job):
-    """Worker of the batched workload's generation (spawned process): one sample's flat arrays."""
-    seed, counts = job
-    from melody2d_b200 import generator as g
-    templates = _sample_scene.templates
-    sc = g.batch_sample_scene(seed, templates)
-    return seed, g.flatten(sc), sc.meta
-
-
-def _init_sample_worker(counts):
-    from melody2d_b200 import generator as g
-    _sample_scene.templates = g.DiscTemplates(counts, workers=1)
-
-
-def make_batch_samples(seeds, workers):
-    """Flat arrays of the batched workload's samples (config-3 draws), built in a spawn pool whose
-    workers each hold the disc templates."""
-    import multiprocessing as mp
-    from concurrent.futures import ProcessPoolExecutor
-    counts = list(range(32, 97))
-    ctx = mp.get_context("spawn")
-    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_init_sample_worker,
-                             initargs=(counts,)) as ex:
-        out = list(ex.map(_sample_scene, [(s, counts) for s in seeds]))
-    return out
-
-
 def create_solvers(flats, precision, device, threads):
     """mel_create for many samples at once (the library call releases the interpreter lock)."""
     from concurrent.futures import ThreadPoolExecutor
     from melody2d_b200.solver import Solver
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        return list(ex.map(lambda f: Solver.from_flat(f, precision=precision, device=device), flats))
+        return list(ex.map(lambda f: Solver.from_flat(f, precision=precision, device=device, retain=False), flats))
 
 
 def run_batch(args, rank, world, local, pg):
@@ -307,16 +280,19 @@ def run_batch(args, rank, world, local, pg):
     border nodes per grain, confinement 50-400 kPa, friction 0.1-0.5) advanced together in one
     mixed-precision batch, against the plain FP64 path run one sample at a time on a subset.
     Samples/h are extrapolated from the timed steps to sample_steps steps per sample."""
-    from melody2d_b200.solver import Batch
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Batch, Solver
     threads = max(1, host_threads() // max(1, world))
-    t0 = time.perf_counter()
     seeds = [1000 * (rank + 1) + i for i in range(args.samples)]
-    samples = make_batch_samples(seeds, threads)
-    t_gen = time.perf_counter() - t0
-    flats = [f for _, f, _ in samples]
+    # the plain FP64 subset; its samples stay mapped for the plain and accuracy legs
+    sub = list(range(0, args.samples, max(1, args.samples // args.plain_subset)))[: args.plain_subset]
     t0 = time.perf_counter()
-    solvers = create_solvers(flats, 1, local, threads)
-    t_create = time.perf_counter() - t0
+    # generation (spawn workers, samples handed over in shared memory) overlapped with mel_create
+    solvers, kept, _ = g.build_batch_samples(
+        seeds, lambda f: Solver.from_flat(f, precision=1, device=local, retain=False),
+        workers=threads, create_threads=max(2, threads // 2), keep=sub)
+    t_build = time.perf_counter() - t0
+    flats = {i: sf.flat for i, sf in kept.items()}
     nodes = [s.step_stats()["n_deformable_nodes"] for s in solvers]
     b = Batch(precision=1, device=local)
     for s in solvers:
@@ -339,7 +315,6 @@ def run_batch(args, rank, world, local, pg):
     for s in solvers:
         s.close()
     # plain FP64 path, one sample at a time, on a subset
-    sub = list(range(0, args.samples, max(1, args.samples // args.plain_subset)))[: args.plain_subset]
     plain_ms = []
     for i in sub:
         a = create_solvers([flats[i]], 0, local, 1)[0]
@@ -380,7 +355,8 @@ def run_batch(args, rank, world, local, pg):
                                    f"friction U[0.1,0.5], mass x100, plates 0.05 m/s; mixed precision",
                        "samples_per_gpu": args.samples, "nodes_per_gpu": int(sum(nodes)),
                        "samples_h_extrapolated_to_steps": args.sample_steps,
-                       "l2": "inputs larger than L2", "generate_s": round(t_gen, 2), "create_s": round(t_create, 2)},
+                       "l2": "inputs larger than L2", "build_s": round(t_build, 2),
+                       "build": "generation in spawn workers, samples handed over in shared memory, overlapped with mel_create"},
             "node_steps_per_s": value,
             "plain_fp64_one_at_a_time": {"samples_h": plain_samples_h, "subset": len(sub),
                                          "ms_per_step_mean": float(np.mean(plain_ms))},
@@ -391,6 +367,9 @@ def run_batch(args, rank, world, local, pg):
             "clocks": clk, "gpu_launches": st["launches"] - launches0,
         }
         print(json.dumps(line), flush=True)
+    flats.clear()
+    for sf in kept.values():
+        sf.release()
 
 
 def run_serve(args, rank, world, local, pg):

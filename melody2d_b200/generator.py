@@ -938,3 +938,156 @@ def batch_sample_scene(seed: int, templates: DiscTemplates, aspect: float = 100.
                  contact_update_period=prox_every * dt,
                  meta=dict(config="batch", seed=seed, dt_crit=dtc, box=(W, H), n_discs=p["n_grains"],
                            sigma=p["sigma"], mu_fric=p["mu_fric"], v_plate=v_plate, mass_factor=mass_factor))
+
+
+# --------------------------------------------------------------------------------------------
+# Moving flattened samples between processes without copying them through a pipe
+# --------------------------------------------------------------------------------------------
+# A batched-workload sample flattens to 250-700 MB of arrays (the Gauss-point shape-function
+# columns dominate).  Returned from a spawned worker, it is pickled through a pipe and unpickled by
+# the parent, one sample after another: for hundreds of samples that transfer, not the
+# generation, bounds the admission path.  A worker instead copies each array into a named
+# shared-memory block and returns only the names; the parent maps the blocks (no copy), creates
+# its solver from them and releases them.  Where shared memory is unavailable or full, the arrays
+# travel the ordinary way.
+
+def share_flat(flat: Dict[str, np.ndarray]) -> dict:
+    """Worker side: the arrays of `flat` in shared-memory blocks.  Returns a small picklable
+    description for SharedFlat; the blocks live until SharedFlat.release() unlinks them."""
+    from multiprocessing import shared_memory
+    blocks, desc = [], {}
+    try:
+        for k, v in flat.items():
+            if isinstance(v, np.ndarray) and v.nbytes >= 4096:
+                shm = shared_memory.SharedMemory(create=True, size=v.nbytes)
+                blocks.append(shm)
+                np.ndarray(v.shape, dtype=v.dtype, buffer=shm.buf)[...] = v
+                desc[k] = ("shm", shm.name, v.dtype.str, v.shape)
+            else:
+                desc[k] = ("value", v)
+    except OSError:
+        for shm in blocks:
+            shm.close()
+            shm.unlink()
+        return {"__plain__": flat}
+    for shm in blocks:
+        shm.close()
+    return desc
+
+
+class SharedFlat:
+    """Parent side: `flat` maps the blocks described by share_flat() (or holds the plain arrays
+    of the fallback).  release() drops the mapping and frees the blocks; the arrays must not be
+    used afterwards."""
+
+    def __init__(self, desc: dict):
+        from multiprocessing import shared_memory
+        self._blocks = []
+        if "__plain__" in desc:
+            self.flat = desc["__plain__"]
+            return
+        self.flat = {}
+        for k, entry in desc.items():
+            if entry[0] == "shm":
+                _, name, dtype, shape = entry
+                shm = shared_memory.SharedMemory(name=name)
+                self._blocks.append(shm)
+                self.flat[k] = np.ndarray(shape, dtype=np.dtype(dtype), buffer=shm.buf)
+            else:
+                self.flat[k] = entry[1]
+
+    @property
+    def nbytes(self) -> int:
+        return sum(np.asarray(v).nbytes for k, v in self.flat.items() if k != "material_names")
+
+    def release(self) -> None:
+        self.flat = None
+        for shm in self._blocks:
+            try:
+                shm.close()
+            except BufferError:          # arrays still referenced elsewhere: the block is freed
+                pass                     # when they go, its name is removed now
+            try:
+                shm.unlink()
+            except FileNotFoundError:
+                pass
+        self._blocks = []
+
+
+_templates_of_worker: Optional["DiscTemplates"] = None
+
+
+def _init_template_worker(counts):
+    global _templates_of_worker
+    _templates_of_worker = DiscTemplates(counts, workers=1)
+
+
+def _shared_sample(seed: int):
+    sc = batch_sample_scene(seed, _templates_of_worker)
+    return seed, share_flat(flatten(sc)), sc.meta, sc.dt
+
+
+def build_batch_samples(seeds, create, workers: int, create_threads: int = 4, keep=(), counts=None):
+    """Generates the batched workload's samples `seeds` in a spawn pool (each worker holds the disc
+    templates) and calls create(flat) for each in a thread pool as soon as it arrives, with at most
+    2 x workers samples generated ahead and 2 x create_threads creations in flight, so that shared
+    memory holds a bounded number of samples.  Returns (created, kept, meta): created[i] =
+    create(flat of seeds[i]); kept[i] the SharedFlat of the indices in `keep` (release them when
+    done; the others are released after their creation); meta[i] = (scene meta, dt)."""
+    import multiprocessing as mp
+    from concurrent.futures import FIRST_COMPLETED, ProcessPoolExecutor, ThreadPoolExecutor, wait
+    counts = list(range(32, 97)) if counts is None else list(counts)
+    keep = set(keep)
+    n = len(seeds)
+    created, kept, meta = [None] * n, {}, [None] * n
+    ctx = mp.get_context("spawn")
+    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_init_template_worker,
+                             initargs=(counts,)) as ex, ThreadPoolExecutor(max_workers=create_threads) as cx:
+        gen, mk = {}, {}
+        nxt = 0
+        finished = False
+        try:
+            while nxt < n or gen or mk:
+                while nxt < n and len(gen) < 2 * workers and len(mk) < 2 * create_threads:
+                    gen[ex.submit(_shared_sample, seeds[nxt])] = nxt
+                    nxt += 1
+                done, _ = wait(list(gen) + list(mk), return_when=FIRST_COMPLETED)
+                for f in done:
+                    if f in gen:
+                        i = gen.pop(f)
+                        _, desc, m, dt = f.result()
+                        sf = SharedFlat(desc)
+                        meta[i] = (m, dt)
+                        mk[cx.submit(create, sf.flat)] = (i, sf)
+                    else:
+                        i, sf = mk.pop(f)
+                        try:
+                            created[i] = f.result()
+                        except BaseException:
+                            sf.release()
+                            raise
+                        if i in keep:
+                            kept[i] = sf
+                        else:
+                            sf.release()
+            finished = True
+        finally:
+            if not finished:                 # the caller gets nothing: free what it would have kept
+                for sf in kept.values():
+                    sf.release()
+            for f, (i, sf) in list(mk.items()):
+                if i not in kept:
+                    f.cancel()
+                    try:
+                        f.result()
+                    except Exception:
+                        pass
+                    sf.release()
+            for f in list(gen):
+                f.cancel()
+            for f in list(gen):              # samples already being built: wait, then free them
+                try:
+                    SharedFlat(f.result()[1]).release()
+                except BaseException:
+                    pass
+    return created, kept, meta

@@ -4,7 +4,8 @@ Requests arrive as a seeded Poisson stream.  Each request is one biaxial sample 
 workload's distribution (grains log-uniform in [50,1000], 32-96 border nodes per grain,
 confinement 50-400 kPa, friction 0.1-0.5) run until 5 % axial strain or a step cap.  The server:
   - builds each arriving request's model in a spawn process pool (the disc templates are built
-    once per worker) and creates its solver in a thread pool (mel_create releases the GIL);
+    once per worker; the arrays come back in shared memory) and creates its solver in a thread
+    pool (mel_create releases the GIL), after which the shared memory is freed;
   - admits created solvers into the resident batch while the estimated device memory of the
     residents stays within the HBM budget;
   - advances the batch in slices of one proximity period (10 steps), retiring each member when it
@@ -40,6 +41,7 @@ class Request:
     kinetic_energy: float = 0.0
     wall_force: Optional[List[float]] = None
     failed: str = ""             # why the run stopped early (diverged state), empty when it completed
+    shared: object = None        # the model's arrays in shared memory until its solver exists
 
 
 def poisson_arrivals(rate: float, duration: float, seed: int) -> List[float]:
@@ -72,9 +74,11 @@ def _init_worker(counts):
 
 
 def _build(seed: int):
+    """Worker: one request's model, its arrays handed over in shared memory (a model is hundreds
+    of MB; through a pipe its transfer would cost more than its generation)."""
     from melody2d_b200 import generator as g
     sc = g.batch_sample_scene(seed, _templates)
-    return seed, g.flatten(sc), sc.meta, sc.dt
+    return seed, g.share_flat(g.flatten(sc)), sc.meta, sc.dt
 
 
 def estimate_device_bytes(flat: dict) -> float:
@@ -99,6 +103,7 @@ class Server:
     def run(self, arrivals: List[float], seeds: List[int], duration: float, drain: float = 0.0) -> Dict:
         from melody2d_b200.solver import Batch, MelError, Solver
         from melody2d_b200.abi import MEL_ERR_NAN, MEL_ERR_BOUNDS
+        from melody2d_b200.generator import SharedFlat
         reqs = [Request(i, s, a) for i, (a, s) in enumerate(zip(arrivals, seeds))]
         ctx = mp.get_context("spawn")
         pool = ProcessPoolExecutor(max_workers=self.build_workers, mp_context=ctx, initializer=_init_worker,
@@ -123,14 +128,18 @@ class Server:
                     nxt += 1
                 for f in [f for f in building if f.done()]:
                     r = building.pop(f)
-                    _, flat, meta, dt = f.result()
+                    _, desc, meta, dt = f.result()
+                    r.shared = SharedFlat(desc)
+                    flat = r.shared.flat
                     r.target_steps = stop_steps(meta, dt, self.strain, self.step_cap)
                     ptr = np.asarray(flat["body_node_ptr"])
                     r.nodes = int(np.sum(np.diff(ptr)[np.asarray(flat["body_type"]) == 0]))
                     r.est_bytes = estimate_device_bytes(flat)
-                    creating[creators.submit(Solver.from_flat, flat, self.precision, self.device)] = r
+                    creating[creators.submit(Solver.from_flat, flat, self.precision, self.device, False)] = r
                 for f in [f for f in creating if f.done()]:
                     r = creating.pop(f)
+                    r.shared.release()
+                    r.shared = None
                     ready.append((r, f.result()))
                 ready.sort(key=lambda x: x[0].arrival)
                 # admission: the batched arm takes every ready request that fits the budget; the plain
@@ -200,8 +209,17 @@ class Server:
                 batch.close()
             creators.shutdown(wait=True, cancel_futures=True)
             for f, r in creating.items():
-                if f.done() and not f.exception():
+                if f.done() and not f.cancelled() and not f.exception():
                     f.result().close()
+                if r.shared is not None:
+                    r.shared.release()
+            for f in building:
+                f.cancel()
+            for f in building:               # models already being built: wait, then free them
+                try:
+                    SharedFlat(f.result()[1]).release()
+                except BaseException:
+                    pass
             pool.shutdown(wait=False, cancel_futures=True)
         wall = time.perf_counter() - t0
         failed = [r for r in reqs if r.done >= 0 and r.failed]

@@ -107,13 +107,16 @@ class Solver:
 
     # ---- construction -------------------------------------------------------------------
     @classmethod
-    def from_flat(cls, flat: dict, precision: int = 0, device: int = 0) -> "Solver":
+    def from_flat(cls, flat: dict, precision: int = 0, device: int = 0, retain: bool = True) -> "Solver":
+        """retain=False drops the references to the description's arrays once mel_create has
+        returned (the handle keeps its own copies), so that arrays mapped from shared memory can
+        be released while the solver lives."""
         L = lib()
         desc = abi.Desc(flat)
         opt = abi.MelOptions(precision=precision, device=device, use_graph=0, max_contacts=0)
         h = C.c_void_p()
         _check(L.mel_create(C.byref(desc.desc), C.byref(opt), C.byref(h)))
-        return cls(h, len(flat["node_domain"]), len(flat["body_type"]), keep=desc)
+        return cls(h, len(flat["node_domain"]), len(flat["body_type"]), keep=desc if retain else None)
 
     @classmethod
     def from_files(cls, directory: str, restart_index: int = 0, precision: int = 0, device: int = 0) -> "Solver":

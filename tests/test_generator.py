@@ -48,3 +48,37 @@ def test_biaxial_oracle_run_stays_bounded(oracle_built):
     W, H = sc.meta["box"]
     assert np.abs(st[:, 0:2]).max() < 0.05 * W        # displacements stay small over 400 steps
     assert (o.contacts()["fx"] != 0).sum() > 0
+
+
+def _shm_blocks():
+    import os
+    return {f for f in os.listdir("/dev/shm") if f.startswith("psm_")} if os.path.isdir("/dev/shm") else set()
+
+
+def test_shared_sample_pipeline_matches_direct_generation():
+    """Samples built by spawn workers and handed over through shared memory are the arrays the
+    generator gives in this process; kept samples stay readable until released, the others are
+    released after their creation, and no block is left behind."""
+    from melody2d_b200 import generator as g
+    seeds = [11, 12, 13]
+    before = _shm_blocks()
+    created, kept, meta = g.build_batch_samples(seeds, input_checksum, workers=2, create_threads=2, keep=[1])
+    templates = g.DiscTemplates(list(range(32, 97)), workers=1)
+    for i, s in enumerate(seeds):
+        sc = g.batch_sample_scene(s, templates)
+        assert created[i] == input_checksum(g.flatten(sc))
+        assert meta[i][1] == sc.dt
+    assert set(kept) == {1}
+    assert input_checksum(kept[1].flat) == created[1]
+    kept[1].release()
+    assert _shm_blocks() <= before
+
+
+def test_share_flat_round_trip():
+    from melody2d_b200 import generator as g
+    flat = {"a": np.arange(10000, dtype=np.float64), "b": np.arange(7, dtype=np.int32), "c": 2.5}
+    sf = g.SharedFlat(g.share_flat(flat))
+    np.testing.assert_array_equal(sf.flat["a"], flat["a"])
+    np.testing.assert_array_equal(sf.flat["b"], flat["b"])
+    assert sf.flat["c"] == 2.5 and sf.nbytes == sum(np.asarray(v).nbytes for v in flat.values())
+    sf.release()
