@@ -955,6 +955,16 @@ def share_flat(flat: Dict[str, np.ndarray]) -> dict:
     """Worker side: the arrays of `flat` in shared-memory blocks.  Returns a small picklable
     description for SharedFlat; the blocks live until SharedFlat.release() unlinks them."""
     from multiprocessing import shared_memory
+    need = sum(v.nbytes for v in flat.values() if isinstance(v, np.ndarray) and v.nbytes >= 4096)
+    try:
+        st = os.statvfs("/dev/shm")
+        free = st.f_bavail * st.f_frsize
+    except OSError:
+        free = 0
+    # tmpfs pages are allocated on write, and a write into a full tmpfs kills the process (SIGBUS)
+    # instead of raising: keep a wide margin for the other samples in flight
+    if free < 4 * need:
+        return {"__plain__": flat}
     blocks, desc = [], {}
     try:
         for k, v in flat.items():
