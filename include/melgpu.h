@@ -228,6 +228,20 @@ mel_status mel_get_works(mel_handle* h, double* works);
 mel_status mel_get_contact_count(mel_handle* h, int* n);
 mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* n);
 mel_status mel_get_time(mel_handle* h, double* time, double* dt);
+
+/* Asynchronous checkpoint (replaces the blocking downloads that precede Write_dynamic,
+ * Code/IO.h:2351, when the host keeps stepping meanwhile).  mel_checkpoint_start snapshots the
+ * node state, rigid records, works, contact list and time on the handle's stream (it sees every
+ * step called before it and none after) and copies it to library-owned pinned memory on a side
+ * stream; it returns without waiting, and further mel_step calls overlap the copy.
+ * mel_checkpoint_read waits for the copy and fills the caller's buffers (any may be NULL):
+ * node_state as mel_get_node_state, rigid as mel_get_rigid, works as mel_get_works, contacts (up
+ * to contacts_capacity records; too small a buffer is an error that leaves the snapshot pending),
+ * *ncont, and time3 = {time, dt, next_contact_update}.  A second start before a read replaces
+ * the unread snapshot.  For a batch member the snapshot is completed before start returns. */
+mel_status mel_checkpoint_start(mel_handle* h);
+mel_status mel_checkpoint_read(mel_handle* h, double* node_state, double* rigid, double* works,
+                               mel_contact* contacts, int contacts_capacity, int* ncont, double* time3);
 mel_status mel_monitor_compute(mel_handle* h, mel_monitor* out);
 
 /* Rigid-body records (layout MEL_RG_*, n_bodies records); node positions follow (restart upload). */

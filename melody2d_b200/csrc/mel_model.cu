@@ -35,6 +35,18 @@ void mel_set_cuda_error(cudaError_t e, const char* what, const char* file, int l
 // ---------------------------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------------------------
+// asynchronous checkpoint (mel_checkpoint_start / mel_checkpoint_read)
+struct mel_ckpt {
+    cudaStream_t side = nullptr;        // device-to-host copies, off the solver's stream
+    cudaEvent_t packed = nullptr;       // snapshot taken on the solver's stream
+    cudaEvent_t landed = nullptr;       // snapshot in pinned host memory
+    char* d_stage = nullptr; size_t d_cap = 0;
+    char* h_stage = nullptr; size_t h_cap = 0;
+    bool pending = false;
+    int nn = 0, nb = 0, ncont = 0;
+    double time = 0., dt = 0., next_cup = 0.;
+};
+
 struct mel_handle {
     mel_dev d;
     mel_prox_state P;
@@ -47,6 +59,7 @@ struct mel_handle {
     std::vector<int> b_type, b_status, b_node0, b_mat;
     std::vector<double> X0, rg_file, rg_mat;
     double time = 0., dt = 0., cup = 0., next_cup = 0.;
+    mel_ckpt ck;
     int solver = 0;
     int flags[MEL_NFLAGS] = { 0 };
     int parity = 0;
@@ -729,6 +742,11 @@ mel_status mel_destroy(mel_handle* h)
                      (void*)P.e_list, (void*)P.cont_alt, (void*)P.cont_w, (void*)P.cont_rt, (void*)h->d.cont })
         if (p) cudaFree(p);
     mel_prox_stage_free(P.stage);
+    if (h->ck.side) { cudaStreamSynchronize(h->ck.side); cudaStreamDestroy(h->ck.side); }
+    if (h->ck.packed) cudaEventDestroy(h->ck.packed);
+    if (h->ck.landed) cudaEventDestroy(h->ck.landed);
+    if (h->ck.d_stage) cudaFree(h->ck.d_stage);
+    if (h->ck.h_stage) cudaFreeHost(h->ck.h_stage);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -978,6 +996,106 @@ mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* 
     if (n) *n = h->d.ncont;
     int m = std::min(capacity, h->d.ncont);
     if (out && m > 0) MEL_CUDA_OK(cudaMemcpy(out, h->d.cont, sizeof(mel_contact) * m, cudaMemcpyDeviceToHost));
+    return MEL_OK;
+}
+
+// node state in the 12-doubles-per-node layout of mel_model_desc::node_state
+static __global__ void ckpt_pack_nodes(const double2* u, const double2* v, const double2* a, const double2* up,
+                                       const double2* vp, const double2* ap, int nn, double* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const double2 w[6] = { u[i], v[i], a[i], up[i], vp[i], ap[i] };
+    double* o = out + 12 * (size_t)i;
+#pragma unroll
+    for (int k = 0; k < 6; k++) { o[2 * k] = w[k].x; o[2 * k + 1] = w[k].y; }
+}
+
+// staging layout: node state | rigid records | works | contact records, each 256-byte aligned
+struct ckpt_layout { size_t nodes, rigid, works, cont, bytes; };
+static ckpt_layout ckpt_sections(int nn, int nb, int ncont)
+{
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    ckpt_layout L;
+    L.nodes = 0;
+    L.rigid = up(sizeof(double) * 12 * (size_t)nn);
+    L.works = L.rigid + up(sizeof(double) * MEL_RIGID_NF * (size_t)nb);
+    L.cont = L.works + up(sizeof(double) * 7 * (size_t)nb);
+    L.bytes = L.cont + up(sizeof(mel_contact) * (size_t)ncont) + 256;
+    return L;
+}
+
+mel_status mel_checkpoint_start(mel_handle* h)
+{
+    if (!h) return MEL_ERR_INVALID;
+    cudaSetDevice(h->device);
+    mel_ckpt& k = h->ck;
+    if (!k.side) {
+        if (cudaStreamCreateWithFlags(&k.side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&k.packed, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&k.landed, cudaEventDisableTiming) != cudaSuccess) {
+            mel_set_cuda_error(cudaGetLastError(), "checkpoint stream", __FILE__, __LINE__);
+            return MEL_ERR_CUDA;
+        }
+    }
+    // an unread snapshot is replaced; its copy must have landed before the staging is reused
+    if (k.pending) MEL_CUDA_OK(cudaEventSynchronize(k.landed));
+    k.pending = false;
+    const ckpt_layout L = ckpt_sections(h->nn, h->nb, h->d.ncont);
+    if (L.bytes > k.d_cap) {
+        if (k.d_stage) cudaFree(k.d_stage);
+        k.d_stage = nullptr; k.d_cap = 0;
+        if (cudaMalloc(&k.d_stage, 2 * L.bytes) != cudaSuccess) { mel_set_error("checkpoint staging (device) allocation failed"); return MEL_ERR_OOM; }
+        k.d_cap = 2 * L.bytes;
+    }
+    if (L.bytes > k.h_cap) {
+        if (k.h_stage) cudaFreeHost(k.h_stage);
+        k.h_stage = nullptr; k.h_cap = 0;
+        if (cudaMallocHost(&k.h_stage, 2 * L.bytes) != cudaSuccess) { mel_set_error("checkpoint staging (pinned host) allocation failed"); return MEL_ERR_OOM; }
+        k.h_cap = 2 * L.bytes;
+    }
+    // the snapshot is taken on the solver's stream, so it sees every step launched before this
+    // call and none launched after it; only the device-to-host copy runs beside later steps
+    if (h->nn > 0)
+        ckpt_pack_nodes<<<(h->nn + 255) / 256, 256, 0, h->stream>>>(h->d.u, h->d.v, h->d.a, h->d.up, h->d.vp, h->d.ap,
+                                                                     h->nn, reinterpret_cast<double*>(k.d_stage + L.nodes));
+    MEL_CUDA_OK(cudaGetLastError());
+    MEL_CUDA_OK(cudaMemcpyAsync(k.d_stage + L.rigid, h->d.rg, sizeof(double) * MEL_RIGID_NF * (size_t)h->nb, cudaMemcpyDeviceToDevice, h->stream));
+    MEL_CUDA_OK(cudaMemcpyAsync(k.d_stage + L.works, h->d.works, sizeof(double) * 7 * (size_t)h->nb, cudaMemcpyDeviceToDevice, h->stream));
+    if (h->d.ncont > 0)
+        MEL_CUDA_OK(cudaMemcpyAsync(k.d_stage + L.cont, h->d.cont, sizeof(mel_contact) * (size_t)h->d.ncont, cudaMemcpyDeviceToDevice, h->stream));
+    MEL_CUDA_OK(cudaEventRecord(k.packed, h->stream));
+    // a batch member is stepped on the batch's stream: finish the snapshot before returning
+    if (h->batch) MEL_CUDA_OK(cudaEventSynchronize(k.packed));
+    MEL_CUDA_OK(cudaStreamWaitEvent(k.side, k.packed, 0));
+    MEL_CUDA_OK(cudaMemcpyAsync(k.h_stage, k.d_stage, L.bytes, cudaMemcpyDeviceToHost, k.side));
+    MEL_CUDA_OK(cudaEventRecord(k.landed, k.side));
+    k.nn = h->nn; k.nb = h->nb; k.ncont = h->d.ncont;
+    k.time = h->time; k.dt = h->dt; k.next_cup = h->next_cup;
+    k.pending = true;
+    return MEL_OK;
+}
+
+mel_status mel_checkpoint_read(mel_handle* h, double* node_state, double* rigid, double* works, mel_contact* contacts,
+                               int contacts_capacity, int* ncont, double* time3)
+{
+    if (!h) return MEL_ERR_INVALID;
+    mel_ckpt& k = h->ck;
+    if (!k.pending) { mel_set_error("no checkpoint has been started since the last read"); return MEL_ERR_INVALID; }
+    if (ncont) *ncont = k.ncont;
+    if (contacts && contacts_capacity < k.ncont) {
+        mel_set_error("checkpoint holds %d contact elements, the buffer %d", k.ncont, contacts_capacity);
+        return MEL_ERR_INVALID;
+    }
+    cudaSetDevice(h->device);
+    MEL_CUDA_OK(cudaEventSynchronize(k.landed));
+    const ckpt_layout L = ckpt_sections(k.nn, k.nb, k.ncont);
+    if (node_state) memcpy(node_state, k.h_stage + L.nodes, sizeof(double) * 12 * (size_t)k.nn);
+    if (rigid) memcpy(rigid, k.h_stage + L.rigid, sizeof(double) * MEL_RIGID_NF * (size_t)k.nb);
+    if (works) memcpy(works, k.h_stage + L.works, sizeof(double) * 7 * (size_t)k.nb);
+    if (contacts && k.ncont > 0) memcpy(contacts, k.h_stage + L.cont, sizeof(mel_contact) * (size_t)k.ncont);
+    if (time3) { time3[0] = k.time; time3[1] = k.dt; time3[2] = k.next_cup; }
+    k.pending = false;
     return MEL_OK;
 }
 

@@ -40,6 +40,8 @@ SIGNATURES = {
     "mel_get_contact_count": [_vp, _ip],
     "mel_get_contacts": [_vp, C.POINTER(abi.MelContact), C.c_int, _ip],
     "mel_get_time": [_vp, _dp, _dp],
+    "mel_checkpoint_start": [_vp],
+    "mel_checkpoint_read": [_vp, _dp, _dp, _dp, C.POINTER(abi.MelContact), C.c_int, _ip, _dp],
     "mel_monitor_compute": [_vp, C.POINTER(abi.MelMonitor)],
     "mel_set_rigid": [_vp, _dp],
     "mel_set_time": [_vp, C.c_double, C.c_double, C.c_double],
@@ -210,6 +212,37 @@ class Solver:
         f = C.c_int()
         _check(lib().mel_get_health(self.h, C.byref(f)))
         return f.value, (lib().mel_last_error_string().decode(errors="replace") if f.value else "")
+
+    def checkpoint_start(self):
+        """Snapshot of the state, copied to host memory while later steps run (mel_checkpoint_start)."""
+        _check(lib().mel_checkpoint_start(self.h))
+
+    def checkpoint_read(self) -> dict:
+        """The snapshot of the last checkpoint_start: node_state (n_nodes, 12), rigid, works
+        (n_bodies, 7), contacts (as contacts()), time, dt, next_contact_update."""
+        n = C.c_int()
+        t3 = np.zeros(3)
+        st = np.zeros(12 * self.nn)
+        rg = np.zeros(abi.MEL_RIGID_NF * self.nb)
+        wk = np.zeros(7 * self.nb)
+        cap = self.contact_capacity_hint()
+        while True:
+            buf = (abi.MelContact * max(1, cap))()
+            rc = lib().mel_checkpoint_read(self.h, _ptr(st), _ptr(rg), _ptr(wk), buf, cap, C.byref(n), _ptr(t3))
+            if rc == 0:
+                break
+            if n.value > cap:              # buffer too small: the snapshot stays pending, retry
+                cap = n.value
+                continue
+            _check(rc)
+        return {"node_state": st.reshape(-1, 12), "rigid": rg.reshape(self.nb, -1), "works": wk.reshape(self.nb, 7),
+                "contacts": abi.contacts_to_numpy(buf, n.value), "time": t3[0], "dt": t3[1],
+                "next_contact_update": t3[2]}
+
+    def contact_capacity_hint(self) -> int:
+        n = C.c_int()
+        _check(lib().mel_get_contact_count(self.h, C.byref(n)))
+        return max(16, 2 * n.value)
 
     def time(self):
         t = C.c_double(); dt = C.c_double()
