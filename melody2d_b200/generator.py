@@ -323,6 +323,7 @@ class Scene:
     solver: int = 0
     solver_params: Tuple[float, ...] = (1e-3, 0.2, 1.0, 100.0, 1.0, 1.0, 0.99, 1e3)
     self_contact: bool = True
+    initialize_czm: bool = False    # INITIALIZE_CZM: internal variables of the set-up contacts (Code/Proximity.h:481)
     meta: dict = dataclasses.field(default_factory=dict)
 
     @property
@@ -445,6 +446,8 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
     flags[7] = 1                          # NO_LOG
     if not scene.self_contact:
         flags[8] = 1                      # NO_MONITORING (also disables self contact, Proximity.h:332)
+    if scene.initialize_czm:
+        flags[3] = 1                      # INITIALIZE_CZM
     f["flags"] = flags
     names = [m[0] for m in scene.materials]
     f["material_type"] = np.array([m[1] for m in scene.materials], dtype=np.int32)
@@ -695,6 +698,8 @@ def write_asc(scene: Scene, directory: str) -> None:
             scene.name, SOLVER_NAMES[scene.solver], _g(scene.dt), _g(tend), _g(tend), _g(0.0)))
         if not scene.self_contact:
             w("NO_MONITORING\n")
+        if scene.initialize_czm:
+            w("INITIALIZE_CZM\n")
         w(" \n")
         for bi, b in enumerate(scene.bodies):
             n = b.nodes.shape[0]

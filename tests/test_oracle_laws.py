@@ -1,0 +1,116 @@
+"""Pins the oracle to the reference solver for every contact law, the NeoHookean material, the
+border conditions of deformable bodies and INITIALIZE_CZM.
+
+tests/golden/laws_ref.json holds SHA-256 digests of the reference's own FP64 state (made by
+tests/golden/make_golden_laws.py with the reference compiled from its sources) after set-up and
+after 50 and 100 steps of a 3x3 lattice pressed by its plates, once per case.  The oracle, run in
+its default mode (glibc pow, as the reference), must reproduce every digest bit for bit: node
+positions, displacement parameters, internal and contact forces, and every contact element with
+its history and internal variables.  The GPU is pinned to the oracle on the same cases by
+tests/test_gpu_laws.py.
+
+Law parameters are complete as the reference's loader reads them (Code/IO.h:700-790); the last
+parameter of BondedMohrCoulomb, CZMlinear and CZMfatigue is the initial-gap threshold that
+INITIALIZE_CZM uses to bond the set-up contacts (Code/Proximity.h:481-545)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, input_checksum
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "laws_ref.json")
+STEPS = [0, 50, 100]
+
+# file parameters per law type (MEL_LAW_*), complete as Load_static reads them
+LAW_PARAMS = {
+    0: [1e10],
+    1: [1e10, 1e9, 2e3, 2e3],
+    2: [1e10, 1e9, 0.3, 0.0, 0.0],
+    3: [1e10, 1e9, 0.3, 0.0, 0.0, 0.2],
+    4: [1e10, 1e9, 0.3, 0.0, 0.0, 0.5],
+    5: [1e10, 1e9, 2e10, 0.5, 4e3, 4e3, 0.3, 0.0, 0.0, 0.05, 1e-6],
+    6: [1e10, 4e3, 1e-6, 1e3, 1.0, 1e-6],
+    7: [1e10, 4e3, 1e-6, 1e3, 1.0, 2e3, 0.01, 0.01, 1e-6],
+}
+
+CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7+czm", "neohookean",
+                                                    "border_conditions"]
+
+
+def case_scene(name):
+    """The pressed 3x3 lattice (about 45 loaded contacts after 100 steps) set up for one case."""
+    from melody2d_b200 import generator as g
+    sc = g.disc_lattice_scene(seed=0, nx=3, ny=3, pitch=2.0e-3, gap0=-1e-6, nsteps=300, v_plate=0.05)
+    if name.startswith("law"):
+        law = int(name[3])
+        sc.laws = [(m1, m2, law, 0, list(LAW_PARAMS[law])) for (m1, m2, _, _, _) in sc.laws]
+        sc.initialize_czm = name.endswith("+czm")
+    elif name == "neohookean":
+        sc.materials = [(n, 1 if n == "Grain" else t, p) for (n, t, p) in sc.materials]
+    elif name == "border_conditions":
+        hist = lambda v: (np.array([0.0, g.T_HIST_END]), np.array([v, v]))
+        combos = [((g.BC_SOFT, (1e8, 1e2), hist(0.02)), (g.BC_ORIENTED, (0.0, 0.0), hist(-2e4))),
+                  ((g.BC_FOLLOWING, (0.0, 0.0), hist(3e4)), (g.BC_SOFT, (5e7, 0.0), hist(-0.01))),
+                  ((g.BC_ORIENTED, (0.0, 0.0), hist(1e4)), (g.BC_FOLLOWING, (0.0, 0.0), hist(-1e4)))]
+        for body, c in zip(sc.bodies[:3], combos):
+            body.borders[0]["bc"] = list(c)
+    return sc
+
+
+def sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(np.asarray(a, dtype=np.float64)).tobytes()).hexdigest()
+
+
+CONTACT_KEYS = ["bodyS", "borderS", "border_nodeS", "nodeS", "bodyM", "borderM", "shiftM", "segmentM", "nb_internal",
+                "shapeM1", "shapeM2", "gapn", "vgapn", "gapt", "vgapt", "xsi", "xnorm", "ynorm", "fx", "fy",
+                "internal0", "internal1", "internal2"]
+
+
+def summary(node, contacts, works):
+    """Digests of one state: node fields (name -> (n, 2) array), contacts (key -> column), works."""
+    out = {"node_" + k: sha(v) for k, v in node.items()}
+    out["n_contacts"] = int(len(contacts["fx"]))
+    for k in CONTACT_KEYS:
+        out["contact_" + k] = sha(contacts[k])
+    out["works"] = sha(works)
+    return out
+
+
+def oracle_columns(c):
+    """The oracle's contact records as the reference dump's columns."""
+    cols = {k: c[k] for k in ("bodyS", "borderS", "border_nodeS", "nodeS", "bodyM", "borderM", "shiftM", "segmentM",
+                              "nb_internal", "gapn", "vgapn", "gapt", "vgapt", "xsi", "xnorm", "ynorm", "fx", "fy")}
+    for i in range(3):
+        cols[f"internal{i}"] = c["internal"][:, i]
+    cols["shapeM1"] = c["shapeM"][:, 1]
+    cols["shapeM2"] = c["shapeM"][:, 2]
+    return cols
+
+
+def oracle_summary(o):
+    st = o.node_state()
+    f = o.forces()
+    node = {"x": o.positions(), "up": st[:, 6:8], "f_int": f["internal"], "f_contact": f["contact"]}
+    return summary(node, oracle_columns(o.contacts()), o.works())
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_matches_reference_per_case(oracle_built, case):
+    from melody2d_b200 import generator as g
+    from oracle.pyoracle import Oracle
+    gold = json.load(open(GOLDEN))["cases"][case]
+    flat = g.flatten(case_scene(case))
+    assert input_checksum(flat) == gold["input_sha256"], "generated input differs from the fixture's input"
+    o = Oracle(flat, correctly_rounded=False)
+    done = 0
+    for step in STEPS:
+        o.step(step - done)
+        done = step
+        ref, got = gold["steps"][str(step)], oracle_summary(o)
+        assert got["n_contacts"] == ref["n_contacts"], (case, step)
+        assert ref["n_contacts"] > 0
+        for k, v in ref.items():
+            assert got[k] == v, f"{case}: {k} differs from the reference at step {step}"
