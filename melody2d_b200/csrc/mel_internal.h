@@ -132,6 +132,8 @@ struct mel_dev {
 
 // kernel launch wrappers (mel_kernels.cu)
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
+// Initialize_CZM's pass over the contact list (contact geometry, then the initial bonds)
+void mel_launch_czm_init(const mel_dev& d, cudaStream_t s);
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s);
 // one step of a batch: the contact pass over thr0[nsamp] threads, the body pass over cta0[nsamp]
 // CTAs and the per-sample time advance (devs, thr0, cta0 in device memory)

@@ -89,10 +89,14 @@ __device__ __forceinline__ void rigid_terms(const mel_dev& d, int tid, const mel
     }
 }
 
-// one thread of the contact pass: contact element `tid`, or border entry tid - ncont
-__device__ void contact_thread(const mel_dev& d, int tid, double law_dt_scale)
+// one thread of the contact pass: contact element `tid`, or border entry tid - ncont.  With
+// czm_init the pass is Initialize_CZM's instead (Code/Proximity.h:481-541): the contact geometry is
+// updated as in Update_contacts, then contacts whose law has bonds start bonded when their gap is
+// below the law's initial-gap parameter; no law is evaluated and no force is written.
+__device__ void contact_thread(const mel_dev& d, int tid, double law_dt_scale, int czm_init = 0)
 {
     if (tid >= d.ncont) {
+        if (czm_init) return;
         // refresh stored border lengths (read by Update_proximity for new contacts)
         int e = tid - d.ncont;
         if (e >= d.ne) return;
@@ -107,7 +111,10 @@ __device__ void contact_thread(const mel_dev& d, int tid, double law_dt_scale)
     mel_contact c = d.cont[tid];
     int b = c.bodyS;
     if (b < 0 || b >= d.nb || c.bodyM < 0 || c.bodyM >= d.nb) { set_err(d, MEL_E_BOUNDS); return; }
-    if (d.b_status[b] == MEL_STATUS_INACTIVE) { rigid_terms(d, tid, c, d.x[d.b_node0[b] + c.nodeS]); return; }
+    if (d.b_status[b] == MEL_STATUS_INACTIVE) {
+        if (!czm_init) rigid_terms(d, tid, c, d.x[d.b_node0[b] + c.nodeS]);
+        return;
+    }
     // ---- Update_contacts (Code/Body.h:1352-1632) -----------------------------------------
     int bodyM = c.bodyM, borderM = c.borderM, shiftM = c.shiftM, segmentM = c.segmentM;
     int gM = d.b_bd0[bodyM] + borderM;
@@ -184,6 +191,21 @@ __device__ void contact_thread(const mel_dev& d, int tid, double law_dt_scale)
     for (int k = 0; k < 4; k++) { c.nodeM[k] = nd[k]; c.shiftMk[k] = sh[k]; c.shapeM[k] = p.N[k]; }
     c.xsi = p.xsi; c.xnorm = p.xn; c.ynorm = p.yn; c.xtan = p.xt; c.ytan = p.yt;
     c.vgapn = vgapn; c.vgapt = vgapt;
+    if (czm_init) {
+        c.gapn = p.gap; c.gapt = gapt;
+        const int lb = d.table[d.b_mat[b] * d.nmat + d.b_mat[bodyM]];
+        if (lb > -1) {
+            const int t = d.law_type[lb];
+            const double* P = d.law_p + MEL_LAW_NPARAM * lb;
+            if (t == MEL_LAW_CZM_LINEAR) { c.nb_internal = 1; c.internal[0] = (c.gapn < P[5]) ? 0. : 1.; }
+            else if (t == MEL_LAW_CZM_FATIGUE || t == MEL_LAW_BONDED_MOHR_COULOMB) {
+                const double gi = (t == MEL_LAW_CZM_FATIGUE) ? P[8] : P[10];
+                c.nb_internal = 3; c.internal[0] = (c.gapn < gi) ? 0. : 1.; c.internal[1] = 0.; c.internal[2] = 0.;
+            }
+        }
+        d.cont[tid] = c;
+        return;
+    }
     // ---- Update_contact_forces (Code/Body.h:1657-1849) ----------------------------------
     int gS = d.b_bd0[b] + c.borderS;
     double length = entry_length(d, b, gS, c.border_nodeS);
@@ -1100,9 +1122,9 @@ __device__ __forceinline__ void body_cta(const mel_dev& d, int bb, double T, cha
     else deformable_body<MX>(d, b, T, smem);
 }
 
-__global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale)
+__global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale, int czm_init)
 {
-    contact_thread(d, blockIdx.x * blockDim.x + threadIdx.x, law_dt_scale);
+    contact_thread(d, blockIdx.x * blockDim.x + threadIdx.x, law_dt_scale, czm_init);
 }
 
 // One model: CTA i is the body d.b_order[i]; time2[parity] is the step's start time, the step's
@@ -1207,7 +1229,13 @@ void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s)
 {
     int total = d.ncont + d.ne;
     if (total <= 0) return;
-    mel::contact_kernel<<<(total + 127) / 128, 128, 0, s>>>(d, law_dt_scale);
+    mel::contact_kernel<<<(total + 127) / 128, 128, 0, s>>>(d, law_dt_scale, 0);
+}
+
+void mel_launch_czm_init(const mel_dev& d, cudaStream_t s)
+{
+    if (d.ncont <= 0) return;
+    mel::contact_kernel<<<(d.ncont + 127) / 128, 128, 0, s>>>(d, 1.0, 1);
 }
 
 size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)

@@ -605,14 +605,21 @@ static void update_borders_only(mel_handle* h)
 
 static mel_status setup(mel_handle* h)
 {
-    // Code/main.cpp:104-127: Update_borders, Update_bc, Update_proximity, Update_material,
-    // Update_proximity.  Update_bc values are evaluated when used; Initialize_CZM is not run.
-    if (h->flags[3] == 1) { mel_set_error("INITIALIZE_CZM is not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
+    // Code/main.cpp:104-127: Update_borders, Update_bc, Update_proximity, Initialize_CZM,
+    // Update_material, Update_proximity.  Update_bc values are evaluated when used.
     // rigid nodes take their positions from the body state
     std::vector<double> st(12 * (size_t)h->nn, 0.);
     mel_status rc = MEL_OK;
     update_borders_only(h);
     if ((rc = proximity(h))) return rc;
+    if (h->flags[3] == 1) {
+        // Initialize_CZM (Code/Proximity.h:481-541) runs once: it clears the flag, so the call after
+        // the second proximity update does nothing
+        mel_launch_czm_init(h->d, h->stream);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { mel_set_cuda_error(e, "Initialize_CZM launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+        h->flags[3] = 0;
+    }
     cudaMemcpyAsync(h->d.rg, h->rg_mat.data(), sizeof(double) * h->rg_mat.size(), cudaMemcpyHostToDevice, h->stream);
     if ((rc = proximity(h))) return rc;
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "setup", __FILE__, __LINE__); return MEL_ERR_CUDA; }

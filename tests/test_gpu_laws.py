@@ -137,3 +137,28 @@ def test_deformable_border_conditions_bit_identical(gpu_lib, oracle_built):
         assert_contacts_equal(g.contacts(), o.contacts())
     np.testing.assert_array_equal(g.works(), o.works())
     g.close()
+
+
+@pytest.mark.parametrize("case", ["law5+czm", "law6+czm", "law7+czm"])
+def test_initialize_czm_bit_identical(gpu_lib, oracle_built, case):
+    """INITIALIZE_CZM (Code/Proximity.h:481-541) bonds the set-up contacts closer than the law's
+    initial-gap parameter; the bonded and damage branches of BondedMohrCoulomb, CZMlinear and
+    CZMfatigue then run bit-identically to the oracle (itself pinned to the compiled reference on
+    these cases, tests/test_oracle_laws.py)."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    from test_oracle_laws import case_scene
+    flat = g.flatten(case_scene(case))
+    assert int(np.asarray(flat["flags"])[3]) == 1
+    gs = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    assert_contacts_equal(gs.contacts(), o.contacts())
+    assert (o.contacts()["internal"][:, 0] == 0).sum() > 10, "the scenario must start with bonded contacts"
+    for _ in range(5):
+        gs.step(20)
+        o.step(20)
+        np.testing.assert_array_equal(gs.node_state(), o.node_state())
+        assert_contacts_equal(gs.contacts(), o.contacts())
+    np.testing.assert_array_equal(gs.works(), o.works())
+    gs.close()
