@@ -1,9 +1,10 @@
 """Pins the oracle to the reference solver for every contact law, the NeoHookean material, the
-border conditions of deformable bodies and INITIALIZE_CZM.
+border conditions of deformable bodies, INITIALIZE_CZM, and two 12-disc biaxial samples (rigid
+plates driven, lateral walls under oriented pressure along long borders, rigid-rigid pairs).
 
 tests/golden/laws_ref.json holds SHA-256 digests of the reference's own FP64 state (made by
 tests/golden/make_golden_laws.py with the reference compiled from its sources) after set-up and
-after 50 and 100 steps of a 3x3 lattice pressed by its plates, once per case.  The oracle, run in
+after 50 and 100 steps of each case (a 3x3 lattice pressed by its plates, or a biaxial sample).  The oracle, run in
 its default mode (glibc pow, as the reference), must reproduce every digest bit for bit: node
 positions, displacement parameters, internal and contact forces, and every contact element with
 its history and internal variables.  The GPU is pinned to the oracle on the same cases by
@@ -37,12 +38,15 @@ LAW_PARAMS = {
 }
 
 CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7+czm", "neohookean",
-                                                    "border_conditions"]
+                                                    "border_conditions", "biaxial12_s5", "biaxial12_s7"]
 
 
 def case_scene(name):
-    """The pressed 3x3 lattice (about 45 loaded contacts after 100 steps) set up for one case."""
+    """The scene of one case: a biaxial sample, or the pressed 3x3 lattice (about 45 loaded
+    contacts after 100 steps) with the case's law, material or border conditions."""
     from melody2d_b200 import generator as g
+    if name.startswith("biaxial12_s"):
+        return g.biaxial_scene(seed=int(name.split("_s")[1]), n_discs=12, n_border=32, n_interior=80, workers=1)
     sc = g.disc_lattice_scene(seed=0, nx=3, ny=3, pitch=2.0e-3, gap0=-1e-6, nsteps=300, v_plate=0.05)
     if name.startswith("law"):
         law = int(name[3])
