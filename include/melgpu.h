@@ -271,10 +271,12 @@ mel_status mel_free_desc(void* owner);
  * held by every GPU that loads the library until the process exits), so it accepts at most
  * 2,097,152 nodes and as many contact elements per call and rejects larger sizes with
  * MEL_ERR_INVALID.  The array keeps the last call's contents; each call writes every record it reads,
- * and calls that overlap on the GPU (on different streams) race on it.  The first call on a device
- * looks up the array's device address with that device current; make that first call before any
- * stream capture.  `stream` is a cudaStream_t (NULL: the legacy default stream); the call returns
- * once the work is queued. */
+ * and calls that overlap on the GPU (on different streams) race on it.  Each call looks up the
+ * array's device address in the current device's context, so the address stays right after a device
+ * reset; the first call on a device loads the library's device code, so make that first call before
+ * any stream capture.  A CUDA error already pending from the caller's own launches is reported as
+ * MEL_ERR_CUDA and left pending, and nothing is launched.  `stream` is a cudaStream_t (NULL: the
+ * legacy default stream); the call returns once the work is queued. */
 mel_status mel_monitor_reduce_static(const double* d_velocity, const double* d_mass, const double* d_displacement,
                                      int n_nodes, const mel_contact* d_contacts, int n_contacts, double* d_out,
                                      void* stream);

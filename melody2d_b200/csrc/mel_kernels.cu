@@ -17,6 +17,7 @@
 #include <mutex>
 #include "mel_internal.h"
 #include "mel_geometry.cuh"
+#include "mel_sincos.h"
 
 namespace mel {
 
@@ -1065,7 +1066,7 @@ __device__ void rigid_body(const mel_dev& d, int b, double T, char* smem)
     const double xvb = rg[MEL_RG_XV], yvb = rg[MEL_RG_YV], rv = rg[MEL_RG_RV];
     const double x0 = rg[MEL_RG_X0], y0 = rg[MEL_RG_Y0], r0 = rg[MEL_RG_R0];
     const double dr = rd - r0;
-    const double cr = cos(dr), sr = sin(dr);
+    const double cr = mel_cos(dr), sr = mel_sin(dr);   // correctly rounded (mel_sincos.h)
     for (int i = tid; i < n; i += blockDim.x) {
         int gi = n0 + i;
         double2 X = d.X0[gi];

@@ -13,6 +13,7 @@
 #include "mel_prox_host.h"
 #include "mel_chunks.h"
 #include "mel_host.h"   // .asc loader (mel_loader.cpp)
+#include "mel_sincos.h"
 
 // ---------------------------------------------------------------------------------------------
 // errors
@@ -659,8 +660,8 @@ static mel_status upload_state(mel_handle* h, const double* st, const double* ri
         double dr = r[MEL_RG_RD] - r[MEL_RG_R0];
         for (int i = h->b_node0[b]; i < h->b_node0[b + 1]; i++) {
             double dx = h->X0[2 * i] - r[MEL_RG_X0], dy = h->X0[2 * i + 1] - r[MEL_RG_Y0];
-            x[2 * i] = r[MEL_RG_XC] + dx * cos(dr) - dy * sin(dr);
-            x[2 * i + 1] = r[MEL_RG_YC] + dx * sin(dr) + dy * cos(dr);
+            x[2 * i] = r[MEL_RG_XC] + dx * mel_cos(dr) - dy * mel_sin(dr);
+            x[2 * i + 1] = r[MEL_RG_YC] + dx * mel_sin(dr) + dy * mel_cos(dr);
             double ddx = x[2 * i] - r[MEL_RG_XC], ddy = x[2 * i + 1] - r[MEL_RG_YC];
             v[2 * i] = -ddy * r[MEL_RG_RV] + r[MEL_RG_XV];
             v[2 * i + 1] = ddx * r[MEL_RG_RV] + r[MEL_RG_YV];

@@ -14,13 +14,11 @@
 // MEL_STATIC_MAX_ELEMENTS nodes and contact elements; larger inputs are rejected with an error.
 // Every GPU that loads the library keeps this array until the process exits.
 #include <cstdio>
-#include <mutex>
 #include "mel_internal.h"
 
 #define MEL_STATIC_MAX_BLOCKS 1024
 #define MEL_STATIC_PER_BLOCK 2048
 #define MEL_STATIC_MAX_ELEMENTS (MEL_STATIC_MAX_BLOCKS * MEL_STATIC_PER_BLOCK)
-#define MEL_STATIC_MAX_DEVICES 64
 
 // five partial sums per block: kinetic energy, sum m*ux, sum m*uy, sum m, active contacts
 static __device__ __align__(256) double mel_static_partials[5 * MEL_STATIC_MAX_BLOCKS];
@@ -65,24 +63,17 @@ __global__ void static_final_kernel(const double* part, int nblk, double* out)
 
 } // namespace mel
 
-// Device address of mel_static_partials, looked up once per device with that device current.
-static double* g_static_ptr[MEL_STATIC_MAX_DEVICES];
-static std::mutex g_static_mu;
-
+// Device address of mel_static_partials in the current device's context.  It is looked up on
+// every call rather than cached: after a cudaDeviceReset (or any other teardown of the primary
+// context) the module is loaded again and the array may sit at a new address, and the lookup costs
+// little once the module is loaded.  The first call on a device loads the module, so that call
+// should come before any stream capture.
 static mel_status static_scratch(double** out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) { mel_set_cuda_error(e, "cudaGetDevice", __FILE__, __LINE__); return MEL_ERR_CUDA; }
-    if (dev < 0 || dev >= MEL_STATIC_MAX_DEVICES) { mel_set_error("device ordinal %d beyond %d", dev, MEL_STATIC_MAX_DEVICES); return MEL_ERR_UNSUPPORTED; }
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, mel_static_partials);
-        if (e != cudaSuccess || !p) { mel_set_cuda_error(e, "cudaGetSymbolAddress(mel_static_partials)", __FILE__, __LINE__); return MEL_ERR_CUDA; }
-        g_static_ptr[dev] = static_cast<double*>(p);
-    }
-    *out = g_static_ptr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, mel_static_partials);
+    if (e != cudaSuccess || !p) { mel_set_cuda_error(e, "cudaGetSymbolAddress(mel_static_partials)", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    *out = static_cast<double*>(p);
     return MEL_OK;
 }
 
@@ -101,6 +92,14 @@ extern "C" mel_status mel_monitor_reduce_static(const double* d_velocity, const 
         mel_set_error("null device pointer");
         return MEL_ERR_INVALID;
     }
+    // an error left by the caller's own launches is reported as such and left pending for the
+    // caller (cudaPeekAtLastError does not clear it); nothing is launched on top of it
+    cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        mel_set_error("a CUDA error from before this call is pending (%s: %s); nothing was launched",
+                      cudaGetErrorName(pending), cudaGetErrorString(pending));
+        return MEL_ERR_CUDA;
+    }
     double* part = nullptr;
     mel_status rc = static_scratch(&part);
     if (rc) return rc;
@@ -112,8 +111,10 @@ extern "C" mel_status mel_monitor_reduce_static(const double* d_velocity, const 
                                                     reinterpret_cast<const double2*>(d_mass),
                                                     reinterpret_cast<const double2*>(d_displacement), n_nodes,
                                                     d_contacts, n_contacts, part, nblk);
-    mel::static_final_kernel<<<1, 32, 0, s>>>(part, nblk, d_out);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) { mel_set_cuda_error(e, "mel_monitor_reduce_static launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    if (e != cudaSuccess) { mel_set_cuda_error(e, "static_partial_kernel launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+    mel::static_final_kernel<<<1, 32, 0, s>>>(part, nblk, d_out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { mel_set_cuda_error(e, "static_final_kernel launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
     return MEL_OK;
 }

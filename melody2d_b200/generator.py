@@ -19,7 +19,7 @@ restates the parts of it the solver's inputs depend on:
 File layout follows Preprocessor/ExportStatic.m and Preprocessor/ExportDynamic.m as read by
 Load_static (Code/IO.h:598-1861) and Load_dynamic (Code/IO.h:1871-2345).
 
-Deviations, all stated in DESIGN.md: the support radius is 2.0x the body's mean Delaunay edge
+Deviations from the preprocessor: the support radius is 2.0x the body's mean Delaunay edge
 length (the workload's definition) instead of the k-nearest-neighbour rule of
 AnalyseSimpleBody.m:64-68; interior nodes come from seeded rejection sampling instead of
 Distmesh; the large packings use a box enlarged to hold 2000 discs at random-sequential-addition
@@ -169,6 +169,7 @@ class Body:
     rigid_mass: float = 0.0
     rigid_inertia: float = 0.0
     velocity: Tuple[float, float] = (0.0, 0.0)
+    angular_velocity: float = 0.0               # rigid only (rad/s)
 
 
 def _ccw(nodes: np.ndarray, tri: np.ndarray) -> np.ndarray:
@@ -260,25 +261,9 @@ def make_disc(rng, centre, radius, n_border, n_interior, min_sep, material, rho,
                 sup=sup, gp_xy=gp_xy, gp_w=gp_w, gp_J=gp_J, gp=gp, n_regions=regions)
 
 
-def make_rect_rigid(x0, y0, x1, y1, spacing, material, rho, bcx, bcy, det, con):
-    """Rigid rectangle with CCW border nodes of roughly `spacing` and two cells."""
-    pts = []
-    def edge(a, b):
-        L = math.hypot(b[0] - a[0], b[1] - a[1])
-        n = max(1, int(math.ceil(L / spacing)))
-        for k in range(n):
-            t = k / n
-            pts.append((a[0] + t * (b[0] - a[0]), a[1] + t * (b[1] - a[1])))
-    c = [(x0, y0), (x1, y0), (x1, y1), (x0, y1)]
-    corner_idx = []
-    for k in range(4):
-        corner_idx.append(len(pts))
-        edge(c[k], c[(k + 1) % 4])
-    nodes = np.array(pts)
-    n = nodes.shape[0]
-    cells = np.array([[corner_idx[0], corner_idx[1], corner_idx[2]],
-                      [corner_idx[0], corner_idx[2], corner_idx[3]]], dtype=np.int64)
-    # AnalyseRigidBody.m: centre of mass, mass, inertia
+def _rigid_mass_props(nodes: np.ndarray, cells: np.ndarray, rho: float):
+    """Centre of mass, mass and inertia about the centre of a rigid body from its cells
+    (Preprocessor/AnalyseRigidBody.m)."""
     m = 0.0; cx = 0.0; cy = 0.0
     for tri in cells:
         p = nodes[tri]
@@ -298,11 +283,68 @@ def make_rect_rigid(x0, y0, x1, y1, spacing, material, rho, bcx, bcy, det, con):
             PQ = (p[a, 0] - xc) * (p[b, 0] - xc) + (p[a, 1] - yc) * (p[b, 1] - yc)
             QQ = (p[b, 0] - xc) ** 2 + (p[b, 1] - yc) ** 2
             inertia += rho * A / 6.0 * (PP + PQ + QQ)
+    return np.array([cx, cy]), m, abs(inertia)
+
+
+def make_rect_rigid(x0, y0, x1, y1, spacing, material, rho, bcx, bcy, det, con):
+    """Rigid rectangle with CCW border nodes of roughly `spacing` and two cells."""
+    pts = []
+    def edge(a, b):
+        L = math.hypot(b[0] - a[0], b[1] - a[1])
+        n = max(1, int(math.ceil(L / spacing)))
+        for k in range(n):
+            t = k / n
+            pts.append((a[0] + t * (b[0] - a[0]), a[1] + t * (b[1] - a[1])))
+    c = [(x0, y0), (x1, y0), (x1, y1), (x0, y1)]
+    corner_idx = []
+    for k in range(4):
+        corner_idx.append(len(pts))
+        edge(c[k], c[(k + 1) % 4])
+    nodes = np.array(pts)
+    n = nodes.shape[0]
+    cells = np.array([[corner_idx[0], corner_idx[1], corner_idx[2]],
+                      [corner_idx[0], corner_idx[2], corner_idx[3]]], dtype=np.int64)
+    centre, m, inertia = _rigid_mass_props(nodes, cells, rho)
     bl = list(range(n)) + [0]
     border_rec = dict(nodes=bl, periodicity=0, interpolant=0, before=0, after=0, bc=[bcx, bcy])
     return Body(kind="rigid", material=material, nodes=nodes, borders=[border_rec], cells=cells,
-                nodal_distance=spacing, detection=det, contact=con, centre=np.array([cx, cy]),
-                rigid_mass=m, rigid_inertia=abs(inertia))
+                nodal_distance=spacing, detection=det, contact=con, centre=centre,
+                rigid_mass=m, rigid_inertia=inertia)
+
+
+def make_rigid_disc(centre, radius, n, material, rho, det, con, velocity=(0.0, 0.0), angular_velocity=0.0):
+    """Free rigid disc: a regular polygon of n CCW border nodes, cells fanned from node 0, no border
+    condition (its centre moves and turns under the contact forces alone)."""
+    th = 2.0 * np.pi * np.arange(n) / n
+    nodes = np.stack([centre[0] + radius * np.cos(th), centre[1] + radius * np.sin(th)], axis=1)
+    cells = np.array([[0, k, k + 1] for k in range(1, n - 1)], dtype=np.int64)
+    c, m, inertia = _rigid_mass_props(nodes, cells, rho)
+    free = (BC_NONE, (0.0, 0.0), None)
+    border_rec = dict(nodes=list(range(n)) + [0], periodicity=0, interpolant=0, before=0, after=0, bc=[free, free])
+    return Body(kind="rigid", material=material, nodes=nodes, borders=[border_rec], cells=cells,
+                nodal_distance=2.0 * math.pi * radius / n, detection=det, contact=con, centre=c,
+                rigid_mass=m, rigid_inertia=inertia, velocity=tuple(velocity), angular_velocity=angular_velocity)
+
+
+def make_periodic_strip_rigid(W, y0, y1, spacing, material, rho, bcx, bcy, det, con):
+    """Rigid strip spanning one period [0, W] of the x-periodic domain, y in [y0, y1]: a body of type
+    "Periodic" with two "Periodic" borders (Code/Body.h:403-606): border 0 is the lower edge, nodes at
+    x = 0, h, ..., W - h walked in +x (its last entry is the first node one period on), border 1 the
+    upper edge, nodes at x = W, W - h, ..., h walked in -x (its last entry is its first node one period
+    back).  Each border is its own neighbour before and after.  The two cells only give the strip a
+    mass; a periodic body never turns."""
+    m = max(2, int(math.ceil(W / spacing)))
+    h = W / m
+    bottom = [(k * h, y0) for k in range(m)]
+    top = [(W - k * h, y1) for k in range(m)]
+    nodes = np.array(bottom + top)
+    cells = np.array([[0, m - 1, m], [0, m, 2 * m - 1]], dtype=np.int64)
+    centre, mass, inertia = _rigid_mass_props(nodes, cells, rho)
+    b0 = dict(nodes=list(range(m)) + [0], periodicity=2, interpolant=0, before=0, after=0, bc=[bcx, bcy])
+    b1 = dict(nodes=list(range(m, 2 * m)) + [m], periodicity=2, interpolant=0, before=1, after=1, bc=[bcx, bcy])
+    return Body(kind="rigid", material=material, nodes=nodes, borders=[b0, b1], cells=cells,
+                nodal_distance=h, detection=det, contact=con, centre=centre, rigid_mass=mass,
+                rigid_inertia=inertia, periodic=1)
 
 
 # --------------------------------------------------------------------------------------------
@@ -417,6 +459,66 @@ def disc_lattice_scene(seed: int = 0, nx: int = 4, ny: int = 4, pitch: float = 2
                  meta=dict(config="lattice", seed=seed, dt_crit=dtc))
 
 
+def periodic_strip_scene(seed: int = 2, nx: int = 3, ny: int = 2, pitch: float = 2.0e-3, rmin: float = 0.9e-3,
+                         rmax: float = 1.1e-3, n_border: int = 32, n_interior: int = 60, min_sep: float = 0.1e-3,
+                         v_plate: float = 0.05, nsteps: int = 300, gap0: float = -1e-6, x_shift: float = -0.3,
+                         prox_every: int = 10, name: str = "periodic") -> Scene:
+    """A lattice of deformable discs in an x-periodic domain of one row's width (period [0, nx*pitch],
+    PERIODIC_BOUNDARIES), squeezed between two rigid "Periodic" strips driven at +-v_plate.  The
+    lattice is offset by x_shift*pitch, so the first column straddles the periodic seam: its discs
+    meet the last column's discs one period away (proximity shifts of -1 and +1), and their nodes
+    slide over the strips' seams, where the contact segment walk changes the master shift."""
+    rng = np.random.default_rng(seed)
+    import random
+    prng = random.Random(seed + 1)
+    E, nu, rho = 1e8, 0.3, 2500.0
+    mats = [("Grain", 0, [rho, 0.0, 0.0, E, nu, 1000.0]), ("Steel", 0, [7800.0, 0.0, 0.0, 2e11, 0.3, 500.0])]
+    laws = [("Grain", "Grain", 2, 0, [1e10, 1e9, 0.3, 0.0, 0.0]),
+            ("Grain", "Steel", 2, 0, [1e10, 1e9, 0.3, 0.0, 0.0])]
+    W = nx * pitch
+    radii = rng.uniform(rmin, rmax, size=nx * ny)
+    bodies = []
+    k = 0
+    for j in range(ny):
+        for i in range(nx):
+            c = ((0.5 + i + x_shift) * pitch, 0.5 * pitch + j * pitch)
+            bodies.append(make_disc(prng, c, float(radii[k]), n_border, n_interior, min_sep, 0, rho))
+            k += 1
+    ymin = min(b.nodes[:, 1].min() for b in bodies)
+    ymax = max(b.nodes[:, 1].max() for b in bodies)
+    h_b = 2.0 * math.pi * rmin / n_border
+    thick = 0.25 * pitch
+    hist = lambda v: (np.array([0.0, T_HIST_END]), np.array([v, v]))
+    bot = make_periodic_strip_rigid(W, ymin - gap0 - thick, ymin - gap0, h_b, 1, 7800.0,
+                                    (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(v_plate)),
+                                    0.5 * h_b, 0.5 * h_b)
+    top = make_periodic_strip_rigid(W, ymax + gap0, ymax + gap0 + thick, h_b, 1, 7800.0,
+                                    (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(-v_plate)),
+                                    0.5 * h_b, 0.5 * h_b)
+    bodies += [bot, top]
+    mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    dtc = min(critical_dt(b, mu, lam, 1e10) for b in bodies if b.kind == "deformable")
+    dt = float("%.4g" % (0.5 * dtc))
+    return Scene(name=name, bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
+                 contact_update_period=prox_every * dt, period=(0.0, W),
+                 meta=dict(config="periodic", seed=seed, dt_crit=dtc))
+
+
+def rotor_scene(seed: int = 0, omega: float = 200.0, nsteps: int = 300, n_rotor: int = 40, name: str = "rotor") -> Scene:
+    """The pressed 3x3 lattice (pitch 2.0 mm, plates starting 1 um inside the outer discs) with its
+    centre disc replaced by a free rigid steel disc of the same radius spinning at `omega` rad/s: its
+    nodes turn through cos and sin of the body's rotation every step, and the contacts with its four
+    neighbours load it with moments."""
+    sc = disc_lattice_scene(seed=seed, nx=3, ny=3, pitch=2.0e-3, gap0=-1e-6, nsteps=nsteps, v_plate=0.05, name=name)
+    d = sc.bodies[4]
+    c = d.nodes[:len(d.borders[0]["nodes"]) - 1].mean(axis=0)
+    R = float(np.mean(np.linalg.norm(d.nodes[:len(d.borders[0]["nodes"]) - 1] - c, axis=1)))
+    h = 2.0 * math.pi * R / n_rotor
+    sc.bodies[4] = make_rigid_disc(c, R, n_rotor, 1, 7800.0, 0.5 * h, 0.5 * h, angular_velocity=omega)
+    sc.meta = dict(sc.meta, config="rotor", omega=omega)
+    return sc
+
+
 # --------------------------------------------------------------------------------------------
 # Flattening (the arrays behind mel_model_desc)
 # --------------------------------------------------------------------------------------------
@@ -488,6 +590,7 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
             rigid[i, 5] = 1.0 / b.rigid_mass
             rigid[i, 6] = 1.0 / b.rigid_inertia
             rigid[i, 13:15] = b.velocity
+            rigid[i, 15] = b.angular_velocity
     f["rigid"] = rigid.reshape(-1)
     N = int(nn.sum())
     x0 = np.concatenate([b.nodes for b in scene.bodies])
@@ -714,8 +817,8 @@ def write_asc(scene: Scene, directory: str) -> None:
                     w("%d 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0\n" % i)
                 w(" \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
             else:
-                w(" \nRIGID\nactive\n%d\n \nKINEMATICS\n%s %s 0\n0 0 0\n%s %s 0\n \n" % (
-                    bi, _g(b.centre[0]), _g(b.centre[1]), _g(vx), _g(vy)))
+                w(" \nRIGID\nactive\n%d\n \nKINEMATICS\n%s %s 0\n0 0 0\n%s %s %s\n \n" % (
+                    bi, _g(b.centre[0]), _g(b.centre[1]), _g(vx), _g(vy), _g(b.angular_velocity)))
                 w("FORCES\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
 
 
@@ -778,6 +881,21 @@ def make_discs_parallel(jobs, workers: Optional[int] = None):
         return list(ex.map(_disc_worker, jobs, chunksize=max(1, len(jobs) // (4 * workers))))
 
 
+def contact_distance(sigma: float, radius: float, kn: float = 1e10, peak: float = 3.0, margin: float = 1.3) -> float:
+    """Contact (and detection) distance a biaxial sample needs so that its contact elements survive
+    the penetration its loading causes.  Update_proximity keeps a node-to-segment candidate only
+    while its gap is above -contact_distance (Code/Proximity.h:269), and the penalty law
+    Pn = -kn * gapn (Code/Model.h:123-128) balances a stress s with a penetration g: a disc of radius
+    R pressed on a flat side carries kn (4/3) sqrt(2R) g^(3/2) per unit depth against s * 2R, so
+    g = (3/4 s sqrt(2R) / kn)^(2/3).  With kn = 1e10 Pa/m and 100 kPa this is about 50 um for a
+    1 mm disc, more than half the border-node spacing; a contact distance of half that spacing
+    drops the contacts at every proximity update and the walls pass through the grains.  The
+    distance is taken at `peak` times the confining stress (the axial stress of the compression),
+    with a `margin`."""
+    g = (0.75 * peak * sigma * math.sqrt(2.0 * radius) / kn) ** (2.0 / 3.0)
+    return margin * g
+
+
 def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax: float = 1.5e-3,
                   n_border: int = 64, n_interior: int = 340, aspect: float = 100.0 / 60.0, fill: float = 0.45,
                   gap: float = 0.02e-3, v_plate: float = 0.05, sigma: float = 100e3, mass_factor: float = 100.0,
@@ -812,8 +930,10 @@ def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax
     jobs = [(int(seeds[i]), (float(centres[i, 0]), float(centres[i, 1])), float(radii[i]), n_border, n_interior,
              rho, mass_factor) for i in range(n_discs)]
     bodies = make_discs_parallel(jobs, workers)
+    for b, r in zip(bodies, radii):
+        b.detection = b.contact = max(b.contact, contact_distance(sigma, float(r)))
     h_min = 2.0 * math.pi * rmin / n_border
-    bodies += _biaxial_frame(W, H, h_min, rho_steel, v_plate, sigma)
+    bodies += _biaxial_frame(W, H, h_min, rho_steel, v_plate, sigma, contact_distance(sigma, rmax))
     mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
     smallest = np.argsort(radii)[:3]
     dtc = min(critical_dt(bodies[i], mu, lam, 1e10) for i in smallest)
@@ -824,25 +944,28 @@ def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax
                            radii=(rmin, rmax), sigma=sigma, v_plate=v_plate, mass_factor=mass_factor))
 
 
-def _biaxial_frame(W: float, H: float, h_min: float, rho_steel: float, v_plate: float, sigma: float) -> List[Body]:
+def _biaxial_frame(W: float, H: float, h_min: float, rho_steel: float, v_plate: float, sigma: float,
+                   dist: float = 0.0) -> List[Body]:
     """Rigid plates (bottom, top) driven towards each other at v_plate and lateral walls (left,
-    right) loaded by the confining pressure sigma, fixed vertically."""
+    right) loaded by the confining pressure sigma, fixed vertically; detection and contact distance
+    max(h_min / 2, dist)."""
     thick = 0.05 * H
+    dd = max(0.5 * h_min, dist)
     hist = lambda v: (np.array([0.0, T_HIST_END]), np.array([v, v]))
     # plates span the box and the walls' inward travel; walls span the plates' full height, so no
     # grain can leave the sample through a corner
     bot = make_rect_rigid(-0.1 * W, -thick, 1.1 * W, 0.0, 2.0 * h_min, 1, rho_steel,
-                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(v_plate)), 0.5 * h_min, 0.5 * h_min)
+                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(v_plate)), dd, dd)
     top = make_rect_rigid(-0.1 * W, H, 1.1 * W, H + thick, 2.0 * h_min, 1, rho_steel,
-                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(-v_plate)), 0.5 * h_min, 0.5 * h_min)
+                          (BC_DRIVEN, (0.0, 0.0), hist(0.0)), (BC_DRIVEN, (0.0, 0.0), hist(-v_plate)), dd, dd)
     wall_h = H + 2.0 * thick
     y0 = -thick
     perim = 2.0 * (wall_h + thick)
     p_eff = sigma * H / perim               # oriented load per unit border length, total = sigma * sample height
     left = make_rect_rigid(-thick, y0, 0.0, y0 + wall_h, 2.0 * h_min, 1, rho_steel,
-                           (BC_ORIENTED, (0.0, 0.0), hist(p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
+                           (BC_ORIENTED, (0.0, 0.0), hist(p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), dd, dd)
     right = make_rect_rigid(W, y0, W + thick, y0 + wall_h, 2.0 * h_min, 1, rho_steel,
-                            (BC_ORIENTED, (0.0, 0.0), hist(-p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), 0.5 * h_min, 0.5 * h_min)
+                            (BC_ORIENTED, (0.0, 0.0), hist(-p_eff)), (BC_DRIVEN, (0.0, 0.0), hist(0.0)), dd, dd)
     return [bot, top, left, right]
 
 
@@ -935,8 +1058,10 @@ def batch_sample_scene(seed: int, templates: DiscTemplates, aspect: float = 100.
             ("Grain", "Steel", 2, 0, [kn, 1e9, p["mu_fric"], 0.0, 0.0]),
             ("Steel", "Steel", 0, 0, [0.0])]
     bodies = [templates.grain(int(nb), c, r, rho, mass_factor) for nb, c, r in zip(p["n_border"], centres, radii)]
+    for b, r in zip(bodies, radii):
+        b.detection = b.contact = max(b.contact, contact_distance(p["sigma"], float(r), kn))
     h_min = float(np.min(2.0 * math.pi * radii / p["n_border"]))
-    bodies += _biaxial_frame(W, H, h_min, rho_steel, v_plate, p["sigma"])
+    bodies += _biaxial_frame(W, H, h_min, rho_steel, v_plate, p["sigma"], contact_distance(p["sigma"], float(radii.max()), kn))
     dtc = min(templates.critical_dt(int(nb), float(r), rho, mass_factor, kn) for nb, r in zip(p["n_border"], radii))
     dt = float("%.4g" % (0.5 * dtc))
     return Scene(name=f"batch{seed}", bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,

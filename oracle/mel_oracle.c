@@ -11,15 +11,18 @@
  */
 #include "mel_oracle.h"
 #include "../melody2d_b200/csrc/mel_rsqrt.h"
+#include "../melody2d_b200/csrc/mel_sincos.h"
 
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
-/* x^(-1/2) as the reference computes it (glibc pow) or correctly rounded (the GPU's value);
- * see orc_set_rsqrt_mode. */
+/* x^(-1/2), and the cosine and sine that turn rigid bodies, as the reference computes them (glibc
+ * pow, cos, sin) or correctly rounded (the GPU's values); see orc_set_rsqrt_mode. */
 static int g_cr_rsqrt = 0;
 static inline double orc_rsqrt(double x) { return g_cr_rsqrt ? mel_rsqrt(x) : pow(x, -0.5); }
+static inline double orc_cos(double x) { return g_cr_rsqrt ? mel_cos(x) : cos(x); }
+static inline double orc_sin(double x) { return g_cr_rsqrt ? mel_sin(x) : sin(x); }
 void orc_set_rsqrt_mode(int correctly_rounded) { g_cr_rsqrt = correctly_rounded; }
 
 typedef struct { int n, cap; mel_contact* a; } cvec;
@@ -1209,8 +1212,8 @@ static void update_kinematics(orc_model* m, int b)
         for (int i = n0; i < m->nptr[b + 1]; i++) {
             double dx = m->X0[2 * i] - rg[MEL_RG_X0], dy = m->X0[2 * i + 1] - rg[MEL_RG_Y0];
             double dr = rg[MEL_RG_RD] - rg[MEL_RG_R0];
-            m->u[2 * i] = rg[MEL_RG_XD] + dx * cos(dr) - dy * sin(dr) - dx;
-            m->u[2 * i + 1] = rg[MEL_RG_YD] + dx * sin(dr) + dy * cos(dr) - dy;
+            m->u[2 * i] = rg[MEL_RG_XD] + dx * orc_cos(dr) - dy * orc_sin(dr) - dx;
+            m->u[2 * i + 1] = rg[MEL_RG_YD] + dx * orc_sin(dr) + dy * orc_cos(dr) - dy;
             m->v[2 * i] = rg[MEL_RG_XV]; m->v[2 * i + 1] = rg[MEL_RG_YV];
         }
     }
@@ -1235,8 +1238,8 @@ static void update_kinematics_temporary(orc_model* m, int b)
         for (int i = n0; i < m->nptr[b + 1]; i++) {
             double dx = m->X0[2 * i] - rg[MEL_RG_X0], dy = m->X0[2 * i + 1] - rg[MEL_RG_Y0];
             double dr = tm[2] - rg[MEL_RG_R0];
-            m->ut[2 * i] = tm[0] + dx * cos(dr) - dy * sin(dr) - dx;
-            m->ut[2 * i + 1] = tm[1] + dx * sin(dr) + dy * cos(dr) - dy;
+            m->ut[2 * i] = tm[0] + dx * orc_cos(dr) - dy * orc_sin(dr) - dx;
+            m->ut[2 * i + 1] = tm[1] + dx * orc_sin(dr) + dy * orc_cos(dr) - dy;
         }
     }
 }
@@ -1258,8 +1261,8 @@ static void update_current_positions(orc_model* m, int b)
         for (int i = n0; i < m->nptr[b + 1]; i++) {
             double dx = m->X0[2 * i] - rg[MEL_RG_X0], dy = m->X0[2 * i + 1] - rg[MEL_RG_Y0];
             double dr = rg[MEL_RG_RD] - rg[MEL_RG_R0];
-            m->x[2 * i] = rg[MEL_RG_XC] + dx * cos(dr) - dy * sin(dr);
-            m->x[2 * i + 1] = rg[MEL_RG_YC] + dx * sin(dr) + dy * cos(dr);
+            m->x[2 * i] = rg[MEL_RG_XC] + dx * orc_cos(dr) - dy * orc_sin(dr);
+            m->x[2 * i + 1] = rg[MEL_RG_YC] + dx * orc_sin(dr) + dy * orc_cos(dr);
             dx = m->x[2 * i] - rg[MEL_RG_XC];
             dy = m->x[2 * i + 1] - rg[MEL_RG_YC];
             m->v[2 * i] = -dy * rg[MEL_RG_RV] + rg[MEL_RG_XV];

@@ -39,8 +39,9 @@ int  orc_get_neighbours(orc_model* m, int* rows, int cap);
 long orc_stale_shape_events(orc_model* m);
 /* Solver_step outputs of the last iteration: neval, max_error, mean_error, total_mass, max_mass */
 void orc_solver_stats(orc_model* m, double* out5);
-/* 0: x^(-1/2) through glibc pow, as the reference (default);
- * 1: correctly rounded x^(-1/2), the value the GPU kernels compute (mel_rsqrt.h). */
+/* 0: x^(-1/2), cos and sin through glibc pow, cos and sin, as the reference (default);
+ * 1: correctly rounded x^(-1/2), cos and sin, the values the GPU kernels compute (mel_rsqrt.h,
+ *    mel_sincos.h). */
 void orc_set_rsqrt_mode(int correctly_rounded);
 
 #ifdef __cplusplus

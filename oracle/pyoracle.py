@@ -56,7 +56,8 @@ def _dp(a):
 
 
 def set_rsqrt_mode(correctly_rounded: bool) -> None:
-    """0: x^(-1/2) through glibc pow as the reference; 1: correctly rounded, as the GPU kernels."""
+    """0: x^(-1/2), cos and sin through glibc (pow, cos, sin) as the reference; 1: correctly rounded,
+    as the GPU kernels."""
     lib().orc_set_rsqrt_mode(1 if correctly_rounded else 0)
 
 

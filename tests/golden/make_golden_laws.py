@@ -1,7 +1,7 @@
 """Generates tests/golden/laws_ref.json: the reference solver's own state for every case of
 tests/test_oracle_laws.py (each contact law, with and without INITIALIZE_CZM where it applies,
-NeoHookean, border conditions of deformable bodies, two 12-disc biaxial samples), at full FP64
-precision.
+NeoHookean, border conditions of deformable bodies, two 12-disc biaxial samples, an x-periodic
+domain and a spinning rigid disc), at full FP64 precision.
 
     python tests/golden/make_golden_laws.py   (needs oracle/_ref/ref_harness, built by oracle/Makefile
                                               from the reference sources)

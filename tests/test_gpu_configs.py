@@ -1,0 +1,173 @@
+"""The workloads themselves on the GPU, against the oracle in both of its modes.
+
+* Correctly-rounded mode (x^(-1/2), cos and sin rounded to nearest, as the kernels compute them):
+  every compared quantity is bit-identical.
+* Default mode (glibc pow, cos and sin: the reference's own arithmetic, pinned bit for bit to the
+  compiled reference by tests/test_oracle_golden.py and tests/test_oracle_laws.py): the GPU is held
+  to a stated relative tolerance on the monitored quantities (kinetic energy, wall contact force,
+  driven-wall reaction, mean displacement) and on the node displacements, and the contact candidate
+  sets and active sets must be equal.  The two modes part only where glibc misrounds one of those
+  three functions (one unit in the last place, a few arguments in ten thousand); the drift this
+  leaves is printed per checkpoint.
+
+Cases: the small lattice workload exactly as specified (16 discs, 4x4 lattice, 2.2 mm pitch,
+10,000 steps, monitored every 100 steps), a 12-disc biaxial sample over 3,000 steps, the
+2000-disc biaxial workload the benchmark times (20 steps with two proximity updates), an
+x-periodic domain and a spinning rigid disc."""
+import os
+
+import numpy as np
+import pytest
+
+from test_gpu_parity import assert_contacts_equal
+
+pytestmark = pytest.mark.gpu
+
+# Relative drift allowed between the GPU and the reference's arithmetic.  Measured on the oracle's
+# two modes: 0 over the 10,000 lattice steps (no misrounded argument occurs), at most 7e-14 over
+# 2,000-3,000 steps of the pressed lattice and of the 12-disc biaxial samples.
+TOL_REF = 1e-10
+
+KEYS = ["bodyS", "borderS", "border_nodeS", "bodyM", "borderM", "shiftM", "segmentM"]
+
+
+def key_sets(c):
+    rows = np.stack([c[k] for k in KEYS], axis=1)
+    act = (c["fx"] != 0) | (c["fy"] != 0)
+    return set(map(tuple, rows.tolist())), set(map(tuple, rows[act].tolist()))
+
+
+def monitored(m, nrigid):
+    return np.array([m.kinetic_energy, *m.mean_displacement, *list(m.rigid_force)[:2 * nrigid],
+                     *list(m.rigid_dirichlet)[:2 * nrigid], m.active_contacts], dtype=np.float64)
+
+
+def rel(a, b):
+    d = np.abs(np.asarray(a) - np.asarray(b))
+    scale = np.maximum(np.abs(np.asarray(b)).max(initial=0.0), 1e-300)
+    return float(d.max(initial=0.0) / scale)
+
+
+class Trio:
+    """The GPU solver and the oracle in both modes on one input, stepped together."""
+
+    def __init__(self, flat):
+        from melody2d_b200.solver import Solver
+        from oracle.pyoracle import Oracle
+        self.gpu = Solver.from_flat(flat)
+        self.cr = Oracle(flat, correctly_rounded=True)
+        self.ref = Oracle(flat, correctly_rounded=False)
+        self.nrigid = int(np.sum(np.asarray(flat["body_type"]) == 1))
+        self.drift = []
+        self.first_set_diff = None
+
+    def step(self, n):
+        self.gpu.step(n)
+        self.cr.step(n)
+        self.ref.step(n)
+
+    def check(self, label, full=True):
+        g, c, r = self.gpu, self.cr, self.ref
+        # bit-identical to the correctly-rounded oracle
+        np.testing.assert_array_equal(g.node_state(), c.node_state(), err_msg=label)
+        np.testing.assert_array_equal(monitored(g.monitor(), self.nrigid), monitored(c.monitor(), self.nrigid),
+                                      err_msg=label)
+        if full:
+            assert_contacts_equal(g.contacts(), c.contacts())
+            np.testing.assert_array_equal(g.rigid()[0], c.rigid()[0], err_msg=label)
+            np.testing.assert_array_equal(g.works(), c.works(), err_msg=label)
+        # within TOL_REF of the reference's arithmetic, same candidate and active sets
+        mg, mr = g.monitor(), r.monitor()
+        d = {"kinetic_energy": rel(mg.kinetic_energy, mr.kinetic_energy),
+             "wall_contact_force": rel(list(mg.rigid_force)[:2 * self.nrigid], list(mr.rigid_force)[:2 * self.nrigid]),
+             "wall_reaction": rel(list(mg.rigid_dirichlet)[:2 * self.nrigid], list(mr.rigid_dirichlet)[:2 * self.nrigid]),
+             "mean_displacement": rel(list(mg.mean_displacement), list(mr.mean_displacement)),
+             "displacements": rel(g.node_state()[:, 0:2], r.node_state()[:, 0:2])}
+        self.drift.append((label, d))
+        for k, v in d.items():
+            assert v <= TOL_REF, f"{label}: {k} drifts {v:.3e} from the reference's arithmetic"
+        sg, sr = key_sets(g.contacts()), key_sets(r.contacts())
+        if self.first_set_diff is None and sg != sr:
+            self.first_set_diff = label
+        assert sg[0] == sr[0], f"{label}: candidate sets differ from the reference's"
+        assert sg[1] == sr[1], f"{label}: active sets differ from the reference's"
+
+    def report(self, name):
+        worst = {k: max(d[k] for _, d in self.drift) for k in self.drift[0][1]}
+        print(f"\n{name}: {len(self.drift)} checkpoints; largest relative drift from the reference's arithmetic: "
+              + ", ".join(f"{k} {v:.2e}" for k, v in worst.items())
+              + f"; contact sets first differ at: {self.first_set_diff}")
+        return worst
+
+    def close(self):
+        self.gpu.close()
+        self.cr.close()
+        self.ref.close()
+
+
+def test_lattice_workload_full_run(gpu_lib, oracle_built):
+    """The small lattice workload as specified: 16 discs on a 4x4 lattice (pitch 2.2 mm), plates at
+    +-0.01 m/s, 10,000 steps, wall force and kinetic energy read every 100 steps."""
+    from melody2d_b200 import generator as g
+    scene = g.disc_lattice_scene()
+    assert (scene.nsteps, len(scene.bodies)) == (10000, 18)
+    t = Trio(g.flatten(scene))
+    max_active = 0
+    for k in range(100):
+        t.step(100)
+        t.check(f"step {100 * (k + 1)}", full=(k % 10 == 9))
+        max_active = max(max_active, t.gpu.monitor().active_contacts)
+    t.report("lattice 4x4, 10,000 steps")
+    assert max_active > 0 and t.gpu.monitor().kinetic_energy > 0
+    t.close()
+
+
+@pytest.mark.parametrize("seed", [5])
+def test_biaxial_sample_against_reference(gpu_lib, oracle_built, seed):
+    from melody2d_b200 import generator as g
+    t = Trio(g.flatten(g.biaxial_scene(seed=seed, n_discs=12, n_border=32, n_interior=80, workers=1)))
+    for k in range(30):
+        t.step(100)
+        t.check(f"step {100 * (k + 1)}", full=(k % 5 == 4))
+    t.report(f"biaxial 12 discs (seed {seed}), 3,000 steps")
+    assert t.gpu.monitor().active_contacts > 0
+    t.close()
+
+
+@pytest.mark.parametrize("case", ["periodic", "rotor"])
+def test_periodic_and_rotor(gpu_lib, oracle_built, case):
+    """x-periodic domain (proximity shifts -1..1, "Periodic" rigid strips whose seams the contacts
+    cross) and a free rigid disc spinning among deformable discs (nodes turned by cos and sin of the
+    body's rotation), 300 steps."""
+    from melody2d_b200 import generator as g
+    scene = g.periodic_strip_scene() if case == "periodic" else g.rotor_scene()
+    t = Trio(g.flatten(scene))
+    t.check("set-up")
+    for k in range(6):
+        t.step(50)
+        t.check(f"step {50 * (k + 1)}")
+    t.report(case)
+    c = t.gpu.contacts()
+    assert ((c["fx"] != 0) | (c["fy"] != 0)).sum() > 0
+    if case == "periodic":
+        assert set(np.unique(c["shiftM"]).tolist()) >= {-1, 0, 1}
+    else:
+        r = t.gpu.rigid()[0]
+        assert abs(r[4, 12]) > 1e-3        # the disc has turned (rd of body 4, radians)
+    t.close()
+
+
+def test_benchmark_workload_slice(gpu_lib, oracle_built):
+    """The 2000-disc biaxial workload the benchmark times (about 820,000 deformable nodes): the
+    set-up and 20 steps with the proximity updates after steps 10 and 20, bit-identical to the
+    correctly-rounded oracle; candidate and active sets equal to the reference's."""
+    from melody2d_b200 import generator as g
+    scene = g.biaxial_scene(seed=1, workers=min(32, os.cpu_count() or 1))
+    t = Trio(g.flatten(scene))
+    t.check("set-up")
+    for k in range(2):
+        t.step(10)
+        t.check(f"step {10 * (k + 1)}")
+    t.report("biaxial 2000 discs, 20 steps")
+    assert t.gpu.monitor().n_contacts > 0
+    t.close()

@@ -1,6 +1,8 @@
 """Pins the oracle to the reference solver for every contact law, the NeoHookean material, the
-border conditions of deformable bodies, INITIALIZE_CZM, and two 12-disc biaxial samples (rigid
-plates driven, lateral walls under oriented pressure along long borders, rigid-rigid pairs).
+border conditions of deformable bodies, INITIALIZE_CZM, two 12-disc biaxial samples (rigid
+plates driven, lateral walls under oriented pressure along long borders, rigid-rigid pairs), an
+x-periodic domain (discs meeting across the seam, "Periodic" rigid strips) and a free rigid disc
+spinning among deformable discs (rigid rotation through cos and sin).
 
 tests/golden/laws_ref.json holds SHA-256 digests of the reference's own FP64 state (made by
 tests/golden/make_golden_laws.py with the reference compiled from its sources) after set-up and
@@ -38,13 +40,18 @@ LAW_PARAMS = {
 }
 
 CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7+czm", "neohookean",
-                                                    "border_conditions", "biaxial12_s5", "biaxial12_s7"]
+                                                    "border_conditions", "biaxial12_s5", "biaxial12_s7",
+                                                    "periodic", "rotor"]
 
 
 def case_scene(name):
     """The scene of one case: a biaxial sample, or the pressed 3x3 lattice (about 45 loaded
     contacts after 100 steps) with the case's law, material or border conditions."""
     from melody2d_b200 import generator as g
+    if name == "periodic":
+        return g.periodic_strip_scene()
+    if name == "rotor":
+        return g.rotor_scene()
     if name.startswith("biaxial12_s"):
         return g.biaxial_scene(seed=int(name.split("_s")[1]), n_discs=12, n_border=32, n_interior=80, workers=1)
     sc = g.disc_lattice_scene(seed=0, nx=3, ny=3, pitch=2.0e-3, gap0=-1e-6, nsteps=300, v_plate=0.05)

@@ -51,6 +51,53 @@ def test_static_scratch_reduction_matches_monitor(gpu_lib):
     s.close()
 
 
+def _reduce_static(L, vel, mass, disp, n, cont, nc, out, stream):
+    return L.mel_monitor_reduce_static(ctypes.c_void_p(vel.data_ptr()), ctypes.c_void_p(mass.data_ptr()),
+                                       ctypes.c_void_p(disp.data_ptr()), n, ctypes.c_void_p(cont.data_ptr()), nc,
+                                       ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream))
+
+
+@pytest.mark.parametrize("n_nodes,n_contacts", [(300_001, 123_457), (2_097_152, 2_097_152)])
+def test_static_scratch_many_blocks(gpu_lib, n_nodes, n_contacts):
+    """Sizes that spread the reduction over many blocks, up to the largest accepted size (1024 blocks
+    of partials), against a float64 reduction in numpy.  The values are positive so that the sums
+    carry no cancellation and the order of the additions only moves the last bits."""
+    import torch
+    from melody2d_b200.abi import CONTACT_DTYPE
+    from melody2d_b200.solver import lib
+    rng = np.random.default_rng(n_nodes)
+    v = rng.uniform(0.5, 1.5, (n_nodes, 2))
+    m = rng.uniform(1e-6, 2e-6, (n_nodes, 2))
+    u = rng.uniform(1e-5, 3e-5, (n_nodes, 2))
+    cont = np.zeros(n_contacts, dtype=CONTACT_DTYPE)
+    act = rng.random(n_contacts) < 0.3
+    cont["fx"][act] = rng.uniform(-1., 1., int(act.sum()))
+    only_y = (~act) & (rng.random(n_contacts) < 0.1)      # a force along y alone also counts as active
+    cont["fy"][only_y] = 1e-3
+    ke = float(np.sum(0.5 * v[:, 0] * v[:, 0] * m[:, 0] + 0.5 * v[:, 1] * v[:, 1] * m[:, 1]))
+    ux = float(np.sum(u[:, 0] * m[:, 0]) / np.sum(m[:, 0]))
+    uy = float(np.sum(u[:, 1] * m[:, 1]) / np.sum(m[:, 0]))
+    n_act = int(act.sum() + only_y.sum())
+    dev = torch.device("cuda", 0)
+    tv, tm, tu = (torch.from_numpy(a).to(dev) for a in (v, m, u))
+    tc = torch.from_numpy(cont.view(np.uint8).reshape(-1)).to(dev)
+    out = torch.zeros(4, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    L = lib()
+    res = []
+    for _ in range(2):
+        out.fill_(-1.)
+        assert _reduce_static(L, tv, tm, tu, n_nodes, tc, n_contacts, out, stream) == 0, L.mel_last_error_string()
+        torch.cuda.synchronize(dev)
+        res.append(out.cpu().numpy().copy())
+    for r in res:
+        np.testing.assert_allclose(r[0], ke, rtol=1e-12)
+        np.testing.assert_allclose(r[1], ux, rtol=1e-12)
+        np.testing.assert_allclose(r[2], uy, rtol=1e-12)
+        assert int(r[3]) == n_act
+    np.testing.assert_array_equal(res[0], res[1])
+
+
 def test_static_scratch_rejects_oversize(gpu_lib):
     from melody2d_b200.solver import lib
     L = lib()
