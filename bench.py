@@ -4,11 +4,16 @@
 
 One JSON line on rank 0.  A step is one Euler_step (Code/Solver.h:10-88) of the whole sample plus
 the proximity updates that fall in it (Code/main.cpp:191-196, every 10 steps).  `value` is deformable
-node-steps per second of device time over the timed K steps (inputs ~1.5 GB per step, larger than
-L2); `e2e` repeats the measurement through the public C ABI with a device->host read of the
-monitored quantities every step; `cpu_baseline` is the reference solver, compiled from its sources,
-timed on this host's cores on a bounded sample of the same workload.  Under torchrun every rank
-advances its own independent sample (weak scaling, no collective in the step)."""
+node-steps per second of device time over the timed K steps (inputs ~1.7 GB per step, larger than
+L2).  `e2e` repeats the measurement through the public C ABI with the state in host memory, as the
+reference keeps it: every step uploads the node state from a pinned host buffer, steps, downloads the
+node state and reads the monitored quantities.  `cpu_baseline` is the reference solver, compiled from
+its sources, timed on this host's cores on a bounded sample of the same workload.  At N=1 the line
+also carries the headline of the batched and serving forms: `batched` (a slice of the batched
+workload, mixed precision in one batch, against the plain FP64 path one sample at a time) and
+`serving` (a short Poisson request stream served by continuous batching, p50/p99 latency).  Under
+torchrun every rank advances its own independent sample (weak scaling, no collective in the step).
+`--impl reference` times the reference itself on the same 2000-disc sample."""
 from __future__ import annotations
 
 import argparse
@@ -127,13 +132,14 @@ def allreduce_sum(pg, x: float) -> float:
 # --------------------------------------------------------------------------------------------
 def reference_sample(n_discs: int, steps: int, threads: int, seed: int = 1):
     """Runs the reference's own Euler_step loop (oracle/_ref/ref_harness) on a seeded sample of the
-    biaxial workload (same disc size distribution, nodes per disc, materials, contact law, loading)
-    and returns node-steps/s of its step loop."""
+    biaxial workload (same disc size distribution, nodes per disc, materials, contact law, loading;
+    seed 1 and 2000 discs is the sample the GPU arm times) and returns node-steps/s of its step
+    loop (wall clock of the loop alone, after Load_static, Load_dynamic and the set-up)."""
     from melody2d_b200 import generator as g
     harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
-    scene = g.biaxial_scene(seed=seed, n_discs=n_discs)
+    scene = g.biaxial_scene(seed=seed, n_discs=n_discs, workers=threads)
     with tempfile.TemporaryDirectory() as tmp:
-        g.write_asc(scene, tmp)
+        g.write_asc(scene, tmp, workers=threads)
         if os.path.exists(harness):
             out = subprocess.run([harness, tmp, str(steps), "-", "0", str(threads)], check=True,
                                  capture_output=True, text=True).stdout
@@ -156,20 +162,29 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def workload_name(discs: int) -> str:
+    return (f"biaxial: {discs} deformable discs, radii U[0.5,1.5] mm, 64 border + 340 interior nodes each, MLS "
+            f"(linear, W1), ElasticLinear, MohrCoulomb, mass x100, plates 0.05 m/s, walls 100 kPa; Euler, "
+            f"dt=0.5 dt_crit; proximity every 10 steps")
+
+
 def run_reference(args, rank, world, pg):
+    """The reference solver alone, on the sample the GPU arm times (seed 1, args.discs discs), for
+    args.ref_arm_steps steps of its own loop on all host threads; only rank 0 works."""
     if rank != 0:
         return
     threads = host_threads()
-    rate, cores, kind, scene = reference_sample(args.ref_discs, args.ref_steps, threads)
+    steps = args.ref_arm_steps
+    rate, cores, kind, scene = reference_sample(args.discs, steps, threads, seed=1)
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "node-steps/s", "n_gpus": args.gpus,
-            "steps": args.ref_steps, "warmup": 0, "ms_per_step": 1e3 * scene.n_deformable_nodes / rate,
+            "steps": steps, "warmup": 0, "ms_per_step": 1e3 * scene.n_deformable_nodes / rate,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded biaxial packing generator)",
-            "config": {"workload": f"biaxial sample: {args.ref_discs} deformable discs of the 2000-disc workload "
-                                   f"(radii U[0.5,1.5] mm, 64 border + 340 interior nodes, MLS, MohrCoulomb), "
-                                   f"2 driven plates, 2 confining walls", "nodes": scene.n_deformable_nodes},
+            "config": {"workload": workload_name(args.discs), "nodes_per_gpu": scene.n_deformable_nodes,
+                       "precision": "fp64", "sample": f"the GPU arm's sample (seed 1), the first {steps} steps "
+                                                    f"of its loop timed after set-up"},
             "cpu_baseline": {"value": rate, "unit": "node-steps/s", "cores": cores, "kind": kind,
-                             "sample": f"{args.ref_discs}-disc sample, {args.ref_steps} steps"},
+                             "sample": f"the full {args.discs}-disc sample, {steps} steps, all host threads"},
             "e2e": {"value": rate, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -178,8 +193,9 @@ def run_reference(args, rank, world, pg):
 # our path
 # --------------------------------------------------------------------------------------------
 def run_ours(args, rank, world, local, pg):
+    import ctypes
     from melody2d_b200 import abi, generator as g
-    from melody2d_b200.solver import Solver
+    from melody2d_b200.solver import PinnedArray, Solver, lib as solver_lib
     workers = max(1, host_threads() // max(1, world))
     t0 = time.perf_counter()
     scene = g.biaxial_scene(seed=1 + rank, n_discs=args.discs, workers=workers)
@@ -196,7 +212,7 @@ def run_ours(args, rank, world, local, pg):
     clocks = ClockSampler(local)
     barrier(pg)
     clocks.start()
-    io = s.step(args.steps)                               # synchronises on its stream at the end
+    io_t = s.step(args.steps)                             # synchronises on its stream at the end
     barrier(pg)
     clk = clocks.stop()
     st = s.step_stats()
@@ -216,43 +232,65 @@ def run_ours(args, rank, world, local, pg):
             traffic = per_gp * s.sizes()["n_gauss"] if per_gp else None
         except Exception:
             traffic = None
-    # end to end through the C ABI: every iteration steps and reads the monitored quantities back
+    # end to end through the C ABI with the state in host memory (where the reference keeps it):
+    # every iteration uploads the node state from a pinned host buffer, steps once, downloads the
+    # node state and reads the monitored quantities back
     s.set_timing(False)
     n_e2e = min(args.steps, args.e2e_steps)
+    L = solver_lib()
+    host = PinnedArray(12 * s.nn)
+    hp = host.array.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     mon = abi.MelMonitor()
+    io = abi.MelStepIO(nsteps=1, run_proximity=1)
+    L.mel_get_node_state(s.h, hp)
     barrier(pg)
     t0 = time.perf_counter()
     for _ in range(n_e2e):
-        s.step(1)
-        m = s.monitor()
+        rc = L.mel_set_node_state(s.h, hp) or L.mel_step(s.h, ctypes.byref(io)) or \
+            L.mel_get_node_state(s.h, hp) or L.mel_monitor_compute(s.h, ctypes.byref(mon))
+        if rc:
+            raise RuntimeError(L.mel_last_error_string().decode())
     t_e2e = time.perf_counter() - t0
     t_e2e = allreduce_max(pg, t_e2e)
+    host.close()
     e2e_value = allreduce_sum(pg, nodes) * n_e2e / t_e2e
+    # the same loop with the state left on the device (only the monitored quantities come back)
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        s.step(1)
+        s.monitor()
+    t_res = allreduce_max(pg, time.perf_counter() - t0)
+    resident_value = allreduce_sum(pg, nodes) * n_e2e / t_res
+    n_solver_nodes = s.nn
+    sizes = s.sizes()
+    s.close()
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras = headline_extras(args, rank, world, local, pg)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         rate, cores, kind, _ = reference_sample(args.ref_discs, args.ref_steps, host_threads())
         cpu = {"value": rate, "unit": "node-steps/s", "cores": cores, "kind": kind,
                "sample": f"{args.ref_discs}-disc sample of the same workload, {args.ref_steps} steps, all host threads"}
     if rank == 0:
-        sizes = s.sizes()
         line = {
             "metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if precision == 0 else "f32 (dN, strain, stress, contributions) + f64",
             "data": "synthetic (seeded biaxial packing generator)",
-            "config": {"workload": f"biaxial: {args.discs} deformable discs, radii U[0.5,1.5] mm, 64 border + 340 "
-                                   f"interior nodes each, MLS (linear, W1), ElasticLinear, MohrCoulomb, mass x100, "
-                                   f"plates 0.05 m/s, walls 100 kPa; Euler, dt=0.5 dt_crit; proximity every 10 steps",
-                       "nodes_per_gpu": nodes, "gauss_points": sizes["n_gauss"], "gp_entries": sizes["n_gp_entries"],
+            "config": {"workload": workload_name(args.discs), "nodes_per_gpu": nodes, "gauss_points": sizes["n_gauss"], "gp_entries": sizes["n_gp_entries"],
                        "contacts": st["n_contacts"], "precision": args.precision,
                        "l2": "inputs larger than L2 (%.2f GB streamed per step)" % ((st["bytes_body"] + st["bytes_contact"]) / 1e9),
                        "generate_s": round(t_gen, 2), "create_s": round(t_create, 2)},
-            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 20 * 8, "steps": n_e2e,
-                    "calls": "per step: mel_step(nsteps=1) then mel_monitor_compute, host wall clock",
-                    "inputs": "the model is uploaded once by mel_create (setup.h2d_bytes); a step takes no new "
-                              "input (time, loading histories and state stay on the device), so each step copies "
-                              "nothing host->device and reads the 20 monitored doubles back",
+            "e2e": {"value": e2e_value, "unit": "node-steps/s", "h2d_bytes_per_step": 96 * n_solver_nodes,
+                    "d2h_bytes_per_step": 96 * n_solver_nodes + ctypes.sizeof(abi.MelMonitor), "steps": n_e2e,
+                    "calls": "per step: mel_set_node_state (pinned host buffer), mel_step(nsteps=1), "
+                             "mel_get_node_state (pinned host buffer), mel_monitor_compute; host wall clock",
+                    "inputs": "the node state (12 doubles per node: u, v, a and their parameters) lives in host "
+                              "memory as in the reference and crosses the host link both ways every step; the "
+                              "model itself is uploaded once by mel_create (setup.h2d_bytes)",
+                    "resident_state": {"value": resident_value, "calls": "mel_step(nsteps=1) then "
+                                       "mel_monitor_compute, state kept on the device"},
                     "setup": {"h2d_bytes": int(model_bytes), "create_s": round(t_create, 2)}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "kernel": "body_kernel", "peak_source": peak_kind,
@@ -261,10 +299,39 @@ def run_ours(args, rank, world, local, pg):
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": kt["launches"],
-            "proximity_updates": io.n_proximity,
+            "proximity_updates": io_t.n_proximity,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
-    s.close()
+
+
+def headline_extras(args, rank, world, local, pg):
+    """The north-star figures beside the single-sample line (one GPU): a slice of the batched
+    workload in one mixed-precision batch against the plain FP64 path one sample at a time (samples
+    per hour extrapolated to the workload's 20,000 steps per sample, and the mixed form's errors),
+    and a short serving run (p50/p99 latency, samples per hour of both arms)."""
+    import copy
+    out = {}
+    a = copy.copy(args)
+    a.samples, a.plain_subset = args.batch_samples, args.batch_plain_subset
+    a.accuracy_samples, a.accuracy_steps = args.batch_accuracy_samples, args.batch_accuracy_steps
+    a.steps, a.warmup = max(args.steps, 20), max(args.warmup, 3)
+    b = run_batch(a, rank, world, local, pg, emit=False)
+    if b is not None:
+        out["batched"] = {"metric": "samples/h", "value": b["value"], "unit": "samples/h",
+                          "ms_per_step": b["ms_per_step"], "steps": a.steps, "node_steps_per_s": b["node_steps_per_s"],
+                          "config": b["config"], "plain_fp64_one_at_a_time": b["plain_fp64_one_at_a_time"],
+                          "ratio_vs_plain_fp64": b["ratio_vs_plain_fp64"], "accuracy_vs_fp64": b["accuracy_vs_fp64"],
+                          "gpu_launches": b["gpu_launches"], "clocks": b["clocks"]}
+    a = copy.copy(args)
+    a.rate, a.duration, a.drain, a.step_cap = args.serve_rate, args.serve_duration, args.serve_drain, args.serve_step_cap
+    v = run_serve(a, rank, world, local, pg, emit=False)
+    if v is not None:
+        out["serving"] = {"metric": "samples/h", "value": v["value"], "unit": "samples/h", "config": v["config"],
+                          "arms": v["arms"], "ratio_samples_h_vs_plain_fp64": v["ratio_samples_h_vs_plain_fp64"],
+                          "same_requests_compared": v["same_requests_compared"],
+                          "max_rel_error_vs_plain_fp64": v["max_rel_error_vs_plain_fp64"]}
+    return out
 
 
 def create_solvers(flats, precision, device, threads):
@@ -275,7 +342,7 @@ def create_solvers(flats, precision, device, threads):
         return list(ex.map(lambda f: Solver.from_flat(f, precision=precision, device=device, retain=False), flats))
 
 
-def run_batch(args, rank, world, local, pg):
+def run_batch(args, rank, world, local, pg, emit=True):
     """Batched workload: S independent biaxial samples (grains log-uniform in [50,1000], 32-96
     border nodes per grain, confinement 50-400 kPa, friction 0.1-0.5) advanced together in one
     mixed-precision batch, against the plain FP64 path run one sample at a time on a subset.
@@ -366,13 +433,15 @@ def run_batch(args, rank, world, local, pg):
                                  "active_contacts_mixed_fp64": [e["active_contacts"] for e in errs]},
             "clocks": clk, "gpu_launches": st["launches"] - launches0,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     flats.clear()
     for sf in kept.values():
         sf.release()
+    return line if rank == 0 else None
 
 
-def run_serve(args, rank, world, local, pg):
+def run_serve(args, rank, world, local, pg, emit=True):
     """Serving: seeded Poisson arrivals (args.rate per second for args.duration seconds) of
     batched-workload requests, each run to 5 % axial strain or args.step_cap steps; the batched
     mixed-precision server against the plain FP64 path serving one request at a time, on the same
@@ -415,7 +484,10 @@ def run_serve(args, rank, world, local, pg):
             "max_rel_error_vs_plain_fp64": {"kinetic_energy": err_ke, "wall_contact_force": err_wall},
             "gpu_launches": summary["batched_mixed"]["gpu_launches"],
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 def compare_precisions(args, rank, world, local, pg):
@@ -489,6 +561,18 @@ def main():
     ap.add_argument("--plain-subset", type=int, default=8)
     ap.add_argument("--accuracy-steps", type=int, default=2000)
     ap.add_argument("--accuracy-samples", type=int, default=4)
+    # the reference arm: steps of the reference's own loop timed on the full sample
+    ap.add_argument("--ref-arm-steps", type=int, default=1000)
+    # headline blocks of the default line (one GPU): batched slice and short serving run
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--batch-samples", type=int, default=32)
+    ap.add_argument("--batch-plain-subset", type=int, default=4)
+    ap.add_argument("--batch-accuracy-samples", type=int, default=2)
+    ap.add_argument("--batch-accuracy-steps", type=int, default=2000)
+    ap.add_argument("--serve-rate", type=float, default=2.0)
+    ap.add_argument("--serve-duration", type=float, default=8.0)
+    ap.add_argument("--serve-drain", type=float, default=60.0)
+    ap.add_argument("--serve-step-cap", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -215,6 +215,11 @@ mel_status mel_set_contacts(mel_handle* h, const mel_contact* contacts, int n);
 /* node_state layout as in mel_model_desc::node_state (12 doubles per node). */
 mel_status mel_get_node_state(mel_handle* h, double* node_state);
 mel_status mel_set_node_state(mel_handle* h, const double* node_state);
+/* Page-lock (pin) a caller-owned host buffer, so that the state transfers above and below move at
+ * the host link's full speed instead of through a pageable bounce; mel_unpin_host releases it.
+ * No counterpart in the reference, whose state lives in host memory only. */
+mel_status mel_pin_host(void* ptr, size_t bytes);
+mel_status mel_unpin_host(void* ptr);
 /* current positions, 2 doubles per node */
 mel_status mel_get_positions(mel_handle* h, double* xy);
 /* nodal force components of the last step, [n_nodes*2] each; any pointer may be NULL.

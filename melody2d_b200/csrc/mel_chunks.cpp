@@ -83,11 +83,13 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
         if (nnb > 4096) { mel_set_error("deformable body %d has %d nodes (pull records hold 12-bit node indices)", b, nnb); return MEL_ERR_UNSUPPORTED; }
         int g = d->body_gp_ptr[b];
         const int g1 = d->body_gp_ptr[b + 1];
+        const int gpcap = mixed ? MEL_CHUNK_GP_MX : MEL_CHUNK_GP_FP64;
         while (g < g1) {
-            // as many points as fit MEL_CHUNK_GP slots, ecap entries and the 10-bit row tables
+            // as many points as fit gpcap slots (one point thread each), ecap entries and the 10-bit
+            // row tables
             int ngp = 0, nent = 0, nsmax = 0;
             ns.clear();
-            while (g + ngp < g1 && ngp < MEL_CHUNK_GP) {
+            while (g + ngp < g1 && ngp < gpcap) {
                 int c = d->gp_sup_ptr[g + ngp + 1] - d->gp_sup_ptr[g + ngp];
                 if (c > 255 || c <= 0) { mel_set_error("Gauss point %d has %d supports (1..255 supported)", g + ngp, c); return MEL_ERR_UNSUPPORTED; }
                 if (nent + c > ecap) break;

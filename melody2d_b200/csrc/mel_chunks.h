@@ -13,7 +13,7 @@ struct mel_chunk_set {
     long long n_pad = 0;           // padding entries (rounding of each chunk to 8 entries)
 };
 
-// Cuts every deformable body's Gauss points into chunks of at most MEL_CHUNK_GP points and
-// at most `ecap` entries.  Returns MEL_OK or an error code with the message set.
+// Cuts every deformable body's Gauss points into chunks of at most MEL_CHUNK_GP_FP64 (FP64
+// images) or MEL_CHUNK_GP_MX (FP32 images) points and at most `ecap` entries.  Returns MEL_OK or an error code with the message set.
 // mixed: dN pairs stored as FP32 (the mixed-precision pass) instead of FP64.
 mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out, bool mixed = false);

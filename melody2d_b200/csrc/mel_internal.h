@@ -10,9 +10,13 @@
 #include <cuda_runtime.h>
 #include "melgpu.h"
 
-#define MEL_BODY_THREADS 256      // threads per body CTA
-#define MEL_BODY_CTHREADS 224     // of which run the Gauss-point pipeline (warps 0-6); warp 7 scatters contacts
-#define MEL_CHUNK_GP MEL_BODY_CTHREADS   // Gauss points per chunk (one compute thread each)
+#define MEL_BODY_THREADS 256      // threads per body CTA: point warps, pull warps, warp 7 (copies, contacts)
+#define MEL_STAGES 3              // chunk buffers in the body kernel's ring
+#define MEL_PT_WARPS(mx) ((mx) ? 4 : 3)   // point warps of the FP64 / mixed body kernel (the rest of 0-6 pull)
+#define MEL_CHUNK_GP_FP64 96      // Gauss points per chunk: one point thread each
+#define MEL_CHUNK_GP_MX 128
+#define MEL_CHUNK_GP_MAX 128
+#define MEL_BAR_BYTES 128         // the ring's mbarriers (3 per stage) and the abort flag
 #define MEL_CHUNK_E_MAX 2048      // support entries per chunk, upper bound (the host may choose less)
 #define MEL_WAIT_NS 1000000000ull // bound of every device-side wait (1 s)
 #define MEL_NBR_CAP_DEFAULT 64    // neighbour slots per body (grown on overflow)

@@ -299,11 +299,12 @@ __device__ void body_drivendof(const mel_dev& d, int b, double T, double* drv)
 // body kernel: deformable path
 // ------------------------------------------------------------------------------------------
 // scatter v * N_j onto the supports of body-local node `node` (one warp; lanes over supports)
-__device__ __forceinline__ void warp_scatter(const mel_dev& d, int n0, int node, double fx, double fy, double2* acc, int lane)
+__device__ __forceinline__ void warp_scatter(const mel_dev& d, int n0, int node, double fx, double fy, double2* acc, int lane,
+                                             int nlanes = 32)
 {
     int gn = n0 + node;
     int a = d.sup_ptr[gn], bnd = d.sup_ptr[gn + 1];
-    for (int j = a + lane; j < bnd; j += 32) {
+    for (int j = a + lane; j < bnd; j += nlanes) {
         double N = d.sup_N[j];
         int t = d.sup_idx[j];
         double2 f = acc[t];
@@ -338,8 +339,19 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 }
 // generic-proxy accesses to a buffer are ordered before the bulk copy that refills it
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// barrier of the Gauss-point warps only (warp 7 runs the contact scatter meanwhile)
-__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, %0;" :: "n"(MEL_BODY_CTHREADS) : "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+// barrier of the pull warps alone (named barrier 3), returning whether any of them passed `v`
+template <int NT>
+__device__ __forceinline__ bool pull_group_any(bool v)
+{
+    unsigned r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 3, %2, p;\n\tselp.u32 %0, 1, 0, q;\n}"
+                 : "=r"(r) : "r"((unsigned)v), "n"(NT) : "memory");
+    return r != 0;
+}
 // barrier of warps 1-7 in the body tail (warp 0 sums the works meanwhile)
 __device__ __forceinline__ void tail_sync() { asm volatile("bar.sync 2, %0;" :: "n"(MEL_BODY_THREADS - 32) : "memory"); }
 __device__ __forceinline__ unsigned long long global_ns()
@@ -587,10 +599,10 @@ __device__ __forceinline__ void chunk_points_mx(int t, int ngp, int mtype, float
 // Shared memory of a deformable body (n nodes, staging buffers of img_cap bytes each):
 //   s_up, s_f, s_fc        3 x n double2       displacements, internal forces, contact forces
 //   s_upf (mixed only)     n2 x float2         displacements relative to node 0 (n2 = n rounded to 2)
-//   2 mbarriers + abort flag                   32 bytes
-//   region                 max(2 img_cap, 112 n) bytes: two chunk images during the Gauss-point
-//                          pass, then s_fn, s_fd, s_vp, s_ap (n double2 each) and the six work
-//                          terms per node (6 x n double)
+//   ring mbarriers + abort flag                MEL_BAR_BYTES
+//   region                 max(MEL_STAGES img_cap, 112 n) bytes: the ring of chunk images during
+//                          the Gauss-point pass, then s_fn, s_fd, s_vp, s_ap (n double2 each) and
+//                          the six work terms per node (6 x n double)
 template <bool MX>
 __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
 {
@@ -605,10 +617,15 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
     float2* s_upf = reinterpret_cast<float2*>(s_fc + n);
     uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
                                                      : reinterpret_cast<char*>(s_fc + n));
-    volatile int* s_abort = reinterpret_cast<volatile int*>(s_bar + 2);
-    char* region = reinterpret_cast<char*>(s_bar + 4);
-    char* const buf0 = region;
-    char* const buf1 = region + d.img_cap;
+    // stage s of the ring: full[s] (the bulk copy landed), pointed[s] (every point thread has
+    // written its contributions), empty[s] (every pull thread is done with the buffer)
+    uint64_t* full = s_bar;
+    uint64_t* pointed = s_bar + MEL_STAGES;
+    uint64_t* empty = s_bar + 2 * MEL_STAGES;
+    volatile int* s_abort = reinterpret_cast<volatile int*>(s_bar + 3 * MEL_STAGES);
+    char* region = reinterpret_cast<char*>(s_bar) + MEL_BAR_BYTES;
+    constexpr int PTW = MEL_PT_WARPS(MX);                 // point warps 0 .. PTW-1
+    constexpr int PLW = 7 - PTW;                          // pull warps PTW .. 6; warp 7 copies and scatters
     const int ch0 = d.b_chunk0[b];
     const int nch = d.b_chunk0[b + 1] - ch0;
     for (int i = tid; i < n; i += blockDim.x) {
@@ -624,60 +641,70 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
         }
     }
     if (tid == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
+        for (int st = 0; st < MEL_STAGES; st++) {
+            mbar_init(&full[st], 1);
+            mbar_init(&pointed[st], 32 * PTW);
+            mbar_init(&empty[st], 32 * PLW);
+        }
         mbar_init_fence();
         *s_abort = 0;
     }
     __syncthreads();
-    if (warp < MEL_BODY_CTHREADS / 32) {
-        // ---- Update_internal_forces: chunk k is computed while chunk k+1 is in flight ----------
-        const int mat = d.b_mat[b];
-        const int mtype = d.mat_type[mat];
-        const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
-        const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
-        int issued = 0;
-        if (tid == 0)
-            for (; issued < 2 && issued < nch; issued++) {
-                const mel_chunk c = d.chunk[ch0 + issued];
-                mbar_arrive_expect_tx(&s_bar[issued], (unsigned)c.bytes);
-                bulk_load(issued ? buf1 : buf0, d.img + c.img, (unsigned)c.bytes, &s_bar[issued]);
+    // ---- Update_internal_forces as a pipeline over the body's chunks: warp 7 streams chunk images
+    // into a ring of MEL_STAGES buffers, the point warps form strain, stress and contributions of
+    // chunk k while the pull warps add those of chunk k-1 to the nodes (in ascending point order,
+    // chunk after chunk), so the two ordered chains and the copies overlap --------------------------
+    const int mat = d.b_mat[b];
+    const int mtype = d.mat_type[mat];
+    const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
+    const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
+    if (warp < PTW) {
+        for (int k = 0; k < nch; k++) {
+            const int st = k % MEL_STAGES;
+            char* bk = region + st * d.img_cap;
+            if (*s_abort) break;
+            if (!mbar_wait_bounded(&full[st], (unsigned)((k / MEL_STAGES) & 1))) {
+                atomicOr(&d.err[MEL_E_WAIT], 1u);
+                *s_abort = 1;
+                break;
             }
-        int k = 0;
-        for (; k < nch; k++) {
-            const int sel = k & 1;
-            char* bk = sel ? buf1 : buf0;
-            long long nxt_img = 0;
-            int nxt_bytes = 0;
-            if (tid == 0 && k + 2 < nch) { const mel_chunk c = d.chunk[ch0 + k + 2]; nxt_img = c.img; nxt_bytes = c.bytes; }
-            const bool ok = mbar_wait_bounded(&s_bar[sel], (unsigned)((k >> 1) & 1));
-            if (!ok) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
-            const int4 hdr = ok ? *reinterpret_cast<const int4*>(bk) : make_int4(0, 0, 0, 0);
+            const int4 hdr = *reinterpret_cast<const int4*>(bk);
             const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
-            const uint16_t* s_idx = reinterpret_cast<const uint16_t*>(bk + L.idx);
+            if (tid < hdr.x) {
+                if (MX)
+                    chunk_points_mx(tid, hdr.x, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN),
+                                    reinterpret_cast<const uint16_t*>(bk + L.idx), reinterpret_cast<const double*>(bk + L.c0),
+                                    reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
+                else
+                    chunk_points(tid, hdr.x, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN),
+                                 reinterpret_cast<const uint16_t*>(bk + L.idx), reinterpret_cast<const double*>(bk + L.c0),
+                                 reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
+            }
+            fence_proxy_async();      // these generic writes precede the copy that will refill the buffer
+            mbar_arrive(&pointed[st]);
+        }
+    } else if (warp < 7) {
+        // pull: each touched node subtracts its contributions in ascending Gauss-point order (the
+        // mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31 of group
+        // t >> 5, its entry j at row j of the group's row table.  Groups are sorted by entry count;
+        // pull warp w takes groups w, 2 PLW - 1 - w, 2 PLW + w, ... (snake order).  The group's
+        // barrier at the top of every chunk keeps a node's chunks in order when different warps
+        // hold it, and makes the group leave together when a wait gives up.
+        const int w = warp - PTW;
+        for (int k = 0; k < nch; k++) {
+            const int st = k % MEL_STAGES;
+            char* bk = region + st * d.img_cap;
+            const bool ok = !*s_abort && mbar_wait_bounded(&pointed[st], (unsigned)((k / MEL_STAGES) & 1));
+            if (!ok && !*s_abort) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
+            if (pull_group_any<32 * PLW>(!ok)) break;
+            const int4 hdr = *reinterpret_cast<const int4*>(bk);
+            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
             const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
             const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
             const uint16_t* s_roff = reinterpret_cast<const uint16_t*>(bk + L.roff);
-            if (tid < hdr.x) {
-                if (MX)
-                    chunk_points_mx(tid, hdr.x, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN), s_idx,
-                                    reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
-                                    reinterpret_cast<const uint16_t*>(bk + L.roff));
-                else
-                    chunk_points(tid, hdr.x, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN), s_idx,
-                                 reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
-                                 reinterpret_cast<const uint16_t*>(bk + L.roff));
-            }
-            compute_sync();
-            if (*s_abort) break;
-            // pull: each touched node subtracts its contributions in ascending Gauss-point order
-            // (the mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31
-            // of group t >> 5, its entry j at row j of the group's row table.  Groups are sorted
-            // by entry count; warp w takes groups w, 13 - w, 14 + w, ... (snake order), so the
-            // heaviest group has a warp to itself and the lighter ones pair up.
             const int ngrp = (hdr.z + 31) >> 5;
-            for (int i = 0; 7 * i < ngrp; i++) {
-                const int t = (7 * i + ((i & 1) ? 6 - warp : warp)) * 32 + lane;
+            for (int i = 0; PLW * i < ngrp; i++) {
+                const int t = (PLW * i + ((i & 1) ? PLW - 1 - w : w)) * 32 + lane;
                 if (t >= hdr.z) continue;
                 const unsigned rec = s_tn[t];
                 const int node = (int)(rec & 0xfffu);
@@ -756,24 +783,42 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
                 s_f[node] = f;
             }
             fence_proxy_async();
-            compute_sync();
-            if (tid == 0 && k + 2 < nch) {
-                mbar_arrive_expect_tx(&s_bar[sel], (unsigned)nxt_bytes);
-                bulk_load(bk, d.img + nxt_img, (unsigned)nxt_bytes, &s_bar[sel]);
-                issued++;
-            }
+            mbar_arrive(&empty[st]);
         }
-        if (tid == 0 && *s_abort)   // give the copies still in flight a bounded time to land
-            for (int c = k; c < issued; c++) mbar_wait_bounded(&s_bar[c & 1], (unsigned)((c >> 1) & 1));
+    } else if (lane == 0) {
+        // ---- producer: the first MEL_STAGES chunks at once, then each chunk into the buffer the
+        // pull warps released ----------------------------------------------------------------------
+        int issued = 0;
+        for (; issued < MEL_STAGES && issued < nch; issued++) {
+            const mel_chunk c = d.chunk[ch0 + issued];
+            mbar_arrive_expect_tx(&full[issued], (unsigned)c.bytes);
+            bulk_load(region + issued * d.img_cap, d.img + c.img, (unsigned)c.bytes, &full[issued]);
+        }
+        for (; issued < nch; issued++) {
+            const int st = issued % MEL_STAGES;
+            const mel_chunk c = d.chunk[ch0 + issued];
+            if (*s_abort) break;
+            if (!mbar_wait_bounded(&empty[st], (unsigned)((issued / MEL_STAGES - 1) & 1))) {
+                atomicOr(&d.err[MEL_E_WAIT], 1u);
+                *s_abort = 1;
+                break;
+            }
+            mbar_arrive_expect_tx(&full[st], (unsigned)c.bytes);
+            bulk_load(region + st * d.img_cap, d.img + c.img, (unsigned)c.bytes, &full[st]);
+        }
+        if (*s_abort)   // give the copies still in flight a bounded time to land before the CTA ends
+            for (int c = issued - 1; c >= 0 && c >= issued - MEL_STAGES; c--)
+                mbar_wait_bounded(&full[c % MEL_STAGES], (unsigned)((c / MEL_STAGES) & 1));
     } else {
-        // ---- contact forces (warp 7): slave scatter in list order, then master scatter in send
-        // order (Body::Update_contact_forces, Code/Body.h:1642-1900) ---------------------------
+        // ---- contact forces (lanes 1-31 of warp 7, meanwhile): slave scatter in list order, then
+        // master scatter in send order (Body::Update_contact_forces, Code/Body.h:1642-1900) ---------
+        const unsigned mask = 0xfffffffeu;
         for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
             const mel_contact* ct = d.cont + c;
             if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
             double Fsx = ct->fx, Fsy = ct->fy;
-            warp_scatter(d, n0, ct->nodeS, Fsx, Fsy, s_fc, lane);
-            __syncwarp();
+            warp_scatter(d, n0, ct->nodeS, Fsx, Fsy, s_fc, lane - 1, 31);
+            __syncwarp(mask);
         }
         for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
             int2 rg = d.inc_rng[r];
@@ -783,12 +828,13 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
                 double Fsx = ct->fx, Fsy = ct->fy;
                 for (int k = 0; k < 4; k++) {
                     double sk = ct->shapeM[k];
-                    warp_scatter(d, n0, ct->nodeM[k], -Fsx * sk, -Fsy * sk, s_fc, lane);
-                    __syncwarp();
+                    warp_scatter(d, n0, ct->nodeM[k], -Fsx * sk, -Fsy * sk, s_fc, lane - 1, 31);
+                    __syncwarp(mask);
                 }
             }
         }
     }
+    __syncwarp();
     __syncthreads();
     if (*s_abort) return;
     double2* s_fn = reinterpret_cast<double2*>(region);
@@ -1241,9 +1287,9 @@ void mel_launch_czm_init(const mel_dev& d, cudaStream_t s)
 
 size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)
 {
-    size_t base = 3 * sizeof(double2) * (size_t)max_nodes + 32;
+    size_t base = 3 * sizeof(double2) * (size_t)max_nodes + MEL_BAR_BYTES;
     if (mixed) base += sizeof(float2) * (size_t)((max_nodes + 1) & ~1);
-    size_t stage = 2 * (size_t)max_image_bytes;
+    size_t stage = MEL_STAGES * (size_t)max_image_bytes;
     size_t post = (4 * sizeof(double2) + 6 * sizeof(double)) * (size_t)max_nodes;
     size_t rigid = (64 + 6 * MEL_RIGID_BATCH) * sizeof(double);
     size_t r = base + (stage > post ? stage : post);

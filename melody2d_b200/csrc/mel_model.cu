@@ -74,6 +74,7 @@ struct mel_handle {
     int timing = 0;
     double* d_monitor = nullptr;
     double* d_monitor_part = nullptr;
+    double* d_state = nullptr;   // node state in the 12-doubles-per-node layout (mel_get/set_node_state)
     int* d_rigid_ids = nullptr;
     int nrigid = 0;
     int precision = MEL_PREC_FP64;
@@ -441,9 +442,9 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     h->H.b_per.assign(d->body_periodic, d->body_periodic + nb);
     h->H.b_bd0.assign(d->body_border_ptr, d->body_border_ptr + nb + 1);
     h->H.bd_e0.assign(d->border_node_ptr, d->border_node_ptr + nbd + 1);
-    // Gauss points: chunk images of <= MEL_CHUNK_GP points and <= ecap support entries.  The entry
-    // cap is the largest that lets two body CTAs share an SM; a body too large for that runs one
-    // CTA per SM.
+    // Gauss points: chunk images of <= gpcap points (one point thread each) and <= ecap support
+    // entries.  The entry cap is the largest that lets two body CTAs, each with its ring of
+    // MEL_STAGES images, share an SM; a body too large for that runs one CTA per SM.
     int max_def_nodes = 1;
     for (int b = 0; b < nb; b++)
         if (d->body_type[b] == MEL_BODY_DEFORMABLE) max_def_nodes = std::max(max_def_nodes, d->body_node_ptr[b + 1] - d->body_node_ptr[b]);
@@ -455,13 +456,14 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     const size_t two_per_sm = (size_t)(smem_sm / 2 - smem_res);
     {
         const bool mixed = h->precision == MEL_PREC_MIXED;
-        // FP32 images hold 12 bytes per entry instead of 20, so the mixed form tries larger chunks
-        const int caps_fp64[] = { MEL_CHUNK_E_MAX, 1536, 1024, 768, 512, 256 };
-        const int caps_mixed[] = { 2 * MEL_CHUNK_E_MAX, 3584, 3072, 2560, MEL_CHUNK_E_MAX, 1536, 1024, 512, 256 };
+        // FP32 images hold 12 bytes per entry instead of 20, and the mixed kernel has more point threads
+        const int gpcap = mixed ? MEL_CHUNK_GP_MX : MEL_CHUNK_GP_FP64;
+        const int caps_fp64[] = { MEL_CHUNK_E_MAX, 1792, 1536, 1408, 1344, 1280, 1216, 1152, 1024, 768, 512, 256 };
+        const int caps_mixed[] = { MEL_CHUNK_E_MAX, 1920, 1792, 1664, 1536, 1408, 1280, 1024, 768, 512, 256 };
         std::vector<int> caps = mixed ? std::vector<int>(std::begin(caps_mixed), std::end(caps_mixed))
                                       : std::vector<int>(std::begin(caps_fp64), std::end(caps_fp64));
         // the cap is chosen from an upper bound of the image size (a chunk holds at most ecap
-        // entries, MEL_CHUNK_GP points, min(ecap, nodes) touched nodes and one row per support
+        // entries, gpcap points, min(ecap, nodes) touched nodes and one row per support
         // of each group's largest point), so the images are built once
         // Pull rows: the first pull group has at most (the most points any node supports) rows,
         // and each later group at most its predecessor's smallest count, so all later groups
@@ -480,9 +482,10 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
                 }
             }
         auto bound = [&](int ecap) {
-            const int groups = (MEL_CHUNK_GP + 31) / 32;
-            const int pull_rows = std::min(max_use, MEL_CHUNK_GP) + ecap / 32;
-            return mel_chunk_sections(MEL_CHUNK_GP, ecap, std::min(ecap, max_def_nodes),
+            const int ne = std::min(ecap, gpcap * max_ns);
+            const int groups = (gpcap + 31) / 32;
+            const int pull_rows = std::min(max_use, gpcap) + ne / 32;
+            return mel_chunk_sections(gpcap, ne, std::min(ne, max_def_nodes),
                                       std::min(1023, groups * max_ns) + pull_rows, mixed ? 8 : 16).bytes;
         };
         int chosen = -1;
@@ -754,6 +757,7 @@ mel_status mel_destroy(mel_handle* h)
     if (h->ck.packed) cudaEventDestroy(h->ck.packed);
     if (h->ck.landed) cudaEventDestroy(h->ck.landed);
     if (h->ck.d_stage) cudaFree(h->ck.d_stage);
+    if (h->d_state) cudaFree(h->d_state);
     if (h->ck.h_stage) cudaFreeHost(h->ck.h_stage);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
@@ -884,18 +888,76 @@ mel_status mel_set_contacts(mel_handle* h, const mel_contact* c, int n)
     return check_errors(h);
 }
 
+// node state in the 12-doubles-per-node layout of mel_model_desc::node_state
+static __global__ void state_pack_kernel(const double2* u, const double2* v, const double2* a, const double2* up,
+                                         const double2* vp, const double2* ap, int nn, double* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const double2 w[6] = { u[i], v[i], a[i], up[i], vp[i], ap[i] };
+    double* o = out + 12 * (size_t)i;
+#pragma unroll
+    for (int k = 0; k < 6; k++) { o[2 * k] = w[k].x; o[2 * k + 1] = w[k].y; }
+}
+
+// The inverse, with the positions that follow from it: deformable nodes x = X0 + u
+// (Code/Node.h:233-237); rigid nodes take position and velocity from their body's state
+// (Code/Body.h:2284-2300), as upload_state computes them on the host.
+static __global__ void state_unpack_kernel(mel_dev d, const double* st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nn) return;
+    int lo = 0, hi = d.nb;                    // body of node i: largest b with b_node0[b] <= i
+    while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (d.b_node0[mid] <= i) lo = mid; else hi = mid; }
+    const double* s = st + 12 * (size_t)i;
+    const double2 u = make_double2(s[0], s[1]);
+    double2 v = make_double2(s[2], s[3]);
+    d.u[i] = u; d.a[i] = make_double2(s[4], s[5]);
+    d.up[i] = make_double2(s[6], s[7]); d.vp[i] = make_double2(s[8], s[9]); d.ap[i] = make_double2(s[10], s[11]);
+    const double2 X = d.X0[i];
+    double2 x = make_double2(X.x + u.x, X.y + u.y);
+    if (d.b_type[lo] == MEL_BODY_RIGID) {
+        double* r = d.rg + MEL_RIGID_NF * lo;
+        const double xc = r[MEL_RG_X0] + r[MEL_RG_XD], yc = r[MEL_RG_Y0] + r[MEL_RG_YD];
+        const double dr = r[MEL_RG_RD] - r[MEL_RG_R0];
+        const double dx = X.x - r[MEL_RG_X0], dy = X.y - r[MEL_RG_Y0];
+        x.x = xc + dx * mel_cos(dr) - dy * mel_sin(dr);
+        x.y = yc + dx * mel_sin(dr) + dy * mel_cos(dr);
+        const double ddx = x.x - xc, ddy = x.y - yc;
+        v = make_double2(-ddy * r[MEL_RG_RV] + r[MEL_RG_XV], ddx * r[MEL_RG_RV] + r[MEL_RG_YV]);
+        if (i == d.b_node0[lo]) { r[MEL_RG_XC] = xc; r[MEL_RG_YC] = yc; r[MEL_RG_RC] = r[MEL_RG_R0] + r[MEL_RG_RD]; }
+    }
+    d.v[i] = v;
+    d.x[i] = x;
+}
+
+static mel_status state_stage(mel_handle* h)
+{
+    if (h->d_state) return MEL_OK;
+    if (cudaMalloc(&h->d_state, sizeof(double) * 12 * (size_t)(h->nn > 0 ? h->nn : 1)) != cudaSuccess) {
+        h->d_state = nullptr;
+        mel_set_error("node-state staging allocation failed");
+        return MEL_ERR_OOM;
+    }
+    return MEL_OK;
+}
+
+// Both directions go through one device staging array in the caller's layout: one copy of
+// 96 bytes per node each way (at full link speed when the caller's buffer is pinned), packed and
+// unpacked by a kernel.
 mel_status mel_get_node_state(mel_handle* h, double* st)
 {
     if (!h || !st) return MEL_ERR_INVALID;
     cudaSetDevice(h->device);
-    cudaStreamSynchronize(h->stream);
+    mel_status rc = state_stage(h);
+    if (rc) return rc;
     const int nn = h->nn;
-    std::vector<double> buf(2 * (size_t)nn);
-    double2* arrs[6] = { h->d.u, h->d.v, h->d.a, h->d.up, h->d.vp, h->d.ap };
-    for (int k = 0; k < 6; k++) {
-        MEL_CUDA_OK(cudaMemcpy(buf.data(), arrs[k], sizeof(double) * 2 * (size_t)nn, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < nn; i++) { st[12 * (size_t)i + 2 * k] = buf[2 * i]; st[12 * (size_t)i + 2 * k + 1] = buf[2 * i + 1]; }
+    if (nn > 0) {
+        state_pack_kernel<<<(nn + 255) / 256, 256, 0, h->stream>>>(h->d.u, h->d.v, h->d.a, h->d.up, h->d.vp, h->d.ap, nn, h->d_state);
+        MEL_CUDA_OK(cudaGetLastError());
+        MEL_CUDA_OK(cudaMemcpyAsync(st, h->d_state, sizeof(double) * 12 * (size_t)nn, cudaMemcpyDeviceToHost, h->stream));
     }
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
     return MEL_OK;
 }
 
@@ -903,8 +965,30 @@ mel_status mel_set_node_state(mel_handle* h, const double* st)
 {
     if (!h || !st) return MEL_ERR_INVALID;
     cudaSetDevice(h->device);
-    cudaStreamSynchronize(h->stream);
-    return upload_state(h, st, nullptr);
+    mel_status rc = state_stage(h);
+    if (rc) return rc;
+    const int nn = h->nn;
+    if (nn > 0) {
+        MEL_CUDA_OK(cudaMemcpyAsync(h->d_state, st, sizeof(double) * 12 * (size_t)nn, cudaMemcpyHostToDevice, h->stream));
+        state_unpack_kernel<<<(nn + 255) / 256, 256, 0, h->stream>>>(h->d, h->d_state);
+        MEL_CUDA_OK(cudaGetLastError());
+    }
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    return MEL_OK;
+}
+
+mel_status mel_pin_host(void* ptr, size_t bytes)
+{
+    if (!ptr || bytes == 0) { mel_set_error("mel_pin_host: null pointer or zero size"); return MEL_ERR_INVALID; }
+    MEL_CUDA_OK(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+    return MEL_OK;
+}
+
+mel_status mel_unpin_host(void* ptr)
+{
+    if (!ptr) { mel_set_error("mel_unpin_host: null pointer"); return MEL_ERR_INVALID; }
+    MEL_CUDA_OK(cudaHostUnregister(ptr));
+    return MEL_OK;
 }
 
 mel_status mel_set_rigid(mel_handle* h, const double* rigid)

@@ -705,9 +705,11 @@ def _bc_lines(axis: str, bc) -> List[str]:
     return out
 
 
-def write_asc(scene: Scene, directory: str) -> None:
+def write_asc(scene: Scene, directory: str, workers: int = 1) -> None:
     """Write STATIC_CONTROL.asc, STATIC_DATA.asc and DYNAMIC_00000.asc readable by Load_static /
-    Load_dynamic (Code/IO.h).  Numbers use 17 significant digits so the files round-trip."""
+    Load_dynamic (Code/IO.h).  Numbers use 17 significant digits so the files round-trip.  With
+    workers > 1 the bodies' blocks are formatted in that many forked processes (a 2000-disc
+    sample is 6 GB of text); fork only from a process that holds no CUDA context."""
     os.makedirs(directory, exist_ok=True)
     mats = scene.materials
     names = [m[0] for m in mats]
@@ -748,78 +750,150 @@ def write_asc(scene: Scene, directory: str) -> None:
     with open(os.path.join(directory, "STATIC_CONTROL.asc"), "w") as fh:
         fh.write("\n".join(L) + "\n")
 
+    parts = _write_body_parts(scene, workers)
     with open(os.path.join(directory, "STATIC_DATA.asc"), "w") as fh:
-        w = fh.write
-        w(" \nSIMULATION_NAME\n%s\n \n \nNUMBER_BODIES\n%d\n \n \n" % (scene.name, len(scene.bodies)))
-        for bi, b in enumerate(scene.bodies):
-            n = b.nodes.shape[0]
-            if b.kind == "deformable":
-                w(" \nDEFORMABLE\n%d\n \nNODES\n%d\n \n" % (bi, n))
-                inv = 1.0 / b.mass
-                for i in range(n):
-                    w("%d %s %s %s %s %s %s %s\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1]), _g(b.domain[i]),
-                                                     _g(b.mass[i, 0]), _g(b.mass[i, 1]), _g(inv[i, 0]), _g(inv[i, 1])))
-            else:
-                w(" \nRIGID\n%d\n%s %s\n%s %s %s %s\n \nNODES\n%d\n \n" % (
-                    bi, _g(b.centre[0]), _g(b.centre[1]), _g(b.rigid_mass), _g(b.rigid_inertia),
-                    _g(1.0 / b.rigid_mass), _g(1.0 / b.rigid_inertia), n))
-                for i in range(n):
-                    w("%d %s %s\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1])))
-            w(" \nBORDERS\n%d\n \n" % len(b.borders))
-            for br in b.borders:
-                w("%s %s\n%d %d %d\n" % (per[br["periodicity"]], itp[br["interpolant"]], len(br["nodes"]),
-                                        br["before"], br["after"]))
-                w("".join("%d\n" % k for k in br["nodes"]))
-                w(" \n")
-            if b.kind == "deformable":
-                ptr, idx, Nv, dx, dy = b.gp
-                w("INTEGRATION\nGauss\n%d %d\n \n" % (ptr.shape[0] - 1, b.n_regions))
-                for g in range(ptr.shape[0] - 1):
-                    w("Gauss Point %d\n%s %s %s %s\n%d\n" % (g, _g(b.gp_xy[g, 0]), _g(b.gp_xy[g, 1]),
-                                                            _g(b.gp_w[g]), _g(b.gp_J[g]), ptr[g + 1] - ptr[g]))
-                    for e in range(ptr[g], ptr[g + 1]):
-                        k = idx[e]
-                        w("%d %d %d %s %s %s\n" % (k, 2 * k, 2 * k + 1, _g(Nv[e]), _g(dx[e]), _g(dy[e])))
-                    w(" \n")
-            w("TRIANGULATION\n%d\n" % b.cells.shape[0])
-            for c, t in enumerate(b.cells):
-                w("%d %d %d %d\n" % (c, t[0], t[1], t[2]))
-            w(" \n")
-            if b.kind == "deformable":
-                ptr, idx, Nv, dx, dy = b.sup
-                w("DOF_TO_DISP\n")
-                for i in range(n):
-                    w(" \nNODE %d\n%d\n" % (i, ptr[i + 1] - ptr[i]))
-                    for e in range(ptr[i], ptr[i + 1]):
-                        w("%d %s %s %s\n" % (idx[e], _g(Nv[e]), _g(dx[e]), _g(dy[e])))
-                w(" \n \nMATRICES\n0\n \n \n \n \n")
-
+        fh.write(" \nSIMULATION_NAME\n%s\n \n \nNUMBER_BODIES\n%d\n \n \n" % (scene.name, len(scene.bodies)))
+        for text in _collect(parts, 0):
+            fh.write(text)
     with open(os.path.join(directory, "DYNAMIC_00000.asc"), "w") as fh:
-        w = fh.write
         tend = scene.dt * scene.nsteps
-        w(" \nSIMULATION_NAME\n%s\n \nSOLVER\n%s\n0 0 0 0 \n%s\n%s %s %s \nNO_LOG\n" % (
+        fh.write(" \nSIMULATION_NAME\n%s\n \nSOLVER\n%s\n0 0 0 0 \n%s\n%s %s %s \nNO_LOG\n" % (
             scene.name, SOLVER_NAMES[scene.solver], _g(scene.dt), _g(tend), _g(tend), _g(0.0)))
         if not scene.self_contact:
-            w("NO_MONITORING\n")
+            fh.write("NO_MONITORING\n")
         if scene.initialize_czm:
-            w("INITIALIZE_CZM\n")
+            fh.write("INITIALIZE_CZM\n")
+        fh.write(" \n")
+        for text in _collect(parts, 1):
+            fh.write(text)
+    for part in parts:
+        if part[0] is not None:
+            for path in part:
+                os.unlink(path)
+            tmp = os.path.dirname(part[0])
+    if parts and parts[0][0] is not None:
+        os.rmdir(tmp)
+
+
+def _static_data_body(bi: int, b: Body) -> str:
+    """The block of body bi in STATIC_DATA.asc (Preprocessor/ExportStatic.m layout)."""
+    out: List[str] = []
+    w = out.append
+    n = b.nodes.shape[0]
+    per = ["Closed", "Simple", "Periodic"]
+    itp = ["Linear", "Spline"]
+    if b.kind == "deformable":
+        w(" \nDEFORMABLE\n%d\n \nNODES\n%d\n \n" % (bi, n))
+        inv = 1.0 / b.mass
+        for i in range(n):
+            w("%d %s %s %s %s %s %s %s\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1]), _g(b.domain[i]),
+                                             _g(b.mass[i, 0]), _g(b.mass[i, 1]), _g(inv[i, 0]), _g(inv[i, 1])))
+    else:
+        w(" \nRIGID\n%d\n%s %s\n%s %s %s %s\n \nNODES\n%d\n \n" % (
+            bi, _g(b.centre[0]), _g(b.centre[1]), _g(b.rigid_mass), _g(b.rigid_inertia),
+            _g(1.0 / b.rigid_mass), _g(1.0 / b.rigid_inertia), n))
+        for i in range(n):
+            w("%d %s %s\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1])))
+    w(" \nBORDERS\n%d\n \n" % len(b.borders))
+    for br in b.borders:
+        w("%s %s\n%d %d %d\n" % (per[br["periodicity"]], itp[br["interpolant"]], len(br["nodes"]),
+                                  br["before"], br["after"]))
+        w("".join("%d\n" % k for k in br["nodes"]))
         w(" \n")
-        for bi, b in enumerate(scene.bodies):
-            n = b.nodes.shape[0]
-            vx, vy = b.velocity
-            if b.kind == "deformable":
-                w(" \nDEFORMABLE\nactive\n%d\n \nKINEMATICS\n%d\n" % (bi, n))
-                for i in range(n):
-                    w("%d %s %s 0 0 %s %s 0 0 0 0 %s %s 0 0\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1]),
-                                                                _g(vx), _g(vy), _g(vx), _g(vy)))
-                w(" \nFORCES\n")
-                for i in range(n):
-                    w("%d 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0\n" % i)
-                w(" \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
-            else:
-                w(" \nRIGID\nactive\n%d\n \nKINEMATICS\n%s %s 0\n0 0 0\n%s %s %s\n \n" % (
-                    bi, _g(b.centre[0]), _g(b.centre[1]), _g(vx), _g(vy), _g(b.angular_velocity)))
-                w("FORCES\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
+    if b.kind == "deformable":
+        ptr, idx, Nv, dx, dy = b.gp
+        w("INTEGRATION\nGauss\n%d %d\n \n" % (ptr.shape[0] - 1, b.n_regions))
+        for g in range(ptr.shape[0] - 1):
+            w("Gauss Point %d\n%s %s %s %s\n%d\n" % (g, _g(b.gp_xy[g, 0]), _g(b.gp_xy[g, 1]),
+                                                      _g(b.gp_w[g]), _g(b.gp_J[g]), ptr[g + 1] - ptr[g]))
+            for e in range(ptr[g], ptr[g + 1]):
+                k = idx[e]
+                w("%d %d %d %s %s %s\n" % (k, 2 * k, 2 * k + 1, _g(Nv[e]), _g(dx[e]), _g(dy[e])))
+            w(" \n")
+    w("TRIANGULATION\n%d\n" % b.cells.shape[0])
+    for c, t in enumerate(b.cells):
+        w("%d %d %d %d\n" % (c, t[0], t[1], t[2]))
+    w(" \n")
+    if b.kind == "deformable":
+        ptr, idx, Nv, dx, dy = b.sup
+        w("DOF_TO_DISP\n")
+        for i in range(n):
+            w(" \nNODE %d\n%d\n" % (i, ptr[i + 1] - ptr[i]))
+            for e in range(ptr[i], ptr[i + 1]):
+                w("%d %s %s %s\n" % (idx[e], _g(Nv[e]), _g(dx[e]), _g(dy[e])))
+        w(" \n \nMATRICES\n0\n \n \n \n \n")
+    return "".join(out)
+
+
+def _dynamic_body(bi: int, b: Body) -> str:
+    """The block of body bi in DYNAMIC_00000.asc (Preprocessor/ExportDynamic.m layout)."""
+    out: List[str] = []
+    w = out.append
+    n = b.nodes.shape[0]
+    vx, vy = b.velocity
+    if b.kind == "deformable":
+        w(" \nDEFORMABLE\nactive\n%d\n \nKINEMATICS\n%d\n" % (bi, n))
+        for i in range(n):
+            w("%d %s %s 0 0 %s %s 0 0 0 0 %s %s 0 0\n" % (i, _g(b.nodes[i, 0]), _g(b.nodes[i, 1]),
+                                                        _g(vx), _g(vy), _g(vx), _g(vy)))
+        w(" \nFORCES\n")
+        for i in range(n):
+            w("%d 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0\n" % i)
+        w(" \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
+    else:
+        w(" \nRIGID\nactive\n%d\n \nKINEMATICS\n%s %s 0\n0 0 0\n%s %s %s\n \n" % (
+            bi, _g(b.centre[0]), _g(b.centre[1]), _g(vx), _g(vy), _g(b.angular_velocity)))
+        w("FORCES\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n0 0 0\n \nNEIGHBOURS\n0\n \nCONTACTS\n0\n \n")
+    return "".join(out)
+
+
+_WRITE_SCENE: Optional[Scene] = None
+
+
+def _write_range(job):
+    """Worker: the STATIC_DATA and DYNAMIC blocks of bodies [b0, b1) into two temporary files."""
+    b0, b1, tmpdir = job
+    paths = []
+    for k, fn in enumerate((_static_data_body, _dynamic_body)):
+        path = os.path.join(tmpdir, "part%07d_%d.asc" % (b0, k))
+        with open(path, "w") as fh:
+            for bi in range(b0, b1):
+                fh.write(fn(bi, _WRITE_SCENE.bodies[bi]))
+        paths.append(path)
+    return tuple(paths)
+
+
+def _write_body_parts(scene: Scene, workers: int):
+    """Per-body text of both files: in this process (a list of string pairs), or, with workers > 1,
+    in forked workers that each write a range of bodies to temporary files (a list of path pairs)."""
+    global _WRITE_SCENE
+    nb = len(scene.bodies)
+    if workers <= 1 or nb < 2 * workers:
+        return [(None, _static_data_body(bi, b), _dynamic_body(bi, b)) for bi, b in enumerate(scene.bodies)]
+    import multiprocessing as mp
+    import tempfile
+    tmpdir = tempfile.mkdtemp(prefix="melasc")
+    step = (nb + 4 * workers - 1) // (4 * workers)
+    jobs = [(b0, min(nb, b0 + step), tmpdir) for b0 in range(0, nb, step)]
+    _WRITE_SCENE = scene
+    try:
+        with mp.get_context("fork").Pool(workers) as pool:
+            return list(pool.map(_write_range, jobs))
+    finally:
+        _WRITE_SCENE = None
+
+
+def _collect(parts, k):
+    for part in parts:
+        if part[0] is None:
+            yield part[1 + k]
+        else:
+            with open(part[k]) as fh:
+                while True:
+                    chunk = fh.read(1 << 24)
+                    if not chunk:
+                        break
+                    yield chunk
 
 
 # --------------------------------------------------------------------------------------------

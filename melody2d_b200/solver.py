@@ -33,6 +33,8 @@ SIGNATURES = {
     "mel_set_contacts": [_vp, C.POINTER(abi.MelContact), C.c_int],
     "mel_get_node_state": [_vp, _dp],
     "mel_set_node_state": [_vp, _dp],
+    "mel_pin_host": [_vp, C.c_size_t],
+    "mel_unpin_host": [_vp],
     "mel_get_positions": [_vp, _dp],
     "mel_get_forces": [_vp, _dp, _dp, _dp, _dp, _dp],
     "mel_get_rigid": [_vp, _dp, _dp],
@@ -62,6 +64,27 @@ SIGNATURES = {
     "mel_batch_destroy": [_vp],
     "mel_get_health": [_vp, _ip],
 }
+
+
+class PinnedArray:
+    """A float64 numpy array page-locked with mel_pin_host for fast state transfers (released by
+    close())."""
+
+    def __init__(self, shape):
+        self.array = np.zeros(shape, dtype=np.float64)
+        _check(lib().mel_pin_host(self.array.ctypes.data, self.array.nbytes))
+        self._pinned = True
+
+    def close(self):
+        if self._pinned:
+            lib().mel_unpin_host(self.array.ctypes.data)
+            self._pinned = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class MelError(RuntimeError):

@@ -45,7 +45,7 @@ extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const dou
             buf.assign(CS.img.begin() + c.img, CS.img.begin() + c.img + c.bytes);
             int hdr[4];
             memcpy(hdr, buf.data(), sizeof hdr);
-            if (hdr[0] > MEL_CHUNK_GP || hdr[1] % 8 || hdr[1] > ecap || hdr[3] > 1024) return 2;
+            if (hdr[0] > MEL_CHUNK_GP_FP64 || hdr[1] % 8 || hdr[1] > ecap || hdr[3] > 1024) return 2;
             const mel_chunk_layout L = mel_chunk_sections(hdr[0], hdr[1], hdr[2], hdr[3], 16);
             if (L.bytes != c.bytes) return 3;
             double* sp = reinterpret_cast<double*>(buf.data() + L.dN);

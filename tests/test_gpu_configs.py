@@ -38,8 +38,14 @@ def key_sets(c):
 
 
 def monitored(m, nrigid):
-    return np.array([m.kinetic_energy, *m.mean_displacement, *list(m.rigid_force)[:2 * nrigid],
-                     *list(m.rigid_dirichlet)[:2 * nrigid], m.active_contacts], dtype=np.float64)
+    """Rigid-body forces and reactions (copied, not reduced) and the active-contact count."""
+    return np.array([*list(m.rigid_force)[:2 * nrigid], *list(m.rigid_dirichlet)[:2 * nrigid], m.active_contacts],
+                    dtype=np.float64)
+
+
+# Kinetic energy and mean displacement are sums over all nodes: the device adds them in a tree of
+# block partials, the oracle serially, so from bit-identical node states they agree to rounding.
+TOL_SUM = 1e-12
 
 
 def rel(a, b):
@@ -70,8 +76,10 @@ class Trio:
         g, c, r = self.gpu, self.cr, self.ref
         # bit-identical to the correctly-rounded oracle
         np.testing.assert_array_equal(g.node_state(), c.node_state(), err_msg=label)
-        np.testing.assert_array_equal(monitored(g.monitor(), self.nrigid), monitored(c.monitor(), self.nrigid),
-                                      err_msg=label)
+        mgc, mcc = g.monitor(), c.monitor()
+        np.testing.assert_array_equal(monitored(mgc, self.nrigid), monitored(mcc, self.nrigid), err_msg=label)
+        assert rel(mgc.kinetic_energy, mcc.kinetic_energy) <= TOL_SUM, label
+        assert rel(list(mgc.mean_displacement), list(mcc.mean_displacement)) <= TOL_SUM, label
         if full:
             assert_contacts_equal(g.contacts(), c.contacts())
             np.testing.assert_array_equal(g.rigid()[0], c.rigid()[0], err_msg=label)
