@@ -48,7 +48,7 @@ def test_reference_arm_under_torchrun(oracle_built):
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
            "--impl", "reference", "--gpus", "2", "--steps", "5", "--warmup", "3",
-           "--ref-discs", "4", "--ref-steps", "5"]
+           "--discs", "4", "--ref-arm-steps", "5"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]

@@ -41,7 +41,15 @@ LAW_PARAMS = {
 
 CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7+czm", "neohookean",
                                                     "border_conditions", "biaxial12_s5", "biaxial12_s7",
-                                                    "periodic", "rotor"]
+                                                    "periodic", "rotor", "adaptive_euler", "euler_2",
+                                                    "mass_scaling", "adaptive_mass_scaling"]
+
+# Solver_step schemes (Code/Solver.h:98-486) with their parameters: Target_error, Control_parameter,
+# Accepted_ratio, Max_mass_scaling, Control_parameter_mass_scaling, Error_factor_mass_scaling,
+# Decrease_factor_mass_scaling (Code/IO.h:821-893)
+SOLVER_CASES = {"adaptive_euler": (1, (2e-3, 0.2, 0.9)), "euler_2": (4, (2e-3, 0.2, 0.9)),
+                "mass_scaling": (2, (2e-3, 0.2, 0.9, 50.0, 1.0, 0.5, 0.99)),
+                "adaptive_mass_scaling": (3, (2e-3, 0.2, 1.0, 50.0, 1.0, 0.5, 0.99))}
 
 
 def case_scene(name):
@@ -59,6 +67,12 @@ def case_scene(name):
         law = int(name[3])
         sc.laws = [(m1, m2, law, 0, list(LAW_PARAMS[law])) for (m1, m2, _, _, _) in sc.laws]
         sc.initialize_czm = name.endswith("+czm")
+    elif name in SOLVER_CASES:
+        solver, prm = SOLVER_CASES[name]
+        sc.solver = solver
+        sp = list(sc.solver_params)
+        sp[:len(prm)] = prm
+        sc.solver_params = tuple(sp)
     elif name == "neohookean":
         sc.materials = [(n, 1 if n == "Grain" else t, p) for (n, t, p) in sc.materials]
     elif name == "border_conditions":
