@@ -231,6 +231,13 @@ mel_status mel_get_rigid(mel_handle* h, double* rigid /* [n_bodies*MEL_RIGID_NF]
 /* works per body [n_bodies*7]: internal, contact, body, dirichlet, neumann, damping, alid (Body.h:111-117) */
 mel_status mel_get_works(mel_handle* h, double* works);
 mel_status mel_get_contact_count(mel_handle* h, int* n);
+/* Border contact pressures of the last step, x and y, one per border entry in the order of the
+ * border node lists (Update_contact_pressures, Code/Proximity.h:1014-1069, which the reference runs
+ * at the end of every accepted step; Border::x_contact_pressure, y_contact_pressure).  They are
+ * computed when first asked for after a step, or before the proximity update that would replace
+ * the contact list they come from; a batch member keeps them across such updates only with
+ * mel_record_forces on. */
+mel_status mel_get_contact_pressures(mel_handle* h, double* px, double* py);
 mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* n);
 mel_status mel_get_time(mel_handle* h, double* time, double* dt);
 

@@ -27,7 +27,8 @@
 
 // device error words (mel_dev::err)
 enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3, MEL_E_CAPACITY = 4,
-       MEL_E_NBR_NEED = 5, MEL_E_WAIT = 6, MEL_E_NWORDS = 8 };
+       MEL_E_NBR_NEED = 5, MEL_E_WAIT = 6, MEL_E_PRESSURE = 7, MEL_E_NWORDS = 8 };
+#define MEL_PRESSURE_CAP 32       // contact contributions one border entry's pressure gathers
 
 // Chunk image (all offsets in bytes from the image start, every section 16-byte aligned):
 //   header   int4 {ngp, ne, ntn, nroff}
@@ -130,6 +131,10 @@ struct mel_dev {
     const int* b_cont0;                       // [nb+1] slave contact ranges (list is body-major)
     const int* b_inc0;                        // [nb+1] into inc_rng
     const int2* inc_rng;                      // incoming (master-side) contact ranges in send order
+    // border contact pressures (Update_contact_pressures): per border entry, the contributions
+    // gathered (contact << 2 | role, at most MEL_PRESSURE_CAP) and the pressures
+    int* cp_cnt; int* cp_item;
+    double *cpx, *cpy;
     // error words
     unsigned int* err;
 };
@@ -146,6 +151,8 @@ void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const
 size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed);
 void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);
+// Update_contact_pressures (Code/Proximity.h:1014-1069) from the current contact list
+void mel_launch_contact_pressures(const mel_dev& d, cudaStream_t s);
 
 int mel_body_kernel_configure(size_t smem);
 

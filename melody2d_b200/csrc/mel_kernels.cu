@@ -1270,7 +1270,77 @@ __global__ void monitor_final_kernel(mel_dev d, const double* part, const int* r
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// Update_contact_pressures (Code/Proximity.h:1014-1069): every contact adds f / length to its
+// slave border entry and subtracts f / length * shapeM1 (shapeM2) from the master entries at the
+// ends of its segment.  The reference adds them in list order, contact by contact (slave, then
+// the two master entries), so each border entry gathers its contributions, sorts them by
+// (contact, role) and adds them in that order.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void pressure_push(const mel_dev& d, int e, int v)
+{
+    if (e < 0 || e >= d.ne) { set_err(d, MEL_E_BOUNDS); return; }
+    const int slot = atomicAdd(&d.cp_cnt[e], 1);
+    if (slot < MEL_PRESSURE_CAP) d.cp_item[(size_t)e * MEL_PRESSURE_CAP + slot] = v;
+    else set_err(d, MEL_E_PRESSURE);
+}
+
+__global__ void pressure_clear_kernel(mel_dev d)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < d.ne) d.cp_cnt[e] = 0;
+}
+
+__global__ void pressure_push_kernel(mel_dev d)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.ncont) return;
+    const mel_contact& k = d.cont[c];
+    if (k.bodyS < 0 || k.bodyS >= d.nb || k.bodyM < 0 || k.bodyM >= d.nb) { set_err(d, MEL_E_BOUNDS); return; }
+    const int eS = d.bd_e0[d.b_bd0[k.bodyS] + k.borderS] + k.border_nodeS;
+    const int eM = d.bd_e0[d.b_bd0[k.bodyM] + k.borderM] + k.segmentM;
+    pressure_push(d, eS, c << 2);
+    pressure_push(d, eM, (c << 2) | 1);
+    pressure_push(d, eM + 1, (c << 2) | 2);
+}
+
+__global__ void pressure_sum_kernel(mel_dev d)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d.ne) return;
+    const int n = min(d.cp_cnt[e], MEL_PRESSURE_CAP);
+    int v[MEL_PRESSURE_CAP];
+    for (int i = 0; i < n; i++) {                         // insertion sort: a handful of items
+        const int x = d.cp_item[(size_t)e * MEL_PRESSURE_CAP + i];
+        int j = i;
+        while (j > 0 && v[j - 1] > x) { v[j] = v[j - 1]; j--; }
+        v[j] = x;
+    }
+    double px = 0., py = 0.;
+    for (int i = 0; i < n; i++) {
+        const mel_contact& k = d.cont[v[i] >> 2];
+        const int role = v[i] & 3;
+        const double il = 1. / k.length;
+        if (role == 0) { px += k.fx * il; py += k.fy * il; }
+        else {
+            const double sh = k.shapeM[role];
+            px -= k.fx * il * sh;
+            py -= k.fy * il * sh;
+        }
+    }
+    d.cpx[e] = px;
+    d.cpy[e] = py;
+}
+
 } // namespace mel
+
+void mel_launch_contact_pressures(const mel_dev& d, cudaStream_t s)
+{
+    if (d.ne <= 0) return;
+    mel::pressure_clear_kernel<<<(d.ne + 255) / 256, 256, 0, s>>>(d);
+    if (d.ncont > 0) mel::pressure_push_kernel<<<(d.ncont + 127) / 128, 128, 0, s>>>(d);
+    mel::pressure_sum_kernel<<<(d.ne + 127) / 128, 128, 0, s>>>(d);
+}
 
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s)
 {

@@ -75,6 +75,10 @@ struct mel_handle {
     double* d_monitor = nullptr;
     double* d_monitor_part = nullptr;
     double* d_state = nullptr;   // node state in the 12-doubles-per-node layout (mel_get/set_node_state)
+    // border contact pressures: 0 = up to date, 1 = the last step's, still computable from the
+    // current contact list, 2 = that list was replaced by a proximity update since (batch member
+    // without recording)
+    int pressure_state = 0;
     int* d_rigid_ids = nullptr;
     int nrigid = 0;
     int precision = MEL_PREC_FP64;
@@ -415,6 +419,10 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.e_len0 = dupload(h, len0);
     std::vector<double> len(len0);
     D.e_len = dupload(h, len);
+    D.cp_cnt = dalloc<int>(h, (size_t)ne + 1);
+    D.cp_item = dalloc<int>(h, (size_t)(ne > 0 ? ne : 1) * MEL_PRESSURE_CAP);
+    D.cpx = dalloc<double>(h, (size_t)ne + 1);
+    D.cpy = dalloc<double>(h, (size_t)ne + 1);
     {
         std::vector<int> blk0(nbd + 1, 0), blk_border;
         for (int g = 0; g < nbd; g++) {
@@ -584,6 +592,7 @@ static mel_status check_errors(mel_handle* h)
     if (cudaMemcpy(w, h->d.err, sizeof w, cudaMemcpyDeviceToHost) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "err", __FILE__, __LINE__); return MEL_ERR_CUDA; }
     if (w[MEL_E_BOUNDS]) { mel_set_error("device index check failed (code %u)", w[MEL_E_BOUNDS]); return MEL_ERR_BOUNDS; }
     if (w[MEL_E_WAIT]) { mel_set_error("a shared-memory bulk copy did not complete within %llu ns", MEL_WAIT_NS); return MEL_ERR_TIMEOUT; }
+    if (w[MEL_E_PRESSURE]) { mel_set_error("a border entry gathers more than %d contact contributions to its pressure", MEL_PRESSURE_CAP); return MEL_ERR_BOUNDS; }
     return MEL_OK;
 }
 
@@ -680,6 +689,15 @@ static mel_status upload_state(mel_handle* h, const double* st, const double* ri
     MEL_CUDA_OK(cudaMemcpy(h->d.x, x.data(), bytes, cudaMemcpyHostToDevice));
     MEL_CUDA_OK(cudaMemcpy(h->d.rg, rg.data(), sizeof(double) * rg.size(), cudaMemcpyHostToDevice));
     return MEL_OK;
+}
+
+// Update_contact_pressures on the handle's stream, if the last step's pressures are not computed yet
+static void update_pressures(mel_handle* h)
+{
+    if (h->pressure_state != 1) return;
+    mel_launch_contact_pressures(h->d, h->stream);
+    h->launches += 3;
+    h->pressure_state = 0;
 }
 
 extern "C" {
@@ -797,8 +815,10 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
         h->launches += 2;
         h->parity ^= 1;
         h->time += h->dt;                       // Code/Solver.h:86
+        h->pressure_state = 1;                  // Update_contact_pressures ends the step (Code/Solver.h:87)
         if (io->run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
             h->next_cup = h->next_cup + h->cup;
+            update_pressures(h);                // from the list the step ended with
             cudaEvent_t p0 = nullptr, p1 = nullptr;
             if (h->timing) { p0 = h->ev_pool[nev++]; p1 = h->ev_pool[nev++]; pev.push_back({ p0, p1 }); }
             mel_status rc = proximity(h, p0, p1);
@@ -1071,6 +1091,24 @@ mel_status mel_get_works(mel_handle* h, double* works)
     cudaStreamSynchronize(h->stream);
     MEL_CUDA_OK(cudaMemcpy(works, h->d.works, sizeof(double) * 7 * (size_t)h->nb, cudaMemcpyDeviceToHost));
     return MEL_OK;
+}
+
+mel_status mel_get_contact_pressures(mel_handle* h, double* px, double* py)
+{
+    if (!h || (!px && !py)) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    if (h->pressure_state == 2) {
+        mel_set_error("the contact list changed since the last step: a batch member keeps its contact pressures only "
+                      "with mel_record_forces on");
+        return MEL_ERR_INVALID;
+    }
+    update_pressures(h);
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    if (h->ne > 0) {
+        if (px) MEL_CUDA_OK(cudaMemcpy(px, h->d.cpx, sizeof(double) * (size_t)h->ne, cudaMemcpyDeviceToHost));
+        if (py) MEL_CUDA_OK(cudaMemcpy(py, h->d.cpy, sizeof(double) * (size_t)h->ne, cudaMemcpyDeviceToHost));
+    }
+    return check_errors(h);
 }
 
 mel_status mel_get_contact_count(mel_handle* h, int* n)
@@ -1433,9 +1471,12 @@ mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity)
         std::vector<mel_handle*> due;
         for (mel_handle* h : b->members) {
             h->time += h->dt;                                    // Code/Solver.h:86
+            h->pressure_state = 1;
             if (run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
                 h->next_cup = h->next_cup + h->cup;
                 due.push_back(h);
+                if (h->d.record_forces) { mel_launch_contact_pressures(h->d, b->stream); b->launches += 3; h->pressure_state = 0; }
+                else h->pressure_state = 2;
             }
         }
         if (!due.empty()) {

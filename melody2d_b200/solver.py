@@ -40,6 +40,7 @@ SIGNATURES = {
     "mel_get_rigid": [_vp, _dp, _dp],
     "mel_get_works": [_vp, _dp],
     "mel_get_contact_count": [_vp, _ip],
+    "mel_get_contact_pressures": [_vp, _dp, _dp],
     "mel_get_contacts": [_vp, C.POINTER(abi.MelContact), C.c_int, _ip],
     "mel_get_time": [_vp, _dp, _dp],
     "mel_checkpoint_start": [_vp],
@@ -224,6 +225,13 @@ class Solver:
         buf = (abi.MelContact * max(1, n.value))()
         _check(lib().mel_get_contacts(self.h, buf, n.value, C.byref(n)))
         return abi.contacts_to_numpy(buf, n.value)
+
+    def contact_pressures(self) -> np.ndarray:
+        """(n_border_nodes, 2): x and y contact pressure of every border entry after the last step."""
+        ne = self.sizes()["n_border_nodes"]
+        px, py = np.zeros(max(ne, 1)), np.zeros(max(ne, 1))
+        _check(lib().mel_get_contact_pressures(self.h, _ptr(px), _ptr(py)))
+        return np.stack([px[:ne], py[:ne]], axis=1)
 
     def set_contacts(self, arr: np.ndarray):
         buf = abi.numpy_to_contacts(arr)

@@ -1867,6 +1867,12 @@ double orc_time(orc_model* m) { return m->time; }
 double orc_dt(orc_model* m) { return m->dt; }
 long orc_stale_shape_events(orc_model* m) { return m->stale; }
 void orc_solver_stats(orc_model* m, double* o) { memcpy(o, m->stats, sizeof m->stats); }
+void orc_get_contact_pressures(orc_model* m, double* px, double* py)
+{
+    int ne = m->bd_ptr[m->nbd];
+    memcpy(px, m->cpx, sizeof(double) * ne);
+    memcpy(py, m->cpy, sizeof(double) * ne);
+}
 
 int orc_n_contacts(orc_model* m) { int n = 0; for (int b = 0; b < m->nb; b++) n += m->cont[b].n; return n; }
 int orc_get_contacts(orc_model* m, mel_contact* out, int cap)

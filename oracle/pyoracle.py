@@ -46,6 +46,7 @@ def lib():
         L.orc_get_neighbours.argtypes = [vp, C.POINTER(C.c_int), C.c_int]
         L.orc_stale_shape_events.argtypes = [vp]; L.orc_stale_shape_events.restype = C.c_long
         L.orc_solver_stats.argtypes = [vp, C.POINTER(C.c_double)]
+        L.orc_get_contact_pressures.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_set_rsqrt_mode.argtypes = [C.c_int]
         _lib = L
     return _lib
@@ -164,6 +165,13 @@ class Oracle:
         m = abi.MelMonitor()
         self.L.orc_monitor(self.h, C.byref(m))
         return m
+
+    def contact_pressures(self) -> np.ndarray:
+        """(n_border_nodes, 2): x and y contact pressure of every border entry."""
+        ne = int(np.asarray(self.flat["border_node_ptr"])[-1])
+        px, py = np.zeros(max(ne, 1)), np.zeros(max(ne, 1))
+        self.L.orc_get_contact_pressures(self.h, _dp(px), _dp(py))
+        return np.stack([px[:ne], py[:ne]], axis=1)
 
     def stale_shape_events(self) -> int:
         return self.L.orc_stale_shape_events(self.h)

@@ -31,7 +31,9 @@ from test_oracle_laws import CASES, STEPS, case_scene, summary  # noqa: E402
 
 def record_summary(r):
     node = {k: r.node_field(k) for k in ("x", "up", "f_int", "f_contact")}
-    return summary(node, r.contacts(), np.array([b.works for b in r.bodies]))
+    px = np.concatenate([p for b in r.bodies for p in b.border_px])
+    py = np.concatenate([p for b in r.bodies for p in b.border_py])
+    return summary(node, r.contacts(), np.array([b.works for b in r.bodies]), np.stack([px, py], axis=1))
 
 
 def main():

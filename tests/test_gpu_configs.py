@@ -84,6 +84,7 @@ class Trio:
             assert_contacts_equal(g.contacts(), c.contacts())
             np.testing.assert_array_equal(g.rigid()[0], c.rigid()[0], err_msg=label)
             np.testing.assert_array_equal(g.works(), c.works(), err_msg=label)
+            np.testing.assert_array_equal(g.contact_pressures(), c.contact_pressures(), err_msg=label)
         # within TOL_REF of the reference's arithmetic, same candidate and active sets
         mg, mr = g.monitor(), r.monitor()
         d = {"kinetic_energy": rel(mg.kinetic_energy, mr.kinetic_energy),

@@ -94,9 +94,12 @@ CONTACT_KEYS = ["bodyS", "borderS", "border_nodeS", "nodeS", "bodyM", "borderM",
                 "internal0", "internal1", "internal2"]
 
 
-def summary(node, contacts, works):
-    """Digests of one state: node fields (name -> (n, 2) array), contacts (key -> column), works."""
+def summary(node, contacts, works, pressures=None):
+    """Digests of one state: node fields (name -> (n, 2) array), contacts (key -> column), works,
+    border contact pressures ((n_border_nodes, 2): x, y)."""
     out = {"node_" + k: sha(v) for k, v in node.items()}
+    if pressures is not None:
+        out["contact_pressures"] = sha(pressures)
     out["n_contacts"] = int(len(contacts["fx"]))
     for k in CONTACT_KEYS:
         out["contact_" + k] = sha(contacts[k])
@@ -119,7 +122,7 @@ def oracle_summary(o):
     st = o.node_state()
     f = o.forces()
     node = {"x": o.positions(), "up": st[:, 6:8], "f_int": f["internal"], "f_contact": f["contact"]}
-    return summary(node, oracle_columns(o.contacts()), o.works())
+    return summary(node, oracle_columns(o.contacts()), o.works(), o.contact_pressures())
 
 
 @pytest.mark.parametrize("case", CASES)
