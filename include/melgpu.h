@@ -203,8 +203,10 @@ mel_status mel_create_from_files(const char* dir, int restart_index, const mel_o
 mel_status mel_destroy(mel_handle* h);
 
 /* ---- stepping --------------------------------------------------------------------- */
-/* io->nsteps iterations of the loop body of Code/main.cpp:141-238 restricted to the solver
- * (Euler_step, Code/Solver.h:10-88) and the proximity update (Code/main.cpp:191-196). */
+/* io->nsteps iterations of the loop body of Code/main.cpp:141-238 restricted to the solver and the
+ * proximity update (Code/main.cpp:191-196): Euler_step (Code/Solver.h:10-88) for MEL_SOLVER_EULER,
+ * Solver_step (Code/Solver.h:98-486: two half-steps, error estimate, mass scaling, accept / reject
+ * with Deltat control) for the other schemes; io->nsteps counts accepted steps. */
 mel_status mel_step(mel_handle* h, mel_step_io* io);
 /* Update_proximity (Code/Proximity.h:48-473) on the current positions. */
 mel_status mel_update_proximity(mel_handle* h);
@@ -231,6 +233,9 @@ mel_status mel_get_rigid(mel_handle* h, double* rigid /* [n_bodies*MEL_RIGID_NF]
 /* works per body [n_bodies*7]: internal, contact, body, dirichlet, neumann, damping, alid (Body.h:111-117) */
 mel_status mel_get_works(mel_handle* h, double* works);
 mel_status mel_get_contact_count(mel_handle* h, int* n);
+/* Solver_step statistics of the last accepted step (Code/Solver.h:98-486): attempts (neval),
+ * max_error, mean_error, total_mass, max_mass; zeros under the Euler scheme. */
+mel_status mel_get_solver_stats(mel_handle* h, double* out5);
 /* Border contact pressures of the last step, x and y, one per border entry in the order of the
  * border node lists (Update_contact_pressures, Code/Proximity.h:1014-1069, which the reference runs
  * at the end of every accepted step; Border::x_contact_pressure, y_contact_pressure).  They are

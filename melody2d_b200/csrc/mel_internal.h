@@ -131,6 +131,17 @@ struct mel_dev {
     const int* b_cont0;                       // [nb+1] slave contact ranges (list is body-major)
     const int* b_inc0;                        // [nb+1] into inc_rng
     const int2* inc_rng;                      // incoming (master-side) contact ranges in send order
+    // Solver_step (Code/Solver.h:98-486): phase of an adaptive launch (1: first half-step, 2: second
+    // half-step), scheme and its parameters (mel_model_desc::solver_params), inverse distance
+    // estimators of the nodes (Code/IO.h:1620,1819), temporary displacement parameters and
+    // displacements, nodal errors, nodal mass-scaling factors; per body: total and largest error,
+    // scaled mass, rigid mass-scaling factor and its last increment, rigid temporary kinematics
+    // (x, y, r displacement then velocity)
+    int phase, solver;
+    double sp[8];
+    const double* ide;
+    double2 *upt, *ut, *errv, *fms;
+    double *terr, *merr, *bmms, *bfms, *bdfms, *rg_tmp;
     // border contact pressures (Update_contact_pressures): per border entry, the contributions
     // gathered (contact << 2 | role, at most MEL_PRESSURE_CAP) and the pressures
     int* cp_cnt; int* cp_item;
@@ -144,6 +155,13 @@ void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 // Initialize_CZM's pass over the contact list (contact geometry, then the initial bonds)
 void mel_launch_czm_init(const mel_dev& d, cudaStream_t s);
 void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s);
+// one half-step of Solver_step (d.phase 1 or 2): T0 = Time, Tf = the time the forces see
+void mel_launch_body_adaptive(const mel_dev& d, double T0, double Tf, int nblocks, size_t smem, cudaStream_t s);
+// Solver_step's error and mass sums over the bodies in order (Code/Solver.h:289-331): out =
+// {mean_error, max_error, total_mass, max_mass}
+void mel_launch_error_reduce(const mel_dev& d, double* out, cudaStream_t s);
+// Body::Restore of the rigid bodies' kinematics from a copy of the rigid records
+void mel_launch_rigid_restore(const mel_dev& d, const double* rg_snap, cudaStream_t s);
 // one step of a batch: the contact pass over thr0[nsamp] threads, the body pass over cta0[nsamp]
 // CTAs and the per-sample time advance (devs, thr0, cta0 in device memory)
 void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta, int nsamp,

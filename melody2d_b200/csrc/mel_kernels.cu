@@ -23,6 +23,17 @@ namespace mel {
 
 __device__ __forceinline__ void set_err(const mel_dev& d, int w, unsigned v = 1u) { atomicOr(&d.err[w], v); }
 
+// pow(x, p) of the mass-scaling increments (Code/Node.h:280, Code/Body.h:2576).  For the exponents 1,
+// 2 and 1/2 the correctly rounded value is x, x*x and sqrt(x), which is what glibc's pow returns;
+// other exponents go through CUDA's pow, whose last bit can differ from glibc's.
+__device__ __forceinline__ double ms_pow(double x, double p)
+{
+    if (p == 1.) return x;
+    if (p == 2.) return x * x;
+    if (p == 0.5) return sqrt(x);
+    return pow(x, p);
+}
+
 // Body::Update_borders length of entry j of global border g of deformable body b
 __device__ __forceinline__ double border_length(const mel_dev& d, int b, int g, int j)
 {
@@ -600,11 +611,12 @@ __device__ __forceinline__ void chunk_points_mx(int t, int ngp, int mtype, float
 //   s_up, s_f, s_fc        3 x n double2       displacements, internal forces, contact forces
 //   s_upf (mixed only)     n2 x float2         displacements relative to node 0 (n2 = n rounded to 2)
 //   ring mbarriers + abort flag                MEL_BAR_BYTES
-//   region                 max(MEL_STAGES img_cap, 112 n) bytes: the ring of chunk images during
-//                          the Gauss-point pass, then s_fn, s_fd, s_vp, s_ap (n double2 each) and
-//                          the six work terms per node (6 x n double)
-template <bool MX>
-__device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
+//   region                 max(MEL_STAGES img_cap, 128 n) bytes: the ring of chunk images during
+//                          the Gauss-point pass, then s_fn, s_fd, s_vp, s_ap (n double2 each), the
+//                          six work terms per node (6 x n double) and, in the first half-step of
+//                          Solver_step, the temporary displacement parameters (n double2)
+template <bool MX, bool AD>
+__device__ void deformable_body(const mel_dev& d, int b, double T, double T0, char* smem)
 {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -900,7 +912,10 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
     // (Code/Body.h:2058-2066) per node, summed in node order below ---------------------------
     const double gx = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gx;
     const double gy = (d.b_status[b] == MEL_STATUS_NOGRAVITY) ? 0. : d.gy;
-    const double hdt = 0.5 * dt;
+    // Apply_Euler's Deltat: the step, or half of it in each half-step of Solver_step
+    const double dte = AD ? dt * 0.5 : dt;
+    const double hdt = 0.5 * dte;
+    double2* s_upt = reinterpret_cast<double2*>(s_T + 6 * n);     // AD phase 1: temporary parameters
     for (int i = tid; i < n; i += blockDim.x) {
         int gi = n0 + i;
         double2 m = d.mass[gi], im = d.minv[gi];
@@ -911,19 +926,27 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
         double2 ft;
         ft.x = fi.x + fc.x + 0. + fb.x + fd.x + fn.x + 0. + 0.;
         ft.y = fi.y + fc.y + 0. + fb.y + fd.y + fn.y + 0. + 0.;
-        double2 ap = make_double2(ft.x * im.x / 1., ft.y * im.y / 1.);
+        double2 ap;
+        if (AD) { const double2 f = d.fms[gi]; ap = make_double2(ft.x * im.x / f.x, ft.y * im.y / f.y); }
+        else ap = make_double2(ft.x * im.x / 1., ft.y * im.y / 1.);
         double2 vp = d.vp[gi];
         s_ap[i] = ap;
         s_vp[i] = vp;
         if (d.record_forces) {
             d.o_fint[gi] = fi; d.o_fcon[gi] = fc; d.o_fneu[gi] = fn; d.o_fdir[gi] = fd; d.o_ftot[gi] = ft;
         }
+        if (AD && d.phase == 1) {      // Apply_Euler_temporary(Deltat) (Code/Node.h:247-251)
+            const double2 up = s_up[i];
+            const double2 t = make_double2(up.x + dt * (vp.x + dt * ap.x), up.y + dt * (vp.y + dt * ap.y));
+            s_upt[i] = t;
+            d.upt[gi] = t;
+        }
         double vx = vp.x + hdt * ap.x, vy = vp.y + hdt * ap.y;
-        s_T[i] = dt * (vx * fi.x + vy * fi.y);
-        s_T[n + i] = dt * (vx * fb.x + vy * fb.y);
-        s_T[2 * n + i] = dt * (vx * fd.x + vy * fd.y);
-        s_T[3 * n + i] = dt * (vx * fn.x + vy * fn.y);
-        double z = dt * (vx * 0. + vy * 0.);
+        s_T[i] = dte * (vx * fi.x + vy * fi.y);
+        s_T[n + i] = dte * (vx * fb.x + vy * fb.y);
+        s_T[2 * n + i] = dte * (vx * fd.x + vy * fd.y);
+        s_T[3 * n + i] = dte * (vx * fn.x + vy * fn.y);
+        double z = dte * (vx * 0. + vy * 0.);
         s_T[4 * n + i] = z;
         s_T[5 * n + i] = z;
     }
@@ -941,8 +964,8 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
         for (int i = tid - 32; i < n; i += blockDim.x - 32) {
             int gi = n0 + i;
             double2 ap = s_ap[i], vp = s_vp[i], up = s_up[i];
-            vp.x = vp.x + dt * ap.x; vp.y = vp.y + dt * ap.y;
-            up.x = up.x + dt * vp.x; up.y = up.y + dt * vp.y;
+            vp.x = vp.x + dte * ap.x; vp.y = vp.y + dte * ap.y;
+            up.x = up.x + dte * vp.x; up.y = up.y + dte * vp.y;
             s_vp[i] = vp; s_up[i] = up;
             d.ap[gi] = ap; d.vp[gi] = vp; d.up[gi] = up;
         }
@@ -989,6 +1012,67 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
         d.a[gi] = make_double2(ax, ay);
         double2 X = d.X0[gi];
         d.x[gi] = make_double2(X.x + dx, X.y + dy);
+        if (AD && d.phase == 1) {      // Update_kinematics_temporary (Code/Body.h:2235-2253)
+            double tx = 0., ty = 0.;
+            for (int q = 0; q < cnt; q++) {
+                const double2 t = s_upt[kidx[32 * q]];
+                const double sv = kN[32 * q];
+                tx += sv * t.x; ty += sv * t.y;
+            }
+            d.ut[gi] = make_double2(tx, ty);
+        }
+    }
+    if (AD && d.phase == 2) {
+        // ---- Update_bc(Time+Deltat) of the body's driven borders, Compute_error and
+        // Compute_mass_scaling (Code/Body.h:2528-2594, Code/Node.h:253-320): nodal terms in
+        // parallel, the body's sums and maximum in node order --------------------------------------
+        double* drv = d.drv + 8 * b;
+        if (tid == 32) body_drivendof(d, b, T0 + dt, drv);
+        tail_sync();
+        double* s_en = reinterpret_cast<double*>(s_fn);
+        double* s_mms = s_en + n;
+        const bool ms = d.solver == MEL_SOLVER_MASS_SCALING || d.solver == MEL_SOLVER_ADAPTIVE_MASS_SCALING;
+        const double te = d.sp[0], mxs = d.sp[3], cms = d.sp[4], efac = d.sp[5], decr = d.sp[6];
+        for (int i = tid - 32; i < n; i += blockDim.x - 32) {
+            const int gi = n0 + i;
+            const double2 u = d.u[gi], ut = d.ut[gi];
+            const double ex = drv[0] == 1. ? 0. : u.x - ut.x;
+            const double ey = drv[4] == 1. ? 0. : u.y - ut.y;
+            const double ide = d.ide[gi];
+            d.errv[gi] = make_double2(ex, ey);
+            s_en[i] = sqrt(ex * ex + ey * ey) * ide;
+            if (ms) {
+                double2 f = d.fms[gi];
+                double e[2] = { fabs(ex * ide), fabs(ey * ide) };
+                double* fk[2] = { &f.x, &f.y };
+                for (int k = 0; k < 2; k++) {
+                    if (e[k] >= te * efac) {
+                        *fk[k] += ms_pow((e[k] - te * efac), cms);
+                        if (*fk[k] > mxs) *fk[k] = mxs;
+                    } else {
+                        if (*fk[k] != 1) *fk[k] *= decr;
+                        if (*fk[k] < 1) *fk[k] = 1;
+                    }
+                }
+                d.fms[gi] = f;
+                const double2 m = d.mass[gi];
+                s_mms[i] = sqrt(m.x * m.x * f.x * f.x + m.y * m.y * f.y * f.y);
+            }
+        }
+        tail_sync();
+        if (tid == 32) {
+            double tot = 0., mx = 0., mm = 0.;
+            for (int i = 0; i < n; i++) {
+                const double en = s_en[i];
+                tot += en;
+                const double e2 = en == 0. ? 1.e-16 : en;
+                if (e2 > mx) mx = e2;
+                if (ms) mm += s_mms[i];
+            }
+            d.terr[b] = tot;
+            d.merr[b] = mx;
+            d.bmms[b] = mm;
+        }
     }
 }
 
@@ -997,7 +1081,8 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, char* smem)
 // ------------------------------------------------------------------------------------------
 #define MEL_RIGID_BATCH 512   // border entries whose terms are staged at once (6 doubles each)
 
-__device__ void rigid_body(const mel_dev& d, int b, double T, char* smem)
+template <bool AD>
+__device__ void rigid_body(const mel_dev& d, int b, double T, double T0, char* smem)
 {
     const int tid = threadIdx.x;
     const int n0 = d.b_node0[b];
@@ -1073,36 +1158,75 @@ __device__ void rigid_body(const mel_dev& d, int b, double T, char* smem)
         double tot[3];
         for (int k = 0; k < 3; k++) tot[k] = rf[k] + rf[3 + k] + rf[6 + k] + rf[9 + k] + rf[12 + k];
         for (int k = 0; k < 3; k++) d.rtot[3 * b + k] = tot[k];
-        rg[MEL_RG_XA] = tot[0] * rg[MEL_RG_INV_MASS] / 1.;
-        rg[MEL_RG_YA] = tot[1] * rg[MEL_RG_INV_MASS] / 1.;
-        rg[MEL_RG_RA] = tot[2] * rg[MEL_RG_INV_INERTIA] / 1.;
+        const double fmsb = AD ? d.bfms[b] : 1.;
+        rg[MEL_RG_XA] = tot[0] * rg[MEL_RG_INV_MASS] / fmsb;
+        rg[MEL_RG_YA] = tot[1] * rg[MEL_RG_INV_MASS] / fmsb;
+        rg[MEL_RG_RA] = tot[2] * rg[MEL_RG_INV_INERTIA] / fmsb;
         sh[0] = rg[MEL_RG_XA]; sh[1] = rg[MEL_RG_YA];
         // nodal copies of the body forces made by Body::Sum_up_forces (Code/Body.h:2000-2013)
         for (int k = 0; k < 3; k++) sh[2 + k] = rf[k];
         for (int k = 0; k < 3; k++) sh[5 + k] = rf[6 + k];
         for (int k = 0; k < 3; k++) sh[8 + k] = rf[9 + k];
         for (int k = 0; k < 3; k++) sh[11 + k] = tot[k];
-        // Update_bc(t+dt) (Code/Body.h:335-395)
+        // Update_bc(t+dt) (Code/Body.h:335-395); the first half-step of Solver_step keeps the
+        // values of the last call
         double* drv = d.drv + 8 * b;
-        body_drivendof(d, b, T + dt, drv);
+        if (!AD) body_drivendof(d, b, T + dt, drv);
+        else if (d.phase == 2) body_drivendof(d, b, T0 + dt, drv);
+        const double dte = AD ? dt * 0.5 : dt;        // Apply_Euler's Deltat
+        if (AD && d.phase == 1) {
+            // Apply_Euler_temporary(Deltat), rigid (Code/Body.h:2133-2167)
+            double* tm = d.rg_tmp + 6 * b;
+            if (drv[0] == 0.) { tm[3] = rg[MEL_RG_XV] + dt * rg[MEL_RG_XA]; tm[0] = rg[MEL_RG_XD] + dt * tm[3]; }
+            else if (drv[0] == 1.) { tm[3] = drv[2]; tm[0] = drv[1]; }
+            if (drv[4] == 0.) { tm[4] = rg[MEL_RG_YV] + dt * rg[MEL_RG_YA]; tm[1] = rg[MEL_RG_YD] + dt * tm[4]; }
+            else if (drv[4] == 1.) { tm[4] = drv[6]; tm[1] = drv[5]; }
+            if (drv[0] == 0. && drv[4] == 0. && !d.b_per[b]) { tm[5] = rg[MEL_RG_RV] + dt * rg[MEL_RG_RA]; tm[2] = rg[MEL_RG_RD] + dt * tm[5]; }
+            else { tm[5] = 0.; tm[2] = 0.; }
+        }
         // Apply_Euler, rigid (Code/Body.h:2071-2117)
         double* W = d.works + 7 * b;
-        double vx = rg[MEL_RG_XV] + 0.5 * dt * rg[MEL_RG_XA];
-        double vy = rg[MEL_RG_YV] + 0.5 * dt * rg[MEL_RG_YA];
-        double vr = rg[MEL_RG_RV] + 0.5 * dt * rg[MEL_RG_RA];
-        W[2] += dt * (vx * rf[3] + vy * rf[4] + vr * rf[5]);
-        W[3] += dt * (vx * rf[6] + vy * rf[7] + vr * rf[8]);
-        W[4] += dt * (vx * rf[9] + vy * rf[10] + vr * rf[11]);
-        W[5] += dt * (vx * rf[12] + vy * rf[13] + vr * rf[14]);
-        if (drv[0] == 0.) { rg[MEL_RG_XV] += dt * rg[MEL_RG_XA]; rg[MEL_RG_XD] = rg[MEL_RG_XD] + dt * rg[MEL_RG_XV]; }
+        double vx = rg[MEL_RG_XV] + 0.5 * dte * rg[MEL_RG_XA];
+        double vy = rg[MEL_RG_YV] + 0.5 * dte * rg[MEL_RG_YA];
+        double vr = rg[MEL_RG_RV] + 0.5 * dte * rg[MEL_RG_RA];
+        W[2] += dte * (vx * rf[3] + vy * rf[4] + vr * rf[5]);
+        W[3] += dte * (vx * rf[6] + vy * rf[7] + vr * rf[8]);
+        W[4] += dte * (vx * rf[9] + vy * rf[10] + vr * rf[11]);
+        W[5] += dte * (vx * rf[12] + vy * rf[13] + vr * rf[14]);
+        if (drv[0] == 0.) { rg[MEL_RG_XV] += dte * rg[MEL_RG_XA]; rg[MEL_RG_XD] = rg[MEL_RG_XD] + dte * rg[MEL_RG_XV]; }
         else if (drv[0] == 1.) { rg[MEL_RG_XA] = drv[3]; rg[MEL_RG_XV] = drv[2]; rg[MEL_RG_XD] = drv[1]; rf[6] = rg[MEL_RG_MASS] * rg[MEL_RG_XA] - tot[0]; }
-        if (drv[4] == 0.) { rg[MEL_RG_YV] += dt * rg[MEL_RG_YA]; rg[MEL_RG_YD] = rg[MEL_RG_YD] + dt * rg[MEL_RG_YV]; }
+        if (drv[4] == 0.) { rg[MEL_RG_YV] += dte * rg[MEL_RG_YA]; rg[MEL_RG_YD] = rg[MEL_RG_YD] + dte * rg[MEL_RG_YV]; }
         else if (drv[4] == 1.) { rg[MEL_RG_YA] = drv[7]; rg[MEL_RG_YV] = drv[6]; rg[MEL_RG_YD] = drv[5]; rf[7] = rg[MEL_RG_MASS] * rg[MEL_RG_YA] - tot[1]; }
-        if (drv[0] == 0. && drv[4] == 0. && !d.b_per[b]) { rg[MEL_RG_RV] += dt * rg[MEL_RG_RA]; rg[MEL_RG_RD] = rg[MEL_RG_RD] + dt * rg[MEL_RG_RV]; }
+        if (drv[0] == 0. && drv[4] == 0. && !d.b_per[b]) { rg[MEL_RG_RV] += dte * rg[MEL_RG_RA]; rg[MEL_RG_RD] = rg[MEL_RG_RD] + dte * rg[MEL_RG_RV]; }
         else { rg[MEL_RG_RV] = 0.; rg[MEL_RG_RD] = 0.; }
         rg[MEL_RG_XC] = rg[MEL_RG_X0] + rg[MEL_RG_XD];
         rg[MEL_RG_YC] = rg[MEL_RG_Y0] + rg[MEL_RG_YD];
         rg[MEL_RG_RC] = rg[MEL_RG_R0] + rg[MEL_RG_RD];
+        if (AD && d.phase == 2) {
+            // Compute_error and Compute_mass_scaling, rigid (Code/Body.h:2538-2552, 2572-2593)
+            const double* tm = d.rg_tmp + 6 * b;
+            double te2 = 0.;
+            if (drv[0] != 1.) te2 += (rg[MEL_RG_XD] - tm[0]) * (rg[MEL_RG_XD] - tm[0]);
+            if (drv[4] != 1.) te2 += (rg[MEL_RG_YD] - tm[1]) * (rg[MEL_RG_YD] - tm[1]);
+            te2 = 0.1 * sqrt(te2) / d.b_dist[3 * b];
+            if (te2 == 0.) te2 = 1.e-16;
+            d.terr[b] = te2;
+            d.merr[b] = te2;
+            if (d.solver == MEL_SOLVER_MASS_SCALING || d.solver == MEL_SOLVER_ADAPTIVE_MASS_SCALING) {
+                const double te = d.sp[0], mxs = d.sp[3], cms = d.sp[4], efac = d.sp[5], decr = d.sp[6];
+                double f = d.bfms[b];
+                if (te2 >= te * efac) {
+                    d.bdfms[b] = ms_pow((te2 - te * efac), cms);
+                    f += d.bdfms[b];
+                    if (f >= mxs) f = mxs;
+                } else {
+                    if (f != 1) f *= decr;
+                    if (f < 1) f = 1;
+                }
+                d.bfms[b] = f;
+                d.bmms[b] = rg[MEL_RG_MASS] * f;
+            }
+        }
     }
     __syncthreads();
     // node kinematics (Code/Body.h:2212-2225, 2284-2300); Apply_Newton's nodal accelerations
@@ -1159,14 +1283,14 @@ __device__ void contact_work(const mel_dev& d, int b)
     d.works[7 * b + 1] = w;
 }
 
-template <bool MX>
-__device__ __forceinline__ void body_cta(const mel_dev& d, int bb, double T, char* smem)
+template <bool MX, bool AD = false>
+__device__ __forceinline__ void body_cta(const mel_dev& d, int bb, double T, char* smem, double T0 = 0.)
 {
     int b = d.b_order[bb];
     if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
     if (d.any_damped && threadIdx.x == 32) contact_work(d, b);
-    if (d.b_type[b] == MEL_BODY_RIGID) rigid_body(d, b, T, smem);
-    else deformable_body<MX>(d, b, T, smem);
+    if (d.b_type[b] == MEL_BODY_RIGID) rigid_body<AD>(d, b, T, T0, smem);
+    else deformable_body<MX, AD>(d, b, T, T0, smem);
 }
 
 __global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale, int czm_init)
@@ -1183,6 +1307,39 @@ __global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel(mel_dev d, in
     const double T = d.time2[parity];
     body_cta<MX>(d, blockIdx.x, T, smem);
     if (blockIdx.x == 0 && threadIdx.x == 0) d.time2[parity ^ 1] = T + d.dt[0];
+}
+
+// One half-step of Solver_step (d.phase 1 or 2) of one model: T0 = Time, Tf = the time the
+// border conditions of the forces are taken at.  The host keeps the time.
+template <bool MX>
+__global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel_adaptive(mel_dev d, double T0, double Tf)
+{
+    extern __shared__ __align__(16) char smem[];
+    body_cta<MX, true>(d, blockIdx.x, Tf, smem, T0);
+}
+
+// Solver_step's sums over bodies in body order (Code/Solver.h:289-331)
+__global__ void error_reduce_kernel(mel_dev d, double* out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double mean = 0., mx = 0., tm = 0., mm = 0.;
+    int nnodes = 0;
+    const bool ms = d.solver == MEL_SOLVER_MASS_SCALING || d.solver == MEL_SOLVER_ADAPTIVE_MASS_SCALING;
+    for (int i = 0; i < d.nb; i++) {
+        if (d.b_status[i] == MEL_STATUS_INACTIVE) continue;
+        mean += d.terr[i];
+        nnodes += d.b_node0[i + 1] - d.b_node0[i];
+        if (d.merr[i] > mx) mx = d.merr[i];
+    }
+    mean /= nnodes;
+    if (ms)
+        for (int i = 0; i < d.nb; i++) {
+            if (d.b_status[i] == MEL_STATUS_INACTIVE) continue;
+            tm += d.bmms[i];
+            const double inv = d.rg[MEL_RIGID_NF * i + MEL_RG_INV_MASS];
+            if (d.bmms[i] * inv > mm) mm = d.bmms[i] * inv;
+        }
+    out[0] = mean; out[1] = mx; out[2] = tm; out[3] = mm;
 }
 
 // ---- batches: several independent models (samples) advanced by the same launches -----------
@@ -1360,7 +1517,7 @@ size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)
     size_t base = 3 * sizeof(double2) * (size_t)max_nodes + MEL_BAR_BYTES;
     if (mixed) base += sizeof(float2) * (size_t)((max_nodes + 1) & ~1);
     size_t stage = MEL_STAGES * (size_t)max_image_bytes;
-    size_t post = (4 * sizeof(double2) + 6 * sizeof(double)) * (size_t)max_nodes;
+    size_t post = (5 * sizeof(double2) + 6 * sizeof(double)) * (size_t)max_nodes;
     size_t rigid = (64 + 6 * MEL_RIGID_BATCH) * sizeof(double);
     size_t r = base + (stage > post ? stage : post);
     return r > rigid ? r : rigid;
@@ -1383,6 +1540,37 @@ void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cud
     else mel::body_kernel<false><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
 }
 
+void mel_launch_body_adaptive(const mel_dev& d, double T0, double Tf, int nblocks, size_t smem, cudaStream_t s)
+{
+    if (d.precision == MEL_PREC_MIXED) mel::body_kernel_adaptive<true><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf);
+    else mel::body_kernel_adaptive<false><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf);
+}
+
+void mel_launch_error_reduce(const mel_dev& d, double* out, cudaStream_t s)
+{
+    mel::error_reduce_kernel<<<1, 32, 0, s>>>(d, out);
+}
+
+namespace mel {
+// Body::Restore of a rigid body's own kinematics (Code/Body.h:2650-2658): current position,
+// displacement and velocity; its accelerations, driven values and mass-scaling factor are not
+// part of the snapshot
+__global__ void rigid_restore_kernel(mel_dev d, const double* rg_snap)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.nb || d.b_type[b] != MEL_BODY_RIGID) return;
+    const double* s = rg_snap + MEL_RIGID_NF * (size_t)b;
+    double* r = d.rg + MEL_RIGID_NF * (size_t)b;
+    const int f[9] = { MEL_RG_XC, MEL_RG_YC, MEL_RG_RC, MEL_RG_XD, MEL_RG_YD, MEL_RG_RD, MEL_RG_XV, MEL_RG_YV, MEL_RG_RV };
+    for (int k = 0; k < 9; k++) r[f[k]] = s[f[k]];
+}
+}  // namespace mel
+
+void mel_launch_rigid_restore(const mel_dev& d, const double* rg_snap, cudaStream_t s)
+{
+    mel::rigid_restore_kernel<<<(d.nb + 127) / 128, 128, 0, s>>>(d, rg_snap);
+}
+
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s)
 {
     mel::monitor_partial_kernel<<<MON_BLOCKS, 256, 0, s>>>(d, part);
@@ -1402,7 +1590,9 @@ int mel_body_kernel_configure(size_t smem)
     if (cudaFuncSetAttribute(mel::body_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
         cudaFuncSetAttribute(mel::body_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
         cudaFuncSetAttribute(mel::body_kernel_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(mel::body_kernel_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaFuncSetAttribute(mel::body_kernel_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_adaptive<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_adaptive<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         mel_set_cuda_error(cudaGetLastError(), "cudaFuncSetAttribute(body_kernel)", __FILE__, __LINE__);
         return MEL_ERR_CUDA;
     }

@@ -79,6 +79,15 @@ struct mel_handle {
     // current contact list, 2 = that list was replaced by a proximity update since (batch member
     // without recording)
     int pressure_state = 0;
+    // Solver_step: Body::Store snapshot (device), time of the last Update_bc, statistics of the
+    // last step {neval, max_error, mean_error, total_mass, max_mass}, reduction output (pinned)
+    std::vector<void*> store_bufs;
+    size_t store_cont_cap = 0;
+    int store_ncont = 0;
+    double t_bc = 0.;
+    double solver_stats[5] = { 0., 0., 0., 0., 0. };
+    double* h_red = nullptr;
+    double* d_red = nullptr;
     int* d_rigid_ids = nullptr;
     int nrigid = 0;
     int precision = MEL_PREC_FP64;
@@ -185,7 +194,7 @@ static mel_status validate(const mel_model_desc* d)
     if (d->n_bodies <= 0 || d->n_nodes <= 0 || d->n_borders <= 0) { mel_set_error("empty model"); return MEL_ERR_INVALID; }
     if (!(d->period[1] > d->period[0])) { mel_set_error("PERIODIC_BOUNDARIES must satisfy Xmin < Xmax"); return MEL_ERR_INVALID; }
     if (!(d->dt > 0.)) { mel_set_error("time step must be positive"); return MEL_ERR_INVALID; }
-    if (d->solver != MEL_SOLVER_EULER) { mel_set_error("solver %d: this build runs the Euler scheme (Code/Solver.h:10-88)", d->solver); return MEL_ERR_UNSUPPORTED; }
+    if (d->solver < MEL_SOLVER_EULER || d->solver > MEL_SOLVER_EULER_2) { mel_set_error("unknown solver %d", d->solver); return MEL_ERR_INVALID; }
     if (d->body_node_ptr[d->n_bodies] != d->n_nodes) { mel_set_error("body_node_ptr does not cover n_nodes"); return MEL_ERR_INVALID; }
     if (d->body_border_ptr[d->n_bodies] != d->n_borders) { mel_set_error("body_border_ptr does not cover n_borders"); return MEL_ERR_INVALID; }
     for (int g = 0; g < d->n_borders; g++) {
@@ -337,6 +346,30 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.up = (double2*)dalloc<double>(h, 2 * (size_t)nn);
     D.vp = (double2*)dalloc<double>(h, 2 * (size_t)nn);
     D.ap = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    // Solver_step state: temporaries, errors, mass-scaling factors (1), estimators (Code/IO.h:1620,1819)
+    D.solver = d->solver;
+    for (int k = 0; k < 8; k++) D.sp[k] = d->solver_params[k];
+    D.upt = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.ut = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    D.errv = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    {
+        std::vector<double> ones(2 * (size_t)nn, 1.), ide(nn, 0.), bones(nb, 1.);
+        for (int b = 0; b < nb; b++)
+            for (int i = d->body_node_ptr[b]; i < d->body_node_ptr[b + 1]; i++) {
+                if (d->body_type[b] == MEL_BODY_DEFORMABLE) {
+                    const int ns = d->node_sup_ptr[i + 1] - d->node_sup_ptr[i];
+                    ide[i] = ns ? 1. / (d->node_domain[i] * sqrt(3.1415927 / 4. / ns)) : 0.;
+                } else ide[i] = 1. / d->body_dist[3 * b];
+            }
+        D.fms = (double2*)dupload(h, ones);
+        D.ide = dupload(h, ide);
+        D.bfms = dupload(h, bones);
+    }
+    D.terr = dalloc<double>(h, nb);
+    D.merr = dalloc<double>(h, nb);
+    D.bmms = dalloc<double>(h, nb);
+    D.bdfms = dalloc<double>(h, nb);
+    D.rg_tmp = dalloc<double>(h, 6 * (size_t)nb);
     h->nse = d->node_sup_ptr[nn];
     std::vector<uint16_t> sidx(h->nse);
     for (int b = 0; b < nb; b++)
@@ -691,6 +724,147 @@ static mel_status upload_state(mel_handle* h, const double* st, const double* ri
     return MEL_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Solver_step (Code/Solver.h:98-486): Body::Store / Body::Restore as device copies
+// ---------------------------------------------------------------------------------------------
+// snapshot: node blob (x, u, v, a, up, vp, ap, upt, ut, fms, errv), works, bdfms, rigid records,
+// contact list
+static mel_status adaptive_store(mel_handle* h, bool restore)
+{
+    mel_dev& D = h->d;
+    const size_t nn = (size_t)h->nn, nb = (size_t)h->nb;
+    double2* nodes[11] = { D.x, D.u, D.v, D.a, D.up, D.vp, D.ap, D.upt, D.ut, D.fms, D.errv };
+    if (h->store_bufs.empty()) {
+        void* p[3] = { nullptr, nullptr, nullptr };
+        if (cudaMalloc(&p[0], sizeof(double2) * 11 * nn) != cudaSuccess ||
+            cudaMalloc(&p[1], sizeof(double) * (8 + MEL_RIGID_NF) * nb) != cudaSuccess) {
+            for (void* q : p) if (q) cudaFree(q);
+            mel_set_error("Solver_step snapshot allocation failed");
+            return MEL_ERR_OOM;
+        }
+        h->store_bufs = { p[0], p[1], nullptr };
+        h->store_cont_cap = 0;
+    }
+    double2* nb_ = static_cast<double2*>(h->store_bufs[0]);
+    double* bb = static_cast<double*>(h->store_bufs[1]);
+    cudaStream_t s = h->stream;
+    const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+    if (!restore) {
+        if ((size_t)D.ncont > h->store_cont_cap) {
+            if (h->store_bufs[2]) cudaFree(h->store_bufs[2]);
+            h->store_bufs[2] = nullptr;
+            const size_t cap = (size_t)D.ncont * 2 + 64;
+            if (cudaMalloc(&h->store_bufs[2], sizeof(mel_contact) * cap) != cudaSuccess) {
+                h->store_bufs[2] = nullptr; h->store_cont_cap = 0;
+                mel_set_error("Solver_step snapshot allocation failed");
+                return MEL_ERR_OOM;
+            }
+            h->store_cont_cap = cap;
+        }
+        for (int a = 0; a < 11; a++) MEL_CUDA_OK(cudaMemcpyAsync(nb_ + a * nn, nodes[a], sizeof(double2) * nn, k, s));
+        MEL_CUDA_OK(cudaMemcpyAsync(bb, D.works, sizeof(double) * 7 * nb, k, s));
+        MEL_CUDA_OK(cudaMemcpyAsync(bb + 7 * nb, D.bdfms, sizeof(double) * nb, k, s));
+        MEL_CUDA_OK(cudaMemcpyAsync(bb + 8 * nb, D.rg, sizeof(double) * MEL_RIGID_NF * nb, k, s));
+        if (D.ncont) MEL_CUDA_OK(cudaMemcpyAsync(h->store_bufs[2], D.cont, sizeof(mel_contact) * D.ncont, k, s));
+        h->store_ncont = D.ncont;
+    } else {
+        for (int a = 0; a < 11; a++) MEL_CUDA_OK(cudaMemcpyAsync(nodes[a], nb_ + a * nn, sizeof(double2) * nn, k, s));
+        MEL_CUDA_OK(cudaMemcpyAsync(D.works, bb, sizeof(double) * 7 * nb, k, s));
+        MEL_CUDA_OK(cudaMemcpyAsync(D.bdfms, bb + 7 * nb, sizeof(double) * nb, k, s));
+        mel_launch_rigid_restore(D, bb + 8 * nb, s);
+        MEL_CUDA_OK(cudaGetLastError());
+        if (h->store_ncont) MEL_CUDA_OK(cudaMemcpyAsync(D.cont, h->store_bufs[2], sizeof(mel_contact) * h->store_ncont, k, s));
+    }
+    return MEL_OK;
+}
+
+// Deltat's correction law shared by the schemes (Code/Solver.h:349-357)
+static void dt_law(mel_handle* h, double c1, double c2)
+{
+    if (c1 > c2) h->dt = h->dt / pow(c1, h->d.sp[1]);
+    else h->dt = h->dt / pow(c2, h->d.sp[1]);
+    if (h->dt > h->cup) h->dt = h->cup;
+}
+
+// One accepted step of Solver_step: two half-steps with the temporary full step beside the first,
+// the error (and mass-scaling) sums, and the scheme's accept / reject rule with its Deltat law;
+// a rejected attempt restores the snapshot and retries with the corrected Deltat.  Like the oracle,
+// gives up after 1000 attempts (the reference would retry for ever).
+static mel_status adaptive_step(mel_handle* h)
+{
+    if (!h->h_red) {
+        if (cudaMallocHost(&h->h_red, 8 * sizeof(double)) != cudaSuccess) { h->h_red = nullptr; mel_set_error("pinned allocation failed"); return MEL_ERR_OOM; }
+        h->d_red = dalloc<double>(h, 8);
+        if (!h->d_red) { mel_set_error("device allocation failed"); return MEL_ERR_OOM; }
+    }
+    mel_status rc = adaptive_store(h, false);
+    if (rc) return rc;
+    const double Target_error = h->d.sp[0], Accepted_ratio = h->d.sp[2], Inv_Target_error = h->d.sp[7];
+    int neval = 0;
+    bool ok = false;
+    double mean_error = 0., max_error = 0., total_mass = 0., max_mass = 0.;
+    while (!ok) {
+        neval++;
+        h->h_red[7] = h->dt;
+        MEL_CUDA_OK(cudaMemcpyAsync(h->d.dt, &h->h_red[7], sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        mel_dev d = h->d;
+        mel_launch_contact(d, 0.5, h->stream);                 // Update_contact_forces(Deltat*0.5)
+        d.phase = 1;
+        mel_launch_body_adaptive(d, h->time, h->t_bc, h->nblocks_body, h->body_smem, h->stream);
+        mel_launch_contact(d, 0.5, h->stream);
+        d.phase = 2;
+        mel_launch_body_adaptive(d, h->time, h->time + h->dt * 0.5, h->nblocks_body, h->body_smem, h->stream);
+        h->t_bc = h->time + h->dt;                              // Update_bc(Time+Deltat) of the second half
+        mel_launch_error_reduce(d, h->d_red, h->stream);
+        h->launches += 5;
+        MEL_CUDA_OK(cudaGetLastError());
+        MEL_CUDA_OK(cudaMemcpyAsync(h->h_red, h->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+        if ((rc = check_errors(h))) return rc;
+        mean_error = h->h_red[0]; max_error = h->h_red[1]; total_mass = h->h_red[2]; max_mass = h->h_red[3];
+        const double error = max_error;
+        bool reject = false;
+        switch (h->solver) {
+        case MEL_SOLVER_ADAPTIVE_EULER:
+            reject = error > Target_error * Accepted_ratio;
+            dt_law(h, error / Target_error, 1. / Accepted_ratio);
+            break;
+        case MEL_SOLVER_EULER_2:
+            dt_law(h, error / Target_error, 1. / Accepted_ratio);
+            break;
+        case MEL_SOLVER_MASS_SCALING:
+            reject = max_error > Target_error * Accepted_ratio;
+            dt_law(h, max_error * Inv_Target_error, 1. / Accepted_ratio);
+            break;
+        case MEL_SOLVER_ADAPTIVE_MASS_SCALING:
+            reject = max_mass > Accepted_ratio + 0.05;
+            if (reject) dt_law(h, max_mass, 1. / Accepted_ratio);
+            else {
+                const double c2 = 1. / Accepted_ratio;
+                h->dt = h->dt / pow(c2, h->d.sp[1]);
+                if (h->dt > h->cup) h->dt = h->cup;
+            }
+            break;
+        }
+        if (reject) {
+            // the correction above used the attempt's Deltat; Time stays
+            if ((rc = adaptive_store(h, true))) return rc;
+        } else {
+            ok = true;
+        }
+        if (!ok && neval > 1000) break;
+    }
+    if (ok) {
+        // Time += Deltat happened with the Deltat of the accepted attempt: recover it from the
+        // snapshot of the attempt (h_red[7]) before the law changed h->dt
+        h->time += h->h_red[7];
+        h->pressure_state = 1;
+    }
+    h->solver_stats[0] = neval; h->solver_stats[1] = max_error; h->solver_stats[2] = mean_error;
+    h->solver_stats[3] = total_mass; h->solver_stats[4] = max_mass;
+    return MEL_OK;
+}
+
 // Update_contact_pressures on the handle's stream, if the last step's pressures are not computed yet
 static void update_pressures(mel_handle* h)
 {
@@ -718,6 +892,7 @@ static mel_status create_impl(const mel_model_desc* desc, const mel_options* opt
     if (cudaSetDevice(h->device) != cudaSuccess) { mel_set_error("cudaSetDevice(%d) failed", h->device); delete h; return MEL_ERR_NO_DEVICE; }
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { mel_set_error("stream"); delete h; return MEL_ERR_CUDA; }
     rc = build(h, desc, opt);
+    h->t_bc = desc->time;                  // set-up's Update_bc(Time) (Code/main.cpp:104-127)
     if (!rc) rc = upload_state(h, desc->node_state, h->rg_file.data());
     if (!rc && nc0 > 0) rc = mel_set_contacts(h, c0, nc0);   // contacts of the DYNAMIC file (Code/IO.h:2236-2302)
     if (!rc) rc = setup(h);
@@ -776,6 +951,8 @@ mel_status mel_destroy(mel_handle* h)
     if (h->ck.landed) cudaEventDestroy(h->ck.landed);
     if (h->ck.d_stage) cudaFree(h->ck.d_stage);
     if (h->d_state) cudaFree(h->d_state);
+    for (void* p : h->store_bufs) cudaFree(p);
+    if (h->h_red) cudaFreeHost(h->h_red);
     if (h->ck.h_stage) cudaFreeHost(h->ck.h_stage);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
@@ -802,20 +979,27 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
     std::vector<cudaEvent_t> ev;
     auto mark = [&]() { if (!h->timing) return; cudaEvent_t e = h->ev_pool[nev++]; cudaEventRecord(e, h->stream); ev.push_back(e); };
     std::vector<int> kinds;
+    const bool adaptive = h->solver != MEL_SOLVER_EULER;
     for (int s = 0; s < io->nsteps; s++) {
-        mark();
-        mel_launch_contact(h->d, 1.0, h->stream);
-        mark(); kinds.push_back(0);
-        mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream);
-        mark(); kinds.push_back(1);
-        {
-            cudaError_t le = cudaGetLastError();
-            if (le != cudaSuccess) { mel_set_cuda_error(le, "step kernel launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+        if (adaptive) {
+            // Solver_step (Code/Solver.h:98-486, dispatched at Code/main.cpp:156-167)
+            mel_status rc = adaptive_step(h);
+            if (rc) return rc;
+        } else {
+            mark();
+            mel_launch_contact(h->d, 1.0, h->stream);
+            mark(); kinds.push_back(0);
+            mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream);
+            mark(); kinds.push_back(1);
+            {
+                cudaError_t le = cudaGetLastError();
+                if (le != cudaSuccess) { mel_set_cuda_error(le, "step kernel launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+            }
+            h->launches += 2;
+            h->parity ^= 1;
+            h->time += h->dt;                       // Code/Solver.h:86
+            h->pressure_state = 1;                  // Update_contact_pressures ends the step (Code/Solver.h:87)
         }
-        h->launches += 2;
-        h->parity ^= 1;
-        h->time += h->dt;                       // Code/Solver.h:86
-        h->pressure_state = 1;                  // Update_contact_pressures ends the step (Code/Solver.h:87)
         if (io->run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
             h->next_cup = h->next_cup + h->cup;
             update_pressures(h);                // from the list the step ended with
@@ -825,6 +1009,12 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             if (rc) return rc;
             nprox++;
         }
+    }
+    if (adaptive) {
+        // the device clock of the Euler launches follows the host's (Time, Deltat)
+        double t2[2] = { h->time, h->time };
+        MEL_CUDA_OK(cudaMemcpyAsync(h->d.time2, t2, sizeof t2, cudaMemcpyHostToDevice, h->stream));
+        MEL_CUDA_OK(cudaMemcpyAsync(h->d.dt, &h->dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
     }
     cudaEventRecord(h->ev_end, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
@@ -1025,6 +1215,7 @@ mel_status mel_set_time(mel_handle* h, double time, double dt, double next_conta
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
     h->time = time; h->dt = dt; h->next_cup = next_contact_update;
+    h->t_bc = time;
     double t2[2] = { time, time };
     MEL_CUDA_OK(cudaMemcpy(h->d.time2, t2, sizeof t2, cudaMemcpyHostToDevice));
     MEL_CUDA_OK(cudaMemcpy(h->d.dt, &dt, sizeof dt, cudaMemcpyHostToDevice));
@@ -1109,6 +1300,13 @@ mel_status mel_get_contact_pressures(mel_handle* h, double* px, double* py)
         if (py) MEL_CUDA_OK(cudaMemcpy(py, h->d.cpy, sizeof(double) * (size_t)h->ne, cudaMemcpyDeviceToHost));
     }
     return check_errors(h);
+}
+
+mel_status mel_get_solver_stats(mel_handle* h, double* out5)
+{
+    if (!h || !out5) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    for (int k = 0; k < 5; k++) out5[k] = h->solver_stats[k];
+    return MEL_OK;
 }
 
 mel_status mel_get_contact_count(mel_handle* h, int* n)
@@ -1423,6 +1621,7 @@ mel_status mel_batch_create(int device, int precision, mel_batch** out)
 
 mel_status mel_batch_admit(mel_batch* b, mel_handle* h)
 {
+    if (h && h->solver != MEL_SOLVER_EULER) { mel_set_error("batches advance the Euler scheme; step Solver_step schemes with mel_step"); return MEL_ERR_UNSUPPORTED; }
     if (!b || !h) return MEL_ERR_INVALID;
     if (h->batch) { mel_set_error("the handle is already a member of a batch"); return MEL_ERR_INVALID; }
     if (h->device != b->device || h->precision != b->precision) {

@@ -170,6 +170,7 @@ class Body:
     rigid_inertia: float = 0.0
     velocity: Tuple[float, float] = (0.0, 0.0)
     angular_velocity: float = 0.0               # rigid only (rad/s)
+    dt_terms: Optional[Tuple[float, float]] = None   # critical-step terms (elastic eigenvalue, h/m per kn)
 
 
 def _ccw(nodes: np.ndarray, tri: np.ndarray) -> np.ndarray:
@@ -217,10 +218,51 @@ def _rejection_interior(rng, centre, radius, n_target, min_sep, existing, margin
     return np.array(pts).reshape(-1, 2)
 
 
+# A lumped mass is the integral of the node's MLS shape function; a node placed where its support
+# is cut short (next to another node, close to the border) can get a mass far below the others, or
+# even a negative one, and with it a critical time step far below its disc's (or no stable step at
+# all).  Such a disc is drawn again: MIN_MASS_RATIO is the smallest accepted ratio of a node's mass to
+# the disc's median.
+MIN_MASS_RATIO = 0.2
+
+
+# The same holds for the disc's critical time step, 2 / sqrt(largest eigenvalue of its lumped-mass
+# elastic operator): over many draws it sits near h_b sqrt(rho / E) (h_b the border-node spacing) with
+# a long lower tail, down to a third of that, and one such disc sets the step of a whole sample.
+# With dt_check, a disc whose step falls below MIN_DT_RATIO of that nominal value is drawn again.
+MIN_DT_RATIO = 0.75
+
+
 def make_disc(rng, centre, radius, n_border, n_interior, min_sep, material, rho, support_factor=2.0,
-              mass_factor=1.0, regions=1):
+              mass_factor=1.0, regions=1, max_draws=20, dt_check=None):
     """Deformable disc: n_border equispaced border nodes (CCW), seeded interior nodes, Delaunay
-    cells, 3 Gauss points per cell, MLS shape functions, lumped masses."""
+    cells, 3 Gauss points per cell, MLS shape functions, lumped masses.  The interior nodes are drawn
+    again (from the same random stream) while some node's lumped mass is below MIN_MASS_RATIO of the
+    median, and, with dt_check = (mu, lambda, E), while the disc's critical step is below MIN_DT_RATIO
+    of h_b sqrt(rho mass_factor / E); the disc then carries dt_terms (the two terms of critical_dt)."""
+    best = None
+    for _ in range(max_draws):
+        b = _make_disc_once(rng, centre, radius, n_border, n_interior, min_sep, material, rho, support_factor,
+                            mass_factor, regions)
+        m = b.mass[:, 0]
+        q = float(m.min() / np.median(m)) / MIN_MASS_RATIO
+        if dt_check is not None and q >= 1.0:   # (a non-positive mass leaves no stable step to compute)
+            mu, lam, E = dt_check
+            lam_el = (2.0 / critical_dt(b, mu, lam, 0.0)) ** 2
+            b.dt_terms = (lam_el, float(np.max(b.nodal_distance / m[: len(b.borders[0]["nodes"]) - 1])))
+            nominal = b.nodal_distance * math.sqrt(rho * mass_factor / E)
+            q = min(q, 2.0 / math.sqrt(lam_el) / nominal / MIN_DT_RATIO)
+        if q >= 1.0:
+            return b
+        if best is None or q > best[0]:
+            best = (q, b)
+    if dt_check is not None and best[1].dt_terms is None:
+        raise RuntimeError("no draw of this disc has positive lumped masses")
+    return best[1]
+
+
+def _make_disc_once(rng, centre, radius, n_border, n_interior, min_sep, material, rho, support_factor,
+                    mass_factor, regions):
     th = 2.0 * np.pi * np.arange(n_border) / n_border
     border = np.stack([centre[0] + radius * np.cos(th), centre[1] + radius * np.sin(th)], axis=1)
     h_b = 2.0 * math.pi * radius / n_border
@@ -934,12 +976,14 @@ def _rsa_pack(rng, radii, width, height, gap, max_tries=2000):
 
 
 def _disc_worker(args):
-    seed, centre, radius, n_border, n_interior, rho, mass_factor = args
+    seed, centre, radius, n_border, n_interior, rho, mass_factor = args[:7]
     import random as _r
     prng = _r.Random(int(seed))
     area = math.pi * radius * radius
     h = math.sqrt(area / (n_border + n_interior))
-    return make_disc(prng, centre, radius, n_border, n_interior, 0.6 * h, 0, rho, mass_factor=mass_factor)
+    # with (mu, lambda, E): draws checked for their critical step, which the disc then carries
+    return make_disc(prng, centre, radius, n_border, n_interior, 0.6 * h, 0, rho, mass_factor=mass_factor,
+                     dt_check=args[7] if len(args) > 7 else None)
 
 
 def make_discs_parallel(jobs, workers: Optional[int] = None):
@@ -1001,16 +1045,19 @@ def biaxial_scene(seed: int = 1, n_discs: int = 2000, rmin: float = 0.5e-3, rmax
             ("Grain", "Steel", 2, 0, [1e10, 1e9, mu_fric, 0.0, 0.0]),
             ("Steel", "Steel", 0, 0, [0.0])]
     seeds = rng.integers(0, 2 ** 31 - 1, size=n_discs)
+    mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
     jobs = [(int(seeds[i]), (float(centres[i, 0]), float(centres[i, 1])), float(radii[i]), n_border, n_interior,
-             rho, mass_factor) for i in range(n_discs)]
+             rho, mass_factor, (mu, lam, E)) for i in range(n_discs)]
     bodies = make_discs_parallel(jobs, workers)
     for b, r in zip(bodies, radii):
         b.detection = b.contact = max(b.contact, contact_distance(sigma, float(r)))
     h_min = 2.0 * math.pi * rmin / n_border
     bodies += _biaxial_frame(W, H, h_min, rho_steel, v_plate, sigma, contact_distance(sigma, rmax))
-    mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
-    smallest = np.argsort(radii)[:3]
-    dtc = min(critical_dt(bodies[i], mu, lam, 1e10) for i in smallest)
+    # every disc's own critical step: a disc whose node layout leaves one node with a small lumped
+    # mass can have a critical step below the smallest discs' (a 1.1 mm disc of the 2000-disc
+    # sample at 0.97 us against 2.3 us), and runs unstable once a contact excites it
+    kn = 1e10
+    dtc = min(2.0 / math.sqrt(max(b.dt_terms[0], kn * b.dt_terms[1])) for b in bodies[:n_discs])
     dt = float("%.4g" % (0.5 * dtc))
     return Scene(name=name, bodies=bodies, materials=mats, laws=laws, dt=dt, nsteps=nsteps,
                  contact_update_period=prox_every * dt,
@@ -1067,9 +1114,9 @@ class DiscTemplates:
         counts = sorted(set(int(c) for c in border_counts))
         rng = np.random.default_rng(seed)
         seeds = rng.integers(0, 2 ** 31 - 1, size=len(counts))
-        jobs = [(int(s), (0.0, 0.0), 1.0, nb, interior_factor * nb, 1.0, 1.0) for s, nb in zip(seeds, counts)]
-        bodies = make_discs_parallel(jobs, workers)
         mu = E / (2 * (1 + nu)); lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+        jobs = [(int(s), (0.0, 0.0), 1.0, nb, interior_factor * nb, 1.0, 1.0, (mu, lam, E)) for s, nb in zip(seeds, counts)]
+        bodies = make_discs_parallel(jobs, workers)
         self.E, self.nu = E, nu
         self.discs = dict(zip(counts, bodies))
         self.terms = {nb: _dt_terms(b, mu, lam) for nb, b in self.discs.items()}

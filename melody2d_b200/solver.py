@@ -41,6 +41,7 @@ SIGNATURES = {
     "mel_get_works": [_vp, _dp],
     "mel_get_contact_count": [_vp, _ip],
     "mel_get_contact_pressures": [_vp, _dp, _dp],
+    "mel_get_solver_stats": [_vp, _dp],
     "mel_get_contacts": [_vp, C.POINTER(abi.MelContact), C.c_int, _ip],
     "mel_get_time": [_vp, _dp, _dp],
     "mel_checkpoint_start": [_vp],
@@ -225,6 +226,13 @@ class Solver:
         buf = (abi.MelContact * max(1, n.value))()
         _check(lib().mel_get_contacts(self.h, buf, n.value, C.byref(n)))
         return abi.contacts_to_numpy(buf, n.value)
+
+    def solver_stats(self) -> np.ndarray:
+        """Solver_step statistics of the last accepted step: neval, max_error, mean_error, total_mass,
+        max_mass."""
+        a = np.zeros(5)
+        _check(lib().mel_get_solver_stats(self.h, _ptr(a)))
+        return a
 
     def contact_pressures(self) -> np.ndarray:
         """(n_border_nodes, 2): x and y contact pressure of every border entry after the last step."""

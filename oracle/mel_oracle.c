@@ -1929,6 +1929,11 @@ void orc_get_rigid(orc_model* m, double* rigid, double* rf)
     if (rigid) memcpy(rigid, m->rg, sizeof(double) * MEL_RIGID_NF * m->nb);
     if (rf) for (int b = 0; b < m->nb; b++) memcpy(rf + 12 * b, m->rf + 15 * b, 12 * sizeof(double));
 }
+void orc_set_time(orc_model* m, double time, double dt, double next_contact_update)
+{
+    m->time = time; m->dt = dt; m->next_cup = next_contact_update;
+}
+
 void orc_set_rigid(orc_model* m, const double* rigid)
 {
     memcpy(m->rg, rigid, sizeof(double) * MEL_RIGID_NF * m->nb);

@@ -37,6 +37,8 @@ int  orc_get_neighbours(orc_model* m, int* rows, int cap);
 /* counts Closest_2_segment calls that left the shape weights unset (stale values reused,
  * Code/Body.h:1347 declares them outside the contact loop) */
 long orc_stale_shape_events(orc_model* m);
+/* Time, Deltat and Next_contact_update (restart) */
+void orc_set_time(orc_model* m, double time, double dt, double next_contact_update);
 /* border contact pressures x, y per border entry (Update_contact_pressures, Code/Proximity.h:1014-1069) */
 void orc_get_contact_pressures(orc_model* m, double* px, double* py);
 /* Solver_step outputs of the last iteration: neval, max_error, mean_error, total_mass, max_mass */

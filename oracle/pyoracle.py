@@ -47,6 +47,7 @@ def lib():
         L.orc_stale_shape_events.argtypes = [vp]; L.orc_stale_shape_events.restype = C.c_long
         L.orc_solver_stats.argtypes = [vp, C.POINTER(C.c_double)]
         L.orc_get_contact_pressures.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_set_time.argtypes = [vp, C.c_double, C.c_double, C.c_double]
         L.orc_set_rsqrt_mode.argtypes = [C.c_int]
         _lib = L
     return _lib
@@ -165,6 +166,9 @@ class Oracle:
         m = abi.MelMonitor()
         self.L.orc_monitor(self.h, C.byref(m))
         return m
+
+    def set_time(self, time: float, dt: float, next_contact_update: float):
+        self.L.orc_set_time(self.h, float(time), float(dt), float(next_contact_update))
 
     def contact_pressures(self) -> np.ndarray:
         """(n_border_nodes, 2): x and y contact pressure of every border entry."""
