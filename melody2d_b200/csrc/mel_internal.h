@@ -28,7 +28,7 @@
 // device error words (mel_dev::err)
 enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3, MEL_E_CAPACITY = 4,
        MEL_E_NBR_NEED = 5, MEL_E_WAIT = 6, MEL_E_PRESSURE = 7, MEL_E_NWORDS = 8 };
-#define MEL_PRESSURE_CAP 32       // contact contributions one border entry's pressure gathers
+#define MEL_PRESSURE_CAP 64       // contact contributions one border entry's pressure gathers
 
 // Chunk image (all offsets in bytes from the image start, every section 16-byte aligned):
 //   header   int4 {ngp, ne, ntn, nroff}
@@ -146,6 +146,9 @@ struct mel_dev {
     // gathered (contact << 2 | role, at most MEL_PRESSURE_CAP) and the pressures
     int* cp_cnt; int* cp_item;
     double *cpx, *cpy;
+    // bound of the body kernel's pipeline waits (MEL_WAIT_NS; the environment variable
+    // MELGPU_WAIT_NS read by mel_create shortens it so that tests can make a wait give up)
+    unsigned long long wait_ns;
     // error words
     unsigned int* err;
 };

@@ -371,15 +371,25 @@ __device__ __forceinline__ unsigned long long global_ns()
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// wait for phase `parity` of `bar` to complete; gives up after MEL_WAIT_NS
-__device__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity)
+// wait for phase `parity` of `bar` to complete; gives up after `limit_ns` (the pipeline's waits use
+// mel_dev::wait_ns, MEL_WAIT_NS unless a test shortens it; the final wait for copies in flight
+// always allows MEL_WAIT_NS)
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, unsigned parity)
 {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned long long limit_ns = MEL_WAIT_NS)
+{
+    if (limit_ns == 0) return mbar_test_wait(bar, parity);     // no waiting at all (tests)
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (true) {
         for (int i = 0; i < 64; i++)
             if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > MEL_WAIT_NS) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 
@@ -675,7 +685,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
             const int st = k % MEL_STAGES;
             char* bk = region + st * d.img_cap;
             if (*s_abort) break;
-            if (!mbar_wait_bounded(&full[st], (unsigned)((k / MEL_STAGES) & 1))) {
+            if (!mbar_wait_bounded(&full[st], (unsigned)((k / MEL_STAGES) & 1), d.wait_ns)) {
                 atomicOr(&d.err[MEL_E_WAIT], 1u);
                 *s_abort = 1;
                 break;
@@ -706,7 +716,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         for (int k = 0; k < nch; k++) {
             const int st = k % MEL_STAGES;
             char* bk = region + st * d.img_cap;
-            const bool ok = !*s_abort && mbar_wait_bounded(&pointed[st], (unsigned)((k / MEL_STAGES) & 1));
+            const bool ok = !*s_abort && mbar_wait_bounded(&pointed[st], (unsigned)((k / MEL_STAGES) & 1), d.wait_ns);
             if (!ok && !*s_abort) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
             if (pull_group_any<32 * PLW>(!ok)) break;
             const int4 hdr = *reinterpret_cast<const int4*>(bk);
@@ -810,7 +820,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
             const int st = issued % MEL_STAGES;
             const mel_chunk c = d.chunk[ch0 + issued];
             if (*s_abort) break;
-            if (!mbar_wait_bounded(&empty[st], (unsigned)((issued / MEL_STAGES - 1) & 1))) {
+            if (!mbar_wait_bounded(&empty[st], (unsigned)((issued / MEL_STAGES - 1) & 1), d.wait_ns)) {
                 atomicOr(&d.err[MEL_E_WAIT], 1u);
                 *s_abort = 1;
                 break;

@@ -2,6 +2,7 @@
 // set-up of Code/main.cpp:104-127, advances the step loop of Code/main.cpp:141-196 and implements
 // the C ABI declared in include/melgpu.h.
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <cmath>
@@ -237,6 +238,12 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.xmin = d->period[0]; D.period = d->period[1] - d->period[0];
     D.gx = d->gravity[0]; D.gy = d->gravity[1];
     D.precision = h->precision;
+    D.wait_ns = MEL_WAIT_NS;
+    if (const char* w = getenv("MELGPU_WAIT_NS")) {       // test knob: shorter pipeline waits
+        char* end = nullptr;
+        const unsigned long long v = strtoull(w, &end, 10);
+        if (end && *end == 0 && v < MEL_WAIT_NS) D.wait_ns = v;
+    }
     // time
     double t2[2] = { d->time, d->time };
     D.time2 = dupload(h, t2, 2);
@@ -624,8 +631,7 @@ static mel_status check_errors(mel_handle* h)
     unsigned w[MEL_E_NWORDS];
     if (cudaMemcpy(w, h->d.err, sizeof w, cudaMemcpyDeviceToHost) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "err", __FILE__, __LINE__); return MEL_ERR_CUDA; }
     if (w[MEL_E_BOUNDS]) { mel_set_error("device index check failed (code %u)", w[MEL_E_BOUNDS]); return MEL_ERR_BOUNDS; }
-    if (w[MEL_E_WAIT]) { mel_set_error("a shared-memory bulk copy did not complete within %llu ns", MEL_WAIT_NS); return MEL_ERR_TIMEOUT; }
-    if (w[MEL_E_PRESSURE]) { mel_set_error("a border entry gathers more than %d contact contributions to its pressure", MEL_PRESSURE_CAP); return MEL_ERR_BOUNDS; }
+    if (w[MEL_E_WAIT]) { mel_set_error("a wait of the body kernel's pipeline gave up after %llu ns", h->d.wait_ns); return MEL_ERR_TIMEOUT; }
     return MEL_OK;
 }
 
@@ -869,6 +875,7 @@ static mel_status adaptive_step(mel_handle* h)
 static void update_pressures(mel_handle* h)
 {
     if (h->pressure_state != 1) return;
+    cudaMemsetAsync(h->d.err + MEL_E_PRESSURE, 0, sizeof(unsigned), h->stream);
     mel_launch_contact_pressures(h->d, h->stream);
     h->launches += 3;
     h->pressure_state = 0;
@@ -1298,6 +1305,14 @@ mel_status mel_get_contact_pressures(mel_handle* h, double* px, double* py)
     if (h->ne > 0) {
         if (px) MEL_CUDA_OK(cudaMemcpy(px, h->d.cpx, sizeof(double) * (size_t)h->ne, cudaMemcpyDeviceToHost));
         if (py) MEL_CUDA_OK(cudaMemcpy(py, h->d.cpy, sizeof(double) * (size_t)h->ne, cudaMemcpyDeviceToHost));
+    }
+    // an output-only quantity: an entry with more contributions than the gather holds fails this
+    // call (its pressure would be incomplete), never a step
+    unsigned w[MEL_E_NWORDS];
+    MEL_CUDA_OK(cudaMemcpy(w, h->d.err, sizeof w, cudaMemcpyDeviceToHost));
+    if (w[MEL_E_PRESSURE]) {
+        mel_set_error("a border entry gathers more than %d contact contributions to its pressure", MEL_PRESSURE_CAP);
+        return MEL_ERR_BOUNDS;
     }
     return check_errors(h);
 }
