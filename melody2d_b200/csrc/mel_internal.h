@@ -163,6 +163,8 @@ void mel_launch_body_adaptive(const mel_dev& d, double T0, double Tf, int nblock
 // Solver_step's error and mass sums over the bodies in order (Code/Solver.h:289-331): out =
 // {mean_error, max_error, total_mass, max_mass}
 void mel_launch_error_reduce(const mel_dev& d, double* out, cudaStream_t s);
+// Update_bc(T) of every body's driven degrees of freedom (mel_dev::drv)
+void mel_launch_drivendof(const mel_dev& d, double T, cudaStream_t s);
 // Body::Restore of the rigid bodies' kinematics from a copy of the rigid records
 void mel_launch_rigid_restore(const mel_dev& d, const double* rg_snap, cudaStream_t s);
 // one step of a batch: the contact pass over thr0[nsamp] threads, the body pass over cta0[nsamp]

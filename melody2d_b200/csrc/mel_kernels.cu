@@ -1576,6 +1576,20 @@ __global__ void rigid_restore_kernel(mel_dev d, const double* rg_snap)
 }
 }  // namespace mel
 
+namespace mel {
+// Update_bc(Time) of every body's driven borders (the set-up call of Code/main.cpp:104-127)
+__global__ void drivendof_kernel(mel_dev d, double T)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < d.nb) body_drivendof(d, b, T, d.drv + 8 * (size_t)b);
+}
+}  // namespace mel
+
+void mel_launch_drivendof(const mel_dev& d, double T, cudaStream_t s)
+{
+    mel::drivendof_kernel<<<(d.nb + 127) / 128, 128, 0, s>>>(d, T);
+}
+
 void mel_launch_rigid_restore(const mel_dev& d, const double* rg_snap, cudaStream_t s)
 {
     mel::rigid_restore_kernel<<<(d.nb + 127) / 128, 128, 0, s>>>(d, rg_snap);

@@ -662,6 +662,8 @@ static mel_status setup(mel_handle* h)
     // rigid nodes take their positions from the body state
     std::vector<double> st(12 * (size_t)h->nn, 0.);
     mel_status rc = MEL_OK;
+    mel_launch_drivendof(h->d, h->time, h->stream);     // Update_bc(Time): the first half-step of
+                                                         // Solver_step moves driven bodies with these
     update_borders_only(h);
     if ((rc = proximity(h))) return rc;
     if (h->flags[3] == 1) {
@@ -1223,6 +1225,9 @@ mel_status mel_set_time(mel_handle* h, double time, double dt, double next_conta
     cudaStreamSynchronize(h->stream);
     h->time = time; h->dt = dt; h->next_cup = next_contact_update;
     h->t_bc = time;
+    mel_launch_drivendof(h->d, time, h->stream);
+    MEL_CUDA_OK(cudaGetLastError());
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
     double t2[2] = { time, time };
     MEL_CUDA_OK(cudaMemcpy(h->d.time2, t2, sizeof t2, cudaMemcpyHostToDevice));
     MEL_CUDA_OK(cudaMemcpy(h->d.dt, &dt, sizeof dt, cudaMemcpyHostToDevice));
