@@ -38,19 +38,30 @@ slot_plan plan_slots(const int* ns, int n)
         const int r0 = (int)P.roff.size();
         for (int j = 0; j < m; j++) { P.first_row[s0 + j] = r0; P.lane[s0 + j] = j; }
         for (int k = 0; k < K; k++) {
+            // every row of a group is m wide: slots with fewer supports are padded (zero
+            // derivatives, node 0), so that entry k of lane j sits at base + m k + (j ^ swizzle)
+            // and the kernel computes every position instead of reading a row table
             P.roff.push_back(P.entries);
-            int mk = 0;                             // slots with more than k supports: a prefix
-            while (mk < m && ns[P.order[s0 + mk]] > k) mk++;
             // rows whose width is a multiple of 8 rotate the lanes' bank groups from row to row
             // (lane ^ (k & 7) stays inside its aligned block of 8, so the row stays a permutation
             // of consecutive entries); otherwise all entries of a point would share one bank
             // group, and the pull, whose lanes read entries of points shared by nearby nodes,
             // would meet them in the same bank
-            P.rsw.push_back(mk % 8 == 0 ? (k & 7) : 0);
-            P.entries += mk;
+            P.rsw.push_back(m % 8 == 0 ? (k & 7) : 0);
+            P.entries += m;
         }
     }
     return P;
+}
+
+// stored entries of points with supports ns[0..n) once the groups are padded to their widest slot
+int padded_entries(const int* ns, int n)
+{
+    std::vector<int> v(ns, ns + n);
+    std::sort(v.begin(), v.end(), std::greater<int>());
+    int e = 0;
+    for (int s0 = 0; s0 < n; s0 += 32) e += std::min(32, n - s0) * v[s0];
+    return e;
 }
 
 // rows of all row tables of points with supports ns[0..n)
@@ -94,6 +105,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 if (c > 255 || c <= 0) { mel_set_error("Gauss point %d has %d supports (1..255 supported)", g + ngp, c); return MEL_ERR_UNSUPPORTED; }
                 if (nent + c > ecap) break;
                 ns.push_back(c);
+                if (padded_entries(ns.data(), ngp + 1) > ecap) { ns.pop_back(); break; }
                 nsmax = std::max(nsmax, c);
                 // row tables are addressed with 10 bits; the exact count is needed only when the
                 // bound (groups x largest count) could exceed that
@@ -123,7 +135,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
             std::sort(tp.begin(), tp.end());
             // touched nodes: (first entry in tp, count), then pull slots sorted by count
             std::vector<std::pair<int, int>> tnodes;
-            for (int q = 0; q < P.entries; q++)
+            for (int q = 0; q < (int)tp.size(); q++)
                 if (q == 0 || (tp[q].first >> 32) != (tp[q - 1].first >> 32)) tnodes.push_back({ q, 1 });
                 else tnodes.back().second++;
             std::stable_sort(tnodes.begin(), tnodes.end(),
@@ -154,7 +166,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 }
             }
             const int nroff = (int)roff_all.size();
-            if (nroff > 4095 || pe != P.entries) {
+            if (nroff > 4095 || pe != nent) {
                 mel_set_error("chunk row tables too large (%d rows)", nroff);
                 return MEL_ERR_UNSUPPORTED;
             }
@@ -190,7 +202,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
             for (int r = 0; r < nroff; r++) roff[r] = (uint16_t)(roff_all[r] | (rsw_all[r] << 12));
             out.img_max = std::max(out.img_max, ch.bytes);
             out.n_entries += ch.ne;
-            out.n_pad += ch.ne - P.entries;
+            out.n_pad += ch.ne - nent;
             out.chunks.push_back(ch);
             g += ngp;
         }

@@ -11,11 +11,13 @@
 #include "melgpu.h"
 
 #define MEL_BODY_THREADS 256      // threads per body CTA: point warps, pull warps, warp 7 (copies, contacts)
-#define MEL_STAGES 3              // chunk buffers in the body kernel's ring
-#define MEL_PT_WARPS(mx) ((mx) ? 4 : 3)   // point warps of the FP64 / mixed body kernel (the rest of 0-6 pull)
-#define MEL_CHUNK_GP_FP64 96      // Gauss points per chunk: one point thread each
+// The FP64 body kernel: warps 0-6 run each chunk's Gauss-point pass and then its pull, over two
+// chunk buffers.  The mixed kernel: a pipeline of point warps, pull warps and a copy warp over a
+// ring of three buffers.
+#define MEL_STAGES(mx) ((mx) ? 3 : 2)     // chunk buffers
+#define MEL_PT_WARPS_MX 4                 // point warps of the mixed pipeline (warps 4-6 pull)
+#define MEL_CHUNK_GP_FP64 224     // Gauss points per chunk: one point thread each
 #define MEL_CHUNK_GP_MX 128
-#define MEL_CHUNK_GP_MAX 128
 #define MEL_BAR_BYTES 128         // the ring's mbarriers (3 per stage) and the abort flag
 #define MEL_CHUNK_E_MAX 2048      // support entries per chunk, upper bound (the host may choose less)
 #define MEL_WAIT_NS 1000000000ull // bound of every device-side wait (1 s)

@@ -350,6 +350,9 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 }
 // generic-proxy accesses to a buffer are ordered before the bulk copy that refills it
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+#define MEL_BODY_CTHREADS 224     // the FP64 kernel's Gauss-point warps (0-6); warp 7 scatters contacts
+// barrier of the FP64 kernel's Gauss-point warps only (warp 7 runs the contact scatter meanwhile)
+__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, %0;" :: "n"(MEL_BODY_CTHREADS) : "memory"); }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
@@ -409,41 +412,42 @@ __device__ __forceinline__ double ordered_sum(double acc, const double* t, int n
     return acc;
 }
 
-// position of the entry of `lane` in a row whose table value is r (offset | swizzle << 12)
-__device__ __forceinline__ int mel_entry(unsigned r, int lane) { return (int)(r & 0xfffu) + (lane ^ (int)(r >> 12)); }
-
 // Gauss-point pass of one chunk held in shared memory (Body::Update_internal_forces,
 // Code/Body.h:960-1050): thread `t` < ngp forms the strain of its point from the staged dN and
 // the body's displacements (supports in the point's own order), applies the material and
-// overwrites its dN pairs with the contributions c0 * B^T.sigma.  Entry k of slot t sits at
-// mel_entry(row[k], lane) (row layout: the lanes of a warp touch a permutation of consecutive
-// entries).
+// overwrites its dN pairs with the contributions c0 * B^T.sigma.  The slot's group of m slots
+// stores row k of all its slots at base + m k (rows padded to the group's largest point with zero
+// derivatives on node 0), lane j's entry at j ^ (k & 7) in rows whose width is a multiple of 8:
+// every position is computed, so a support's loads depend on nothing but its own index.
+struct mel_rows { int base, m, sw, lane, ns; };
+__device__ __forceinline__ mel_rows point_rows(int t, int ngp, const unsigned* s_gpm, const uint16_t* s_roff)
+{
+    const unsigned gm = s_gpm[t];
+    mel_rows R;
+    R.base = (int)(s_roff[gm & 0x3ffu] & 0xfffu);
+    R.m = min(32, ngp - (t & ~31));
+    R.sw = (R.m & 7) == 0 ? 7 : 0;
+    R.lane = (int)((gm >> 10) & 0x1fu);
+    R.ns = (int)(gm >> 15);
+    return R;
+}
+#define E(k) (R.base + R.m * (k) + (R.lane ^ ((k) & R.sw)))
+
 __device__ __forceinline__ void chunk_points(int t, int ngp, int mtype, double Mu, double Lam, const double2* s_up,
                                              double2* s_p, const uint16_t* s_idx, const double* s_c0,
                                              const unsigned* s_gpm, const uint16_t* s_roff)
 {
-    const unsigned gm = s_gpm[t];
-    const uint16_t* row = s_roff + (gm & 0x3ffu);          // row table of the slot's group
-    const int lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
+    const mel_rows R = point_rows(t, ngp, s_gpm, s_roff);
+    const int ns = R.ns;
     const double c0 = s_c0[t];
-    // rows that every slot of a full group has are 32 wide and contiguous: their positions follow
-    // from the group's first row without a table load (swizzle k & 7)
-    const int nfull = (t | 31) < ngp ? (int)(s_gpm[t | 31] >> 15) : 0;
-    const int base = (int)(row[0] & 0xfffu);
-#define E(k) ((k) < nfull ? base + 32 * (k) + (lane ^ ((k) & 7)) : mel_entry(row[(k)], lane))
     if (mtype == MEL_MAT_ELASTIC_LINEAR) {
-        // strain sums in support order; loads issued eight supports ahead of the adds.  Rows below
-        // nfull are addressed without the row table (k is a multiple of 8 there, so the swizzle
-        // of row k + j is j).
+        // strain sums in support order; loads issued eight supports ahead of the adds
         double E11 = 0., E12 = 0., E22 = 0.;
         int k = 0;
-        for (; k + 8 <= nfull; k += 8) {
+        for (; k + 8 <= ns; k += 8) {
             double2 dN[8], u[8];
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int e = base + 32 * (k + j) + (lane ^ j);
-                dN[j] = s_p[e]; u[j] = s_up[s_idx[e]];
-            }
+            for (int j = 0; j < 8; j++) { const int e = E(k + j); dN[j] = s_p[e]; u[j] = s_up[s_idx[e]]; }
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 E11 = E11 + dN[j].x * u[j].x;
@@ -451,43 +455,26 @@ __device__ __forceinline__ void chunk_points(int t, int ngp, int mtype, double M
                 E22 = E22 + dN[j].y * u[j].y;
             }
         }
-        for (; k + 4 <= ns; k += 4) {
-            double2 dN[4], u[4];
+        if (k < ns) {                   // the last rows: loads of up to eight issued together
+            double2 dN[8], u[8];
 #pragma unroll
-            for (int j = 0; j < 4; j++) { dN[j] = s_p[E(k + j)]; u[j] = s_up[s_idx[E(k + j)]]; }
+            for (int j = 0; j < 8; j++)
+                if (k + j < ns) { const int e = E(k + j); dN[j] = s_p[e]; u[j] = s_up[s_idx[e]]; }
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                E11 = E11 + dN[j].x * u[j].x;
-                E12 = E12 + (dN[j].x * u[j].y + dN[j].y * u[j].x);
-                E22 = E22 + dN[j].y * u[j].y;
-            }
-        }
-        for (; k < ns; k++) {
-            double2 dN = s_p[E(k)];
-            double2 u = s_up[s_idx[E(k)]];
-            E11 = E11 + dN.x * u.x;
-            E12 = E12 + (dN.x * u.y + dN.y * u.x);
-            E22 = E22 + dN.y * u.y;
+            for (int j = 0; j < 8; j++)
+                if (k + j < ns) {
+                    E11 = E11 + dN[j].x * u[j].x;
+                    E12 = E12 + (dN[j].x * u[j].y + dN[j].y * u[j].x);
+                    E22 = E22 + dN[j].y * u[j].y;
+                }
         }
         E12 = 0.5 * E12;
         double J = 1. + E11 + E22;               // Apply_Elastic_Linear (Code/Model.h:19-29)
         double S33 = Lam * (J - 1.);
         double Mu2 = 2 * Mu;
         double S11 = S33 + Mu2 * E11, S22 = S33 + Mu2 * E22, S12 = Mu2 * E12;
-        int k2 = 0;
-        for (; k2 + 8 <= nfull; k2 += 8) {
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int e = base + 32 * (k2 + j) + (lane ^ j);
-                const double2 dN = s_p[e];
-                double2 q;
-                q.x = c0 * (dN.x * S11 + dN.y * S12);
-                q.y = c0 * (dN.y * S22 + dN.x * S12);
-                s_p[e] = q;
-            }
-        }
-#pragma unroll 4
-        for (; k2 < ns; k2++) {
+#pragma unroll 8
+        for (int k2 = 0; k2 < ns; k2++) {
             const int e = E(k2);
             const double2 dN = s_p[e];
             double2 q;
@@ -532,22 +519,16 @@ __device__ __forceinline__ void chunk_points_mx(int t, int ngp, int mtype, float
                                                 float2* s_p, const uint16_t* s_idx, const double* s_c0,
                                                 const unsigned* s_gpm, const uint16_t* s_roff)
 {
-    const unsigned gm = s_gpm[t];
-    const uint16_t* row = s_roff + (gm & 0x3ffu);
-    const int lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
+    const mel_rows R = point_rows(t, ngp, s_gpm, s_roff);
+    const int ns = R.ns;
     const float c0 = (float)s_c0[t];
-    const int nfull = (t | 31) < ngp ? (int)(s_gpm[t | 31] >> 15) : 0;   // as in chunk_points
-    const int base = (int)(row[0] & 0xfffu);
     if (mtype == MEL_MAT_ELASTIC_LINEAR) {
         float E11 = 0.f, E12 = 0.f, E22 = 0.f;
         int k = 0;
-        for (; k + 8 <= nfull; k += 8) {
+        for (; k + 8 <= ns; k += 8) {
             float2 dN[8], u[8];
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int e = base + 32 * (k + j) + (lane ^ j);
-                dN[j] = s_p[e]; u[j] = s_upf[s_idx[e]];
-            }
+            for (int j = 0; j < 8; j++) { const int e = E(k + j); dN[j] = s_p[e]; u[j] = s_upf[s_idx[e]]; }
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 E11 = __fmaf_rn(dN[j].x, u[j].x, E11);
@@ -555,30 +536,25 @@ __device__ __forceinline__ void chunk_points_mx(int t, int ngp, int mtype, float
                 E22 = __fmaf_rn(dN[j].y, u[j].y, E22);
             }
         }
-#pragma unroll 4
-        for (; k < ns; k++) {
-            const int e = E(k);
-            const float2 dN = s_p[e];
-            const float2 u = s_upf[s_idx[e]];
-            E11 = __fmaf_rn(dN.x, u.x, E11);
-            E12 = __fmaf_rn(dN.x, u.y, __fmaf_rn(dN.y, u.x, E12));
-            E22 = __fmaf_rn(dN.y, u.y, E22);
+        if (k < ns) {
+            float2 dN[8], u[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if (k + j < ns) { const int e = E(k + j); dN[j] = s_p[e]; u[j] = s_upf[s_idx[e]]; }
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if (k + j < ns) {
+                    E11 = __fmaf_rn(dN[j].x, u[j].x, E11);
+                    E12 = __fmaf_rn(dN[j].x, u[j].y, __fmaf_rn(dN[j].y, u[j].x, E12));
+                    E22 = __fmaf_rn(dN[j].y, u[j].y, E22);
+                }
         }
         E12 = 0.5f * E12;
         const float S33 = Lam * (E11 + E22);      // Apply_Elastic_Linear (Code/Model.h:19-29), J - 1 = tr E
         const float Mu2 = 2.f * Mu;
         const float S11 = __fmaf_rn(Mu2, E11, S33), S22 = __fmaf_rn(Mu2, E22, S33), S12 = Mu2 * E12;
-        int k2 = 0;
-        for (; k2 + 8 <= nfull; k2 += 8) {
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int e = base + 32 * (k2 + j) + (lane ^ j);
-                const float2 dN = s_p[e];
-                s_p[e] = make_float2(c0 * __fmaf_rn(dN.x, S11, dN.y * S12), c0 * __fmaf_rn(dN.y, S22, dN.x * S12));
-            }
-        }
-#pragma unroll 4
-        for (; k2 < ns; k2++) {
+#pragma unroll 8
+        for (int k2 = 0; k2 < ns; k2++) {
             const int e = E(k2);
             const float2 dN = s_p[e];
             s_p[e] = make_float2(c0 * __fmaf_rn(dN.x, S11, dN.y * S12), c0 * __fmaf_rn(dN.y, S22, dN.x * S12));
@@ -637,228 +613,423 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
     double2* s_f = s_up + n;
     double2* s_fc = s_f + n;
     float2* s_upf = reinterpret_cast<float2*>(s_fc + n);
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
-                                                     : reinterpret_cast<char*>(s_fc + n));
-    // stage s of the ring: full[s] (the bulk copy landed), pointed[s] (every point thread has
-    // written its contributions), empty[s] (every pull thread is done with the buffer)
-    uint64_t* full = s_bar;
-    uint64_t* pointed = s_bar + MEL_STAGES;
-    uint64_t* empty = s_bar + 2 * MEL_STAGES;
-    volatile int* s_abort = reinterpret_cast<volatile int*>(s_bar + 3 * MEL_STAGES);
-    char* region = reinterpret_cast<char*>(s_bar) + MEL_BAR_BYTES;
-    constexpr int PTW = MEL_PT_WARPS(MX);                 // point warps 0 .. PTW-1
-    constexpr int PLW = 7 - PTW;                          // pull warps PTW .. 6; warp 7 copies and scatters
-    const int ch0 = d.b_chunk0[b];
-    const int nch = d.b_chunk0[b + 1] - ch0;
-    for (int i = tid; i < n; i += blockDim.x) {
-        s_up[i] = d.up[n0 + i];
-        s_f[i] = make_double2(0., 0.);
-        s_fc[i] = make_double2(0., 0.);
-    }
-    if (MX) {
-        const double2 u0 = d.up[n0];
+    // the chunk loop, which leaves the internal forces in s_f and the contact forces in s_fc
+    char* region;
+    volatile int* s_abort;
+    if (!MX) {
+        uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
+                                                         : reinterpret_cast<char*>(s_fc + n));
+        s_abort = reinterpret_cast<volatile int*>(s_bar + 2);
+        region = reinterpret_cast<char*>(s_bar) + MEL_BAR_BYTES;
+        char* const buf0 = region;
+        char* const buf1 = region + d.img_cap;
+        const int ch0 = d.b_chunk0[b];
+        const int nch = d.b_chunk0[b + 1] - ch0;
         for (int i = tid; i < n; i += blockDim.x) {
-            const double2 u = d.up[n0 + i];
-            s_upf[i] = make_float2((float)(u.x - u0.x), (float)(u.y - u0.y));
+            s_up[i] = d.up[n0 + i];
+            s_f[i] = make_double2(0., 0.);
+            s_fc[i] = make_double2(0., 0.);
         }
-    }
-    if (tid == 0) {
-        for (int st = 0; st < MEL_STAGES; st++) {
-            mbar_init(&full[st], 1);
-            mbar_init(&pointed[st], 32 * PTW);
-            mbar_init(&empty[st], 32 * PLW);
-        }
-        mbar_init_fence();
-        *s_abort = 0;
-    }
-    __syncthreads();
-    // ---- Update_internal_forces as a pipeline over the body's chunks: warp 7 streams chunk images
-    // into a ring of MEL_STAGES buffers, the point warps form strain, stress and contributions of
-    // chunk k while the pull warps add those of chunk k-1 to the nodes (in ascending point order,
-    // chunk after chunk), so the two ordered chains and the copies overlap --------------------------
-    const int mat = d.b_mat[b];
-    const int mtype = d.mat_type[mat];
-    const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
-    const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
-    if (warp < PTW) {
-        for (int k = 0; k < nch; k++) {
-            const int st = k % MEL_STAGES;
-            char* bk = region + st * d.img_cap;
-            if (*s_abort) break;
-            if (!mbar_wait_bounded(&full[st], (unsigned)((k / MEL_STAGES) & 1), d.wait_ns)) {
-                atomicOr(&d.err[MEL_E_WAIT], 1u);
-                *s_abort = 1;
-                break;
+        if (MX) {
+            const double2 u0 = d.up[n0];
+            for (int i = tid; i < n; i += blockDim.x) {
+                const double2 u = d.up[n0 + i];
+                s_upf[i] = make_float2((float)(u.x - u0.x), (float)(u.y - u0.y));
             }
-            const int4 hdr = *reinterpret_cast<const int4*>(bk);
-            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
-            if (tid < hdr.x) {
-                if (MX)
-                    chunk_points_mx(tid, hdr.x, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN),
-                                    reinterpret_cast<const uint16_t*>(bk + L.idx), reinterpret_cast<const double*>(bk + L.c0),
-                                    reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
-                else
-                    chunk_points(tid, hdr.x, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN),
-                                 reinterpret_cast<const uint16_t*>(bk + L.idx), reinterpret_cast<const double*>(bk + L.c0),
-                                 reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
-            }
-            fence_proxy_async();      // these generic writes precede the copy that will refill the buffer
-            mbar_arrive(&pointed[st]);
         }
-    } else if (warp < 7) {
-        // pull: each touched node subtracts its contributions in ascending Gauss-point order (the
-        // mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31 of group
-        // t >> 5, its entry j at row j of the group's row table.  Groups are sorted by entry count;
-        // pull warp w takes groups w, 2 PLW - 1 - w, 2 PLW + w, ... (snake order).  The group's
-        // barrier at the top of every chunk keeps a node's chunks in order when different warps
-        // hold it, and makes the group leave together when a wait gives up.
-        const int w = warp - PTW;
-        for (int k = 0; k < nch; k++) {
-            const int st = k % MEL_STAGES;
-            char* bk = region + st * d.img_cap;
-            const bool ok = !*s_abort && mbar_wait_bounded(&pointed[st], (unsigned)((k / MEL_STAGES) & 1), d.wait_ns);
-            if (!ok && !*s_abort) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
-            if (pull_group_any<32 * PLW>(!ok)) break;
-            const int4 hdr = *reinterpret_cast<const int4*>(bk);
-            const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
-            const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
-            const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
-            const uint16_t* s_roff = reinterpret_cast<const uint16_t*>(bk + L.roff);
-            const int ngrp = (hdr.z + 31) >> 5;
-            for (int i = 0; PLW * i < ngrp; i++) {
-                const int t = (PLW * i + ((i & 1) ? PLW - 1 - w : w)) * 32 + lane;
-                if (t >= hdr.z) continue;
-                const unsigned rec = s_tn[t];
-                const int node = (int)(rec & 0xfffu);
-                const int cnt = (int)((rec >> 12) & 0xffu);
-                const uint16_t* prow = s_roff + (rec >> 20);
-                // rows every slot of a full group has: 32 wide and contiguous
-                const int pfull = (t | 31) < hdr.z ? (int)((s_tn[t | 31] >> 12) & 0xffu) : 0;
-                const int pbase = prow[0];
-#define PQ(j) ((j) < pfull ? pbase + 32 * (j) + lane : prow[(j)] + lane)
-                double2 f = s_f[node];
-                int j = 0;
-                if (MX) {
-                    const float2* s_q = reinterpret_cast<const float2*>(bk + L.dN);
-                    for (; j + 8 <= pfull; j += 8) {
-                        float2 c[8];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[pbase + 32 * (j + i) + lane]];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
-                    }
-                    for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
-                        int q[8];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
-                        float2 c[8];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[q[i]]];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
-                    }
-                    for (; j + 4 <= cnt; j += 4) {
-                        float2 c[4];
-#pragma unroll
-                        for (int i = 0; i < 4; i++) c[i] = s_q[s_tpos[PQ(j + i)]];
-#pragma unroll
-                        for (int i = 0; i < 4; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
-                    }
-                    for (; j < cnt; j++) {
-                        const float2 c = s_q[s_tpos[PQ(j)]];
-                        f.x = f.x - (double)c.x;
-                        f.y = f.y - (double)c.y;
-                    }
-                } else {
-                    const double2* s_p = reinterpret_cast<const double2*>(bk + L.dN);
-                    for (; j + 8 <= pfull; j += 8) {
-                        double2 c[8];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[pbase + 32 * (j + i) + lane]];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
-                    }
-                    for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
-                        int q[8];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
-                        double2 c[8];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[q[i]]];
-#pragma unroll
-                        for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
-                    }
-                    for (; j + 4 <= cnt; j += 4) {
-                        double2 c[4];
-#pragma unroll
-                        for (int i = 0; i < 4; i++) c[i] = s_p[s_tpos[PQ(j + i)]];
-#pragma unroll
-                        for (int i = 0; i < 4; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
-                    }
-                    for (; j < cnt; j++) {
-                        const double2 c = s_p[s_tpos[PQ(j)]];
-                        f.x = f.x - c.x;
-                        f.y = f.y - c.y;
-                    }
+        if (tid == 0) {
+            mbar_init(&s_bar[0], 1);
+            mbar_init(&s_bar[1], 1);
+            mbar_init_fence();
+            *s_abort = 0;
+        }
+        __syncthreads();
+        if (warp < MEL_BODY_CTHREADS / 32) {
+            // ---- Update_internal_forces: chunk k is computed while chunk k+1 is in flight ----------
+            const int mat = d.b_mat[b];
+            const int mtype = d.mat_type[mat];
+            const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
+            const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
+            int issued = 0;
+            if (tid == 0)
+                for (; issued < 2 && issued < nch; issued++) {
+                    const mel_chunk c = d.chunk[ch0 + issued];
+                    mbar_arrive_expect_tx(&s_bar[issued], (unsigned)c.bytes);
+                    bulk_load(issued ? buf1 : buf0, d.img + c.img, (unsigned)c.bytes, &s_bar[issued]);
                 }
-#undef PQ
-                s_f[node] = f;
+            int k = 0;
+            for (; k < nch; k++) {
+                const int sel = k & 1;
+                char* bk = sel ? buf1 : buf0;
+                long long nxt_img = 0;
+                int nxt_bytes = 0;
+                if (tid == 0 && k + 2 < nch) { const mel_chunk c = d.chunk[ch0 + k + 2]; nxt_img = c.img; nxt_bytes = c.bytes; }
+                const bool ok = mbar_wait_bounded(&s_bar[sel], (unsigned)((k >> 1) & 1), d.wait_ns);
+                if (!ok) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
+                const int4 hdr = ok ? *reinterpret_cast<const int4*>(bk) : make_int4(0, 0, 0, 0);
+                const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
+                const uint16_t* s_idx = reinterpret_cast<const uint16_t*>(bk + L.idx);
+                const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
+                const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
+                const uint16_t* s_roff = reinterpret_cast<const uint16_t*>(bk + L.roff);
+                if (tid < hdr.x) {
+                    if (MX)
+                        chunk_points_mx(tid, hdr.x, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN), s_idx,
+                                        reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
+                                        reinterpret_cast<const uint16_t*>(bk + L.roff));
+                    else
+                        chunk_points(tid, hdr.x, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN), s_idx,
+                                     reinterpret_cast<const double*>(bk + L.c0), reinterpret_cast<const unsigned*>(bk + L.gpm),
+                                     reinterpret_cast<const uint16_t*>(bk + L.roff));
+                }
+                compute_sync();
+                if (*s_abort) break;
+                // pull: each touched node subtracts its contributions in ascending Gauss-point order
+                // (the mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31
+                // of group t >> 5, its entry j at row j of the group's row table.  Groups are sorted
+                // by entry count; warp w takes groups w, 13 - w, 14 + w, ... (snake order), so the
+                // heaviest group has a warp to itself and the lighter ones pair up.
+                const int ngrp = (hdr.z + 31) >> 5;
+                for (int i = 0; 7 * i < ngrp; i++) {
+                    const int t = (7 * i + ((i & 1) ? 6 - warp : warp)) * 32 + lane;
+                    if (t >= hdr.z) continue;
+                    const unsigned rec = s_tn[t];
+                    const int node = (int)(rec & 0xfffu);
+                    const int cnt = (int)((rec >> 12) & 0xffu);
+                    const uint16_t* prow = s_roff + (rec >> 20);
+                    // rows every slot of a full group has: 32 wide and contiguous
+                    const int pfull = (t | 31) < hdr.z ? (int)((s_tn[t | 31] >> 12) & 0xffu) : 0;
+                    const int pbase = prow[0];
+    #define PQ(j) ((j) < pfull ? pbase + 32 * (j) + lane : prow[(j)] + lane)
+                    double2 f = s_f[node];
+                    int j = 0;
+                    if (MX) {
+                        const float2* s_q = reinterpret_cast<const float2*>(bk + L.dN);
+                        for (; j + 8 <= pfull; j += 8) {
+                            float2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[pbase + 32 * (j + i) + lane]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                        }
+                        for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
+                            int q[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
+                            float2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[q[i]]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                        }
+                        for (; j + 4 <= cnt; j += 4) {
+                            float2 c[4];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) c[i] = s_q[s_tpos[PQ(j + i)]];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                        }
+                        for (; j < cnt; j++) {
+                            const float2 c = s_q[s_tpos[PQ(j)]];
+                            f.x = f.x - (double)c.x;
+                            f.y = f.y - (double)c.y;
+                        }
+                    } else {
+                        const double2* s_p = reinterpret_cast<const double2*>(bk + L.dN);
+                        for (; j + 8 <= pfull; j += 8) {
+                            double2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[pbase + 32 * (j + i) + lane]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                        }
+                        for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
+                            int q[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
+                            double2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[q[i]]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                        }
+                        for (; j + 4 <= cnt; j += 4) {
+                            double2 c[4];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) c[i] = s_p[s_tpos[PQ(j + i)]];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                        }
+                        for (; j < cnt; j++) {
+                            const double2 c = s_p[s_tpos[PQ(j)]];
+                            f.x = f.x - c.x;
+                            f.y = f.y - c.y;
+                        }
+                    }
+    #undef PQ
+                    s_f[node] = f;
+                }
+                fence_proxy_async();
+                compute_sync();
+                if (tid == 0 && k + 2 < nch) {
+                    mbar_arrive_expect_tx(&s_bar[sel], (unsigned)nxt_bytes);
+                    bulk_load(bk, d.img + nxt_img, (unsigned)nxt_bytes, &s_bar[sel]);
+                    issued++;
+                }
             }
-            fence_proxy_async();
-            mbar_arrive(&empty[st]);
-        }
-    } else if (lane == 0) {
-        // ---- producer: the first MEL_STAGES chunks at once, then each chunk into the buffer the
-        // pull warps released ----------------------------------------------------------------------
-        int issued = 0;
-        for (; issued < MEL_STAGES && issued < nch; issued++) {
-            const mel_chunk c = d.chunk[ch0 + issued];
-            mbar_arrive_expect_tx(&full[issued], (unsigned)c.bytes);
-            bulk_load(region + issued * d.img_cap, d.img + c.img, (unsigned)c.bytes, &full[issued]);
-        }
-        for (; issued < nch; issued++) {
-            const int st = issued % MEL_STAGES;
-            const mel_chunk c = d.chunk[ch0 + issued];
-            if (*s_abort) break;
-            if (!mbar_wait_bounded(&empty[st], (unsigned)((issued / MEL_STAGES - 1) & 1), d.wait_ns)) {
-                atomicOr(&d.err[MEL_E_WAIT], 1u);
-                *s_abort = 1;
-                break;
-            }
-            mbar_arrive_expect_tx(&full[st], (unsigned)c.bytes);
-            bulk_load(region + st * d.img_cap, d.img + c.img, (unsigned)c.bytes, &full[st]);
-        }
-        if (*s_abort)   // give the copies still in flight a bounded time to land before the CTA ends
-            for (int c = issued - 1; c >= 0 && c >= issued - MEL_STAGES; c--)
-                mbar_wait_bounded(&full[c % MEL_STAGES], (unsigned)((c / MEL_STAGES) & 1));
-    } else {
-        // ---- contact forces (lanes 1-31 of warp 7, meanwhile): slave scatter in list order, then
-        // master scatter in send order (Body::Update_contact_forces, Code/Body.h:1642-1900) ---------
-        const unsigned mask = 0xfffffffeu;
-        for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
-            const mel_contact* ct = d.cont + c;
-            if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
-            double Fsx = ct->fx, Fsy = ct->fy;
-            warp_scatter(d, n0, ct->nodeS, Fsx, Fsy, s_fc, lane - 1, 31);
-            __syncwarp(mask);
-        }
-        for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
-            int2 rg = d.inc_rng[r];
-            for (int c = rg.x; c < rg.y; c++) {
+            if (tid == 0 && *s_abort)   // give the copies still in flight a bounded time to land
+                for (int c = k; c < issued; c++) mbar_wait_bounded(&s_bar[c & 1], (unsigned)((c >> 1) & 1));
+        } else {
+            // ---- contact forces (warp 7): slave scatter in list order, then master scatter in send
+            // order (Body::Update_contact_forces, Code/Body.h:1642-1900) ---------------------------
+            for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
                 const mel_contact* ct = d.cont + c;
-                if (d.table[d.b_mat[ct->bodyS] * d.nmat + d.b_mat[b]] <= -1) continue;
+                if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
                 double Fsx = ct->fx, Fsy = ct->fy;
-                for (int k = 0; k < 4; k++) {
-                    double sk = ct->shapeM[k];
-                    warp_scatter(d, n0, ct->nodeM[k], -Fsx * sk, -Fsy * sk, s_fc, lane - 1, 31);
-                    __syncwarp(mask);
+                warp_scatter(d, n0, ct->nodeS, Fsx, Fsy, s_fc, lane);
+                __syncwarp();
+            }
+            for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
+                int2 rg = d.inc_rng[r];
+                for (int c = rg.x; c < rg.y; c++) {
+                    const mel_contact* ct = d.cont + c;
+                    if (d.table[d.b_mat[ct->bodyS] * d.nmat + d.b_mat[b]] <= -1) continue;
+                    double Fsx = ct->fx, Fsy = ct->fy;
+                    for (int k = 0; k < 4; k++) {
+                        double sk = ct->shapeM[k];
+                        warp_scatter(d, n0, ct->nodeM[k], -Fsx * sk, -Fsy * sk, s_fc, lane);
+                        __syncwarp();
+                    }
                 }
             }
         }
+        __syncthreads();
+        if (*s_abort) return;
+    } else {
+        constexpr int NS = MEL_STAGES(1);
+        uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
+                                                         : reinterpret_cast<char*>(s_fc + n));
+        // stage s of the ring: full[s] (the bulk copy landed), pointed[s] (every point thread has
+        // written its contributions), empty[s] (every pull thread is done with the buffer)
+        uint64_t* full = s_bar;
+        uint64_t* pointed = s_bar + NS;
+        uint64_t* empty = s_bar + 2 * NS;
+        s_abort = reinterpret_cast<volatile int*>(s_bar + 3 * NS);
+        region = reinterpret_cast<char*>(s_bar) + MEL_BAR_BYTES;
+        constexpr int PTW = MEL_PT_WARPS_MX;                  // point warps 0 .. PTW-1
+        constexpr int PLW = 7 - PTW;                          // pull warps PTW .. 6; warp 7 copies and scatters
+        const int ch0 = d.b_chunk0[b];
+        const int nch = d.b_chunk0[b + 1] - ch0;
+        for (int i = tid; i < n; i += blockDim.x) {
+            s_up[i] = d.up[n0 + i];
+            s_f[i] = make_double2(0., 0.);
+            s_fc[i] = make_double2(0., 0.);
+        }
+        if (MX) {
+            const double2 u0 = d.up[n0];
+            for (int i = tid; i < n; i += blockDim.x) {
+                const double2 u = d.up[n0 + i];
+                s_upf[i] = make_float2((float)(u.x - u0.x), (float)(u.y - u0.y));
+            }
+        }
+        if (tid == 0) {
+            for (int st = 0; st < NS; st++) {
+                mbar_init(&full[st], 1);
+                mbar_init(&pointed[st], 32 * PTW);
+                mbar_init(&empty[st], 32 * PLW);
+            }
+            mbar_init_fence();
+            *s_abort = 0;
+        }
+        __syncthreads();
+        // ---- Update_internal_forces as a pipeline over the body's chunks: warp 7 streams chunk images
+        // into a ring of NS buffers, the point warps form strain, stress and contributions of
+        // chunk k while the pull warps add those of chunk k-1 to the nodes (in ascending point order,
+        // chunk after chunk), so the two ordered chains and the copies overlap --------------------------
+        const int mat = d.b_mat[b];
+        const int mtype = d.mat_type[mat];
+        const double Mu = d.mat_p[MEL_MAT_NPARAM * mat + 3];
+        const double Lam = d.mat_p[MEL_MAT_NPARAM * mat + 4];
+        if (warp < PTW) {
+            for (int k = 0; k < nch; k++) {
+                const int st = k % NS;
+                char* bk = region + st * d.img_cap;
+                if (*s_abort) break;
+                if (!mbar_wait_bounded(&full[st], (unsigned)((k / NS) & 1), d.wait_ns)) {
+                    atomicOr(&d.err[MEL_E_WAIT], 1u);
+                    *s_abort = 1;
+                    break;
+                }
+                const int4 hdr = *reinterpret_cast<const int4*>(bk);
+                const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
+                if (tid < hdr.x) {
+                    if (MX)
+                        chunk_points_mx(tid, hdr.x, mtype, (float)Mu, (float)Lam, s_upf, reinterpret_cast<float2*>(bk + L.dN),
+                                        reinterpret_cast<const uint16_t*>(bk + L.idx), reinterpret_cast<const double*>(bk + L.c0),
+                                        reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
+                    else
+                        chunk_points(tid, hdr.x, mtype, Mu, Lam, s_up, reinterpret_cast<double2*>(bk + L.dN),
+                                     reinterpret_cast<const uint16_t*>(bk + L.idx), reinterpret_cast<const double*>(bk + L.c0),
+                                     reinterpret_cast<const unsigned*>(bk + L.gpm), reinterpret_cast<const uint16_t*>(bk + L.roff));
+                }
+                fence_proxy_async();      // these generic writes precede the copy that will refill the buffer
+                mbar_arrive(&pointed[st]);
+            }
+        } else if (warp < 7) {
+            // pull: each touched node subtracts its contributions in ascending Gauss-point order (the
+            // mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31 of group
+            // t >> 5, its entry j at row j of the group's row table.  Groups are sorted by entry count;
+            // pull warp w takes groups w, 2 PLW - 1 - w, 2 PLW + w, ... (snake order).  The group's
+            // barrier at the top of every chunk keeps a node's chunks in order when different warps
+            // hold it, and makes the group leave together when a wait gives up.
+            const int w = warp - PTW;
+            for (int k = 0; k < nch; k++) {
+                const int st = k % NS;
+                char* bk = region + st * d.img_cap;
+                const bool ok = !*s_abort && mbar_wait_bounded(&pointed[st], (unsigned)((k / NS) & 1), d.wait_ns);
+                if (!ok && !*s_abort) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
+                if (pull_group_any<32 * PLW>(!ok)) break;
+                const int4 hdr = *reinterpret_cast<const int4*>(bk);
+                const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
+                const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
+                const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
+                const uint16_t* s_roff = reinterpret_cast<const uint16_t*>(bk + L.roff);
+                const int ngrp = (hdr.z + 31) >> 5;
+                for (int i = 0; PLW * i < ngrp; i++) {
+                    const int t = (PLW * i + ((i & 1) ? PLW - 1 - w : w)) * 32 + lane;
+                    if (t >= hdr.z) continue;
+                    const unsigned rec = s_tn[t];
+                    const int node = (int)(rec & 0xfffu);
+                    const int cnt = (int)((rec >> 12) & 0xffu);
+                    const uint16_t* prow = s_roff + (rec >> 20);
+                    // rows every slot of a full group has: 32 wide and contiguous
+                    const int pfull = (t | 31) < hdr.z ? (int)((s_tn[t | 31] >> 12) & 0xffu) : 0;
+                    const int pbase = prow[0];
+    #define PQ(j) ((j) < pfull ? pbase + 32 * (j) + lane : prow[(j)] + lane)
+                    double2 f = s_f[node];
+                    int j = 0;
+                    if (MX) {
+                        const float2* s_q = reinterpret_cast<const float2*>(bk + L.dN);
+                        for (; j + 8 <= pfull; j += 8) {
+                            float2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[pbase + 32 * (j + i) + lane]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                        }
+                        for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
+                            int q[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
+                            float2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[q[i]]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                        }
+                        for (; j + 4 <= cnt; j += 4) {
+                            float2 c[4];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) c[i] = s_q[s_tpos[PQ(j + i)]];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                        }
+                        for (; j < cnt; j++) {
+                            const float2 c = s_q[s_tpos[PQ(j)]];
+                            f.x = f.x - (double)c.x;
+                            f.y = f.y - (double)c.y;
+                        }
+                    } else {
+                        const double2* s_p = reinterpret_cast<const double2*>(bk + L.dN);
+                        for (; j + 8 <= pfull; j += 8) {
+                            double2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[pbase + 32 * (j + i) + lane]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                        }
+                        for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
+                            int q[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
+                            double2 c[8];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[q[i]]];
+    #pragma unroll
+                            for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                        }
+                        for (; j + 4 <= cnt; j += 4) {
+                            double2 c[4];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) c[i] = s_p[s_tpos[PQ(j + i)]];
+    #pragma unroll
+                            for (int i = 0; i < 4; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
+                        }
+                        for (; j < cnt; j++) {
+                            const double2 c = s_p[s_tpos[PQ(j)]];
+                            f.x = f.x - c.x;
+                            f.y = f.y - c.y;
+                        }
+                    }
+    #undef PQ
+                    s_f[node] = f;
+                }
+                fence_proxy_async();
+                mbar_arrive(&empty[st]);
+            }
+        } else if (lane == 0) {
+            // ---- producer: the first NS chunks at once, then each chunk into the buffer the
+            // pull warps released ----------------------------------------------------------------------
+            int issued = 0;
+            for (; issued < NS && issued < nch; issued++) {
+                const mel_chunk c = d.chunk[ch0 + issued];
+                mbar_arrive_expect_tx(&full[issued], (unsigned)c.bytes);
+                bulk_load(region + issued * d.img_cap, d.img + c.img, (unsigned)c.bytes, &full[issued]);
+            }
+            for (; issued < nch; issued++) {
+                const int st = issued % NS;
+                const mel_chunk c = d.chunk[ch0 + issued];
+                if (*s_abort) break;
+                if (!mbar_wait_bounded(&empty[st], (unsigned)((issued / NS - 1) & 1), d.wait_ns)) {
+                    atomicOr(&d.err[MEL_E_WAIT], 1u);
+                    *s_abort = 1;
+                    break;
+                }
+                mbar_arrive_expect_tx(&full[st], (unsigned)c.bytes);
+                bulk_load(region + st * d.img_cap, d.img + c.img, (unsigned)c.bytes, &full[st]);
+            }
+            if (*s_abort)   // give the copies still in flight a bounded time to land before the CTA ends
+                for (int c = issued - 1; c >= 0 && c >= issued - NS; c--)
+                    mbar_wait_bounded(&full[c % NS], (unsigned)((c / NS) & 1));
+        } else {
+            // ---- contact forces (lanes 1-31 of warp 7, meanwhile): slave scatter in list order, then
+            // master scatter in send order (Body::Update_contact_forces, Code/Body.h:1642-1900) ---------
+            const unsigned mask = 0xfffffffeu;
+            for (int c = d.b_cont0[b]; c < d.b_cont0[b + 1]; c++) {
+                const mel_contact* ct = d.cont + c;
+                if (d.table[d.b_mat[b] * d.nmat + d.b_mat[ct->bodyM]] <= -1) continue;
+                double Fsx = ct->fx, Fsy = ct->fy;
+                warp_scatter(d, n0, ct->nodeS, Fsx, Fsy, s_fc, lane - 1, 31);
+                __syncwarp(mask);
+            }
+            for (int r = d.b_inc0[b]; r < d.b_inc0[b + 1]; r++) {
+                int2 rg = d.inc_rng[r];
+                for (int c = rg.x; c < rg.y; c++) {
+                    const mel_contact* ct = d.cont + c;
+                    if (d.table[d.b_mat[ct->bodyS] * d.nmat + d.b_mat[b]] <= -1) continue;
+                    double Fsx = ct->fx, Fsy = ct->fy;
+                    for (int k = 0; k < 4; k++) {
+                        double sk = ct->shapeM[k];
+                        warp_scatter(d, n0, ct->nodeM[k], -Fsx * sk, -Fsy * sk, s_fc, lane - 1, 31);
+                        __syncwarp(mask);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        __syncthreads();
+        if (*s_abort) return;
     }
-    __syncwarp();
-    __syncthreads();
-    if (*s_abort) return;
     double2* s_fn = reinterpret_cast<double2*>(region);
     double2* s_fd = s_fn + n;
     double2* s_vp = s_fd + n;
@@ -1526,7 +1697,7 @@ size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)
 {
     size_t base = 3 * sizeof(double2) * (size_t)max_nodes + MEL_BAR_BYTES;
     if (mixed) base += sizeof(float2) * (size_t)((max_nodes + 1) & ~1);
-    size_t stage = MEL_STAGES * (size_t)max_image_bytes;
+    size_t stage = MEL_STAGES(mixed) * (size_t)max_image_bytes;
     size_t post = (5 * sizeof(double2) + 6 * sizeof(double)) * (size_t)max_nodes;
     size_t rigid = (64 + 6 * MEL_RIGID_BATCH) * sizeof(double);
     size_t r = base + (stage > post ? stage : post);

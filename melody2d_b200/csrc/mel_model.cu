@@ -220,6 +220,34 @@ static mel_status validate(const mel_model_desc* d)
     return MEL_OK;
 }
 
+// Chunk entry cap for a model of this precision whose largest deformable body has max_nodes
+// nodes: MELGPU_CHUNK_CAP if set, else the first line of the tuning table (the file named by
+// MELGPU_TUNE_FILE; lines "precision max_body_nodes cap", '#' comments) whose precision matches and
+// whose node bound covers max_nodes; 0 when neither applies.
+static int tuned_chunk_cap(int precision, int max_nodes)
+{
+    if (const char* c = getenv("MELGPU_CHUNK_CAP")) {
+        const int v = atoi(c);
+        if (v >= 64 && v <= MEL_CHUNK_E_MAX) return v & ~7;
+    }
+    const char* path = getenv("MELGPU_TUNE_FILE");
+    if (!path) return 0;
+    FILE* f = fopen(path, "r");
+    if (!f) return 0;
+    char line[256];
+    int cap = 0;
+    while (fgets(line, sizeof line, f)) {
+        if (line[0] == '#') continue;
+        int p = -1, mn = 0, c = 0;
+        if (sscanf(line, "%d %d %d", &p, &mn, &c) == 3 && p == precision && max_nodes <= mn && c >= 64 && c <= MEL_CHUNK_E_MAX) {
+            cap = c & ~7;
+            break;
+        }
+    }
+    fclose(f);
+    return cap;
+}
+
 static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_options* opt)
 {
     mel_dev& D = h->d;
@@ -537,8 +565,13 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
                                       std::min(1023, groups * max_ns) + pull_rows, mixed ? 8 : 16).bytes;
         };
         int chosen = -1;
-        for (int ecap : caps)
-            if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed) <= two_per_sm) { chosen = ecap; break; }
+        // a cap from the tuning table (MELGPU_TUNE_FILE, written by melody2d_b200.autotune), or forced
+        // by MELGPU_CHUNK_CAP (the tuner's own runs), is taken when it fits the shared memory
+        const int tuned = tuned_chunk_cap(h->precision, max_def_nodes);
+        if (tuned > 0 && mel_body_smem_bytes(max_def_nodes, bound(tuned), mixed) <= (size_t)smem_blk) chosen = tuned;
+        if (chosen < 0)
+            for (int ecap : caps)
+                if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed) <= two_per_sm) { chosen = ecap; break; }
         if (chosen < 0)     // one CTA per SM: largest cap that fits
             for (int ecap : caps)
                 if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed) <= (size_t)smem_blk) { chosen = ecap; break; }

@@ -101,6 +101,10 @@ def lib():
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m melody2d_b200.build`")
+        # the chunk-size tuning table written by melody2d_b200.autotune, unless the caller names one
+        table = os.path.join(_HERE, "tuning.txt")
+        if "MELGPU_TUNE_FILE" not in os.environ and os.path.exists(table):
+            os.environ["MELGPU_TUNE_FILE"] = table
         L = C.CDLL(LIB_PATH)
         for name, args in SIGNATURES.items():
             f = getattr(L, name)

@@ -60,13 +60,14 @@ extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const dou
                 const uint32_t gm = sgpm[t];
                 const int r0 = (int)(gm & 0x3ffu), lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
                 if (r0 + ns > hdr[3] || lane != t % 32) return 4;
-                // the kernel computes the positions of rows every slot of a full group has; they
-                // must agree with the row table
-                const int nfull = (t | 31) < hdr[0] ? (int)(sgpm[t | 31] >> 15) : 0;
+                // the kernel computes every position from the group's first entry, its width m and
+                // the row's lane swizzle; they must agree with the row table
+                const int m = (hdr[0] - (t & ~31)) < 32 ? hdr[0] - (t & ~31) : 32;
+                const int sw = (m & 7) == 0 ? 7 : 0;
                 const int base = (int)(sroff[r0] & 0xfffu);
                 auto Et = [&](int k) { const unsigned r = sroff[r0 + k]; return (int)(r & 0xfffu) + (lane ^ (int)(r >> 12)); };
-                for (int k = 0; k < nfull && k < ns; k++) if (base + 32 * k + (lane ^ (k & 7)) != Et(k)) return 10;
-                auto E = [&](int k) { return k < nfull ? base + 32 * k + (lane ^ (k & 7)) : Et(k); };
+                auto E = [&](int k) { return base + m * k + (lane ^ (k & sw)); };
+                for (int k = 0; k < ns; k++) if (E(k) != Et(k)) return 10;
                 for (int k = 0; k < ns; k++) if (E(k) >= ne || sidx[E(k)] >= n) return 5;
                 const double c0 = sc0[t];
                 auto U = [&](int k) { int i = sidx[E(k)]; return std::make_pair(up[2 * (n0 + i)], up[2 * (n0 + i) + 1]); };

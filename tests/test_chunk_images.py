@@ -43,6 +43,7 @@ def test_chunk_pass_matches_oracle(emul, oracle_built, ecap):
     rc = emul.emul_internal_forces(C.byref(desc.desc), ecap, up.ctypes.data, f.ctypes.data, stats.ctypes.data)
     assert rc == 0, (rc, emul.emul_error())
     assert stats[0] > 0 and stats[3] % 16 == 0
-    assert stats[2] < 8 * stats[0], "only the rounding of each chunk to 8 entries pads"
+    # padding: point groups padded to their widest slot, and each chunk rounded to 8 entries
+    assert stats[2] < 0.2 * stats[1], "padding above a fifth of the stored entries"
     np.testing.assert_array_equal(f, ref)
     assert np.abs(ref).max() > 0
