@@ -323,6 +323,10 @@ def headline_extras(args, rank, world, local, pg):
                           "config": b["config"], "plain_fp64_one_at_a_time": b["plain_fp64_one_at_a_time"],
                           "ratio_vs_plain_fp64": b["ratio_vs_plain_fp64"], "accuracy_vs_fp64": b["accuracy_vs_fp64"],
                           "gpu_launches": b["gpu_launches"], "clocks": b["clocks"]}
+    try:
+        out["input_generation"] = input_generation(args, local)
+    except Exception as e:                       # reported, never silently dropped
+        out["input_generation"] = {"error": str(e)}
     a = copy.copy(args)
     a.rate, a.duration, a.drain, a.step_cap = args.serve_rate, args.serve_duration, args.serve_drain, args.serve_step_cap
     v = run_serve(a, rank, world, local, pg, emit=False)
@@ -332,6 +336,44 @@ def headline_extras(args, rank, world, local, pg):
                           "same_requests_compared": v["same_requests_compared"],
                           "max_rel_error_vs_plain_fp64": v["max_rel_error_vs_plain_fp64"]}
     return out
+
+
+def input_generation(args, local):
+    """Gauss-point shape functions of a generated sample on the device (mel_mls_shapes) against
+    the host restatement of the pre-processor's MLS pass (generator.mls_shape, one thread), in
+    Gauss points per second; the device figure is the value pass's CUDA-event time, the e2e figure
+    the whole call with its host transfers."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import mls_shapes
+    sc = g.biaxial_scene(seed=11, n_discs=args.mls_discs, workers=host_threads())
+    bodies = [b for b in sc.bodies if b.kind == "deformable"]
+    jobs = [(b.gp_xy, b.nodes, b.domain) for b in bodies]
+    npts = sum(j[0].shape[0] for j in jobs)
+    mls_shapes(jobs[:8], device=local)                      # warm-up (module load, allocations)
+    best_k, best_w, entries = None, None, 0
+    for _ in range(3):
+        tm = {}
+        t0 = time.perf_counter()
+        out = mls_shapes(jobs, device=local, timing=tm)
+        w = time.perf_counter() - t0
+        best_k = tm["kernel_ms"] if best_k is None else min(best_k, tm["kernel_ms"])
+        best_w = w if best_w is None else min(best_w, w)
+        entries = sum(len(o[1]) for o in out)
+    sub = jobs[:args.mls_cpu_bodies]
+    t0 = time.perf_counter()
+    for pts, nodes, radii in sub:
+        g.mls_shape(pts, nodes, radii, np.zeros(2))
+    cpu_s = time.perf_counter() - t0
+    cpu_pts = sum(j[0].shape[0] for j in sub)
+    written = entries * (4 + 3 * 8) + (npts + 1) * 8
+    return {"metric": "Gauss points/s", "value": npts / (best_k * 1e-3), "unit": "points/s",
+            "e2e": {"value": npts / best_w, "unit": "points/s"},
+            "config": {"workload": "shape functions of the %d-disc biaxial sample" % args.mls_discs,
+                       "gauss_points": npts, "support_entries": entries},
+            "value_pass_ms": best_k, "bytes_written": written,
+            "achieved_write_gbs": written / (best_k * 1e-3) / 1e9,
+            "cpu_baseline": {"value": cpu_pts / cpu_s, "unit": "points/s", "cores": 1, "kind": "port",
+                             "sample": "%d bodies (%d points) through generator.mls_shape" % (len(sub), cpu_pts)}}
 
 
 def create_solvers(flats, precision, device, threads):
@@ -573,6 +615,8 @@ def main():
     ap.add_argument("--serve-duration", type=float, default=8.0)
     ap.add_argument("--serve-drain", type=float, default=60.0)
     ap.add_argument("--serve-step-cap", type=int, default=2000)
+    ap.add_argument("--mls-discs", type=int, default=400)
+    ap.add_argument("--mls-cpu-bodies", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -261,6 +261,75 @@ mel_status mel_checkpoint_read(mel_handle* h, double* node_state, double* rigid,
                                mel_contact* contacts, int contacts_capacity, int* ncont, double* time3);
 mel_status mel_monitor_compute(mel_handle* h, mel_monitor* out);
 
+/* Border-condition pressures of the last step, x and y, one per border entry in the order of the
+ * border node lists (Border::x_bc_pressure, y_bc_pressure, set by Update_bc_forces,
+ * Code/Body.h:669-901; zero on borders whose conditions are both none). */
+mel_status mel_get_bc_pressures(mel_handle* h, double* px, double* py);
+
+/* ---- monitoring and reference-format output ------------------------------------------ */
+#define MEL_MON_NF 7   /* doubles per monitored entry: the vector Read_spy_line builds (Code/IO.h:11-590), zero-padded */
+/* Monitoring (Code/Monitoring.h:8-559) on the device: after every accepted step of mel_step one row
+ * is appended to a device buffer of ring_rows rows, without a host download, until
+ * mel_monitor_rows drains it (the reference keeps rows in memory and flushes them at save time,
+ * Code/IO.h:2644-2668).  `monitored` holds n_monitored entries of MEL_MON_NF doubles, the rows of the
+ * reference's Monitored array as Read_spy_line builds them from STATIC_CONTROL's MONITORING section
+ * (mel_load_run fills them); monitor_energy and monitor_boundaries are DYNAMIC flags[1] and flags[2];
+ * first_iteration is Number_iteration before the next step.  A row holds Number_iteration, Time,
+ * Deltat, neval, max_error, mean_error (the last three are 0 under the Euler scheme, which never
+ * sets them), one value per entry that yields one, then Dwork, elastic energy and kinetic energy
+ * (monitor_energy) and the four boundary sums (monitor_boundaries).  Contact entries yield a value
+ * only while their slave node has a contact element, so rows can differ in length;
+ * *max_row_length receives the longest.  Entry types 5 (Jacobian), 6 (Stress) and 8 (Damage) need
+ * the nodal stress post-processing or Body::Update_damage, which this library does not run:
+ * MEL_ERR_UNSUPPORTED.  Force entries of nodes or deformable bodies keep mel_record_forces on.
+ * Entries are checked against the model (the reference indexes its arrays with them unchecked):
+ * out of range is MEL_ERR_INVALID.  n_monitored = 0 with both flags 0 turns monitoring off.  A
+ * batch member cannot monitor (MEL_ERR_INVALID).  mel_step refuses (MEL_ERR_INVALID, nothing done)
+ * to take more steps than the buffer has free rows. */
+mel_status mel_monitor_setup(mel_handle* h, const double* monitored, int n_monitored, int monitor_energy,
+                             int monitor_boundaries, int ring_rows, int first_iteration, int* max_row_length);
+/* The rows recorded since the last call, oldest first, and empties the buffer: row i occupies
+ * rows[i*(max_row_length+1) ...], its first double the number L of values that follow.
+ * rows = NULL with max_rows = 0 only sets *n_rows to the number held.  A buffer of fewer than
+ * *n_rows rows is MEL_ERR_INVALID and drains nothing (*n_rows says how many are held). */
+mel_status mel_monitor_rows(mel_handle* h, double* rows, int max_rows, int* n_rows);
+
+/* What the input files say about output (Code/IO.h:598-2345), for a host loop that writes the
+ * reference's files: Simulation_name, Save_period and Print_period (STATIC_CONTROL SOLVER block),
+ * Number_save, Number_iteration, Number_print, Next_save, Next_print (DYNAMIC SOLVER block), the
+ * MONITORING entries (Code/IO.h:933-945, the vectors Read_spy_line builds, zero-padded to
+ * MEL_MON_NF) and the DYNAMIC flags. */
+#define MEL_MON_MAX 256
+typedef struct mel_run_control {
+    char   simulation_name[256];
+    double save_period, print_period, next_save, next_print;
+    int    number_save, number_iteration, number_print;
+    int    n_monitored;
+    double monitored[MEL_MON_MAX * MEL_MON_NF];
+    int    flags[MEL_NFLAGS];
+} mel_run_control;
+/* Fills *out from a model read by mel_load_desc (its owner). */
+mel_status mel_load_run_control(const void* owner, mel_run_control* out);
+/* mel_create from a model read by mel_load_desc, with the contact list of its DYNAMIC file (as
+ * mel_create_from_files, without reading the files again). */
+mel_status mel_create_loaded(const void* owner, const mel_options* opt, mel_handle** out);
+
+/* Run counters of Code/main.cpp that Write_dynamic records but the solver does not keep. */
+typedef struct mel_save_info {
+    const char* simulation_name;
+    int    number_save;       /* the file is DYNAMIC_<number_save, 5 digits>.asc */
+    int    number_iteration;
+    int    number_print;
+    double next_save, next_print;
+} mel_save_info;
+/* Write_dynamic (Code/IO.h:2351-2640): writes <dir>/DYNAMIC_nnnnn.asc from the handle's state in
+ * the reference's layout and number formatting (what Load_dynamic and mel_create_from_files read
+ * back to restart): kinematics, forces, works, neighbours, border segments, contact elements,
+ * contact and border-condition pressures, and the Time, Deltat and Next_contact_update of the
+ * handle.  The FORCES blocks are the nodal forces of the last step, so mel_record_forces must have
+ * been on during it (MEL_ERR_INVALID otherwise); damping and self-contact components are zero. */
+mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info* info);
+
 /* Rigid-body records (layout MEL_RG_*, n_bodies records); node positions follow (restart upload). */
 mel_status mel_set_rigid(mel_handle* h, const double* rigid);
 /* Time, Deltat and Next_contact_update of the loop (Code/IO.h:1944-1953; restart upload). */
@@ -297,6 +366,26 @@ mel_status mel_free_desc(void* owner);
 mel_status mel_monitor_reduce_static(const double* d_velocity, const double* d_mass, const double* d_displacement,
                                      int n_nodes, const mel_contact* d_contacts, int n_contacts, double* d_out,
                                      void* stream);
+
+/* ---- input generation ------------------------------------------------------------------ */
+/* Shape functions and derivatives at the Gauss points of n_bodies bodies, computed on the device:
+ * the moving-least-squares pass of the reference's pre-processor with the linear basis
+ * (Preprocessor/MLS2DWithDerivatives.m:65-165), the cubic-spline weight W1
+ * (Preprocessor/WeightW1WithDerivatives.m:17-47) and the support rule |x_p - x_i| < r_i
+ * (Preprocessor/SupportDomain.m:16-18).  Host arrays: body b owns nodes [body_node_ptr[b],
+ * body_node_ptr[b+1]) (x,y pairs in `nodes`, influence radii in `radii`) and Gauss points
+ * [body_point_ptr[b], body_point_ptr[b+1]) (x,y pairs in `points`), at most 4096 nodes per body.
+ * Output in CSR: sup_ptr[n_points+1] offsets, then per entry the body-local support node (ascending
+ * within a point, as SupportDomain lists them), N, dN/dx, dN/dy -- the layout of
+ * mel_model_desc::gp_sup_*, gp_N, gp_dNdx, gp_dNdy.  Call with sup_idx = NULL to get sup_ptr and
+ * *n_entries only; then with buffers of `capacity` >= *n_entries entries.  A point whose supports
+ * do not span the plane (singular moment matrix) is MEL_ERR_INVALID, naming it.  kernel_ms (may be
+ * NULL) receives the device time of the value pass.  No counterpart in the solver (the reference
+ * computes these in MATLAB before the run). */
+mel_status mel_mls_shapes(int n_bodies, const int* body_node_ptr, const double* nodes, const double* radii,
+                          const int* body_point_ptr, const double* points, long long* sup_ptr, int* sup_idx,
+                          double* N, double* dNdx, double* dNdy, long long capacity, long long* n_entries, int device,
+                          double* kernel_ms);
 
 /* ---- batches ------------------------------------------------------------------------ */
 /* No counterpart in the reference (one simulation per process there).  A batch advances several

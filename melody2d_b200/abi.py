@@ -71,6 +71,23 @@ class MelMonitor(C.Structure):
                 ("active_contacts", C.c_int), ("n_contacts", C.c_int)]
 
 
+MEL_MON_NF = 7
+MEL_MON_MAX = 256
+MEL_NFLAGS = 11
+
+
+class MelSaveInfo(C.Structure):
+    _fields_ = [("simulation_name", C.c_char_p), ("number_save", C.c_int), ("number_iteration", C.c_int),
+                ("number_print", C.c_int), ("next_save", C.c_double), ("next_print", C.c_double)]
+
+
+class MelRunControl(C.Structure):
+    _fields_ = [("simulation_name", C.c_char * 256), ("save_period", C.c_double), ("print_period", C.c_double),
+                ("next_save", C.c_double), ("next_print", C.c_double), ("number_save", C.c_int),
+                ("number_iteration", C.c_int), ("number_print", C.c_int), ("n_monitored", C.c_int),
+                ("monitored", C.c_double * (MEL_MON_MAX * MEL_MON_NF)), ("flags", C.c_int * MEL_NFLAGS)]
+
+
 class MelOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("use_graph", C.c_int), ("max_contacts", C.c_int)]
 

@@ -24,6 +24,12 @@ struct mel_host_model {
     std::vector<int> cells, body_matrix_ptr, matrix_dofs;
     std::vector<double> matrix_stiffness, matrix_damping;
     std::vector<mel_contact> contacts;   // CONTACTS of the DYNAMIC file
+    // run control that drives output only: Save_period, Print_period (STATIC_CONTROL SOLVER block),
+    // Number_save, Number_iteration, Number_print, Next_save, Next_print (DYNAMIC SOLVER block), and
+    // the MONITORING entries as Read_spy_line builds them (Code/IO.h:933-945)
+    double save_period = 0., print_period = 0., next_save = 0., next_print = 0.;
+    int number_save = 0, number_iteration = 0, number_print = 0;
+    std::vector<std::vector<double>> monitored;
     void finalize();                     // points desc at the vectors
 };
 

@@ -111,6 +111,9 @@ struct mel_dev {
     const int *e_node, *e_sn, *e_ss;         // e_sn/e_ss: 4 per entry (node0..3, shift0..3)
     const double* e_len0;
     double* e_len;                            // lengths of the last Update_borders
+    double2* e_bcp;                           // border-condition pressures of the last Update_bc_forces
+                                              // (Border::x_bc_pressure, y_bc_pressure; zero on borders
+                                              // whose conditions are both none)
     int nblk;                                 // segment blocks (MEL_SEGB segments of one border)
     const int* bd_blk0;                       // [nbd+1] first block of each border
     const int* blk_border;                    // border of each block
@@ -178,6 +181,18 @@ void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);
 // Update_contact_pressures (Code/Proximity.h:1014-1069) from the current contact list
 void mel_launch_contact_pressures(const mel_dev& d, cudaStream_t s);
+
+// one monitored entry of STATIC_CONTROL's MONITORING list (the vector Read_spy_line builds,
+// Code/IO.h:11-590): type (0 position, 1 displacement, 2 velocity, 3 acceleration, 4 force,
+// 7 contact, 9 energy, 10 work), kind (component or quantity), sub (force kind), body, node (-1:
+// the whole body), border and border node (contact entries)
+struct mel_mon_op { int type, kind, sub, body, node, border, bnode, pad; };
+// the row's leading columns (Code/Monitoring.h:25)
+struct mel_mon_head { double iteration, time, dt, neval, max_error, mean_error; };
+// Monitoring after a step: per-body partial sums into part[3*nb], then the row into row[0..]
+// (row[0] = number of values that follow)
+void mel_launch_monitor(const mel_dev& d, const mel_mon_op* ops, int nops, int energy, int boundaries,
+                        double* part, double* row, const mel_mon_head& hd, cudaStream_t s);
 
 int mel_body_kernel_configure(size_t smem);
 

@@ -1069,6 +1069,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
                     if (ty == MEL_BC_ORIENTED) py = yv;
                     else if (ty == MEL_BC_FOLLOWING) { px += yv * (fty * ftpx - ftx * ftpy); py += yv * (fty * ftpy + ftx * ftpx); }
                     else if (ty == MEL_BC_SOFT) py = d.bd_bcp[4 * g + 2] * (yv - ub.y) - d.bd_bcp[4 * g + 3] * (yvel - vb.y);
+                    if (lane == 0) d.e_bcp[e] = make_double2(px, py);   // Border::x_bc_pressure, y_bc_pressure
                     int gn = n0 + bn;
                     for (int j = d.sup_ptr[gn] + lane; j < d.sup_ptr[gn + 1]; j += 32) {
                         double sf = d.sup_N[j];
@@ -1295,10 +1296,12 @@ __device__ void rigid_body(const mel_dev& d, int b, double T, double T0, char* s
                 double length = d.e_len0[e];
                 double fxn = 0., fyn = 0., fxd = 0., fyd = 0.;
                 double2 ub = d.u[gn], vb = d.v[gn], xb = d.x[gn];
-                if (tx == MEL_BC_ORIENTED || tx == MEL_BC_FOLLOWING) fxn = xv * length;
-                else if (tx == MEL_BC_SOFT) fxd = (d.bd_bcp[4 * g] * (xv - ub.x) + d.bd_bcp[4 * g + 1] * (xvel - vb.x)) * length;
-                if (ty == MEL_BC_ORIENTED || ty == MEL_BC_FOLLOWING) fyn = yv * length;
-                else if (ty == MEL_BC_SOFT) fyd = (d.bd_bcp[4 * g + 2] * (yv - ub.y) + d.bd_bcp[4 * g + 3] * (yvel - vb.y)) * length;
+                double px = 0., py = 0.;                  // Border::x_bc_pressure, y_bc_pressure
+                if (tx == MEL_BC_ORIENTED || tx == MEL_BC_FOLLOWING) { px = xv; fxn = px * length; }
+                else if (tx == MEL_BC_SOFT) { px = d.bd_bcp[4 * g] * (xv - ub.x) + d.bd_bcp[4 * g + 1] * (xvel - vb.x); fxd = px * length; }
+                if (ty == MEL_BC_ORIENTED || ty == MEL_BC_FOLLOWING) { py = yv; fyn = py * length; }
+                else if (ty == MEL_BC_SOFT) { py = d.bd_bcp[4 * g + 2] * (yv - ub.y) + d.bd_bcp[4 * g + 3] * (yvel - vb.y); fyd = py * length; }
+                d.e_bcp[e] = make_double2(px, py);
                 double dx = xb.x - xcs, dy = xb.y - ycs;
                 sT[i] = fxn;
                 sT[MEL_RIGID_BATCH + i] = fyn;

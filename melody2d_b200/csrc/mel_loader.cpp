@@ -114,6 +114,98 @@ bool read_bc(std::istream& f, BodyTmp::Bd& br, int dir)
 
 } // namespace
 
+// One entry of a MONITORING (or SPIES / DEACTIVATION) list: the keyword grammar of Read_spy_line
+// (Code/IO.h:11-590) and the vector it builds, {type, ...}.  Tables map each keyword to its code; the
+// numbers that follow are read as the grammar says.  A keyword the grammar does not know leaves `v`
+// as it was (the reference reuses the caller's vector the same way).
+static void read_spy_line(std::istream& C, std::vector<double>& v)
+{
+    static const std::map<std::string, int> quantity = { { "Position", 0 }, { "Displacement", 1 }, { "Velocity", 2 },
+                                                         { "Acceleration", 3 }, { "Force", 4 }, { "Jacobian", 5 },
+                                                         { "Stress", 6 }, { "Contact", 7 }, { "Damage", 8 },
+                                                         { "Energy", 9 }, { "Work", 10 }, { "Error", 11 },
+                                                         { "MassScaling", 12 } };
+    static const std::vector<std::string> position = { "X", "Y", "R", "Length", "LengthInContact", "Area", "AllX", "AllY" };
+    static const std::vector<std::string> vector4 = { "X", "Y", "Mag", "R" };
+    static const std::vector<std::string> forces = { "Total", "Internal", "Contact", "Body", "Dirichlet", "Neumann", "Damping", "Alid" };
+    static const std::vector<std::string> stress = { "XX", "YY", "XY", "ZZ", "Tresca", "VM", "Major", "Intermediate", "Minor", "Spherical" };
+    static const std::vector<std::string> contact = { "Gapn", "Gapt", "Xsi", "Xnorm", "Ynorm", "Damage", "Fx", "Fy", "Length",
+                                                      "Master", "Px", "Py", "Slave", "Xslave", "Yslave" };
+    static const std::vector<std::string> energy = { "Kinetic", "Deformation" };
+    static const std::vector<std::string> work = { "Internal", "Contact", "Body", "Dirichlet", "Neumann", "Damping", "Alid" };
+    static const std::vector<std::string> error = { "X", "Y", "Mag", "Norm", "Max" };
+    static const std::vector<std::string> mass = { "X", "Y", "Moy", "dX", "dY", "dMoy", "Xmass", "Ymass", "Mass" };
+    auto code = [](const std::vector<std::string>& t, const std::string& k) {
+        for (size_t i = 0; i < t.size(); i++) if (t[i] == k) return (int)i;
+        return -1;
+    };
+    std::string kw, sub;
+    C >> kw;
+    auto q = quantity.find(kw);
+    if (q == quantity.end()) return;
+    const double T = q->second;
+    double b = 0, bo = 0, n = 0;
+    int k;
+    switch (q->second) {
+    case 0:
+        C >> sub;
+        if ((k = code(position, sub)) < 0) return;
+        if (k <= 2) { C >> b >> n; v = { T, (double)k, b, n }; }
+        else if (k <= 5) { C >> b; v = { T, (double)k, b }; }
+        else v = { T, (double)k };
+        return;
+    case 1: case 2: case 3:
+        C >> sub;
+        if ((k = code(vector4, sub)) < 0) return;
+        C >> b >> n; v = { T, (double)k, b, n };
+        return;
+    case 4: {
+        C >> sub;
+        const int comp = code(vector4, sub);
+        if (comp < 0) return;
+        C >> sub;
+        if ((k = code(forces, sub)) < 0) return;
+        C >> b >> n; v = { T, (double)comp, (double)k, b, n };
+        return;
+    }
+    case 5: case 8:
+        if (q->second == 5) { C >> b >> n; v = { T, b, n }; }
+        else { C >> b; v = { T, b }; }
+        return;
+    case 6:
+        C >> sub;
+        if ((k = code(stress, sub)) < 0) return;
+        C >> b >> n; v = { T, (double)k, b, n };
+        return;
+    case 7:
+        C >> sub;
+        if ((k = code(contact, sub)) < 0) return;
+        C >> b >> bo >> n; v = { T, (double)k, b, bo, n };
+        return;
+    case 9: case 10:
+        C >> sub >> b;
+        if ((k = code(q->second == 9 ? energy : work, sub)) < 0) return;
+        v = { T, (double)k, b };
+        return;
+    case 11:
+        C >> sub;
+        if ((k = code(error, sub)) < 0) return;
+        C >> b >> n; v = { T, (double)k, b, n };
+        return;
+    case 12:
+        C >> sub;
+        if (sub == "Polar") {
+            double x0, x1, y0, y1;
+            C >> sub >> n >> x0 >> x1 >> y0 >> y1;
+            if (sub == "Contact_Normal") v = { 11., 0., n, x0, x1, y0, y1 };
+            return;
+        }
+        if ((k = code(mass, sub)) < 0) return;
+        C >> b >> n; v = { T, (double)k, b, n };
+        return;
+    }
+}
+
 mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* out)
 {
     mel_host_model& M = *out;
@@ -209,6 +301,16 @@ mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* ou
             C >> n;
             std::getline(C, token);
             if (n > 0) { mel_set_error("DEACTIVATION (Update_status, Code/Proximity.h:550) is not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
+        }
+        if (line.compare(0, 10, "MONITORING") == 0) {        // Code/IO.h:933-945
+            int n = 0;
+            C >> n; std::getline(C, token);
+            std::vector<double> entry;
+            for (int i = 0; i < n; i++) {
+                read_spy_line(C, entry);
+                M.monitored.push_back(entry);
+                std::getline(C, token);
+            }
         }
         if (line.compare(0, 13, "NUMBER_BODIES") == 0) { C >> nbodies; std::getline(C, token); B.resize(nbodies); }
         if (line.compare(0, 10, "DEFORMABLE") == 0 || line.compare(0, 5, "RIGID") == 0) {
@@ -489,6 +591,9 @@ mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* ou
     if (d.solver < 0) { mel_set_error("unknown solver %s", solver.c_str()); return MEL_ERR_INVALID; }
     for (int k = 0; k < 8; k++) d.solver_params[k] = sp[k];
     for (int k = 0; k < MEL_NFLAGS; k++) d.flags[k] = flags[k];
-    (void)tini; (void)save; (void)print; (void)nsave; (void)niter; (void)nprint; (void)next_save; (void)next_print;
+    (void)tini;
+    M.save_period = save; M.print_period = print;
+    M.number_save = nsave; M.number_iteration = niter; M.number_print = nprint;
+    M.next_save = next_save; M.next_print = next_print;
     return MEL_OK;
 }

@@ -10,6 +10,8 @@
 #include <numeric>
 #include <vector>
 #include <algorithm>
+#include <fstream>
+#include <iomanip>
 #include "mel_internal.h"
 #include "mel_prox_host.h"
 #include "mel_chunks.h"
@@ -97,6 +99,15 @@ struct mel_handle {
     std::vector<cudaEvent_t> ev_pool;
     double bytes_body = 0., bytes_contact = 0.;
     int n_def_nodes = 0;
+    // Monitoring on the device (mel_monitor_setup): entries, per-body partial sums, row buffer of
+    // mon_cap rows of mon_stride doubles, rows recorded since the last drain, Number_iteration
+    mel_mon_op* mon_ops = nullptr;
+    int mon_nops = 0, mon_energy = 0, mon_bound = 0;
+    double* mon_part = nullptr;
+    double* mon_rows = nullptr;
+    int mon_cap = 0, mon_stride = 0, mon_count = 0;
+    bool mon_on = false, mon_forces = false;
+    long long iteration = 0;
     mel_batch* batch = nullptr;  // batch the handle is a member of (steps only through the batch)
     int failed = 0;                 // model-level failure (MEL_ERR_NAN, MEL_ERR_BOUNDS) that retired it from a batch
     std::string failed_msg;
@@ -487,6 +498,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.e_len0 = dupload(h, len0);
     std::vector<double> len(len0);
     D.e_len = dupload(h, len);
+    D.e_bcp = dalloc<double2>(h, (size_t)ne + 1);
     D.cp_cnt = dalloc<int>(h, (size_t)ne + 1);
     D.cp_item = dalloc<int>(h, (size_t)(ne > 0 ? ne : 1) * MEL_PRESSURE_CAP);
     D.cpx = dalloc<double>(h, (size_t)ne + 1);
@@ -968,6 +980,34 @@ mel_status mel_load_desc(const char* dir, int restart_index, mel_model_desc** de
     return MEL_OK;
 }
 
+mel_status mel_create_loaded(const void* owner, const mel_options* opt, mel_handle** out)
+{
+    if (!owner || !out) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    const mel_host_model* hm = static_cast<const mel_host_model*>(owner);
+    return create_impl(&hm->desc, opt, hm->contacts.data(), (int)hm->contacts.size(), out);
+}
+
+mel_status mel_load_run_control(const void* owner, mel_run_control* out)
+{
+    if (!owner || !out) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    const mel_host_model* hm = static_cast<const mel_host_model*>(owner);
+    if (hm->monitored.size() > MEL_MON_MAX) {
+        mel_set_error("%zu monitored entries, at most %d are supported", hm->monitored.size(), MEL_MON_MAX);
+        return MEL_ERR_UNSUPPORTED;
+    }
+    memset(out, 0, sizeof *out);
+    snprintf(out->simulation_name, sizeof out->simulation_name, "%s", hm->name.c_str());
+    out->save_period = hm->save_period; out->print_period = hm->print_period;
+    out->next_save = hm->next_save; out->next_print = hm->next_print;
+    out->number_save = hm->number_save; out->number_iteration = hm->number_iteration; out->number_print = hm->number_print;
+    out->n_monitored = (int)hm->monitored.size();
+    for (size_t i = 0; i < hm->monitored.size(); i++)
+        for (size_t k = 0; k < hm->monitored[i].size() && k < MEL_MON_NF; k++)
+            out->monitored[MEL_MON_NF * i + k] = hm->monitored[i][k];
+    for (int k = 0; k < MEL_NFLAGS; k++) out->flags[k] = hm->desc.flags[k];
+    return MEL_OK;
+}
+
 mel_status mel_free_desc(void* owner)
 {
     delete static_cast<mel_host_model*>(owner);
@@ -995,6 +1035,7 @@ mel_status mel_destroy(mel_handle* h)
     if (h->d_state) cudaFree(h->d_state);
     for (void* p : h->store_bufs) cudaFree(p);
     if (h->h_red) cudaFreeHost(h->h_red);
+    for (void* p : { (void*)h->mon_ops, (void*)h->mon_part, (void*)h->mon_rows }) if (p) cudaFree(p);
     if (h->ck.h_stage) cudaFreeHost(h->ck.h_stage);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->ev_start) { cudaEventDestroy(h->ev_start); cudaEventDestroy(h->ev_end); }
@@ -1022,6 +1063,11 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
     auto mark = [&]() { if (!h->timing) return; cudaEvent_t e = h->ev_pool[nev++]; cudaEventRecord(e, h->stream); ev.push_back(e); };
     std::vector<int> kinds;
     const bool adaptive = h->solver != MEL_SOLVER_EULER;
+    if (h->mon_on && h->mon_count + io->nsteps > h->mon_cap) {
+        mel_set_error("monitoring rows: %d recorded and %d more steps exceed the buffer of %d rows; drain them with "
+                      "mel_monitor_rows first", h->mon_count, io->nsteps, h->mon_cap);
+        return MEL_ERR_INVALID;
+    }
     for (int s = 0; s < io->nsteps; s++) {
         if (adaptive) {
             // Solver_step (Code/Solver.h:98-486, dispatched at Code/main.cpp:156-167)
@@ -1041,6 +1087,18 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             h->parity ^= 1;
             h->time += h->dt;                       // Code/Solver.h:86
             h->pressure_state = 1;                  // Update_contact_pressures ends the step (Code/Solver.h:87)
+        }
+        h->iteration++;                             // Number_iteration (Code/main.cpp:143)
+        if (h->mon_on) {                            // Monitoring (Code/main.cpp:173-177)
+            mel_mon_head hd;
+            hd.iteration = (double)h->iteration; hd.time = h->time; hd.dt = h->dt;
+            hd.neval = h->solver_stats[0]; hd.max_error = h->solver_stats[1]; hd.mean_error = h->solver_stats[2];
+            mel_launch_monitor(h->d, h->mon_ops, h->mon_nops, h->mon_energy, h->mon_bound, h->mon_part,
+                               h->mon_rows + (size_t)h->mon_count * h->mon_stride, hd, h->stream);
+            cudaError_t le = cudaGetLastError();
+            if (le != cudaSuccess) { mel_set_cuda_error(le, "monitoring launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
+            h->mon_count++;
+            h->launches += 2;
         }
         if (io->run_proximity && h->time > h->next_cup - 1.e-6 * h->dt) {   // Code/main.cpp:191-196
             h->next_cup = h->next_cup + h->cup;
@@ -1295,7 +1353,7 @@ mel_status mel_get_forces(mel_handle* h, double* internal, double* contact, doub
 mel_status mel_record_forces(mel_handle* h, int on)
 {
     if (!h) return MEL_ERR_INVALID;
-    h->d.record_forces = on ? 1 : 0;
+    h->d.record_forces = (on || h->mon_forces) ? 1 : 0;    // force entries of the monitoring keep it on
     return MEL_OK;
 }
 
@@ -1377,6 +1435,299 @@ mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* 
     if (n) *n = h->d.ncont;
     int m = std::min(capacity, h->d.ncont);
     if (out && m > 0) MEL_CUDA_OK(cudaMemcpy(out, h->d.cont, sizeof(mel_contact) * m, cudaMemcpyDeviceToHost));
+    return MEL_OK;
+}
+
+mel_status mel_get_bc_pressures(mel_handle* h, double* px, double* py)
+{
+    if (!h || (!px && !py)) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    if (h->ne > 0) {
+        std::vector<double2> p(h->ne);
+        MEL_CUDA_OK(cudaMemcpy(p.data(), h->d.e_bcp, sizeof(double2) * (size_t)h->ne, cudaMemcpyDeviceToHost));
+        for (int e = 0; e < h->ne; e++) { if (px) px[e] = p[e].x; if (py) py[e] = p[e].y; }
+    }
+    return MEL_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Monitoring on the device (Code/Monitoring.h:8-559, rows drained as Write_monitoring flushes them)
+// ---------------------------------------------------------------------------------------------
+mel_status mel_monitor_setup(mel_handle* h, const double* monitored, int n_monitored, int monitor_energy,
+                             int monitor_boundaries, int ring_rows, int first_iteration, int* max_row_length)
+{
+    if (!h || n_monitored < 0 || ring_rows < 0 || (n_monitored > 0 && !monitored)) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    if (h->batch) { mel_set_error("monitoring runs on handles stepped with mel_step, not on batch members"); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    const bool on = n_monitored > 0 || monitor_energy || monitor_boundaries;
+    if (on && ring_rows == 0) { mel_set_error("monitoring needs a row buffer (ring_rows > 0)"); return MEL_ERR_INVALID; }
+    // the entries as the kernel reads them, checked against the model (the reference indexes its
+    // arrays with them unchecked)
+    std::vector<int> nodes_of(h->nb);
+    for (int b = 0; b < h->nb; b++) nodes_of[b] = h->b_node0[b + 1] - h->b_node0[b];
+    std::vector<int> bd0(h->nb + 1);
+    MEL_CUDA_OK(cudaMemcpy(bd0.data(), h->d.b_bd0, sizeof(int) * (h->nb + 1), cudaMemcpyDeviceToHost));
+    std::vector<mel_mon_op> ops;
+    int row = 6;
+    bool forces = false;
+    for (int i = 0; i < n_monitored; i++) {
+        const double* e = monitored + (size_t)MEL_MON_NF * i;
+        mel_mon_op o;
+        memset(&o, 0, sizeof o);
+        o.type = (int)e[0];
+        o.node = -1;
+        auto body_ok = [&](int b) { return b >= 0 && b < h->nb; };
+        auto bad = [&](const char* what) {
+            mel_set_error("monitored entry %d (type %d): %s", i, o.type, what);
+            return MEL_ERR_INVALID;
+        };
+        if (o.type >= 0 && o.type <= 3) {
+            o.kind = (int)e[1]; o.body = (int)e[2]; o.node = (int)e[3];
+            if (o.type == 0 && o.kind >= 3) continue;    // Length / Area / AllX / AllY: spies only
+            if (!body_ok(o.body) || o.node >= nodes_of[o.body]) return bad("body or node out of range");
+            if (o.kind >= 0 && o.kind <= (o.type == 0 ? 2 : 3)) row++;
+        } else if (o.type == 4) {
+            o.kind = (int)e[1]; o.sub = (int)e[2]; o.body = (int)e[3]; o.node = (int)e[4];
+            if (!body_ok(o.body) || o.node >= nodes_of[o.body] || o.sub < 0 || o.sub > 7) return bad("body, node or force kind out of range");
+            if (o.node < 0 && h->b_type[o.body] == MEL_BODY_DEFORMABLE) {
+                // Code/Monitoring.h:232 walks as many nodes as body number `sub` has
+                if (o.sub >= h->nb || nodes_of[o.sub] > nodes_of[o.body])
+                    return bad("the reference sums over as many nodes as body number <force kind> has, more than the body holds");
+            }
+            if (o.node >= 0 || h->b_type[o.body] == MEL_BODY_DEFORMABLE) forces = true;
+            if (o.kind >= 0 && o.kind <= 3) row++;
+        } else if (o.type == 5 || o.type == 6 || o.type == 8) {
+            mel_set_error("monitored entry %d: type %d (%s) needs %s, which this library does not run", i, o.type,
+                          o.type == 5 ? "Jacobian" : o.type == 6 ? "Stress" : "Damage",
+                          o.type == 8 ? "Body::Update_damage" : "the nodal stress post-processing (Code/Body.h:2310-2519)");
+            return MEL_ERR_UNSUPPORTED;
+        } else if (o.type == 7) {
+            o.kind = (int)e[1]; o.body = (int)e[2]; o.border = (int)e[3]; o.bnode = (int)e[4];
+            if (!body_ok(o.body)) return bad("body out of range");
+            // a value only while that slave node has a contact element: rows vary in length
+            if (o.kind >= 0 && o.kind <= 5) row++;
+        } else if (o.type == 9) {
+            o.kind = (int)e[1]; o.body = (int)e[2];
+            if (o.body >= h->nb || o.body < -1) return bad("body out of range");
+            row++;
+        } else if (o.type == 10) {
+            o.kind = (int)e[1]; o.body = (int)e[2];
+            if (o.body >= h->nb || o.body < -1) return bad("body out of range");
+            if (o.body == -1 || (o.kind >= 0 && o.kind < 7)) row++;
+        } else {
+            continue;                                    // types Monitoring ignores add no column
+        }
+        ops.push_back(o);
+    }
+    if (monitor_energy) row += 3;
+    if (monitor_boundaries) {
+        if (h->nb < 2 || bd0[1] - bd0[0] < 1 || bd0[2] - bd0[1] < 2) {
+            mel_set_error("MONITOR_BOUNDARIES reads border 0 of body 0 and border 1 of body 1, which this model lacks");
+            return MEL_ERR_INVALID;
+        }
+        row += 4;
+    }
+    for (void* p : { (void*)h->mon_ops, (void*)h->mon_part, (void*)h->mon_rows }) if (p) cudaFree(p);
+    h->mon_ops = nullptr; h->mon_part = nullptr; h->mon_rows = nullptr;
+    h->mon_on = false; h->mon_forces = false; h->mon_count = 0; h->mon_cap = 0; h->mon_nops = 0;
+    if (max_row_length) *max_row_length = on ? row : 0;
+    h->iteration = first_iteration;
+    if (!on) return MEL_OK;
+    const size_t stride = (size_t)row + 1;
+    if (cudaMalloc(&h->mon_ops, sizeof(mel_mon_op) * (ops.size() + 1)) != cudaSuccess ||
+        cudaMalloc(&h->mon_part, sizeof(double) * 3 * ((size_t)h->nb + 1)) != cudaSuccess ||
+        cudaMalloc(&h->mon_rows, sizeof(double) * stride * (size_t)ring_rows) != cudaSuccess) {
+        for (void* p : { (void*)h->mon_ops, (void*)h->mon_part, (void*)h->mon_rows }) if (p) cudaFree(p);
+        h->mon_ops = nullptr; h->mon_part = nullptr; h->mon_rows = nullptr;
+        mel_set_error("monitoring buffers (%d rows of %d values) could not be allocated", ring_rows, row);
+        return MEL_ERR_OOM;
+    }
+    if (!ops.empty()) MEL_CUDA_OK(cudaMemcpy(h->mon_ops, ops.data(), sizeof(mel_mon_op) * ops.size(), cudaMemcpyHostToDevice));
+    h->mon_nops = (int)ops.size();
+    h->mon_energy = monitor_energy ? 1 : 0;
+    h->mon_bound = monitor_boundaries ? 1 : 0;
+    h->mon_stride = (int)stride;
+    h->mon_cap = ring_rows;
+    h->mon_on = true;
+    h->mon_forces = forces;
+    if (forces) h->d.record_forces = 1;
+    return MEL_OK;
+}
+
+mel_status mel_monitor_rows(mel_handle* h, double* rows, int max_rows, int* n_rows)
+{
+    if (!h || !n_rows || max_rows < 0) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    *n_rows = h->mon_count;
+    if (h->mon_count == 0 || (!rows && max_rows == 0)) return MEL_OK;    // nothing held, or a count query
+    if (!rows || max_rows < h->mon_count) {
+        mel_set_error("%d monitoring rows are recorded, the buffer holds %d", h->mon_count, max_rows);
+        return MEL_ERR_INVALID;
+    }
+    MEL_CUDA_OK(cudaMemcpy(rows, h->mon_rows, sizeof(double) * (size_t)h->mon_stride * h->mon_count, cudaMemcpyDeviceToHost));
+    h->mon_count = 0;
+    return MEL_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Write_dynamic (Code/IO.h:2351-2640): the reference's restart file from the device state
+// ---------------------------------------------------------------------------------------------
+mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info* info)
+{
+    if (!h || !dir || !info) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    if (info->number_save < 0 || info->number_save >= 100000) { mel_set_error("number_save %d outside 0..99999", info->number_save); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    if (!h->d.record_forces) {
+        mel_set_error("the FORCES blocks need the nodal forces of the last step: call mel_record_forces(h, 1) before it");
+        return MEL_ERR_INVALID;
+    }
+    if (h->pressure_state == 2) {
+        mel_set_error("the contact list changed since the last step: its contact pressures are gone");
+        return MEL_ERR_INVALID;
+    }
+    update_pressures(h);
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    const size_t nn = (size_t)h->nn, nb = (size_t)h->nb, ne = (size_t)h->ne, nbd = (size_t)h->nbd;
+    const mel_dev& D = h->d;
+    auto get = [&](auto* dst, const auto* src, size_t n) {
+        return n ? cudaMemcpy(dst, src, sizeof(*dst) * n, cudaMemcpyDeviceToHost) : cudaSuccess;
+    };
+    std::vector<double2> x(nn), u(nn), v(nn), a(nn), up(nn), vp(nn), ap(nn), mass(nn);
+    std::vector<double2> fint(nn), fcon(nn), fneu(nn), fdir(nn), ftot(nn), bcp(ne);
+    std::vector<double> rg(MEL_RIGID_NF * nb), rf(15 * nb), rtot(3 * nb), works(7 * nb), len(ne), cpx(ne), cpy(ne);
+    std::vector<int> bd0(nb + 1), e0(nbd + 1), sn(4 * ne), ss(4 * ne), nbn(nb), cont0(nb + 1);
+    std::vector<mel_contact> cont(D.ncont);
+    const double2* srcs[] = { D.x, D.u, D.v, D.a, D.up, D.vp, D.ap, D.mass, D.o_fint, D.o_fcon, D.o_fneu, D.o_fdir, D.o_ftot };
+    std::vector<double2>* dsts[] = { &x, &u, &v, &a, &up, &vp, &ap, &mass, &fint, &fcon, &fneu, &fdir, &ftot };
+    for (int k = 0; k < 13; k++) MEL_CUDA_OK(get(dsts[k]->data(), srcs[k], nn));
+    MEL_CUDA_OK(get(bcp.data(), D.e_bcp, ne));
+    MEL_CUDA_OK(get(rg.data(), D.rg, rg.size()));
+    MEL_CUDA_OK(get(rf.data(), D.rf, rf.size()));
+    MEL_CUDA_OK(get(rtot.data(), D.rtot, rtot.size()));
+    MEL_CUDA_OK(get(works.data(), D.works, works.size()));
+    MEL_CUDA_OK(get(len.data(), D.e_len, ne));
+    MEL_CUDA_OK(get(cpx.data(), D.cpx, ne));
+    MEL_CUDA_OK(get(cpy.data(), D.cpy, ne));
+    MEL_CUDA_OK(get(bd0.data(), D.b_bd0, nb + 1));
+    MEL_CUDA_OK(get(e0.data(), D.bd_e0, nbd + 1));
+    MEL_CUDA_OK(get(sn.data(), D.e_sn, 4 * ne));
+    MEL_CUDA_OK(get(ss.data(), D.e_ss, 4 * ne));
+    MEL_CUDA_OK(get(cont0.data(), D.b_cont0, nb + 1));
+    MEL_CUDA_OK(get(cont.data(), D.cont, (size_t)D.ncont));
+    std::vector<int> nbr;
+    if (h->P.nbr && h->P.nbn) {
+        MEL_CUDA_OK(get(nbn.data(), h->P.nbn, nb));
+        nbr.resize((size_t)3 * h->P.nbr_cap * nb);
+        MEL_CUDA_OK(get(nbr.data(), h->P.nbr, nbr.size()));
+    }
+    static const char* solver_names[] = { "Euler", "Adaptive_Euler", "Mass_Scaling", "Adaptive_Mass_Scaling", "Euler_2" };
+    static const char* status_names[] = { "active", "inactive", "nogravity" };
+    char fname[64];
+    snprintf(fname, sizeof fname, "/DYNAMIC_%05d.asc", info->number_save);
+    const std::string path = std::string(dir) + fname;
+    std::ofstream F(path);
+    if (!F) { mel_set_error("cannot write %s", path.c_str()); return MEL_ERR_IO; }
+    const char* bar = "%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%%";
+    F << std::endl << bar << std::endl << "%%%%%%%          GENERAL DATA          %%%%%%%" << std::endl << bar << std::endl << std::endl;
+    F << "SIMULATION_NAME" << std::endl << (info->simulation_name ? info->simulation_name : "") << std::endl << std::endl;
+    F << "SOLVER" << std::endl << solver_names[h->solver] << std::endl;
+    F << std::setprecision(16) << info->number_save << ' ' << info->number_iteration << ' ' << h->time << ' ' << info->number_print << std::endl;
+    F << std::setprecision(10) << h->dt << std::endl;       // this precision holds for the rest of the file
+    F << info->next_save << ' ' << info->next_print << ' ' << h->next_cup << std::endl << std::endl;
+    const char* flag_lines[MEL_NFLAGS] = { nullptr, "MONITOR_ENERGY", "MONITOR_BOUNDARIES", nullptr, "UPDATE_MASS_MATRIX",
+                                           "UPDATE_STIFFNESS_MATRIX", "UPDATE_DAMPING_MATRIX", "NO_LOG", "NO_MONITORING",
+                                           "NO_SELF_CONTACT", nullptr };
+    for (int k = 0; k < MEL_NFLAGS; k++) if (flag_lines[k] && h->flags[k] == 1) F << flag_lines[k] << std::endl;
+    F << std::endl;
+    for (size_t i = 0; i < nb; i++) {
+        const int n0 = h->b_node0[i], nbn_i = h->b_node0[i + 1] - n0;
+        const bool def = h->b_type[i] == MEL_BODY_DEFORMABLE;
+        const int st = h->b_status[i] >= 0 && h->b_status[i] <= 2 ? h->b_status[i] : 0;
+        F << bar << std::endl << "%%%%%%%             BODY " << i << "             %%%%%%%" << std::endl << bar << std::endl << std::endl;
+        F << (def ? "DEFORMABLE" : "RIGID") << std::endl << status_names[st] << std::endl << i << std::endl << std::endl;
+        F << "KINEMATICS" << std::endl;
+        if (def) {
+            F << nbn_i << std::endl;
+            for (int j = 0; j < nbn_i; j++) {
+                const size_t q = (size_t)n0 + j;
+                F << j << ' ' << x[q].x << ' ' << x[q].y << ' ' << u[q].x << ' ' << u[q].y << ' ' << v[q].x << ' ' << v[q].y << ' '
+                  << a[q].x << ' ' << a[q].y << ' ' << up[q].x << ' ' << up[q].y << ' ' << vp[q].x << ' ' << vp[q].y << ' '
+                  << ap[q].x << ' ' << ap[q].y << std::endl;
+            }
+            F << std::endl << "FORCES" << std::endl;
+            const bool ng = h->b_status[i] == MEL_STATUS_NOGRAVITY;
+            const double gx = ng ? 0. : D.gx, gy = ng ? 0. : D.gy;
+            for (int j = 0; j < nbn_i; j++) {
+                const size_t q = (size_t)n0 + j;
+                // self-contact, damping: zero (no damping matrices; the reference never fills the
+                // self-contact components)
+                F << j << ' ' << fint[q].x << ' ' << fint[q].y << ' ' << fcon[q].x << ' ' << fcon[q].y << ' ' << 0. << ' ' << 0. << ' '
+                  << mass[q].x * gx << ' ' << mass[q].y * gy << ' ' << fdir[q].x << ' ' << fdir[q].y << ' '
+                  << fneu[q].x << ' ' << fneu[q].y << ' ' << 0. << ' ' << 0. << ' ' << ftot[q].x << ' ' << ftot[q].y << std::endl;
+            }
+            F << std::endl;
+        } else {
+            const double* r = &rg[MEL_RIGID_NF * i];
+            const double* f = &rf[15 * i];
+            F << r[MEL_RG_XC] << ' ' << r[MEL_RG_YC] << ' ' << r[MEL_RG_RC] << std::endl;
+            F << r[MEL_RG_XD] << ' ' << r[MEL_RG_YD] << ' ' << r[MEL_RG_RD] << std::endl;
+            F << r[MEL_RG_XV] << ' ' << r[MEL_RG_YV] << ' ' << r[MEL_RG_RV] << std::endl << std::endl;
+            F << "FORCES" << std::endl;
+            for (int k = 0; k < 5; k++) F << f[3 * k] << ' ' << f[3 * k + 1] << ' ' << f[3 * k + 2] << std::endl;
+            F << rtot[3 * i] << ' ' << rtot[3 * i + 1] << ' ' << rtot[3 * i + 2] << std::endl << std::endl;
+        }
+        const double* w = &works[7 * i];
+        F << "WORKS" << std::endl << w[0] << ' ' << w[1] << ' ' << w[2] << ' ' << w[3] << ' ' << w[4] << ' ' << w[5] << ' ' << w[6]
+          << std::endl << std::endl;
+        F << "NEIGHBOURS" << std::endl;
+        const int nnb = nbr.empty() ? 0 : nbn[i];
+        F << nnb << std::endl;
+        for (int j = 0; j < nnb; j++) {
+            const int* q = &nbr[(size_t)3 * h->P.nbr_cap * i + 3 * j];
+            F << q[0] << ' ' << q[1] << ' ' << q[2] << std::endl;
+        }
+        F << std::endl << "BORDERS" << std::endl << std::endl;
+        for (int g = bd0[i]; g < bd0[i + 1]; g++) {
+            F << g - bd0[i] << std::endl << e0[g + 1] - e0[g] << std::endl;
+            for (int e = e0[g]; e < e0[g + 1]; e++) {
+                F << len[e] << ' ';
+                F << sn[4 * e] << ' ' << ss[4 * e] << ' ' << sn[4 * e + 1] << ' ' << ss[4 * e + 1] << ' ';
+                F << sn[4 * e + 2] << ' ' << ss[4 * e + 2] << ' ' << sn[4 * e + 3] << ' ' << ss[4 * e + 3] << std::endl;
+            }
+            F << std::endl;
+        }
+        F << "CONTACTS" << std::endl << cont0[i + 1] - cont0[i] << std::endl;
+        for (int k = cont0[i]; k < cont0[i + 1]; k++) {
+            const mel_contact& c = cont[k];
+            F << c.borderS << ' ' << c.border_nodeS << ' ' << c.nodeS << ' ';
+            F << c.bodyM << ' ' << c.borderM << ' ' << c.shiftM << ' ' << c.segmentM << ' ';
+            F << c.gapn << ' ' << c.gapt << ' ' << c.xsi << ' ';
+            F << c.xnorm << ' ' << c.ynorm << ' ' << c.xtan << ' ' << c.ytan << ' ';
+            F << c.length << ' ' << c.fx << ' ' << c.fy << ' ';
+            for (int q = 0; q < 4; q++) F << c.nodeM[q] << ' ' << c.shapeM[q] << ' ' << c.shiftMk[q] << ' ';
+            F << c.effective_mass << ' ' << c.nb_internal;
+            for (int q = 0; q < c.nb_internal && q < MEL_NINTERNAL; q++) F << ' ' << c.internal[q];
+            F << std::endl;
+        }
+        F << std::endl << "CONTACT_PRESSURES" << std::endl << std::endl;
+        for (int g = bd0[i]; g < bd0[i + 1]; g++) {
+            F << g - bd0[i] << std::endl << e0[g + 1] - e0[g] << std::endl;
+            for (int e = e0[g]; e < e0[g + 1]; e++) F << cpx[e] << ' ' << cpy[e] << std::endl;
+            F << std::endl;
+        }
+        F << std::endl << "BC_PRESSURES" << std::endl << std::endl;
+        for (int g = bd0[i]; g < bd0[i + 1]; g++) {
+            F << g - bd0[i] << std::endl << e0[g + 1] - e0[g] << std::endl;
+            for (int e = e0[g]; e < e0[g + 1]; e++) F << bcp[e].x << ' ' << bcp[e].y << std::endl;
+            F << std::endl;
+        }
+        F << std::endl;
+    }
+    F.close();
+    if (!F) { mel_set_error("writing %s failed", path.c_str()); return MEL_ERR_IO; }
     return MEL_OK;
 }
 

@@ -408,6 +408,14 @@ class Scene:
     solver_params: Tuple[float, ...] = (1e-3, 0.2, 1.0, 100.0, 1.0, 1.0, 0.99, 1e3)
     self_contact: bool = True
     initialize_czm: bool = False    # INITIALIZE_CZM: internal variables of the set-up contacts (Code/Proximity.h:481)
+    # output control: MONITORING entries as STATIC_CONTROL lines (the Read_spy_line grammar,
+    # Code/IO.h:11-590), MONITOR_ENERGY / MONITOR_BOUNDARIES, Save_period and Print_period (None:
+    # one save and one print at the end)
+    monitored: List[str] = dataclasses.field(default_factory=list)
+    monitor_energy: bool = False
+    monitor_boundaries: bool = False
+    save_period: Optional[float] = None
+    print_period: Optional[float] = None
     meta: dict = dataclasses.field(default_factory=dict)
 
     @property
@@ -592,6 +600,8 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
         flags[8] = 1                      # NO_MONITORING (also disables self contact, Proximity.h:332)
     if scene.initialize_czm:
         flags[3] = 1                      # INITIALIZE_CZM
+    flags[1] = int(scene.monitor_energy)
+    flags[2] = int(scene.monitor_boundaries)
     f["flags"] = flags
     names = [m[0] for m in scene.materials]
     f["material_type"] = np.array([m[1] for m in scene.materials], dtype=np.int32)
@@ -771,11 +781,14 @@ def write_asc(scene: Scene, directory: str, workers: int = 1) -> None:
         L.append(f"{_g(sp_[0])} {_g(sp_[1])} {_g(sp_[2])}")
     if scene.solver in (2, 3):
         L.append(f"{_g(sp_[3])} {_g(sp_[4])} {_g(sp_[5])} {_g(sp_[6])}")
-    L += [f"{_g(tend)} {_g(tend)} {_g(scene.contact_update_period)}", " ",
+    save = scene.save_period if scene.save_period is not None else tend
+    prnt = scene.print_period if scene.print_period is not None else tend
+    L += [f"{_g(save)} {_g(prnt)} {_g(scene.contact_update_period)}", " ",
           "PERIODIC_BOUNDARIES", f"{_g(scene.period[0])} {_g(scene.period[1])}", " ",
           "GRAVITY", f"{_g(scene.gravity[0])} {_g(scene.gravity[1])}", " ",
           "NUMBER_BODIES", str(len(scene.bodies)), " ",
-          "MONITORING", "0", " ", "SPIES", "0", " ", "DEACTIVATION", "0", " "]
+          "MONITORING", str(len(scene.monitored))] + list(scene.monitored) + [
+          " ", "SPIES", "0", " ", "DEACTIVATION", "0", " "]
     for bi, b in enumerate(scene.bodies):
         L += [" ", "DEFORMABLE" if b.kind == "deformable" else "RIGID", str(bi), names[b.material],
               "Periodic" if b.periodic else "Simple",
@@ -800,9 +813,13 @@ def write_asc(scene: Scene, directory: str, workers: int = 1) -> None:
     with open(os.path.join(directory, "DYNAMIC_00000.asc"), "w") as fh:
         tend = scene.dt * scene.nsteps
         fh.write(" \nSIMULATION_NAME\n%s\n \nSOLVER\n%s\n0 0 0 0 \n%s\n%s %s %s \nNO_LOG\n" % (
-            scene.name, SOLVER_NAMES[scene.solver], _g(scene.dt), _g(tend), _g(tend), _g(0.0)))
+            scene.name, SOLVER_NAMES[scene.solver], _g(scene.dt), _g(save), _g(prnt), _g(0.0)))
         if not scene.self_contact:
             fh.write("NO_MONITORING\n")
+        if scene.monitor_energy:
+            fh.write("MONITOR_ENERGY\n")
+        if scene.monitor_boundaries:
+            fh.write("MONITOR_BOUNDARIES\n")
         if scene.initialize_czm:
             fh.write("INITIALIZE_CZM\n")
         fh.write(" \n")

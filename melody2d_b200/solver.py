@@ -65,6 +65,14 @@ SIGNATURES = {
     "mel_batch_stats": [_vp, _dp, C.POINTER(C.c_longlong), _ip],
     "mel_batch_destroy": [_vp],
     "mel_get_health": [_vp, _ip],
+    "mel_get_bc_pressures": [_vp, _dp, _dp],
+    "mel_monitor_setup": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip],
+    "mel_monitor_rows": [_vp, _dp, C.c_int, _ip],
+    "mel_write_dynamic": [_vp, C.c_char_p, C.POINTER(abi.MelSaveInfo)],
+    "mel_load_run_control": [_vp, C.POINTER(abi.MelRunControl)],
+    "mel_create_loaded": [_vp, C.POINTER(abi.MelOptions), C.POINTER(_vp)],
+    "mel_mls_shapes": [C.c_int, _ip, _dp, _dp, _ip, _dp, C.POINTER(C.c_longlong), _ip, _dp, _dp, _dp,
+                       C.c_longlong, C.POINTER(C.c_longlong), C.c_int, _dp],
 }
 
 
@@ -135,6 +143,7 @@ class Solver:
         self.nn = nn
         self.nb = nb
         self._keep = keep
+        self._mon_len = 0
 
     # ---- construction -------------------------------------------------------------------
     @classmethod
@@ -245,6 +254,45 @@ class Solver:
         _check(lib().mel_get_contact_pressures(self.h, _ptr(px), _ptr(py)))
         return np.stack([px[:ne], py[:ne]], axis=1)
 
+    def bc_pressures(self) -> np.ndarray:
+        """Border-condition pressures of the last step, (n_border_entries, 2)."""
+        ne = self.sizes()["n_border_nodes"]
+        px = np.zeros(max(ne, 1)); py = np.zeros(max(ne, 1))
+        _check(lib().mel_get_bc_pressures(self.h, _ptr(px), _ptr(py)))
+        return np.stack([px[:ne], py[:ne]], axis=1)
+
+    def monitor_setup(self, monitored, energy: bool = False, boundaries: bool = False, ring_rows: int = 1000,
+                      first_iteration: int = 0) -> int:
+        """Device Monitoring (mel_monitor_setup): `monitored` is a list of Read_spy_line vectors;
+        returns the longest row."""
+        m = np.zeros((max(len(monitored), 1), abi.MEL_MON_NF))
+        for i, e in enumerate(monitored):
+            m[i, :len(e)] = e
+        L = C.c_int()
+        _check(lib().mel_monitor_setup(self.h, _ptr(m), len(monitored), int(energy), int(boundaries), ring_rows,
+                                       first_iteration, C.byref(L)))
+        self._mon_len = L.value
+        return L.value
+
+    def monitor_rows(self) -> list:
+        """The monitoring rows recorded since the last call, one float64 array each."""
+        n = C.c_int()
+        _check(lib().mel_monitor_rows(self.h, None, 0, C.byref(n)))
+        if n.value == 0:
+            return []
+        stride = self._mon_len + 1
+        buf = np.zeros(n.value * stride)
+        _check(lib().mel_monitor_rows(self.h, _ptr(buf), n.value, C.byref(n)))
+        rows = buf.reshape(n.value, stride)
+        return [r[1:1 + int(r[0])].copy() for r in rows]
+
+    def write_dynamic(self, directory: str, number_save: int, number_iteration: int, number_print: int = 0,
+                      next_save: float = 0.0, next_print: float = 0.0, name: str = "") -> str:
+        """Write_dynamic: <directory>/DYNAMIC_<number_save>.asc in the reference's layout."""
+        info = abi.MelSaveInfo(name.encode(), number_save, number_iteration, number_print, next_save, next_print)
+        _check(lib().mel_write_dynamic(self.h, directory.encode(), C.byref(info)))
+        return os.path.join(directory, "DYNAMIC_%05d.asc" % number_save)
+
     def set_contacts(self, arr: np.ndarray):
         buf = abi.numpy_to_contacts(arr)
         _check(lib().mel_set_contacts(self.h, buf, len(arr)))
@@ -320,6 +368,62 @@ class Solver:
         _check(lib().mel_get_sizes(self.h, *[C.byref(x) for x in v]))
         keys = ("n_bodies", "n_nodes", "n_gauss", "n_gp_entries", "n_node_entries", "n_border_nodes")
         return {k: x.value for k, x in zip(keys, v)}
+
+
+def mls_shapes(bodies, device: int = 0, timing: Optional[dict] = None):
+    """Shape functions at Gauss points on the device (mel_mls_shapes) for a list of bodies, each a
+    (points (P,2), nodes (n,2), radii (n,)) triple.  Returns one (ptr, idx, N, dNdx, dNdy) CSR
+    tuple per body, the layout generator.mls_shape returns.  `timing`, when given, receives the
+    value pass's device milliseconds."""
+    bnp = np.zeros(len(bodies) + 1, dtype=np.int32)
+    bpp = np.zeros(len(bodies) + 1, dtype=np.int32)
+    for i, (pts, nodes, radii) in enumerate(bodies):
+        bnp[i + 1] = bnp[i] + nodes.shape[0]
+        bpp[i + 1] = bpp[i] + pts.shape[0]
+    nodes = np.ascontiguousarray(np.concatenate([b[1] for b in bodies]), dtype=np.float64)
+    radii = np.ascontiguousarray(np.concatenate([b[2] for b in bodies]), dtype=np.float64)
+    pts = np.ascontiguousarray(np.concatenate([b[0] for b in bodies]), dtype=np.float64)
+    np_ = int(bpp[-1])
+    ptr = np.zeros(np_ + 1, dtype=np.int64)
+    ne = C.c_longlong()
+    ip = lambda a: a.ctypes.data_as(_ip)
+    lp = ptr.ctypes.data_as(C.POINTER(C.c_longlong))
+    L = lib()
+    _check(L.mel_mls_shapes(len(bodies), ip(bnp), _ptr(nodes), _ptr(radii), ip(bpp), _ptr(pts), lp, None, None,
+                            None, None, 0, C.byref(ne), device, None))
+    n = ne.value
+    idx = np.zeros(max(n, 1), dtype=np.int32)
+    N, Nx, Ny = np.zeros(max(n, 1)), np.zeros(max(n, 1)), np.zeros(max(n, 1))
+    ms = C.c_double()
+    _check(L.mel_mls_shapes(len(bodies), ip(bnp), _ptr(nodes), _ptr(radii), ip(bpp), _ptr(pts), lp, ip(idx),
+                            _ptr(N), _ptr(Nx), _ptr(Ny), n, C.byref(ne), device, C.byref(ms)))
+    if timing is not None:
+        timing["kernel_ms"] = ms.value
+    out = []
+    for i in range(len(bodies)):
+        a, b = int(bpp[i]), int(bpp[i + 1])
+        e0, e1 = int(ptr[a]), int(ptr[b])
+        out.append((ptr[a:b + 1] - e0, idx[e0:e1].astype(np.int64), N[e0:e1], Nx[e0:e1], Ny[e0:e1]))
+    return out
+
+
+def load_run_control(directory: str, restart_index: int = 0) -> dict:
+    """What the input files say about output (mel_load_run_control): periods, counters, the
+    MONITORING entries (Read_spy_line vectors) and the DYNAMIC flags.  No GPU needed."""
+    L = lib()
+    dp = C.POINTER(abi.MelModelDesc)()
+    owner = C.c_void_p()
+    _check(L.mel_load_desc(directory.encode(), restart_index, C.byref(dp), C.byref(owner)))
+    try:
+        rc = abi.MelRunControl()
+        _check(L.mel_load_run_control(owner, C.byref(rc)))
+        mon = np.ctypeslib.as_array(rc.monitored).reshape(abi.MEL_MON_MAX, abi.MEL_MON_NF)[:rc.n_monitored].copy()
+        return {"simulation_name": rc.simulation_name.decode(), "save_period": rc.save_period,
+                "print_period": rc.print_period, "next_save": rc.next_save, "next_print": rc.next_print,
+                "number_save": rc.number_save, "number_iteration": rc.number_iteration,
+                "number_print": rc.number_print, "monitored": mon, "flags": list(rc.flags)}
+    finally:
+        L.mel_free_desc(owner)
 
 
 def load_desc_arrays(directory: str, restart_index: int = 0) -> dict:

@@ -8,6 +8,10 @@
 // usage: ref_harness <case_dir> <nsteps> <dump_file> <dump_every> [threads]
 //   dump records: after set-up (step 0), after each multiple of dump_every, and around every
 //   proximity update (tag 0 = before Update_proximity, tag 1 = after).
+// environment: REF_RESTART=k starts from DYNAMIC_k (argv[1] of Code/main.cpp); REF_OUTPUTS=1 also
+//   runs the loop's output steps (Code/main.cpp:170-222): Monitoring every iteration unless
+//   NO_MONITORING, the print counter, and at each save Write_dynamic and Write_monitoring, which
+//   write DYNAMIC_nnnnn.asc and MONITORING.asc into case_dir as the reference does.
 #include <iostream>
 #include <fstream>
 #include <iomanip>
@@ -165,7 +169,9 @@ int main(int argc, char** argv)
                  Activate_plot, Xmin_plot, Xmax_plot, Ymin_plot, Ymax_plot,
                  Nb_monitored, Monitored, Nb_deactivated, Deactivated, Nb_spies, Spies,
                  Nb_regions, Regions, Nb_bodies, Bodies, To_Plot ) ;
-    Number_save = 0 ;
+    Number_save = getenv("REF_RESTART") ? atoi(getenv("REF_RESTART")) : 0 ;
+    const bool outputs = getenv("REF_OUTPUTS") && atoi(getenv("REF_OUTPUTS")) == 1 ;
+    vector<vector<double>> monitoring ;
     Load_dynamic( Number_save, Number_print, Time, Number_iteration, Deltat, Solver,
                   Next_save, Next_print, Next_contact_update, Xmin_period, Xmax_period, Bodies, flags ) ;
     // set-up of Code/main.cpp:104-127
@@ -197,6 +203,9 @@ int main(int argc, char** argv)
                         Target_error, Inv_Target_error, Control_parameter, Accepted_ratio,
                         Max_mass_scaling, Control_parameter_mass_scaling, Error_factor_mass_scaling, Decrease_factor_mass_scaling,
                         neval, max_error, mean_error, flags, total_mass, max_mass, Solver) ;
+        if (outputs && flags[8]==0)
+            Monitoring(Nb_bodies, Bodies, Time, Deltat, Number_iteration, neval, max_error, mean_error, flags,
+                       monitoring, Nb_monitored, Monitored) ;
         bool prox = Time > Next_contact_update-1.e-6*Deltat ;
         if (prox || (every > 0 && it % every == 0)) dump_state(it, 0, Time, Deltat, Bodies);
         if (prox) {
@@ -206,6 +215,19 @@ int main(int argc, char** argv)
             Update_status(Nb_bodies, Bodies, Nb_deactivated, Deactivated) ;
             t_prox += std::chrono::duration<double>(std::chrono::steady_clock::now() - p0).count();
             dump_state(it, 1, Time, Deltat, Bodies);
+        }
+        if (outputs) {
+            if ( Time > Next_print-1.e-6*Deltat ) {
+                Number_print = Number_print + 1 ;
+                Next_print = Next_print + Print_period ;
+            }
+            if ( Time > Next_save-1.e-6*Deltat ) {
+                Number_save = Number_save + 1 ;
+                Next_save = Next_save + Save_period ;
+                Write_dynamic( Simulation_name, Number_save, Number_print, Time, Number_iteration, Deltat, Solver,
+                               Next_save, Next_print, Next_contact_update, Nb_bodies, Bodies, flags ) ;
+                if (flags[8]==0) Write_monitoring( monitoring, flags ) ;
+            }
         }
     }
     double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
