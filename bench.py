@@ -545,6 +545,13 @@ def compare_precisions(args, rank, world, local, pg):
     flat = g.flatten(scene)
     a = Solver.from_flat(flat, precision=0, device=local)
     b = Solver.from_flat(flat, precision=1, device=local)
+    # chaos gauge: an FP64 twin whose displacement parameters start one unit in the last place away
+    # (relative 1e-16, far below the mixed form's first-step difference): how fast the sample itself
+    # amplifies a difference, whatever its source
+    c = Solver.from_flat(flat, precision=0, device=local)
+    st = c.node_state()
+    st[:, 6:8] = np.nextafter(st[:, 6:8], np.inf)
+    c.set_node_state(st)
 
     def rel(x, y):
         x, y = np.asarray(x, float), np.asarray(y, float)
@@ -556,21 +563,29 @@ def compare_precisions(args, rank, world, local, pg):
         try:
             a.step(k - done)
             b.step(k - done)
+            c.step(k - done)
         except MelError as e:          # the sample diverged (both forms run the same physics)
             stopped = {"after_steps": done, "error": str(e)}
             break
         done = k
-        ma, mb = a.monitor(), b.monitor()
-        rows.append({"steps": k,
-                     "kinetic_energy": rel(mb.kinetic_energy, ma.kinetic_energy),
-                     "wall_contact_force": rel(list(mb.rigid_force), list(ma.rigid_force)),
-                     "wall_reaction": rel(list(mb.rigid_dirichlet), list(ma.rigid_dirichlet)),
-                     "mean_displacement": rel(list(mb.mean_displacement), list(ma.mean_displacement)),
-                     "active_contacts": [mb.active_contacts, ma.active_contacts]})
-    print(json.dumps({"report": "mixed vs fp64 (relative errors; active_contacts = [mixed, fp64])",
+        ma, mb, mc = a.monitor(), b.monitor(), c.monitor()
+
+        def errs(m):
+            return {"kinetic_energy": rel(m.kinetic_energy, ma.kinetic_energy),
+                    "wall_contact_force": rel(list(m.rigid_force), list(ma.rigid_force)),
+                    "wall_reaction": rel(list(m.rigid_dirichlet), list(ma.rigid_dirichlet)),
+                    "mean_displacement": rel(list(m.mean_displacement), list(ma.mean_displacement))}
+        row = {"steps": k}
+        row.update(errs(mb))
+        row["active_contacts"] = [mb.active_contacts, ma.active_contacts]
+        row["fp64_twin_1ulp"] = errs(mc)
+        rows.append(row)
+    print(json.dumps({"report": "mixed vs fp64 (relative errors; active_contacts = [mixed, fp64]); fp64_twin_1ulp: "
+                                "an FP64 run started one ulp away, against the FP64 run",
                       "workload": f"biaxial {args.discs} discs", "rows": rows, "diverged": stopped}), flush=True)
     a.close()
     b.close()
+    c.close()
 
 
 def main():

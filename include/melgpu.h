@@ -327,7 +327,8 @@ typedef struct mel_save_info {
  * back to restart): kinematics, forces, works, neighbours, border segments, contact elements,
  * contact and border-condition pressures, and the Time, Deltat and Next_contact_update of the
  * handle.  The FORCES blocks are the nodal forces of the last step, so mel_record_forces must have
- * been on during it (MEL_ERR_INVALID otherwise); damping and self-contact components are zero. */
+ * been on during it (MEL_ERR_INVALID otherwise); the self-contact components are zero, as the
+ * reference never fills them. */
 mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info* info);
 
 /* Rigid-body records (layout MEL_RG_*, n_bodies records); node positions follow (restart upload). */

@@ -105,6 +105,12 @@ struct mel_dev {
     const int* b_ks0; const unsigned* ks_rec; const int* kg_base;
     const uint16_t* ks_idx; const double* ks_N;
     double2 *o_fint, *o_fcon, *o_fneu, *o_fdir, *o_ftot;
+    // damping matrices (Body::Update_damping_forces): for each degree of freedom (2 node + direction)
+    // the terms it receives, in matrix-entry order: source degree of freedom and coefficient; the
+    // damping forces of the step (NULL without matrices)
+    const int *dmp_ptr, *dmp_src;
+    const double* dmp_c;
+    double2* fdamp;
     // borders and border entries
     const int *bd_body, *bd_per, *bd_bef, *bd_aft, *bd_e0, *bd_bc, *bd_h0;
     const double *bd_bcp, *ht, *hv;
@@ -159,6 +165,8 @@ struct mel_dev {
 };
 
 // kernel launch wrappers (mel_kernels.cu)
+// Update_damping_forces of every deformable body with matrices, from the velocity parameters
+void mel_launch_damping(const mel_dev& d, cudaStream_t s);
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 // Initialize_CZM's pass over the contact list (contact geometry, then the initial bonds)
 void mel_launch_czm_init(const mel_dev& d, cudaStream_t s);

@@ -1105,9 +1105,10 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         double2 fi = s_f[i], fc = s_fc[i];
         double2 fn = has_bc ? s_fn[i] : make_double2(0., 0.);
         double2 fd = has_bc ? s_fd[i] : make_double2(0., 0.);
+        const double2 fdp = d.fdamp ? d.fdamp[gi] : make_double2(0., 0.);
         double2 ft;
-        ft.x = fi.x + fc.x + 0. + fb.x + fd.x + fn.x + 0. + 0.;
-        ft.y = fi.y + fc.y + 0. + fb.y + fd.y + fn.y + 0. + 0.;
+        ft.x = fi.x + fc.x + 0. + fb.x + fd.x + fn.x + fdp.x + 0.;
+        ft.y = fi.y + fc.y + 0. + fb.y + fd.y + fn.y + fdp.y + 0.;
         double2 ap;
         if (AD) { const double2 f = d.fms[gi]; ap = make_double2(ft.x * im.x / f.x, ft.y * im.y / f.y); }
         else ap = make_double2(ft.x * im.x / 1., ft.y * im.y / 1.);
@@ -1128,9 +1129,8 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         s_T[n + i] = dte * (vx * fb.x + vy * fb.y);
         s_T[2 * n + i] = dte * (vx * fd.x + vy * fd.y);
         s_T[3 * n + i] = dte * (vx * fn.x + vy * fn.y);
-        double z = dte * (vx * 0. + vy * 0.);
-        s_T[4 * n + i] = z;
-        s_T[5 * n + i] = z;
+        s_T[4 * n + i] = dte * (vx * fdp.x + vy * fdp.y);
+        s_T[5 * n + i] = dte * (vx * 0. + vy * 0.);
     }
     __syncthreads();
     if (warp == 0) {
@@ -1681,6 +1681,29 @@ void mel_launch_contact_pressures(const mel_dev& d, cudaStream_t s)
     mel::pressure_clear_kernel<<<(d.ne + 255) / 256, 256, 0, s>>>(d);
     if (d.ncont > 0) mel::pressure_push_kernel<<<(d.ncont + 127) / 128, 128, 0, s>>>(d);
     mel::pressure_sum_kernel<<<(d.ne + 127) / 128, 128, 0, s>>>(d);
+}
+
+namespace mel {
+// Body::Update_damping_forces (Code/Body.h:1057-1154): each degree of freedom subtracts its terms
+// v_param(source) * c in matrix-entry order, the order the reference's loop over the entries adds
+// them in; one thread per degree of freedom
+__global__ void __launch_bounds__(256) damping_kernel(mel_dev d)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * d.nn) return;
+    const int a = d.dmp_ptr[k], e = d.dmp_ptr[k + 1];
+    if (a == e) return;
+    const double* vp = reinterpret_cast<const double*>(d.vp);
+    double f = 0.;
+    for (int j = a; j < e; j++) f = f - vp[d.dmp_src[j]] * d.dmp_c[j];
+    reinterpret_cast<double*>(d.fdamp)[k] = f;
+}
+}  // namespace mel
+
+void mel_launch_damping(const mel_dev& d, cudaStream_t s)
+{
+    if (!d.fdamp || d.nn == 0) return;
+    mel::damping_kernel<<<(2 * d.nn + 255) / 256, 256, 0, s>>>(d);
 }
 
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s)

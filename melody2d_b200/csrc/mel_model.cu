@@ -226,8 +226,21 @@ static mel_status validate(const mel_model_desc* d)
         }
         if (d->body_material[b] < 0 || d->body_material[b] >= d->n_materials) { mel_set_error("body %d material out of range", b); return MEL_ERR_INVALID; }
     }
-    for (int i = 0; i < d->n_matrix; i++)
-        if (d->matrix_damping[i] != 0. || d->flags[6] == 1) { mel_set_error("damping matrices (Body::Update_damping_forces) are not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
+    if (d->flags[5] == 1 || d->flags[6] == 1) {
+        mel_set_error("UPDATE_STIFFNESS_MATRIX / UPDATE_DAMPING_MATRIX (matrices rebuilt by Body::Update_material) are not supported on the GPU path");
+        return MEL_ERR_UNSUPPORTED;
+    }
+    if (d->n_matrix > 0) {
+        if (!d->body_matrix_ptr || d->body_matrix_ptr[d->n_bodies] != d->n_matrix) { mel_set_error("body_matrix_ptr does not cover the matrix entries"); return MEL_ERR_INVALID; }
+        for (int b = 0; b < d->n_bodies; b++) {
+            const int nd = 2 * (d->body_node_ptr[b + 1] - d->body_node_ptr[b]);
+            for (int i = d->body_matrix_ptr[b]; i < d->body_matrix_ptr[b + 1]; i++)
+                if (d->matrix_dofs[2 * i] < 0 || d->matrix_dofs[2 * i] >= nd || d->matrix_dofs[2 * i + 1] < 0 || d->matrix_dofs[2 * i + 1] >= nd) {
+                    mel_set_error("matrix entry %d of body %d names a degree of freedom outside the body", i, b);
+                    return MEL_ERR_INVALID;
+                }
+        }
+    }
     return MEL_OK;
 }
 
@@ -392,6 +405,38 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.up = (double2*)dalloc<double>(h, 2 * (size_t)nn);
     D.vp = (double2*)dalloc<double>(h, 2 * (size_t)nn);
     D.ap = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+    // damping matrices (Body::Update_damping_forces, Code/Body.h:1057-1154): every entry (dof0, dof1,
+    // c) of a deformable body gives the terms the reference's branches add, in their order; bucketed
+    // by receiving degree of freedom with the entries' order kept, so each one adds its terms in the
+    // reference's sequence
+    if (d->n_matrix > 0) {
+        std::vector<int> cnt(2 * (size_t)nn + 1, 0);
+        auto terms = [&](auto&& emit) {
+            for (int b = 0; b < nb; b++) {
+                if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+                const int n0 = d->body_node_ptr[b];
+                for (int i = d->body_matrix_ptr[b]; i < d->body_matrix_ptr[b + 1]; i++) {
+                    const int dof0 = d->matrix_dofs[2 * i], dof1 = d->matrix_dofs[2 * i + 1];
+                    const int a = 2 * (n0 + dof0 / 2), c = 2 * (n0 + dof1 / 2);
+                    const int dir0 = dof0 % 2, dir1 = dof1 % 2;
+                    const double cf = d->matrix_damping[i];
+                    emit(a + dir0, c + dir1, cf);                               // node0 receives from node1
+                    if (dir0 != dir1 || dof0 != dof1) emit(c + dir1, a + dir0, cf); // and node1 from node0
+                }
+            }
+        };
+        terms([&](int t, int, double) { cnt[t + 1]++; });
+        for (size_t k = 1; k < cnt.size(); k++) cnt[k] += cnt[k - 1];
+        if (cnt.back() > 0) {
+            std::vector<int> pos(cnt.begin(), cnt.end() - 1), src(cnt.back());
+            std::vector<double> cf(cnt.back());
+            terms([&](int t, int s_, double c_) { src[pos[t]] = s_; cf[pos[t]] = c_; pos[t]++; });
+            D.dmp_ptr = dupload(h, cnt);
+            D.dmp_src = dupload(h, src);
+            D.dmp_c = dupload(h, cf);
+            D.fdamp = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+        }
+    }
     // Solver_step state: temporaries, errors, mass-scaling factors (1), estimators (Code/IO.h:1620,1819)
     D.solver = d->solver;
     for (int k = 0; k < 8; k++) D.sp[k] = d->solver_params[k];
@@ -862,9 +907,11 @@ static mel_status adaptive_step(mel_handle* h)
         MEL_CUDA_OK(cudaMemcpyAsync(h->d.dt, &h->h_red[7], sizeof(double), cudaMemcpyHostToDevice, h->stream));
         mel_dev d = h->d;
         mel_launch_contact(d, 0.5, h->stream);                 // Update_contact_forces(Deltat*0.5)
+        mel_launch_damping(d, h->stream);
         d.phase = 1;
         mel_launch_body_adaptive(d, h->time, h->t_bc, h->nblocks_body, h->body_smem, h->stream);
         mel_launch_contact(d, 0.5, h->stream);
+        mel_launch_damping(d, h->stream);
         d.phase = 2;
         mel_launch_body_adaptive(d, h->time, h->time + h->dt * 0.5, h->nblocks_body, h->body_smem, h->stream);
         h->t_bc = h->time + h->dt;                              // Update_bc(Time+Deltat) of the second half
@@ -1077,6 +1124,7 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             mark();
             mel_launch_contact(h->d, 1.0, h->stream);
             mark(); kinds.push_back(0);
+            if (h->d.fdamp) { mel_launch_damping(h->d, h->stream); h->launches++; }
             mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream);
             mark(); kinds.push_back(1);
             {
@@ -1596,7 +1644,7 @@ mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info
         return n ? cudaMemcpy(dst, src, sizeof(*dst) * n, cudaMemcpyDeviceToHost) : cudaSuccess;
     };
     std::vector<double2> x(nn), u(nn), v(nn), a(nn), up(nn), vp(nn), ap(nn), mass(nn);
-    std::vector<double2> fint(nn), fcon(nn), fneu(nn), fdir(nn), ftot(nn), bcp(ne);
+    std::vector<double2> fint(nn), fcon(nn), fneu(nn), fdir(nn), ftot(nn), bcp(ne), fdmp(nn, make_double2(0., 0.));
     std::vector<double> rg(MEL_RIGID_NF * nb), rf(15 * nb), rtot(3 * nb), works(7 * nb), len(ne), cpx(ne), cpy(ne);
     std::vector<int> bd0(nb + 1), e0(nbd + 1), sn(4 * ne), ss(4 * ne), nbn(nb), cont0(nb + 1);
     std::vector<mel_contact> cont(D.ncont);
@@ -1604,6 +1652,7 @@ mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info
     std::vector<double2>* dsts[] = { &x, &u, &v, &a, &up, &vp, &ap, &mass, &fint, &fcon, &fneu, &fdir, &ftot };
     for (int k = 0; k < 13; k++) MEL_CUDA_OK(get(dsts[k]->data(), srcs[k], nn));
     MEL_CUDA_OK(get(bcp.data(), D.e_bcp, ne));
+    if (D.fdamp) MEL_CUDA_OK(get(fdmp.data(), D.fdamp, nn));
     MEL_CUDA_OK(get(rg.data(), D.rg, rg.size()));
     MEL_CUDA_OK(get(rf.data(), D.rf, rf.size()));
     MEL_CUDA_OK(get(rtot.data(), D.rtot, rtot.size()));
@@ -1662,11 +1711,10 @@ mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info
             const double gx = ng ? 0. : D.gx, gy = ng ? 0. : D.gy;
             for (int j = 0; j < nbn_i; j++) {
                 const size_t q = (size_t)n0 + j;
-                // self-contact, damping: zero (no damping matrices; the reference never fills the
-                // self-contact components)
+                // self-contact: zero (the reference never fills those components)
                 F << j << ' ' << fint[q].x << ' ' << fint[q].y << ' ' << fcon[q].x << ' ' << fcon[q].y << ' ' << 0. << ' ' << 0. << ' '
                   << mass[q].x * gx << ' ' << mass[q].y * gy << ' ' << fdir[q].x << ' ' << fdir[q].y << ' '
-                  << fneu[q].x << ' ' << fneu[q].y << ' ' << 0. << ' ' << 0. << ' ' << ftot[q].x << ' ' << ftot[q].y << std::endl;
+                  << fneu[q].x << ' ' << fneu[q].y << ' ' << fdmp[q].x << ' ' << fdmp[q].y << ' ' << ftot[q].x << ' ' << ftot[q].y << std::endl;
             }
             F << std::endl;
         } else {
@@ -2026,6 +2074,7 @@ mel_status mel_batch_create(int device, int precision, mel_batch** out)
 mel_status mel_batch_admit(mel_batch* b, mel_handle* h)
 {
     if (h && h->solver != MEL_SOLVER_EULER) { mel_set_error("batches advance the Euler scheme; step Solver_step schemes with mel_step"); return MEL_ERR_UNSUPPORTED; }
+    if (h && h->d.fdamp) { mel_set_error("models with damping matrices are stepped with mel_step, not in a batch"); return MEL_ERR_UNSUPPORTED; }
     if (!b || !h) return MEL_ERR_INVALID;
     if (h->batch) { mel_set_error("the handle is already a member of a batch"); return MEL_ERR_INVALID; }
     if (h->device != b->device || h->precision != b->precision) {

@@ -171,6 +171,9 @@ class Body:
     velocity: Tuple[float, float] = (0.0, 0.0)
     angular_velocity: float = 0.0               # rigid only (rad/s)
     dt_terms: Optional[Tuple[float, float]] = None   # critical-step terms (elastic eigenvalue, h/m per kn)
+    # MATRICES of STATIC_DATA (Code/IO.h:1827-1851): upper-triangle (dof0, dof1) pairs, dof = 2 node +
+    # direction, with their stiffness and damping coefficients; None writes an empty section
+    matrices: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
 
 
 def _ccw(nodes: np.ndarray, tri: np.ndarray) -> np.ndarray:
@@ -434,11 +437,10 @@ def material_params_stored(mtype: int, p: List[float]) -> List[float]:
     return [p[0], p[1], p[2], mu, lam, p[5]]
 
 
-def critical_dt(body: Body, mu: float, lam: float, kn: float) -> float:
-    """2/omega_max of the body's lumped-mass elastic operator (the linear part of
-    Update_internal_forces, Body.h:974-997), plus the contact penalty kn*length/m of border nodes."""
+def stiffness_matrix(body: Body, mu: float, lam: float):
+    """The body's linear elastic stiffness K = sum over Gauss points of w J B^T D B (plane strain,
+    the linear part of Update_internal_forces, Body.h:974-997), sparse over dofs 2 node + direction."""
     import scipy.sparse as sp
-    from scipy.sparse.linalg import eigsh
     n = body.nodes.shape[0]
     ptr, idx, _, dx, dy = body.gp
     c0 = body.gp_w * body.gp_J
@@ -453,7 +455,32 @@ def critical_dt(body: Body, mu: float, lam: float, kn: float) -> float:
     B = sp.csr_matrix((v, (r, c)), shape=(3 * G, 2 * n))
     D = np.array([[lam + 2 * mu, lam, 0.0], [lam, lam + 2 * mu, 0.0], [0.0, 0.0, mu]])
     Dg = sp.kron(sp.diags(c0), sp.csr_matrix(D))
-    K = (B.T @ Dg @ B).tocsr()
+    return (B.T @ Dg @ B).tocsr()
+
+
+def add_damping(scene: "Scene", alpha: float, beta: float, mu: float, lam: float) -> None:
+    """Gives every deformable body a MATRICES list: the upper triangle of its stiffness matrix in
+    row-major order, with Rayleigh damping coefficients alpha K_ij (+ beta m_i on the diagonal), the
+    matrix Body::Update_damping_forces (Code/Body.h:1057-1154) applies to the velocity parameters."""
+    for b in scene.bodies:
+        if b.kind != "deformable":
+            continue
+        K = stiffness_matrix(b, mu, lam).tocoo()
+        keep = K.row <= K.col
+        r, c, v = K.row[keep], K.col[keep], K.data[keep]
+        order = np.lexsort((c, r))
+        r, c, v = r[order], c[order], v[order]
+        m = b.mass.reshape(-1)
+        d = alpha * v + np.where(r == c, beta * m[r], 0.0)
+        b.matrices = (np.stack([r, c], axis=1).astype(np.int64), v.astype(np.float64), d.astype(np.float64))
+
+
+def critical_dt(body: Body, mu: float, lam: float, kn: float) -> float:
+    """2/omega_max of the body's lumped-mass elastic operator (the linear part of
+    Update_internal_forces, Body.h:974-997), plus the contact penalty kn*length/m of border nodes."""
+    import scipy.sparse as sp
+    from scipy.sparse.linalg import eigsh
+    K = stiffness_matrix(body, mu, lam)
     minv_sqrt = 1.0 / np.sqrt(body.mass.reshape(-1))
     S = sp.diags(minv_sqrt) @ K @ sp.diags(minv_sqrt)
     v0 = np.ones(S.shape[0])
@@ -723,10 +750,17 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
     f["gp_weight"] = np.concatenate(gw).astype(np.float64)
     f["gp_jacobian"] = np.concatenate(gJ).astype(np.float64)
     f["cells"] = np.concatenate([b.cells for b in scene.bodies]).reshape(-1).astype(np.int32)
-    f["body_matrix_ptr"] = np.zeros(nb + 1, dtype=np.int32)
-    f["matrix_dofs"] = np.zeros(0, dtype=np.int32)
-    f["matrix_stiffness"] = np.zeros(0, dtype=np.float64)
-    f["matrix_damping"] = np.zeros(0, dtype=np.float64)
+    mptr = [0]; mdofs = []; mk = []; mc = []
+    for b in scene.bodies:
+        if b.matrices is not None:
+            mdofs.append(b.matrices[0].reshape(-1)); mk.append(b.matrices[1]); mc.append(b.matrices[2])
+            mptr.append(mptr[-1] + b.matrices[1].shape[0])
+        else:
+            mptr.append(mptr[-1])
+    f["body_matrix_ptr"] = np.array(mptr, dtype=np.int32)
+    f["matrix_dofs"] = np.concatenate(mdofs).astype(np.int32) if mdofs else np.zeros(0, dtype=np.int32)
+    f["matrix_stiffness"] = np.concatenate(mk).astype(np.float64) if mk else np.zeros(0, dtype=np.float64)
+    f["matrix_damping"] = np.concatenate(mc).astype(np.float64) if mc else np.zeros(0, dtype=np.float64)
     f["material_names"] = names
     return f  # type: ignore[return-value]
 
@@ -880,7 +914,14 @@ def _static_data_body(bi: int, b: Body) -> str:
             w(" \nNODE %d\n%d\n" % (i, ptr[i + 1] - ptr[i]))
             for e in range(ptr[i], ptr[i + 1]):
                 w("%d %s %s %s\n" % (idx[e], _g(Nv[e]), _g(dx[e]), _g(dy[e])))
-        w(" \n \nMATRICES\n0\n \n \n \n \n")
+        if b.matrices is None:
+            w(" \n \nMATRICES\n0\n \n \n \n \n")
+        else:
+            dofs, kv, cv = b.matrices
+            w(" \n \nMATRICES\n%d\n \n" % kv.shape[0])
+            for (d0, d1), k_, c_ in zip(dofs, kv, cv):
+                w("%d %d %s %s\n" % (d0, d1, _g(k_), _g(c_)))
+            w(" \n \n \n")
     return "".join(out)
 
 

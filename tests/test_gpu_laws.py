@@ -162,3 +162,26 @@ def test_initialize_czm_bit_identical(gpu_lib, oracle_built, case):
         assert_contacts_equal(gs.contacts(), o.contacts())
     np.testing.assert_array_equal(gs.works(), o.works())
     gs.close()
+
+
+def test_damping_matrices_bit_identical(gpu_lib, oracle_built):
+    """Rayleigh damping matrices on the grains (MATRICES of STATIC_DATA, applied by
+    Body::Update_damping_forces, Code/Body.h:1057-1154, to the velocity parameters): node state,
+    contacts and works equal the oracle's (itself pinned to the compiled reference on this case,
+    tests/test_oracle_laws.py) over 100 steps, and the damping work is non-zero."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    from test_oracle_laws import case_scene
+    flat = g.flatten(case_scene("damping"))
+    assert len(flat["matrix_damping"]) > 1000
+    gs = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    for _ in range(5):
+        gs.step(20)
+        o.step(20)
+        np.testing.assert_array_equal(gs.node_state(), o.node_state())
+        assert_contacts_equal(gs.contacts(), o.contacts())
+    np.testing.assert_array_equal(gs.works(), o.works())
+    assert np.abs(gs.works()[:, 5]).max() > 0
+    gs.close()

@@ -42,7 +42,7 @@ LAW_PARAMS = {
 CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7+czm", "neohookean",
                                                     "border_conditions", "biaxial12_s5", "biaxial12_s7",
                                                     "periodic", "rotor", "adaptive_euler", "euler_2",
-                                                    "mass_scaling", "adaptive_mass_scaling"]
+                                                    "mass_scaling", "adaptive_mass_scaling", "damping"]
 
 # Solver_step schemes (Code/Solver.h:98-486) with their parameters: Target_error, Control_parameter,
 # Accepted_ratio, Max_mass_scaling, Control_parameter_mass_scaling, Error_factor_mass_scaling,
@@ -73,6 +73,10 @@ def case_scene(name):
         sp = list(sc.solver_params)
         sp[:len(prm)] = prm
         sc.solver_params = tuple(sp)
+    elif name == "damping":
+        # Rayleigh damping matrices on the grains (MATRICES, Body::Update_damping_forces)
+        E, nu = 1e8, 0.3
+        g.add_damping(sc, 0.02 * sc.dt, 0.05 / sc.dt, E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu)))
     elif name == "neohookean":
         sc.materials = [(n, 1 if n == "Grain" else t, p) for (n, t, p) in sc.materials]
     elif name == "border_conditions":
