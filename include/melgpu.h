@@ -64,6 +64,7 @@ enum { MEL_PREC_FP64 = 0, MEL_PREC_MIXED = 1 };
 #define MEL_RIGID_NF    20   /* see MEL_RG_* below                                                    */
 #define MEL_NFLAGS      11   /* DYNAMIC flags[0..10]                               (Code/IO.h:1912-1933) */
 #define MEL_NINTERNAL    3   /* Contact_element::internal values kept on device                         */
+#define MEL_DEACT_NF     8   /* doubles per DEACTIVATION entry in mel_model_desc::deactivated          */
 
 /* Layout of one rigid-body record in mel_model_desc::rigid (Body.h:46-95 rigid attributes). */
 enum { MEL_RG_X0 = 0, MEL_RG_Y0, MEL_RG_R0, MEL_RG_MASS, MEL_RG_INERTIA, MEL_RG_INV_MASS, MEL_RG_INV_INERTIA,
@@ -148,6 +149,12 @@ typedef struct mel_model_desc {
     const int*    matrix_dofs;          /* [2*n_matrix] */
     const double* matrix_stiffness;
     const double* matrix_damping;
+    /* DEACTIVATION entries of STATIC_CONTROL (Code/IO.h:947-968): the vector Read_spy_line builds,
+     * then the comparison (0 below, 1 equal, 2 above) and the threshold, zero-padded to
+     * MEL_DEACT_NF doubles; Update_status (Code/Proximity.h:550-1007) applies them after every
+     * proximity update */
+    int           n_deactivated;
+    const double* deactivated;          /* [n_deactivated*MEL_DEACT_NF] or NULL */
 } mel_model_desc;
 
 /* One contact element (Contact_Element.h:5-55) in the reference's own field order. */
@@ -244,6 +251,9 @@ mel_status mel_get_solver_stats(mel_handle* h, double* out5);
  * mel_record_forces on. */
 mel_status mel_get_contact_pressures(mel_handle* h, double* px, double* py);
 mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* n);
+/* Body statuses (MEL_STATUS_*, n_bodies values): Update_status (Code/Proximity.h:550-1007) turns
+ * bodies inactive after a proximity update when a DEACTIVATION entry's condition holds. */
+mel_status mel_get_body_status(mel_handle* h, int* status);
 mel_status mel_get_time(mel_handle* h, double* time, double* dt);
 
 /* Asynchronous checkpoint (replaces the blocking downloads that precede Write_dynamic,

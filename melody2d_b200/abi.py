@@ -17,6 +17,7 @@ MEL_RIGID_NF = 20
 MEL_LAW_NPARAM = 11
 MEL_MAT_NPARAM = 6
 MEL_NINTERNAL = 3
+MEL_DEACT_NF = 8
 
 MEL_OK, MEL_ERR_INVALID, MEL_ERR_UNSUPPORTED, MEL_ERR_CUDA, MEL_ERR_OOM, MEL_ERR_NAN, MEL_ERR_BOUNDS, \
     MEL_ERR_TIMEOUT, MEL_ERR_IO, MEL_ERR_NO_DEVICE = range(10)
@@ -45,6 +46,7 @@ class MelModelDesc(C.Structure):
         ("gp_weight", _dp), ("gp_jacobian", _dp),
         ("n_cells", C.c_int), ("cells", _ip),
         ("n_matrix", C.c_int), ("body_matrix_ptr", _ip), ("matrix_dofs", _ip), ("matrix_stiffness", _dp), ("matrix_damping", _dp),
+        ("n_deactivated", C.c_int), ("deactivated", _dp),
     ]
 
 
@@ -158,6 +160,11 @@ class Desc:
         d.n_matrix = len(flat["matrix_stiffness"])
         d.body_matrix_ptr = iptr("body_matrix_ptr"); d.matrix_dofs = iptr("matrix_dofs")
         d.matrix_stiffness = dptr("matrix_stiffness"); d.matrix_damping = dptr("matrix_damping")
+        deact = np.asarray(flat.get("deactivated", np.zeros((0, MEL_DEACT_NF))), dtype=np.float64).reshape(-1, MEL_DEACT_NF)
+        d.n_deactivated = deact.shape[0]
+        if deact.shape[0]:
+            self.arrays["deactivated"] = np.ascontiguousarray(deact.reshape(-1))
+            d.deactivated = self.arrays["deactivated"].ctypes.data_as(_dp)
         self.desc = d
 
     def ref(self):

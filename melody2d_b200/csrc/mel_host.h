@@ -30,6 +30,9 @@ struct mel_host_model {
     double save_period = 0., print_period = 0., next_save = 0., next_print = 0.;
     int number_save = 0, number_iteration = 0, number_print = 0;
     std::vector<std::vector<double>> monitored;
+    // DEACTIVATION entries (Code/IO.h:947-968), and the same zero-padded for mel_model_desc
+    std::vector<std::vector<double>> deactivated;
+    std::vector<double> deactivated_flat;
     void finalize();                     // points desc at the vectors
 };
 

@@ -91,7 +91,8 @@ struct mel_dev {
     const int* mat_type; const double* mat_p;
     const int* law_type; const int* law_len; const double* law_p; const int* table;
     // bodies
-    const int *b_type, *b_mat, *b_per, *b_status, *b_node0, *b_bd0, *b_chunk0, *b_order;
+    const int *b_type, *b_mat, *b_per, *b_node0, *b_bd0, *b_chunk0, *b_order;
+    int* b_status;           // MEL_STATUS_*; Update_status turns bodies inactive during the run
     const double* b_dist;
     const int* b_has_bc;     // body has a non-"none" border condition
     double *rg, *rf, *rtot, *drv, *works;
@@ -199,6 +200,9 @@ struct mel_mon_op { int type, kind, sub, body, node, border, bnode, pad; };
 struct mel_mon_head { double iteration, time, dt, neval, max_error, mean_error; };
 // Monitoring after a step: per-body partial sums into part[3*nb], then the row into row[0..]
 // (row[0] = number of values that follow)
+// Update_status (Code/Proximity.h:550-1007): the DEACTIVATION entries (MEL_DEACT_NF doubles each)
+// evaluated on the current state; bodies whose condition holds become inactive
+void mel_launch_status(const mel_dev& d, const double* entries, int n, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, const mel_mon_op* ops, int nops, int energy, int boundaries,
                         double* part, double* row, const mel_mon_head& hd, cudaStream_t s);
 

@@ -45,6 +45,11 @@ void mel_host_model::finalize()
     d.n_matrix = (int)matrix_stiffness.size();
     d.body_matrix_ptr = I(body_matrix_ptr); d.matrix_dofs = I(matrix_dofs);
     d.matrix_stiffness = D(matrix_stiffness); d.matrix_damping = D(matrix_damping);
+    deactivated_flat.assign(deactivated.size() * MEL_DEACT_NF, 0.);
+    for (size_t i = 0; i < deactivated.size(); i++)
+        for (size_t k = 0; k < deactivated[i].size() && k < MEL_DEACT_NF; k++) deactivated_flat[MEL_DEACT_NF * i + k] = deactivated[i][k];
+    d.n_deactivated = (int)deactivated.size();
+    d.deactivated = deactivated.empty() ? nullptr : deactivated_flat.data();
 }
 
 namespace {
@@ -296,11 +301,24 @@ mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* ou
         if (line.compare(0, 17, "PENALTY_PARAMETER") == 0) { double p; C >> p; std::getline(C, token); }
         if (line.compare(0, 7, "GRAVITY") == 0) { C >> gx >> gy; std::getline(C, token); }
         if (line.compare(0, 8, "PLOTTING") == 0) { std::getline(C, token); std::getline(C, token); }
-        if (line.compare(0, 12, "DEACTIVATION") == 0) {     // Code/IO.h:947-951; acted on by Update_status
+        if (line.compare(0, 12, "DEACTIVATION") == 0) {     // Code/IO.h:947-968; acted on by Update_status
             int n = 0;
             C >> n;
             std::getline(C, token);
-            if (n > 0) { mel_set_error("DEACTIVATION (Update_status, Code/Proximity.h:550) is not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
+            std::vector<double> entry;
+            for (int i = 0; i < n; i++) {
+                read_spy_line(C, entry);
+                std::string kw;
+                double threshold = 0.;
+                C >> kw >> threshold;
+                if (kw == "below") entry.push_back(0.);
+                else if (kw == "equal") entry.push_back(1.);
+                else if (kw == "above") entry.push_back(2.);
+                entry.push_back(threshold);
+                if (entry.size() > MEL_DEACT_NF) { mel_set_error("DEACTIVATION entry %d has %zu values", i, entry.size()); return MEL_ERR_UNSUPPORTED; }
+                M.deactivated.push_back(entry);
+                std::getline(C, token);
+            }
         }
         if (line.compare(0, 10, "MONITORING") == 0) {        // Code/IO.h:933-945
             int n = 0;

@@ -107,6 +107,10 @@ struct mel_handle {
     double* mon_rows = nullptr;
     int mon_cap = 0, mon_stride = 0, mon_count = 0;
     bool mon_on = false, mon_forces = false;
+    // DEACTIVATION entries (device copy) that Update_status evaluates after each proximity update
+    double* d_deact = nullptr;
+    int n_deact = 0;
+    bool deact_forces = false;
     long long iteration = 0;
     mel_batch* batch = nullptr;  // batch the handle is a member of (steps only through the batch)
     int failed = 0;                 // model-level failure (MEL_ERR_NAN, MEL_ERR_BOUNDS) that retired it from a batch
@@ -317,6 +321,40 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.b_mat = dupload(h, d->body_material, nb);
     D.b_per = dupload(h, d->body_periodic, nb);
     D.b_status = dupload(h, d->body_status, nb);
+    // DEACTIVATION entries that Update_status compares (Code/Proximity.h:550-1007), checked against
+    // the model: the reference indexes its arrays with them unchecked
+    if (d->n_deactivated > 0) {
+        if (!d->deactivated) { mel_set_error("n_deactivated > 0 without entries"); return MEL_ERR_INVALID; }
+        auto nodes_of = [&](int b) { return d->body_node_ptr[b + 1] - d->body_node_ptr[b]; };
+        std::vector<double> keep;
+        for (int i = 0; i < d->n_deactivated; i++) {
+            const double* e = d->deactivated + (size_t)MEL_DEACT_NF * i;
+            const int type = (int)e[0];
+            if (type == 8) {
+                mel_set_error("DEACTIVATION entry %d compares a body's damage, which needs Body::Update_damage (not run by this library)", i);
+                return MEL_ERR_UNSUPPORTED;
+            }
+            if (type < 0 || type > 4) continue;                    // Update_status has no branch for it
+            const int body = (int)(type <= 3 ? e[2] : e[3]), node = (int)(type <= 3 ? e[3] : e[4]);
+            if (body < 0 || body >= nb || node >= nodes_of(body)) { mel_set_error("DEACTIVATION entry %d: body or node out of range", i); return MEL_ERR_INVALID; }
+            if (type == 4) {
+                const int fk = (int)e[2];
+                if (fk < 0 || fk > 7) { mel_set_error("DEACTIVATION entry %d: force kind %d", i, fk); return MEL_ERR_INVALID; }
+                if (node < 0 && (fk >= nb || (d->body_type[fk] == MEL_BODY_DEFORMABLE && nodes_of(fk) > nodes_of(body)))) {
+                    mel_set_error("DEACTIVATION entry %d: the reference reads the type and node count of body number <force kind> "
+                                  "(Code/Proximity.h:866-882), which this model does not allow", i);
+                    return MEL_ERR_INVALID;
+                }
+                if (node >= 0 || d->body_type[fk] == MEL_BODY_DEFORMABLE) h->deact_forces = true;
+            }
+            keep.insert(keep.end(), e, e + MEL_DEACT_NF);
+        }
+        if (!keep.empty()) {
+            h->d_deact = dupload(h, keep);
+            h->n_deact = (int)(keep.size() / MEL_DEACT_NF);
+            if (h->deact_forces) D.record_forces = 1;
+        }
+    }
     D.b_node0 = dupload(h, d->body_node_ptr, nb + 1);
     D.b_bd0 = dupload(h, d->body_border_ptr, nb + 1);
     D.b_dist = dupload(h, d->body_dist, 3 * (size_t)nb);
@@ -1156,6 +1194,10 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             mel_status rc = proximity(h, p0, p1);
             if (rc) return rc;
             nprox++;
+            if (h->n_deact) {                   // Update_status (Code/main.cpp:195)
+                mel_launch_status(h->d, h->d_deact, h->n_deact, h->stream);
+                h->launches++;
+            }
         }
     }
     if (adaptive) {
@@ -1401,7 +1443,7 @@ mel_status mel_get_forces(mel_handle* h, double* internal, double* contact, doub
 mel_status mel_record_forces(mel_handle* h, int on)
 {
     if (!h) return MEL_ERR_INVALID;
-    h->d.record_forces = (on || h->mon_forces) ? 1 : 0;    // force entries of the monitoring keep it on
+    h->d.record_forces = (on || h->mon_forces || h->deact_forces) ? 1 : 0;   // force entries keep it on
     return MEL_OK;
 }
 
@@ -1483,6 +1525,15 @@ mel_status mel_get_contacts(mel_handle* h, mel_contact* out, int capacity, int* 
     if (n) *n = h->d.ncont;
     int m = std::min(capacity, h->d.ncont);
     if (out && m > 0) MEL_CUDA_OK(cudaMemcpy(out, h->d.cont, sizeof(mel_contact) * m, cudaMemcpyDeviceToHost));
+    return MEL_OK;
+}
+
+mel_status mel_get_body_status(mel_handle* h, int* status)
+{
+    if (!h || !status) { mel_set_error("invalid arguments"); return MEL_ERR_INVALID; }
+    cudaSetDevice(h->device);
+    MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
+    MEL_CUDA_OK(cudaMemcpy(status, h->d.b_status, sizeof(int) * (size_t)h->nb, cudaMemcpyDeviceToHost));
     return MEL_OK;
 }
 
@@ -1665,6 +1716,8 @@ mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info
     MEL_CUDA_OK(get(sn.data(), D.e_sn, 4 * ne));
     MEL_CUDA_OK(get(ss.data(), D.e_ss, 4 * ne));
     MEL_CUDA_OK(get(cont0.data(), D.b_cont0, nb + 1));
+    std::vector<int> status(nb);
+    MEL_CUDA_OK(get(status.data(), (const int*)D.b_status, nb));
     MEL_CUDA_OK(get(cont.data(), D.cont, (size_t)D.ncont));
     std::vector<int> nbr;
     if (h->P.nbr && h->P.nbn) {
@@ -1694,7 +1747,7 @@ mel_status mel_write_dynamic(mel_handle* h, const char* dir, const mel_save_info
     for (size_t i = 0; i < nb; i++) {
         const int n0 = h->b_node0[i], nbn_i = h->b_node0[i + 1] - n0;
         const bool def = h->b_type[i] == MEL_BODY_DEFORMABLE;
-        const int st = h->b_status[i] >= 0 && h->b_status[i] <= 2 ? h->b_status[i] : 0;
+        const int st = status[i] >= 0 && status[i] <= 2 ? status[i] : 0;
         F << bar << std::endl << "%%%%%%%             BODY " << i << "             %%%%%%%" << std::endl << bar << std::endl << std::endl;
         F << (def ? "DEFORMABLE" : "RIGID") << std::endl << status_names[st] << std::endl << i << std::endl << std::endl;
         F << "KINEMATICS" << std::endl;
@@ -2074,7 +2127,7 @@ mel_status mel_batch_create(int device, int precision, mel_batch** out)
 mel_status mel_batch_admit(mel_batch* b, mel_handle* h)
 {
     if (h && h->solver != MEL_SOLVER_EULER) { mel_set_error("batches advance the Euler scheme; step Solver_step schemes with mel_step"); return MEL_ERR_UNSUPPORTED; }
-    if (h && h->d.fdamp) { mel_set_error("models with damping matrices are stepped with mel_step, not in a batch"); return MEL_ERR_UNSUPPORTED; }
+    if (h && (h->d.fdamp || h->n_deact)) { mel_set_error("models with damping matrices or DEACTIVATION entries are stepped with mel_step, not in a batch"); return MEL_ERR_UNSUPPORTED; }
     if (!b || !h) return MEL_ERR_INVALID;
     if (h->batch) { mel_set_error("the handle is already a member of a batch"); return MEL_ERR_INVALID; }
     if (h->device != b->device || h->precision != b->precision) {

@@ -222,7 +222,89 @@ __global__ void mon_row_kernel(mel_dev d, const mel_mon_op* ops, int nops, int e
     row[0] = (double)(c - 1);
 }
 
+// Update_status (Code/Proximity.h:550-1007), one thread, entries in order.  e = the entry (type,
+// then the fields Read_spy_line stores, the comparison 0 below / 1 equal / 2 above, the threshold).
+// x, y, r carry over between entries of one call as in the reference (they start at 0 each call).
+__global__ void status_kernel(mel_dev d, const double* entries, int n)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double x = 0., y = 0., r = 0., m = 0.;
+    for (int k = 0; k < n; k++) {
+        const double* e = entries + MEL_DEACT_NF * k;
+        const int type = (int)e[0], kind = (int)e[1];
+        int body, mode;
+        double thr;
+        if (type <= 3) {
+            // Position, Displacement, Velocity, Acceleration of a node or a whole body
+            body = (int)e[2];
+            const int node = (int)e[3];
+            mode = (int)e[4]; thr = e[5];
+            const double2* a = type == 0 ? d.x : type == 1 ? d.u : type == 2 ? d.v : d.a;
+            const int rx = type == 0 ? MEL_RG_XC : type == 1 ? MEL_RG_XD : type == 2 ? MEL_RG_XV : MEL_RG_XA;
+            const int n0 = d.b_node0[body];
+            if (node >= 0) {
+                const double2 p = a[n0 + node];
+                x = p.x; y = p.y;
+            } else if (d.b_type[body] == MEL_BODY_DEFORMABLE) {
+                x = 0.; y = 0.; m = 0.;
+                for (int j = n0; j < d.b_node0[body + 1]; j++) {
+                    const double2 p = a[j], w = d.mass[j];
+                    x += p.x * w.x;
+                    y += p.y * w.y;
+                    m += w.x;
+                }
+                x /= m;
+                y /= m;
+            } else {
+                const double* rg = d.rg + (size_t)MEL_RIGID_NF * body;
+                x = rg[rx]; y = rg[rx + 1]; r = rg[rx + 2];
+            }
+        } else if (type == 4) {
+            // Force: e[2] = force kind, e[3] = body, e[4] = node
+            const int fk = (int)e[2];
+            body = (int)e[3];
+            const int node = (int)e[4];
+            mode = (int)e[5]; thr = e[6];
+            if (node >= 0) {
+                if (fk <= 6) {
+                    const double2 f = node_force(d, body, d.b_node0[body] + node, fk);
+                    x = f.x; y = f.y;
+                }
+            } else if (d.b_type[fk] == MEL_BODY_DEFORMABLE) {
+                // the reference tests the type of body number <force kind>, walks as many nodes as
+                // that body has, and adds total forces (kind 0) or damping forces (kind 1) of body
+                // e[3] (Code/Proximity.h:866-882); the host checked that the walk stays inside it
+                x = 0.; y = 0.;
+                const int n0 = d.b_node0[body], cnt = d.b_node0[fk + 1] - d.b_node0[fk];
+                for (int j = 0; j < cnt; j++) {
+                    if (fk == 0) { const double2 f = node_force(d, body, n0 + j, 0); x += f.x; y += f.y; }
+                    else if (fk == 1) { const double2 f = node_force(d, body, n0 + j, 6); x += f.x; y += f.y; }
+                }
+            } else {
+                const double* rf = d.rf + 15 * body;
+                if (fk == 0) { x = d.rtot[3 * body]; y = d.rtot[3 * body + 1]; r = d.rtot[3 * body + 2]; }
+                else if (fk >= 2 && fk <= 6) { const int q = 3 * (fk - 2); x = rf[q]; y = rf[q + 1]; r = rf[q + 2]; }
+            }
+        } else {
+            continue;
+        }
+        double v;
+        if (kind == 0) v = x;
+        else if (kind == 1) v = y;
+        else if (kind == 2) v = type == 0 ? r : sqrt(x * x + y * y);    // pow(.,0.5): both correctly rounded
+        else if (kind == 3 && type != 0) v = r;
+        else continue;                                                 // no comparison in the reference
+        if ((mode == 0 && v <= thr) || (mode == 1 && v == thr) || (mode == 2 && v >= thr))
+            d.b_status[body] = MEL_STATUS_INACTIVE;
+    }
+}
+
 }  // namespace mel
+
+void mel_launch_status(const mel_dev& d, const double* entries, int n, cudaStream_t s)
+{
+    if (n > 0) mel::status_kernel<<<1, 32, 0, s>>>(d, entries, n);
+}
 
 void mel_launch_monitor(const mel_dev& d, const mel_mon_op* ops, int nops, int energy, int boundaries,
                         double* part, double* row, const mel_mon_head& hd, cudaStream_t s)

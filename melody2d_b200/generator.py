@@ -419,6 +419,9 @@ class Scene:
     monitor_boundaries: bool = False
     save_period: Optional[float] = None
     print_period: Optional[float] = None
+    # DEACTIVATION entries as STATIC_CONTROL lines: a Read_spy_line quantity, then below / equal /
+    # above and the threshold (Code/IO.h:947-968)
+    deactivation: List[str] = dataclasses.field(default_factory=list)
     meta: dict = dataclasses.field(default_factory=dict)
 
     @property
@@ -435,6 +438,29 @@ def material_params_stored(mtype: int, p: List[float]) -> List[float]:
     else:
         lam = E / (3.0 * (1.0 - 2.0 * nu))
     return [p[0], p[1], p[2], mu, lam, p[5]]
+
+
+_SPY_CODES = {
+    "Position": (0, ["X", "Y", "R"]), "Displacement": (1, ["X", "Y", "Mag", "R"]),
+    "Velocity": (2, ["X", "Y", "Mag", "R"]), "Acceleration": (3, ["X", "Y", "Mag", "R"]),
+}
+_FORCE_KINDS = ["Total", "Internal", "Contact", "Body", "Dirichlet", "Neumann", "Damping", "Alid"]
+
+
+def deactivation_vector(line: str) -> List[float]:
+    """The vector Load_static stores for one DEACTIVATION line (Code/IO.h:955-967): the quantity as
+    Read_spy_line encodes it (position, displacement, velocity, acceleration or force entries), then
+    0 / 1 / 2 for below / equal / above and the threshold, zero-padded to 8 values."""
+    t = line.split()
+    if t[0] == "Force":
+        v = [4.0, float(["X", "Y", "Mag", "R"].index(t[1])), float(_FORCE_KINDS.index(t[2])), float(t[3]), float(t[4])]
+        rest = t[5:]
+    else:
+        code, comps = _SPY_CODES[t[0]]
+        v = [float(code), float(comps.index(t[1])), float(t[2]), float(t[3])]
+        rest = t[4:]
+    v += [float(["below", "equal", "above"].index(rest[0])), float(rest[1])]
+    return v + [0.0] * (8 - len(v))
 
 
 def stiffness_matrix(body: Body, mu: float, lam: float):
@@ -761,6 +787,8 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
     f["matrix_dofs"] = np.concatenate(mdofs).astype(np.int32) if mdofs else np.zeros(0, dtype=np.int32)
     f["matrix_stiffness"] = np.concatenate(mk).astype(np.float64) if mk else np.zeros(0, dtype=np.float64)
     f["matrix_damping"] = np.concatenate(mc).astype(np.float64) if mc else np.zeros(0, dtype=np.float64)
+    f["deactivated"] = np.array([deactivation_vector(line) for line in scene.deactivation],
+                                dtype=np.float64).reshape(-1, 8)
     f["material_names"] = names
     return f  # type: ignore[return-value]
 
@@ -822,7 +850,7 @@ def write_asc(scene: Scene, directory: str, workers: int = 1) -> None:
           "GRAVITY", f"{_g(scene.gravity[0])} {_g(scene.gravity[1])}", " ",
           "NUMBER_BODIES", str(len(scene.bodies)), " ",
           "MONITORING", str(len(scene.monitored))] + list(scene.monitored) + [
-          " ", "SPIES", "0", " ", "DEACTIVATION", "0", " "]
+          " ", "SPIES", "0", " ", "DEACTIVATION", str(len(scene.deactivation))] + list(scene.deactivation) + [" "]
     for bi, b in enumerate(scene.bodies):
         L += [" ", "DEFORMABLE" if b.kind == "deformable" else "RIGID", str(bi), names[b.material],
               "Periodic" if b.periodic else "Simple",

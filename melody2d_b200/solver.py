@@ -66,6 +66,7 @@ SIGNATURES = {
     "mel_batch_destroy": [_vp],
     "mel_get_health": [_vp, _ip],
     "mel_get_bc_pressures": [_vp, _dp, _dp],
+    "mel_get_body_status": [_vp, _ip],
     "mel_monitor_setup": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip],
     "mel_monitor_rows": [_vp, _dp, C.c_int, _ip],
     "mel_write_dynamic": [_vp, C.c_char_p, C.POINTER(abi.MelSaveInfo)],
@@ -253,6 +254,12 @@ class Solver:
         px, py = np.zeros(max(ne, 1)), np.zeros(max(ne, 1))
         _check(lib().mel_get_contact_pressures(self.h, _ptr(px), _ptr(py)))
         return np.stack([px[:ne], py[:ne]], axis=1)
+
+    def body_status(self) -> np.ndarray:
+        """MEL_STATUS_* of every body (Update_status can turn bodies inactive)."""
+        a = np.zeros(self.nb, dtype=np.int32)
+        _check(lib().mel_get_body_status(self.h, a.ctypes.data_as(_ip)))
+        return a
 
     def bc_pressures(self) -> np.ndarray:
         """Border-condition pressures of the last step, (n_border_entries, 2)."""
@@ -483,6 +490,7 @@ def load_desc_arrays(directory: str, restart_index: int = 0) -> dict:
         out["matrix_dofs"] = arr(d.matrix_dofs, 2 * d.n_matrix, np.int32)
         out["matrix_stiffness"] = arr(d.matrix_stiffness, d.n_matrix, np.float64)
         out["matrix_damping"] = arr(d.matrix_damping, d.n_matrix, np.float64)
+        out["deactivated"] = arr(d.deactivated, d.n_deactivated * abi.MEL_DEACT_NF, np.float64).reshape(-1, abi.MEL_DEACT_NF)
         return out
     finally:
         L.mel_free_desc(owner)

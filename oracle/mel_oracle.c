@@ -67,6 +67,7 @@ struct orc_model {
     /* Gauss points */
     int ng; int *gsp, *gsi; double *gN, *gdx, *gdy, *gw, *gJ;
     double* eenergy;             /* [nb] Elastic_energy summed (always 0, Model.h:28,72) */
+    int ndeact; double* deact;   /* DEACTIVATION entries, MEL_DEACT_NF doubles each */
     int* cells;
     int nmx; int* mx_ptr; int* mx_dofs; double *mx_k, *mx_c;
     /* dynamic lists */
@@ -1748,6 +1749,78 @@ static void solver_step(orc_model* m)
     m->stats[0] = neval; m->stats[1] = max_error; m->stats[2] = mean_error; m->stats[3] = total_mass; m->stats[4] = max_mass;
 }
 
+/* nodal force of kind k (total, internal, contact, body, dirichlet, neumann, damping, alid) of
+ * global node i, as Node holds it after Sum_up_forces */
+static void node_force(const orc_model* m, int i, int k, double* fx, double* fy)
+{
+    const double* a[8] = { m->ftot, m->fint, m->fcon, m->fbody, m->fdir, m->fneu, m->fdamp, m->falid };
+    *fx = a[k][2 * i]; *fy = a[k][2 * i + 1];
+}
+
+/* Update_status (Code/Proximity.h:550-1007): entries of type position, displacement, velocity,
+ * acceleration (e = {type, kind, body, node, mode, threshold}) and force (e = {4, kind, force kind,
+ * body, node, mode, threshold}); x, y, r start at 0 and carry over between entries */
+static void update_status(orc_model* m)
+{
+    double x = 0., y = 0., r = 0., mm;
+    for (int k = 0; k < m->ndeact; k++) {
+        const double* e = m->deact + MEL_DEACT_NF * k;
+        const int type = (int)e[0], kind = (int)e[1];
+        int body, mode;
+        double thr;
+        if (type >= 0 && type <= 3) {
+            body = (int)e[2];
+            const int node = (int)e[3];
+            mode = (int)e[4]; thr = e[5];
+            const double* arr = type == 0 ? m->x : type == 1 ? m->u : type == 2 ? m->v : m->a;
+            const int rx = type == 0 ? MEL_RG_XC : type == 1 ? MEL_RG_XD : type == 2 ? MEL_RG_XV : MEL_RG_XA;
+            const int n0 = m->nptr[body];
+            if (node >= 0) { x = arr[2 * (n0 + node)]; y = arr[2 * (n0 + node) + 1]; }
+            else if (m->btype[body] == MEL_BODY_DEFORMABLE) {
+                x = 0.; y = 0.; mm = 0.;
+                for (int j = n0; j < m->nptr[body + 1]; j++) {
+                    x += arr[2 * j] * m->mass[2 * j];
+                    y += arr[2 * j + 1] * m->mass[2 * j + 1];
+                    mm += m->mass[2 * j];
+                }
+                x /= mm; y /= mm;
+            } else {
+                const double* rg = m->rg + MEL_RIGID_NF * body;
+                x = rg[rx]; y = rg[rx + 1]; r = rg[rx + 2];
+            }
+        } else if (type == 4) {
+            const int fk = (int)e[2];
+            body = (int)e[3];
+            const int node = (int)e[4];
+            mode = (int)e[5]; thr = e[6];
+            if (node >= 0) {
+                if (fk <= 6) node_force(m, m->nptr[body] + node, fk, &x, &y);
+            } else if (m->btype[fk] == MEL_BODY_DEFORMABLE) {
+                /* Code/Proximity.h:866-882: the type and node count of body number <force kind> */
+                x = 0.; y = 0.;
+                const int n0 = m->nptr[body], cnt = m->nptr[fk + 1] - m->nptr[fk];
+                for (int j = 0; j < cnt; j++) {
+                    double fx, fy;
+                    if (fk == 0) { node_force(m, n0 + j, 0, &fx, &fy); x += fx; y += fy; }
+                    else if (fk == 1) { node_force(m, n0 + j, 6, &fx, &fy); x += fx; y += fy; }
+                }
+            } else {
+                const double* rf = m->rf + 15 * body;
+                if (fk == 0) { x = m->rtot[3 * body]; y = m->rtot[3 * body + 1]; r = m->rtot[3 * body + 2]; }
+                else if (fk >= 2 && fk <= 6) { const int q = 3 * (fk - 2); x = rf[q]; y = rf[q + 1]; r = rf[q + 2]; }
+            }
+        } else continue;
+        double v;
+        if (kind == 0) v = x;
+        else if (kind == 1) v = y;
+        else if (kind == 2) v = type == 0 ? r : pow(x * x + y * y, 0.5);
+        else if (kind == 3 && type != 0) v = r;
+        else continue;
+        if ((mode == 0 && v <= thr) || (mode == 1 && v == thr) || (mode == 2 && v >= thr))
+            m->bstatus[body] = MEL_STATUS_INACTIVE;
+    }
+}
+
 int orc_step(orc_model* m, int nsteps, int run_proximity)
 {
     for (int s = 0; s < nsteps; s++) {
@@ -1756,6 +1829,7 @@ int orc_step(orc_model* m, int nsteps, int run_proximity)
         if (run_proximity && m->time > m->next_cup - 1.e-6 * m->dt) {
             m->next_cup = m->next_cup + m->cup;
             orc_update_proximity(m);
+            update_status(m);                 /* Code/main.cpp:195 */
         }
     }
     return 0;
@@ -1774,6 +1848,8 @@ int orc_create(const mel_model_desc* d, const int* n_regions, orc_model** out)
     m->nlaw = d->n_laws; m->law_type = dupi(d->law_type, m->nlaw); m->law_len = dupi(d->law_length, m->nlaw);
     m->law_p = dupd(d->law_params, (size_t)m->nlaw * MEL_LAW_NPARAM); m->table = dupi(d->contacts_table, (size_t)m->nmat * m->nmat);
     int nb = m->nb = d->n_bodies;
+    m->ndeact = d->n_deactivated;
+    m->deact = d->n_deactivated > 0 ? dupd(d->deactivated, (size_t)d->n_deactivated * MEL_DEACT_NF) : NULL;
     m->btype = dupi(d->body_type, nb); m->bmat = dupi(d->body_material, nb); m->bper = dupi(d->body_periodic, nb);
     m->bstatus = dupi(d->body_status, nb); m->bdist = dupd(d->body_dist, 3 * (size_t)nb);
     m->nptr = dupi(d->body_node_ptr, nb + 1); m->bptr = dupi(d->body_border_ptr, nb + 1); m->gptr = dupi(d->body_gp_ptr, nb + 1);
@@ -1849,6 +1925,8 @@ int orc_create(const mel_model_desc* d, const int* n_regions, orc_model** out)
     *out = m;
     return 0;
 }
+
+void orc_get_body_status(const orc_model* m, int* status) { memcpy(status, m->bstatus, sizeof(int) * (size_t)m->nb); }
 
 void orc_destroy(orc_model* m)
 {

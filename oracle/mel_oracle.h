@@ -47,6 +47,8 @@ void orc_solver_stats(orc_model* m, double* out5);
  * 1: correctly rounded x^(-1/2), cos and sin, the values the GPU kernels compute (mel_rsqrt.h,
  *    mel_sincos.h). */
 void orc_set_rsqrt_mode(int correctly_rounded);
+/* body statuses (MEL_STATUS_*), which Update_status changes after proximity updates */
+void orc_get_body_status(const orc_model* m, int* status);
 
 #ifdef __cplusplus
 }

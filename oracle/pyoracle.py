@@ -120,6 +120,11 @@ class Oracle:
         a = np.ascontiguousarray(st, dtype=np.float64).reshape(-1)
         self.L.orc_set_node_state(self.h, _dp(a))
 
+    def body_status(self) -> np.ndarray:
+        a = np.zeros(self.nb, dtype=np.int32)
+        self.L.orc_get_body_status(self.h, a.ctypes.data_as(C.POINTER(C.c_int)))
+        return a
+
     def positions(self) -> np.ndarray:
         a = np.zeros(2 * self.nn)
         self.L.orc_get_positions(self.h, _dp(a))

@@ -68,6 +68,8 @@ def input_checksum(flat) -> str:
     for k in sorted(flat):
         if k == "material_names":
             continue
+        if k == "deactivated" and np.asarray(flat[k]).size == 0:
+            continue                      # models without DEACTIVATION hash as before the field existed
         h.update(k.encode())
         h.update(np.ascontiguousarray(np.asarray(flat[k])).tobytes())
     return h.hexdigest()

@@ -185,3 +185,28 @@ def test_damping_matrices_bit_identical(gpu_lib, oracle_built):
     np.testing.assert_array_equal(gs.works(), o.works())
     assert np.abs(gs.works()[:, 5]).max() > 0
     gs.close()
+
+
+def test_deactivation_bit_identical(gpu_lib, oracle_built):
+    """DEACTIVATION entries (Update_status after each proximity update, Code/Proximity.h:550-1007):
+    the centre disc (mean speed), the top plate (displacement) and disc 0 (summed total force)
+    turn inactive at the same steps as in the oracle (pinned to the compiled reference on this
+    case, tests/test_oracle_laws.py), and the trajectories stay bit-identical."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    from test_oracle_laws import case_scene
+    flat = g.flatten(case_scene("deactivation"))
+    gs = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    seen = set()
+    for _ in range(10):
+        gs.step(10)
+        o.step(10)
+        np.testing.assert_array_equal(gs.body_status(), o.body_status())
+        np.testing.assert_array_equal(gs.node_state(), o.node_state())
+        assert_contacts_equal(gs.contacts(), o.contacts())
+        seen |= set(np.nonzero(gs.body_status() == 1)[0].tolist())
+    np.testing.assert_array_equal(gs.works(), o.works())
+    assert {4, 10} <= seen, seen
+    gs.close()

@@ -42,7 +42,8 @@ LAW_PARAMS = {
 CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7+czm", "neohookean",
                                                     "border_conditions", "biaxial12_s5", "biaxial12_s7",
                                                     "periodic", "rotor", "adaptive_euler", "euler_2",
-                                                    "mass_scaling", "adaptive_mass_scaling", "damping"]
+                                                    "mass_scaling", "adaptive_mass_scaling", "damping",
+                                                    "deactivation"]
 
 # Solver_step schemes (Code/Solver.h:98-486) with their parameters: Target_error, Control_parameter,
 # Accepted_ratio, Max_mass_scaling, Control_parameter_mass_scaling, Error_factor_mass_scaling,
@@ -73,6 +74,13 @@ def case_scene(name):
         sp = list(sc.solver_params)
         sp[:len(prm)] = prm
         sc.solver_params = tuple(sp)
+    elif name == "deactivation":
+        # Update_status after each proximity update: the centre disc by its mean speed (step 40),
+        # the top plate by its displacement (step 50), disc 0 by its summed total force; two
+        # entries that never hold
+        sc.deactivation = ["Velocity Mag 4 -1 above 0.5", "Displacement Y 10 -1 below -9e-7",
+                           "Force Y Total 0 -1 above 4.5", "Position X 3 5 below 1.0e-3",
+                           "Velocity X 8 -1 equal 12345"]
     elif name == "damping":
         # Rayleigh damping matrices on the grains (MATRICES, Body::Update_damping_forces)
         E, nu = 1e8, 0.3
