@@ -327,6 +327,10 @@ def headline_extras(args, rank, world, local, pg):
         out["input_generation"] = input_generation(args, local)
     except Exception as e:                       # reported, never silently dropped
         out["input_generation"] = {"error": str(e)}
+    try:
+        out["launch_overhead"] = launch_overhead(args, local)
+    except Exception as e:
+        out["launch_overhead"] = {"error": str(e)}
     a = copy.copy(args)
     a.rate, a.duration, a.drain, a.step_cap = args.serve_rate, args.serve_duration, args.serve_drain, args.serve_step_cap
     v = run_serve(a, rank, world, local, pg, emit=False)
@@ -374,6 +378,35 @@ def input_generation(args, local):
             "achieved_write_gbs": written / (best_k * 1e-3) / 1e9,
             "cpu_baseline": {"value": cpu_pts / cpu_s, "unit": "points/s", "cores": 1, "kind": "port",
                              "sample": "%d bodies (%d points) through generator.mls_shape" % (len(sub), cpu_pts)}}
+
+
+def launch_overhead(args, local):
+    """Evidence for the K-step CUDA graph question on the smallest workload, where launches weigh
+    most: the 4x4 lattice (config 0, 2.4 k nodes) stepped 1000 times in one mel_step call.  Host wall
+    clock, device time between the first and last launch (CUDA events), and the sum of the kernels'
+    own times (events around each launch, a separate run); the gap between the last two is the time
+    the GPU waits for launches, which a captured graph could remove."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Solver
+    s = Solver.from_flat(g.flatten(g.disc_lattice_scene()), device=local)
+    try:
+        s.step(20)
+        n = 1000
+        t0 = time.perf_counter()
+        s.step(n)
+        wall = (time.perf_counter() - t0) * 1e3 / n
+        st = s.step_stats()
+        dev = st["ms_total"] / n
+        launches = s.kernel_times()["launches"] / n
+        s.set_timing(True)
+        s.step(n)
+        kt = s.kernel_times()
+        kern = (kt["contact"] + kt["body"] + kt["proximity"]) / n
+        return {"workload": "4x4 lattice, 2.4 k nodes, 1000 steps per mel_step call",
+                "host_wall_ms_per_step": wall, "device_ms_per_step": dev, "kernel_ms_per_step": kern,
+                "launches_per_step": launches, "gpu_waiting_fraction": max(0.0, 1.0 - kern / dev)}
+    finally:
+        s.close()
 
 
 def create_solvers(flats, precision, device, threads):
@@ -549,16 +582,21 @@ def compare_precisions(args, rank, world, local, pg):
     # (relative 1e-16, far below the mixed form's first-step difference): how fast the sample itself
     # amplifies a difference, whatever its source
     c = Solver.from_flat(flat, precision=0, device=local)
+    # perturbed after 100 steps, once the displacement parameters are no longer zero (a one-ulp step
+    # from zero is a subnormal that the strain products round away)
+    for sv in (a, b, c):
+        sv.step(100)
     st = c.node_state()
     st[:, 6:8] = np.nextafter(st[:, 6:8], np.inf)
     c.set_node_state(st)
+    done0 = 100
 
     def rel(x, y):
         x, y = np.asarray(x, float), np.asarray(y, float)
         return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
     from melody2d_b200.solver import MelError
     checkpoints = sorted({k for k in range(5000, args.compare_fp64, 5000)} | {1000, args.compare_fp64})
-    rows, done, stopped = [], 0, None
+    rows, done, stopped = [], done0, None
     for k in checkpoints:
         try:
             a.step(k - done)

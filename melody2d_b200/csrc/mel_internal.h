@@ -29,7 +29,7 @@
 
 // device error words (mel_dev::err)
 enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3, MEL_E_CAPACITY = 4,
-       MEL_E_NBR_NEED = 5, MEL_E_WAIT = 6, MEL_E_PRESSURE = 7, MEL_E_NWORDS = 8 };
+       MEL_E_NBR_NEED = 5, MEL_E_WAIT = 6, MEL_E_PRESSURE = 7, MEL_E_DEACT = 8, MEL_E_NWORDS = 9 };
 #define MEL_PRESSURE_CAP 64       // contact contributions one border entry's pressure gathers
 
 // Chunk image (all offsets in bytes from the image start, every section 16-byte aligned):
@@ -182,9 +182,11 @@ void mel_launch_drivendof(const mel_dev& d, double T, cudaStream_t s);
 // Body::Restore of the rigid bodies' kinematics from a copy of the rigid records
 void mel_launch_rigid_restore(const mel_dev& d, const double* rg_snap, cudaStream_t s);
 // one step of a batch: the contact pass over thr0[nsamp] threads, the body pass over cta0[nsamp]
-// CTAs and the per-sample time advance (devs, thr0, cta0 in device memory)
-void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta, int nsamp,
-                           int mixed, size_t smem, cudaStream_t s);
+// CTAs and the per-sample time advance (devs, thr0, cta0 in device memory).  The body pass is two
+// launches: CTAs [0, ncta_small) with smem_small bytes (members whose bodies fit two CTAs per SM,
+// ordered first), then the rest with smem bytes
+void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta_small, int ncta,
+                           int nsamp, int mixed, size_t smem_small, size_t smem, cudaStream_t s);
 size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed);
 void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);

@@ -1548,18 +1548,20 @@ __global__ void __launch_bounds__(128) contact_kernel_batch(const mel_dev* devs,
 }
 
 template <bool MX>
-__global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel_batch(const mel_dev* devs, const int* cta0, int nsamp)
+__global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel_batch(const mel_dev* devs, const int* cta0, int nsamp,
+                                                                         int cta_base)
 {
     extern __shared__ __align__(16) char smem[];
     __shared__ mel_dev sd;                   // the sample's descriptor, read once per CTA
-    const int s = batch_member(cta0, nsamp, blockIdx.x);
+    const int c = (int)blockIdx.x + cta_base;
+    const int s = batch_member(cta0, nsamp, c);
     {
         const int* src = reinterpret_cast<const int*>(devs + s);
         int* dst = reinterpret_cast<int*>(&sd);
         for (int k = threadIdx.x; k < (int)(sizeof(mel_dev) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
     }
     __syncthreads();
-    body_cta<MX>(sd, blockIdx.x - cta0[s], sd.time2[0], smem);
+    body_cta<MX>(sd, c - cta0[s], sd.time2[0], smem);
 }
 
 __global__ void advance_kernel(const mel_dev* devs, int nsamp)
@@ -1730,13 +1732,18 @@ size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)
     return r > rigid ? r : rigid;
 }
 
-void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta, int nsamp,
-                           int mixed, size_t smem, cudaStream_t s)
+void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta_small, int ncta,
+                           int nsamp, int mixed, size_t smem_small, size_t smem, cudaStream_t s)
 {
     if (nthr > 0) mel::contact_kernel_batch<<<(nthr + 127) / 128, 128, 0, s>>>(devs, thr0, nsamp, 1.0);
-    if (ncta > 0) {
-        if (mixed) mel::body_kernel_batch<true><<<ncta, MEL_BODY_THREADS, smem, s>>>(devs, cta0, nsamp);
-        else mel::body_kernel_batch<false><<<ncta, MEL_BODY_THREADS, smem, s>>>(devs, cta0, nsamp);
+    // members whose bodies fit two CTAs per SM first, in their own launch, then the others
+    if (ncta_small > 0) {
+        if (mixed) mel::body_kernel_batch<true><<<ncta_small, MEL_BODY_THREADS, smem_small, s>>>(devs, cta0, nsamp, 0);
+        else mel::body_kernel_batch<false><<<ncta_small, MEL_BODY_THREADS, smem_small, s>>>(devs, cta0, nsamp, 0);
+    }
+    if (ncta > ncta_small) {
+        if (mixed) mel::body_kernel_batch<true><<<ncta - ncta_small, MEL_BODY_THREADS, smem, s>>>(devs, cta0, nsamp, ncta_small);
+        else mel::body_kernel_batch<false><<<ncta - ncta_small, MEL_BODY_THREADS, smem, s>>>(devs, cta0, nsamp, ncta_small);
     }
     mel::advance_kernel<<<(nsamp + 127) / 128, 128, 0, s>>>(devs, nsamp);
 }

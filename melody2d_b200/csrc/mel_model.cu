@@ -760,6 +760,12 @@ static mel_status check_errors(mel_handle* h)
     if (cudaMemcpy(w, h->d.err, sizeof w, cudaMemcpyDeviceToHost) != cudaSuccess) { mel_set_cuda_error(cudaGetLastError(), "err", __FILE__, __LINE__); return MEL_ERR_CUDA; }
     if (w[MEL_E_BOUNDS]) { mel_set_error("device index check failed (code %u)", w[MEL_E_BOUNDS]); return MEL_ERR_BOUNDS; }
     if (w[MEL_E_WAIT]) { mel_set_error("a wait of the body kernel's pipeline gave up after %llu ns", h->d.wait_ns); return MEL_ERR_TIMEOUT; }
+    if (w[MEL_E_DEACT]) {
+        mel_set_error("body %u turned inactive while one of its contact elements carried a force: the reference keeps "
+                      "sending that force to the other bodies for the rest of the run (its send list is no longer cleared, "
+                      "Code/Solver.h:37-61), which this library does not reproduce", w[MEL_E_DEACT] - 1);
+        return MEL_ERR_UNSUPPORTED;
+    }
     return MEL_OK;
 }
 
@@ -2025,7 +2031,10 @@ struct mel_batch {
     int* d_cta0 = nullptr;
     size_t cap = 0;                      // members the device arrays hold
     bool dirty = true;                   // descriptors changed (admission, retirement, proximity)
-    size_t smem = 0;
+    size_t smem = 0;                     // largest body-kernel shared memory of the members
+    size_t smem_small = 0;               // the same over the members that fit two CTAs per SM
+    int nsmall = 0;                      // those members, ordered first
+    size_t two_per_sm = 0;
     long long launches = 0;
     double ms_last = 0.;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -2049,16 +2058,28 @@ static mel_status batch_refresh(mel_batch* b)
         }
         b->cap = cap;
     }
+    if (!b->two_per_sm) {
+        int smem_sm = 0, smem_res = 0;
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, b->device);
+        cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, b->device);
+        b->two_per_sm = (size_t)(smem_sm / 2 - smem_res);
+    }
+    // members whose body kernel fits two CTAs per SM first: one launch of the body pass runs them
+    // at that occupancy, a second the members that need more shared memory (one launch sized for
+    // the largest member would hold every CTA to one per SM)
+    std::stable_partition(b->members.begin(), b->members.end(),
+                          [&](const mel_handle* h) { return h->body_smem <= b->two_per_sm; });
     b->h_devs.resize(n);
     b->h_thr0.assign(n + 1, 0);
     b->h_cta0.assign(n + 1, 0);
-    b->smem = 0;
+    b->smem = 0; b->smem_small = 0; b->nsmall = 0;
     for (int i = 0; i < n; i++) {
         mel_handle* h = b->members[i];
         b->h_devs[i] = h->d;
         b->h_thr0[i + 1] = b->h_thr0[i] + h->d.ncont + h->d.ne;
         b->h_cta0[i + 1] = b->h_cta0[i] + h->nblocks_body;
         b->smem = std::max(b->smem, h->body_smem);
+        if (h->body_smem <= b->two_per_sm) { b->smem_small = std::max(b->smem_small, h->body_smem); b->nsmall = i + 1; }
     }
     if (n > 0) {
         MEL_CUDA_OK(cudaMemcpy(b->d_devs, b->h_devs.data(), sizeof(mel_dev) * n, cudaMemcpyHostToDevice));
@@ -2168,9 +2189,9 @@ mel_status mel_batch_step(mel_batch* b, int nsteps, int run_proximity)
         if (b->dirty) { mel_status rc = batch_refresh(b); if (rc) return rc; }
         const int n = (int)b->members.size();
         if (n == 0) break;
-        mel_launch_batch_step(b->d_devs, b->d_thr0, b->h_thr0[n], b->d_cta0, b->h_cta0[n], n,
-                              b->precision == MEL_PREC_MIXED, b->smem, b->stream);
-        b->launches += 3;
+        mel_launch_batch_step(b->d_devs, b->d_thr0, b->h_thr0[n], b->d_cta0, b->h_cta0[b->nsmall], b->h_cta0[n], n,
+                              b->precision == MEL_PREC_MIXED, b->smem_small, b->smem, b->stream);
+        b->launches += 2 + (b->nsmall > 0) + (b->nsmall < n);
         cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) { mel_set_cuda_error(le, "batch step launch", __FILE__, __LINE__); return MEL_ERR_CUDA; }
         std::vector<mel_handle*> due;

@@ -294,8 +294,21 @@ __global__ void status_kernel(mel_dev d, const double* entries, int n)
         else if (kind == 2) v = type == 0 ? r : sqrt(x * x + y * y);    // pow(.,0.5): both correctly rounded
         else if (kind == 3 && type != 0) v = r;
         else continue;                                                 // no comparison in the reference
-        if ((mode == 0 && v <= thr) || (mode == 1 && v == thr) || (mode == 2 && v >= thr))
+        if ((mode == 0 && v <= thr) || (mode == 1 && v == thr) || (mode == 2 && v >= thr)) {
+            if (d.b_status[body] != MEL_STATUS_INACTIVE) {
+                // the reference stops clearing the send list of an inactive body but goes on
+                // sending it (Code/Solver.h:37-61: Initialize_contact_forces skipped,
+                // Send_contact_forces not), so a body switched off while one of its contact
+                // elements carries a force keeps pushing that force onto its masters for the rest
+                // of the run; that is reported rather than reproduced
+                for (int j = d.b_cont0[body]; j < d.b_cont0[body + 1]; j++)
+                    if (d.cont[j].bodyM != body && (d.cont[j].fx != 0. || d.cont[j].fy != 0.)) {
+                        atomicCAS(d.err + MEL_E_DEACT, 0u, (unsigned)body + 1u);
+                        break;
+                    }
+            }
             d.b_status[body] = MEL_STATUS_INACTIVE;
+        }
     }
 }
 

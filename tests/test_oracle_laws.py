@@ -75,11 +75,17 @@ def case_scene(name):
         sp[:len(prm)] = prm
         sc.solver_params = tuple(sp)
     elif name == "deactivation":
-        # Update_status after each proximity update: the centre disc by its mean speed (step 40),
-        # the top plate by its displacement (step 50), disc 0 by its summed total force; two
-        # entries that never hold
-        sc.deactivation = ["Velocity Mag 4 -1 above 0.5", "Displacement Y 10 -1 below -9e-7",
-                           "Force Y Total 0 -1 above 4.5", "Position X 3 5 below 1.0e-3",
+        # Update_status after each proximity update: a free rigid disc flying beside the pressed
+        # lattice (body 11) turns inactive by its displacement at step 50 and stops; the other
+        # entries (speed, node position, summed total force of a loaded disc) are evaluated at
+        # every update and never hold
+        xmax = max(b.nodes[:, 0].max() for b in sc.bodies)
+        ymid = 0.5 * (min(b.nodes[:, 1].min() for b in sc.bodies) + max(b.nodes[:, 1].max() for b in sc.bodies))
+        h = 2.0 * np.pi * 0.8e-3 / 32
+        sc.bodies.append(g.make_rigid_disc((xmax + 4e-3, ymid), 0.8e-3, 32, 1, 7800.0, 0.5 * h, 0.5 * h,
+                                           velocity=(0.01, 0.0)))
+        sc.deactivation = ["Displacement X 11 -1 above 2e-7", "Velocity Mag 4 -1 above 100",
+                           "Position Y 3 5 below -1", "Force Y Total 0 -1 above 1e9",
                            "Velocity X 8 -1 equal 12345"]
     elif name == "damping":
         # Rayleigh damping matrices on the grains (MATRICES, Body::Update_damping_forces)
