@@ -434,6 +434,9 @@ mel_status  mel_get_kernel_times(mel_handle* h, double* ms_contact, double* ms_b
  * sizes of the resident layout), deformable node count and current contact count. */
 mel_status  mel_get_step_stats(mel_handle* h, double* ms_total, double* bytes_body, double* bytes_contact,
                                int* n_deformable_nodes, int* n_contacts);
+/* Launch configuration of the body kernel chosen at mel_create: support entries per chunk image,
+ * dynamic shared memory per CTA (bytes) and CTAs per launch (one per body). */
+mel_status  mel_get_kernel_config(mel_handle* h, int* chunk_cap, long long* body_smem, int* body_ctas);
 /* Sizes of the resident model. */
 mel_status  mel_get_sizes(mel_handle* h, int* n_bodies, int* n_nodes, int* n_gauss,
                           int* n_gp_entries, int* n_node_entries, int* n_border_nodes);

@@ -2006,6 +2006,15 @@ mel_status mel_get_step_stats(mel_handle* h, double* ms_total, double* bytes_bod
     return MEL_OK;
 }
 
+mel_status mel_get_kernel_config(mel_handle* h, int* chunk_cap, long long* body_smem, int* body_ctas)
+{
+    if (!h) return MEL_ERR_INVALID;
+    if (chunk_cap) *chunk_cap = h->chunk_cap;
+    if (body_smem) *body_smem = (long long)h->body_smem;
+    if (body_ctas) *body_ctas = h->nblocks_body;
+    return MEL_OK;
+}
+
 mel_status mel_get_error_words(mel_handle* h, unsigned* words, int n)
 {
     if (!h || !words) return MEL_ERR_INVALID;

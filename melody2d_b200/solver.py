@@ -67,6 +67,7 @@ SIGNATURES = {
     "mel_get_health": [_vp, _ip],
     "mel_get_bc_pressures": [_vp, _dp, _dp],
     "mel_get_body_status": [_vp, _ip],
+    "mel_get_kernel_config": [_vp, _ip, C.POINTER(C.c_longlong), _ip],
     "mel_monitor_setup": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip],
     "mel_monitor_rows": [_vp, _dp, C.c_int, _ip],
     "mel_write_dynamic": [_vp, C.c_char_p, C.POINTER(abi.MelSaveInfo)],
@@ -353,8 +354,8 @@ class Solver:
         return m
 
     def error_words(self) -> np.ndarray:
-        w = (C.c_uint * 8)()
-        _check(lib().mel_get_error_words(self.h, w, 8))
+        w = (C.c_uint * 9)()
+        _check(lib().mel_get_error_words(self.h, w, 9))
         return np.array(list(w), dtype=np.uint32)
 
     def kernel_times(self) -> dict:
@@ -369,6 +370,13 @@ class Solver:
         _check(lib().mel_get_step_stats(self.h, *[C.byref(x) for x in v], *[C.byref(x) for x in n]))
         return dict(ms_total=v[0].value, bytes_body=v[1].value, bytes_contact=v[2].value,
                     n_deformable_nodes=n[0].value, n_contacts=n[1].value)
+
+    def kernel_config(self) -> dict:
+        """Body-kernel launch configuration: chunk entry cap, shared memory per CTA, CTAs."""
+        cap, ctas = C.c_int(), C.c_int()
+        smem = C.c_longlong()
+        _check(lib().mel_get_kernel_config(self.h, C.byref(cap), C.byref(smem), C.byref(ctas)))
+        return {"chunk_cap": cap.value, "body_smem": smem.value, "body_ctas": ctas.value}
 
     def sizes(self) -> dict:
         v = [C.c_int() for _ in range(6)]
