@@ -76,9 +76,15 @@ int table_rows(const int* ns, int n)
 
 }  // namespace
 
-mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out, bool mixed)
+long long mel_body_entries(const mel_model_desc* d, int b)
+{
+    return (long long)d->gp_sup_ptr[d->body_gp_ptr[b + 1]] - d->gp_sup_ptr[d->body_gp_ptr[b]];
+}
+
+mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& out, bool mixed, long long pipe_min_entries)
 {
     const int nb = d->n_bodies;
+    out.b_pipe.assign(nb, 0);
     out.chunks.clear();
     out.img.clear();
     out.b_chunk0.assign(nb + 1, 0);
@@ -94,7 +100,9 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
         if (nnb > 4096) { mel_set_error("deformable body %d has %d nodes (pull records hold 12-bit node indices)", b, nnb); return MEL_ERR_UNSUPPORTED; }
         int g = d->body_gp_ptr[b];
         const int g1 = d->body_gp_ptr[b + 1];
-        const int gpcap = mixed ? MEL_CHUNK_GP_MX : MEL_CHUNK_GP_FP64;
+        const bool pipe = mixed && mel_body_entries(d, b) >= pipe_min_entries;
+        out.b_pipe[b] = pipe ? 1 : 0;
+        const int gpcap = pipe ? MEL_CHUNK_GP_MX : MEL_CHUNK_GP_FP64;
         while (g < g1) {
             // as many points as fit gpcap slots (one point thread each), ecap entries and the 10-bit
             // row tables

@@ -18,6 +18,12 @@
 #define MEL_PT_WARPS_MX 4                 // point warps of the mixed pipeline (warps 4-6 pull)
 #define MEL_CHUNK_GP_FP64 224     // Gauss points per chunk: one point thread each
 #define MEL_CHUNK_GP_MX 128
+// mixed-precision bodies with at least this many support entries run the three-stage pipeline,
+// the others the two-buffer loop.  Measured on B200 (mixed body pass): the pipeline takes 0.537 ms
+// against 0.588 ms on the 2000-disc sample, but a 32-sample batch of the batched workload steps in
+// 3.36 ms with it against 2.02 ms with the loop; so by default no body runs the pipeline
+// (MELGPU_PIPE_MIN_ENTRIES, read by mel_create, sets another threshold)
+#define MEL_PIPE_MIN_ENTRIES (1LL << 62)
 #define MEL_BAR_BYTES 128         // the ring's mbarriers (3 per stage) and the abort flag
 #define MEL_CHUNK_E_MAX 2048      // support entries per chunk, upper bound (the host may choose less)
 #define MEL_WAIT_NS 1000000000ull // bound of every device-side wait (1 s)
@@ -131,6 +137,8 @@ struct mel_dev {
     double4* seg_sblk;                        // superblock boxes (unions of their block boxes)
     // Gauss points: chunk table and chunk images
     const mel_chunk* chunk;
+    const int* b_pipe;                        // per body: 1 = three-stage pipeline (mixed pass), else
+                                              // the two-buffer loop; NULL for FP64
     const char* img;
     int img_cap;                              // bytes of one shared-memory staging buffer
     // contacts
@@ -187,7 +195,7 @@ void mel_launch_rigid_restore(const mel_dev& d, const double* rg_snap, cudaStrea
 // ordered first), then the rest with smem bytes
 void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const int* cta0, int ncta_small, int ncta,
                            int nsamp, int mixed, size_t smem_small, size_t smem, cudaStream_t s);
-size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed);
+size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed, int stages);
 void mel_launch_update_borders(const mel_dev& d, cudaStream_t s);
 void mel_launch_monitor(const mel_dev& d, double* part, const int* rigid_ids, int nrigid, double* out, cudaStream_t s);
 // Update_contact_pressures (Code/Proximity.h:1014-1069) from the current contact list

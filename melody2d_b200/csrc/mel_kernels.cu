@@ -593,7 +593,8 @@ __device__ __forceinline__ void chunk_points_mx(int t, int ngp, int mtype, float
 
 #undef E
 
-// Shared memory of a deformable body (n nodes, staging buffers of img_cap bytes each):
+// Shared memory of a deformable body (n nodes, staging buffers of img_cap bytes each; two for the
+// two-buffer loop, MEL_STAGES(1) for the pipeline):
 //   s_up, s_f, s_fc        3 x n double2       displacements, internal forces, contact forces
 //   s_upf (mixed only)     n2 x float2         displacements relative to node 0 (n2 = n rounded to 2)
 //   ring mbarriers + abort flag                MEL_BAR_BYTES
@@ -616,7 +617,10 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
     // the chunk loop, which leaves the internal forces in s_f and the contact forces in s_fc
     char* region;
     volatile int* s_abort;
-    if (!MX) {
+    // the mixed pass runs the pipeline on bodies with many chunks and the two-buffer loop on the
+    // others, whose few chunks leave a three-stage pipeline mostly filling and draining
+    const bool pipe = MX && d.b_pipe && d.b_pipe[b];
+    if (!pipe) {
         uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
                                                          : reinterpret_cast<char*>(s_fc + n));
         s_abort = reinterpret_cast<volatile int*>(s_bar + 2);
@@ -1721,11 +1725,11 @@ void mel_launch_czm_init(const mel_dev& d, cudaStream_t s)
     mel::contact_kernel<<<(d.ncont + 127) / 128, 128, 0, s>>>(d, 1.0, 1);
 }
 
-size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed)
+size_t mel_body_smem_bytes(int max_nodes, int max_image_bytes, int mixed, int stages)
 {
     size_t base = 3 * sizeof(double2) * (size_t)max_nodes + MEL_BAR_BYTES;
     if (mixed) base += sizeof(float2) * (size_t)((max_nodes + 1) & ~1);
-    size_t stage = MEL_STAGES(mixed) * (size_t)max_image_bytes;
+    size_t stage = (size_t)stages * (size_t)max_image_bytes;
     size_t post = (5 * sizeof(double2) + 6 * sizeof(double)) * (size_t)max_nodes;
     size_t rigid = (64 + 6 * MEL_RIGID_BATCH) * sizeof(double);
     size_t r = base + (stage > post ? stage : post);

@@ -70,6 +70,7 @@ struct mel_handle {
     size_t body_smem = 0;
     int nblocks_body = 0;
     int chunk_cap = 0;          // support entries per chunk chosen at build time
+    int body_stages = 2;        // image buffers per CTA (3 when a body runs the mixed pipeline)
     double img_bytes = 0.;      // bytes of all chunk images
     long long n_pad = 0;        // padding entries in the chunk images
     int launches = 0;
@@ -620,6 +621,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     for (int b = 0; b < nb; b++)
         if (d->body_type[b] == MEL_BODY_DEFORMABLE) max_def_nodes = std::max(max_def_nodes, d->body_node_ptr[b + 1] - d->body_node_ptr[b]);
     mel_chunk_set CS;
+    long long pipe_min = 0;
     int smem_sm = 0, smem_blk = 0, smem_res = 0;
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device);
     cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
@@ -627,8 +629,20 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     const size_t two_per_sm = (size_t)(smem_sm / 2 - smem_res);
     {
         const bool mixed = h->precision == MEL_PREC_MIXED;
-        // FP32 images hold 12 bytes per entry instead of 20, and the mixed kernel has more point threads
-        const int gpcap = mixed ? MEL_CHUNK_GP_MX : MEL_CHUNK_GP_FP64;
+        // which mixed bodies run the three-stage pipeline: those with at least pipe_min support
+        // entries (MELGPU_PIPE_MIN_ENTRIES overrides the default); the others run the two-buffer loop
+        if (mixed) {
+            pipe_min = MEL_PIPE_MIN_ENTRIES;
+            if (const char* e = getenv("MELGPU_PIPE_MIN_ENTRIES")) pipe_min = atoll(e);
+        }
+        bool any_pipe = false, any_loop = false;
+        for (int b = 0; b < nb; b++)
+            if (d->body_type[b] == MEL_BODY_DEFORMABLE) {
+                if (mixed && mel_body_entries(d, b) >= pipe_min) any_pipe = true; else any_loop = true;
+            }
+        const int stages = any_pipe ? MEL_STAGES(1) : 2;
+        // FP32 images hold 12 bytes per entry instead of 20; pipeline bodies have fewer point threads
+        const int gpcap = any_loop ? MEL_CHUNK_GP_FP64 : MEL_CHUNK_GP_MX;
         const int caps_fp64[] = { MEL_CHUNK_E_MAX, 1792, 1536, 1408, 1344, 1280, 1216, 1152, 1024, 768, 512, 256 };
         const int caps_mixed[] = { MEL_CHUNK_E_MAX, 1920, 1792, 1664, 1536, 1408, 1280, 1024, 768, 512, 256 };
         std::vector<int> caps = mixed ? std::vector<int>(std::begin(caps_mixed), std::end(caps_mixed))
@@ -663,18 +677,18 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         // a cap from the tuning table (MELGPU_TUNE_FILE, written by melody2d_b200.autotune), or forced
         // by MELGPU_CHUNK_CAP (the tuner's own runs), is taken when it fits the shared memory
         const int tuned = tuned_chunk_cap(h->precision, max_def_nodes);
-        if (tuned > 0 && mel_body_smem_bytes(max_def_nodes, bound(tuned), mixed) <= (size_t)smem_blk) chosen = tuned;
+        if (tuned > 0 && mel_body_smem_bytes(max_def_nodes, bound(tuned), mixed, stages) <= (size_t)smem_blk) chosen = tuned;
         if (chosen < 0)
             for (int ecap : caps)
-                if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed) <= two_per_sm) { chosen = ecap; break; }
+                if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed, stages) <= two_per_sm) { chosen = ecap; break; }
         if (chosen < 0)     // one CTA per SM: largest cap that fits
             for (int ecap : caps)
-                if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed) <= (size_t)smem_blk) { chosen = ecap; break; }
+                if (mel_body_smem_bytes(max_def_nodes, bound(ecap), mixed, stages) <= (size_t)smem_blk) { chosen = ecap; break; }
         if (chosen < 0) {
             mel_set_error("deformable body of %d nodes does not fit the body kernel's shared memory", max_def_nodes);
             return MEL_ERR_UNSUPPORTED;
         }
-        mel_status rc = mel_build_chunks(d, chosen, CS, mixed);
+        mel_status rc = mel_build_chunks(d, chosen, CS, mixed, pipe_min);
         if (rc) return rc;
         h->chunk_cap = chosen;
     }
@@ -685,6 +699,9 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.b_chunk0 = dupload(h, CS.b_chunk0);
     D.img = reinterpret_cast<const char*>(dupload(h, CS.img));
     D.img_cap = CS.img_max;
+    if (h->precision == MEL_PREC_MIXED) D.b_pipe = dupload(h, CS.b_pipe);
+    h->body_stages = 2;
+    for (int v : CS.b_pipe) if (v) h->body_stages = MEL_STAGES(1);
     h->img_bytes = (double)CS.img.size();
     // contacts and proximity buffers
     D.err = dalloc<unsigned>(h, MEL_E_NWORDS);
@@ -718,7 +735,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     if (cudaMalloc(&P.inc_rng, sizeof(int2) * 16) != cudaSuccess) return MEL_ERR_OOM;
     P.inc_rng_bytes = sizeof(int2) * 16;
     D.inc_rng = P.inc_rng;
-    h->body_smem = mel_body_smem_bytes(max_def_nodes, CS.img_max, h->precision == MEL_PREC_MIXED);
+    h->body_smem = mel_body_smem_bytes(max_def_nodes, CS.img_max, h->precision == MEL_PREC_MIXED, h->body_stages);
     if (mel_body_kernel_configure(h->body_smem) != MEL_OK) return MEL_ERR_CUDA;
     h->d_monitor = dalloc<double>(h, 32);
     h->d_monitor_part = dalloc<double>(h, 5 * 148);
