@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define MELGPU_ABI_VERSION 1
+#define MELGPU_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------------------- */
 typedef enum {
@@ -155,6 +155,16 @@ typedef struct mel_model_desc {
      * proximity update */
     int           n_deactivated;
     const double* deactivated;          /* [n_deactivated*MEL_DEACT_NF] or NULL */
+    /* ALID absorbing layers (the ALID block of STATIC_CONTROL, Code/IO.h:1395-1480): per body and
+     * direction the history of the layer's reference velocity (a body has a layer when either
+     * history is non-empty), and per node alid_alpha and alid_beta as Load_static computes them
+     * from the node's initial position (Code/IO.h:1548-1600).  Body::Update_alid_forces
+     * (Code/Body.h:1163-1296) also uses the body's matrix_stiffness entries.  All NULL when no
+     * body has a layer. */
+    const int*    body_alid_ptr;        /* [2*n_bodies+1]: history of (body, dir) k is [ptr[k], ptr[k+1]) */
+    const double* alid_time;
+    const double* alid_value;
+    const double* node_alid;            /* [2*n_nodes] alid_alpha, alid_beta */
 } mel_model_desc;
 
 /* One contact element (Contact_Element.h:5-55) in the reference's own field order. */

@@ -47,6 +47,7 @@ class MelModelDesc(C.Structure):
         ("n_cells", C.c_int), ("cells", _ip),
         ("n_matrix", C.c_int), ("body_matrix_ptr", _ip), ("matrix_dofs", _ip), ("matrix_stiffness", _dp), ("matrix_damping", _dp),
         ("n_deactivated", C.c_int), ("deactivated", _dp),
+        ("body_alid_ptr", _ip), ("alid_time", _dp), ("alid_value", _dp), ("node_alid", _dp),
     ]
 
 
@@ -112,7 +113,7 @@ class Desc:
     def __init__(self, flat: Dict):
         self.arrays = {}
         d = MelModelDesc()
-        d.abi_version = 1
+        d.abi_version = 2
 
         def dptr(name):
             a = np.ascontiguousarray(np.asarray(flat[name], dtype=np.float64))
@@ -165,6 +166,9 @@ class Desc:
         if deact.shape[0]:
             self.arrays["deactivated"] = np.ascontiguousarray(deact.reshape(-1))
             d.deactivated = self.arrays["deactivated"].ctypes.data_as(_dp)
+        if "body_alid_ptr" in flat and len(flat["alid_time"]) > 0:      # ALID layers
+            d.body_alid_ptr = iptr("body_alid_ptr")
+            d.alid_time = dptr("alid_time"); d.alid_value = dptr("alid_value"); d.node_alid = dptr("node_alid")
         self.desc = d
 
     def ref(self):

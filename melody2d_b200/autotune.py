@@ -21,6 +21,7 @@ import time
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_TABLE = os.path.join(HERE, "tuning.txt")
 CAPS = [2048, 1792, 1536, 1408, 1280, 1152, 1024, 896, 768]
+CAPS_MIXED = [3584, 3328, 3072, 2816, 2560, 2304] + CAPS   # FP32 images: larger chunks fit the same memory
 CLASSES = [(64, 340), (96, 480)]          # (border nodes, interior nodes) of the class's discs
 
 
@@ -49,7 +50,7 @@ def tune(out: str, discs: int, steps: int, workers: int) -> dict:
         flat = g.flatten(g.biaxial_scene(seed=7, n_discs=discs, n_border=nb, n_interior=ni, workers=workers))
         gen_s = time.perf_counter() - t0
         for precision in (0, 1):
-            times = {cap: time_cap(flat, precision, cap, steps) for cap in CAPS}
+            times = {cap: time_cap(flat, precision, cap, steps) for cap in (CAPS_MIXED if precision else CAPS)}
             best = min(times, key=times.get)
             rows.append((precision, nb + ni, best))
             report.append({"precision": ["fp64", "mixed"][precision], "max_body_nodes": nb + ni, "best_cap": best,

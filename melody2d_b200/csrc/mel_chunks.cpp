@@ -4,6 +4,7 @@
 // in ascending Gauss-point order (the order Body::Update_internal_forces accumulates them in,
 // Code/Body.h:960-1050), in rows of up to 32 nodes sorted by entry count.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include "mel_chunks.h"
@@ -141,6 +142,82 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 }
             }
             std::sort(tp.begin(), tp.end());
+            if (mixed && !pipe) {
+                // pull of the mixed two-buffer loop: the entries in (node, point) order with their
+                // stored positions, cut into pieces of at most MEL_PIECE entries of one node, and the
+                // seven pull warps' ranges of pieces cut at node boundaries (every node belongs to
+                // one warp), balanced by entries
+                const int nent_l = (int)tp.size();
+                std::vector<uint32_t> pcs;
+                std::vector<int> pc_first;                       // first piece of each node run
+                for (int q = 0; q < nent_l;) {
+                    int r = q;
+                    while (r < nent_l && (tp[r].first >> 32) == (tp[q].first >> 32)) r++;
+                    const int len = r - q, np = (len + MEL_PIECE - 1) / MEL_PIECE;
+                    pc_first.push_back((int)pcs.size());
+                    for (int k = 0, at = q; k < np; k++) {
+                        const int c = len / np + (k < len % np ? 1 : 0);
+                        pcs.push_back((uint32_t)at | ((uint32_t)(c - 1) << 13) | ((uint32_t)(tp[q].first >> 32) << 16));
+                        at += c;
+                    }
+                    q = r;
+                }
+                const int npc = (int)pcs.size();
+                pc_first.push_back(npc);
+                const int segw = (2 * (MEL_PULL_WARPS + 1) + 4 * npc + 3) / 4 + 1;
+                ch.ntn = segw;
+                const int nroff = (int)P.roff.size();
+                if (nroff > 4095) { mel_set_error("chunk row tables too large (%d rows)", nroff); return MEL_ERR_UNSUPPORTED; }
+                const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, segw, nroff, 8);
+                ch.bytes = L.bytes;
+                ch.img = (long long)out.img.size();
+                out.img.resize(out.img.size() + L.bytes, 0);
+                uint8_t* I = out.img.data() + ch.img;
+                int hdr[4] = { ch.ngp, ch.ne, segw, nroff };
+                memcpy(I, hdr, sizeof hdr);
+                float* dNf = reinterpret_cast<float*>(I + L.dN);
+                uint16_t* idx = reinterpret_cast<uint16_t*>(I + L.idx);
+                uint16_t* spos = reinterpret_cast<uint16_t*>(I + L.tpos);
+                double* c0 = reinterpret_cast<double*>(I + L.c0);
+                uint32_t* gpm = reinterpret_cast<uint32_t*>(I + L.gpm);
+                uint16_t* wr = reinterpret_cast<uint16_t*>(I + L.tn);       // MEL_PULL_WARPS + 1 bounds
+                uint32_t* pcr = reinterpret_cast<uint32_t*>(I + L.tn + 16);  // piece records
+                uint16_t* roff = reinterpret_cast<uint16_t*>(I + L.roff);
+                for (int slot = 0; slot < ngp; slot++) {
+                    const int gg = g + P.order[slot];
+                    const int c = d->gp_sup_ptr[gg + 1] - d->gp_sup_ptr[gg];
+                    c0[slot] = d->gp_weight[gg] * d->gp_jacobian[gg];   // c0 of Code/Body.h:994
+                    gpm[slot] = (uint32_t)P.first_row[slot] | ((uint32_t)P.lane[slot] << 10) | ((uint32_t)c << 15);
+                    for (int k = 0, j = d->gp_sup_ptr[gg]; k < c; k++, j++) {
+                        const int e = P.pos(slot, k);
+                        idx[e] = (uint16_t)d->gp_sup_idx[j];
+                        dNf[2 * e] = (float)d->gp_dNdx[j];
+                        dNf[2 * e + 1] = (float)d->gp_dNdy[j];
+                    }
+                }
+                for (int q = 0; q < nent_l; q++) spos[q] = (uint16_t)tp[q].second;
+                for (int k = 0; k < npc; k++) pcr[k] = pcs[k];
+                // warp w takes the pieces [wr[w], wr[w+1]): cut at the node boundary whose entry
+                // offset is nearest to w/7 of the entries
+                const int nruns = (int)pc_first.size() - 1;
+                std::vector<int> run_at(nruns + 1, nent_l);      // first entry of each node run
+                for (int r = 0; r < nruns; r++) run_at[r] = (int)(pcs[pc_first[r]] & 0x1fffu);
+                wr[0] = 0;
+                int r = 0;
+                for (int w = 1; w < MEL_PULL_WARPS; w++) {
+                    const long long target = ((long long)w * nent_l) / MEL_PULL_WARPS;
+                    while (r < nruns && std::llabs(run_at[r + 1] - target) <= std::llabs(run_at[r] - target)) r++;
+                    wr[w] = (uint16_t)pc_first[r];
+                }
+                wr[MEL_PULL_WARPS] = (uint16_t)npc;
+                for (int r = 0; r < nroff; r++) roff[r] = (uint16_t)(P.roff[r] | (P.rsw[r] << 12));
+                out.img_max = std::max(out.img_max, ch.bytes);
+                out.n_entries += ch.ne;
+                out.n_pad += ch.ne - nent;
+                out.chunks.push_back(ch);
+                g += ngp;
+                continue;
+            }
             // touched nodes: (first entry in tp, count), then pull slots sorted by count
             std::vector<std::pair<int, int>> tnodes;
             for (int q = 0; q < (int)tp.size(); q++)

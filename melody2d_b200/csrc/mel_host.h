@@ -23,6 +23,8 @@ struct mel_host_model {
     std::vector<double> gp_N, gp_dNdx, gp_dNdy, gp_weight, gp_jacobian;
     std::vector<int> cells, body_matrix_ptr, matrix_dofs;
     std::vector<double> matrix_stiffness, matrix_damping;
+    std::vector<int> body_alid_ptr;                       // empty: no ALID layer
+    std::vector<double> alid_time, alid_value, node_alid;
     std::vector<mel_contact> contacts;   // CONTACTS of the DYNAMIC file
     // run control that drives output only: Save_period, Print_period (STATIC_CONTROL SOLVER block),
     // Number_save, Number_iteration, Number_print, Next_save, Next_print (DYNAMIC SOLVER block), and

@@ -18,6 +18,8 @@
 #define MEL_PT_WARPS_MX 4                 // point warps of the mixed pipeline (warps 4-6 pull)
 #define MEL_CHUNK_GP_FP64 224     // Gauss points per chunk: one point thread each
 #define MEL_CHUNK_GP_MX 128
+#define MEL_PULL_WARPS 7          // warps 0-6 of the two-buffer loop: point pass, then pull
+#define MEL_PIECE 8               // entries of one node a lane of the mixed pull sums before the warp combines
 // mixed-precision bodies with at least this many support entries run the three-stage pipeline,
 // the others the two-buffer loop.  Measured on B200 (mixed body pass): the pipeline takes 0.537 ms
 // against 0.588 ms on the 2000-disc sample, but a 32-sample batch of the batched workload steps in
@@ -26,6 +28,7 @@
 #define MEL_PIPE_MIN_ENTRIES (1LL << 62)
 #define MEL_BAR_BYTES 128         // the ring's mbarriers (3 per stage) and the abort flag
 #define MEL_CHUNK_E_MAX 2048      // support entries per chunk, upper bound (the host may choose less)
+#define MEL_CHUNK_E_MAX_MX 3584   // the same for the mixed pass's FP32 images (its caps above 2048 come from the tuning table)
 #define MEL_WAIT_NS 1000000000ull // bound of every device-side wait (1 s)
 #define MEL_NBR_CAP_DEFAULT 64    // neighbour slots per body (grown on overflow)
 #define MEL_MAX_BODY_NODES 4096   // nodes per deformable body held in shared memory
@@ -59,6 +62,12 @@ enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3,
 // is lane t & 31 of group t >> 5).  Row j of a pull group holds, for every slot with more than j
 // entries, the position of its node's entry j; a node's entries are in ascending point order.
 // ne is the number of entries rounded up to a multiple of 8 (zero entries at the end).
+// Images of the mixed pass's two-buffer loop replace the pull slots by pieces: tpos lists the
+// positions of all entries in (node, point) order; the tn section holds MEL_PULL_WARPS + 1 uint16
+// warp bounds (16 bytes), then one uint32 record per piece (first listed entry | (count - 1) << 13 |
+// node << 16), a piece being at most MEL_PIECE consecutive entries of one node.  Pull warp w takes
+// the pieces [bound w, bound w+1), which start and end at node boundaries; nroff counts the point
+// rows only.
 struct mel_chunk {        // one chunk of a body's Gauss points
     long long img;        // byte offset of the image in mel_dev::img
     int bytes;            // image size (multiple of 16)
@@ -118,6 +127,15 @@ struct mel_dev {
     const int *dmp_ptr, *dmp_src;
     const double* dmp_c;
     double2* fdamp;
+    // ALID layers (Body::Update_alid_forces): the bodies with a layer, each body's x and y history of
+    // the layer's reference velocity, alid_beta per node, and per receiving degree of freedom its
+    // stiffness terms (source degree of freedom, k / (1/alpha0 + 1/alpha1)) in entry order
+    int n_alid;
+    const int *alid_b, *alid_hptr;
+    const double *alid_ht, *alid_hv, *alid_beta;
+    const int *al_ptr, *al_src;
+    const double* al_c;
+    double2* falid;
     // borders and border entries
     const int *bd_body, *bd_per, *bd_bef, *bd_aft, *bd_e0, *bd_bc, *bd_h0;
     const double *bd_bcp, *ht, *hv;
@@ -176,6 +194,8 @@ struct mel_dev {
 // kernel launch wrappers (mel_kernels.cu)
 // Update_damping_forces of every deformable body with matrices, from the velocity parameters
 void mel_launch_damping(const mel_dev& d, cudaStream_t s);
+// Update_alid_forces at the step's start time time2[parity], or at T when use_T (Solver_step)
+void mel_launch_alid(const mel_dev& d, int parity, double T, int use_T, cudaStream_t s);
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 // Initialize_CZM's pass over the contact list (contact geometry, then the initial bonds)
 void mel_launch_czm_init(const mel_dev& d, cudaStream_t s);

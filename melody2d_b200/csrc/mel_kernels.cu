@@ -688,80 +688,88 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
                 }
                 compute_sync();
                 if (*s_abort) break;
-                // pull: each touched node subtracts its contributions in ascending Gauss-point order
-                // (the mixed form adds its FP32 contributions in FP64).  Pull slot t is lane t & 31
-                // of group t >> 5, its entry j at row j of the group's row table.  Groups are sorted
-                // by entry count; warp w takes groups w, 13 - w, 14 + w, ... (snake order), so the
-                // heaviest group has a warp to itself and the lighter ones pair up.
-                const int ngrp = (hdr.z + 31) >> 5;
-                for (int i = 0; 7 * i < ngrp; i++) {
-                    const int t = (7 * i + ((i & 1) ? 6 - warp : warp)) * 32 + lane;
-                    if (t >= hdr.z) continue;
-                    const unsigned rec = s_tn[t];
-                    const int node = (int)(rec & 0xfffu);
-                    const int cnt = (int)((rec >> 12) & 0xffu);
-                    const uint16_t* prow = s_roff + (rec >> 20);
-                    // rows every slot of a full group has: 32 wide and contiguous
-                    const int pfull = (t | 31) < hdr.z ? (int)((s_tn[t | 31] >> 12) & 0xffu) : 0;
-                    const int pbase = prow[0];
-    #define PQ(j) ((j) < pfull ? pbase + 32 * (j) + lane : prow[(j)] + lane)
-                    double2 f = s_f[node];
-                    int j = 0;
-                    if (MX) {
-                        const float2* s_q = reinterpret_cast<const float2*>(bk + L.dN);
-                        for (; j + 8 <= pfull; j += 8) {
-                            float2 c[8];
-    #pragma unroll
-                            for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[pbase + 32 * (j + i) + lane]];
-    #pragma unroll
-                            for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                if (MX) {
+                    // pull of the mixed form, a two-level segmented reduction in place of the ordered
+                    // chains: each lane sums one piece (at most MEL_PIECE entries of one node) in FP64,
+                    // then the pieces of a node, on consecutive lanes, are combined by a Hillis-Steele
+                    // scan over warp shuffles (equal node keys 2^i lanes apart mean one segment, as
+                    // keys are sorted) and the last lane of each segment subtracts the sum from the
+                    // node.  Warp w owns the pieces [wr[w], wr[w+1]), whole nodes only, balanced by
+                    // entries, so no two warps touch one node.
+                    const float2* s_q = reinterpret_cast<const float2*>(bk + L.dN);
+                    const uint16_t* s_wr = reinterpret_cast<const uint16_t*>(bk + L.tn);
+                    const unsigned* s_pc = reinterpret_cast<const unsigned*>(bk + L.tn + 16);
+                    const int p1 = s_wr[warp + 1];
+                    for (int p0 = s_wr[warp]; p0 < p1; p0 += 32) {
+                        const int pi = p0 + lane;
+                        const bool v = pi < p1;
+                        const unsigned rec = v ? s_pc[pi] : 0u;
+                        const int node = v ? (int)((rec >> 16) & 0xfffu) : -1;
+                        const int q0 = (int)(rec & 0x1fffu), cnt = v ? (int)((rec >> 13) & 7u) + 1 : 0;
+                        float2 c[MEL_PIECE];
+#pragma unroll
+                        for (int i = 0; i < MEL_PIECE; i++) c[i] = i < cnt ? s_q[s_tpos[q0 + i]] : make_float2(0.f, 0.f);
+                        double fx = 0., fy = 0.;
+#pragma unroll
+                        for (int i = 0; i < MEL_PIECE; i++) { fx = fx + (double)c[i].x; fy = fy + (double)c[i].y; }
+#pragma unroll
+                        for (int dd = 1; dd < 32; dd <<= 1) {
+                            const double ox = __shfl_up_sync(0xffffffffu, fx, dd);
+                            const double oy = __shfl_up_sync(0xffffffffu, fy, dd);
+                            const int on = __shfl_up_sync(0xffffffffu, node, dd);
+                            if (lane >= dd && on == node) { fx = fx + ox; fy = fy + oy; }
                         }
-                        for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
-                            int q[8];
-    #pragma unroll
-                            for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
-                            float2 c[8];
-    #pragma unroll
-                            for (int i = 0; i < 8; i++) c[i] = s_q[s_tpos[q[i]]];
-    #pragma unroll
-                            for (int i = 0; i < 8; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
+                        const int nn = __shfl_down_sync(0xffffffffu, node, 1);
+                        if (v && (lane == 31 || nn != node)) {
+                            double2 f = s_f[node];
+                            f.x = f.x - fx;
+                            f.y = f.y - fy;
+                            s_f[node] = f;
                         }
-                        for (; j + 4 <= cnt; j += 4) {
-                            float2 c[4];
-    #pragma unroll
-                            for (int i = 0; i < 4; i++) c[i] = s_q[s_tpos[PQ(j + i)]];
-    #pragma unroll
-                            for (int i = 0; i < 4; i++) { f.x = f.x - (double)c[i].x; f.y = f.y - (double)c[i].y; }
-                        }
-                        for (; j < cnt; j++) {
-                            const float2 c = s_q[s_tpos[PQ(j)]];
-                            f.x = f.x - (double)c.x;
-                            f.y = f.y - (double)c.y;
-                        }
-                    } else {
+                        __syncwarp();     // a node continued by the next round reads this update
+                    }
+                } else {
+                    // pull: each touched node subtracts its contributions in ascending Gauss-point order.
+                    // Pull slot t is lane t & 31 of group t >> 5, its entry j at row j of the group's row
+                    // table.  Groups are sorted by entry count; warp w takes groups w, 13 - w, 14 + w, ...
+                    // (snake order), so the heaviest group has a warp to itself and the lighter ones pair up.
+                    const int ngrp = (hdr.z + 31) >> 5;
+                    for (int i = 0; 7 * i < ngrp; i++) {
+                        const int t = (7 * i + ((i & 1) ? 6 - warp : warp)) * 32 + lane;
+                        if (t >= hdr.z) continue;
+                        const unsigned rec = s_tn[t];
+                        const int node = (int)(rec & 0xfffu);
+                        const int cnt = (int)((rec >> 12) & 0xffu);
+                        const uint16_t* prow = s_roff + (rec >> 20);
+                        // rows every slot of a full group has: 32 wide and contiguous
+                        const int pfull = (t | 31) < hdr.z ? (int)((s_tn[t | 31] >> 12) & 0xffu) : 0;
+                        const int pbase = prow[0];
+        #define PQ(j) ((j) < pfull ? pbase + 32 * (j) + lane : prow[(j)] + lane)
+                        double2 f = s_f[node];
+                        int j = 0;
                         const double2* s_p = reinterpret_cast<const double2*>(bk + L.dN);
                         for (; j + 8 <= pfull; j += 8) {
                             double2 c[8];
-    #pragma unroll
+#pragma unroll
                             for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[pbase + 32 * (j + i) + lane]];
-    #pragma unroll
+#pragma unroll
                             for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
                         }
                         for (; j + 8 <= cnt; j += 8) {      // remaining rows: row-table loads issued together
                             int q[8];
-    #pragma unroll
+#pragma unroll
                             for (int i = 0; i < 8; i++) q[i] = PQ(j + i);
                             double2 c[8];
-    #pragma unroll
+#pragma unroll
                             for (int i = 0; i < 8; i++) c[i] = s_p[s_tpos[q[i]]];
-    #pragma unroll
+#pragma unroll
                             for (int i = 0; i < 8; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
                         }
                         for (; j + 4 <= cnt; j += 4) {
                             double2 c[4];
-    #pragma unroll
+#pragma unroll
                             for (int i = 0; i < 4; i++) c[i] = s_p[s_tpos[PQ(j + i)]];
-    #pragma unroll
+#pragma unroll
                             for (int i = 0; i < 4; i++) { f.x = f.x - c[i].x; f.y = f.y - c[i].y; }
                         }
                         for (; j < cnt; j++) {
@@ -769,9 +777,9 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
                             f.x = f.x - c.x;
                             f.y = f.y - c.y;
                         }
+        #undef PQ
+                        s_f[node] = f;
                     }
-    #undef PQ
-                    s_f[node] = f;
                 }
                 fence_proxy_async();
                 compute_sync();
@@ -1110,9 +1118,10 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         double2 fn = has_bc ? s_fn[i] : make_double2(0., 0.);
         double2 fd = has_bc ? s_fd[i] : make_double2(0., 0.);
         const double2 fdp = d.fdamp ? d.fdamp[gi] : make_double2(0., 0.);
+        const double2 fal = d.falid ? d.falid[gi] : make_double2(0., 0.);
         double2 ft;
-        ft.x = fi.x + fc.x + 0. + fb.x + fd.x + fn.x + fdp.x + 0.;
-        ft.y = fi.y + fc.y + 0. + fb.y + fd.y + fn.y + fdp.y + 0.;
+        ft.x = fi.x + fc.x + 0. + fb.x + fd.x + fn.x + fdp.x + fal.x;
+        ft.y = fi.y + fc.y + 0. + fb.y + fd.y + fn.y + fdp.y + fal.y;
         double2 ap;
         if (AD) { const double2 f = d.fms[gi]; ap = make_double2(ft.x * im.x / f.x, ft.y * im.y / f.y); }
         else ap = make_double2(ft.x * im.x / 1., ft.y * im.y / 1.);
@@ -1134,7 +1143,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         s_T[2 * n + i] = dte * (vx * fd.x + vy * fd.y);
         s_T[3 * n + i] = dte * (vx * fn.x + vy * fn.y);
         s_T[4 * n + i] = dte * (vx * fdp.x + vy * fdp.y);
-        s_T[5 * n + i] = dte * (vx * 0. + vy * 0.);
+        s_T[5 * n + i] = dte * (vx * fal.x + vy * fal.y);
     }
     __syncthreads();
     if (warp == 0) {
@@ -1705,6 +1714,52 @@ __global__ void __launch_bounds__(256) damping_kernel(mel_dev d)
     reinterpret_cast<double*>(d.fdamp)[k] = f;
 }
 }  // namespace mel
+
+namespace mel {
+// Body::Update_alid_forces (Code/Body.h:1163-1296), one CTA per body with a layer: the reference
+// velocity of each direction from its history (the first interval holding T; 0 when none does,
+// where the reference reads past its vector), then per degree of freedom the nodal term
+// -beta m (v - pv) followed by its stiffness terms -(v_param(source) - pv(source)) d in the
+// order the reference's entry loop adds them; a direction without history keeps a zero force
+__global__ void __launch_bounds__(256) alid_kernel(mel_dev d, int parity, double T, int use_T)
+{
+    const int b = d.alid_b[blockIdx.x];
+    __shared__ double s_pv[2];
+    __shared__ int s_fl[2];
+    if (threadIdx.x < 2) {
+        const int dir = threadIdx.x;
+        const double t = use_T ? T : d.time2[parity];
+        const int h0 = d.alid_hptr[2 * b + dir], h1 = d.alid_hptr[2 * b + dir + 1];
+        double pv = 0.;
+        for (int k = h0; k + 1 < h1; k++) {
+            const double t0 = d.alid_ht[k], p0 = d.alid_hv[k], t1 = d.alid_ht[k + 1], p1 = d.alid_hv[k + 1];
+            if ((t0 <= t) & (t <= t1)) { pv = p0 + (p1 - p0) / (t1 - t0) * (t - t0); break; }
+        }
+        s_pv[dir] = pv;
+        s_fl[dir] = h1 > h0;
+    }
+    __syncthreads();
+    const double* v = reinterpret_cast<const double*>(d.v);
+    const double* vp = reinterpret_cast<const double*>(d.vp);
+    const double* m = reinterpret_cast<const double*>(d.mass);
+    double* f = reinterpret_cast<double*>(d.falid);
+    for (int k = 2 * d.b_node0[b] + threadIdx.x; k < 2 * d.b_node0[b + 1]; k += blockDim.x) {
+        const int dir = k & 1;
+        double a = s_fl[dir] ? -d.alid_beta[k >> 1] * m[k] * (v[k] - s_pv[dir]) : 0.;
+        for (int j = d.al_ptr[k]; j < d.al_ptr[k + 1]; j++) {
+            const int src = d.al_src[j];
+            a += -(vp[src] - s_pv[src & 1]) * d.al_c[j];
+        }
+        f[k] = a;
+    }
+}
+}  // namespace mel
+
+void mel_launch_alid(const mel_dev& d, int parity, double T, int use_T, cudaStream_t s)
+{
+    if (!d.falid || d.n_alid == 0) return;
+    mel::alid_kernel<<<d.n_alid, 256, 0, s>>>(d, parity, T, use_T);
+}
 
 void mel_launch_damping(const mel_dev& d, cudaStream_t s)
 {

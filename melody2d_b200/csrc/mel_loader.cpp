@@ -50,6 +50,10 @@ void mel_host_model::finalize()
         for (size_t k = 0; k < deactivated[i].size() && k < MEL_DEACT_NF; k++) deactivated_flat[MEL_DEACT_NF * i + k] = deactivated[i][k];
     d.n_deactivated = (int)deactivated.size();
     d.deactivated = deactivated.empty() ? nullptr : deactivated_flat.data();
+    if (!alid_time.empty()) {
+        d.body_alid_ptr = body_alid_ptr.data();
+        d.alid_time = alid_time.data(); d.alid_value = alid_value.data(); d.node_alid = node_alid.data();
+    }
 }
 
 namespace {
@@ -79,8 +83,47 @@ struct BodyTmp {
     std::vector<int> mdofs;
     std::vector<double> mk, mc;
     std::vector<double> state;   // 12 per node
-    bool has_alid = false;
+    // ALID block (Code/IO.h:1395-1480): histories and the layer's geometry and grading
+    std::vector<double> alid_t[2], alid_v[2];
+    double alid[10] = { 0., 0., 0., 0., 0., 0., 0., 0., 0., 0. };   // xmin xmax ymin ymax range ain aout bin bout exponent
+    std::vector<double> alid_ab;   // 2 per node
 };
+
+// alid_alpha, alid_beta of a node at (x, y) as Load_static computes them while reading NODES
+// (Code/IO.h:1548-1600): graded layers along y, then along x keeping the larger value
+void alid_node(const double* A, double x, double y, double* al, double* be)
+{
+    const double xmin = A[0], xmax = A[1], ymin = A[2], ymax = A[3], range = A[4];
+    const double ain = A[5], aout = A[6], bin = A[7], bout = A[8], ex = A[9];
+    double ka, kb, temp;
+    *al = 0.; *be = 0.;
+    if (y < ymin + range) {
+        ka = (aout - ain) / pow(-range, ex);
+        kb = (bout - bin) / pow(-range, ex);
+        *al = ain + ka * pow(y - (ymin + range), ex);
+        *be = bin + kb * pow(y - (ymin + range), ex);
+    } else if (y > ymax - range) {
+        ka = (aout - ain) / pow(range, ex);
+        kb = (bout - bin) / pow(range, ex);
+        *al = ain + ka * pow(y - (ymax - range), ex);
+        *be = bin + kb * pow(y - (ymax - range), ex);
+    }
+    if (x < xmin + range) {
+        ka = (aout - ain) / pow(-range, ex);
+        kb = (bout - bin) / pow(-range, ex);
+        temp = ain + ka * pow(x - (xmin + range), ex);
+        if (temp > *al) *al = temp;
+        temp = bin + kb * pow(x - (xmin + range), ex);
+        if (temp > *be) *be = temp;
+    } else if (x > xmax - range) {
+        ka = (aout - ain) / pow(range, ex);
+        kb = (bout - bin) / pow(range, ex);
+        temp = ain + ka * pow(x - (xmax - range), ex);
+        if (temp > *al) *al = temp;
+        temp = bin + kb * pow(x - (xmax - range), ex);
+        if (temp > *be) *be = temp;
+    }
+}
 
 int per_code(const std::string& s) { return s == "Periodic" ? MEL_PER_PERIODIC : (s == "Simple" ? MEL_PER_SIMPLE : MEL_PER_CLOSED); }
 
@@ -360,10 +403,25 @@ mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* ou
                 std::getline(C, token);
             }
         }
-        if (line.compare(0, 4, "ALID") == 0) { B[index_body].has_alid = true; }
+        if (line.compare(0, 4, "ALID") == 0) {
+            // counts and the twelve numbers, the rest of their line and one more line, the x history,
+            // one separating line when both histories exist, the y history (Code/IO.h:1395-1480)
+            if (index_body < 0 || index_body >= (int)B.size()) { mel_set_error("ALID before any body"); return MEL_ERR_INVALID; }
+            BodyTmp& b = B[index_body];
+            int nx = 0, ny = 0;
+            C >> nx >> ny;
+            for (int k = 0; k < 10; k++) C >> b.alid[k];
+            if (!C || nx < 0 || ny < 0) { mel_set_error("malformed ALID block in body %d", index_body); return MEL_ERR_INVALID; }
+            std::getline(C, token); std::getline(C, token);
+            for (int dir = 0; dir < 2; dir++) {
+                const int nv = dir ? ny : nx;
+                if (dir == 1 && nx > 0 && ny > 0) std::getline(C, token);
+                b.alid_t[dir].resize(nv); b.alid_v[dir].resize(nv);
+                for (int j = 0; j < nv; j++) { C >> b.alid_t[dir][j] >> b.alid_v[dir][j]; std::getline(C, token); }
+            }
+        }
     }
     C.close();
-    for (auto& b : B) if (b.has_alid) { mel_set_error("ALID absorbing layers are not supported on the GPU path"); return MEL_ERR_UNSUPPORTED; }
 
     std::ifstream S(base + "/STATIC_DATA.asc");
     if (!S) { mel_set_error("cannot open %s/STATIC_DATA.asc", base.c_str()); return MEL_ERR_IO; }
@@ -390,6 +448,9 @@ mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* ou
                 else S >> j >> b.x0[2 * i] >> b.x0[2 * i + 1];
                 std::getline(S, token);
             }
+            b.alid_ab.assign(2 * nn, 0.);
+            if (!rigid && (!b.alid_t[0].empty() || !b.alid_t[1].empty()))
+                for (int i = 0; i < nn; i++) alid_node(b.alid, b.x0[2 * i], b.x0[2 * i + 1], &b.alid_ab[2 * i], &b.alid_ab[2 * i + 1]);
         }
         if (line.compare(0, 7, "BORDERS") == 0) {
             int nbd = 0;
@@ -596,6 +657,21 @@ mel_status mel_load_files(const char* dir, int restart_index, mel_host_model* ou
         M.matrix_damping.insert(M.matrix_damping.end(), b.mc.begin(), b.mc.end());
         M.body_matrix_ptr.push_back((int)M.matrix_stiffness.size());
         for (auto& c : dyn_contacts[bi]) M.contacts.push_back(c);
+    }
+    // ALID layers: histories per (body, direction) and the nodal coefficients, when any body has one
+    bool any_alid = false;
+    for (auto& b : B) any_alid = any_alid || !b.alid_t[0].empty() || !b.alid_t[1].empty();
+    if (any_alid) {
+        M.body_alid_ptr.push_back(0);
+        for (auto& b : B) {
+            for (int dir = 0; dir < 2; dir++) {
+                M.alid_time.insert(M.alid_time.end(), b.alid_t[dir].begin(), b.alid_t[dir].end());
+                M.alid_value.insert(M.alid_value.end(), b.alid_v[dir].begin(), b.alid_v[dir].end());
+                M.body_alid_ptr.push_back((int)M.alid_time.size());
+            }
+            if (b.alid_ab.size() == b.x0.size()) M.node_alid.insert(M.node_alid.end(), b.alid_ab.begin(), b.alid_ab.end());
+            else M.node_alid.insert(M.node_alid.end(), b.x0.size(), 0.);
+        }
     }
     mel_model_desc& d = M.desc;
     M.finalize();

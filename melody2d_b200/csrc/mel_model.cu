@@ -257,7 +257,7 @@ static int tuned_chunk_cap(int precision, int max_nodes)
 {
     if (const char* c = getenv("MELGPU_CHUNK_CAP")) {
         const int v = atoi(c);
-        if (v >= 64 && v <= MEL_CHUNK_E_MAX) return v & ~7;
+        if (v >= 64 && v <= (precision == MEL_PREC_MIXED ? MEL_CHUNK_E_MAX_MX : MEL_CHUNK_E_MAX)) return v & ~7;
     }
     const char* path = getenv("MELGPU_TUNE_FILE");
     if (!path) return 0;
@@ -268,7 +268,8 @@ static int tuned_chunk_cap(int precision, int max_nodes)
     while (fgets(line, sizeof line, f)) {
         if (line[0] == '#') continue;
         int p = -1, mn = 0, c = 0;
-        if (sscanf(line, "%d %d %d", &p, &mn, &c) == 3 && p == precision && max_nodes <= mn && c >= 64 && c <= MEL_CHUNK_E_MAX) {
+        if (sscanf(line, "%d %d %d", &p, &mn, &c) == 3 && p == precision && max_nodes <= mn && c >= 64 &&
+            c <= (precision == MEL_PREC_MIXED ? MEL_CHUNK_E_MAX_MX : MEL_CHUNK_E_MAX)) {
             cap = c & ~7;
             break;
         }
@@ -476,6 +477,57 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
             D.fdamp = (double2*)dalloc<double>(h, 2 * (size_t)nn);
         }
     }
+    // ALID layers (Body::Update_alid_forces, Code/Body.h:1163-1296): the bodies whose x or y history
+    // is non-empty; per receiving degree of freedom, the terms the reference's entry loop adds when
+    // the receiving direction has a history, with d = k / (1/alpha0 + 1/alpha1) evaluated here in the
+    // reference's arithmetic
+    D.n_alid = 0;
+    if (d->body_alid_ptr && d->alid_time && d->alid_value && d->node_alid) {
+        const int* hp = d->body_alid_ptr;
+        std::vector<int> bl;
+        for (int b = 0; b < nb; b++)
+            if (d->body_type[b] == MEL_BODY_DEFORMABLE && hp[2 * b + 2] > hp[2 * b]) bl.push_back(b);
+        if (!bl.empty()) {
+            for (int k = 0; k < 2 * nb; k++)
+                if (hp[k + 1] < hp[k]) { mel_set_error("body_alid_ptr must not decrease"); return MEL_ERR_INVALID; }
+            const double* ab = d->node_alid;
+            std::vector<int> cnt(2 * (size_t)nn + 1, 0);
+            auto terms = [&](auto&& emit) {
+                for (int b : bl) {
+                    if (!d->body_matrix_ptr) break;
+                    const int n0 = d->body_node_ptr[b];
+                    const bool fl[2] = { hp[2 * b + 1] > hp[2 * b], hp[2 * b + 2] > hp[2 * b + 1] };
+                    for (int i = d->body_matrix_ptr[b]; i < d->body_matrix_ptr[b + 1]; i++) {
+                        const int dof0 = d->matrix_dofs[2 * i], dof1 = d->matrix_dofs[2 * i + 1];
+                        const int a = n0 + dof0 / 2, c = n0 + dof1 / 2;
+                        const int dir0 = dof0 % 2, dir1 = dof1 % 2;
+                        const double cf = d->matrix_stiffness[i] / (1. / ab[2 * a] + 1. / ab[2 * c]);
+                        if (fl[dir0]) emit(2 * a + dir0, 2 * c + dir1, cf);
+                        if ((dir0 != dir1 || dof0 != dof1) && fl[dir1]) emit(2 * c + dir1, 2 * a + dir0, cf);
+                    }
+                }
+            };
+            terms([&](int t, int, double) { cnt[t + 1]++; });
+            for (size_t k = 1; k < cnt.size(); k++) cnt[k] += cnt[k - 1];
+            std::vector<int> pos(cnt.begin(), cnt.end() - 1), src(std::max(cnt.back(), 1), 0);
+            std::vector<double> cf(std::max(cnt.back(), 1), 0.);
+            terms([&](int t, int s_, double c_) { src[pos[t]] = s_; cf[pos[t]] = c_; pos[t]++; });
+            std::vector<double> beta(nn);
+            for (int i = 0; i < nn; i++) beta[i] = ab[2 * i + 1];
+            const int nh = hp[2 * nb];
+            D.n_alid = (int)bl.size();
+            D.alid_b = dupload(h, bl);
+            D.alid_hptr = dupload(h, std::vector<int>(hp, hp + 2 * nb + 1));
+            D.alid_ht = dupload(h, std::vector<double>(d->alid_time, d->alid_time + nh));     // nh >= 1: a body has history
+            D.alid_hv = dupload(h, std::vector<double>(d->alid_value, d->alid_value + nh));
+            D.alid_beta = dupload(h, beta);
+            D.al_ptr = dupload(h, cnt);
+            D.al_src = dupload(h, src);
+            D.al_c = dupload(h, cf);
+            D.falid = (double2*)dalloc<double>(h, 2 * (size_t)nn);
+            MEL_CUDA_OK(cudaMemset(D.falid, 0, sizeof(double2) * (size_t)nn));
+        }
+    }
     // Solver_step state: temporaries, errors, mass-scaling factors (1), estimators (Code/IO.h:1620,1819)
     D.solver = d->solver;
     for (int k = 0; k < 8; k++) D.sp[k] = d->solver_params[k];
@@ -670,8 +722,11 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
             const int ne = std::min(ecap, gpcap * max_ns);
             const int groups = (gpcap + 31) / 32;
             const int pull_rows = std::min(max_use, gpcap) + ne / 32;
-            return mel_chunk_sections(gpcap, ne, std::min(ne, max_def_nodes),
-                                      std::min(1023, groups * max_ns) + pull_rows, mixed ? 8 : 16).bytes;
+            // pull records: touched-node slots, or (mixed two-buffer loop) the segmented list
+            // pull records: touched-node slots, or (mixed two-buffer loop) the warp bounds and at most
+            // one piece per touched node plus one per MEL_PIECE entries
+            const int tn_words = std::max(std::min(ne, max_def_nodes), mixed ? 5 + std::min(ne, max_def_nodes) + ne / MEL_PIECE : 0);
+            return mel_chunk_sections(gpcap, ne, tn_words, std::min(1023, groups * max_ns) + pull_rows, mixed ? 8 : 16).bytes;
         };
         int chosen = -1;
         // a cap from the tuning table (MELGPU_TUNE_FILE, written by melody2d_b200.autotune), or forced
@@ -713,6 +768,46 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     P.aabb = dalloc<double>(h, 4 * (size_t)nbd);
     P.shmin = dalloc<int>(h, nbd);
     P.shmax = dalloc<int>(h, nbd);
+    {
+        // cell-list broad phase for models of at least MELGPU_CELL_MIN_BODIES bodies (default 64;
+        // smaller ones take the all-pairs pass): cells 1.5 x the largest initial border box of a
+        // deformable body (with its detection distance), so a grain's box covers at most 2 x 2 cells
+        int min_bodies = 64;
+        if (const char* e = getenv("MELGPU_CELL_MIN_BODIES")) min_bodies = atoi(e);
+        double ext = 0., ext_all = 0.;
+        for (int b = 0; b < nb; b++) {
+            const int n0 = d->body_node_ptr[b];
+            const double det = d->body_dist[3 * b + 1];
+            for (int g = d->body_border_ptr[b]; g < d->body_border_ptr[b + 1]; g++) {
+                double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+                for (int k = d->border_node_ptr[g]; k < d->border_node_ptr[g + 1]; k++) {
+                    const int i = n0 + d->border_nodes[k];
+                    x0 = std::min(x0, d->node_x0[2 * i]); x1 = std::max(x1, d->node_x0[2 * i]);
+                    y0 = std::min(y0, d->node_x0[2 * i + 1]); y1 = std::max(y1, d->node_x0[2 * i + 1]);
+                }
+                const double e = std::max(x1 - x0, y1 - y0) + 2. * det;
+                if (std::isfinite(e)) {
+                    ext_all = std::max(ext_all, e);
+                    if (d->body_type[b] == MEL_BODY_DEFORMABLE) ext = std::max(ext, e);
+                }
+            }
+        }
+        if (ext <= 0.) ext = ext_all;
+        const double period = d->period[1] - d->period[0];
+        if (nb >= min_bodies && ext > 0. && std::isfinite(period) && period > 0.) {
+            P.cl_on = 1;
+            P.cl_h = 1.5 * ext;
+            P.cl_ncx = (int)std::max(1., std::min(1e6, std::floor(period / P.cl_h)));
+            P.cl_hx = period / P.cl_ncx;
+            P.cl_T = 64;
+            while (P.cl_T < 2 * nbd) P.cl_T *= 2;
+            P.cl_cnt = dalloc<int>(h, P.cl_T + 1);
+            P.cl_cur = dalloc<int>(h, P.cl_T + 1);
+            P.cl_start = dalloc<int>(h, P.cl_T + 1);
+            P.cl_idx = dalloc<int>(h, nbd);
+            P.cl_w = reinterpret_cast<unsigned long long*>(dalloc<double>(h, 2));
+        }
+    }
     P.b_inc0 = dalloc<int>(h, nb + 1);
     P.tcnt = dalloc<int>(h, nb + 1);
     P.btask0 = dalloc<int>(h, nb + 2);
@@ -969,15 +1064,17 @@ static mel_status adaptive_step(mel_handle* h)
         mel_dev d = h->d;
         mel_launch_contact(d, 0.5, h->stream);                 // Update_contact_forces(Deltat*0.5)
         mel_launch_damping(d, h->stream);
+        mel_launch_alid(d, 0, h->time, 1, h->stream);            // Update_alid_forces(Time)
         d.phase = 1;
         mel_launch_body_adaptive(d, h->time, h->t_bc, h->nblocks_body, h->body_smem, h->stream);
         mel_launch_contact(d, 0.5, h->stream);
         mel_launch_damping(d, h->stream);
+        mel_launch_alid(d, 0, h->time + h->dt * 0.5, 1, h->stream);   // Update_alid_forces(Time+Deltat*0.5)
         d.phase = 2;
         mel_launch_body_adaptive(d, h->time, h->time + h->dt * 0.5, h->nblocks_body, h->body_smem, h->stream);
         h->t_bc = h->time + h->dt;                              // Update_bc(Time+Deltat) of the second half
         mel_launch_error_reduce(d, h->d_red, h->stream);
-        h->launches += 5;
+        h->launches += 5 + (h->d.fdamp ? 2 : 0) + (h->d.falid ? 2 : 0);
         MEL_CUDA_OK(cudaGetLastError());
         MEL_CUDA_OK(cudaMemcpyAsync(h->h_red, h->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
@@ -1186,6 +1283,7 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             mel_launch_contact(h->d, 1.0, h->stream);
             mark(); kinds.push_back(0);
             if (h->d.fdamp) { mel_launch_damping(h->d, h->stream); h->launches++; }
+            if (h->d.falid) { mel_launch_alid(h->d, h->parity, 0., 0, h->stream); h->launches++; }
             mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream);
             mark(); kinds.push_back(1);
             {
@@ -2174,7 +2272,7 @@ mel_status mel_batch_create(int device, int precision, mel_batch** out)
 mel_status mel_batch_admit(mel_batch* b, mel_handle* h)
 {
     if (h && h->solver != MEL_SOLVER_EULER) { mel_set_error("batches advance the Euler scheme; step Solver_step schemes with mel_step"); return MEL_ERR_UNSUPPORTED; }
-    if (h && (h->d.fdamp || h->n_deact)) { mel_set_error("models with damping matrices or DEACTIVATION entries are stepped with mel_step, not in a batch"); return MEL_ERR_UNSUPPORTED; }
+    if (h && (h->d.fdamp || h->d.falid || h->n_deact)) { mel_set_error("models with damping matrices, ALID layers or DEACTIVATION entries are stepped with mel_step, not in a batch"); return MEL_ERR_UNSUPPORTED; }
     if (!b || !h) return MEL_ERR_INVALID;
     if (h->batch) { mel_set_error("the handle is already a member of a batch"); return MEL_ERR_INVALID; }
     if (h->device != b->device || h->precision != b->precision) {

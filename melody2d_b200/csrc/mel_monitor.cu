@@ -80,7 +80,8 @@ __device__ double2 node_force(const mel_dev& d, int b, int i, int s)
     case 4: return d.o_fdir[i];
     case 5: return d.o_fneu[i];
     case 6: return rigid ? make_double2(rf[12], rf[13]) : (d.fdamp ? d.fdamp[i] : make_double2(0., 0.));
-    default: return make_double2(0., 0.);   // ALID layers are not part of this solver
+    case 7: return rigid ? make_double2(0., 0.) : (d.falid ? d.falid[i] : make_double2(0., 0.));
+    default: return make_double2(0., 0.);
     }
 }
 

@@ -122,6 +122,60 @@ __device__ __forceinline__ void aabb_item(const mel_dev& d, double* aabb, int* s
     }
 }
 
+// the neighbour entries of border g1 (of body b1) against every active body, appended to out at
+// `count` in the reference's order (body, border, shift ascending; Code/Proximity.h:112-169): an
+// entry already listed for an earlier border of b1 (out[0..count_before)) is not repeated
+__device__ __forceinline__ void nbr_scan_all(const mel_dev& d, const double* aabb, const int* shmin, const int* shmax,
+                                             int* out, int cap, int b1, int g1, int count_before, int& count, int lane)
+{
+    const double xmin1 = aabb[4 * g1], xmax1 = aabb[4 * g1 + 1], ymin1 = aabb[4 * g1 + 2], ymax1 = aabb[4 * g1 + 3];
+    const int smin1 = shmin[g1], smax1 = shmax[g1];
+    const int first_border = (g1 == d.b_bd0[b1]);
+    for (int base = 0; base < d.nb; base += 32) {
+        int b2 = base + lane;
+        bool ok = b2 < d.nb && b2 != b1 && d.b_status[b2] != MEL_STATUS_INACTIVE;
+        int mine = 0;
+        for (int pass = 0; pass < 2; pass++) {
+            int k = 0;
+            if (ok) {
+                for (int g2 = d.b_bd0[b2]; g2 < d.b_bd0[b2 + 1]; g2++) {
+                    double xmin2 = aabb[4 * g2], xmax2 = aabb[4 * g2 + 1], ymin2 = aabb[4 * g2 + 2], ymax2 = aabb[4 * g2 + 3];
+                    if ((ymax2 < ymin1) || (ymax1 < ymin2)) continue;
+                    int r2 = g2 - d.b_bd0[b2];
+                    for (int s = smin1 - shmax[g2]; s <= smax1 - shmin[g2]; s++) {
+                        if ((xmax2 + s * d.period > xmin1) && (xmin2 + s * d.period < xmax1)) {
+                            bool dup = false;
+                            if (!first_border) {
+                                for (int q = 0; q < count_before && q < cap; q++)
+                                    if (out[3 * q] == b2 && out[3 * q + 1] == r2 && out[3 * q + 2] == s) { dup = true; break; }
+                            }
+                            if (dup) continue;
+                            if (pass == 1) {
+                                int pos = mine + k;
+                                if (pos < cap) { out[3 * pos] = b2; out[3 * pos + 1] = r2; out[3 * pos + 2] = s; }
+                            }
+                            k++;
+                        }
+                    }
+                }
+            }
+            if (pass == 0) {
+                // exclusive prefix of k across lanes
+                int incl = k;
+                for (int o = 1; o < 32; o <<= 1) {
+                    int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                int total = __shfl_sync(0xffffffffu, incl, 31);
+                mine = count + incl - k;
+                count += total;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// neighbour lists by all pairs of bodies, one warp per body
 __device__ __forceinline__ void neighbour_item(const mel_dev& d, const double* aabb, const int* shmin, const int* shmax,
                                                int* nbr, int* nbn, int cap, int b1, int lane)
 {
@@ -130,55 +184,211 @@ __device__ __forceinline__ void neighbour_item(const mel_dev& d, const double* a
     int* out = nbr + (size_t)3 * cap * b1;
     int count = 0;
     for (int g1 = d.b_bd0[b1]; g1 < d.b_bd0[b1 + 1]; g1++) {
-        double xmin1 = aabb[4 * g1], xmax1 = aabb[4 * g1 + 1], ymin1 = aabb[4 * g1 + 2], ymax1 = aabb[4 * g1 + 3];
-        int smin1 = shmin[g1], smax1 = shmax[g1];
-        int first_border = (g1 == d.b_bd0[b1]);
-        int count_before = count;   // entries of earlier border1 iterations (dedup scope)
-        for (int base = 0; base < d.nb; base += 32) {
-            int b2 = base + lane;
-            bool ok = b2 < d.nb && b2 != b1 && d.b_status[b2] != MEL_STATUS_INACTIVE;
+        const int count_before = count;   // entries of earlier border1 iterations (dedup scope)
+        nbr_scan_all(d, aabb, shmin, shmax, out, cap, b1, g1, count_before, count, lane);
+    }
+    if (lane == 0) {
+        nbn[b1] = count;
+        if (count > cap) { atomicOr(&d.err[MEL_E_NBR_OVERFLOW], 1u); atomicMax(&d.err[MEL_E_NBR_NEED], (unsigned)count); }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// cell-list broad phase: the same neighbour lists from a hashed uniform grid.  Each border box is
+// binned by its lower corner (x wrapped over the period, so that shifted copies share columns)
+// into cells of side cl_h (the largest initial box, widened; columns cl_hx = period / cl_ncx), the
+// borders are counting-sorted by bucket, and each border of a body gathers the borders whose
+// lower corner lies in a cell that a box of the run's largest width and height overlapping it
+// can occupy.  The gathered borders (hash collisions and repeated columns included) are sorted,
+// made unique and emitted with the exact overlap and shift tests of the all-pairs pass, so the
+// lists are entry for entry those of nbr_scan_all; a border whose cell range or candidate count
+// is too large takes the all-pairs pass instead.
+// ---------------------------------------------------------------------------------------------
+#define PROX_THREADS_CL 256  // threads of the job kernels (PROX_THREADS below)
+#define CL_CAND 256          // gathered candidates per border (beyond: all-pairs for that border)
+#define CL_MAX_CELLS 64      // cells one border's query visits (beyond: all-pairs)
+
+__device__ __forceinline__ int cl_bucket(const mel_prox_job& j, double x, double y)
+{
+    // (a coordinate beyond the integer range saturates: such a box is only ever found by the
+    // all-pairs pass of the borders that query it)
+    long long cx = (long long)floor((x - j.d.xmin) / j.cl_hx);
+    long long cw = cx % j.cl_ncx;
+    if (cw < 0) cw += j.cl_ncx;
+    const long long cy = (long long)floor(y / j.cl_h);
+    const unsigned k = (unsigned)cw * 73856093u ^ (unsigned)cy * 19349663u;
+    return (int)(k & (unsigned)(j.cl_T - 1));
+}
+
+__device__ __forceinline__ bool cl_box_ok(const mel_dev& d, const double* a, int g)
+{
+    return d.b_status[d.bd_body[g]] != MEL_STATUS_INACTIVE && a[4 * g] <= a[4 * g + 1] && a[4 * g + 2] <= a[4 * g + 3];
+}
+
+// a box wider or higher than a cell (a long wall, a plate) is kept out of the grid: every query
+// tests it, and its own border takes the all-pairs pass
+__device__ __forceinline__ bool cl_big(const mel_prox_job& j, const double* a)
+{
+    return a[1] - a[0] > j.cl_h || a[3] - a[2] > j.cl_h;
+}
+
+// bucket counts and the largest width and height of the binned boxes (non-negative doubles order
+// as their bits); big boxes are listed at the end of cl_idx, counted in cl_cur[cl_T]
+__device__ __forceinline__ void cl_count_item(const mel_prox_job& j, int g)
+{
+    const mel_dev& d = j.d;
+    if (g >= d.nbd || !cl_box_ok(d, j.aabb, g)) return;
+    const double* a = j.aabb + 4 * g;
+    if (cl_big(j, a)) { j.cl_idx[d.nbd - 1 - atomicAdd(&j.cl_cur[j.cl_T], 1)] = g; return; }
+    atomicMax(&j.cl_w[0], (unsigned long long)__double_as_longlong(a[1] - a[0]));
+    atomicMax(&j.cl_w[1], (unsigned long long)__double_as_longlong(a[3] - a[2]));
+    atomicAdd(&j.cl_cnt[cl_bucket(j, a[0], a[2])], 1);
+}
+
+__device__ __forceinline__ void cl_fill_item(const mel_prox_job& j, int g)
+{
+    const mel_dev& d = j.d;
+    if (g >= d.nbd || !cl_box_ok(d, j.aabb, g)) return;
+    const double* a = j.aabb + 4 * g;
+    if (cl_big(j, a)) return;
+    const int bk = cl_bucket(j, a[0], a[2]);
+    j.cl_idx[j.cl_start[bk] + atomicAdd(&j.cl_cur[bk], 1)] = g;
+}
+
+__device__ __forceinline__ void cl_zero_item(const mel_prox_job& j, int i)
+{
+    if (i > j.cl_T) return;
+    j.cl_cnt[i] = 0;
+    j.cl_cur[i] = 0;
+    if (i == 0) { j.cl_w[0] = 0ull; j.cl_w[1] = 0ull; }
+}
+
+__device__ __forceinline__ void cl_neighbour_item(const mel_prox_job& j, int b1, int lane)
+{
+    __shared__ int s_cl[PROX_THREADS_CL / 32][2 * CL_CAND];
+    const mel_dev& d = j.d;
+    if (b1 >= d.nb) return;
+    if (d.b_status[b1] == MEL_STATUS_INACTIVE) { if (lane == 0) j.nbn[b1] = 0; return; }
+    int* cand = s_cl[(threadIdx.x >> 5) % (PROX_THREADS_CL / 32)];
+    int* srt = cand + CL_CAND;
+    const double* aabb = j.aabb;
+    const int cap = j.nbr_cap;
+    int* out = j.nbr + (size_t)3 * cap * b1;
+    const double W = __longlong_as_double((long long)j.cl_w[0]), H = __longlong_as_double((long long)j.cl_w[1]);
+    int count = 0;
+    for (int g1 = d.b_bd0[b1]; g1 < d.b_bd0[b1 + 1]; g1++) {
+        const int count_before = count;
+        const double xmin1 = aabb[4 * g1], xmax1 = aabb[4 * g1 + 1], ymin1 = aabb[4 * g1 + 2], ymax1 = aabb[4 * g1 + 3];
+        // boxes left out, big boxes and boxes too far out for integer cell indices: all pairs
+        bool all = !(xmin1 <= xmax1) || !(ymin1 <= ymax1) || cl_big(j, aabb + 4 * g1) ||
+                   !(fabs(ymin1 - H) < 1e12 * j.cl_h && fabs(ymax1) < 1e12 * j.cl_h &&
+                     fabs(xmin1 - W - d.xmin) < 1e12 * j.cl_hx && fabs(xmax1 - d.xmin) < 1e12 * j.cl_hx);
+        long long cx0 = 0, cx1 = -1, cy0 = 0, cy1 = -1;
+        if (!all) {
+            // a border g2 overlapping g1 (with some shift) has its lower corner in x within
+            // [xmin1 - W, xmax1] modulo the period and in y within [ymin1 - H, ymax1]
+            cx0 = (long long)floor((xmin1 - W - d.xmin) / j.cl_hx);
+            cx1 = (long long)floor((xmax1 - d.xmin) / j.cl_hx);
+            cy0 = (long long)floor((ymin1 - H) / j.cl_h);
+            cy1 = (long long)floor(ymax1 / j.cl_h);
+            // one more cell on every side: a corner's cell is computed from its unshifted position,
+            // and rounding may put it across a cell edge from the shifted value tested here
+            cx0--; cx1++; cy0--; cy1++;
+            if (cx1 - cx0 + 1 > j.cl_ncx) cx1 = cx0 + j.cl_ncx - 1;      // every wrapped column once
+            all = (cx1 - cx0 + 1) * (cy1 - cy0 + 1) > CL_MAX_CELLS;
+        }
+        int n = 0;
+        if (!all) {
+            for (long long cy = cy0; cy <= cy1; cy++)
+                for (long long cx = cx0; cx <= cx1; cx++) {
+                    const double xc = d.xmin + ((double)cx + 0.5) * j.cl_hx, yc = ((double)cy + 0.5) * j.cl_h;
+                    const int bk = cl_bucket(j, xc, yc);
+                    const int e0 = j.cl_start[bk], e1 = j.cl_start[bk + 1];
+                    for (int e = e0; e < e1; e += 32) {
+                        bool ok = false;
+                        int g2 = -1;
+                        if (e + lane < e1) {
+                            g2 = j.cl_idx[e + lane];
+                            const int b2 = d.bd_body[g2];
+                            ok = b2 != b1 && !((aabb[4 * g2 + 3] < ymin1) || (ymax1 < aabb[4 * g2 + 2]));
+                        }
+                        const unsigned m = __ballot_sync(0xffffffffu, ok);
+                        const int pos = n + __popc(m & ((1u << lane) - 1u));
+                        if (ok && pos < CL_CAND) cand[pos] = g2;
+                        n += __popc(m);
+                    }
+                }
+            // the big boxes, outside the grid
+            const int nbig = j.cl_cur[j.cl_T];
+            for (int e = 0; e < nbig; e += 32) {
+                bool ok = false;
+                int g2 = -1;
+                if (e + lane < nbig) {
+                    g2 = j.cl_idx[d.nbd - 1 - (e + lane)];
+                    ok = d.bd_body[g2] != b1 && !((aabb[4 * g2 + 3] < ymin1) || (ymax1 < aabb[4 * g2 + 2]));
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, ok);
+                const int pos = n + __popc(m & ((1u << lane) - 1u));
+                if (ok && pos < CL_CAND) cand[pos] = g2;
+                n += __popc(m);
+            }
+            all = n > CL_CAND;
+        }
+        __syncwarp();
+        if (all) { nbr_scan_all(d, aabb, j.shmin, j.shmax, out, cap, b1, g1, count_before, count, lane); continue; }
+        // stable rank sort of the gathered borders, then the first of each run of equal values
+        for (int i = lane; i < n; i += 32) {
+            const int v = cand[i];
+            int r = 0;
+            for (int k = 0; k < n; k++) r += (cand[k] < v) || (cand[k] == v && k < i);
+            srt[r] = v;
+        }
+        __syncwarp();
+        const int smin1 = j.shmin[g1], smax1 = j.shmax[g1];
+        const int first_border = (g1 == d.b_bd0[b1]);
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            const bool valid = i < n && (i == 0 || srt[i] != srt[i - 1]);
+            const int g2 = valid ? srt[i] : 0;
+            const int b2 = valid ? d.bd_body[g2] : 0;
+            const int r2 = g2 - (valid ? d.b_bd0[b2] : 0);
             int mine = 0;
             for (int pass = 0; pass < 2; pass++) {
                 int k = 0;
-                if (ok) {
-                    for (int g2 = d.b_bd0[b2]; g2 < d.b_bd0[b2 + 1]; g2++) {
-                        double xmin2 = aabb[4 * g2], xmax2 = aabb[4 * g2 + 1], ymin2 = aabb[4 * g2 + 2], ymax2 = aabb[4 * g2 + 3];
-                        if ((ymax2 < ymin1) || (ymax1 < ymin2)) continue;
-                        int r2 = g2 - d.b_bd0[b2];
-                        for (int s = smin1 - shmax[g2]; s <= smax1 - shmin[g2]; s++) {
-                            if ((xmax2 + s * d.period > xmin1) && (xmin2 + s * d.period < xmax1)) {
-                                bool dup = false;
-                                if (!first_border) {
-                                    for (int q = 0; q < count_before && q < cap; q++)
-                                        if (out[3 * q] == b2 && out[3 * q + 1] == r2 && out[3 * q + 2] == s) { dup = true; break; }
-                                }
-                                if (dup) continue;
-                                if (pass == 1) {
-                                    int pos = mine + k;
-                                    if (pos < cap) { out[3 * pos] = b2; out[3 * pos + 1] = r2; out[3 * pos + 2] = s; }
-                                }
-                                k++;
+                if (valid) {
+                    const double xmin2 = aabb[4 * g2], xmax2 = aabb[4 * g2 + 1];
+                    for (int s = smin1 - j.shmax[g2]; s <= smax1 - j.shmin[g2]; s++) {
+                        if ((xmax2 + s * d.period > xmin1) && (xmin2 + s * d.period < xmax1)) {
+                            bool dup = false;
+                            if (!first_border)
+                                for (int q = 0; q < count_before && q < cap; q++)
+                                    if (out[3 * q] == b2 && out[3 * q + 1] == r2 && out[3 * q + 2] == s) { dup = true; break; }
+                            if (dup) continue;
+                            if (pass == 1) {
+                                const int pos = mine + k;
+                                if (pos < cap) { out[3 * pos] = b2; out[3 * pos + 1] = r2; out[3 * pos + 2] = s; }
                             }
+                            k++;
                         }
                     }
                 }
                 if (pass == 0) {
-                    // exclusive prefix of k across lanes
                     int incl = k;
                     for (int o = 1; o < 32; o <<= 1) {
-                        int t = __shfl_up_sync(0xffffffffu, incl, o);
+                        const int t = __shfl_up_sync(0xffffffffu, incl, o);
                         if (lane >= o) incl += t;
                     }
-                    int total = __shfl_sync(0xffffffffu, incl, 31);
+                    const int total = __shfl_sync(0xffffffffu, incl, 31);
                     mine = count + incl - k;
                     count += total;
                 }
             }
             __syncwarp();
         }
+        __syncwarp();
     }
     if (lane == 0) {
-        nbn[b1] = count;
+        j.nbn[b1] = count;
         if (count > cap) { atomicOr(&d.err[MEL_E_NBR_OVERFLOW], 1u); atomicMax(&d.err[MEL_E_NBR_NEED], (unsigned)count); }
     }
 }
@@ -589,6 +799,7 @@ __device__ __forceinline__ void carry_item(const mel_dev& d, mel_contact* cont, 
 // one warp per item, TPI 1: one thread).
 // ---------------------------------------------------------------------------------------------
 #define PROX_THREADS 256
+static_assert(PROX_THREADS == PROX_THREADS_CL, "cell-list scratch is sized for the job kernels' block");
 #define JOB_KERNEL(name, TPI, ...)                                                                  \
     __global__ void __launch_bounds__(PROX_THREADS) name(const mel_prox_job* J, const int* bpre, int nj) \
     {                                                                                               \
@@ -613,6 +824,10 @@ JOB_KERNEL(aabb_kernel, 32, aabb_item(d, j.aabb, j.shmin, j.shmax, it, lane))
 JOB_KERNEL(segblock_kernel, 1, segblock_item(d, it))
 JOB_KERNEL(superblock_kernel, 1, superblock_item(d, it))
 JOB_KERNEL(neighbour_kernel, 32, neighbour_item(d, j.aabb, j.shmin, j.shmax, j.nbr, j.nbn, j.nbr_cap, it, lane))
+JOB_KERNEL(cl_zero_kernel, 1, cl_zero_item(j, it))
+JOB_KERNEL(cl_count_kernel, 1, cl_count_item(j, it))
+JOB_KERNEL(cl_fill_kernel, 1, cl_fill_item(j, it))
+JOB_KERNEL(cl_neighbour_kernel, 32, cl_neighbour_item(j, it, lane))
 JOB_KERNEL(task_count_kernel, 1, task_count_item(d, j.nbn, j.tcnt, j.scnt, it))
 JOB_KERNEL(zero_tcnt_kernel, 1, if (it <= d.nb) j.tcnt[it] = 0)
 JOB_KERNEL(task_fill_kernel, 1, task_fill_item(d, j.nbr, j.nbn, j.nbr_cap, j.btask0, j.bslot0, j.task, j.tns, j.tslot,
@@ -841,6 +1056,8 @@ mel_prox_job make_job(const mel_prox_member& m, int* readback)
     j.e_cnt = P.e_cnt; j.e_ptr = P.e_ptr; j.e_cur = P.e_cur; j.e_list = P.e_list;
     j.cont_new = P.cont_alt;
     j.readback = readback;
+    j.cl_on = P.cl_on; j.cl_T = P.cl_T; j.cl_ncx = P.cl_ncx; j.cl_h = P.cl_h; j.cl_hx = P.cl_hx;
+    j.cl_cnt = P.cl_cnt; j.cl_cur = P.cl_cur; j.cl_start = P.cl_start; j.cl_idx = P.cl_idx; j.cl_w = P.cl_w;
     return j;
 }
 
@@ -925,7 +1142,7 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
         m[i].msg.clear();
         mel_prox_state& P = *m[i].P;
         const int nsc = std::max(m[i].d->nb, m[i].d->ne);
-        if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(nsc))) return MEL_ERR_OOM;
+        if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(std::max(nsc, P.cl_T)))) return MEL_ERR_OOM;
         act.push_back(i);
     }
     // 1. border boxes and segment-block boxes
@@ -942,7 +1159,21 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
         if (!J) return MEL_ERR_CUDA;
         const int np = (int)pend.size();
         nbr_clear_kernel<<<(np + 127) / 128, 128, 0, s>>>(J, np); C.launches++;
-        if ((rc = launch_jobs(C, neighbour_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 32))) return rc;
+        // members with the cell list: bucket the border boxes (counting sort), then query; the
+        // others: all pairs of bodies
+        bool any_cl = false, any_ap = false;
+        for (const mel_prox_job& jj : hj) { any_cl = any_cl || jj.cl_on; any_ap = any_ap || !jj.cl_on; }
+        if (any_cl) {
+            if ((rc = launch_jobs(C, cl_zero_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.cl_on ? j.cl_T + 1 : 0; }), 1))) return rc;
+            if ((rc = launch_jobs(C, cl_count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.cl_on ? j.d.nbd : 0; }), 1))) return rc;
+            std::vector<scan_req> sc;
+            for (int i : pend) if (m[i].P->cl_on) sc.push_back({ m[i].P->cl_cnt, m[i].P->cl_start, m[i].P->cl_T, m[i].P->scan_ws });
+            if ((rc = scan_many(C, sc))) return rc;
+            if ((rc = launch_jobs(C, cl_fill_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.cl_on ? j.d.nbd : 0; }), 1))) return rc;
+            if ((rc = launch_jobs(C, cl_neighbour_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.cl_on ? j.d.nb : 0; }), 32))) return rc;
+        }
+        if (any_ap)
+            if ((rc = launch_jobs(C, neighbour_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.cl_on ? 0 : j.d.nb; }), 32))) return rc;
         if ((rc = launch_jobs(C, task_count_kernel, J, items_of(hj, [](const mel_prox_job& j) { return j.d.nb; }), 1))) return rc;
         std::vector<scan_req> sc1, sc2;
         for (int i : pend) {
@@ -1001,7 +1232,7 @@ int mel_run_proximity_many(mel_prox_member* m, int n, mel_prox_stage*& stage, in
         if (ensure((void**)&P.nzoff, &P.nzoff_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
         if (ensure((void**)&P.nzlist, &P.nzlist_bytes, sizeof(int) * ns)) return MEL_ERR_OOM;
         const int nsc = std::max(std::max(m[i].d->nb, m[i].d->ne), P.nslot);
-        if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(nsc))) return MEL_ERR_OOM;
+        if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(std::max(nsc, P.cl_T)))) return MEL_ERR_OOM;
     }
     J = upload_jobs(C, m, act, hj);
     if (!J) return MEL_ERR_CUDA;
@@ -1109,7 +1340,7 @@ int mel_index_external(mel_dev& d, mel_prox_state& P, const mel_contact* host_li
     d.b_inc0 = P.b_inc0;
     d.b_cont0 = P.b_cont0;
     if (ensure((void**)&P.e_list, &P.e_list_bytes, sizeof(int) * ((size_t)d.ncont + 1))) return MEL_ERR_OOM;
-    if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(std::max(d.nb, d.ne)))) return MEL_ERR_OOM;
+    if (ensure((void**)&P.scan_ws, &P.scan_ws_bytes, sizeof(int) * scan_scratch_ints(std::max(std::max(d.nb, d.ne), P.cl_T)))) return MEL_ERR_OOM;
     if (!stage_ready(P.stage, 1)) { mel_set_error("proximity read-back buffers could not be allocated"); return MEL_ERR_OOM; }
     mel_prox_member m;
     m.d = &d;

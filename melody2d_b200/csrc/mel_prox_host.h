@@ -33,6 +33,13 @@ struct mel_prox_state {
     double* cont_w = nullptr; size_t cont_w_bytes = 0;
     double* cont_rt = nullptr; size_t cont_rt_bytes = 0;
     int* scan_ws = nullptr; size_t scan_ws_bytes = 0;    // scan block totals
+    // cell-list broad phase (cl_on): bucket counts / cursors and starts (cl_T + 1 each), border
+    // indices by bucket, the run's largest box width and height; cell side cl_h, columns cl_hx
+    // (cl_ncx per period)
+    int cl_on = 0, cl_T = 0, cl_ncx = 1;
+    double cl_h = 0., cl_hx = 0.;
+    int *cl_cnt = nullptr, *cl_cur = nullptr, *cl_start = nullptr, *cl_idx = nullptr;
+    unsigned long long* cl_w = nullptr;
     int ntask = 0, nslot = 0;
     int launches = 0;                                      // kernels launched by the pipeline (running count)
     mel_prox_stage* stage = nullptr;                       // staging of this handle's own runs
@@ -56,6 +63,10 @@ struct mel_prox_job {
     int* e_cnt; int* e_ptr; int* e_cur; int* e_list;
     mel_contact* cont_new;        // the list being written (write stage)
     int* readback;                // this member's words of the run's read-back array
+    int cl_on, cl_T, cl_ncx;      // cell-list broad phase (mel_prox_state)
+    double cl_h, cl_hx;
+    int *cl_cnt, *cl_cur, *cl_start, *cl_idx;
+    unsigned long long* cl_w;
 };
 
 // A model taking part in a run.  rc: MEL_OK, or the member's own failure (MEL_ERR_NAN,

@@ -174,6 +174,10 @@ class Body:
     # MATRICES of STATIC_DATA (Code/IO.h:1827-1851): upper-triangle (dof0, dof1) pairs, dof = 2 node +
     # direction, with their stiffness and damping coefficients; None writes an empty section
     matrices: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
+    # ALID absorbing layer of STATIC_CONTROL (Code/IO.h:1395-1480): keys x_hist and y_hist (lists
+    # of (time, value) of the layer's reference velocity) and xmin, xmax, ymin, ymax, range,
+    # alphain, alphaout, betain, betaout, exponent; None: no layer
+    alid: Optional[dict] = None
 
 
 def _ccw(nodes: np.ndarray, tri: np.ndarray) -> np.ndarray:
@@ -445,6 +449,67 @@ _SPY_CODES = {
     "Velocity": (2, ["X", "Y", "Mag", "R"]), "Acceleration": (3, ["X", "Y", "Mag", "R"]),
 }
 _FORCE_KINDS = ["Total", "Internal", "Contact", "Body", "Dirichlet", "Neumann", "Damping", "Alid"]
+
+
+_libm = None
+
+
+def _cpow(x: float, y: float) -> float:
+    """The C library's pow, the one Load_static calls (CPython's ** refuses a negative base)."""
+    global _libm
+    if _libm is None:
+        import ctypes
+        import ctypes.util
+        _libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+        _libm.pow.restype = ctypes.c_double
+        _libm.pow.argtypes = [ctypes.c_double, ctypes.c_double]
+    return _libm.pow(x, y)
+
+
+def alid_coefficients(body: "Body") -> np.ndarray:
+    """alid_alpha and alid_beta of every node of a deformable body, as Load_static computes them
+    from the initial position while reading NODES (Code/IO.h:1548-1600): layers of width `range`
+    inside [ymin, ymax] (bottom/top) and [xmin, xmax] (left/right), graded from *in to *out with
+    the given exponent; a node in a side layer keeps the larger of the two values."""
+    n = body.nodes.shape[0]
+    out = np.zeros((n, 2))
+    A = body.alid
+    if A is None or (not A["x_hist"] and not A["y_hist"]):
+        return out
+    ain, aout, bin_, bout, rng_, ex = A["alphain"], A["alphaout"], A["betain"], A["betaout"], A["range"], A["exponent"]
+    for i in range(n):
+        x, y = float(body.nodes[i, 0]), float(body.nodes[i, 1])
+        al = be = 0.0
+        if y < A["ymin"] + rng_:
+            ka = (aout - ain) / _cpow(-rng_, ex)
+            kb = (bout - bin_) / _cpow(-rng_, ex)
+            al = ain + ka * _cpow(y - (A["ymin"] + rng_), ex)
+            be = bin_ + kb * _cpow(y - (A["ymin"] + rng_), ex)
+        elif y > A["ymax"] - rng_:
+            ka = (aout - ain) / _cpow(rng_, ex)
+            kb = (bout - bin_) / _cpow(rng_, ex)
+            al = ain + ka * _cpow(y - (A["ymax"] - rng_), ex)
+            be = bin_ + kb * _cpow(y - (A["ymax"] - rng_), ex)
+        if x < A["xmin"] + rng_:
+            ka = (aout - ain) / _cpow(-rng_, ex)
+            kb = (bout - bin_) / _cpow(-rng_, ex)
+            t = ain + ka * _cpow(x - (A["xmin"] + rng_), ex)
+            if t > al:
+                al = t
+            t = bin_ + kb * _cpow(x - (A["xmin"] + rng_), ex)
+            if t > be:
+                be = t
+        elif x > A["xmax"] - rng_:
+            ka = (aout - ain) / _cpow(rng_, ex)
+            kb = (bout - bin_) / _cpow(rng_, ex)
+            t = ain + ka * _cpow(x - (A["xmax"] - rng_), ex)
+            if t > al:
+                al = t
+            t = bin_ + kb * _cpow(x - (A["xmax"] - rng_), ex)
+            if t > be:
+                be = t
+        out[i] = (al, be)
+    return out
 
 
 def deactivation_vector(line: str) -> List[float]:
@@ -789,6 +854,18 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
     f["matrix_damping"] = np.concatenate(mc).astype(np.float64) if mc else np.zeros(0, dtype=np.float64)
     f["deactivated"] = np.array([deactivation_vector(line) for line in scene.deactivation],
                                 dtype=np.float64).reshape(-1, 8)
+    if any(b.alid is not None for b in scene.bodies):
+        aptr = [0]; at = []; av = []; ab = []
+        for b in scene.bodies:
+            for key in ("x_hist", "y_hist"):
+                h = b.alid[key] if b.alid is not None else []
+                at += [float(t) for t, _ in h]; av += [float(v) for _, v in h]
+                aptr.append(len(at))
+            ab.append(alid_coefficients(b) if b.kind == "deformable" else np.zeros((b.nodes.shape[0], 2)))
+        f["body_alid_ptr"] = np.array(aptr, dtype=np.int32)
+        f["alid_time"] = np.array(at, dtype=np.float64)
+        f["alid_value"] = np.array(av, dtype=np.float64)
+        f["node_alid"] = np.concatenate(ab).reshape(-1).astype(np.float64)
     f["material_names"] = names
     return f  # type: ignore[return-value]
 
@@ -864,6 +941,18 @@ def write_asc(scene: Scene, directory: str, workers: int = 1) -> None:
         if b.kind == "deformable":
             L += ["INTEGRATION", f"{b.gp[0].shape[0] - 1} {b.n_regions}", " "]
         L += ["TRIANGULATION", str(b.cells.shape[0]), " ", " "]
+        if b.alid is not None:
+            # Load_static reads the twelve numbers, skips the rest of their line and one more line,
+            # then the x history, one separating line when both exist, and the y history
+            A = b.alid
+            L += ["ALID", " ".join([str(len(A["x_hist"])), str(len(A["y_hist"]))] +
+                                   [_g(A[k]) for k in ("xmin", "xmax", "ymin", "ymax", "range", "alphain",
+                                                       "alphaout", "betain", "betaout", "exponent")]), " "]
+            L += [f"{_g(t)} {_g(v)}" for t, v in A["x_hist"]]
+            if A["x_hist"] and A["y_hist"]:
+                L += [" "]
+            L += [f"{_g(t)} {_g(v)}" for t, v in A["y_hist"]]
+            L += [" "]
     with open(os.path.join(directory, "STATIC_CONTROL.asc"), "w") as fh:
         fh.write("\n".join(L) + "\n")
 

@@ -499,6 +499,11 @@ def load_desc_arrays(directory: str, restart_index: int = 0) -> dict:
         out["matrix_stiffness"] = arr(d.matrix_stiffness, d.n_matrix, np.float64)
         out["matrix_damping"] = arr(d.matrix_damping, d.n_matrix, np.float64)
         out["deactivated"] = arr(d.deactivated, d.n_deactivated * abi.MEL_DEACT_NF, np.float64).reshape(-1, abi.MEL_DEACT_NF)
+        if d.body_alid_ptr:
+            out["body_alid_ptr"] = arr(d.body_alid_ptr, 2 * nb + 1, np.int32)
+            na = int(out["body_alid_ptr"][-1])
+            out["alid_time"] = arr(d.alid_time, na, np.float64); out["alid_value"] = arr(d.alid_value, na, np.float64)
+            out["node_alid"] = arr(d.node_alid, 2 * nn, np.float64)
         return out
     finally:
         L.mel_free_desc(owner)

@@ -70,6 +70,7 @@ struct orc_model {
     int ndeact; double* deact;   /* DEACTIVATION entries, MEL_DEACT_NF doubles each */
     int* cells;
     int nmx; int* mx_ptr; int* mx_dofs; double *mx_k, *mx_c;
+    int* alid_ptr; double *alid_t, *alid_v, *alid_ab;   /* ALID histories and nodal alpha, beta (or NULL) */
     /* dynamic lists */
     cvec* cont; nbr_t** nbl; int* nbn; int* nbc; svec* send;
     /* Solver_step storage (Body::Store/Restore, Body.h:2601-2659) */
@@ -769,6 +770,53 @@ static void update_damping_forces(orc_model* m, int b)
         } else {
             m->fdamp[2 * a + 1] -= m->vp[2 * c + 1] * d;
             if (dof0 != dof1) m->fdamp[2 * c + 1] -= m->vp[2 * a + 1] * d;
+        }
+    }
+}
+
+/* Body::Update_alid_forces (Code/Body.h:1163-1296): the layer's reference velocity of each
+ * direction interpolated in its history at Time (the first interval holding Time; the reference
+ * scans past the end of its vector when none does, here the value stays 0), the nodal term
+ * -beta m (v - pv), then the stiffness entries' terms -(v_param - pv) d with
+ * d = k / (1/alpha0 + 1/alpha1), in entry order; a direction without history gets no force */
+static void update_alid_forces(orc_model* m, int b, double T)
+{
+    if (m->btype[b] != MEL_BODY_DEFORMABLE || !m->alid_ptr) return;
+    int flag[2];
+    double pv[2] = { 0., 0. };
+    for (int dir = 0; dir < 2; dir++) {
+        int h0 = m->alid_ptr[2 * b + dir], h1 = m->alid_ptr[2 * b + dir + 1];
+        flag[dir] = h1 > h0;
+        for (int k = h0; k + 1 < h1; k++) {
+            double t0 = m->alid_t[k], p0 = m->alid_v[k], t1 = m->alid_t[k + 1], p1 = m->alid_v[k + 1];
+            if ((t0 <= T) & (T <= t1)) { pv[dir] = p0 + (p1 - p0) / (t1 - t0) * (T - t0); break; }
+        }
+    }
+    if (!flag[0] && !flag[1]) return;          /* flag_alid == 0 */
+    int n0 = m->nptr[b];
+    for (int i = n0; i < m->nptr[b + 1]; i++) {
+        double beta = m->alid_ab[2 * i + 1];
+        m->falid[2 * i] = flag[0] ? -beta * m->mass[2 * i] * (m->v[2 * i] - pv[0]) : 0.;
+        m->falid[2 * i + 1] = flag[1] ? -beta * m->mass[2 * i + 1] * (m->v[2 * i + 1] - pv[1]) : 0.;
+    }
+    if (!m->mx_ptr) return;
+    for (int i = m->mx_ptr[b]; i < m->mx_ptr[b + 1]; i++) {
+        int dof0 = m->mx_dofs[2 * i], dof1 = m->mx_dofs[2 * i + 1];
+        int node0 = dof0 / 2, dir0 = dof0 - node0 * 2, node1 = dof1 / 2, dir1 = dof1 - node1 * 2;
+        int a = n0 + node0, c = n0 + node1;
+        double d = m->mx_k[i] / (1. / m->alid_ab[2 * a] + 1. / m->alid_ab[2 * c]);
+        if (dir0 == 0 && dir1 == 0) {
+            if (flag[0]) m->falid[2 * a] += -(m->vp[2 * c] - pv[0]) * d;
+            if ((dof0 != dof1) && flag[0]) m->falid[2 * c] += -(m->vp[2 * a] - pv[0]) * d;
+        } else if (dir0 == 0 && dir1 == 1) {
+            if (flag[0]) m->falid[2 * a] += -(m->vp[2 * c + 1] - pv[1]) * d;
+            if (flag[1]) m->falid[2 * c + 1] += -(m->vp[2 * a] - pv[0]) * d;
+        } else if (dir0 == 1 && dir1 == 0) {
+            if (flag[1]) m->falid[2 * a + 1] += -(m->vp[2 * c] - pv[0]) * d;
+            if (flag[0]) m->falid[2 * c] += -(m->vp[2 * a + 1] - pv[1]) * d;
+        } else {
+            if (flag[1]) m->falid[2 * a + 1] += -(m->vp[2 * c + 1] - pv[1]) * d;
+            if ((dof0 != dof1) && flag[1]) m->falid[2 * c + 1] += -(m->vp[2 * a + 1] - pv[1]) * d;
         }
     }
 }
@@ -1576,7 +1624,7 @@ static void initialize_czm(orc_model* m)
 /* ------------------------------------------------------------------------------------------ */
 /* Step drivers (Code/Solver.h)                                                                 */
 /* ------------------------------------------------------------------------------------------ */
-static void force_evaluation(orc_model* m, double law_dt, double bc_time, int update_bc_first)
+static void force_evaluation(orc_model* m, double law_dt, double bc_time, int update_bc_first, double alid_time)
 {
     for (int i = 0; i < m->nb; i++) {
         if (!is_active(m, i)) continue;
@@ -1590,6 +1638,7 @@ static void force_evaluation(orc_model* m, double law_dt, double bc_time, int up
         update_bc_forces(m, i);
         update_body_forces(m, i);
         update_damping_forces(m, i);
+        update_alid_forces(m, i, alid_time);
         update_contact_forces(m, i, law_dt);
     }
     for (int i = 0; i < m->nb; i++) send_contact_forces(m, i);
@@ -1602,7 +1651,7 @@ static void force_evaluation(orc_model* m, double law_dt, double bc_time, int up
 /* Euler_step (Code/Solver.h:10-88) */
 static void euler_step(orc_model* m)
 {
-    force_evaluation(m, m->dt, 0., 0);
+    force_evaluation(m, m->dt, 0., 0, m->time);
     for (int i = 0; i < m->nb; i++) {
         if (!is_active(m, i)) continue;
         sum_up_forces(m, i);
@@ -1681,7 +1730,7 @@ static void solver_step(orc_model* m)
     double max_error = 0., mean_error = 0., total_mass = 0., max_mass = 0.;
     while (!ok) {
         neval++;
-        force_evaluation(m, m->dt * 0.5, 0., 0);
+        force_evaluation(m, m->dt * 0.5, 0., 0, m->time);
         for (int i = 0; i < m->nb; i++) {
             if (!is_active(m, i)) continue;
             sum_up_forces(m, i);
@@ -1692,7 +1741,7 @@ static void solver_step(orc_model* m)
             update_kinematics(m, i);
             update_current_positions(m, i);
         }
-        force_evaluation(m, m->dt * 0.5, m->time + m->dt * 0.5, 1);
+        force_evaluation(m, m->dt * 0.5, m->time + m->dt * 0.5, 1, m->time + m->dt * 0.5);
         for (int i = 0; i < m->nb; i++) {
             if (!is_active(m, i)) continue;
             sum_up_forces(m, i);
@@ -1905,6 +1954,12 @@ int orc_create(const mel_model_desc* d, const int* n_regions, orc_model** out)
     if (d->n_matrix > 0 && d->body_matrix_ptr) {
         m->mx_ptr = dupi(d->body_matrix_ptr, nb + 1); m->mx_dofs = dupi(d->matrix_dofs, 2 * (size_t)d->n_matrix);
         m->mx_k = dupd(d->matrix_stiffness, d->n_matrix); m->mx_c = dupd(d->matrix_damping, d->n_matrix);
+    }
+    if (d->body_alid_ptr && d->alid_time && d->alid_value && d->node_alid) {
+        m->alid_ptr = dupi(d->body_alid_ptr, 2 * (size_t)nb + 1);
+        int nh = m->alid_ptr[2 * nb];
+        m->alid_t = dupd(d->alid_time, nh); m->alid_v = dupd(d->alid_value, nh);
+        m->alid_ab = dupd(d->node_alid, 2 * (size_t)nn);
     }
     m->cont = (cvec*)xcalloc((size_t)nb, sizeof(cvec)); m->s_cont = (cvec*)xcalloc((size_t)nb, sizeof(cvec));
     m->nbl = (nbr_t**)xcalloc((size_t)nb, sizeof(nbr_t*)); m->nbn = NEWI(nb); m->nbc = NEWI(nb);

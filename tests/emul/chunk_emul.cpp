@@ -115,3 +115,105 @@ extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const dou
     }
     return 0;
 }
+
+// The mixed pass's two-buffer images (pull pieces).  Checks every index the kernel follows and
+// the layout's invariants: the pieces list the entries back to back in node order, at most
+// MEL_PIECE each, every piece's entries are stored for its node, a node's pieces belong to one
+// warp, and every stored entry of a point is listed once.  Then forms FP64 contributions
+// c0 * (dN . up) from the stored FP32 derivatives (a stand-in for the kernel's strain and stress,
+// enough to exercise the indexing) and returns the nodal sums two ways: f_list piece by piece,
+// f_direct by scattering each point's contributions directly.  stats: [chunks, listed entries, largest
+// image bytes, largest warp share / mean share x 1000].
+extern "C" int emul_segmented_pull(const mel_model_desc* d, int ecap, const double* up, double* f_list,
+                                   double* f_direct, long long* stats)
+{
+    mel_chunk_set CS;
+    if (mel_build_chunks(d, ecap, CS, true, 1LL << 62) != MEL_OK) return 100;
+    stats[0] = (long long)CS.chunks.size(); stats[1] = 0; stats[2] = CS.img_max; stats[3] = 0;
+    memset(f_list, 0, sizeof(double) * 2 * (size_t)d->n_nodes);
+    memset(f_direct, 0, sizeof(double) * 2 * (size_t)d->n_nodes);
+    for (int b = 0; b < d->n_bodies; b++) {
+        if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
+        if (CS.b_pipe[b]) return 20;
+        const int n0 = d->body_node_ptr[b], n = d->body_node_ptr[b + 1] - n0;
+        for (int ci = CS.b_chunk0[b]; ci < CS.b_chunk0[b + 1]; ci++) {
+            const mel_chunk& c = CS.chunks[ci];
+            if (c.bytes % 16 || c.img % 16 || c.bytes > CS.img_max) return 21;
+            std::vector<uint8_t> buf(CS.img.begin() + c.img, CS.img.begin() + c.img + c.bytes);
+            int hdr[4];
+            memcpy(hdr, buf.data(), sizeof hdr);
+            if (hdr[0] > MEL_CHUNK_GP_FP64 || hdr[1] % 8 || hdr[1] > ecap || hdr[3] > 1024) return 22;
+            const mel_chunk_layout L = mel_chunk_sections(hdr[0], hdr[1], hdr[2], hdr[3], 8);
+            if (L.bytes != c.bytes) return 23;
+            const float* sp = reinterpret_cast<const float*>(buf.data() + L.dN);
+            const uint16_t* sidx = reinterpret_cast<const uint16_t*>(buf.data() + L.idx);
+            const uint16_t* spos = reinterpret_cast<const uint16_t*>(buf.data() + L.tpos);
+            const double* sc0 = reinterpret_cast<const double*>(buf.data() + L.c0);
+            const uint32_t* sgpm = reinterpret_cast<const uint32_t*>(buf.data() + L.gpm);
+            const uint16_t* swr = reinterpret_cast<const uint16_t*>(buf.data() + L.tn);
+            const uint16_t* ssn = swr + (MEL_PULL_WARPS + 1);
+            const uint16_t* sroff = reinterpret_cast<const uint16_t*>(buf.data() + L.roff);
+            const int ne = hdr[1];
+            // contributions per stored position, and the direct scatter
+            std::vector<double> q(2 * (size_t)ne, 0.);
+            std::vector<int> listed(ne, 0), stored(ne, 0);
+            for (int t = 0; t < hdr[0]; t++) {
+                const uint32_t gm = sgpm[t];
+                const int r0 = (int)(gm & 0x3ffu), lane = (int)((gm >> 10) & 0x1fu), ns = (int)(gm >> 15);
+                if (r0 + ns > hdr[3] || lane != t % 32) return 24;
+                const int m = (hdr[0] - (t & ~31)) < 32 ? hdr[0] - (t & ~31) : 32;
+                const int sw = (m & 7) == 0 ? 7 : 0;
+                const int base = (int)(sroff[r0] & 0xfffu);
+                for (int k = 0; k < ns; k++) {
+                    const int e = base + m * k + (lane ^ (k & sw));
+                    if (e >= ne || sidx[e] >= n) return 25;
+                    const int i = sidx[e];
+                    const double v = (double)sp[2 * e] * up[2 * (n0 + i)] + (double)sp[2 * e + 1] * up[2 * (n0 + i) + 1];
+                    q[2 * e] = sc0[t] * v;
+                    q[2 * e + 1] = sc0[t] * (v + (double)sp[2 * e]);
+                    stored[e]++;
+                    f_direct[2 * (n0 + i)] -= q[2 * e];
+                    f_direct[2 * (n0 + i) + 1] -= q[2 * e + 1];
+                }
+            }
+            // pieces: (first listed entry, count, node); the listed entries, in order, are the
+            // pieces' entries back to back
+            const uint32_t* spc = reinterpret_cast<const uint32_t*>(buf.data() + L.tn + 16);
+            const int npc = swr[MEL_PULL_WARPS];
+            if (swr[0] != 0 || 16 + 4 * npc > 4 * ((hdr[2] + 3) & ~3)) return 26;
+            int nl = 0, share_max = 0, prev_node = -1, prev_warp = -1;
+            for (int w = 0; w < MEL_PULL_WARPS; w++) {
+                const int a = swr[w], e1 = swr[w + 1];
+                if (e1 < a || e1 > npc) return 27;
+                int share = 0;
+                for (int pi = a; pi < e1; pi++) {
+                    const uint32_t rec = spc[pi];
+                    const int q0 = (int)(rec & 0x1fffu), cnt = (int)((rec >> 13) & 7u) + 1, node = (int)((rec >> 16) & 0xfffu);
+                    if (q0 != nl || cnt > MEL_PIECE || node >= n) return 28;
+                    if (node < prev_node) return 31;                           // sorted by node
+                    if (node == prev_node && w != prev_warp) return 33;        // a node within one warp
+                    double sx = 0., sy = 0.;
+                    for (int i = 0; i < cnt; i++) {
+                        const int qq = q0 + i;
+                        if (qq >= ne || spos[qq] >= ne) return 29;
+                        if (sidx[spos[qq]] != node) return 30;                 // listed node is the stored one
+                        listed[spos[qq]]++;
+                        sx += q[2 * spos[qq]];
+                        sy += q[2 * spos[qq] + 1];
+                    }
+                    f_list[2 * (n0 + node)] -= sx;
+                    f_list[2 * (n0 + node) + 1] -= sy;
+                    nl += cnt;
+                    share += cnt;
+                    prev_node = node;
+                    prev_warp = w;
+                }
+                share_max = std::max(share_max, share);
+            }
+            stats[1] += nl;
+            for (int e = 0; e < ne; e++) if (listed[e] != stored[e]) return 32;   // each stored entry once
+            if (nl > 0) stats[3] = std::max(stats[3], (long long)share_max * 1000 * MEL_PULL_WARPS / nl);
+        }
+    }
+    return 0;
+}

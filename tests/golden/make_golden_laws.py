@@ -3,8 +3,9 @@ tests/test_oracle_laws.py (each contact law, with and without INITIALIZE_CZM whe
 NeoHookean, border conditions of deformable bodies, two 12-disc biaxial samples, an x-periodic
 domain and a spinning rigid disc), at full FP64 precision.
 
-    python tests/golden/make_golden_laws.py   (needs oracle/_ref/ref_harness, built by oracle/Makefile
-                                              from the reference sources)
+    python tests/golden/make_golden_laws.py [case ...]
+        (needs oracle/_ref/ref_harness, built by oracle/Makefile from the reference sources; with
+        case names, only those cases are rerun and the others are kept from the existing file)
 
 The harness (oracle/ref_harness.cpp) runs the reference's Load_static / Load_dynamic / set-up /
 Euler_step / Update_proximity unchanged on one thread and dumps every node, work and contact
@@ -40,8 +41,14 @@ def main():
     harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     if not os.path.exists(harness):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    out = os.path.join(HERE, "laws_ref.json")
+    only = sys.argv[1:]
     cases = {}
+    if only and os.path.exists(out):
+        cases = json.load(open(out))["cases"]
     for name in CASES:
+        if only and name not in only:
+            continue
         sc = case_scene(name)
         flat = g.flatten(sc)
         with tempfile.TemporaryDirectory() as tmp:
@@ -56,9 +63,10 @@ def main():
         cases[name] = {"input_sha256": input_checksum(flat),
                        "steps": {str(s): record_summary(by_step[s]) for s in STEPS}}
         print(name, "contacts", cases[name]["steps"][str(STEPS[-1])]["n_contacts"])
-    with open(os.path.join(HERE, "laws_ref.json"), "w") as fh:
+    cases = {k: cases[k] for k in CASES if k in cases}
+    with open(out, "w") as fh:
         json.dump({"cases": cases}, fh, indent=1)
-    print("wrote", os.path.join(HERE, "laws_ref.json"))
+    print("wrote", out)
 
 
 if __name__ == "__main__":

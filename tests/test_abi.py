@@ -19,7 +19,7 @@ def test_library_exports_all_declared_symbols(gpu_lib):
 
 
 def test_abi_version(gpu_lib):
-    assert gpu_lib.mel_abi_version() == 1
+    assert gpu_lib.mel_abi_version() == 2
 
 
 def test_struct_sizes_match_header():

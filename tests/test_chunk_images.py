@@ -47,3 +47,29 @@ def test_chunk_pass_matches_oracle(emul, oracle_built, ecap):
     assert stats[2] < 0.2 * stats[1], "padding above a fifth of the stored entries"
     np.testing.assert_array_equal(f, ref)
     assert np.abs(ref).max() > 0
+
+
+@pytest.mark.parametrize("ecap", [3584, 2048, 1024, 256])
+def test_segmented_pull_layout(emul, ecap):
+    """Images of the mixed pass's two-buffer loop: the pull pieces list every stored entry once,
+    each piece's entries are stored for its node, a node's pieces belong to one of the seven pull
+    warps, and the piece sums give the nodal forces of a direct scatter."""
+    from melody2d_b200.abi import Desc
+    flat = flat_of(squeezed_lattice(3, 3))
+    desc = Desc(flat)
+    rng = np.random.default_rng(5)
+    up = rng.standard_normal((len(flat["node_x0"]) // 2, 2)) * 1e-5
+    f_list = np.zeros_like(up)
+    f_direct = np.zeros_like(up)
+    stats = np.zeros(4, dtype=np.int64)
+    emul.emul_segmented_pull.restype = C.c_int
+    emul.emul_segmented_pull.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rc = emul.emul_segmented_pull(C.byref(desc.desc), ecap, up.ctypes.data, f_list.ctypes.data,
+                                  f_direct.ctypes.data, stats.ctypes.data)
+    assert rc == 0, (rc, emul.emul_error())
+    assert stats[0] > 0 and stats[1] > 0
+    # the heaviest warp's share of the entries stays near the mean (whole nodes only)
+    assert stats[3] < 1500, stats
+    scale = np.abs(f_direct).max()
+    assert scale > 0
+    np.testing.assert_allclose(f_list, f_direct, rtol=0, atol=1e-12 * scale)

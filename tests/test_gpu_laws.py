@@ -187,6 +187,38 @@ def test_damping_matrices_bit_identical(gpu_lib, oracle_built):
     gs.close()
 
 
+def test_alid_layers_bit_identical(gpu_lib, oracle_built):
+    """ALID absorbing layers on the grains (the ALID block of STATIC_CONTROL with x and y histories
+    of the layer's reference velocity, Body::Update_alid_forces, Code/Body.h:1163-1296): node state,
+    contacts and works equal the oracle's (itself pinned to the compiled reference on this case,
+    tests/test_oracle_laws.py) over 100 steps; the ALID work is non-zero, and the model with its
+    layers read from the case's files by the library's loader steps to the same state."""
+    import tempfile
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    from test_oracle_laws import case_scene
+    scene = case_scene("alid")
+    flat = g.flatten(scene)
+    assert np.count_nonzero(flat["node_alid"]) > 100
+    gs = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    for _ in range(5):
+        gs.step(20)
+        o.step(20)
+        np.testing.assert_array_equal(gs.node_state(), o.node_state())
+        assert_contacts_equal(gs.contacts(), o.contacts())
+    np.testing.assert_array_equal(gs.works(), o.works())
+    assert np.abs(gs.works()[:, 6]).max() > 0
+    with tempfile.TemporaryDirectory() as tmp:
+        g.write_asc(scene, tmp)
+        gf = Solver.from_files(tmp)
+        gf.step(100)
+        np.testing.assert_array_equal(gf.node_state(), gs.node_state())
+        gf.close()
+    gs.close()
+
+
 def test_deactivation_bit_identical(gpu_lib, oracle_built):
     """DEACTIVATION entries (Update_status after each proximity update, Code/Proximity.h:550-1007):
     a free rigid disc beside the pressed lattice turns inactive by its displacement at the same

@@ -25,18 +25,24 @@ def test_missing_files_report_io_error(tmp_path, gpu_lib):
     assert e.value.code == 8
 
 
-def test_asc_roundtrip_matrices_and_deactivation(tmp_path, gpu_lib):
+def test_asc_roundtrip_matrices_deactivation_alid(tmp_path, gpu_lib):
     """MATRICES (Code/IO.h:1827-1851) and DEACTIVATION entries (Read_spy_line plus below / equal /
     above and the threshold, Code/IO.h:947-968) read back as the generator encoded them."""
     import sys, os
     sys.path.insert(0, os.path.dirname(__file__))
     from melody2d_b200 import generator as g, solver
     from test_oracle_laws import case_scene
-    for name in ("damping", "deactivation"):
+    for name in ("damping", "deactivation", "alid"):
         scene = case_scene(name)
         d_ = tmp_path / name
         g.write_asc(scene, str(d_))
         d = solver.load_desc_arrays(str(d_))
         f = g.flatten(scene)
-        for k in ("body_matrix_ptr", "matrix_dofs", "matrix_stiffness", "matrix_damping", "deactivated"):
+        keys = ["body_matrix_ptr", "matrix_dofs", "matrix_stiffness", "matrix_damping", "deactivated"]
+        if name == "alid":
+            # the ALID block (Code/IO.h:1395-1480) and the nodal coefficients the loader computes
+            # from the initial positions (Code/IO.h:1548-1600), equal to the generator's
+            keys += ["body_alid_ptr", "alid_time", "alid_value", "node_alid"]
+            assert np.count_nonzero(f["node_alid"]) > 0
+        for k in keys:
             np.testing.assert_array_equal(np.asarray(f[k]), np.asarray(d[k]), err_msg=(name, k))

@@ -43,7 +43,7 @@ CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7
                                                     "border_conditions", "biaxial12_s5", "biaxial12_s7",
                                                     "periodic", "rotor", "adaptive_euler", "euler_2",
                                                     "mass_scaling", "adaptive_mass_scaling", "damping",
-                                                    "deactivation"]
+                                                    "deactivation", "alid"]
 
 # Solver_step schemes (Code/Solver.h:98-486) with their parameters: Target_error, Control_parameter,
 # Accepted_ratio, Max_mass_scaling, Control_parameter_mass_scaling, Error_factor_mass_scaling,
@@ -91,6 +91,19 @@ def case_scene(name):
         # Rayleigh damping matrices on the grains (MATRICES, Body::Update_damping_forces)
         E, nu = 1e8, 0.3
         g.add_damping(sc, 0.02 * sc.dt, 0.05 / sc.dt, E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu)))
+    elif name == "alid":
+        # ALID absorbing layers on every grain: layers 0.9 mm wide along the lattice's outline,
+        # graded quadratically, reference velocities of the layer in x and y; the stiffness
+        # matrices (MATRICES, no damping) give the layers' coupling terms
+        E, nu = 1e8, 0.3
+        g.add_damping(sc, 0.0, 0.0, E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu)))
+        grains = [b for b in sc.bodies if b.kind == "deformable"]
+        x0 = min(b.nodes[:, 0].min() for b in grains); x1 = max(b.nodes[:, 0].max() for b in grains)
+        y0 = min(b.nodes[:, 1].min() for b in grains); y1 = max(b.nodes[:, 1].max() for b in grains)
+        for b in grains:
+            b.alid = {"x_hist": [(0.0, 0.0), (2e-5, 0.02), (g.T_HIST_END, 0.02)], "y_hist": [(0.0, -0.01), (g.T_HIST_END, -0.01)],
+                      "xmin": x0, "xmax": x1, "ymin": y0, "ymax": y1, "range": 0.9e-3, "alphain": 0.0,
+                      "alphaout": 0.05 * sc.dt, "betain": 0.0, "betaout": 0.1 / sc.dt, "exponent": 2.0}
     elif name == "neohookean":
         sc.materials = [(n, 1 if n == "Grain" else t, p) for (n, t, p) in sc.materials]
     elif name == "border_conditions":
