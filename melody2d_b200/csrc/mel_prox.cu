@@ -202,11 +202,13 @@ __device__ __forceinline__ void neighbour_item(const mel_dev& d, const double* a
 // can occupy.  The gathered borders (hash collisions and repeated columns included) are sorted,
 // made unique and emitted with the exact overlap and shift tests of the all-pairs pass, so the
 // lists are entry for entry those of nbr_scan_all; a border whose cell range or candidate count
-// is too large takes the all-pairs pass instead.
+// is too large takes the all-pairs pass instead.  A big box is itself a query like any other: the
+// borders it can meet have their corners in the cells its extent (widened by the binned boxes'
+// largest width and height) covers, or are big themselves.
 // ---------------------------------------------------------------------------------------------
 #define PROX_THREADS_CL 256  // threads of the job kernels (PROX_THREADS below)
 #define CL_CAND 256          // gathered candidates per border (beyond: all-pairs for that border)
-#define CL_MAX_CELLS 64      // cells one border's query visits (beyond: all-pairs)
+#define CL_MAX_CELLS 4096    // cells one border's query visits (beyond: all-pairs)
 
 __device__ __forceinline__ int cl_bucket(const mel_prox_job& j, double x, double y)
 {
@@ -279,8 +281,9 @@ __device__ __forceinline__ void cl_neighbour_item(const mel_prox_job& j, int b1,
     for (int g1 = d.b_bd0[b1]; g1 < d.b_bd0[b1 + 1]; g1++) {
         const int count_before = count;
         const double xmin1 = aabb[4 * g1], xmax1 = aabb[4 * g1 + 1], ymin1 = aabb[4 * g1 + 2], ymax1 = aabb[4 * g1 + 3];
-        // boxes left out, big boxes and boxes too far out for integer cell indices: all pairs
-        bool all = !(xmin1 <= xmax1) || !(ymin1 <= ymax1) || cl_big(j, aabb + 4 * g1) ||
+        // boxes left out and boxes too far out for integer cell indices: all pairs.  A big box (a
+        // wall) queries the cells its own extent covers, which may be many
+        bool all = !(xmin1 <= xmax1) || !(ymin1 <= ymax1) ||
                    !(fabs(ymin1 - H) < 1e12 * j.cl_h && fabs(ymax1) < 1e12 * j.cl_h &&
                      fabs(xmin1 - W - d.xmin) < 1e12 * j.cl_hx && fabs(xmax1 - d.xmin) < 1e12 * j.cl_hx);
         long long cx0 = 0, cx1 = -1, cy0 = 0, cy1 = -1;
@@ -295,29 +298,54 @@ __device__ __forceinline__ void cl_neighbour_item(const mel_prox_job& j, int b1,
             // and rounding may put it across a cell edge from the shifted value tested here
             cx0--; cx1++; cy0--; cy1++;
             if (cx1 - cx0 + 1 > j.cl_ncx) cx1 = cx0 + j.cl_ncx - 1;      // every wrapped column once
-            all = (cx1 - cx0 + 1) * (cy1 - cy0 + 1) > CL_MAX_CELLS;
+            all = cx1 - cx0 + 1 > CL_MAX_CELLS || cy1 - cy0 + 1 > CL_MAX_CELLS ||
+                  (cx1 - cx0 + 1) * (cy1 - cy0 + 1) > CL_MAX_CELLS;      // each factor bounded first: no overflow
         }
         int n = 0;
         if (!all) {
-            for (long long cy = cy0; cy <= cy1; cy++)
-                for (long long cx = cx0; cx <= cx1; cx++) {
+            // the cells' bucket ranges looked up by the lanes together (one cell per lane), then
+            // their entries taken as one concatenated list, 32 at a time; the owner cell of list
+            // item t is found by a search over the per-lane offsets kept in shared memory
+            const int ncx = (int)(cx1 - cx0 + 1), ncell = ncx * (int)(cy1 - cy0 + 1);
+            int* c_off = srt;                 // [33]: list offset of each lane's cell, then the total
+            int* c_e0 = srt + 64;             // [32]: first entry of each lane's cell
+            for (int cb = 0; cb < ncell; cb += 32) {
+                const int c = cb + lane;
+                int e0 = 0, len = 0;
+                if (c < ncell) {
+                    const long long cx = cx0 + c % ncx, cy = cy0 + c / ncx;
                     const double xc = d.xmin + ((double)cx + 0.5) * j.cl_hx, yc = ((double)cy + 0.5) * j.cl_h;
                     const int bk = cl_bucket(j, xc, yc);
-                    const int e0 = j.cl_start[bk], e1 = j.cl_start[bk + 1];
-                    for (int e = e0; e < e1; e += 32) {
-                        bool ok = false;
-                        int g2 = -1;
-                        if (e + lane < e1) {
-                            g2 = j.cl_idx[e + lane];
-                            const int b2 = d.bd_body[g2];
-                            ok = b2 != b1 && !((aabb[4 * g2 + 3] < ymin1) || (ymax1 < aabb[4 * g2 + 2]));
-                        }
-                        const unsigned m = __ballot_sync(0xffffffffu, ok);
-                        const int pos = n + __popc(m & ((1u << lane) - 1u));
-                        if (ok && pos < CL_CAND) cand[pos] = g2;
-                        n += __popc(m);
-                    }
+                    e0 = j.cl_start[bk];
+                    len = j.cl_start[bk + 1] - e0;
                 }
+                int incl = len;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                c_off[lane] = incl - len;
+                c_e0[lane] = e0;
+                if (lane == 31) c_off[32] = total;
+                __syncwarp();
+                for (int tb = 0; tb < total; tb += 32) {
+                    const int t = tb + lane;
+                    bool ok = false;
+                    int g2 = -1;
+                    if (t < total) {
+                        int lo = 0, hi = 32;          // last lane whose offset is <= t
+                        while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (c_off[mid] <= t) lo = mid; else hi = mid; }
+                        g2 = j.cl_idx[c_e0[lo] + (t - c_off[lo])];
+                        ok = d.bd_body[g2] != b1 && !((aabb[4 * g2 + 3] < ymin1) || (ymax1 < aabb[4 * g2 + 2]));
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, ok);
+                    const int pos = n + __popc(m & ((1u << lane) - 1u));
+                    if (ok && pos < CL_CAND) cand[pos] = g2;
+                    n += __popc(m);
+                }
+                __syncwarp();
+            }
             // the big boxes, outside the grid
             const int nbig = j.cl_cur[j.cl_T];
             for (int e = 0; e < nbig; e += 32) {
