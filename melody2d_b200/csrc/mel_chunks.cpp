@@ -98,10 +98,13 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
         out.b_chunk0[b] = (int)out.chunks.size();
         if (d->body_type[b] != MEL_BODY_DEFORMABLE) continue;
         const int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
-        if (nnb > 4096) { mel_set_error("deformable body %d has %d nodes (pull records hold 12-bit node indices)", b, nnb); return MEL_ERR_UNSUPPORTED; }
+        if (nnb > MEL_MAX_WIDE_NODES) { mel_set_error("deformable body %d has %d nodes (16-bit node indices: at most %d)", b, nnb, MEL_MAX_WIDE_NODES); return MEL_ERR_UNSUPPORTED; }
+        // a body above MEL_MAX_BODY_NODES nodes: its FP64 pull slots name their node in a 16-bit
+        // section (the records hold 12 bits), and it never runs the mixed pipeline
+        const int wide = nnb > MEL_MAX_BODY_NODES ? 1 : 0;
         int g = d->body_gp_ptr[b];
         const int g1 = d->body_gp_ptr[b + 1];
-        const bool pipe = mixed && mel_body_entries(d, b) >= pipe_min_entries;
+        const bool pipe = mixed && !wide && mel_body_entries(d, b) >= pipe_min_entries;
         out.b_pipe[b] = pipe ? 1 : 0;
         const int gpcap = pipe ? MEL_CHUNK_GP_MX : MEL_CHUNK_GP_FP64;
         while (g < g1) {
@@ -157,7 +160,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                     pc_first.push_back((int)pcs.size());
                     for (int k = 0, at = q; k < np; k++) {
                         const int c = len / np + (k < len % np ? 1 : 0);
-                        pcs.push_back((uint32_t)at | ((uint32_t)(c - 1) << 13) | ((uint32_t)(tp[q].first >> 32) << 16));
+                        pcs.push_back((uint32_t)at | ((uint32_t)(c - 1) << 13) | ((uint32_t)(tp[q].first >> 32) << 16));   // node: 16 bits
                         at += c;
                     }
                     q = r;
@@ -231,6 +234,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
             std::vector<int> roff_all(P.roff);
             std::vector<int> rsw_all(P.rsw);
             std::vector<uint32_t> tn(ch.ntn);
+            std::vector<uint16_t> tnv(ch.ntn);
             std::vector<uint16_t> tposv(P.entries);
             int pe = 0;
             for (int s0 = 0; s0 < ch.ntn; s0 += 32) {
@@ -247,7 +251,8 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 }
                 for (int l = 0; l < m; l++) {
                     const int node = (int)(tp[tnodes[s0 + l].first].first >> 32);
-                    tn[s0 + l] = (uint32_t)node | ((uint32_t)tnodes[s0 + l].second << 12) | ((uint32_t)r0 << 20);
+                    tn[s0 + l] = (uint32_t)(node & 0xfff) | ((uint32_t)tnodes[s0 + l].second << 12) | ((uint32_t)r0 << 20);
+                    tnv[s0 + l] = (uint16_t)node;
                 }
             }
             const int nroff = (int)roff_all.size();
@@ -255,7 +260,8 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
                 mel_set_error("chunk row tables too large (%d rows)", nroff);
                 return MEL_ERR_UNSUPPORTED;
             }
-            const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn, nroff, mixed ? 8 : 16);
+            const int wsec = (wide && !mixed) ? 1 : 0;     // the mixed pipeline is off for wide bodies
+            const mel_chunk_layout L = mel_chunk_sections(ch.ngp, ch.ne, ch.ntn, nroff, mixed ? 8 : 16, wsec);
             ch.bytes = L.bytes;
             ch.img = (long long)out.img.size();
             out.img.resize(out.img.size() + L.bytes, 0);
@@ -284,6 +290,7 @@ mel_status mel_build_chunks(const mel_model_desc* d, int ecap, mel_chunk_set& ou
             }
             for (int q = 0; q < P.entries; q++) tpos[q] = tposv[q];
             memcpy(tnr, tn.data(), sizeof(uint32_t) * tn.size());
+            if (wsec) memcpy(I + L.tnode, tnv.data(), sizeof(uint16_t) * tnv.size());
             for (int r = 0; r < nroff; r++) roff[r] = (uint16_t)(roff_all[r] | (rsw_all[r] << 12));
             out.img_max = std::max(out.img_max, ch.bytes);
             out.n_entries += ch.ne;

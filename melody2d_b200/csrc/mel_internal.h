@@ -32,6 +32,11 @@
 #define MEL_WAIT_NS 1000000000ull // bound of every device-side wait (1 s)
 #define MEL_NBR_CAP_DEFAULT 64    // neighbour slots per body (grown on overflow)
 #define MEL_MAX_BODY_NODES 4096   // nodes per deformable body held in shared memory
+#define MEL_MAX_WIDE_NODES 65535  // larger bodies keep their node arrays in global memory (16-bit indices)
+// bytes of a wide body's node arrays in global memory (mel_dev::gscr): s_f, s_fc, s_upf, then the
+// post-loop arrays s_fn, s_fd, s_vp, s_ap, the six work terms and the temporary parameters
+__host__ __device__ inline long long mel_wide_pre_bytes(int n) { return 32LL * n + 8LL * ((n + 1) & ~1); }
+__host__ __device__ inline long long mel_wide_bytes(int n) { return mel_wide_pre_bytes(n) + (64LL + 48LL + 16LL) * n; }
 #define MEL_SEGB 16               // segments per segment-block box (proximity pruning)
 #define MEL_SEGB2 16              // blocks per superblock box (second pruning level)
 #define MEL_MAX_SHIFT_SPAN 64     // periods one border box may span at a proximity update
@@ -50,6 +55,7 @@ enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3,
 //   c0       ngp2 x double         weight x jacobian of each point slot (ngp2 = ngp rounded to 2)
 //   gpm      ngp4 x uint32         point slot: row table start | lane << 10 | support count << 15
 //   tn       tn4 x uint32          pull slot: node | entry count << 12 | row table start << 20
+//   tnode    ntn8 x uint16         (wide bodies only) each pull slot's node, 16 bits
 //   roff     nroff8 x uint16       row tables: the point groups' rows, then the pull groups'
 //                                  rows; each value is an offset (12 bits) | lane swizzle << 12
 // Point slots: the chunk's points sorted by (support count descending, index), cut into groups of
@@ -65,7 +71,7 @@ enum { MEL_E_BOUNDS = 0, MEL_E_NBR_OVERFLOW = 1, MEL_E_STALE = 2, MEL_E_NAN = 3,
 // Images of the mixed pass's two-buffer loop replace the pull slots by pieces: tpos lists the
 // positions of all entries in (node, point) order; the tn section holds MEL_PULL_WARPS + 1 uint16
 // warp bounds (16 bytes), then one uint32 record per piece (first listed entry | (count - 1) << 13 |
-// node << 16), a piece being at most MEL_PIECE consecutive entries of one node.  Pull warp w takes
+// node << 16, 16 bits of node), a piece being at most MEL_PIECE consecutive entries of one node.  Pull warp w takes
 // the pieces [bound w, bound w+1), which start and end at node boundaries; nroff counts the point
 // rows only.
 struct mel_chunk {        // one chunk of a body's Gauss points
@@ -77,10 +83,12 @@ struct mel_chunk {        // one chunk of a body's Gauss points
 };
 
 struct mel_chunk_layout {  // section offsets of an image
-    int dN, idx, tpos, c0, gpm, tn, roff, bytes;
+    int dN, idx, tpos, c0, gpm, tn, tnode, roff, bytes;
 };
-// dnb: bytes of one dN pair, 16 (FP64 images) or 8 (FP32 images of the mixed-precision pass)
-__host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, int ntn, int nroff, int dnb)
+// dnb: bytes of one dN pair, 16 (FP64 images) or 8 (FP32 images of the mixed-precision pass).
+// wide: the FP64 image of a body above MEL_MAX_BODY_NODES nodes, whose pull slots take their
+// node from a uint16 section tnode (ntn8 entries) after tn instead of the record's 12 bits
+__host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, int ntn, int nroff, int dnb, int wide = 0)
 {
     mel_chunk_layout L;
     L.dN = 16;
@@ -89,7 +97,8 @@ __host__ __device__ inline mel_chunk_layout mel_chunk_sections(int ngp, int ne, 
     L.c0 = L.tpos + 2 * ne;
     L.gpm = L.c0 + 8 * ((ngp + 1) & ~1);
     L.tn = L.gpm + 4 * ((ngp + 3) & ~3);
-    L.roff = L.tn + 4 * ((ntn + 3) & ~3);
+    L.tnode = L.tn + 4 * ((ntn + 3) & ~3);
+    L.roff = L.tnode + (wide ? 2 * ((ntn + 7) & ~7) : 0);
     L.bytes = L.roff + 2 * ((nroff + 7) & ~7);
     return L;
 }
@@ -110,6 +119,10 @@ struct mel_dev {
     int* b_status;           // MEL_STATUS_*; Update_status turns bodies inactive during the run
     const double* b_dist;
     const int* b_has_bc;     // body has a non-"none" border condition
+    // bodies above MEL_MAX_BODY_NODES nodes: byte offset of the body's node arrays in gscr (-1 for
+    // the others, whose node arrays live in shared memory); NULL when the model has none
+    const long long* b_gscr;
+    char* gscr;
     double *rg, *rf, *rtot, *drv, *works;
     // nodes
     const double2 *X0, *minv, *mass;
@@ -117,7 +130,7 @@ struct mel_dev {
     const int* sup_ptr; const uint16_t* sup_idx; const double* sup_N;
     // the same supports of deformable bodies laid out for the kinematics: a body's nodes as slots
     // sorted by support count (slot ranges start at multiples of 32), groups of 32 slots; slot
-    // record = node | support count << 12; entry k of lane l of group G at kg_base[G] + 32 k + l
+    // record = node | support count << 16; entry k of lane l of group G at kg_base[G] + 32 k + l
     const int* b_ks0; const unsigned* ks_rec; const int* kg_base;
     const uint16_t* ks_idx; const double* ks_N;
     double2 *o_fint, *o_fcon, *o_fneu, *o_fdir, *o_ftot;
@@ -199,9 +212,10 @@ void mel_launch_alid(const mel_dev& d, int parity, double T, int use_T, cudaStre
 void mel_launch_contact(const mel_dev& d, double law_dt_scale, cudaStream_t s);
 // Initialize_CZM's pass over the contact list (contact geometry, then the initial bonds)
 void mel_launch_czm_init(const mel_dev& d, cudaStream_t s);
-void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s);
+// nblocks: bodies b_order[0, nblocks); nwide: the wide bodies after them
+void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s, int nwide = 0);
 // one half-step of Solver_step (d.phase 1 or 2): T0 = Time, Tf = the time the forces see
-void mel_launch_body_adaptive(const mel_dev& d, double T0, double Tf, int nblocks, size_t smem, cudaStream_t s);
+void mel_launch_body_adaptive(const mel_dev& d, double T0, double Tf, int nblocks, size_t smem, cudaStream_t s, int nwide = 0);
 // Solver_step's error and mass sums over the bodies in order (Code/Solver.h:289-331): out =
 // {mean_error, max_error, total_mass, max_mass}
 void mel_launch_error_reduce(const mel_dev& d, double* out, cudaStream_t s);

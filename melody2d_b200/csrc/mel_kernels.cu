@@ -602,7 +602,7 @@ __device__ __forceinline__ void chunk_points_mx(int t, int ngp, int mtype, float
 //                          the Gauss-point pass, then s_fn, s_fd, s_vp, s_ap (n double2 each), the
 //                          six work terms per node (6 x n double) and, in the first half-step of
 //                          Solver_step, the temporary displacement parameters (n double2)
-template <bool MX, bool AD>
+template <bool MX, bool AD, bool WIDE>
 __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, char* smem)
 {
     const int tid = threadIdx.x;
@@ -610,10 +610,17 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
     const int n0 = d.b_node0[b];
     const int n = d.b_node0[b + 1] - n0;
     const double dt = d.dt[0];
-    double2* s_up = reinterpret_cast<double2*>(smem);
-    double2* s_f = s_up + n;
+    // a body above MEL_MAX_BODY_NODES nodes ("wide", its own instantiation so that the others keep
+    // plain shared-memory addressing) keeps its node arrays in global memory: it reads its
+    // displacement parameters in place and accumulates its forces in gscr; shared memory then holds
+    // only the mbarriers and the chunk images
+    constexpr bool wide = WIDE;
+    const long long go = WIDE ? d.b_gscr[b] : 0LL;
+    double2* s_up = wide ? d.up + n0 : reinterpret_cast<double2*>(smem);
+    double2* s_f = wide ? reinterpret_cast<double2*>(d.gscr + go) : s_up + n;
     double2* s_fc = s_f + n;
     float2* s_upf = reinterpret_cast<float2*>(s_fc + n);
+    char* const s_after = wide ? smem : (MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1)) : reinterpret_cast<char*>(s_fc + n));
     // the chunk loop, which leaves the internal forces in s_f and the contact forces in s_fc
     char* region;
     volatile int* s_abort;
@@ -621,8 +628,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
     // others, whose few chunks leave a three-stage pipeline mostly filling and draining
     const bool pipe = MX && d.b_pipe && d.b_pipe[b];
     if (!pipe) {
-        uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
-                                                         : reinterpret_cast<char*>(s_fc + n));
+        uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_after);
         s_abort = reinterpret_cast<volatile int*>(s_bar + 2);
         region = reinterpret_cast<char*>(s_bar) + MEL_BAR_BYTES;
         char* const buf0 = region;
@@ -630,7 +636,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         const int ch0 = d.b_chunk0[b];
         const int nch = d.b_chunk0[b + 1] - ch0;
         for (int i = tid; i < n; i += blockDim.x) {
-            s_up[i] = d.up[n0 + i];
+            if (!wide) s_up[i] = d.up[n0 + i];
             s_f[i] = make_double2(0., 0.);
             s_fc[i] = make_double2(0., 0.);
         }
@@ -671,7 +677,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
                 const bool ok = mbar_wait_bounded(&s_bar[sel], (unsigned)((k >> 1) & 1), d.wait_ns);
                 if (!ok) { atomicOr(&d.err[MEL_E_WAIT], 1u); *s_abort = 1; }
                 const int4 hdr = ok ? *reinterpret_cast<const int4*>(bk) : make_int4(0, 0, 0, 0);
-                const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16);
+                const mel_chunk_layout L = mel_chunk_sections(hdr.x, hdr.y, hdr.z, hdr.w, MX ? 8 : 16, (!MX && wide) ? 1 : 0);
                 const uint16_t* s_idx = reinterpret_cast<const uint16_t*>(bk + L.idx);
                 const uint16_t* s_tpos = reinterpret_cast<const uint16_t*>(bk + L.tpos);
                 const unsigned* s_tn = reinterpret_cast<const unsigned*>(bk + L.tn);
@@ -704,7 +710,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
                         const int pi = p0 + lane;
                         const bool v = pi < p1;
                         const unsigned rec = v ? s_pc[pi] : 0u;
-                        const int node = v ? (int)((rec >> 16) & 0xfffu) : -1;
+                        const int node = v ? (int)((rec >> 16) & 0xffffu) : -1;
                         const int q0 = (int)(rec & 0x1fffu), cnt = v ? (int)((rec >> 13) & 7u) + 1 : 0;
                         float2 c[MEL_PIECE];
 #pragma unroll
@@ -738,7 +744,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
                         const int t = (7 * i + ((i & 1) ? 6 - warp : warp)) * 32 + lane;
                         if (t >= hdr.z) continue;
                         const unsigned rec = s_tn[t];
-                        const int node = (int)(rec & 0xfffu);
+                        const int node = wide ? (int)reinterpret_cast<const uint16_t*>(bk + L.tnode)[t] : (int)(rec & 0xfffu);
                         const int cnt = (int)((rec >> 12) & 0xffu);
                         const uint16_t* prow = s_roff + (rec >> 20);
                         // rows every slot of a full group has: 32 wide and contiguous
@@ -819,8 +825,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         if (*s_abort) return;
     } else {
         constexpr int NS = MEL_STAGES(1);
-        uint64_t* s_bar = reinterpret_cast<uint64_t*>(MX ? reinterpret_cast<char*>(s_upf + ((n + 1) & ~1))
-                                                         : reinterpret_cast<char*>(s_fc + n));
+        uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_after);
         // stage s of the ring: full[s] (the bulk copy landed), pointed[s] (every point thread has
         // written its contributions), empty[s] (every pull thread is done with the buffer)
         uint64_t* full = s_bar;
@@ -1042,7 +1047,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
         __syncthreads();
         if (*s_abort) return;
     }
-    double2* s_fn = reinterpret_cast<double2*>(region);
+    double2* s_fn = reinterpret_cast<double2*>(wide ? d.gscr + go + mel_wide_pre_bytes(n) : region);
     double2* s_fd = s_fn + n;
     double2* s_vp = s_fd + n;
     double2* s_ap = s_vp + n;
@@ -1173,7 +1178,7 @@ __device__ void deformable_body(const mel_dev& d, int b, double T, double T0, ch
     const int ks = d.b_ks0[b];
     for (int i = tid - 32; i < n; i += blockDim.x - 32) {
         const unsigned rec = d.ks_rec[ks + i];
-        const int node = (int)(rec & 0xfffu), cnt = (int)(rec >> 12);
+        const int node = (int)(rec & 0xffffu), cnt = (int)(rec >> 16);
         const int* kb = d.kg_base + ((ks + i) >> 5);
         const uint16_t* kidx = d.ks_idx + *kb + lane;
         const double* kN = d.ks_N + *kb + lane;
@@ -1487,7 +1492,19 @@ __device__ __forceinline__ void body_cta(const mel_dev& d, int bb, double T, cha
     if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
     if (d.any_damped && threadIdx.x == 32) contact_work(d, b);
     if (d.b_type[b] == MEL_BODY_RIGID) rigid_body<AD>(d, b, T, T0, smem);
-    else deformable_body<MX, AD>(d, b, T, T0, smem);
+    else deformable_body<MX, AD, false>(d, b, T, T0, smem);
+}
+
+// bodies above MEL_MAX_BODY_NODES nodes, ordered last in b_order, run in a launch of their own so
+// that their global-memory variant does not weigh on the registers of the kernel every other body
+// runs
+template <bool MX, bool AD = false>
+__device__ __forceinline__ void wide_body_cta(const mel_dev& d, int bb, double T, char* smem, double T0 = 0.)
+{
+    const int b = d.b_order[bb];
+    if (d.b_status[b] == MEL_STATUS_INACTIVE) return;
+    if (d.any_damped && threadIdx.x == 32) contact_work(d, b);
+    deformable_body<MX, AD, true>(d, b, T, T0, smem);
 }
 
 __global__ void __launch_bounds__(128) contact_kernel(mel_dev d, double law_dt_scale, int czm_init)
@@ -1513,6 +1530,24 @@ __global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel_adaptive(mel_
 {
     extern __shared__ __align__(16) char smem[];
     body_cta<MX, true>(d, blockIdx.x, Tf, smem, T0);
+}
+
+// The wide bodies b_order[first + i]; the step's end time is written here when the launch above
+// had no CTA (set_time)
+template <bool MX>
+__global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel_wide(mel_dev d, int parity, int first, int set_time)
+{
+    extern __shared__ __align__(16) char smem[];
+    const double T = d.time2[parity];
+    wide_body_cta<MX>(d, first + blockIdx.x, T, smem);
+    if (set_time && blockIdx.x == 0 && threadIdx.x == 0) d.time2[parity ^ 1] = T + d.dt[0];
+}
+
+template <bool MX>
+__global__ void __launch_bounds__(MEL_BODY_THREADS, 2) body_kernel_adaptive_wide(mel_dev d, double T0, double Tf, int first)
+{
+    extern __shared__ __align__(16) char smem[];
+    wide_body_cta<MX, true>(d, first + blockIdx.x, Tf, smem, T0);
 }
 
 // Solver_step's sums over bodies in body order (Code/Solver.h:289-331)
@@ -1807,16 +1842,29 @@ void mel_launch_batch_step(const mel_dev* devs, const int* thr0, int nthr, const
     mel::advance_kernel<<<(nsamp + 127) / 128, 128, 0, s>>>(devs, nsamp);
 }
 
-void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s)
+void mel_launch_body(const mel_dev& d, int parity, int nblocks, size_t smem, cudaStream_t s, int nwide)
 {
-    if (d.precision == MEL_PREC_MIXED) mel::body_kernel<true><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
-    else mel::body_kernel<false><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
+    if (nblocks > 0) {
+        if (d.precision == MEL_PREC_MIXED) mel::body_kernel<true><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
+        else mel::body_kernel<false><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, parity);
+    }
+    if (nwide > 0) {
+        const int set_time = nblocks > 0 ? 0 : 1;
+        if (d.precision == MEL_PREC_MIXED) mel::body_kernel_wide<true><<<nwide, MEL_BODY_THREADS, smem, s>>>(d, parity, nblocks, set_time);
+        else mel::body_kernel_wide<false><<<nwide, MEL_BODY_THREADS, smem, s>>>(d, parity, nblocks, set_time);
+    }
 }
 
-void mel_launch_body_adaptive(const mel_dev& d, double T0, double Tf, int nblocks, size_t smem, cudaStream_t s)
+void mel_launch_body_adaptive(const mel_dev& d, double T0, double Tf, int nblocks, size_t smem, cudaStream_t s, int nwide)
 {
-    if (d.precision == MEL_PREC_MIXED) mel::body_kernel_adaptive<true><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf);
-    else mel::body_kernel_adaptive<false><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf);
+    if (nblocks > 0) {
+        if (d.precision == MEL_PREC_MIXED) mel::body_kernel_adaptive<true><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf);
+        else mel::body_kernel_adaptive<false><<<nblocks, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf);
+    }
+    if (nwide > 0) {
+        if (d.precision == MEL_PREC_MIXED) mel::body_kernel_adaptive_wide<true><<<nwide, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf, nblocks);
+        else mel::body_kernel_adaptive_wide<false><<<nwide, MEL_BODY_THREADS, smem, s>>>(d, T0, Tf, nblocks);
+    }
 }
 
 void mel_launch_error_reduce(const mel_dev& d, double* out, cudaStream_t s)
@@ -1879,7 +1927,11 @@ int mel_body_kernel_configure(size_t smem)
         cudaFuncSetAttribute(mel::body_kernel_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
         cudaFuncSetAttribute(mel::body_kernel_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
         cudaFuncSetAttribute(mel::body_kernel_adaptive<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(mel::body_kernel_adaptive<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaFuncSetAttribute(mel::body_kernel_adaptive<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_wide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_wide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_adaptive_wide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(mel::body_kernel_adaptive_wide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         mel_set_cuda_error(cudaGetLastError(), "cudaFuncSetAttribute(body_kernel)", __FILE__, __LINE__);
         return MEL_ERR_CUDA;
     }

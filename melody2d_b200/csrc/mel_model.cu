@@ -68,7 +68,8 @@ struct mel_handle {
     int flags[MEL_NFLAGS] = { 0 };
     int parity = 0;
     size_t body_smem = 0;
-    int nblocks_body = 0;
+    int nblocks_body = 0;     // body-kernel CTAs, and the wide bodies' CTAs after them
+    int nwide = 0;
     int chunk_cap = 0;          // support entries per chunk chosen at build time
     int body_stages = 2;        // image buffers per CTA (3 when a body runs the mixed pipeline)
     double img_bytes = 0.;      // bytes of all chunk images
@@ -225,8 +226,8 @@ static mel_status validate(const mel_model_desc* d)
     }
     for (int b = 0; b < d->n_bodies; b++) {
         int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
-        if (d->body_type[b] == MEL_BODY_DEFORMABLE && nnb > MEL_MAX_BODY_NODES) {
-            mel_set_error("deformable body %d has %d nodes; this build holds at most %d nodes of a body in shared memory", b, nnb, MEL_MAX_BODY_NODES);
+        if (d->body_type[b] == MEL_BODY_DEFORMABLE && nnb > MEL_MAX_WIDE_NODES) {
+            mel_set_error("deformable body %d has %d nodes; this build indexes at most %d nodes of a body (16 bits)", b, nnb, MEL_MAX_WIDE_NODES);
             return MEL_ERR_UNSUPPORTED;
         }
         if (d->body_material[b] < 0 || d->body_material[b] >= d->n_materials) { mel_set_error("body %d material out of range", b); return MEL_ERR_INVALID; }
@@ -364,11 +365,16 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     for (int g = 0; g < nbd; g++)
         if (d->border_bc_type[2 * g] != MEL_BC_NONE || d->border_bc_type[2 * g + 1] != MEL_BC_NONE) has_bc[d->border_body[g]] = 1;
     D.b_has_bc = dupload(h, has_bc);
+    // CTA order of the body kernel: rigid bodies, deformable bodies, then the deformable bodies above
+    // MEL_MAX_BODY_NODES nodes, which run in a launch of their own (body_kernel_wide)
     std::vector<int> order;
+    auto is_wide = [&](int b) { return d->body_type[b] != MEL_BODY_RIGID && d->body_node_ptr[b + 1] - d->body_node_ptr[b] > MEL_MAX_BODY_NODES; };
     for (int b = 0; b < nb; b++) if (d->body_type[b] == MEL_BODY_RIGID) order.push_back(b);
-    for (int b = 0; b < nb; b++) if (d->body_type[b] != MEL_BODY_RIGID) order.push_back(b);
+    for (int b = 0; b < nb; b++) if (d->body_type[b] != MEL_BODY_RIGID && !is_wide(b)) order.push_back(b);
+    h->nwide = 0;
+    for (int b = 0; b < nb; b++) if (is_wide(b)) { order.push_back(b); h->nwide++; }
     D.b_order = dupload(h, order);
-    h->nblocks_body = nb;
+    h->nblocks_body = nb - h->nwide;
     // rigid state: file masses first (the first Update_proximity precedes Update_material,
     // Code/main.cpp:112-123); Update_material masses kept for later
     h->rg_file.assign(d->rigid, d->rigid + (size_t)nb * MEL_RIGID_NF);
@@ -589,8 +595,8 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
                 kN.resize(base + 32 * (size_t)K, 0.);
                 for (int l = 0; l < m; l++) {
                     const int i = order[s0 + l];
-                    if (cnt(i) > 0xfffff) { mel_set_error("node %d has %d supports", b0 + i, cnt(i)); return MEL_ERR_UNSUPPORTED; }
-                    rec.push_back((unsigned)i | ((unsigned)cnt(i) << 12));
+                    if (cnt(i) > 0xffff) { mel_set_error("node %d has %d supports", b0 + i, cnt(i)); return MEL_ERR_UNSUPPORTED; }
+                    rec.push_back((unsigned)i | ((unsigned)cnt(i) << 16));
                     for (int k = 0, j = d->node_sup_ptr[b0 + i]; k < cnt(i); k++, j++) {
                         kidx[base + 32 * (size_t)k + l] = sidx[j];
                         kN[base + 32 * (size_t)k + l] = d->node_sup_N[j];
@@ -669,9 +675,32 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     // Gauss points: chunk images of <= gpcap points (one point thread each) and <= ecap support
     // entries.  The entry cap is the largest that lets two body CTAs, each with its ring of
     // MEL_STAGES images, share an SM; a body too large for that runs one CTA per SM.
-    int max_def_nodes = 1;
+    // Bodies above MEL_MAX_BODY_NODES nodes keep their node arrays in global memory (gscr), so
+    // shared memory is sized by the others (max_def_nodes); max_all_nodes bounds the touched nodes
+    // of a chunk.
+    int max_def_nodes = 1, max_all_nodes = 1;
+    bool any_wide = false;
     for (int b = 0; b < nb; b++)
-        if (d->body_type[b] == MEL_BODY_DEFORMABLE) max_def_nodes = std::max(max_def_nodes, d->body_node_ptr[b + 1] - d->body_node_ptr[b]);
+        if (d->body_type[b] == MEL_BODY_DEFORMABLE) {
+            const int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+            max_all_nodes = std::max(max_all_nodes, nnb);
+            if (nnb > MEL_MAX_BODY_NODES) any_wide = true;
+            else max_def_nodes = std::max(max_def_nodes, nnb);
+        }
+    if (any_wide) {
+        // per wide body: s_f, s_fc (16 B per node), s_upf (8 B, mixed), then the post-loop arrays
+        // s_fn, s_fd, s_vp, s_ap (16 B), six work terms (48 B) and the temporary parameters (16 B)
+        std::vector<long long> off(nb, -1);
+        long long tot = 0;
+        for (int b = 0; b < nb; b++) {
+            const int nnb = d->body_node_ptr[b + 1] - d->body_node_ptr[b];
+            if (d->body_type[b] != MEL_BODY_DEFORMABLE || nnb <= MEL_MAX_BODY_NODES) continue;
+            off[b] = tot;
+            tot += ((long long)mel_wide_bytes(nnb) + 255) & ~255LL;
+        }
+        D.b_gscr = dupload(h, off);
+        D.gscr = reinterpret_cast<char*>(dalloc<double>(h, (size_t)(tot / 8) + 32));
+    }
     mel_chunk_set CS;
     long long pipe_min = 0;
     int smem_sm = 0, smem_blk = 0, smem_res = 0;
@@ -725,7 +754,8 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
             // pull records: touched-node slots, or (mixed two-buffer loop) the segmented list
             // pull records: touched-node slots, or (mixed two-buffer loop) the warp bounds and at most
             // one piece per touched node plus one per MEL_PIECE entries
-            const int tn_words = std::max(std::min(ne, max_def_nodes), mixed ? 5 + std::min(ne, max_def_nodes) + ne / MEL_PIECE : 0);
+            int tn_words = std::max(std::min(ne, max_all_nodes), mixed ? 5 + std::min(ne, max_all_nodes) + ne / MEL_PIECE : 0);
+            if (any_wide && !mixed) tn_words += (tn_words + 1) / 2 + 4;     // the 16-bit node section of wide bodies
             return mel_chunk_sections(gpcap, ne, tn_words, std::min(1023, groups * max_ns) + pull_rows, mixed ? 8 : 16).bytes;
         };
         int chosen = -1;
@@ -1066,15 +1096,15 @@ static mel_status adaptive_step(mel_handle* h)
         mel_launch_damping(d, h->stream);
         mel_launch_alid(d, 0, h->time, 1, h->stream);            // Update_alid_forces(Time)
         d.phase = 1;
-        mel_launch_body_adaptive(d, h->time, h->t_bc, h->nblocks_body, h->body_smem, h->stream);
+        mel_launch_body_adaptive(d, h->time, h->t_bc, h->nblocks_body, h->body_smem, h->stream, h->nwide);
         mel_launch_contact(d, 0.5, h->stream);
         mel_launch_damping(d, h->stream);
         mel_launch_alid(d, 0, h->time + h->dt * 0.5, 1, h->stream);   // Update_alid_forces(Time+Deltat*0.5)
         d.phase = 2;
-        mel_launch_body_adaptive(d, h->time, h->time + h->dt * 0.5, h->nblocks_body, h->body_smem, h->stream);
+        mel_launch_body_adaptive(d, h->time, h->time + h->dt * 0.5, h->nblocks_body, h->body_smem, h->stream, h->nwide);
         h->t_bc = h->time + h->dt;                              // Update_bc(Time+Deltat) of the second half
         mel_launch_error_reduce(d, h->d_red, h->stream);
-        h->launches += 5 + (h->d.fdamp ? 2 : 0) + (h->d.falid ? 2 : 0);
+        h->launches += 5 + (h->d.fdamp ? 2 : 0) + (h->d.falid ? 2 : 0) + (h->nwide && h->nblocks_body ? 2 : 0);
         MEL_CUDA_OK(cudaGetLastError());
         MEL_CUDA_OK(cudaMemcpyAsync(h->h_red, h->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         MEL_CUDA_OK(cudaStreamSynchronize(h->stream));
@@ -1284,7 +1314,8 @@ mel_status mel_step(mel_handle* h, mel_step_io* io)
             mark(); kinds.push_back(0);
             if (h->d.fdamp) { mel_launch_damping(h->d, h->stream); h->launches++; }
             if (h->d.falid) { mel_launch_alid(h->d, h->parity, 0., 0, h->stream); h->launches++; }
-            mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream);
+            mel_launch_body(h->d, h->parity, h->nblocks_body, h->body_smem, h->stream, h->nwide);
+            if (h->nwide && h->nblocks_body) h->launches++;
             mark(); kinds.push_back(1);
             {
                 cudaError_t le = cudaGetLastError();
@@ -2126,7 +2157,7 @@ mel_status mel_get_kernel_config(mel_handle* h, int* chunk_cap, long long* body_
     if (!h) return MEL_ERR_INVALID;
     if (chunk_cap) *chunk_cap = h->chunk_cap;
     if (body_smem) *body_smem = (long long)h->body_smem;
-    if (body_ctas) *body_ctas = h->nblocks_body;
+    if (body_ctas) *body_ctas = h->nblocks_body + h->nwide;
     return MEL_OK;
 }
 
@@ -2272,7 +2303,10 @@ mel_status mel_batch_create(int device, int precision, mel_batch** out)
 mel_status mel_batch_admit(mel_batch* b, mel_handle* h)
 {
     if (h && h->solver != MEL_SOLVER_EULER) { mel_set_error("batches advance the Euler scheme; step Solver_step schemes with mel_step"); return MEL_ERR_UNSUPPORTED; }
-    if (h && (h->d.fdamp || h->d.falid || h->n_deact)) { mel_set_error("models with damping matrices, ALID layers or DEACTIVATION entries are stepped with mel_step, not in a batch"); return MEL_ERR_UNSUPPORTED; }
+    if (h && (h->d.fdamp || h->d.falid || h->n_deact || h->d.b_gscr)) {
+        mel_set_error("models with damping matrices, ALID layers, DEACTIVATION entries or deformable bodies above %d nodes are stepped with mel_step, not in a batch", MEL_MAX_BODY_NODES);
+        return MEL_ERR_UNSUPPORTED;
+    }
     if (!b || !h) return MEL_ERR_INVALID;
     if (h->batch) { mel_set_error("the handle is already a member of a batch"); return MEL_ERR_INVALID; }
     if (h->device != b->device || h->precision != b->precision) {

@@ -46,7 +46,8 @@ extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const dou
             int hdr[4];
             memcpy(hdr, buf.data(), sizeof hdr);
             if (hdr[0] > MEL_CHUNK_GP_FP64 || hdr[1] % 8 || hdr[1] > ecap || hdr[3] > 1024) return 2;
-            const mel_chunk_layout L = mel_chunk_sections(hdr[0], hdr[1], hdr[2], hdr[3], 16);
+            const int wide = n > MEL_MAX_BODY_NODES ? 1 : 0;
+            const mel_chunk_layout L = mel_chunk_sections(hdr[0], hdr[1], hdr[2], hdr[3], 16, wide);
             if (L.bytes != c.bytes) return 3;
             double* sp = reinterpret_cast<double*>(buf.data() + L.dN);
             const uint16_t* sidx = reinterpret_cast<const uint16_t*>(buf.data() + L.idx);
@@ -91,9 +92,11 @@ extern "C" int emul_internal_forces(const mel_model_desc* d, int ecap, const dou
                     sp[2 * E(k) + 1] = c0 * (dy * S22 + dx * S12);
                 }
             }
+            const uint16_t* stnode = reinterpret_cast<const uint16_t*>(buf.data() + L.tnode);
             for (int t = 0; t < hdr[2]; t++) {
                 const uint32_t rec = stn[t];
-                const int node = (int)(rec & 0xfffu), cnt = (int)((rec >> 12) & 0xffu), pr = (int)(rec >> 20);
+                const int node = wide ? (int)stnode[t] : (int)(rec & 0xfffu), cnt = (int)((rec >> 12) & 0xffu), pr = (int)(rec >> 20);
+                if (wide && (int)(rec & 0xfffu) != (node & 0xfff)) return 12;
                 const int lane = t & 31;
                 if (node >= n || cnt == 0 || pr + cnt > hdr[3]) return 7;
                 // counts descend within a group, so slots with more than j entries are a prefix
@@ -188,7 +191,7 @@ extern "C" int emul_segmented_pull(const mel_model_desc* d, int ecap, const doub
                 int share = 0;
                 for (int pi = a; pi < e1; pi++) {
                     const uint32_t rec = spc[pi];
-                    const int q0 = (int)(rec & 0x1fffu), cnt = (int)((rec >> 13) & 7u) + 1, node = (int)((rec >> 16) & 0xfffu);
+                    const int q0 = (int)(rec & 0x1fffu), cnt = (int)((rec >> 13) & 7u) + 1, node = (int)((rec >> 16) & 0xffffu);
                     if (q0 != nl || cnt > MEL_PIECE || node >= n) return 28;
                     if (node < prev_node) return 31;                           // sorted by node
                     if (node == prev_node && w != prev_warp) return 33;        // a node within one warp

@@ -73,3 +73,56 @@ def test_segmented_pull_layout(emul, ecap):
     scale = np.abs(f_direct).max()
     assert scale > 0
     np.testing.assert_allclose(f_list, f_direct, rtol=0, atol=1e-12 * scale)
+
+
+def wide_scene():
+    """Two discs of 4,360 nodes each (above the 4,096 a body's shared memory holds) between plates
+    and walls: their images carry the 16-bit node section."""
+    from melody2d_b200 import generator as g
+    return g.biaxial_scene(seed=3, n_discs=2, n_border=160, n_interior=4200, workers=1)
+
+
+def test_chunk_pass_wide_bodies_match_oracle(emul, oracle_built):
+    """The FP64 images of bodies above 4,096 nodes name each pull slot's node in a 16-bit section;
+    the CPU model of the kernel's chunk pass reproduces the oracle's internal forces bit for bit."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.abi import Desc
+    from oracle.pyoracle import Oracle
+    flat = g.flatten(wide_scene())
+    assert np.diff(flat["body_node_ptr"]).max() > 4096
+    o = Oracle(flat)
+    # a seeded field of displacement parameters (the sample is barely loaded after a few steps)
+    st = o.node_state()
+    deform = np.repeat(np.asarray(flat["body_type"]) == 0, np.diff(flat["body_node_ptr"]))
+    st[deform, 6:8] = np.random.default_rng(8).standard_normal((int(deform.sum()), 2)) * 1e-7
+    o.set_node_state(st)
+    up = np.ascontiguousarray(st[:, 6:8]).copy()
+    o.step(1, proximity=False)
+    ref = o.forces()["internal"]
+    desc = Desc(flat)
+    f = np.zeros_like(up)
+    stats = np.zeros(4, dtype=np.int64)
+    rc = emul.emul_internal_forces(C.byref(desc.desc), 2048, up.ctypes.data, f.ctypes.data, stats.ctypes.data)
+    assert rc == 0, (rc, emul.emul_error())
+    np.testing.assert_array_equal(f, ref)
+    assert np.abs(ref).max() > 0
+
+
+def test_segmented_pull_wide_bodies(emul):
+    """Mixed images of bodies above 4,096 nodes: pieces carry 16-bit nodes."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.abi import Desc
+    flat = g.flatten(wide_scene())
+    desc = Desc(flat)
+    rng = np.random.default_rng(6)
+    up = rng.standard_normal((len(flat["node_x0"]) // 2, 2)) * 1e-5
+    f_list = np.zeros_like(up)
+    f_direct = np.zeros_like(up)
+    stats = np.zeros(4, dtype=np.int64)
+    emul.emul_segmented_pull.restype = C.c_int
+    emul.emul_segmented_pull.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rc = emul.emul_segmented_pull(C.byref(desc.desc), 3328, up.ctypes.data, f_list.ctypes.data,
+                                  f_direct.ctypes.data, stats.ctypes.data)
+    assert rc == 0, (rc, emul.emul_error())
+    scale = np.abs(f_direct).max()
+    np.testing.assert_allclose(f_list, f_direct, rtol=0, atol=1e-12 * scale)
