@@ -117,6 +117,7 @@ struct mel_dev {
     // bodies
     const int *b_type, *b_mat, *b_per, *b_node0, *b_bd0, *b_chunk0, *b_order;
     int* b_status;           // MEL_STATUS_*; Update_status turns bodies inactive during the run
+    double* b_damage;        // Body::damage: the running value of Update_damage (starts at 0)
     const double* b_dist;
     const int* b_has_bc;     // body has a non-"none" border condition
     // bodies above MEL_MAX_BODY_NODES nodes: byte offset of the body's node arrays in gscr (-1 for

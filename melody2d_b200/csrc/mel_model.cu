@@ -324,6 +324,8 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
     D.b_mat = dupload(h, d->body_material, nb);
     D.b_per = dupload(h, d->body_periodic, nb);
     D.b_status = dupload(h, d->body_status, nb);
+    D.b_damage = dalloc<double>(h, nb);
+    MEL_CUDA_OK(cudaMemset(D.b_damage, 0, sizeof(double) * (size_t)nb));
     // DEACTIVATION entries that Update_status compares (Code/Proximity.h:550-1007), checked against
     // the model: the reference indexes its arrays with them unchecked
     if (d->n_deactivated > 0) {
@@ -333,9 +335,11 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
         for (int i = 0; i < d->n_deactivated; i++) {
             const double* e = d->deactivated + (size_t)MEL_DEACT_NF * i;
             const int type = (int)e[0];
-            if (type == 8) {
-                mel_set_error("DEACTIVATION entry %d compares a body's damage, which needs Body::Update_damage (not run by this library)", i);
-                return MEL_ERR_UNSUPPORTED;
+            if (type == 8) {                                        // Damage: {8, body, mode, threshold}
+                const int body = (int)e[1];
+                if (body < 0 || body >= nb) { mel_set_error("DEACTIVATION entry %d: body out of range", i); return MEL_ERR_INVALID; }
+                keep.insert(keep.end(), e, e + MEL_DEACT_NF);
+                continue;
             }
             if (type < 0 || type > 4) continue;                    // Update_status has no branch for it
             const int body = (int)(type <= 3 ? e[2] : e[3]), node = (int)(type <= 3 ? e[3] : e[4]);
@@ -1749,11 +1753,14 @@ mel_status mel_monitor_setup(mel_handle* h, const double* monitored, int n_monit
             }
             if (o.node >= 0 || h->b_type[o.body] == MEL_BODY_DEFORMABLE) forces = true;
             if (o.kind >= 0 && o.kind <= 3) row++;
-        } else if (o.type == 5 || o.type == 6 || o.type == 8) {
-            mel_set_error("monitored entry %d: type %d (%s) needs %s, which this library does not run", i, o.type,
-                          o.type == 5 ? "Jacobian" : o.type == 6 ? "Stress" : "Damage",
-                          o.type == 8 ? "Body::Update_damage" : "the nodal stress post-processing (Code/Body.h:2310-2519)");
+        } else if (o.type == 5 || o.type == 6) {
+            mel_set_error("monitored entry %d: type %d (%s) needs the nodal stress post-processing (Code/Body.h:2310-2519), "
+                          "which this library does not run", i, o.type, o.type == 5 ? "Jacobian" : "Stress");
             return MEL_ERR_UNSUPPORTED;
+        } else if (o.type == 8) {
+            o.body = (int)e[1];                          // Damage: Update_damage of the body
+            if (!body_ok(o.body)) return bad("body out of range");
+            row++;
         } else if (o.type == 7) {
             o.kind = (int)e[1]; o.body = (int)e[2]; o.border = (int)e[3]; o.bnode = (int)e[4];
             if (!body_ok(o.body)) return bad("body out of range");

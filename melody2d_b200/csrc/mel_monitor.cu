@@ -85,6 +85,34 @@ __device__ double2 node_force(const mel_dev& d, int b, int i, int s)
     }
 }
 
+// Body::Update_damage (Code/Body.h:2667-2700) of body b: per border node the smallest internal[0]
+// of the body's contact elements on that node that carry internal variables (1 when none does),
+// averaged over the border nodes in border order, never below the body's previous value, which it
+// replaces (d.b_damage); one thread
+__device__ double body_damage(const mel_dev& d, int b)
+{
+    double total_nodes = 0., dmg = 0.;
+    const double previous = d.b_damage[b];
+    const int c0 = d.b_cont0[b], c1 = d.b_cont0[b + 1];
+    for (int g = d.b_bd0[b]; g < d.b_bd0[b + 1]; g++) {
+        const int i = g - d.b_bd0[b];
+        const int nbn = d.bd_e0[g + 1] - d.bd_e0[g];
+        total_nodes += nbn;
+        for (int j = 0; j < nbn; j++) {
+            double v = 1.;
+            for (int k = c0; k < c1; k++) {
+                const mel_contact& c = d.cont[k];
+                if (c.borderS == i && c.border_nodeS == j && c.nb_internal > 0 && c.internal[0] < v) v = c.internal[0];
+            }
+            dmg += v;
+        }
+    }
+    dmg = dmg / total_nodes;
+    if (dmg < previous) dmg = previous;
+    d.b_damage[b] = dmg;
+    return dmg;
+}
+
 // one row of Monitoring (Code/Monitoring.h:8-559) into row[1..], its length into row[0]
 __global__ void mon_row_kernel(mel_dev d, const mel_mon_op* ops, int nops, int energy, int boundaries,
                                const double* part, double* row, mel_mon_head hd)
@@ -165,6 +193,9 @@ __global__ void mon_row_kernel(mel_dev d, const mel_mon_op* ops, int nops, int e
                     break;
                 }
             }
+        } else if (o.type == 8) {
+            // Damage (Monitoring.h:385-390): Update_damage of the body, then its damage
+            row[c++] = body_damage(d, o.body);
         } else if (o.type == 9) {
             // Energy (Monitoring.h:390-458); the elastic energy of both material laws is zero
             // (Code/Model.h:19-73 set energy = 0), so Deformation entries read +0
@@ -226,6 +257,22 @@ __global__ void mon_row_kernel(mel_dev d, const mel_mon_op* ops, int nops, int e
 // Update_status (Code/Proximity.h:550-1007), one thread, entries in order.  e = the entry (type,
 // then the fields Read_spy_line stores, the comparison 0 below / 1 equal / 2 above, the threshold).
 // x, y, r carry over between entries of one call as in the reference (they start at 0 each call).
+// sets a body inactive.  The reference stops clearing the send list of an inactive body but goes
+// on sending it (Code/Solver.h:37-61: Initialize_contact_forces skipped, Send_contact_forces not),
+// so a body switched off while one of its contact elements carries a force keeps pushing that force
+// onto its masters for the rest of the run; that is reported rather than reproduced
+__device__ void deactivate(const mel_dev& d, int body)
+{
+    if (d.b_status[body] != MEL_STATUS_INACTIVE) {
+        for (int j = d.b_cont0[body]; j < d.b_cont0[body + 1]; j++)
+            if (d.cont[j].bodyM != body && (d.cont[j].fx != 0. || d.cont[j].fy != 0.)) {
+                atomicCAS(d.err + MEL_E_DEACT, 0u, (unsigned)body + 1u);
+                break;
+            }
+    }
+    d.b_status[body] = MEL_STATUS_INACTIVE;
+}
+
 __global__ void status_kernel(mel_dev d, const double* entries, int n)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -286,6 +333,13 @@ __global__ void status_kernel(mel_dev d, const double* entries, int n)
                 if (fk == 0) { x = d.rtot[3 * body]; y = d.rtot[3 * body + 1]; r = d.rtot[3 * body + 2]; }
                 else if (fk >= 2 && fk <= 6) { const int q = 3 * (fk - 2); x = rf[q]; y = rf[q + 1]; r = rf[q + 2]; }
             }
+        } else if (type == 8) {
+            // Damage (Code/Proximity.h:988-998): e = {8, body, mode, threshold}
+            body = (int)e[1];
+            mode = (int)e[2]; thr = e[3];
+            const double dm = body_damage(d, body);
+            if ((mode == 0 && dm <= thr) || (mode == 1 && dm == thr) || (mode == 2 && dm >= thr)) deactivate(d, body);
+            continue;
         } else {
             continue;
         }
@@ -295,21 +349,7 @@ __global__ void status_kernel(mel_dev d, const double* entries, int n)
         else if (kind == 2) v = type == 0 ? r : sqrt(x * x + y * y);    // pow(.,0.5): both correctly rounded
         else if (kind == 3 && type != 0) v = r;
         else continue;                                                 // no comparison in the reference
-        if ((mode == 0 && v <= thr) || (mode == 1 && v == thr) || (mode == 2 && v >= thr)) {
-            if (d.b_status[body] != MEL_STATUS_INACTIVE) {
-                // the reference stops clearing the send list of an inactive body but goes on
-                // sending it (Code/Solver.h:37-61: Initialize_contact_forces skipped,
-                // Send_contact_forces not), so a body switched off while one of its contact
-                // elements carries a force keeps pushing that force onto its masters for the rest
-                // of the run; that is reported rather than reproduced
-                for (int j = d.b_cont0[body]; j < d.b_cont0[body + 1]; j++)
-                    if (d.cont[j].bodyM != body && (d.cont[j].fx != 0. || d.cont[j].fy != 0.)) {
-                        atomicCAS(d.err + MEL_E_DEACT, 0u, (unsigned)body + 1u);
-                        break;
-                    }
-            }
-            d.b_status[body] = MEL_STATUS_INACTIVE;
-        }
+        if ((mode == 0 && v <= thr) || (mode == 1 && v == thr) || (mode == 2 && v >= thr)) deactivate(d, body);
     }
 }
 

@@ -517,6 +517,11 @@ def deactivation_vector(line: str) -> List[float]:
     Read_spy_line encodes it (position, displacement, velocity, acceleration or force entries), then
     0 / 1 / 2 for below / equal / above and the threshold, zero-padded to 8 values."""
     t = line.split()
+    if t[0] == "Damage":                      # Read_spy_line: {8, body} (Code/IO.h:454-458)
+        v = [8.0, float(t[1])]
+        rest = t[2:]
+        v += [float(["below", "equal", "above"].index(rest[0])), float(rest[1])]
+        return v + [0.0] * (8 - len(v))
     if t[0] == "Force":
         v = [4.0, float(["X", "Y", "Mag", "R"].index(t[1])), float(_FORCE_KINDS.index(t[2])), float(t[3]), float(t[4])]
         rest = t[5:]

@@ -71,6 +71,8 @@ struct orc_model {
     int* cells;
     int nmx; int* mx_ptr; int* mx_dofs; double *mx_k, *mx_c;
     int* alid_ptr; double *alid_t, *alid_v, *alid_ab;   /* ALID histories and nodal alpha, beta (or NULL) */
+    double* damage;       /* [nb] Body::damage, the running value of Update_damage */
+    int dmg_bodies[16], dmg_n, dmg_count, dmg_cap; double* dmg_log;   /* Monitoring's Damage entries (tests) */
     /* dynamic lists */
     cvec* cont; nbr_t** nbl; int* nbn; int* nbc; svec* send;
     /* Solver_step storage (Body::Store/Restore, Body.h:2601-2659) */
@@ -1806,6 +1808,35 @@ static void node_force(const orc_model* m, int i, int k, double* fx, double* fy)
     *fx = a[k][2 * i]; *fy = a[k][2 * i + 1];
 }
 
+/* Body::Update_damage (Code/Body.h:2667-2700): per border node the smallest internal[0] of the
+ * body's contact elements on that node that carry internal variables (1 when none does), averaged
+ * over the border nodes, and never below the previous value */
+static double update_damage(orc_model* m, int b)
+{
+    double total_nodes = 0., dmg = 0.;
+    const double previous = m->damage[b];
+    const cvec* cv = &m->cont[b];
+    for (int i = 0; i < m->bptr[b + 1] - m->bptr[b]; i++) {
+        const int g = m->bptr[b] + i;
+        const int nbn = m->bd_ptr[g + 1] - m->bd_ptr[g];
+        total_nodes += nbn;
+        for (int j = 0; j < nbn; j++) {
+            double d = 1.;
+            for (int k = 0; k < cv->n; k++) {
+                const mel_contact* c = &cv->a[k];
+                if (c->borderS == i && c->border_nodeS == j && c->nb_internal > 0 && c->internal[0] < d) d = c->internal[0];
+            }
+            dmg += d;
+        }
+    }
+    dmg = dmg / total_nodes;
+    if (dmg < previous) dmg = previous;
+    m->damage[b] = dmg;
+    return dmg;
+}
+void orc_get_damage(orc_model* m, double* out) { memcpy(out, m->damage, sizeof(double) * m->nb); }
+double orc_update_damage(orc_model* m, int b) { return update_damage(m, b); }
+
 /* Update_status (Code/Proximity.h:550-1007): entries of type position, displacement, velocity,
  * acceleration (e = {type, kind, body, node, mode, threshold}) and force (e = {4, kind, force kind,
  * body, node, mode, threshold}); x, y, r start at 0 and carry over between entries */
@@ -1858,6 +1889,14 @@ static void update_status(orc_model* m)
                 if (fk == 0) { x = m->rtot[3 * body]; y = m->rtot[3 * body + 1]; r = m->rtot[3 * body + 2]; }
                 else if (fk >= 2 && fk <= 6) { const int q = 3 * (fk - 2); x = rf[q]; y = rf[q + 1]; r = rf[q + 2]; }
             }
+        } else if (type == 8) {
+            /* Damage (e = {8, body, mode, threshold}), Code/Proximity.h:988-998 */
+            body = (int)e[1];
+            mode = (int)e[2]; thr = e[3];
+            const double dm = update_damage(m, body);
+            if ((mode == 0 && dm <= thr) || (mode == 1 && dm == thr) || (mode == 2 && dm >= thr))
+                m->bstatus[body] = MEL_STATUS_INACTIVE;
+            continue;
         } else continue;
         double v;
         if (kind == 0) v = x;
@@ -1870,11 +1909,32 @@ static void update_status(orc_model* m)
     }
 }
 
+/* Damage entries of Monitoring (Code/Monitoring.h:385-390): after every step, before its proximity
+ * update (Code/main.cpp:173-196), Update_damage of the listed bodies, logged in order */
+void orc_monitor_damage(orc_model* m, const int* bodies, int n, int cap)
+{
+    m->dmg_n = n < 16 ? (n > 0 ? n : 0) : 16;
+    for (int i = 0; i < m->dmg_n; i++) m->dmg_bodies[i] = (bodies[i] >= 0 && bodies[i] < m->nb) ? bodies[i] : 0;
+    free(m->dmg_log);
+    m->dmg_log = NEWD((size_t)(cap > 0 ? cap : 1) * (m->dmg_n > 0 ? m->dmg_n : 1));
+    m->dmg_cap = cap;
+    m->dmg_count = 0;
+}
+int orc_damage_log(orc_model* m, double* out)
+{
+    if (out && m->dmg_log) memcpy(out, m->dmg_log, sizeof(double) * (size_t)m->dmg_count * m->dmg_n);
+    return m->dmg_count;
+}
+
 int orc_step(orc_model* m, int nsteps, int run_proximity)
 {
     for (int s = 0; s < nsteps; s++) {
         if (m->solver == MEL_SOLVER_EULER) euler_step(m);
         else solver_step(m);
+        if (m->dmg_n > 0 && m->dmg_count < m->dmg_cap) {
+            for (int i = 0; i < m->dmg_n; i++) m->dmg_log[(size_t)m->dmg_count * m->dmg_n + i] = update_damage(m, m->dmg_bodies[i]);
+            m->dmg_count++;
+        }
         if (run_proximity && m->time > m->next_cup - 1.e-6 * m->dt) {
             m->next_cup = m->next_cup + m->cup;
             orc_update_proximity(m);
@@ -1911,7 +1971,7 @@ int orc_create(const mel_model_desc* d, const int* n_regions, orc_model** out)
     m->rg = dupd(d->rigid, (size_t)nb * MEL_RIGID_NF);
     m->rg_tmp = NEWD(6 * nb); m->rf = NEWD(15 * nb); m->rtot = NEWD(3 * nb); m->drv = NEWD(8 * nb); m->works = NEWD(7 * nb);
     m->terr = NEWD(nb); m->merr = NEWD(nb); m->nmerr = NEWI(nb); m->bfms = NEWD(nb); m->bdfms = NEWD(nb); m->bmms = NEWD(nb);
-    m->bmaxfms = NEWD(nb); m->eenergy = NEWD(nb);
+    m->bmaxfms = NEWD(nb); m->eenergy = NEWD(nb); m->damage = NEWD(nb);
     for (int b = 0; b < nb; b++) m->bfms[b] = 1.;
     int nn = m->nn = d->n_nodes;
     m->X0 = dupd(d->node_x0, 2 * (size_t)nn); m->mass = dupd(d->node_mass, 2 * (size_t)nn); m->invm = dupd(d->node_inv_mass, 2 * (size_t)nn);

@@ -49,6 +49,15 @@ void orc_solver_stats(orc_model* m, double* out5);
 void orc_set_rsqrt_mode(int correctly_rounded);
 /* body statuses (MEL_STATUS_*), which Update_status changes after proximity updates */
 void orc_get_body_status(const orc_model* m, int* status);
+/* Body::damage of every body, as Update_damage left it (0 until a Damage entry is evaluated) */
+void orc_get_damage(orc_model* m, double* out);
+/* Body::Update_damage of body b (the Damage entry of Monitoring), returning the new damage */
+double orc_update_damage(orc_model* m, int b);
+/* Monitoring's Damage entries for the listed bodies: after every later step, before its proximity
+ * update, Update_damage of each is logged (at most cap steps); orc_damage_log copies the log and
+ * returns its steps */
+void orc_monitor_damage(orc_model* m, const int* bodies, int n, int cap);
+int orc_damage_log(orc_model* m, double* out);
 
 #ifdef __cplusplus
 }

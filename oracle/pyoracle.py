@@ -38,7 +38,7 @@ def lib():
         L.orc_n_contacts.argtypes = [vp]
         L.orc_get_contacts.argtypes = [vp, C.POINTER(abi.MelContact), C.c_int]
         L.orc_set_contacts.argtypes = [vp, C.POINTER(abi.MelContact), C.c_int]
-        for f in ("orc_get_node_state", "orc_set_node_state", "orc_get_positions", "orc_get_works", "orc_set_rigid"):
+        for f in ("orc_get_node_state", "orc_set_node_state", "orc_get_positions", "orc_get_works", "orc_set_rigid", "orc_get_damage"):
             getattr(L, f).argtypes = [vp, C.POINTER(C.c_double)]
         L.orc_get_forces.argtypes = [vp] + [C.POINTER(C.c_double)] * 5
         L.orc_get_rigid.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -123,6 +123,30 @@ class Oracle:
     def body_status(self) -> np.ndarray:
         a = np.zeros(self.nb, dtype=np.int32)
         self.L.orc_get_body_status(self.h, a.ctypes.data_as(C.POINTER(C.c_int)))
+        return a
+
+    def update_damage(self, b: int) -> float:
+        self.L.orc_update_damage.argtypes = [C.c_void_p, C.c_int]
+        self.L.orc_update_damage.restype = C.c_double
+        return self.L.orc_update_damage(self.h, int(b))
+
+    def monitor_damage(self, bodies, cap: int = 10000):
+        b = np.ascontiguousarray(bodies, dtype=np.int32)
+        self.L.orc_monitor_damage.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_int]
+        self.L.orc_monitor_damage(self.h, b.ctypes.data_as(C.POINTER(C.c_int)), len(b), int(cap))
+        self._dmg = (len(b), cap)
+
+    def damage_log(self) -> np.ndarray:
+        n, cap = self._dmg
+        out = np.zeros(cap * n)
+        self.L.orc_damage_log.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        self.L.orc_damage_log.restype = C.c_int
+        k = self.L.orc_damage_log(self.h, _dp(out))
+        return out[: k * n].reshape(k, n)
+
+    def damage(self) -> np.ndarray:
+        a = np.zeros(self.nb)
+        self.L.orc_get_damage(self.h, _dp(a))
         return a
 
     def positions(self) -> np.ndarray:

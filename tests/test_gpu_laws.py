@@ -219,6 +219,38 @@ def test_alid_layers_bit_identical(gpu_lib, oracle_built):
     gs.close()
 
 
+def test_damage_deactivation_and_monitoring(gpu_lib, oracle_built):
+    """Damage (Body::Update_damage, Code/Body.h:2667-2700) on bonded contacts.  DEACTIVATION on
+    damage: the free rigid disc (no contact, damage 1) turns inactive at the first update and the
+    loaded discs' entries never hold, as in the oracle (pinned to the compiled reference on this
+    case); the trajectories stay bit-identical.  Monitoring's Damage entries (Monitoring.h:385-390)
+    of two loaded discs, one row per step, equal the oracle's Update_damage evaluated where
+    Monitoring runs (after each step, before its proximity update), bit for bit, and vary."""
+    from melody2d_b200 import generator as g
+    from melody2d_b200.solver import Solver
+    from oracle.pyoracle import Oracle
+    from test_oracle_laws import case_scene
+    flat = g.flatten(case_scene("deactivation_damage"))
+    gs = Solver.from_flat(flat)
+    o = Oracle(flat, correctly_rounded=True)
+    gs.monitor_setup([[8, 0], [8, 4]], ring_rows=200, first_iteration=0)
+    o.monitor_damage([0, 4], cap=200)
+    for _ in range(10):
+        gs.step(10)
+        o.step(10)
+        np.testing.assert_array_equal(gs.body_status(), o.body_status())
+        np.testing.assert_array_equal(gs.node_state(), o.node_state())
+        assert_contacts_equal(gs.contacts(), o.contacts())
+    rows = gs.monitor_rows()
+    got = np.array([r[6:8] for r in rows])
+    want = o.damage_log()
+    assert got.shape == want.shape == (100, 2)
+    np.testing.assert_array_equal(got, want)
+    assert len(np.unique(got[:, 1])) > 1 and got.min() < 1.0
+    assert np.nonzero(gs.body_status() == 1)[0].tolist() == [11]
+    gs.close()
+
+
 def test_deactivation_bit_identical(gpu_lib, oracle_built):
     """DEACTIVATION entries (Update_status after each proximity update, Code/Proximity.h:550-1007):
     a free rigid disc beside the pressed lattice turns inactive by its displacement at the same

@@ -43,7 +43,7 @@ CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7
                                                     "border_conditions", "biaxial12_s5", "biaxial12_s7",
                                                     "periodic", "rotor", "adaptive_euler", "euler_2",
                                                     "mass_scaling", "adaptive_mass_scaling", "damping",
-                                                    "deactivation", "alid"]
+                                                    "deactivation", "alid", "deactivation_damage"]
 
 # Solver_step schemes (Code/Solver.h:98-486) with their parameters: Target_error, Control_parameter,
 # Accepted_ratio, Max_mass_scaling, Control_parameter_mass_scaling, Error_factor_mass_scaling,
@@ -91,6 +91,19 @@ def case_scene(name):
         # Rayleigh damping matrices on the grains (MATRICES, Body::Update_damping_forces)
         E, nu = 1e8, 0.3
         g.add_damping(sc, 0.02 * sc.dt, 0.05 / sc.dt, E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu)))
+    elif name == "deactivation_damage":
+        # Update_status on damage (Update_damage, Code/Body.h:2667-2700) with bonded contacts
+        # (BondedMohrCoulomb after INITIALIZE_CZM, whose internal[0] the damage averages): two
+        # entries evaluate the damage of loaded discs and never hold; a free rigid disc flying beside
+        # the lattice (body 11, no contact: damage 1) turns inactive at the first update
+        sc.laws = [(m1, m2, 5, 0, list(LAW_PARAMS[5])) for (m1, m2, _, _, _) in sc.laws]
+        sc.initialize_czm = True
+        xmax = max(b.nodes[:, 0].max() for b in sc.bodies)
+        ymid = 0.5 * (min(b.nodes[:, 1].min() for b in sc.bodies) + max(b.nodes[:, 1].max() for b in sc.bodies))
+        h = 2.0 * np.pi * 0.8e-3 / 32
+        sc.bodies.append(g.make_rigid_disc((xmax + 4e-3, ymid), 0.8e-3, 32, 1, 7800.0, 0.5 * h, 0.5 * h,
+                                           velocity=(0.01, 0.0)))
+        sc.deactivation = ["Damage 0 above 2", "Damage 4 below 0.5", "Damage 11 above 0.99"]
     elif name == "alid":
         # ALID absorbing layers on every grain: layers 0.9 mm wide along the lattice's outline,
         # graded quadratically, reference velocities of the layer in x and y; the stiffness
