@@ -306,7 +306,7 @@ def run_ours(args, rank, world, local, pg):
 
 
 def headline_extras(args, rank, world, local, pg):
-    """The north-star figures beside the single-sample line (one GPU): a slice of the batched
+    """The batched and serving figures beside the single-sample line (one GPU): a slice of the batched
     workload in one mixed-precision batch against the plain FP64 path one sample at a time (samples
     per hour extrapolated to the workload's 20,000 steps per sample, and the mixed form's errors),
     and a short serving run (p50/p99 latency, samples per hour of both arms)."""
