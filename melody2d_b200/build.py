@@ -21,7 +21,7 @@ EXE = os.path.join(HERE, "melody_gpu")
 BUILD = os.path.join(HERE, "_build")
 
 CU_SOURCES = ["mel_kernels.cu", "mel_prox.cu", "mel_model.cu", "mel_noalloc.cu", "mel_monitor.cu", "mel_mls.cu"]
-CPP_SOURCES = ["mel_loader.cpp", "mel_chunks.cpp"]
+CPP_SOURCES = ["mel_loader.cpp", "mel_chunks.cpp", "mel_material.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -15,6 +15,7 @@
 #include "mel_internal.h"
 #include "mel_prox_host.h"
 #include "mel_chunks.h"
+#include "mel_material.h"
 #include "mel_host.h"   // .asc loader (mel_loader.cpp)
 #include "mel_sincos.h"
 
@@ -232,10 +233,6 @@ static mel_status validate(const mel_model_desc* d)
         }
         if (d->body_material[b] < 0 || d->body_material[b] >= d->n_materials) { mel_set_error("body %d material out of range", b); return MEL_ERR_INVALID; }
     }
-    if (d->flags[5] == 1 || d->flags[6] == 1) {
-        mel_set_error("UPDATE_STIFFNESS_MATRIX / UPDATE_DAMPING_MATRIX (matrices rebuilt by Body::Update_material) are not supported on the GPU path");
-        return MEL_ERR_UNSUPPORTED;
-    }
     if (d->n_matrix > 0) {
         if (!d->body_matrix_ptr || d->body_matrix_ptr[d->n_bodies] != d->n_matrix) { mel_set_error("body_matrix_ptr does not cover the matrix entries"); return MEL_ERR_INVALID; }
         for (int b = 0; b < d->n_bodies; b++) {
@@ -444,6 +441,15 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
             h->rg_mat[(size_t)b * MEL_RIGID_NF + MEL_RG_INV_MASS] = 1 / bm;
         }
     }
+    // MATRICES entries, with the stiffness and damping updates of Body::Update_material applied
+    // (UPDATE_STIFFNESS_MATRIX, UPDATE_DAMPING_MATRIX; the damping takes the masses above)
+    std::vector<double> mk, mc;
+    if (d->n_matrix > 0) {
+        mk.assign(d->matrix_stiffness, d->matrix_stiffness + d->n_matrix);
+        mc.assign(d->matrix_damping, d->matrix_damping + d->n_matrix);
+        mel_status st = mel_update_matrices(d, mass.data(), mk.data(), mc.data());
+        if (st != MEL_OK) return st;
+    }
     h->X0.assign(d->node_x0, d->node_x0 + 2 * (size_t)nn);
     D.X0 = (const double2*)dupload(h, d->node_x0, 2 * (size_t)nn);
     D.mass = (const double2*)dupload(h, mass);
@@ -469,7 +475,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
                     const int dof0 = d->matrix_dofs[2 * i], dof1 = d->matrix_dofs[2 * i + 1];
                     const int a = 2 * (n0 + dof0 / 2), c = 2 * (n0 + dof1 / 2);
                     const int dir0 = dof0 % 2, dir1 = dof1 % 2;
-                    const double cf = d->matrix_damping[i];
+                    const double cf = mc[i];
                     emit(a + dir0, c + dir1, cf);                               // node0 receives from node1
                     if (dir0 != dir1 || dof0 != dof1) emit(c + dir1, a + dir0, cf); // and node1 from node0
                 }
@@ -511,7 +517,7 @@ static mel_status build(mel_handle* h, const mel_model_desc* d, const mel_option
                         const int dof0 = d->matrix_dofs[2 * i], dof1 = d->matrix_dofs[2 * i + 1];
                         const int a = n0 + dof0 / 2, c = n0 + dof1 / 2;
                         const int dir0 = dof0 % 2, dir1 = dof1 % 2;
-                        const double cf = d->matrix_stiffness[i] / (1. / ab[2 * a] + 1. / ab[2 * c]);
+                        const double cf = mk[i] / (1. / ab[2 * a] + 1. / ab[2 * c]);
                         if (fl[dir0]) emit(2 * a + dir0, 2 * c + dir1, cf);
                         if ((dir0 != dir1 || dof0 != dof1) && fl[dir1]) emit(2 * c + dir1, 2 * a + dir0, cf);
                     }

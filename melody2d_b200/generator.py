@@ -415,6 +415,7 @@ class Scene:
     solver_params: Tuple[float, ...] = (1e-3, 0.2, 1.0, 100.0, 1.0, 1.0, 0.99, 1e3)
     self_contact: bool = True
     initialize_czm: bool = False    # INITIALIZE_CZM: internal variables of the set-up contacts (Code/Proximity.h:481)
+    update_matrices: Tuple[bool, bool, bool] = (False, False, False)   # UPDATE_MASS/STIFFNESS/DAMPING_MATRIX (Code/IO.h:1920-1925)
     # output control: MONITORING entries as STATIC_CONTROL lines (the Read_spy_line grammar,
     # Code/IO.h:11-590), MONITOR_ENERGY / MONITOR_BOUNDARIES, Save_period and Print_period (None:
     # one save and one print at the end)
@@ -723,6 +724,8 @@ def flatten(scene: Scene) -> Dict[str, np.ndarray]:
         flags[8] = 1                      # NO_MONITORING (also disables self contact, Proximity.h:332)
     if scene.initialize_czm:
         flags[3] = 1                      # INITIALIZE_CZM
+    for k, on in enumerate(scene.update_matrices):
+        flags[4 + k] = int(bool(on))      # rebuilt by Body::Update_material (Code/Body.h:2708-2875)
     flags[1] = int(scene.monitor_energy)
     flags[2] = int(scene.monitor_boundaries)
     f["flags"] = flags
@@ -978,6 +981,9 @@ def write_asc(scene: Scene, directory: str, workers: int = 1) -> None:
             fh.write("MONITOR_BOUNDARIES\n")
         if scene.initialize_czm:
             fh.write("INITIALIZE_CZM\n")
+        for on, kw in zip(scene.update_matrices, ("UPDATE_MASS_MATRIX", "UPDATE_STIFFNESS_MATRIX", "UPDATE_DAMPING_MATRIX")):
+            if on:
+                fh.write(kw + "\n")
         fh.write(" \n")
         for text in _collect(parts, 1):
             fh.write(text)

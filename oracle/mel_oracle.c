@@ -473,8 +473,73 @@ static void initialize_segments(orc_model* m, int b)
     }
 }
 
-/* Body::Update_material (Code/Body.h:2708-2906); the stiffness re-assembly (flags[5]) needs the
- * MATRICES triplets and is done only when they are present. */
+/* The stiffness re-assembly of Body::Update_material (Code/Body.h:2784-2859): E and Nu from the
+ * material (Body.h:2727-2746), the plane-strain elasticity matrix scaled by E/((1+Nu)(1-2Nu)), and per
+ * Gauss point the local matrix of the support's dofs, each entry summed from 0 in the reference's
+ * four-term order; every upper-triangle pair (dof0 <= dof1) adds L*weight*jacobian into the first
+ * MATRICES entry with those dofs (pairs without an entry are dropped).  The first-entry lookup is a
+ * dense table over the body's dof pairs instead of the reference's linear search; the sums are
+ * the same. */
+static void assemble_stiffness(orc_model* m, int b)
+{
+    const double* P = m->mat_p + MEL_MAT_NPARAM * m->bmat[b];
+    double E = 0., Nu = 0.;
+    if (m->mat_type[m->bmat[b]] == MEL_MAT_ELASTIC_LINEAR) {
+        double Mu = P[3], Lambda = P[4];
+        E = Mu * (3. * Lambda + 2. * Mu) / (Lambda + Mu);
+        Nu = Mu / (2. * Lambda + 2. * Mu);
+    } else if (m->mat_type[m->bmat[b]] == MEL_MAT_NEOHOOKEAN) {
+        double Mu = P[3], Kappa = P[4];
+        E = 9. * Kappa * Mu / (3. * Kappa + Mu);
+        Nu = (3. * Kappa - 2. * Mu) / (6. * Kappa + 2. * Mu);
+    }
+    double C[3][3] = { { 1. - Nu, Nu, 0 }, { Nu, 1. - Nu, 0 }, { 0, 0, 1. - 2. * Nu } };
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) C[i][j] *= E / ((1. + Nu) * (1. - 2. * Nu));
+    const int nd = 2 * nb_nodes(m, b);
+    int* first = (int*)malloc(sizeof(int) * (size_t)nd * nd);
+    for (size_t k = 0; k < (size_t)nd * nd; k++) first[k] = -1;
+    for (int i = m->mx_ptr[b + 1] - 1; i >= m->mx_ptr[b]; i--) {
+        m->mx_k[i] = 0.;
+        first[(size_t)m->mx_dofs[2 * i] * nd + m->mx_dofs[2 * i + 1]] = i;
+    }
+    for (int g = m->gptr[b]; g < m->gptr[b + 1]; g++) {
+        const int s0 = m->gsp[g], nin = m->gsp[g + 1] - s0;
+        const double* xd = m->gdx + s0; const double* yd = m->gdy + s0;
+        double* L = (double*)calloc((size_t)4 * nin * nin, sizeof(double));
+        const int w = 2 * nin;
+        for (int ii = 0; ii < nin; ii++)
+            for (int jj = 0; jj < nin; jj++) {
+                double* e = L + (size_t)(2 * ii) * w + 2 * jj;       /* x row, x column */
+                *e += xd[ii] * C[0][0] * xd[jj]; *e += xd[ii] * C[0][2] * yd[jj];
+                *e += yd[ii] * C[2][0] * xd[jj]; *e += yd[ii] * C[2][2] * yd[jj];
+                e = L + (size_t)(2 * ii) * w + 2 * jj + 1;           /* x row, y column */
+                *e += xd[ii] * C[0][1] * yd[jj]; *e += xd[ii] * C[0][2] * xd[jj];
+                *e += yd[ii] * C[2][1] * yd[jj]; *e += yd[ii] * C[2][2] * xd[jj];
+                e = L + (size_t)(2 * ii + 1) * w + 2 * jj;           /* y row, x column */
+                *e += yd[ii] * C[1][0] * xd[jj]; *e += yd[ii] * C[1][2] * yd[jj];
+                *e += xd[ii] * C[2][0] * xd[jj]; *e += xd[ii] * C[2][2] * yd[jj];
+                e = L + (size_t)(2 * ii + 1) * w + 2 * jj + 1;       /* y row, y column */
+                *e += yd[ii] * C[1][1] * yd[jj]; *e += yd[ii] * C[1][2] * xd[jj];
+                *e += xd[ii] * C[2][1] * yd[jj]; *e += xd[ii] * C[2][2] * xd[jj];
+            }
+        for (int i = 0; i < w; i++) {
+            const int dof0 = 2 * m->gsi[s0 + i / 2] + (i - 2 * (i / 2));
+            for (int j = 0; j < w; j++) {
+                const int dof1 = 2 * m->gsi[s0 + j / 2] + (j - 2 * (j / 2));
+                if (dof1 < dof0) continue;
+                const int n = first[(size_t)dof0 * nd + dof1];
+                if (n >= 0) m->mx_k[n] += L[(size_t)i * w + j] * m->gw[g] * m->gJ[g];
+            }
+        }
+        free(L);
+    }
+    free(first);
+}
+
+/* Body::Update_material (Code/Body.h:2708-2906): masses (flags[4]), stiffness (flags[5]) and
+ * damping (flags[6]) entries rebuilt from the material, in that order; the matrix updates act on
+ * the MATRICES triplets and are skipped when there are none. */
 static void update_material(orc_model* m, int b)
 {
     const double* P = m->mat_p + MEL_MAT_NPARAM * m->bmat[b];
@@ -501,6 +566,7 @@ static void update_material(orc_model* m, int b)
                 rg[MEL_RG_INV_MASS] = 1 / rg[MEL_RG_MASS];
             }
         }
+        if (m->flags[5] == 1 && m->mx_ptr) assemble_stiffness(m, b);
         if (m->flags[6] == 1 && m->mx_ptr) {
             for (int i = m->mx_ptr[b]; i < m->mx_ptr[b + 1]; i++) {
                 int d0 = m->mx_dofs[2 * i], d1 = m->mx_dofs[2 * i + 1];
@@ -1835,6 +1901,13 @@ static double update_damage(orc_model* m, int b)
     return dmg;
 }
 void orc_get_damage(orc_model* m, double* out) { memcpy(out, m->damage, sizeof(double) * m->nb); }
+int orc_get_matrices(orc_model* m, double* k, double* c)
+{
+    if (!m->mx_ptr) return 0;
+    memcpy(k, m->mx_k, sizeof(double) * m->nmx);
+    memcpy(c, m->mx_c, sizeof(double) * m->nmx);
+    return m->nmx;
+}
 double orc_update_damage(orc_model* m, int b) { return update_damage(m, b); }
 
 /* Update_status (Code/Proximity.h:550-1007): entries of type position, displacement, velocity,

@@ -51,6 +51,8 @@ void orc_set_rsqrt_mode(int correctly_rounded);
 void orc_get_body_status(const orc_model* m, int* status);
 /* Body::damage of every body, as Update_damage left it (0 until a Damage entry is evaluated) */
 void orc_get_damage(orc_model* m, double* out);
+/* the MATRICES stiffness and damping entries after the set-up (n_matrix each); 0 when there are none */
+int orc_get_matrices(orc_model* m, double* k, double* c);
 /* Body::Update_damage of body b (the Damage entry of Monitoring), returning the new damage */
 double orc_update_damage(orc_model* m, int b);
 /* Monitoring's Damage entries for the listed bodies: after every later step, before its proximity

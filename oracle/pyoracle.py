@@ -149,6 +149,15 @@ class Oracle:
         self.L.orc_get_damage(self.h, _dp(a))
         return a
 
+    def matrices(self, n_matrix: int):
+        """The MATRICES stiffness and damping entries as the set-up left them (after the updates
+        of Body::Update_material)."""
+        k, c = np.zeros(n_matrix), np.zeros(n_matrix)
+        self.L.orc_get_matrices.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        self.L.orc_get_matrices.restype = C.c_int
+        assert self.L.orc_get_matrices(self.h, _dp(k), _dp(c)) == n_matrix
+        return k, c
+
     def positions(self) -> np.ndarray:
         a = np.zeros(2 * self.nn)
         self.L.orc_get_positions(self.h, _dp(a))

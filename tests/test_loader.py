@@ -27,19 +27,22 @@ def test_missing_files_report_io_error(tmp_path, gpu_lib):
 
 def test_asc_roundtrip_matrices_deactivation_alid(tmp_path, gpu_lib):
     """MATRICES (Code/IO.h:1827-1851) and DEACTIVATION entries (Read_spy_line plus below / equal /
-    above and the threshold, Code/IO.h:947-968) read back as the generator encoded them."""
+    above and the threshold, Code/IO.h:947-968) read back as the generator encoded them, and so do
+    the UPDATE_MASS/STIFFNESS/DAMPING_MATRIX lines of DYNAMIC (flags[4..6], Code/IO.h:1920-1925)."""
     import sys, os
     sys.path.insert(0, os.path.dirname(__file__))
     from melody2d_b200 import generator as g, solver
     from test_oracle_laws import case_scene
-    for name in ("damping", "deactivation", "alid"):
+    for name in ("damping", "deactivation", "alid", "update_matrices"):
         scene = case_scene(name)
         d_ = tmp_path / name
         g.write_asc(scene, str(d_))
         d = solver.load_desc_arrays(str(d_))
         f = g.flatten(scene)
-        keys = ["body_matrix_ptr", "matrix_dofs", "matrix_stiffness", "matrix_damping", "deactivated"]
-        if name == "alid":
+        keys = ["body_matrix_ptr", "matrix_dofs", "matrix_stiffness", "matrix_damping", "deactivated", "flags"]
+        if name == "update_matrices":
+            assert list(np.asarray(d["flags"])[4:7]) == [1, 1, 1]
+        if name in ("alid", "update_matrices"):
             # the ALID block (Code/IO.h:1395-1480) and the nodal coefficients the loader computes
             # from the initial positions (Code/IO.h:1548-1600), equal to the generator's
             keys += ["body_alid_ptr", "alid_time", "alid_value", "node_alid"]

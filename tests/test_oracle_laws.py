@@ -43,7 +43,8 @@ CASES = [f"law{l}" for l in sorted(LAW_PARAMS)] + ["law5+czm", "law6+czm", "law7
                                                     "border_conditions", "biaxial12_s5", "biaxial12_s7",
                                                     "periodic", "rotor", "adaptive_euler", "euler_2",
                                                     "mass_scaling", "adaptive_mass_scaling", "damping",
-                                                    "deactivation", "alid", "deactivation_damage"]
+                                                    "deactivation", "alid", "deactivation_damage",
+                                                    "update_matrices"]
 
 # Solver_step schemes (Code/Solver.h:98-486) with their parameters: Target_error, Control_parameter,
 # Accepted_ratio, Max_mass_scaling, Control_parameter_mass_scaling, Error_factor_mass_scaling,
@@ -104,12 +105,19 @@ def case_scene(name):
         sc.bodies.append(g.make_rigid_disc((xmax + 4e-3, ymid), 0.8e-3, 32, 1, 7800.0, 0.5 * h, 0.5 * h,
                                            velocity=(0.01, 0.0)))
         sc.deactivation = ["Damage 0 above 2", "Damage 4 below 0.5", "Damage 11 above 0.99"]
-    elif name == "alid":
+    elif name in ("alid", "update_matrices"):
         # ALID absorbing layers on every grain: layers 0.9 mm wide along the lattice's outline,
         # graded quadratically, reference velocities of the layer in x and y; the stiffness
-        # matrices (MATRICES, no damping) give the layers' coupling terms
-        E, nu = 1e8, 0.3
+        # matrices (MATRICES, no damping) give the layers' coupling terms.  update_matrices: the
+        # file's matrices come from half the grains' modulus and carry no damping, and
+        # UPDATE_MASS/STIFFNESS/DAMPING_MATRIX rebuild masses, stiffness and Rayleigh damping
+        # from the material (Body::Update_material), whose alpha and beta are set
+        E, nu = (1e8, 0.3) if name == "alid" else (0.5e8, 0.3)
         g.add_damping(sc, 0.0, 0.0, E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu)))
+        if name == "update_matrices":
+            sc.update_matrices = (True, True, True)
+            sc.materials = [(n, t, [p[0], 0.02 * sc.dt, 0.05 / sc.dt] + list(p[3:])) if n == "Grain" else (n, t, p)
+                            for (n, t, p) in sc.materials]
         grains = [b for b in sc.bodies if b.kind == "deformable"]
         x0 = min(b.nodes[:, 0].min() for b in grains); x1 = max(b.nodes[:, 0].max() for b in grains)
         y0 = min(b.nodes[:, 1].min() for b in grains); y1 = max(b.nodes[:, 1].max() for b in grains)
