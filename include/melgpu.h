@@ -147,8 +147,9 @@ typedef struct mel_model_desc {
     int           n_matrix;
     const int*    body_matrix_ptr;      /* [n_bodies+1] or NULL when n_matrix == 0 */
     const int*    matrix_dofs;          /* [2*n_matrix] */
-    const double* matrix_stiffness;
-    const double* matrix_damping;
+    const double* matrix_stiffness;     /* as in the file: with flags[5] / flags[6] (UPDATE_STIFFNESS_MATRIX, */
+    const double* matrix_damping;       /* UPDATE_DAMPING_MATRIX) mel_create rebuilds its own copies from the
+                                           material (Body::Update_material, Code/Body.h:2784-2875) */
     /* DEACTIVATION entries of STATIC_CONTROL (Code/IO.h:947-968): the vector Read_spy_line builds,
      * then the comparison (0 below, 1 equal, 2 above) and the threshold, zero-padded to
      * MEL_DEACT_NF doubles; Update_status (Code/Proximity.h:550-1007) applies them after every
